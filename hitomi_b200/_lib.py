@@ -1,0 +1,87 @@
+"""ctypes binding of the C ABI in include/hitomi_gpu.h.
+
+The shared library is built in-tree (hitomi_b200/build.py).  There is no fallback:
+if the library is missing or a GPU call fails, the error surfaces to the caller.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhitomi_b200.so")
+
+# exported symbols, in include/hitomi_gpu.h order
+SYMBOLS = (
+    "hg_create",
+    "hg_destroy",
+    "hg_last_error",
+    "hg_set_particles",
+    "hg_pk_box",
+    "hg_bk_box",
+    "hg_zeta_box",
+    "hg_survey_scalars",
+    "hg_pk_survey",
+    "hg_last_timing",
+)
+
+HG_NGP, HG_CIC, HG_TSC, HG_PCS = 0, 1, 2, 3
+HG_FP64, HG_FP32 = 0, 1
+
+
+class HgConfig(ctypes.Structure):
+    _fields_ = [
+        ("n_mesh", ctypes.c_int * 3),
+        ("boxsize", ctypes.c_double * 3),
+        ("assign", ctypes.c_int),
+        ("interlace", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("kmin", ctypes.c_double),
+        ("kmax", ctypes.c_double),
+        ("n_kbin", ctypes.c_int),
+        ("rmin", ctypes.c_double),
+        ("rmax", ctypes.c_double),
+        ("n_rbin", ctypes.c_int),
+        ("periodic", ctypes.c_int),
+        ("device", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Load the library once.  Raises OSError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise OSError(f"hitomi_b200 CUDA library not built: {p} is missing (run python hitomi_b200/build.py)")
+    lib = ctypes.CDLL(p)
+    c_dp = ctypes.POINTER(ctypes.c_double)
+    c_ip = ctypes.POINTER(ctypes.c_int)
+    vp = ctypes.c_void_p
+    lib.hg_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(HgConfig)]
+    lib.hg_create.restype = ctypes.c_int
+    lib.hg_destroy.argtypes = [vp]
+    lib.hg_destroy.restype = ctypes.c_int
+    lib.hg_last_error.argtypes = [vp]
+    lib.hg_last_error.restype = ctypes.c_char_p
+    lib.hg_set_particles.argtypes = [vp, ctypes.c_int, c_dp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int]
+    lib.hg_set_particles.restype = ctypes.c_int
+    lib.hg_pk_box.argtypes = [vp, ctypes.c_int, c_dp, c_ip, c_dp]
+    lib.hg_pk_box.restype = ctypes.c_int
+    lib.hg_bk_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, c_dp]
+    lib.hg_bk_box.restype = ctypes.c_int
+    lib.hg_zeta_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, c_dp]
+    lib.hg_zeta_box.restype = ctypes.c_int
+    lib.hg_survey_scalars.argtypes = [vp, c_dp, c_dp, c_dp, c_dp, c_dp]
+    lib.hg_survey_scalars.restype = ctypes.c_int
+    lib.hg_pk_survey.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, c_dp, c_ip, c_dp]
+    lib.hg_pk_survey.restype = ctypes.c_int
+    lib.hg_last_timing.argtypes = [vp, c_dp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.hg_last_timing.restype = ctypes.c_int
+    _lib = lib
+    return lib

@@ -1,0 +1,160 @@
+"""Python host API over the C ABI (include/hitomi_gpu.h).
+
+`Context` owns one hg_ctx (one GPU, one precision form).  Its methods return the
+reference's raw FP64 sums (pk_save, bk_save, sn_save) as complex numpy arrays plus the
+normalisation factor, so `norm * pk_save` is what the reference prints to pk{l}.dat
+(src/hitomi_measurement/powerspec.hpp:316-327) and `norm * (bk_save - sn_save)` what it
+prints to bk{l1}{l2}{L}_{ith}.dat (bispec.hpp:1184-1196).
+
+Errors follow the reference's int-status convention at the ABI; here a non-zero status
+raises HitomiError with the library's message.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+
+ASSIGN = {"NGP": _lib.HG_NGP, "CIC": _lib.HG_CIC, "TSC": _lib.HG_TSC, "PCS": _lib.HG_PCS}
+PRECISION = {"fp64": _lib.HG_FP64, "fp32": _lib.HG_FP32}
+
+
+class HitomiError(RuntimeError):
+    pass
+
+
+@dataclass
+class Binning:
+    kmin: float
+    kmax: float
+    n_kbin: int
+    rmin: float = 30.0
+    rmax: float = 150.0
+    n_rbin: int = 25
+
+    def kbin(self) -> np.ndarray:
+        """ToolClass::setKbin (tools.hpp:118-124)."""
+        dk = (self.kmax - self.kmin) / float(self.n_kbin - 1)
+        return np.array([self.kmin + dk * float(i) for i in range(self.n_kbin)])
+
+    def rbin(self) -> np.ndarray:
+        """ToolClass::setRbin (tools.hpp:126-132)."""
+        dr = (self.rmax - self.rmin) / float(self.n_rbin - 1)
+        return np.array([self.rmin + dr * float(i) for i in range(self.n_rbin)])
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Context:
+    def __init__(self, n_mesh, boxsize, binning: Binning, assign: str = "TSC", precision: str = "fp64",
+                 periodic: bool = False, interlace: bool = False, device: int = 0):
+        self._lib = _lib.load()
+        cfg = _lib.HgConfig()
+        nm = [int(n_mesh)] * 3 if np.isscalar(n_mesh) else [int(v) for v in n_mesh]
+        bs = [float(boxsize)] * 3 if np.isscalar(boxsize) else [float(v) for v in boxsize]
+        for a in range(3):
+            cfg.n_mesh[a] = nm[a]
+            cfg.boxsize[a] = bs[a]
+        if assign not in ASSIGN:
+            raise HitomiError(f"assignment must be one of {sorted(ASSIGN)}")
+        cfg.assign = ASSIGN[assign]
+        cfg.interlace = int(bool(interlace))
+        cfg.precision = PRECISION[precision]
+        cfg.kmin, cfg.kmax, cfg.n_kbin = binning.kmin, binning.kmax, binning.n_kbin
+        cfg.rmin, cfg.rmax, cfg.n_rbin = binning.rmin, binning.rmax, binning.n_rbin
+        cfg.periodic = int(bool(periodic))
+        cfg.device = int(device)
+        self.n_mesh, self.boxsize, self.binning = nm, bs, binning
+        self.precision = precision
+        h = ctypes.c_void_p()
+        if self._lib.hg_create(ctypes.byref(h), ctypes.byref(cfg)) != 0:
+            raise HitomiError(self._lib.hg_last_error(None).decode())
+        self._h = h
+        self._keep = {}
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise HitomiError(self._lib.hg_last_error(self._h).decode())
+
+    # -- particles
+    def set_particles(self, slot: int, arr: np.ndarray, pos_off: int = 0, los_off: int = -1, w_off: int = -1):
+        """arr: (n, fields) float64 array of structs, C-contiguous (e.g. x y z or x y z vx vy vz)."""
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.ndim != 2:
+            raise HitomiError("particle array must be 2-D (n, fields)")
+        self._keep[slot] = a
+        self._check(self._lib.hg_set_particles(self._h, slot, _dp(a), a.shape[0], a.shape[1] * 8, pos_off, los_off,
+                                               w_off))
+
+    # -- statistics
+    def pk_box(self, ell: int):
+        nk = self.binning.n_kbin
+        out = np.zeros(2 * nk)
+        nmode = np.zeros(nk, dtype=np.int32)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_pk_box(self._h, ell, _dp(out), nmode.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                        ctypes.byref(norm)))
+        return out[0::2] + 1j * out[1::2], nmode, norm.value
+
+    def bk_box(self, ell1: int, ell2: int, ELL: int, ith_kbin: int = -1):
+        nk = self.binning.n_kbin
+        rows = nk if ith_kbin < 0 else 1
+        bk = np.zeros(2 * rows * nk)
+        sn = np.zeros(2 * rows * nk)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_bk_box(self._h, ell1, ell2, ELL, ith_kbin, _dp(bk), _dp(sn), ctypes.byref(norm)))
+        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(rows, nk)
+        return c(bk), c(sn), norm.value
+
+    def zeta_box(self, ell1: int, ell2: int, ELL: int, ith_rbin: int = -1):
+        nr = self.binning.n_rbin
+        rows = nr if ith_rbin < 0 else 1
+        z = np.zeros(2 * rows * nr)
+        sn = np.zeros(2 * rows * nr)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_zeta_box(self._h, ell1, ell2, ELL, ith_rbin, _dp(z), _dp(sn), ctypes.byref(norm)))
+        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(rows, nr)
+        return c(z), c(sn), norm.value
+
+    def survey_scalars(self):
+        vals = [ctypes.c_double() for _ in range(5)]
+        self._check(self._lib.hg_survey_scalars(self._h, *[ctypes.byref(v) for v in vals]))
+        return tuple(v.value for v in vals)
+
+    def pk_survey(self, ell: int, alpha: float, vsurvey: float):
+        nk = self.binning.n_kbin
+        out = np.zeros(2 * nk)
+        nmode = np.zeros(nk, dtype=np.int32)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_pk_survey(self._h, ell, alpha, vsurvey, _dp(out),
+                                           nmode.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(norm)))
+        return out[0::2] + 1j * out[1::2], nmode, norm.value
+
+    def last_timing(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        self._lib.hg_last_timing(self._h, ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value

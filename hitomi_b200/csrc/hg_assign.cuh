@@ -1,0 +1,286 @@
+// hg_assign.cuh -- particle-to-mesh assignment (NGP/CIC/TSC, PCS extension) for sm_100a.
+//
+// Sorted-by-tile scatter with no global float atomics:
+//   1. k_bin_count   : per particle, the reference's cell/weight arithmetic in FP64
+//                      (field.hpp:80-90 NGP, :117-129 CIC, :158-172 TSC), the set of
+//                      output tiles its stencil touches, and the FP64 in-bounds mass;
+//   2. exclusive scan of the per-tile counts;
+//   3. k_bin_scatter : one compact record per (particle, tile) in tile order;
+//   4. k_tile_accum  : one CTA per tile accumulates its records in shared memory and
+//                      writes the tile exactly once, coalesced.
+// A particle whose stencil straddles tiles is duplicated into each of them; each CTA
+// keeps only the stencil points that fall in its own tile.
+//
+// Boundary rule.  The reference tests only 0 <= flat < N (field.hpp:92-96): an axis
+// index of -1 or n lands in the neighbouring row/plane rather than wrapping, and
+// points past either end of the array are dropped.  periodic = 0 reproduces that
+// (needed for parity); periodic = 1 wraps each axis (PCS / interlacing extension).
+#pragma once
+
+#include "hg_common.cuh"
+
+namespace hg {
+
+struct AssignGeom {
+    int n[3];
+    double L[3];
+    long long ntot;
+    int scheme;       // HG_NGP..HG_PCS
+    int periodic;     // 0 = reference flat-index rule
+    double shift;     // added to the scaled position (0, or 0.5 for the interlaced copy)
+    int t[3];         // tile extent per axis
+    int nt[3];        // tiles per axis
+    double factor;    // 1/dV (field.hpp:76-77)
+};
+
+__host__ __device__ __forceinline__ int stencil_width(int scheme) { return scheme + 1; }
+__host__ __device__ __forceinline__ int stencil_start(int scheme) { return (scheme >= 2) ? -1 : 0; }
+
+// Anchor index and offset per axis, exactly the reference's FP64 expressions.
+__device__ __forceinline__ void anchor(double pos, int n, double L, int scheme, double shift, int &i, double &d) {
+    double xp = pos * double(n) / L;
+    if (shift != 0.0) xp += shift;
+    if (scheme == 0) {          // NGP: iw = int(xp + 0.5)
+        i = int(xp + 0.5);
+        d = 0.0;
+    } else if (scheme == 1) {   // CIC: iw0 = int(xp), dx = xp - iw0
+        i = int(xp);
+        d = xp - double(i);
+    } else if (scheme == 2) {   // TSC: iw1 = int(xp + 0.5), dx = xp - iw1
+        i = int(xp + 0.5);
+        d = xp - double(i);
+    } else {                    // PCS: i = floor(xp), t = xp - i
+        i = (int)floor(xp);
+        d = xp - double(i);
+    }
+}
+
+// Stencil weights per axis (index 0 = first stencil point).
+template <typename T>
+__device__ __forceinline__ void axis_weights(int scheme, T d, T *w) {
+    if (scheme == 0) {
+        w[0] = (T)1;
+    } else if (scheme == 1) {
+        w[0] = (T)1 - d;
+        w[1] = d;
+    } else if (scheme == 2) {
+        w[0] = (T)0.5 * ((T)0.5 - d) * ((T)0.5 - d);
+        w[1] = (T)0.75 - d * d;
+        w[2] = (T)0.5 * ((T)0.5 + d) * ((T)0.5 + d);
+    } else {
+        T t = d, u = (T)1 - d;
+        w[0] = u * u * u / (T)6;
+        w[1] = ((T)4 - (T)6 * t * t + (T)3 * t * t * t) / (T)6;
+        w[2] = ((T)1 + (T)3 * t + (T)3 * t * t - (T)3 * t * t * t) / (T)6;
+        w[3] = t * t * t / (T)6;
+    }
+}
+
+// Effective cell of stencil point (ix, iy, iz); false if the reference drops it.
+__device__ __forceinline__ bool effective_cell(const AssignGeom &g, int ix, int iy, int iz, int &cx, int &cy, int &cz) {
+    if (g.periodic) {
+        cx = ((ix % g.n[0]) + g.n[0]) % g.n[0];
+        cy = ((iy % g.n[1]) + g.n[1]) % g.n[1];
+        cz = ((iz % g.n[2]) + g.n[2]) % g.n[2];
+        return true;
+    }
+    if (ix >= 0 && ix < g.n[0] && iy >= 0 && iy < g.n[1] && iz >= 0 && iz < g.n[2]) {
+        cx = ix;
+        cy = iy;
+        cz = iz;
+        return true;
+    }
+    long long coord = ((long long)ix * g.n[1] + iy) * (long long)g.n[2] + iz;
+    if (coord < 0 || coord >= g.ntot) return false;
+    long long nyz = (long long)g.n[1] * g.n[2];
+    cx = (int)(coord / nyz);
+    long long rem = coord - (long long)cx * nyz;
+    cy = (int)(rem / g.n[2]);
+    cz = (int)(rem - (long long)cy * g.n[2]);
+    return true;
+}
+
+__device__ __forceinline__ int tile_of(const AssignGeom &g, int cx, int cy, int cz) {
+    return ((cx / g.t[0]) * g.nt[1] + cy / g.t[1]) * g.nt[2] + cz / g.t[2];
+}
+
+struct PartSrc {
+    const unsigned char *base;  // device copy of the caller's array of structs
+    long long n;
+    long long stride;           // bytes
+    int pos_off;                // doubles
+    int w_off;                  // doubles, < 0: weight 1
+    const double2 *cw;          // optional per-particle complex weight (Y_lm-weighted), overrides w
+    double scale;               // multiplies the weight (e.g. -alpha for randoms)
+};
+
+__device__ __forceinline__ void load_particle(const PartSrc &s, long long p, double pos[3], double &wr, double &wi) {
+    const double *rec = reinterpret_cast<const double *>(s.base + p * s.stride);
+    pos[0] = rec[s.pos_off + 0];
+    pos[1] = rec[s.pos_off + 1];
+    pos[2] = rec[s.pos_off + 2];
+    if (s.cw) {
+        double2 c = s.cw[p];
+        wr = c.x;
+        wi = c.y;
+    } else {
+        wr = (s.w_off >= 0) ? rec[s.w_off] : 1.0;
+        wi = 0.0;
+    }
+    wr *= s.scale;
+    wi *= s.scale;
+}
+
+template <typename T>
+struct PRec {
+    int i[3];
+    T d[3];
+    T wr, wi;
+};
+
+// Enumerate the distinct tiles a particle's stencil touches.  Returns the count.
+__device__ __forceinline__ int particle_tiles(const AssignGeom &g, const int anc[3], int *tiles) {
+    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+    bool inside = true;
+    for (int a = 0; a < 3; a++) {
+        int lo = anc[a] + s0, hi = anc[a] + s0 + W - 1;
+        if (g.periodic || lo < 0 || hi >= g.n[a]) inside = false;
+    }
+    int nt = 0;
+    if (inside) {
+        int tlo[3], thi[3];
+        for (int a = 0; a < 3; a++) {
+            tlo[a] = (anc[a] + s0) / g.t[a];
+            thi[a] = (anc[a] + s0 + W - 1) / g.t[a];
+        }
+        for (int tx = tlo[0]; tx <= thi[0]; tx++)
+            for (int ty = tlo[1]; ty <= thi[1]; ty++)
+                for (int tz = tlo[2]; tz <= thi[2]; tz++) tiles[nt++] = (tx * g.nt[1] + ty) * g.nt[2] + tz;
+        return nt;
+    }
+    for (int a = 0; a < W; a++)
+        for (int b = 0; b < W; b++)
+            for (int c = 0; c < W; c++) {
+                int cx, cy, cz;
+                if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
+                int t = tile_of(g, cx, cy, cz);
+                bool seen = false;
+                for (int q = 0; q < nt; q++) seen |= (tiles[q] == t);
+                if (!seen) tiles[nt++] = t;
+            }
+    return nt;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Pass 1: tile counts + FP64 in-bounds mass  sum_p w_p factor prod(w_axis)  (the field's
+// exact integral, needed for the k = 0 mode since boundary drops lose mass).
+__global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double *mass) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double m_re = 0.0, m_im = 0.0;
+    if (p < src.n) {
+        double pos[3], wr, wi;
+        load_particle(src, p, pos, wr, wi);
+        int anc[3];
+        double d[3];
+        for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
+        int tiles[64];
+        int nt = particle_tiles(g, anc, tiles);
+        for (int q = 0; q < nt; q++) atomicAdd(&cnt[tiles[q]], 1u);
+        // in-bounds mass in the reference's product order
+        const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+        double w[3][4];
+        for (int a = 0; a < 3; a++) axis_weights<double>(g.scheme, d[a], w[a]);
+        for (int a = 0; a < W; a++)
+            for (int b = 0; b < W; b++)
+                for (int c = 0; c < W; c++) {
+                    int cx, cy, cz;
+                    if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
+                    m_re += wr * g.factor * w[0][a] * w[1][b] * w[2][c];
+                    m_im += wi * g.factor * w[0][a] * w[1][b] * w[2][c];
+                }
+    }
+    m_re = warp_sum_d(m_re);
+    m_im = warp_sum_d(m_im);
+    if ((threadIdx.x & 31) == 0 && (m_re != 0.0 || m_im != 0.0)) {
+        atomicAdd(&mass[0], m_re);
+        atomicAdd(&mass[1], m_im);
+    }
+}
+
+template <typename T>
+__global__ void k_bin_scatter(PartSrc src, AssignGeom g, const unsigned int *off, unsigned int *cursor, PRec<T> *rec) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= src.n) return;
+    double pos[3], wr, wi;
+    load_particle(src, p, pos, wr, wi);
+    int anc[3];
+    double d[3];
+    for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
+    int tiles[64];
+    int nt = particle_tiles(g, anc, tiles);
+    PRec<T> r;
+    for (int a = 0; a < 3; a++) {
+        r.i[a] = anc[a];
+        r.d[a] = (T)d[a];
+    }
+    r.wr = (T)wr;
+    r.wi = (T)wi;
+    for (int q = 0; q < nt; q++) {
+        unsigned int slot = atomicAdd(&cursor[tiles[q]], 1u);
+        rec[off[tiles[q]] + slot] = r;
+    }
+}
+
+// One CTA per tile.  ACC is the shared-memory accumulator type (float/double); the
+// mesh stores the density rho = sum_p w_p (1/dV) prod(w_axis) like the reference.
+template <typename T, bool CPLX>
+__global__ void k_tile_accum(const PRec<T> *rec, const unsigned int *off, AssignGeom g, T *mesh_re, T *mesh_im) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *acc = reinterpret_cast<T *>(smem_raw);
+    const int tcells = g.t[0] * g.t[1] * g.t[2];
+    T *acc_im = acc + tcells;
+    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
+    __syncthreads();
+    const int tile = blockIdx.x;
+    const int tz = tile % g.nt[2];
+    const int ty = (tile / g.nt[2]) % g.nt[1];
+    const int tx = tile / (g.nt[2] * g.nt[1]);
+    const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
+    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+    const unsigned int r0 = off[tile], r1 = off[tile + 1];
+    const T factor = (T)g.factor;
+    for (unsigned int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+        PRec<T> pr = rec[r];
+        T w[3][4];
+        for (int a = 0; a < 3; a++) axis_weights<T>(g.scheme, pr.d[a], w[a]);
+        for (int a = 0; a < W; a++)
+            for (int b = 0; b < W; b++)
+                for (int c = 0; c < W; c++) {
+                    int cx, cy, cz;
+                    if (!effective_cell(g, pr.i[0] + s0 + a, pr.i[1] + s0 + b, pr.i[2] + s0 + c, cx, cy, cz)) continue;
+                    int lx = cx - ox, ly = cy - oy, lz = cz - oz;
+                    if ((unsigned)lx >= (unsigned)g.t[0] || (unsigned)ly >= (unsigned)g.t[1] ||
+                        (unsigned)lz >= (unsigned)g.t[2])
+                        continue;
+                    int li = (lx * g.t[1] + ly) * g.t[2] + lz;
+                    T v = pr.wr * factor * w[0][a] * w[1][b] * w[2][c];
+                    atomicAdd(&acc[li], v);
+                    if (CPLX) atomicAdd(&acc_im[li], pr.wi * factor * w[0][a] * w[1][b] * w[2][c]);
+                }
+    }
+    __syncthreads();
+    for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
+        int lz = li % g.t[2];
+        int ly = (li / g.t[2]) % g.t[1];
+        int lx = li / (g.t[2] * g.t[1]);
+        long long cell = ((long long)(ox + lx) * g.n[1] + (oy + ly)) * g.n[2] + (oz + lz);
+        mesh_re[cell] = acc[li];
+        if (CPLX) mesh_im[cell] = acc_im[li];
+    }
+}
+
+}  // namespace hg

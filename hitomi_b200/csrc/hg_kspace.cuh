@@ -1,0 +1,457 @@
+// hg_kspace.cuh -- k-space and configuration-space kernels of the estimators.
+//
+//   k_axis_tables   per-axis sinc / sine tables with the reference's window index quirk
+//   k_pk_bin        binned  (f1 conj f2 - S C(k)) / W^2 * Yhat_lm(k)  (field.hpp:765-852)
+//   k_shell_D       delta(k)/W(k) for every (shell, mode) entry      (field.hpp:346-401)
+//   k_family_A      A_f,i(k) = Yhat_f(k) delta/W / n_i
+//   k_scatter_*     place k-space inputs on the (reduced) transform grid
+//   k_extract_neg   gather Qhat(-k) at the shell entries
+//   k_pair_dot      sum over a shell of A_a(k) Qhat_b(-k)
+//   k_xi_orbit_hist last inverse-FFT pass of the shot-noise correlation field fused with
+//                   its radial histogram over integer n^2 = |x/dr|^2
+//   k_bessel_table, k_sn_matrix   spline-evaluated j_l products summed over n^2
+#pragma once
+
+#include "hg_common.cuh"
+#include "hg_fft.cuh"
+
+namespace hg {
+
+// Per-axis tables indexed by array index i (mode n = wrap(i)):
+//   tw[i] = sinc(pi w / n)   with w = (int)(n dk / dk + 1e-5)   (window, field.hpp:664-675)
+//   ts[i] = sin(pi w / n)    (0 when w == 0)                   (shot noise, field.hpp:1261-1272)
+struct AxisTabs {
+    const double *tw[3];
+    const double *ts[3];
+};
+
+__global__ void k_axis_tables(Grid g, int axis, double *tw, double *ts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = g.n[axis];
+    if (i >= n) return;
+    double kv = kcomp(wrap_index(i, n), g.dk[axis]);
+    int w = window_index(kv, g.dk[axis]);
+    tw[i] = sinc_axis(w, n);
+    ts[i] = (w != 0) ? sin(HG_PI * (double)w / (double)n) : 0.0;
+}
+
+__device__ __forceinline__ double window_tab(const AxisTabs &t, int ix, int iy, int iz, int p) {
+    double ret = t.tw[0][ix] * t.tw[1][iy] * t.tw[2][iz];
+    double w = ret;
+    for (int q = 1; q < p; q++) w *= ret;
+    return w;
+}
+
+__device__ __forceinline__ double shot_tab(const AxisTabs &t, int ix, int iy, int iz, int assign) {
+    if (assign == 0) return 1.0;
+    const double s[3] = {t.ts[0][ix], t.ts[1][iy], t.ts[2][iz]};
+    double ret = 1.0;
+    for (int a = 0; a < 3; a++) {
+        double s2 = s[a] * s[a];
+        double f;
+        if (assign == 1) f = 1.0 - (2.0 / 3.0) * s2;
+        else if (assign == 2) f = 1.0 - s2 + 2.0 * (s2 * s2) / 15.0;
+        else f = 1.0 - (4.0 / 3.0) * s2 + (2.0 / 5.0) * s2 * s2 - (4.0 / 315.0) * s2 * s2 * s2;
+        ret *= f;
+    }
+    return ret;
+}
+
+// Read access to a transformed field, either a half spectrum [n0][n1][n2/2+1] of a real
+// input (negative kz by Hermitian symmetry) or a full [n0][n1][n2] spectrum.
+template <typename T>
+struct Spec {
+    const cplx<T> *p;
+    int n0, n1, n2;
+    int half;
+    __device__ __forceinline__ zd at(int ix, int iy, int iz) const {
+        if (!half) {
+            cplx<T> v = p[((long long)ix * n1 + iy) * n2 + iz];
+            return mk<double>((double)v.x, (double)v.y);
+        }
+        int hz = n2 / 2 + 1;
+        if (iz < hz) {
+            cplx<T> v = p[((long long)ix * n1 + iy) * hz + iz];
+            return mk<double>((double)v.x, (double)v.y);
+        }
+        int jx = (n0 - ix) % n0, jy = (n1 - iy) % n1, jz = n2 - iz;
+        cplx<T> v = p[((long long)jx * n1 + jy) * hz + jz];
+        return mk<double>((double)v.x, -(double)v.y);
+    }
+};
+
+struct LM {
+    int l, m;
+};
+
+#define HG_MAX_LM 16
+
+struct LMList {
+    int n;
+    LM lm[HG_MAX_LM];
+};
+
+// P-binning over the mode cube [lo, lo+cnt) (wrapped modes).  acc: [nbin][nlm] complex,
+// nmode: [nbin].  lut maps the fine index int(|k|/1e-4 + 0.5) to up to two coarse bins.
+template <typename T>
+__global__ void k_pk_bin(Spec<T> f1, Spec<T> f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt, const int2 *lut, int lutn,
+                         int nbin, LMList lms, double S_re, double S_im, int assign, int wpow, double *acc,
+                         unsigned long long *nmode, int k0_special, double k0_re, double k0_im) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sacc = reinterpret_cast<double *>(smem_raw);
+    unsigned long long *scnt = reinterpret_cast<unsigned long long *>(sacc + 2 * nbin * lms.n);
+    for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x) sacc[q] = 0.0;
+    for (int q = threadIdx.x; q < nbin; q += blockDim.x) scnt[q] = 0ull;
+    __syncthreads();
+    const long long total = (long long)cnt.x * cnt.y * cnt.z;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int nz = lo.z + (int)(idx % cnt.z);
+        int ny = lo.y + (int)((idx / cnt.z) % cnt.y);
+        int nx = lo.x + (int)(idx / ((long long)cnt.z * cnt.y));
+        int ix = (nx + g.n[0]) % g.n[0], iy = (ny + g.n[1]) % g.n[1], iz = (nz + g.n[2]) % g.n[2];
+        double kv[3] = {kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
+                        kcomp(wrap_index(iz, g.n[2]), g.dk[2])};
+        double kmag = kmag_exact(kv[0], kv[1], kv[2]);
+        int kindex = (int)__dadd_rn(__ddiv_rn(kmag, 0.0001), 0.5);
+        if (kindex >= lutn) continue;
+        int2 b = lut[kindex];
+        if (b.x < 0) continue;
+        zd d1 = f1.at(ix, iy, iz), d2 = f2.at(ix, iy, iz);
+        zd pk2;
+        if (k0_special && ix == 0 && iy == 0 && iz == 0) {
+            pk2 = mk<double>(k0_re, k0_im);
+        } else {
+            pk2 = d1 * conjg(d2);
+        }
+        double C = shot_tab(tabs, ix, iy, iz, assign);
+        pk2 = pk2 - mk<double>(S_re * C, S_im * C);
+        double wf = window_tab(tabs, ix, iy, iz, wpow);
+        double w2 = wf * wf;
+        pk2 = mk<double>(pk2.x / w2, pk2.y / w2);
+        for (int q = 0; q < lms.n; q++) {
+            zd y = ylm_reduced(lms.lm[q].l, lms.lm[q].m, kv[0], kv[1], kv[2]);
+            zd v = pk2 * y;
+            atomicAdd(&sacc[2 * (b.x * lms.n + q)], v.x);
+            atomicAdd(&sacc[2 * (b.x * lms.n + q) + 1], v.y);
+            if (b.y >= 0) {
+                atomicAdd(&sacc[2 * (b.y * lms.n + q)], v.x);
+                atomicAdd(&sacc[2 * (b.y * lms.n + q) + 1], v.y);
+            }
+        }
+        atomicAdd(&scnt[b.x], 1ull);
+        if (b.y >= 0) atomicAdd(&scnt[b.y], 1ull);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x)
+        if (sacc[q] != 0.0) atomicAdd(&acc[q], sacc[q]);
+    for (int q = threadIdx.x; q < nbin; q += blockDim.x)
+        if (scnt[q]) atomicAdd(&nmode[q], scnt[q]);
+}
+
+// Shell entries: wrapped mode (nx, ny, nz) and shell index.
+struct ShellEnt {
+    int nx, ny, nz, shell;
+};
+
+__device__ __forceinline__ int mod_idx(int n, int N) { return ((n % N) + N) % N; }
+
+template <typename T>
+__global__ void k_shell_D(const ShellEnt *ent, long long ne, Spec<T> f, Grid g, AxisTabs tabs, int wpow, double2 *D) {
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    ShellEnt s = ent[e];
+    int ix = mod_idx(s.nx, g.n[0]), iy = mod_idx(s.ny, g.n[1]), iz = mod_idx(s.nz, g.n[2]);
+    zd d = f.at(ix, iy, iz);
+    double wf = window_tab(tabs, ix, iy, iz, wpow);
+    D[e] = make_double2(d.x / wf, d.y / wf);
+}
+
+// A[e] = (Yhat_lm(k) * D[e]) * scale_shell[shell(e)]   (scale = 1/n_mode or a Bessel weight)
+__global__ void k_family_A(const ShellEnt *ent, long long ne, Grid g, int l, int m, const double2 *D,
+                           const double *shell_scale, double2 *A) {
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    ShellEnt s = ent[e];
+    zd y = ylm_reduced(l, m, kcomp(s.nx, g.dk[0]), kcomp(s.ny, g.dk[1]), kcomp(s.nz, g.dk[2]));
+    zd v = y * mk<double>(D[e].x, D[e].y);
+    double sc = shell_scale[s.shell];
+    A[e] = make_double2(v.x * sc, v.y * sc);
+}
+
+// Scatter A[e] into batch slot shell(e) of a [ns][M0][M1][M2] transform buffer.
+template <typename T>
+__global__ void k_scatter_entries(const ShellEnt *ent, long long ne, const double2 *A, int3 M, cplx<T> *buf) {
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    ShellEnt s = ent[e];
+    long long vol = (long long)M.x * M.y * M.z;
+    long long idx = (long long)s.shell * vol +
+                    ((long long)mod_idx(s.nx, M.x) * M.y + mod_idx(s.ny, M.y)) * M.z + mod_idx(s.nz, M.z);
+    buf[idx] = mk<T>((T)A[e].x, (T)A[e].y);
+}
+
+// G input: g(k) = (delta(k)/W(k)) / V on the cube |n_a| <= ext_a of the M grid.
+template <typename T>
+__global__ void k_scatter_G(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int3 lo, int3 cnt, int3 M, double k0_re,
+                            double k0_im, cplx<T> *buf) {
+    long long total = (long long)cnt.x * cnt.y * cnt.z;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int nz = lo.z + (int)(idx % cnt.z);
+        int ny = lo.y + (int)((idx / cnt.z) % cnt.y);
+        int nx = lo.x + (int)(idx / ((long long)cnt.z * cnt.y));
+        int ix = mod_idx(nx, g.n[0]), iy = mod_idx(ny, g.n[1]), iz = mod_idx(nz, g.n[2]);
+        zd d = (ix == 0 && iy == 0 && iz == 0) ? mk<double>(k0_re, k0_im) : f.at(ix, iy, iz);
+        double wf = window_tab(tabs, ix, iy, iz, wpow);
+        double re = d.x / wf / g.volume, im = d.y / wf / g.volume;
+        long long o = ((long long)mod_idx(nx, M.x) * M.y + mod_idx(ny, M.y)) * M.z + mod_idx(nz, M.z);
+        buf[o] = mk<T>((T)re, (T)im);
+    }
+}
+
+// QE[j][e] = Qhat_j(-n_e)
+template <typename T>
+__global__ void k_extract_neg(const ShellEnt *ent, long long ne, int ns, int3 M, const cplx<T> *buf, double2 *QE) {
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y;
+    if (e >= ne) return;
+    ShellEnt s = ent[e];
+    long long vol = (long long)M.x * M.y * M.z;
+    long long idx = (long long)j * vol +
+                    ((long long)mod_idx(-s.nx, M.x) * M.y + mod_idx(-s.ny, M.y)) * M.z + mod_idx(-s.nz, M.z);
+    cplx<T> v = buf[idx];
+    QE[(long long)j * ne + e] = make_double2((double)v.x, (double)v.y);
+}
+
+// out[i][j] = sum_{e in shell i} A[e] * QE[j][e]; one block per (i, j); deterministic.
+__global__ void k_pair_dot(const int *start, int ns_i, const double2 *A, const double2 *QE, long long ne, int ns_j,
+                           double2 *out) {
+    int i = blockIdx.x, j = blockIdx.y;
+    __shared__ double red[2][32];
+    double sr = 0.0, si = 0.0;
+    for (int e = start[i] + threadIdx.x; e < start[i + 1]; e += blockDim.x) {
+        double2 a = A[e], q = QE[(long long)j * ne + e];
+        sr += a.x * q.x - a.y * q.y;
+        si += a.x * q.y + a.y * q.x;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_down_sync(0xffffffffu, sr, o);
+        si += __shfl_down_sync(0xffffffffu, si, o);
+    }
+    int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (ln == 0) {
+        red[0][w] = sr;
+        red[1][w] = si;
+    }
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        sr = (ln < nw) ? red[0][ln] : 0.0;
+        si = (ln < nw) ? red[1][ln] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, o);
+            si += __shfl_down_sync(0xffffffffu, si, o);
+        }
+        if (ln == 0) out[(long long)i * ns_j + j] = make_double2(sr, si);
+    }
+}
+
+// ---------------------------------------------------------------- shot-noise field
+// Loader for the first inverse pass (along x) of
+//   xi(x) = (1/V) sum_k (f1 conj f2 - S C(k)) / W(k)^2 e^{ikx}   (field.hpp:1116-1160)
+// synthesising the k-space input from the half spectrum on the fly.
+template <typename T>
+struct LdXiHat {
+    Spec<T> f;
+    Grid g;
+    AxisTabs tabs;
+    int assign, wpow;
+    double S_re, S_im;
+    double k0_re, k0_im;  // (f1 conj f2)(k = 0) from the FP64 field integrals
+    double invV;
+    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
+        int ix = l;
+        int iy = (int)(i / g.n[2]);
+        int iz = (int)(i - (long long)iy * g.n[2]);
+        zd pk2;
+        if (ix == 0 && iy == 0 && iz == 0) {
+            pk2 = mk<double>(k0_re, k0_im);
+        } else {
+            zd d = f.at(ix, iy, iz);
+            pk2 = d * conjg(d);
+        }
+        double C = shot_tab(tabs, ix, iy, iz, assign);
+        pk2 = pk2 - mk<double>(S_re * C, S_im * C);
+        double wf = window_tab(tabs, ix, iy, iz, wpow);
+        double w2 = wf * wf;
+        return mk<T>((T)(invV * (pk2.x / w2)), (T)(invV * (pk2.y / w2)));
+    }
+};
+
+// One product of reduced harmonics with its Wigner weight: w Yhat_l1m1 Yhat_l2m2.
+struct YTerm {
+    int l1, m1, l2, m2;
+    double w;
+};
+#define HG_MAX_TERMS 24
+#define HG_MAX_HIST 8
+struct HistSpec {
+    int nh;                      // number of histograms
+    int nterm[HG_MAX_HIST];      // terms per histogram
+    int parity[HG_MAX_HIST];     // (-1)^(l1+l2) of the histogram's terms
+    YTerm term[HG_MAX_HIST][12];
+};
+
+// Last inverse pass (along z) over one symmetry orbit of (x, y) lines, fused with
+//   T_h(n^2) += sum over the orbit and z <-> -z of xi(x) f_h(theta)
+// where f_h = sum_terms w Yhat_l1m1 Yhat_l2m2 depends only on the polar angle (m1+m2 = 0),
+// and n^2 = wx^2 + wy^2 + wz^2 in cell units (cubic cells).
+template <typename T, int L>
+__global__ void __launch_bounds__(L) k_xi_orbit_hist(const cplx<T> *xi, const int *orbit_lines, const int *orbit_n2xy,
+                                                    int n_orbits, const cplx<T> *tw, HistSpec hs, long long n2dim,
+                                                    double *hist) {
+    constexpr int B = 8;
+    constexpr int LP = L + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *s = reinterpret_cast<cplx<T> *>(smem_raw);
+    const int orb = blockIdx.x;
+    const int *lines = orbit_lines + 8 * orb;
+    for (int e = threadIdx.x; e < B * L; e += L) {
+        int b = e / L, z = e - b * L;
+        int line = lines[b];
+        s[b * LP + z] = (line >= 0) ? xi[(long long)line * L + z] : mk<T>(0, 0);
+    }
+    __syncthreads();
+    smem_fft<T, L, +1, L>(s, LP, B, tw);
+    const int n2xy = orbit_n2xy[orb];
+    const double rho = sqrt((double)n2xy);
+    for (int iz = threadIdx.x; iz <= L / 2; iz += L) {
+        int iz2 = (L - iz) % L;
+        double er = 0, ei = 0, orr = 0, oi = 0;
+        for (int b = 0; b < B; b++) {
+            if (lines[b] < 0) continue;
+            cplx<T> a = s[b * LP + iz];
+            if (iz2 == iz) {
+                er += (double)a.x;
+                ei += (double)a.y;
+            } else {
+                cplx<T> c = s[b * LP + iz2];
+                er += (double)a.x + (double)c.x;
+                ei += (double)a.y + (double)c.y;
+                orr += (double)a.x - (double)c.x;
+                oi += (double)a.y - (double)c.y;
+            }
+        }
+        int wz = wrap_index(iz, L);
+        long long n2 = (long long)n2xy + (long long)wz * wz;
+        for (int h = 0; h < hs.nh; h++) {
+            zd f = mk<double>(0.0, 0.0);
+            for (int t = 0; t < hs.nterm[h]; t++) {
+                const YTerm &yt = hs.term[h][t];
+                zd y1 = ylm_reduced(yt.l1, yt.m1, rho, 0.0, (double)wz);
+                zd y2 = ylm_reduced(yt.l2, yt.m2, rho, 0.0, (double)wz);
+                f = f + (y1 * y2) * yt.w;
+            }
+            zd src = (hs.parity[h] > 0) ? mk<double>(er, ei) : mk<double>(orr, oi);
+            zd v = f * src;
+            if (v.x != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2)], v.x);
+            if (v.y != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2) + 1], v.y);
+        }
+    }
+}
+
+// Natural-spline evaluation of j_l at x (knots xmin + dx i, bessel.hpp:14-25).
+__device__ __forceinline__ double spline_eval(const double *y, const double *c, int n, double xmin, double dx, double xv) {
+    long i = (long)((xv - xmin) / dx);
+    if (i > n - 2) i = n - 2;
+    if (i < 0) i = 0;
+    while (i > 0 && xmin + dx * double(i) > xv) i--;
+    while (i < n - 2 && xmin + dx * double(i + 1) <= xv) i++;
+    double xi = xmin + dx * double(i), xi1 = xmin + dx * double(i + 1);
+    double h = xi1 - xi, t = xv - xi;
+    double b = (y[i + 1] - y[i]) / h - h * (c[i + 1] + 2.0 * c[i]) / 3.0;
+    double d = (c[i + 1] - c[i]) / (3.0 * h);
+    return y[i] + t * (b + t * (c[i] + t * d));
+}
+
+// J[i][n2] = j_l(k_i * r(n2)),  r(n2) = dr sqrt(n2)
+__global__ void k_bessel_table(const double *sy, const double *sc, int sn, double xmin, double dx, const double *kv,
+                               int nk, double dr, long long n2dim, double *J) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)nk * n2dim) return;
+    int i = (int)(q / n2dim);
+    long long n2 = q - (long long)i * n2dim;
+    double r = dr * sqrt((double)n2);
+    double x = kv[i] * r;
+    double xmax = xmin + dx * double(sn - 1);
+    J[q] = (x <= xmax) ? spline_eval(sy, sc, sn, xmin, dx, x) : 0.0;
+}
+
+// out[i1][i2] = sum_n2 J1[i1][n2] J2[i2][n2] hist[n2]; one block per (i1, i2).
+__global__ void k_sn_matrix(const double *J1, const double *J2, const double *hist, long long n2dim, int nk,
+                            double2 *out) {
+    int i1 = blockIdx.x, i2 = blockIdx.y;
+    __shared__ double red[2][32];
+    double sr = 0.0, si = 0.0;
+    const double *a = J1 + (long long)i1 * n2dim, *b = J2 + (long long)i2 * n2dim;
+    for (long long n2 = threadIdx.x; n2 < n2dim; n2 += blockDim.x) {
+        double hr = hist[2 * n2], hi = hist[2 * n2 + 1];
+        if (hr == 0.0 && hi == 0.0) continue;
+        double jj = a[n2] * b[n2];
+        sr += jj * hr;
+        si += jj * hi;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_down_sync(0xffffffffu, sr, o);
+        si += __shfl_down_sync(0xffffffffu, si, o);
+    }
+    int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (ln == 0) {
+        red[0][w] = sr;
+        red[1][w] = si;
+    }
+    __syncthreads();
+    if (w == 0) {
+        int nw = blockDim.x >> 5;
+        sr = (ln < nw) ? red[0][ln] : 0.0;
+        si = (ln < nw) ? red[1][ln] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, o);
+            si += __shfl_down_sync(0xffffffffu, si, o);
+        }
+        if (ln == 0) out[(long long)i1 * nk + i2] = make_double2(sr, si);
+    }
+}
+
+// Functors used by the transform passes.
+template <typename T>
+struct LdMeshDelta {  // real density rho -> (rho - nbar) dV  (field.hpp:520-523, 313-318)
+    const T *mesh;
+    long long L;
+    T nbar, dV;
+    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
+        return mk<T>((mesh[o * L + l] - nbar) * dV, (T)0);
+    }
+};
+template <typename T>
+struct StHalf {  // keep the non-negative half of the last axis
+    cplx<T> *H;
+    int L, hz;
+    __device__ __forceinline__ void operator()(long long o, int l, long long i, cplx<T> v) const {
+        if (l < hz) H[o * hz + l] = v;
+    }
+};
+template <typename T>
+struct LdMulG {  // chain[o][l] * G[(o mod plane)][l]
+    const cplx<T> *p;
+    const cplx<T> *G;
+    long long L, plane;
+    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
+        cplx<T> a = p[o * L + l];
+        cplx<T> b = G[(o % plane) * L + l];
+        return a * b;
+    }
+};
+
+}  // namespace hg

@@ -1,0 +1,122 @@
+/*
+ * hitomi_gpu.h -- C ABI of the B200 (sm_100a) implementation of hitomi_measurement's
+ * FFT-based clustering estimators: power-spectrum multipoles P_l(k), bispectrum
+ * multipoles B_{l1 l2 L}(k1,k2) and 3PCF multipoles zeta_{l1 l2 L}(r1,r2).
+ *
+ * The reference has no plugin API: its CLI drivers call free C++ functions
+ * (src/hitomi_measurement/main_box.cpp:175-193, main.cpp:242-266).  The entry points
+ * below are what the bodies of those functions delegate to; each names the reference
+ * function whose arithmetic it replaces.  Plain pointers and sizes only; complex arrays
+ * are interleaved (re, im) doubles.
+ *
+ * Conventions (mirroring the reference, src/hitomi_measurement/field.hpp:61,
+ * powerspec.hpp:12-16): every function returns 0 on success and -1 on failure;
+ * hg_last_error() gives the reason.  No exception crosses the ABI.  One context per
+ * process per GPU; calls on one context are synchronous and not reentrant.
+ *
+ * Results are the reference's RAW FP64 sums before normalisation and printing
+ * (pk_save / bk_save / sn_save / zeta_save), plus the normalisation factor the
+ * reference multiplies them by, so a caller reproduces the reference's output files.
+ */
+#ifndef HITOMI_GPU_H
+#define HITOMI_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HG_NGP 0
+#define HG_CIC 1
+#define HG_TSC 2
+#define HG_PCS 3 /* project extension: not in the reference (parameter.hpp:504-510 rejects it) */
+
+#define HG_FP64 0 /* plain form: FP64 everywhere */
+#define HG_FP32 1 /* chosen form: FP32 mesh/FFT/fields, FP64 sums, scalars and shot noise */
+
+typedef struct hg_ctx hg_ctx;
+
+/* Mirrors the fields of the reference's ParameterClass that the estimators read
+ * (parameter.hpp:12-49).  kbin / rbin follow ToolClass::setKbin / setRbin
+ * (tools.hpp:118-134): kbin[i] = kmin + i (kmax - kmin)/(n_kbin - 1). */
+typedef struct hg_config {
+    int n_mesh[3];      /* n_mesh_x/y/z; powers of two in [8, 1024] */
+    double boxsize[3];  /* boxsize_x/y/z */
+    int assign;         /* HG_NGP / HG_CIC / HG_TSC / HG_PCS  (parameter "assignment") */
+    int interlace;      /* 0/1, project extension (reference has no interlacing) */
+    int precision;      /* HG_FP64 or HG_FP32 */
+    double kmin, kmax;  /* k bins */
+    int n_kbin;
+    double rmin, rmax;  /* r bins */
+    int n_rbin;
+    int periodic;       /* 0: the reference's flat-index bounds rule (field.hpp:92-96);
+                           1: periodic wrap (forced for PCS / interlacing) */
+    int device;         /* CUDA device ordinal */
+} hg_config;
+
+/* Create / destroy a context.  Replaces the per-call setup the reference does inside
+ * each estimator (DensityFieldClass allocation, field.hpp:20-30; FFTW planning,
+ * field.hpp:321).  The context owns all device memory, plans, tables and graphs. */
+int hg_create(hg_ctx **ctx, const hg_config *cfg);
+int hg_destroy(hg_ctx *ctx);
+const char *hg_last_error(const hg_ctx *ctx);
+
+/* Hand a particle catalogue to the context.  Reads the caller's array-of-structs in
+ * place: particle p's position is the three doubles at base + p*stride_bytes +
+ * pos_off*8; its weight the double at w_off*8 (w_off < 0: weight 1).
+ *   slot 0 = data  (ParticleGadgetClass {pos[3],vel[3]}: stride 48, pos_off 0, w_off -1,
+ *                   particleGadget.hpp:12-15; ParticleBOSSClass {pos[3],los[3],w}:
+ *                   stride 56, pos_off 0, los_off 3, w_off 6, particle.hpp:12-16)
+ *   slot 1 = randoms (survey geometry only).
+ * los_off < 0: no line of sight (periodic box, global LOS along z).
+ * Positions must already be in FFT-box coordinates (after the reference's
+ * resetParticleForFFT / periodic wrap). */
+int hg_set_particles(hg_ctx *ctx, int slot, const double *base, long long n, long long stride_bytes, int pos_off,
+                     int los_off, int w_off);
+
+/* Periodic-box power-spectrum multipole.  Replaces the arithmetic of
+ * calcPowerSpectrumForBOX (powerspec.hpp:273-332): TSC/CIC/NGP assignment
+ * (field.hpp:67-184), dn = n - N/V (field.hpp:505-525), FFT (field.hpp:310-325) and the
+ * binned estimator (field.hpp:765-852) with shot noise N and Y_l0.
+ * pk_save[2*n_kbin]: the reference's pk_save = (2l+1) * stat.pk; n_mode[n_kbin] may be
+ * NULL; *norm = V / N^2 (powerspec.hpp:316). */
+int hg_pk_box(hg_ctx *ctx, int ell, double *pk_save, int *n_mode, double *norm);
+
+/* Periodic-box bispectrum multipole.  Replaces calcBiSpectrumForBOX (bispec.hpp:877-1203).
+ * ith_kbin >= 0 computes that k1 row (the reference's one-row-per-run behaviour);
+ * ith_kbin = -1 computes all n_kbin rows.  bk_save, sn_save: [rows][n_kbin] complex
+ * (2*rows*n_kbin doubles).  Output file value = norm * (bk_save - sn_save)
+ * (bispec.hpp:1184-1195). */
+int hg_bk_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_kbin, double *bk_save, double *sn_save,
+              double *norm);
+
+/* Periodic-box 3PCF multipole.  Replaces calcThreePointCorrelationFunctionForBOX
+ * (bispec.hpp:1205-1424).  Layout as hg_bk_box with r bins; output file value =
+ * norm * Re(zeta_save - sn_save) (bispec.hpp:1409-1416). */
+int hg_zeta_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double *zeta_save, double *sn_save,
+                double *norm);
+
+/* Survey-geometry scalars on the current data (slot 0) and randoms (slot 1):
+ * alpha = sum w_D / sum w_R (particle.hpp:268-282), V_survey = (sum w_R)^2 /
+ * sum_cells n_R^2 dV (field.hpp:449-503), nbar (particle.hpp:284-300), and the summed
+ * weights.  All FP64.  Any output pointer may be NULL. */
+int hg_survey_scalars(hg_ctx *ctx, double *alpha, double *vsurvey, double *nbar, double *wsum_data,
+                      double *wsum_rand);
+
+/* Survey-geometry (Yamamoto) power-spectrum multipole with local LOS.  Replaces
+ * calcPowerSpectrum (powerspec.hpp:4-91): Y_lm-weighted fields
+ * (field.hpp:186-228), shot noise (field.hpp:1164-1190) and the (M, m1) sums with
+ * Wigner-3j weights.  alpha and vsurvey are the values the caller passes to the
+ * reference function.  *norm = V_survey / (sum w_D)^2 (particle.hpp:303-316). */
+int hg_pk_survey(hg_ctx *ctx, int ell, double alpha, double vsurvey, double *pk_save, int *n_mode, double *norm);
+
+/* Device-side time of the last statistic call in milliseconds (CUDA events on the
+ * context's stream), and the number of kernels it launched. */
+int hg_last_timing(const hg_ctx *ctx, double *device_ms, long long *kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HITOMI_GPU_H */

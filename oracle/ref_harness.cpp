@@ -1,0 +1,226 @@
+/*
+ * oracle/ref_harness.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Builds the reference's own, unmodified estimator headers
+ * (src/hitomi_measurement/{common,parameter,tools,bessel,particle,particleGadget,
+ * particle_reconstruction,field,powerspec,bispec}.hpp) against the project-written
+ * FFTW/GSL shims in oracle/shim/, and drives them the way the reference's CLI drivers
+ * do (src/hitomi_measurement/main_box.cpp:50-230 for the periodic box,
+ * src/hitomi_measurement/main.cpp:86-275 for the survey geometry).
+ *
+ * Only the particle source differs: instead of a Gadget snapshot or an ASCII
+ * catalogue, positions (and weights) come from raw float64 files written by the
+ * synthetic catalogue generators, so the oracle sees bit-identical inputs to the GPU.
+ *
+ * Usage:
+ *   ref_harness param.ini data.f64 [random.f64] [--all-rows]
+ *     box    : data.f64 holds n x 3 doubles (x y z)
+ *     survey : data.f64 / random.f64 hold n x 4 doubles (x y z w)
+ *   --all-rows : for measure = bk / 3PCF, run every ith_kbin / ith_rbin row
+ *                (the reference computes one row per process, main.cpp:78-84).
+ * Environment:
+ *   HX_FULL=1    : result files are written with 17 significant digits instead of
+ *                  the reference's %.7e / %.5f (format strings are rewritten at
+ *                  fprintf time; the reference sources are untouched).
+ *   HX_VERBOSE=1 : keep the reference's progress printf output (stderr).
+ *   HX_TIMING=1  : print the wall time of the estimator call(s) to stdout as
+ *                  "HX_WALL_SECONDS <t>" (std::chrono; the reference's clock() is CPU time).
+ */
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <string>
+#include <vector>
+
+static int hx_printf(const char *fmt, ...) {
+    if (!getenv("HX_VERBOSE")) return 0;
+    va_list ap;
+    va_start(ap, fmt);
+    int r = vfprintf(stderr, fmt, ap);
+    va_end(ap);
+    return r;
+}
+
+static int hx_fprintf(FILE *fp, const char *fmt, ...) {
+    std::string f(fmt);
+    if (getenv("HX_FULL")) {
+        std::string out;
+        for (size_t i = 0; i < f.size();) {
+            if (f.compare(i, 4, "%.7e") == 0) {
+                out += "%.17e";
+                i += 4;
+            } else if (f.compare(i, 4, "%.5f") == 0) {
+                out += "%.17g";
+                i += 4;
+            } else {
+                out += f[i++];
+            }
+        }
+        f = out;
+    }
+    va_list ap;
+    va_start(ap, fmt);
+    int r = vfprintf(fp, f.c_str(), ap);
+    va_end(ap);
+    return r;
+}
+
+#define printf hx_printf
+#define fprintf hx_fprintf
+
+#include "common.hpp"
+#include "parameter.hpp"
+#include "tools.hpp"
+#include "bessel.hpp"
+#include "particle.hpp"
+#include "particleGadget.hpp"
+#include "particle_reconstruction.hpp"
+#include "field.hpp"
+#include "powerspec.hpp"
+#include "bispec.hpp"
+
+#undef printf
+#undef fprintf
+
+static std::vector<double> read_f64(const char *path) {
+    std::vector<double> v;
+    FILE *fp = fopen(path, "rb");
+    if (!fp) {
+        std::fprintf(stderr, "cannot open %s\n", path);
+        exit(2);
+    }
+    fseek(fp, 0, SEEK_END);
+    long sz = ftell(fp);
+    fseek(fp, 0, SEEK_SET);
+    v.resize(sz / sizeof(double));
+    if (fread(v.data(), sizeof(double), v.size(), fp) != v.size()) {
+        std::fprintf(stderr, "short read %s\n", path);
+        exit(2);
+    }
+    fclose(fp);
+    return v;
+}
+
+static void fill_boss(ParticleBOSSClass &P, const std::vector<double> &a) {
+    long long n = (long long)(a.size() / 4);
+    if (P.initializeParticle(n)) exit(2);
+    for (long long i = 0; i < n; i++) {
+        P[i].pos[0] = a[4 * i + 0];
+        P[i].pos[1] = a[4 * i + 1];
+        P[i].pos[2] = a[4 * i + 2];
+        P[i].w = a[4 * i + 3];
+    }
+    P.calcMinAndMax();
+}
+
+static int fail(const char *what) {
+    std::fprintf(stderr, "'%s' fails.\n", what);
+    return 1;
+}
+
+int main(int argc, char **argv) {
+    if (argc < 3) {
+        std::fprintf(stderr, "usage: ref_harness param.ini data.f64 [random.f64] [--all-rows]\n");
+        return 2;
+    }
+    bool all_rows = false;
+    std::vector<const char *> pos;
+    for (int i = 1; i < argc; i++) {
+        if (!strcmp(argv[i], "--all-rows")) all_rows = true;
+        else pos.push_back(argv[i]);
+    }
+    char *pargv[2] = {argv[0], (char *)pos[0]};
+    ParameterClass param;
+    if (param.readParameters(pargv)) return fail("param.readParameters");
+    if (param.makeOutputDirectory()) return fail("param.makeOutputDirectory");
+    if (param.printParameters()) return fail("param.printParameters");
+    std::vector<double> kbin(param.n_kbin), rbin(param.n_rbin);
+    ToolClass::setKbin(param, kbin.data());
+    ToolClass::setRbin(param, rbin.data());
+
+    auto t0 = std::chrono::steady_clock::now();
+    int rc = 0;
+    if (pos.size() == 2) {
+        /* periodic box: main_box.cpp:96-228 (reader replaced, boxsize from param) */
+        std::vector<double> a = read_f64(pos[1]);
+        ParticleGadgetClass P_D;
+        long long n = (long long)(a.size() / 3);
+        if (P_D.initializeParticle(n)) return fail("P_D.initializeParticle");
+        for (long long i = 0; i < n; i++)
+            for (int ax = 0; ax < 3; ax++) P_D[i].pos[ax] = a[3 * i + ax];
+        P_D.calcMinAndMax();
+        t0 = std::chrono::steady_clock::now();
+        if (param.measure == "pk") {
+            rc = calcPowerSpectrumForBOX(P_D, param, kbin.data());
+        } else if (param.measure == "2PCF") {
+            rc = calcTwoPointCorrelationFunctionForBOX(P_D, param, rbin.data());
+        } else if (param.measure == "bk") {
+            int lo = all_rows ? 0 : param.ith_kbin, hi = all_rows ? param.n_kbin : param.ith_kbin + 1;
+            for (int i = lo; i < hi && rc == 0; i++) {
+                param.ith_kbin = i;
+                rc = calcBiSpectrumForBOX(P_D, param, kbin.data());
+            }
+        } else if (param.measure == "3PCF") {
+            int lo = all_rows ? 0 : param.ith_rbin, hi = all_rows ? param.n_rbin : param.ith_rbin + 1;
+            for (int i = lo; i < hi && rc == 0; i++) {
+                param.ith_rbin = i;
+                rc = calcThreePointCorrelationFunctionForBOX(P_D, param, rbin.data());
+            }
+        } else {
+            return fail("measure");
+        }
+    } else {
+        /* survey geometry: main.cpp:129-275 (ASCII reader replaced by raw doubles) */
+        ParticleBOSSClass P_D, P_R;
+        fill_boss(P_D, read_f64(pos[1]));
+        fill_boss(P_R, read_f64(pos[2]));
+        if (P_D.calcTotalNumberOfParticlesWithWeights()) return fail("P_D.calcTotalNumberOfParticlesWithWeights");
+        if (P_R.calcTotalNumberOfParticlesWithWeights()) return fail("P_R.calcTotalNumberOfParticlesWithWeights");
+        if (P_D.calcLOS()) return fail("P_D.calcLOS");
+        if (P_R.calcLOS()) return fail("P_R.calcLOS");
+        double alpha = ParticleBOSSClass::calcAlpha(P_D, P_R);
+        if (alpha < 0.0) return fail("calcAlpha");
+        if (ParticleBOSSClass::resetParticleForFFT(P_D, P_R, param)) return fail("resetParticleForFFT");
+        t0 = std::chrono::steady_clock::now();
+        DensityFieldClass<ParticleBOSSClass> Vol(param);
+        double Vsurvey = Vol.calcSurveyVolume(P_R);
+        Vol.finalizeDensityField();
+        double nbar = ParticleBOSSClass::calcMeanNumberDensity(P_D, Vsurvey);
+        if (nbar < 0.0) return fail("calcMeanNumberDensity");
+        if (ParticleBOSSClass::printParameters(param, P_D, P_R, alpha, Vsurvey, nbar)) return fail("printParameters");
+        {
+            /* full-precision survey scalars for the parity tests */
+            std::string fn = param.output_dir + "/survey_scalars_full";
+            FILE *fp = fopen(fn.c_str(), "w");
+            std::fprintf(fp, "%.17e %.17e %.17e %.17e %.17e\n", alpha, Vsurvey, nbar, P_D.n_tot_weight,
+                         P_R.n_tot_weight);
+            fclose(fp);
+        }
+        if (param.measure == "pk") {
+            rc = calcPowerSpectrum(P_D, P_R, param, alpha, kbin.data(), Vsurvey);
+        } else if (param.measure == "2PCF") {
+            rc = calcTwoPointCorrelationFunction(P_D, P_R, param, alpha, rbin.data(), Vsurvey);
+        } else if (param.measure == "bk") {
+            int lo = all_rows ? 0 : param.ith_kbin, hi = all_rows ? param.n_kbin : param.ith_kbin + 1;
+            for (int i = lo; i < hi && rc == 0; i++) {
+                param.ith_kbin = i;
+                rc = calcBiSpectrum(P_D, P_R, param, alpha, kbin.data(), Vsurvey);
+            }
+        } else if (param.measure == "3PCF") {
+            int lo = all_rows ? 0 : param.ith_rbin, hi = all_rows ? param.n_rbin : param.ith_rbin + 1;
+            for (int i = lo; i < hi && rc == 0; i++) {
+                param.ith_rbin = i;
+                rc = calcThreePointCorrelationFunction(P_D, P_R, param, alpha, rbin.data(), Vsurvey);
+            }
+        } else {
+            return fail("measure");
+        }
+    }
+    double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (getenv("HX_TIMING")) std::printf("HX_WALL_SECONDS %.6f\n", wall);
+    if (rc) return fail(param.measure.c_str());
+    return 0;
+}
