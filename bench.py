@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""Throughput of the periodic-box clustering estimators: mocks/s for P_l (l = 0, 2, 4) plus
+bispectrum multipoles B_{l1 l2 L} in {(000), (110), (202), (022)} over all (k1, k2) shell
+pairs, on a 512^3 mesh with 10^7 particles (the clustered lognormal catalogue with
+Zel'dovich RSD), TSC assignment, 25 k shells 0.01-0.26 h/Mpc.
+
+One step = one mock through the whole pipeline (assignment, FFT, P_l binning, shell
+transforms, bispectrum sums and shot noise).  `value` has the catalogue resident in HBM;
+`e2e` copies it from pinned host memory through hg_set_particles every step and reads
+the results back.  Both forms are measured: the chosen FP32 form (the headline) and the
+plain FP64 form, with the per-bin relative difference between them.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--small]
+Under torchrun every rank runs its own mocks (weak scaling, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "mocks/sec P_ℓ+B_ℓ @512³,1e7 pts: batched FP32 vs FP64 GPU, ≤1e-5 rel err"
+UNIT = "mocks/s"
+PK_ELLS = (0, 2, 4)
+MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2))
+
+
+def workload(small: bool):
+    from hitomi_b200.api import Binning
+    if small:
+        return dict(name="box P_l+B_l, 64^3 mesh, 2e5 particles (reduced check size)", n_mesh=64, boxsize=1000.0,
+                    n_part=200_000, ngrid=64, binning=Binning(0.015, 0.255, 25))
+    return dict(name="box P_l(l=0,2,4)+B_l(000,110,202,022), all k1,k2; 512^3 mesh, 1e7 particles, TSC", n_mesh=512,
+                boxsize=1000.0, n_part=10_000_000, ngrid=256, binning=Binning(0.015, 0.255, 25))
+
+
+def catalogue(wl, seed):
+    from hitomi_b200.synthetic import lognormal_box
+    return lognormal_box(wl["n_part"], wl["boxsize"], ngrid=wl["ngrid"], seed=seed, exact_n=wl["n_part"])
+
+
+def run_mock(ctx):
+    """One mock: P_l for l in PK_ELLS and all B multipoles; returns results and launch count."""
+    out = {}
+    launches = 0
+    for ell in PK_ELLS:
+        pk, _, norm = ctx.pk_box(ell)
+        out[("pk", ell)] = norm * pk
+        launches += ctx.last_timing()[1]
+    for mp in MULTIPOLES:
+        bk, sn, norm = ctx.bk_box(*mp)
+        out[("bk",) + mp] = norm * (bk - sn)
+        launches += ctx.last_timing()[1]
+    return out, launches
+
+
+def result_bytes(res) -> int:
+    return int(sum(v.size * 16 for v in res.values()))
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.p = None
+        self.path = os.path.join("/tmp", f"hg_clocks_{os.getpid()}_{device_index}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    p = os.path.join(HERE, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+def max_rel_err(a, ref):
+    floor = 1e-12 * float(np.max(np.abs(ref))) if np.size(ref) else 0.0
+    return float(np.max(np.abs(a - ref) / np.maximum(np.abs(ref), floor))) if np.size(ref) else 0.0
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, wl, world, rank):
+    """Reference arm: the reference's own CPU code (oracle/_ref) on the host cores."""
+    if rank != 0:
+        return 0
+    from oracle import cpu_baseline, ref_runner
+    line = {"impl": "reference", "metric": METRIC, "unit": UNIT, "higher_is_better": True, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic"}
+    if not ref_runner.available():
+        line["unavailable"] = "oracle/_ref/ref_harness was not built on this machine"
+        print(json.dumps(line), flush=True)
+        return 0
+    pos = catalogue(wl, 2)
+    vals, per = [], []
+    for s in range(args.warmup + args.steps):
+        r = cpu_baseline.baseline(pos, wl["n_mesh"], wl["boxsize"], wl["binning"], PK_ELLS, MULTIPOLES)
+        if s >= args.warmup:
+            vals.append(r["mocks_per_s"])
+            per.append(r["sample_wall_seconds"])
+    v = statistics.median(vals)
+    line.update({
+        "value": v,
+        "ms_per_step": 1000.0 * statistics.median(per),
+        "config": {"workload": wl["name"], "n_mesh": wl["n_mesh"], "n_particles": wl["n_part"],
+                   "n_kbin": wl["binning"].n_kbin},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                         "sample": "each step: every building block of the reference's box P/B drivers timed once "
+                                   "at 512^3 / 1e7 particles (one single-core process per block, concurrently); "
+                                   "per-mock time extrapolated by the drivers' call counts; FFT is the project "
+                                   "shim, not FFTW"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    })
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="64^3 / 2e5-particle case for quick checks")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="fp32,fp64")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    wl = workload(args.small)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        rc = run_reference(args, wl, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+    from hitomi_b200.api import Context
+    torch.cuda.set_device(local)
+    pos = catalogue(wl, 2 + rank)
+    n = pos.shape[0]
+    d_pos = torch.from_numpy(pos).to(f"cuda:{local}")
+    h_pos = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    h_pos.copy_(torch.from_numpy(pos))
+    h_np = h_pos.numpy()
+    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
+    results = {}
+    timing = {}
+    for form in forms:
+        ctx = Context(wl["n_mesh"], wl["boxsize"], wl["binning"], "TSC", form, device=local)
+        for _ in range(args.warmup):
+            ctx.set_particles_device(0, d_pos.data_ptr(), n, 24, keep=d_pos)
+            run_mock(ctx)
+        # ---- device-resident value
+        clk = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
+                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else local)
+        barrier(world)
+        torch.cuda.synchronize()
+        clk.start()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        launches = 0
+        for _ in range(args.steps):
+            ctx.set_particles_device(0, d_pos.data_ptr(), n, 24, keep=d_pos)
+            res, nl = run_mock(ctx)
+            launches += nl
+        ev1.record()
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        barrier(world)
+        ms = reduce_max(ev0.elapsed_time(ev1) / args.steps, world)
+        results[form] = res
+        # ---- end to end through the public API with host buffers
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d2h = 0
+        for _ in range(args.steps):
+            ctx.set_particles(0, h_np)
+            r2, _ = run_mock(ctx)
+            d2h = result_bytes(r2)
+        e1.record()
+        torch.cuda.synchronize()
+        ems = reduce_max(e0.elapsed_time(e1) / args.steps, world)
+        # ---- one profiled step: per-kernel CUDA-event timing
+        ctx.set_profiling(True)
+        ctx.set_particles_device(0, d_pos.data_ptr(), n, 24, keep=d_pos)
+        run_mock(ctx)
+        stats = ctx.kernel_stats()
+        ctx.set_profiling(False)
+        timing[form] = dict(ms=ms, e2e_ms=ems, launches=launches // args.steps, clocks=clocks, stats=stats,
+                            d2h=d2h)
+        ctx.close()
+
+    head = forms[0]
+    t = timing[head]
+    value = world * 1000.0 / t["ms"]
+    evalue = world * 1000.0 / t["e2e_ms"]
+    peak, peak_kind = measured_peaks()
+    top = max(t["stats"].items(), key=lambda kv: kv[1]["ms"]) if t["stats"] else None
+    roof = None
+    if top:
+        name, st = top
+        per_launch_ms = st["ms"] / st["launches"]
+        per_launch_bytes = st["bytes"] / st["launches"]
+        achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+        trf = ncu_traffic().get(f"{head}:{name}")
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": trf,
+                "share_of_step": st["ms"] / sum(v["ms"] for v in t["stats"].values())}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if head == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": wl["name"], "n_mesh": wl["n_mesh"], "n_particles": n, "boxsize": wl["boxsize"],
+                   "assignment": "TSC", "n_kbin": wl["binning"].n_kbin, "kmin": wl["binning"].kmin,
+                   "kmax": wl["binning"].kmax, "pk_ells": list(PK_ELLS), "bk_multipoles": [list(m) for m in MULTIPOLES],
+                   "form": head, "l2": "inputs larger than L2 (mesh and catalogue > 126 MB)",
+                   "parallelism": f"mocks sharded over {world} GPU(s), no collective on the data path"},
+        "clocks": t["clocks"],
+        "e2e": {"value": evalue, "unit": UNIT, "h2d_bytes_per_step": int(n * 24), "d2h_bytes_per_step": int(t["d2h"])},
+        "gpu_launches": int(t["launches"] * args.steps),
+        "roofline": roof,
+    }
+    if "fp64" in timing and head != "fp64":
+        errs = {f"{k[0]}{''.join(map(str, k[1:]))}": max_rel_err(results[head][k], results["fp64"][k])
+                for k in results[head]}
+        line["fp64_form"] = {"value": world * 1000.0 / timing["fp64"]["ms"], "ms_per_step": timing["fp64"]["ms"],
+                             "e2e_value": world * 1000.0 / timing["fp64"]["e2e_ms"]}
+        line["fp32_over_fp64"] = timing["fp64"]["ms"] / t["ms"]
+        line["max_rel_err_fp32_vs_fp64"] = max(errs.values())
+        line["rel_err_by_statistic"] = errs
+    line["kernel_ms"] = {k: round(v["ms"], 4) for k, v in sorted(t["stats"].items(), key=lambda kv: -kv[1]["ms"])}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import cpu_baseline
+            cb = cpu_baseline.baseline(pos, wl["n_mesh"], wl["boxsize"], wl["binning"], PK_ELLS, MULTIPOLES)
+            line["cpu_baseline"] = {
+                "value": cb["mocks_per_s"], "unit": UNIT, "cores": cb["cores"], "kind": "reference",
+                "sample": f"reference box P/B building blocks timed once each at {wl['n_mesh']}^3 / {n} particles "
+                          f"(single-core processes, concurrently, {cb['sample_wall_seconds']:.1f} s wall); "
+                          f"per-mock {cb['per_mock_seconds']:.0f} s extrapolated by the drivers' call counts; "
+                          f"FFT is the project shim, not FFTW",
+                "unit_seconds": cb["unit_seconds"]}
+        except Exception as e:  # reported, not fatal
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": f"failed: {e}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -17,11 +17,14 @@ SYMBOLS = (
     "hg_destroy",
     "hg_last_error",
     "hg_set_particles",
+    "hg_set_particles_device",
     "hg_pk_box",
     "hg_bk_box",
     "hg_zeta_box",
     "hg_survey_scalars",
     "hg_pk_survey",
+    "hg_set_profiling",
+    "hg_kernel_stats",
     "hg_last_timing",
 )
 
@@ -71,6 +74,12 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_set_particles.argtypes = [vp, ctypes.c_int, c_dp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int]
     lib.hg_set_particles.restype = ctypes.c_int
+    lib.hg_set_particles_device.argtypes = lib.hg_set_particles.argtypes
+    lib.hg_set_particles_device.restype = ctypes.c_int
+    lib.hg_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.hg_set_profiling.restype = ctypes.c_int
+    lib.hg_kernel_stats.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
+    lib.hg_kernel_stats.restype = ctypes.c_int
     lib.hg_pk_box.argtypes = [vp, ctypes.c_int, c_dp, c_ip, c_dp]
     lib.hg_pk_box.restype = ctypes.c_int
     lib.hg_bk_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, c_dp]

@@ -109,6 +109,26 @@ class Context:
         self._check(self._lib.hg_set_particles(self._h, slot, _dp(a), a.shape[0], a.shape[1] * 8, pos_off, los_off,
                                                w_off))
 
+    def set_particles_device(self, slot: int, ptr: int, n: int, stride_bytes: int, pos_off: int = 0,
+                             los_off: int = -1, w_off: int = -1, keep=None):
+        """Use a caller-owned device array (e.g. a torch CUDA tensor's data_ptr()) in place."""
+        self._keep[slot] = keep
+        self._check(self._lib.hg_set_particles_device(self._h, slot, ctypes.cast(ctypes.c_void_p(ptr),
+                                                      ctypes.POINTER(ctypes.c_double)), n, stride_bytes, pos_off,
+                                                      los_off, w_off))
+
+    def set_profiling(self, on: bool = True):
+        self._check(self._lib.hg_set_profiling(self._h, int(bool(on))))
+
+    def kernel_stats(self) -> dict:
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self._lib.hg_kernel_stats(self._h, buf, len(buf)))
+        out = {}
+        for line in buf.value.decode().splitlines():
+            name, n, ms, by = line.split("\t")
+            out[name] = dict(launches=int(n), ms=float(ms), bytes=float(by))
+        return out
+
     # -- statistics
     def pk_box(self, ell: int):
         nk = self.binning.n_kbin

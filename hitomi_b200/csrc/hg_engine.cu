@@ -111,7 +111,9 @@ struct hg_ctx {
     long long last_launches = 0;
     virtual ~hg_ctx() {}
     virtual void set_particles(int slot, const double *base, long long n, long long stride, int pos_off, int los_off,
-                               int w_off) = 0;
+                               int w_off, bool on_device) = 0;
+    virtual void set_profiling(bool on) = 0;
+    virtual std::string kernel_stats() = 0;
     virtual void pk_box(int ell, double *pk_save, int *n_mode, double *norm) = 0;
     virtual void bk_box(int l1, int l2, int L, int ith, double *bk_save, double *sn_save, double *norm) = 0;
     virtual void zeta_box(int l1, int l2, int L, int ith, double *zeta_save, double *sn_save, double *norm) = 0;
@@ -136,7 +138,11 @@ struct Engine : public hg_ctx {
         long long n = 0, stride = 0;
         int pos_off = 0, los_off = -1, w_off = -1;
         std::vector<double> host_w;  // weights (survey), for FP64 host sums
+        const void *ext = nullptr;   // caller-owned device array (hg_set_particles_device)
         bool set = false;
+        const unsigned char *base() const {
+            return reinterpret_cast<const unsigned char *>(ext ? ext : raw.p);
+        }
     } slot[2];
 
     // tables
@@ -185,6 +191,59 @@ struct Engine : public hg_ctx {
 
     long long launches = 0;
 
+    // per-kernel device timing (CUDA events on the context stream) and modelled bytes
+    bool profiling = false;
+    struct PRecd {
+        const char *name;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<PRecd> pend;
+    std::vector<cudaEvent_t> ev_pool;
+    struct KAgg {
+        long long launches = 0;
+        double ms = 0.0, bytes = 0.0;
+    };
+    std::map<std::string, KAgg> kagg;
+    cudaEvent_t take_ev() {
+        if (!ev_pool.empty()) {
+            cudaEvent_t e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        HG_CK(cudaEventCreate(&e));
+        return e;
+    }
+    void kb(const char *name, double bytes) {
+        launches++;
+        if (!profiling) return;
+        PRecd r{name, take_ev(), nullptr, bytes};
+        HG_CK(cudaEventRecord(r.a, st));
+        pend.push_back(r);
+    }
+    void ke() {
+        HG_CK(cudaGetLastError());
+        if (!profiling || pend.empty() || pend.back().b) return;
+        pend.back().b = take_ev();
+        HG_CK(cudaEventRecord(pend.back().b, st));
+    }
+    void prof_flush() {
+        if (pend.empty()) return;
+        HG_CK(cudaStreamSynchronize(st));
+        for (auto &r : pend) {
+            float ms = 0.f;
+            if (r.b) HG_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+            KAgg &k = kagg[r.name];
+            k.launches++;
+            k.ms += ms;
+            k.bytes += r.bytes;
+            ev_pool.push_back(r.a);
+            if (r.b) ev_pool.push_back(r.b);
+        }
+        pend.clear();
+    }
+
     explicit Engine(const hg_config &c) {
         cfg = c;
         for (int a = 0; a < 3; a++) {
@@ -228,6 +287,21 @@ struct Engine : public hg_ctx {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (st) cudaStreamDestroy(st);
+    }
+
+    void set_profiling(bool on) override {
+        profiling = on;
+        if (on) kagg.clear();
+    }
+    std::string kernel_stats() override {
+        std::string out;
+        char line[256];
+        for (auto &kv : kagg) {
+            snprintf(line, sizeof(line), "%s\t%lld\t%.6f\t%.6e\n", kv.first.c_str(), kv.second.launches, kv.second.ms,
+                     kv.second.bytes);
+            out += line;
+        }
+        return out;
     }
 
     // ------------------------------------------------------------------ tables
@@ -292,7 +366,7 @@ struct Engine : public hg_ctx {
 
     // ------------------------------------------------------------------ particles
     void set_particles(int s, const double *base, long long n, long long stride, int pos_off, int los_off,
-                       int w_off) override {
+                       int w_off, bool on_device) override {
         HG_REQUIRE(s == 0 || s == 1, "slot must be 0 (data) or 1 (randoms)");
         HG_REQUIRE(n > 0, "The number of particles should be > 0");
         HG_REQUIRE(base != nullptr, "null particle array");
@@ -301,8 +375,13 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(w_off < 0 || (w_off + 1) * 8 <= stride, "w_off outside the record");
         HG_REQUIRE(los_off < 0 || (los_off + 3) * 8 <= stride, "los_off outside the record");
         Slot &S = slot[s];
-        HG_CK(S.raw.ensure((size_t)(n * stride)));
-        HG_CK(cudaMemcpyAsync(S.raw.p, base, (size_t)(n * stride), cudaMemcpyHostToDevice, st));
+        if (on_device) {
+            S.ext = base;
+        } else {
+            S.ext = nullptr;
+            HG_CK(S.raw.ensure((size_t)(n * stride)));
+            HG_CK(cudaMemcpyAsync(S.raw.p, base, (size_t)(n * stride), cudaMemcpyHostToDevice, st));
+        }
         S.n = n;
         S.stride = stride;
         S.pos_off = pos_off;
@@ -351,46 +430,51 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(mass.p, 0, sizeof(double) * 2, st));
+        kb("assign_bin_count", double(src.n) * 24.0);
         k_bin_count<<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(cnt), dp<double>(mass));
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         size_t tb = 0;
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
         HG_CK(cubtmp.ensure(tb));
+        kb("assign_scan", double(ntiles + 1) * 8.0);
         HG_CK(cub::DeviceScan::ExclusiveSum(cubtmp.p, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
-        launches++;
+        ke();
         unsigned total = 0;
         double hm[2];
         HG_CK(cudaMemcpyAsync(&total, dp<unsigned>(off) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaMemcpyAsync(hm, mass.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
         HG_CK(rec.ensure(sizeof(PRec<T>) * std::max<size_t>(total, 1)));
+        kb("assign_bin_scatter", double(src.n) * 24.0 + double(total) * sizeof(PRec<T>));
         k_bin_scatter<T><<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(off), dp<unsigned>(cursor),
                                                             dp<PRec<T>>(rec));
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2];
         HG_CK(cudaFuncSetAttribute(k_tile_accum<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kb("assign_tile_accum", double(total) * sizeof(PRec<T>) + double(g.ntot) * sizeof(T));
         k_tile_accum<T, false><<<ntiles, 256, smem, st>>>(dp<PRec<T>>(rec), dp<unsigned>(off), ag, out, nullptr);
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         return hm[0];
     }
 
     template <int DIR, class LD, class ST>
-    void pass(int L, LD ld, ST stt, long long outer, long long inner) {
+    void pass(int L, LD ld, ST stt, long long outer, long long inner, const char *name = "fft_pass",
+              double bytes = -1.0) {
         PassGeom pg{outer, inner};
-        HG_CK((launch_fft_pass<T, DIR>(L, ld, stt, pg, twiddles(L), st)));
-        launches++;
+        if (bytes < 0) bytes = 2.0 * double(outer) * L * inner * sizeof(C);
+        const C *twp = twiddles(L);
+        kb(name, bytes);
+        HG_CK((launch_fft_pass<T, DIR>(L, ld, stt, pg, twp, st)));
+        ke();
     }
 
     // In-place 3-D c2c transform of a batch of nb arrays [nb][M0][M1][M2].
     template <int DIR>
-    void fft3(C *p, long long nb, const int *M) {
-        pass<DIR>(M[2], LdArr<T>{p, M[2], 1}, StArr<T>{p, M[2], 1}, nb * M[0] * M[1], 1);
-        pass<DIR>(M[1], LdArr<T>{p, M[1], M[2]}, StArr<T>{p, M[1], M[2]}, nb * M[0], M[2]);
+    void fft3(C *p, long long nb, const int *M, const char *name) {
+        pass<DIR>(M[2], LdArr<T>{p, M[2], 1}, StArr<T>{p, M[2], 1}, nb * M[0] * M[1], 1, name);
+        pass<DIR>(M[1], LdArr<T>{p, M[1], M[2]}, StArr<T>{p, M[1], M[2]}, nb * M[0], M[2], name);
         pass<DIR>(M[0], LdArr<T>{p, M[0], (long long)M[1] * M[2]}, StArr<T>{p, M[0], (long long)M[1] * M[2]}, nb,
-                  (long long)M[1] * M[2]);
+                  (long long)M[1] * M[2], name);
     }
 
     // Box density contrast, forward transformed: H = FFT[dV (rho - N/V)] (half spectrum).
@@ -399,7 +483,7 @@ struct Engine : public hg_ctx {
         Slot &S = slot[0];
         HG_REQUIRE(S.set, "no particles: call hg_set_particles(ctx, 0, ...) first");
         AssignGeom ag = make_geom(0.0);
-        PartSrc src{reinterpret_cast<const unsigned char *>(S.raw.p), S.n, S.stride, S.pos_off, -1, nullptr, 1.0};
+        PartSrc src{S.base(), S.n, S.stride, S.pos_off, -1, nullptr, 1.0};
         HG_CK(mesh.ensure(sizeof(T) * g.ntot));
         dens_mass = assign_real(src, ag, dp<T>(mesh));
         const int hz = g.n[2] / 2 + 1;
@@ -407,10 +491,11 @@ struct Engine : public hg_ctx {
         const double dV = g.volume / double(g.ntot);
         const double nbar = double(S.n) / g.volume;  // field.hpp:521
         pass<-1>(g.n[2], LdMeshDelta<T>{dp<T>(mesh), g.n[2], (T)nbar, (T)dV}, StHalf<T>{dp<C>(H), g.n[2], hz},
-                 (long long)g.n[0] * g.n[1], 1);
-        pass<-1>(g.n[1], LdArr<T>{dp<C>(H), g.n[1], hz}, StArr<T>{dp<C>(H), g.n[1], hz}, g.n[0], hz);
+                 (long long)g.n[0] * g.n[1], 1, "fft_density_r2c_z",
+                 double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
+        pass<-1>(g.n[1], LdArr<T>{dp<C>(H), g.n[1], hz}, StArr<T>{dp<C>(H), g.n[1], hz}, g.n[0], hz, "fft_density_yx");
         pass<-1>(g.n[0], LdArr<T>{dp<C>(H), g.n[0], (long long)g.n[1] * hz},
-                 StArr<T>{dp<C>(H), g.n[0], (long long)g.n[1] * hz}, 1, (long long)g.n[1] * hz);
+                 StArr<T>{dp<C>(H), g.n[0], (long long)g.n[1] * hz}, 1, (long long)g.n[1] * hz, "fft_density_yx");
         // k = 0 from the FP64 integral: sum_c (rho_c - nbar) dV
         delta0 = (dens_mass - nbar * double(g.ntot)) * dV;
         N0 = dens_mass * dV;
@@ -458,11 +543,11 @@ struct Engine : public hg_ctx {
         HG_CK(cudaFuncSetAttribute(k_pk_bin<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         long long total = (long long)cn.x * cn.y * cn.z;
         unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 8);
+        kb("pk_bin", double(total) * sizeof(C));
         k_pk_bin<T><<<blocks, 256, smem, st>>>(half_spec(), half_spec(), g, tabs, lo, cn, dp<int2>(lut), lutn, nbin, L,
                                                S_re, S_im, cfg.assign, wpow, dp<double>(acc),
                                                dp<unsigned long long>(cnt_d), 0, 0.0, 0.0);
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         std::vector<double> a(2 * nbin * L.n);
         nm.assign(nbin, 0);
         HG_CK(cudaMemcpyAsync(a.data(), acc.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, st));
@@ -483,6 +568,7 @@ struct Engine : public hg_ctx {
         HG_CK(cudaEventRecord(ev0, st));
     }
     void end() {
+        prof_flush();
         HG_CK(cudaEventRecord(ev1, st));
         HG_CK(cudaEventSynchronize(ev1));
         float ms = 0.f;
@@ -580,11 +666,11 @@ struct Engine : public hg_ctx {
         auto b = std::make_unique<DBuf>();
         HG_CK(b->ensure(sizeof(double2) * std::max<long long>(n_ent(), 1)));
         if (n_ent() > 0) {
+            kb("shell_family_A", double(n_ent()) * 48.0);
             k_family_A<<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), g, f.l, f.m,
                                                             dp<double2>(shD), dp<double>(shells.d_scale),
                                                             dp<double2>(*b));
-            HG_CK(cudaGetLastError());
-            launches++;
+            ke();
         }
         const double2 *p = dp<double2>(*b);
         famA[f] = std::move(b);
@@ -611,11 +697,11 @@ struct Engine : public hg_ctx {
         }
         long long total = (long long)cn.x * cn.y * cn.z;
         unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 16);
+        kb("scatter_G", double(total) * (sizeof(C) * 2));
         k_scatter_G<T><<<blocks, 256, 0, st>>>(half_spec(), g, tabs, wpow, lo, cn,
                                                make_int3(S.M[0], S.M[1], S.M[2]), delta0, 0.0, dp<C>(Gbuf));
-        HG_CK(cudaGetLastError());
-        launches++;
-        fft3<+1>(dp<C>(Gbuf), 1, S.M);
+        ke();
+        fft3<+1>(dp<C>(Gbuf), 1, S.M, "fft_G_inv");
         G_valid = true;
     }
 
@@ -630,24 +716,25 @@ struct Engine : public hg_ctx {
         HG_CK(chain.ensure(sizeof(C) * vol * S.ns));
         HG_CK(cudaMemsetAsync(chain.p, 0, sizeof(C) * vol * S.ns, st));
         int3 M3 = make_int3(S.M[0], S.M[1], S.M[2]);
+        kb("scatter_entries", double(n_ent()) * (16.0 + sizeof(C)));
         k_scatter_entries<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), A, M3,
                                                                   dp<C>(chain));
-        HG_CK(cudaGetLastError());
-        launches++;
-        fft3<+1>(dp<C>(chain), S.ns, S.M);
+        ke();
+        fft3<+1>(dp<C>(chain), S.ns, S.M, "fft_chain_inv");
         // forward: first pass multiplies by G
         C *p = dp<C>(chain);
         pass<-1>(S.M[2], LdMulG<T>{p, dp<C>(Gbuf), S.M[2], (long long)S.M[0] * S.M[1]}, StArr<T>{p, S.M[2], 1},
-                 (long long)S.ns * S.M[0] * S.M[1], 1);
-        pass<-1>(S.M[1], LdArr<T>{p, S.M[1], S.M[2]}, StArr<T>{p, S.M[1], S.M[2]}, (long long)S.ns * S.M[0], S.M[2]);
+                 (long long)S.ns * S.M[0] * S.M[1], 1, "fft_chain_fwd_mulG");
+        pass<-1>(S.M[1], LdArr<T>{p, S.M[1], S.M[2]}, StArr<T>{p, S.M[1], S.M[2]}, (long long)S.ns * S.M[0], S.M[2],
+                 "fft_chain_fwd");
         pass<-1>(S.M[0], LdArr<T>{p, S.M[0], (long long)S.M[1] * S.M[2]},
-                 StArr<T>{p, S.M[0], (long long)S.M[1] * S.M[2]}, S.ns, (long long)S.M[1] * S.M[2]);
+                 StArr<T>{p, S.M[0], (long long)S.M[1] * S.M[2]}, S.ns, (long long)S.M[1] * S.M[2], "fft_chain_fwd");
         auto q = std::make_unique<DBuf>();
         HG_CK(q->ensure(sizeof(double2) * std::max<long long>(n_ent(), 1) * S.ns));
         dim3 gr(grid1(n_ent(), 256), S.ns);
+        kb("extract_neg", double(n_ent()) * S.ns * (16.0 + sizeof(C)));
         k_extract_neg<T><<<gr, 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), S.ns, M3, p, dp<double2>(*q));
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         const double2 *r = dp<double2>(*q);
         famQ[b] = std::move(q);
         return r;
@@ -664,9 +751,9 @@ struct Engine : public hg_ctx {
         DBuf out;
         HG_CK(out.ensure(sizeof(double2) * S.ns * S.ns));
         dim3 gr(S.ns, S.ns);
+        kb("pair_dot", double(n_ent()) * (S.ns + 1) * 16.0);
         k_pair_dot<<<gr, 256, 0, st>>>(dp<int>(shells.d_start), S.ns, A, Q, n_ent(), S.ns, dp<double2>(out));
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         std::vector<double> h(2 * S.ns * S.ns);
         HG_CK(cudaMemcpyAsync(h.data(), out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
@@ -699,10 +786,10 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(n_ent() > 0, "no Fourier modes fall inside the k shells");
         if (!shD.p || shD.n < sizeof(double2) * n_ent() || famA.empty()) {
             HG_CK(shD.ensure(sizeof(double2) * n_ent()));
+            kb("shell_D", double(n_ent()) * (16.0 + sizeof(C)));
             k_shell_D<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), half_spec(), g,
                                                               tabs, wpow, dp<double2>(shD));
-            HG_CK(cudaGetLastError());
-            launches++;
+            ke();
         }
     }
 
@@ -747,8 +834,10 @@ struct Engine : public hg_ctx {
         const double invV = 1.0 / g.volume;  // field.hpp:1122
         LdXiHat<T> ld{half_spec(), g, tabs, cfg.assign, wpow, S, 0.0, delta0 * N0, 0.0, invV};
         long long yz = (long long)g.n[1] * g.n[2];
-        pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz);
-        pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2]);
+        pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
+                 double(g.ntot) * sizeof(C) * 1.5);
+        pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
+                 "fft_xi_y");
         HG_CK(hist.ensure(sizeof(double) * 2 * n2dim * hs.nh));
         HG_CK(cudaMemsetAsync(hist.p, 0, sizeof(double) * 2 * n2dim * hs.nh, st));
         int n_orb = (int)orbit_n2xy.size();
@@ -759,10 +848,10 @@ struct Engine : public hg_ctx {
     void launch_orbit_L(const HistSpec &hs, int n_orb) {
         size_t smem = sizeof(C) * 8 * (L + 1);
         HG_CK(cudaFuncSetAttribute(k_xi_orbit_hist<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kb("xi_orbit_hist", double(g.ntot) * sizeof(C));
         k_xi_orbit_hist<T, L><<<n_orb, L, smem, st>>>(dp<C>(xi), dp<int>(d_orbit_lines), dp<int>(d_orbit_n2xy),
                                                      n_orb, twiddles(L), hs, n2dim, dp<double>(hist));
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
     }
     void launch_orbit(int L, const HistSpec &hs, int n_orb) {
         switch (L) {
@@ -802,11 +891,11 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemcpyAsync(d_kv.p, kv.data(), sizeof(double) * kv.size(), cudaMemcpyHostToDevice, st));
         HG_CK(J.ensure(sizeof(double) * kv.size() * n2dim));
         long long tot = (long long)kv.size() * n2dim;
+        kb("bessel_table", double(tot) * 8.0);
         k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second),
                                                         s.n, s.xmin, s.dx, dp<double>(d_kv), (int)kv.size(), g.dr[0],
                                                         n2dim, dp<double>(J));
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         HG_CK(cudaStreamSynchronize(st));
     }
 
@@ -882,10 +971,10 @@ struct Engine : public hg_ctx {
         bessel_table(l1, kbin, Jtab1);
         bessel_table(l2, kbin, Jtab2);
         HG_CK(snmat.ensure(sizeof(double2) * ns * ns));
+        kb("sn_matrix", double(ns) * ns * n2dim * 24.0);
         k_sn_matrix<<<dim3(ns, ns), 256, 0, st>>>(dp<double>(Jtab1), dp<double>(Jtab2), dp<double>(hist), n2dim, ns,
                                                  dp<double2>(snmat));
-        HG_CK(cudaGetLastError());
-        launches++;
+        ke();
         std::vector<double> sd(2 * ns * ns);
         HG_CK(cudaMemcpyAsync(sd.data(), snmat.p, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
@@ -981,7 +1070,29 @@ const char *hg_last_error(const hg_ctx *ctx) {
 
 int hg_set_particles(hg_ctx *ctx, int slot, const double *base, long long n, long long stride_bytes, int pos_off,
                      int los_off, int w_off) {
-    HG_GUARD(ctx, ctx->set_particles(slot, base, n, stride_bytes, pos_off, los_off, w_off));
+    HG_GUARD(ctx, ctx->set_particles(slot, base, n, stride_bytes, pos_off, los_off, w_off, false));
+}
+
+int hg_set_particles_device(hg_ctx *ctx, int slot, const double *dev_base, long long n, long long stride_bytes,
+                            int pos_off, int los_off, int w_off) {
+    HG_GUARD(ctx, ctx->set_particles(slot, dev_base, n, stride_bytes, pos_off, los_off, w_off, true));
+}
+
+int hg_set_profiling(hg_ctx *ctx, int on) { HG_GUARD(ctx, ctx->set_profiling(on != 0)); }
+
+int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen) {
+    if (!ctx || !buf || buflen <= 0) return -1;
+    std::string s;
+    try {
+        s = ctx->kernel_stats();
+    } catch (const HgError &e) {
+        ctx->err = e.msg;
+        return -1;
+    }
+    long long n = std::min<long long>((long long)s.size(), buflen - 1);
+    memcpy(buf, s.data(), (size_t)n);
+    buf[n] = 0;
+    return 0;
 }
 
 int hg_pk_box(hg_ctx *ctx, int ell, double *pk_save, int *n_mode, double *norm) {

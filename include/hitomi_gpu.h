@@ -75,6 +75,12 @@ const char *hg_last_error(const hg_ctx *ctx);
 int hg_set_particles(hg_ctx *ctx, int slot, const double *base, long long n, long long stride_bytes, int pos_off,
                      int los_off, int w_off);
 
+/* As hg_set_particles, but base points to DEVICE memory on the context's GPU that the
+ * caller keeps alive and unchanged until the next hg_set_particles* call on this slot or
+ * hg_destroy.  Nothing is copied.  (Same reference interface as hg_set_particles.) */
+int hg_set_particles_device(hg_ctx *ctx, int slot, const double *dev_base, long long n, long long stride_bytes,
+                            int pos_off, int los_off, int w_off);
+
 /* Periodic-box power-spectrum multipole.  Replaces the arithmetic of
  * calcPowerSpectrumForBOX (powerspec.hpp:273-332): TSC/CIC/NGP assignment
  * (field.hpp:67-184), dn = n - N/V (field.hpp:505-525), FFT (field.hpp:310-325) and the
@@ -110,6 +116,13 @@ int hg_survey_scalars(hg_ctx *ctx, double *alpha, double *vsurvey, double *nbar,
  * Wigner-3j weights.  alpha and vsurvey are the values the caller passes to the
  * reference function.  *norm = V_survey / (sum w_D)^2 (particle.hpp:303-316). */
 int hg_pk_survey(hg_ctx *ctx, int ell, double alpha, double vsurvey, double *pk_save, int *n_mode, double *norm);
+
+/* Per-kernel device timing: when on, every kernel launch of this library is bracketed by
+ * CUDA events on the context's stream.  hg_kernel_stats writes one line per kernel name:
+ * "name<TAB>launches<TAB>total_ms<TAB>modelled_bytes".  These replace the reference's
+ * clock() progress prints (bispec.hpp:1170-1171, powerspec.hpp:63-66). */
+int hg_set_profiling(hg_ctx *ctx, int on);
+int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen);
 
 /* Device-side time of the last statistic call in milliseconds (CUDA events on the
  * context's stream), and the number of kernels it launched. */

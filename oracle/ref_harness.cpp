@@ -18,6 +18,9 @@
  *     survey : data.f64 / random.f64 hold n x 4 doubles (x y z w)
  *   --all-rows : for measure = bk / 3PCF, run every ith_kbin / ith_rbin row
  *                (the reference computes one row per process, main.cpp:78-84).
+ *   --unit OP  : (box) time one building block of the reference's estimators once and
+ *                print "HX_UNIT OP seconds"; OP in assign fft ifft corr bin_l0 bin_l2
+ *                xi_ijk ylmk ylmx shell triple snloop spline.
  * Environment:
  *   HX_FULL=1    : result files are written with 17 significant digits instead of
  *                  the reference's %.7e / %.5f (format strings are rewritten at
@@ -121,15 +124,151 @@ static int fail(const char *what) {
     return 1;
 }
 
+/* --unit OP: time one of the reference's periodic-box building blocks once, at the
+ * parameter file's mesh, on this process's single core.  Set-up is not timed.  The
+ * loops "triple" and "snloop" restate the inline driver loops of bispec.hpp:1158-1166
+ * and bispec.hpp:1023-1050 (they are not functions in the reference). */
+static volatile double hx_sink = 0.0;
+
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+static int unit_op(const std::string &op, ParticleGadgetClass &P_D, ParameterClass &param, std::vector<double> &kbin) {
+    double t = 0.0;
+    std::complex<double> shotnoise = double(P_D.n_tot);
+    double dk = kbin[1] - kbin[0];
+    int mid = param.n_kbin / 2;
+    if (op == "assign") {
+        DensityFieldClass<ParticleGadgetClass> dn(param);
+        t = now_s();
+        dn.calcNormalDensityFluctuationForBOX(P_D, param);
+        t = now_s() - t;
+    } else if (op == "fft" || op == "ifft" || op == "corr" || op == "bin_l0" || op == "bin_l2" || op == "xi_ijk") {
+        DensityFieldClass<ParticleGadgetClass> dn(param);
+        dn.calcNormalDensityFluctuationForBOX(P_D, param);
+        if (op == "fft") {
+            t = now_s();
+            dn.calcFourierTransform();
+            t = now_s() - t;
+        } else {
+            dn.calcFourierTransform();
+            TwoPointStatisticsClass<ParticleGadgetClass> stat(param);
+            if (op == "ifft") {
+                t = now_s();
+                dn.calcInverseFourierTransform();
+                t = now_s() - t;
+            } else if (op == "corr") {
+                t = now_s();
+                dn.calcAssignmentFunctionCorrection();
+                t = now_s() - t;
+            } else if (op == "bin_l0" || op == "bin_l2") {
+                int ell = (op == "bin_l0") ? 0 : 2;
+                t = now_s();
+                stat.calcPowerSpectrum(dn, dn, kbin.data(), shotnoise, ell, 0);
+                t = now_s() - t;
+            } else {
+                fftw_complex *xi = fftw_alloc_complex(param.n_mesh_tot);
+                for (long long i = 0; i < param.n_mesh_tot; i++) xi[i][0] = xi[i][1] = 0.0;
+                t = now_s();
+                stat.calcShotNoiseForBispectrum_ijk(dn, dn, shotnoise, 0, 0, xi);
+                t = now_s() - t;
+                fftw_free(xi);
+            }
+        }
+    } else if (op == "ylmk" || op == "ylmx") {
+        std::complex<double> *Y = new std::complex<double>[param.n_mesh_tot];
+        t = now_s();
+        if (op == "ylmk") ToolClass::storeReducedSphericalHarmonicsInFourierSpace(1, 0, param, Y);
+        else ToolClass::storeReducedSphericalHarmonicsInConfigurationSpace(1, 0, param, Y);
+        t = now_s() - t;
+        delete[] Y;
+    } else if (op == "shell") {
+        DensityFieldClass<ParticleGadgetClass> dn(param);
+        dn.calcNormalDensityFluctuationForBOX(P_D, param);
+        dn.calcFourierTransform();
+        std::complex<double> *Y = new std::complex<double>[param.n_mesh_tot];
+        ToolClass::storeReducedSphericalHarmonicsInFourierSpace(0, 0, param, Y);
+        DensityFieldClass<ParticleGadgetClass> tilde(param);
+        t = now_s();
+        tilde.calcInverseFourierTransformForBispectrum(dn, kbin[mid], dk, Y);
+        t = now_s() - t;
+        delete[] Y;
+    } else if (op == "triple") {
+        DensityFieldClass<ParticleGadgetClass> f1(param), f2(param), f3(param);
+        f1.calcNormalDensityFluctuationForBOX(P_D, param);
+        for (long long i = 0; i < param.n_mesh_tot; i++) {
+            f2.field[i][0] = f3.field[i][0] = f1.field[i][0];
+            f2.field[i][1] = f3.field[i][1] = 0.5;
+        }
+        t = now_s();
+        std::complex<double> bk_sum = 0.0;
+        double fac = param.volume / double(param.n_mesh_tot);
+        for (long long coord = 0; coord < param.n_mesh_tot; coord++) {
+            std::complex<double> a(f1[coord][0], f1[coord][1]);
+            std::complex<double> b(f2[coord][0], f2[coord][1]);
+            std::complex<double> c(f3[coord][0], f3[coord][1]);
+            bk_sum += (fac * a * b * c);
+        }
+        t = now_s() - t;
+        hx_sink = bk_sum.real() + bk_sum.imag();
+    } else if (op == "snloop" || op == "spline") {
+        double t0 = now_s();
+        SphericalBesselClass sj1(0), sj2(0);
+        double tsp = now_s() - t0;
+        if (op == "spline") {
+            t = tsp / 2.0;
+        } else {
+            std::complex<double> *Y1 = new std::complex<double>[param.n_mesh_tot];
+            std::complex<double> *Y2 = new std::complex<double>[param.n_mesh_tot];
+            fftw_complex *xi = fftw_alloc_complex(param.n_mesh_tot);
+            for (long long i = 0; i < param.n_mesh_tot; i++) {
+                Y1[i] = Y2[i] = 1.0;
+                xi[i][0] = 1.0e-3 * double(i % 7);
+                xi[i][1] = 0.0;
+            }
+            double kmag1 = kbin[0], kmag2 = kbin[mid];
+            t = now_s();
+            std::complex<double> sn_sum = 0.0;
+            double dr[3] = {param.boxsize[0] / double(param.n_mesh[0]), param.boxsize[1] / double(param.n_mesh[1]),
+                            param.boxsize[2] / double(param.n_mesh[2])};
+            for (int i = 0; i < param.n_mesh[0]; i++)
+                for (int j = 0; j < param.n_mesh[1]; j++)
+                    for (int k = 0; k < param.n_mesh[2]; k++) {
+                        long long coord = ((long long)i * param.n_mesh[1] + j) * param.n_mesh[2] + k;
+                        double rv0 = (i < param.n_mesh[0] / 2) ? (double)i * dr[0] : (double)(i - param.n_mesh[0]) * dr[0];
+                        double rv1 = (j < param.n_mesh[1] / 2) ? (double)j * dr[1] : (double)(j - param.n_mesh[1]) * dr[1];
+                        double rv2 = (k < param.n_mesh[2] / 2) ? (double)k * dr[2] : (double)(k - param.n_mesh[2]) * dr[2];
+                        double rmag = sqrt(rv0 * rv0 + rv1 * rv1 + rv2 * rv2);
+                        std::complex<double> ff(xi[coord][0], xi[coord][1]);
+                        double j1 = sj1.getSphericalBessel(kmag1 * rmag);
+                        double j2 = sj2.getSphericalBessel(kmag2 * rmag);
+                        sn_sum += (j1 * j2 * ff * Y1[coord] * Y2[coord]);
+                    }
+            t = now_s() - t;
+            hx_sink = sn_sum.real() + sn_sum.imag();
+            delete[] Y1;
+            delete[] Y2;
+            fftw_free(xi);
+        }
+    } else {
+        return fail(("unknown unit op " + op).c_str());
+    }
+    std::printf("HX_UNIT %s %.6f\n", op.c_str(), t);
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc < 3) {
         std::fprintf(stderr, "usage: ref_harness param.ini data.f64 [random.f64] [--all-rows]\n");
         return 2;
     }
     bool all_rows = false;
+    std::string unit;
     std::vector<const char *> pos;
     for (int i = 1; i < argc; i++) {
         if (!strcmp(argv[i], "--all-rows")) all_rows = true;
+        else if (!strcmp(argv[i], "--unit") && i + 1 < argc) unit = argv[++i];
         else pos.push_back(argv[i]);
     }
     char *pargv[2] = {argv[0], (char *)pos[0]};
@@ -152,6 +291,7 @@ int main(int argc, char **argv) {
         for (long long i = 0; i < n; i++)
             for (int ax = 0; ax < 3; ax++) P_D[i].pos[ax] = a[3 * i + ax];
         P_D.calcMinAndMax();
+        if (!unit.empty()) return unit_op(unit, P_D, param, kbin);
         t0 = std::chrono::steady_clock::now();
         if (param.measure == "pk") {
             rc = calcPowerSpectrumForBOX(P_D, param, kbin.data());

@@ -11,9 +11,10 @@
  *   FFTW_BACKWARD (+1):  X[k] = sum_j x[j] exp(+2 pi i j k / n)
  * applied along each of the three axes of a row-major n0 x n1 x n2 array.
  *
- * Algorithm: recursive decimation-in-time Cooley-Tukey over the prime factors of
- * n (radix 4/2 fast paths, direct DFT for odd prime factors), twiddles from
- * sincos of an exactly reduced angle.  Nothing here is FFTW's code; results
+ * Algorithm: power-of-two lengths use an iterative Stockham autosort FFT (radix 4,
+ * one radix-2 stage when log2 n is odd); other lengths a recursive Cooley-Tukey over
+ * their prime factors with direct DFTs of the odd primes.  Twiddles come from sincos
+ * of an exactly reduced angle.  Nothing here is FFTW's code; results
  * agree with FFTW-double to ~1e-15 relative, far inside the oracle's 1e-10 budget.
  */
 #ifndef HITOMI_ORACLE_FFTW3_SHIM_H
@@ -76,10 +77,16 @@ static inline cd twiddle(long long k, long long n, int sign) {
 struct Plan1D {
     int n;
     int sign;
-    std::vector<int> factors;      /* radix sequence */
+    bool pow2;
+    std::vector<int> factors;      /* radix sequence (general sizes) */
     std::vector<cd> tw;            /* tw[k] = exp(sign 2 pi i k / n), k in [0,n) */
     mutable std::vector<cd> work;
+    /* power-of-two sizes: iterative Stockham, radix 4 then one radix 2 if needed,
+       per-stage twiddles stored contiguously */
+    std::vector<int> radix;
+    std::vector<std::vector<cd>> stw;
     Plan1D(int n_, int sign_) : n(n_), sign(sign_) {
+        pow2 = (n & (n - 1)) == 0;
         int m = n;
         while (m % 4 == 0) { factors.push_back(4); m /= 4; }
         while (m % 2 == 0) { factors.push_back(2); m /= 2; }
@@ -89,15 +96,26 @@ struct Plan1D {
         tw.resize(n);
         for (int k = 0; k < n; k++) tw[k] = twiddle(k, n, sign);
         work.resize(n);
+        if (pow2) {
+            int Ns = 1;
+            while (Ns < n) {
+                int R = (n / Ns >= 4) ? 4 : 2;
+                radix.push_back(R);
+                /* twiddles w_{Ns R}^{r k}, k in [0,Ns), r in [1,R) */
+                std::vector<cd> t((size_t)Ns * (R - 1));
+                for (int k = 0; k < Ns; k++)
+                    for (int r = 1; r < R; r++) t[(size_t)k * (R - 1) + (r - 1)] = tw[(size_t)((long long)r * k * (n / (Ns * R)))];
+                stw.push_back(t);
+                Ns *= R;
+            }
+        }
     }
     /* out[k*os] = sum_j in[j*is] w^(jk), length len = product of factors[f..] */
     void rec(const cd *in, long long is, cd *out, int len, size_t f) const {
         if (len == 1) { out[0] = in[0]; return; }
         int p = factors[f];
         int m = len / p;
-        /* sub-transforms of the p decimated sequences, stored contiguously */
         for (int r = 0; r < p; r++) rec(in + r * is, is * p, out + (long long)r * m, m, f + 1);
-        /* combine: X[k + q m] = sum_r w_len^{r (k + q m)} Y_r[k] */
         long long tstride = (long long)n / len;
         cd tmp[64];
         std::vector<cd> big;
@@ -105,30 +123,55 @@ struct Plan1D {
         if (p > 64) { big.resize(p); t = big.data(); }
         for (int k = 0; k < m; k++) {
             for (int r = 0; r < p; r++) t[r] = out[(long long)r * m + k] * tw[(size_t)((long long)r * k * tstride % n)];
-            if (p == 2) {
-                out[k] = t[0] + t[1];
-                out[k + m] = t[0] - t[1];
-            } else if (p == 4) {
-                cd a0 = t[0] + t[2], a1 = t[0] - t[2];
-                cd b0 = t[1] + t[3], b1 = t[1] - t[3];
-                /* multiply by exp(sign * i pi/2) = sign * i */
-                cd jb1 = cd(-sign * b1.imag(), sign * b1.real());
-                out[k] = a0 + b0;
-                out[k + m] = a1 + jb1;
-                out[k + 2 * m] = a0 - b0;
-                out[k + 3 * m] = a1 - jb1;
-            } else {
-                long long ps = (long long)n / p;
-                for (int q = 0; q < p; q++) {
-                    cd acc = 0.0;
-                    for (int r = 0; r < p; r++) acc += t[r] * tw[(size_t)(((long long)r * q % p) * ps)];
-                    work[q] = acc;
-                }
-                for (int q = 0; q < p; q++) out[k + (long long)q * m] = work[q];
+            long long ps = (long long)n / p;
+            for (int q = 0; q < p; q++) {
+                cd acc = 0.0;
+                for (int r = 0; r < p; r++) acc += t[r] * tw[(size_t)(((long long)r * q % p) * ps)];
+                work[q] = acc;
             }
+            for (int q = 0; q < p; q++) out[k + (long long)q * m] = work[q];
         }
     }
+    /* Stockham autosort: X = DFT(x), ping-pong between a and b, result returned */
+    cd *stockham(cd *a, cd *b) const {
+        int Ns = 1;
+        const double sg = (double)sign;
+        for (size_t s = 0; s < radix.size(); s++) {
+            int R = radix[s];
+            int LR = n / R;
+            const cd *t = stw[s].data();
+            if (R == 4) {
+                for (int j = 0; j < LR; j++) {
+                    int k = j % Ns;
+                    cd v0 = a[j], v1 = a[j + LR] * t[3 * k], v2 = a[j + 2 * LR] * t[3 * k + 1], v3 = a[j + 3 * LR] * t[3 * k + 2];
+                    cd a0 = v0 + v2, a1 = v0 - v2, b0 = v1 + v3, b1 = v1 - v3;
+                    cd jb1(-sg * b1.imag(), sg * b1.real());
+                    int d = (j / Ns) * Ns * 4 + k;
+                    b[d] = a0 + b0;
+                    b[d + Ns] = a1 + jb1;
+                    b[d + 2 * Ns] = a0 - b0;
+                    b[d + 3 * Ns] = a1 - jb1;
+                }
+            } else {
+                for (int j = 0; j < LR; j++) {
+                    int k = j % Ns;
+                    cd v0 = a[j], v1 = a[j + LR] * t[k];
+                    int d = (j / Ns) * Ns * 2 + k;
+                    b[d] = v0 + v1;
+                    b[d + Ns] = v0 - v1;
+                }
+            }
+            std::swap(a, b);
+            Ns *= R;
+        }
+        return a;
+    }
     void exec(cd *data, cd *scratch) const {
+        if (pow2) {
+            cd *r = stockham(data, scratch);
+            if (r != data) memcpy((void *)data, (const void *)r, sizeof(cd) * n);
+            return;
+        }
         rec(data, 1, scratch, n, 0);
         memcpy((void *)data, (const void *)scratch, sizeof(cd) * n);
     }

@@ -1,0 +1,124 @@
+"""Regenerate the golden fixtures in tests/golden/ from the CPU oracle.
+
+The values come from oracle/_ref/ref_harness: the reference's own estimator headers
+(src/hitomi_measurement/*.hpp) compiled against the project's FFTW/GSL shims, run
+with 17-significant-digit output.  Inputs are stored in the fixture next to the outputs
+so the GPU tests need neither the reference sources nor the harness.
+
+    python tests/golden/make_golden.py        (needs `make -C oracle` first)
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from hitomi_b200.api import Binning  # noqa: E402
+from hitomi_b200.synthetic import lognormal_box, uniform_box  # noqa: E402
+from oracle import ref_runner  # noqa: E402
+
+MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2))
+
+
+def binning_arr(b: Binning):
+    return np.array([b.kmin, b.kmax, b.n_kbin, b.rmin, b.rmax, b.n_rbin], dtype=np.float64)
+
+
+def edge_catalogue(n_mesh: int, boxsize: float, n: int, seed: int) -> np.ndarray:
+    """Particles concentrated on cell edges and on the box faces, where the reference's
+    flat-index rule (field.hpp:92-96) drops or moves stencil points."""
+    rng = np.random.default_rng(seed)
+    dr = boxsize / n_mesh
+    pos = rng.uniform(0.0, boxsize, size=(n, 3))
+    k = n // 3
+    # on cell edges and half-cell points
+    pos[:k] = np.floor(pos[:k] / dr) * dr + rng.choice([0.0, 0.5 * dr, 1e-9, dr - 1e-9], size=(k, 3))
+    # hugging the upper and lower faces
+    face = rng.integers(0, 3, size=k)
+    side = rng.random(k) < 0.5
+    vals = np.where(side, boxsize - rng.uniform(0.0, 0.75 * dr, k), rng.uniform(0.0, 0.75 * dr, k))
+    pos[k:2 * k][np.arange(k), face] = vals
+    pos = np.clip(pos, 0.0, np.nextafter(boxsize, 0.0))
+    return np.ascontiguousarray(pos)
+
+
+def run_pk(pos, n_mesh, boxsize, b, assign, ells=(0, 2, 4)):
+    out = {}
+    for ell in ells:
+        with ref_runner.RefRun() as r:
+            r.run("pk", pos, ell, 0, ell, n_mesh, boxsize, b, assign=assign)
+            out[ell] = r.pk(ell)[1]
+    return out
+
+
+def run_bk(pos, n_mesh, boxsize, b, assign, mps=MULTIPOLES):
+    out = {}
+    for mp in mps:
+        with ref_runner.RefRun() as r:
+            r.run("bk", pos, *mp, n_mesh, boxsize, b, assign=assign)
+            out[mp] = r.bk(*mp, b.n_kbin)
+    return out
+
+
+def main():
+    if not ref_runner.available():
+        raise SystemExit("build the oracle first: make -C oracle")
+    # smoke case
+    pos = lognormal_box(20000, 1000.0, ngrid=32, seed=5, exact_n=20000)
+    b = Binning(0.02, 0.08, 4, 4.0, 156.0, 20)
+    pk = run_pk(pos, 32, 1000.0, b, "TSC", ells=(0,))
+    bk = run_bk(pos, 32, 1000.0, b, "TSC", mps=((0, 0, 0),))
+    np.savez_compressed(os.path.join(HERE, "smoke_box_32.npz"), pos=pos, n_mesh=32, boxsize=1000.0,
+                        binning=binning_arr(b), pk0=pk[0], bk000=bk[(0, 0, 0)])
+
+    # power spectrum multipoles, every assignment scheme, two meshes
+    pos = lognormal_box(15000, 1000.0, ngrid=32, seed=11, exact_n=15000)
+    bp = Binning(0.005, 0.295, 30, 4.0, 156.0, 20)
+    d = dict(pos=pos, boxsize=1000.0, binning=binning_arr(bp))
+    for nm in (32, 64):
+        for assign in ("NGP", "CIC", "TSC"):
+            for ell, v in run_pk(pos, nm, 1000.0, bp, assign).items():
+                d[f"pk_{nm}_{assign}_{ell}"] = v
+    np.savez_compressed(os.path.join(HERE, "box_pk.npz"), **d)
+
+    # bispectrum multipoles, all rows, TSC; (000) also for NGP and CIC
+    pos = lognormal_box(12000, 1000.0, ngrid=32, seed=12, exact_n=12000)
+    bb = Binning(0.015, 0.075, 7, 4.0, 156.0, 20)
+    d = dict(pos=pos, boxsize=1000.0, binning=binning_arr(bb), n_mesh=32)
+    for mp, v in run_bk(pos, 32, 1000.0, bb, "TSC").items():
+        d["bk_TSC_" + "".join(map(str, mp))] = v
+    for assign in ("NGP", "CIC"):
+        for mp, v in run_bk(pos, 32, 1000.0, bb, assign, mps=((0, 0, 0),)).items():
+            d[f"bk_{assign}_" + "".join(map(str, mp))] = v
+    np.savez_compressed(os.path.join(HERE, "box_bk.npz"), **d)
+
+    # boundary-stress catalogue (flat-index bleed rule), P and B
+    pos = edge_catalogue(16, 400.0, 6000, seed=13)
+    be = Binning(0.02, 0.1, 5, 4.0, 156.0, 20)
+    d = dict(pos=pos, boxsize=400.0, n_mesh=16, binning=binning_arr(be))
+    for assign in ("NGP", "CIC", "TSC"):
+        for ell, v in run_pk(pos, 16, 400.0, be, assign, ells=(0, 2)).items():
+            d[f"pk_{assign}_{ell}"] = v
+        d[f"bk_{assign}_000"] = run_bk(pos, 16, 400.0, be, assign, mps=((0, 0, 0),))[(0, 0, 0)]
+    np.savez_compressed(os.path.join(HERE, "box_edges.npz"), **d)
+
+    # a uniform catalogue on a non-cubic mesh (P only: shot-noise histograms need cubic cells)
+    pos = uniform_box(8000, 1000.0, seed=14)
+    bn = Binning(0.01, 0.15, 8, 4.0, 156.0, 20)
+    d = dict(pos=pos, boxsize=np.array([1000.0, 1000.0, 1000.0]), n_mesh=np.array([16, 32, 64]),
+             binning=binning_arr(bn))
+    for ell in (0, 2):
+        with ref_runner.RefRun() as r:
+            r.run("pk", pos, ell, 0, ell, [16, 32, 64], 1000.0, bn)
+            d[f"pk_{ell}"] = r.pk(ell)[1]
+    np.savez_compressed(os.path.join(HERE, "box_noncubic.npz"), **d)
+    print("fixtures written")
+
+
+if __name__ == "__main__":
+    main()
