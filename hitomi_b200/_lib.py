@@ -20,6 +20,7 @@ SYMBOLS = (
     "hg_set_particles_device",
     "hg_pk_box",
     "hg_bk_box",
+    "hg_bk_box_multi",
     "hg_zeta_box",
     "hg_survey_scalars",
     "hg_pk_survey",
@@ -84,6 +85,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_pk_box.restype = ctypes.c_int
     lib.hg_bk_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, c_dp]
     lib.hg_bk_box.restype = ctypes.c_int
+    lib.hg_bk_box_multi.argtypes = [vp, ctypes.c_int, c_ip, ctypes.c_int, c_dp, c_dp, c_dp]
+    lib.hg_bk_box_multi.restype = ctypes.c_int
     lib.hg_zeta_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, c_dp]
     lib.hg_zeta_box.restype = ctypes.c_int
     lib.hg_survey_scalars.argtypes = [vp, c_dp, c_dp, c_dp, c_dp, c_dp]

@@ -149,6 +149,20 @@ class Context:
         c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(rows, nk)
         return c(bk), c(sn), norm.value
 
+    def bk_box_multi(self, multipoles, ith_kbin: int = -1):
+        """Several (ell1, ell2, ELL) multipoles at once; returns lists of (bk, sn) and norm."""
+        nk = self.binning.n_kbin
+        rows = nk if ith_kbin < 0 else 1
+        m = len(multipoles)
+        ells = np.array([v for mp in multipoles for v in mp], dtype=np.int32)
+        bk = np.zeros(2 * m * rows * nk)
+        sn = np.zeros(2 * m * rows * nk)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_bk_box_multi(self._h, m, ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                              ith_kbin, _dp(bk), _dp(sn), ctypes.byref(norm)))
+        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nk)
+        return c(bk), c(sn), norm.value
+
     def zeta_box(self, ell1: int, ell2: int, ELL: int, ith_rbin: int = -1):
         nr = self.binning.n_rbin
         rows = nr if ith_rbin < 0 else 1

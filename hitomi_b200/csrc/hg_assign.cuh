@@ -1,13 +1,17 @@
 // hg_assign.cuh -- particle-to-mesh assignment (NGP/CIC/TSC, PCS extension) for sm_100a.
 //
-// Sorted-by-tile scatter with no global float atomics:
+// Sorted-by-tile scatter with no global float atomics in the particle loop:
 //   1. k_bin_count   : per particle, the reference's cell/weight arithmetic in FP64
 //                      (field.hpp:80-90 NGP, :117-129 CIC, :158-172 TSC), the set of
-//                      output tiles its stencil touches, and the FP64 in-bounds mass;
-//   2. exclusive scan of the per-tile counts;
+//                      output tiles its stencil touches (warp-aggregated counts), and
+//                      the FP64 in-bounds mass;
+//   2. exclusive scan of the per-tile counts; tiles cut into chunks of <= CH records;
 //   3. k_bin_scatter : one compact record per (particle, tile) in tile order;
-//   4. k_tile_accum  : one CTA per tile accumulates its records in shared memory and
-//                      writes the tile exactly once, coalesced.
+//   4. k_tile_accum  : one CTA per chunk accumulates its records in an FP64 shared-memory
+//                      tile; a tile with a single chunk is written once, coalesced; the
+//                      chunks of a densely populated tile (clustered catalogues) are
+//                      zeroed first and add their partial tiles (one add per cell per
+//                      chunk, not per particle).
 // A particle whose stencil straddles tiles is duplicated into each of them; each CTA
 // keeps only the stencil points that fall in its own tile.
 //
@@ -177,19 +181,20 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 }
 
 // Pass 1: tile counts + FP64 in-bounds mass  sum_p w_p factor prod(w_axis)  (the field's
-// exact integral, needed for the k = 0 mode since boundary drops lose mass).
+// exact integral, needed for the k = 0 mode since boundary drops lose mass).  Clustered
+// catalogues put many lanes of a warp on the same tile, so the count is warp-aggregated.
 __global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double *mass) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double m_re = 0.0, m_im = 0.0;
+    int tiles[64];
+    int nt = 0;
     if (p < src.n) {
         double pos[3], wr, wi;
         load_particle(src, p, pos, wr, wi);
         int anc[3];
         double d[3];
         for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
-        int tiles[64];
-        int nt = particle_tiles(g, anc, tiles);
-        for (int q = 0; q < nt; q++) atomicAdd(&cnt[tiles[q]], 1u);
+        nt = particle_tiles(g, anc, tiles);
         // in-bounds mass in the reference's product order
         const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
         double w[3][4];
@@ -203,9 +208,16 @@ __global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double
                     m_im += wi * g.factor * w[0][a] * w[1][b] * w[2][c];
                 }
     }
+    const int lane = threadIdx.x & 31;
+    int maxnt = __reduce_max_sync(0xffffffffu, nt);
+    for (int q = 0; q < maxnt; q++) {
+        int t = (q < nt) ? tiles[q] : -1;
+        unsigned grp = __match_any_sync(0xffffffffu, t);
+        if (t >= 0 && lane == __ffs(grp) - 1) atomicAdd(&cnt[t], (unsigned)__popc(grp));
+    }
     m_re = warp_sum_d(m_re);
     m_im = warp_sum_d(m_im);
-    if ((threadIdx.x & 31) == 0 && (m_re != 0.0 || m_im != 0.0)) {
+    if (lane == 0 && (m_re != 0.0 || m_im != 0.0)) {
         atomicAdd(&mass[0], m_re);
         atomicAdd(&mass[1], m_im);
     }
@@ -214,49 +226,116 @@ __global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double
 template <typename T>
 __global__ void k_bin_scatter(PartSrc src, AssignGeom g, const unsigned int *off, unsigned int *cursor, PRec<T> *rec) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= src.n) return;
-    double pos[3], wr, wi;
-    load_particle(src, p, pos, wr, wi);
-    int anc[3];
-    double d[3];
-    for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
     int tiles[64];
-    int nt = particle_tiles(g, anc, tiles);
+    int nt = 0;
     PRec<T> r;
-    for (int a = 0; a < 3; a++) {
-        r.i[a] = anc[a];
-        r.d[a] = (T)d[a];
+    if (p < src.n) {
+        double pos[3], wr, wi;
+        load_particle(src, p, pos, wr, wi);
+        int anc[3];
+        double d[3];
+        for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
+        nt = particle_tiles(g, anc, tiles);
+        for (int a = 0; a < 3; a++) {
+            r.i[a] = anc[a];
+            r.d[a] = (T)d[a];
+        }
+        r.wr = (T)wr;
+        r.wi = (T)wi;
     }
-    r.wr = (T)wr;
-    r.wi = (T)wi;
-    for (int q = 0; q < nt; q++) {
-        unsigned int slot = atomicAdd(&cursor[tiles[q]], 1u);
-        rec[off[tiles[q]] + slot] = r;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int maxnt = __reduce_max_sync(0xffffffffu, nt);
+    for (int q = 0; q < maxnt; q++) {
+        int t = (q < nt) ? tiles[q] : -1;
+        unsigned grp = __match_any_sync(0xffffffffu, t);
+        if (t >= 0) {
+            int leader = __ffs(grp) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(&cursor[t], (unsigned)__popc(grp));
+            base = __shfl_sync(grp, base, leader);
+            rec[off[t] + base + __popc(grp & lt)] = r;
+        }
     }
 }
 
-// One CTA per tile.  ACC is the shared-memory accumulator type (float/double); the
-// mesh stores the density rho = sum_p w_p (1/dV) prod(w_axis) like the reference.
+// Work item of the accumulation: records [r0, r1) of tile `tile`; `multi` when the tile's
+// records are split over several chunks (a clustered tile), in which case the tile is
+// zeroed first and every chunk adds its partial tile.
+struct Chunk {
+    int tile;
+    unsigned r0, r1;
+    int multi;  // 0: sole chunk; 1: first chunk of a split tile; 2: later chunk of a split tile
+};
+
+__global__ void k_chunk_count(const unsigned int *cnt, int ntiles, unsigned chunk, unsigned int *nch) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > ntiles) return;
+    nch[t] = (t == ntiles) ? 0u : max(1u, (cnt[t] + chunk - 1) / chunk);
+}
+
+__global__ void k_chunk_fill(const unsigned int *off, const unsigned int *choff, int ntiles, unsigned chunk, Chunk *ch) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    unsigned b = off[t], e = off[t + 1];
+    unsigned n = choff[t + 1] - choff[t];
+    for (unsigned c = 0; c < n; c++) {
+        Chunk k;
+        k.tile = t;
+        k.r0 = b + c * chunk;
+        k.r1 = min(e, b + (c + 1) * chunk);
+        k.multi = (n == 1) ? 0 : (c == 0 ? 1 : 2);
+        ch[choff[t] + c] = k;
+    }
+}
+
+__device__ __forceinline__ long long tile_cell(const AssignGeom &g, int tile, int li, int &lx, int &ly, int &lz) {
+    const int tz = tile % g.nt[2];
+    const int ty = (tile / g.nt[2]) % g.nt[1];
+    const int tx = tile / (g.nt[2] * g.nt[1]);
+    lz = li % g.t[2];
+    ly = (li / g.t[2]) % g.t[1];
+    lx = li / (g.t[2] * g.t[1]);
+    return ((long long)(tx * g.t[0] + lx) * g.n[1] + (ty * g.t[1] + ly)) * g.n[2] + (tz * g.t[2] + lz);
+}
+
+// Zero the cells of every split tile (run before the accumulation).
 template <typename T, bool CPLX>
-__global__ void k_tile_accum(const PRec<T> *rec, const unsigned int *off, AssignGeom g, T *mesh_re, T *mesh_im) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *acc = reinterpret_cast<T *>(smem_raw);
+__global__ void k_zero_split_tiles(const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
+    Chunk k = ch[blockIdx.x];
+    if (k.multi != 1) return;
     const int tcells = g.t[0] * g.t[1] * g.t[2];
-    T *acc_im = acc + tcells;
-    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
+    for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
+        int lx, ly, lz;
+        long long cell = tile_cell(g, k.tile, li, lx, ly, lz);
+        mesh_re[cell] = (T)0;
+        if (CPLX) mesh_im[cell] = (T)0;
+    }
+}
+
+// One CTA per chunk.  FP64 shared-memory accumulator (both forms); the mesh stores the
+// density rho = sum_p w_p (1/dV) prod(w_axis) like the reference, in T.
+template <typename T, bool CPLX>
+__global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *acc = reinterpret_cast<double *>(smem_raw);
+    const int tcells = g.t[0] * g.t[1] * g.t[2];
+    double *acc_im = acc + tcells;
+    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = 0.0;
     __syncthreads();
-    const int tile = blockIdx.x;
+    const Chunk k = ch[blockIdx.x];
+    const int tile = k.tile;
     const int tz = tile % g.nt[2];
     const int ty = (tile / g.nt[2]) % g.nt[1];
     const int tx = tile / (g.nt[2] * g.nt[1]);
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
     const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
-    const unsigned int r0 = off[tile], r1 = off[tile + 1];
-    const T factor = (T)g.factor;
-    for (unsigned int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    const double factor = g.factor;
+    for (unsigned r = k.r0 + threadIdx.x; r < k.r1; r += blockDim.x) {
         PRec<T> pr = rec[r];
-        T w[3][4];
-        for (int a = 0; a < 3; a++) axis_weights<T>(g.scheme, pr.d[a], w[a]);
+        double w[3][4];
+        for (int a = 0; a < 3; a++) axis_weights<double>(g.scheme, (double)pr.d[a], w[a]);
+        const double wr = (double)pr.wr, wi = (double)pr.wi;
         for (int a = 0; a < W; a++)
             for (int b = 0; b < W; b++)
                 for (int c = 0; c < W; c++) {
@@ -267,19 +346,21 @@ __global__ void k_tile_accum(const PRec<T> *rec, const unsigned int *off, Assign
                         (unsigned)lz >= (unsigned)g.t[2])
                         continue;
                     int li = (lx * g.t[1] + ly) * g.t[2] + lz;
-                    T v = pr.wr * factor * w[0][a] * w[1][b] * w[2][c];
-                    atomicAdd(&acc[li], v);
-                    if (CPLX) atomicAdd(&acc_im[li], pr.wi * factor * w[0][a] * w[1][b] * w[2][c]);
+                    atomicAdd(&acc[li], wr * factor * w[0][a] * w[1][b] * w[2][c]);
+                    if (CPLX) atomicAdd(&acc_im[li], wi * factor * w[0][a] * w[1][b] * w[2][c]);
                 }
     }
     __syncthreads();
     for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
-        int lz = li % g.t[2];
-        int ly = (li / g.t[2]) % g.t[1];
-        int lx = li / (g.t[2] * g.t[1]);
-        long long cell = ((long long)(ox + lx) * g.n[1] + (oy + ly)) * g.n[2] + (oz + lz);
-        mesh_re[cell] = acc[li];
-        if (CPLX) mesh_im[cell] = acc_im[li];
+        int lx, ly, lz;
+        long long cell = tile_cell(g, tile, li, lx, ly, lz);
+        if (k.multi == 0) {
+            mesh_re[cell] = (T)acc[li];
+            if (CPLX) mesh_im[cell] = (T)acc_im[li];
+        } else {
+            if (acc[li] != 0.0) atomicAdd(&mesh_re[cell], (T)acc[li]);
+            if (CPLX && acc_im[li] != 0.0) atomicAdd(&mesh_im[cell], (T)acc_im[li]);
+        }
     }
 }
 

@@ -1,7 +1,8 @@
 // hg_engine.cu -- the estimator engine behind the C ABI in include/hitomi_gpu.h.
 //
 // One Engine<T> per context; T = double for the plain FP64 form, float for the chosen
-// FP32 form (FP32 mesh / FFT / fields; FP64 bin sums, shell sums, scalars, shot noise).
+// FP32 form (FP32 mesh / FFT / fields; FP64 assignment accumulators, bin sums, shell
+// sums, scalars and shot-noise histograms).
 //
 // Periodic-box pipeline for one catalogue (cached until the particles change):
 //   assignment (hg_assign.cuh) -> rho(x) -> r2c forward FFT (z, y, x passes) -> delta(k)
@@ -14,8 +15,8 @@
 //   Qhat_b,j = FFT[F_b,j G],
 // on a reduced M^3 grid: the shells only hold modes with |n_a| <= s, so F F G needs
 // G only up to |n_a| <= 2s and is sampled without aliasing on any grid with M >= 4s+1.
-// One chain (inverse FFT, multiply by G, forward FFT) per (family b, shell j) then gives
-// the whole k1 x k2 matrix for every family a paired with b.
+// One chain (hg_chain.cuh: pruned inverse FFT, multiply by G, pruned forward FFT) per
+// (family b, shell j) then gives the whole k1 x k2 matrix for every family a paired with b.
 //
 // Bispectrum shot noise.  xi(x) = IFFT[(|delta|^2 - N C)/W^2]/V is transformed on the full
 // mesh; its last pass is fused with a histogram over integer n^2 = |x/dr|^2 (cubic cells),
@@ -25,11 +26,14 @@
 #include "hg_fft.cuh"
 #include "hg_assign.cuh"
 #include "hg_kspace.cuh"
+#include "hg_chain.cuh"
+#include "hg_fft2.cuh"
 #include "hg_special.hpp"
 
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -55,11 +59,12 @@ struct DBuf {
         p = nullptr;
         n = 0;
     }
+    // grows only; contents are not preserved across a growth
     cudaError_t ensure(size_t bytes) {
         if (bytes <= n && p) return cudaSuccess;
         release();
         cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
-        if (e == cudaSuccess) n = bytes;
+        if (e == cudaSuccess) n = bytes ? bytes : 16;
         else p = nullptr;
         return e;
     }
@@ -82,8 +87,8 @@ struct HgError {
                           std::to_string(__LINE__) + ")"};                                          \
     } while (0)
 
-#define HG_REQUIRE(cond, text)                  \
-    do {                                        \
+#define HG_REQUIRE(cond, text)                         \
+    do {                                               \
         if (!(cond)) throw HgError{std::string(text)}; \
     } while (0)
 
@@ -99,7 +104,10 @@ int next_pow2(int v) {
 struct Fam {
     int l, m;
     bool operator<(const Fam &o) const { return l != o.l ? l < o.l : m < o.m; }
-    bool operator==(const Fam &o) const { return l == o.l && m == o.m; }
+};
+
+struct MP {
+    int l1, l2, L;
 };
 
 }  // namespace
@@ -115,7 +123,8 @@ struct hg_ctx {
     virtual void set_profiling(bool on) = 0;
     virtual std::string kernel_stats() = 0;
     virtual void pk_box(int ell, double *pk_save, int *n_mode, double *norm) = 0;
-    virtual void bk_box(int l1, int l2, int L, int ith, double *bk_save, double *sn_save, double *norm) = 0;
+    virtual void bk_box_multi(const std::vector<MP> &mps, int ith, double *bk_save, double *sn_save,
+                              double *norm) = 0;
     virtual void zeta_box(int l1, int l2, int L, int ith, double *zeta_save, double *sn_save, double *norm) = 0;
     virtual void survey_scalars(double *alpha, double *vs, double *nbar, double *wd, double *wr) = 0;
     virtual void pk_survey(int ell, double alpha, double vs, double *pk_save, int *n_mode, double *norm) = 0;
@@ -137,12 +146,9 @@ struct Engine : public hg_ctx {
         DBuf raw;
         long long n = 0, stride = 0;
         int pos_off = 0, los_off = -1, w_off = -1;
-        std::vector<double> host_w;  // weights (survey), for FP64 host sums
-        const void *ext = nullptr;   // caller-owned device array (hg_set_particles_device)
+        const void *ext = nullptr;  // caller-owned device array (hg_set_particles_device)
         bool set = false;
-        const unsigned char *base() const {
-            return reinterpret_cast<const unsigned char *>(ext ? ext : raw.p);
-        }
+        const unsigned char *base() const { return reinterpret_cast<const unsigned char *>(ext ? ext : raw.p); }
     } slot[2];
 
     // tables
@@ -153,41 +159,53 @@ struct Engine : public hg_ctx {
     int lutn = 0;
 
     // assignment scratch
-    DBuf cnt, off, cursor, rec, cubtmp, mass;
+    DBuf cnt, off, cursor, rec, cubtmp, mass, nch, choff, chunks;
+    static constexpr unsigned CHUNK = 2048;  // records per accumulation CTA
     // fields
-    DBuf mesh;        // real density rho (box)
-    DBuf H;           // half spectrum of dV (rho - nbar)
+    DBuf mesh;  // real density rho (box)
+    DBuf H;     // half spectrum of dV (rho - nbar)
     bool dens_valid = false;
-    double dens_mass = 0.0;   // sum_cells rho  (FP64)
+    double dens_mass = 0.0;  // sum_cells rho  (FP64)
     double delta0 = 0.0, N0 = 0.0;
 
-    // bispectrum state
+    // binning scratch
+    DBuf bin_acc, bin_cnt;
+
+    // bispectrum state (geometry: built once per context)
     struct ShellSet {
         bool built = false;
         int ns = 0;
-        std::vector<int> start;       // [ns+1]
-        std::vector<int> nmode;       // [ns]
-        std::vector<ShellEnt> ent;    // sorted by shell
-        int s[3] = {0, 0, 0};         // max |n_a| of any shell mode
-        int M[3] = {0, 0, 0};         // reduced transform grid
-        int gext[3] = {0, 0, 0};      // G cube half extent (or -1: whole axis)
+        std::vector<int> start, nmode;
+        std::vector<ShellEnt> ent;  // sorted by shell
+        int s[3] = {0, 0, 0};       // max |n_a| of any shell mode; compact side K = 2s+1
+        int K[3] = {0, 0, 0};
+        int M[3] = {0, 0, 0};       // reduced transform grid
+        int gs[3] = {0, 0, 0};      // G cube half extent (2s, or n/2 when the axis is not reduced)
+        int KG[3] = {0, 0, 0};
         DBuf d_ent, d_start, d_scale;
     } shells;
+    // per-catalogue bispectrum state
     DBuf shD;                                   // delta/W per entry
-    std::map<Fam, std::unique_ptr<DBuf>> famA;  // A_f per entry
-    std::map<Fam, std::unique_ptr<DBuf>> famQ;  // QE_f [ns][ne]
-    DBuf Gbuf, chain;
-    bool G_valid = false;
-    std::map<std::pair<Fam, Fam>, std::vector<double>> pairs;  // [ns][ns] complex, key (a, b): sum A_a,i Q_b,j
+    std::map<Fam, std::unique_ptr<DBuf>> famA;  // A_f per entry (memory kept across catalogues)
+    std::set<Fam> famA_ok;
+    std::map<Fam, std::unique_ptr<DBuf>> famQ;  // Q cube per chain family
+    std::set<Fam> famQ_ok;
+    DBuf Gc, Gbuf, Ac, T1, T2, pair_out;
+    bool G_valid = false, shD_valid = false;
+    std::map<std::pair<Fam, Fam>, std::vector<double>> pairs;  // key (a, b): sum_e A_a[e] Q_b,j(-n_e)
 
     // shot-noise state
     DBuf xi;
+    bool xi_valid = false;
     std::vector<int> orbit_lines, orbit_n2xy;
     DBuf d_orbit_lines, d_orbit_n2xy;
     long long n2dim = 0;
     std::map<int, std::unique_ptr<BesselSpline>> splines;
     std::map<int, std::pair<std::unique_ptr<DBuf>, std::unique_ptr<DBuf>>> d_splines;
-    DBuf hist, Jtab1, Jtab2, snmat, d_kv;
+    std::map<int, std::unique_ptr<DBuf>> jtab_k;  // J_l[i][n2] at the k bins (geometry only)
+    std::map<std::array<int, 3>, std::unique_ptr<DBuf>> hist_mp;  // per multipole (catalogue)
+    std::set<std::array<int, 3>> hist_ok;
+    DBuf hist_tmp, snmat, d_kv;
 
     long long launches = 0;
 
@@ -205,44 +223,6 @@ struct Engine : public hg_ctx {
         double ms = 0.0, bytes = 0.0;
     };
     std::map<std::string, KAgg> kagg;
-    cudaEvent_t take_ev() {
-        if (!ev_pool.empty()) {
-            cudaEvent_t e = ev_pool.back();
-            ev_pool.pop_back();
-            return e;
-        }
-        cudaEvent_t e;
-        HG_CK(cudaEventCreate(&e));
-        return e;
-    }
-    void kb(const char *name, double bytes) {
-        launches++;
-        if (!profiling) return;
-        PRecd r{name, take_ev(), nullptr, bytes};
-        HG_CK(cudaEventRecord(r.a, st));
-        pend.push_back(r);
-    }
-    void ke() {
-        HG_CK(cudaGetLastError());
-        if (!profiling || pend.empty() || pend.back().b) return;
-        pend.back().b = take_ev();
-        HG_CK(cudaEventRecord(pend.back().b, st));
-    }
-    void prof_flush() {
-        if (pend.empty()) return;
-        HG_CK(cudaStreamSynchronize(st));
-        for (auto &r : pend) {
-            float ms = 0.f;
-            if (r.b) HG_CK(cudaEventElapsedTime(&ms, r.a, r.b));
-            KAgg &k = kagg[r.name];
-            k.launches++;
-            k.ms += ms;
-            k.bytes += r.bytes;
-            ev_pool.push_back(r.a);
-            if (r.b) ev_pool.push_back(r.b);
-        }
-        pend.clear();
-    }
 
     explicit Engine(const hg_config &c) {
         cfg = c;
@@ -284,11 +264,55 @@ struct Engine : public hg_ctx {
 
     ~Engine() override {
         if (st) cudaStreamSynchronize(st);
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        for (auto &r : pend) {
+            cudaEventDestroy(r.a);
+            if (r.b) cudaEventDestroy(r.b);
+        }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (st) cudaStreamDestroy(st);
     }
 
+    // ------------------------------------------------------------------ profiling
+    cudaEvent_t take_ev() {
+        if (!ev_pool.empty()) {
+            cudaEvent_t e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        HG_CK(cudaEventCreate(&e));
+        return e;
+    }
+    void kb(const char *name, double bytes) {
+        launches++;
+        if (!profiling) return;
+        PRecd r{name, take_ev(), nullptr, bytes};
+        HG_CK(cudaEventRecord(r.a, st));
+        pend.push_back(r);
+    }
+    void ke() {
+        HG_CK(cudaGetLastError());
+        if (!profiling || pend.empty() || pend.back().b) return;
+        pend.back().b = take_ev();
+        HG_CK(cudaEventRecord(pend.back().b, st));
+    }
+    void prof_flush() {
+        if (pend.empty()) return;
+        HG_CK(cudaStreamSynchronize(st));
+        for (auto &r : pend) {
+            float ms = 0.f;
+            if (r.b) HG_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+            KAgg &k = kagg[r.name];
+            k.launches++;
+            k.ms += ms;
+            k.bytes += r.bytes;
+            ev_pool.push_back(r.a);
+            if (r.b) ev_pool.push_back(r.b);
+        }
+        pend.clear();
+    }
     void set_profiling(bool on) override {
         profiling = on;
         if (on) kagg.clear();
@@ -302,6 +326,19 @@ struct Engine : public hg_ctx {
             out += line;
         }
         return out;
+    }
+    void begin() {
+        launches = 0;
+        HG_CK(cudaEventRecord(ev0, st));
+    }
+    void end() {
+        prof_flush();
+        HG_CK(cudaEventRecord(ev1, st));
+        HG_CK(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        HG_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        last_ms = ms;
+        last_launches = launches;
     }
 
     // ------------------------------------------------------------------ tables
@@ -365,10 +402,11 @@ struct Engine : public hg_ctx {
     }
 
     // ------------------------------------------------------------------ particles
-    void set_particles(int s, const double *base, long long n, long long stride, int pos_off, int los_off,
-                       int w_off, bool on_device) override {
+    void set_particles(int s, const double *base, long long n, long long stride, int pos_off, int los_off, int w_off,
+                       bool on_device) override {
         HG_REQUIRE(s == 0 || s == 1, "slot must be 0 (data) or 1 (randoms)");
         HG_REQUIRE(n > 0, "The number of particles should be > 0");
+        HG_REQUIRE(n < (1LL << 31), "more than 2^31 - 1 particles in one catalogue");
         HG_REQUIRE(base != nullptr, "null particle array");
         HG_REQUIRE(stride >= 24 && stride % 8 == 0, "stride_bytes must be a multiple of 8 and >= 24");
         HG_REQUIRE(pos_off >= 0 && (pos_off + 3) * 8 <= stride, "pos_off outside the record");
@@ -376,6 +414,10 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(los_off < 0 || (los_off + 3) * 8 <= stride, "los_off outside the record");
         Slot &S = slot[s];
         if (on_device) {
+            cudaPointerAttributes at;
+            HG_CK(cudaPointerGetAttributes(&at, base));
+            HG_REQUIRE(at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged,
+                       "hg_set_particles_device needs a device pointer");
             S.ext = base;
         } else {
             S.ext = nullptr;
@@ -395,8 +437,11 @@ struct Engine : public hg_ctx {
     void invalidate() {
         dens_valid = false;
         G_valid = false;
-        famA.clear();
-        famQ.clear();
+        shD_valid = false;
+        xi_valid = false;
+        famA_ok.clear();
+        famQ_ok.clear();
+        hist_ok.clear();
         pairs.clear();
     }
 
@@ -426,6 +471,8 @@ struct Engine : public hg_ctx {
         HG_CK(cnt.ensure(sizeof(unsigned) * (ntiles + 1)));
         HG_CK(off.ensure(sizeof(unsigned) * (ntiles + 1)));
         HG_CK(cursor.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(nch.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(choff.ensure(sizeof(unsigned) * (ntiles + 1)));
         HG_CK(mass.ensure(sizeof(double) * 2));
         HG_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned) * (ntiles + 1), st));
@@ -433,26 +480,43 @@ struct Engine : public hg_ctx {
         kb("assign_bin_count", double(src.n) * 24.0);
         k_bin_count<<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(cnt), dp<double>(mass));
         ke();
-        size_t tb = 0;
+        size_t tb = 0, tb2 = 0;
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
-        HG_CK(cubtmp.ensure(tb));
+        HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
+        HG_CK(cubtmp.ensure(std::max(tb, tb2)));
         kb("assign_scan", double(ntiles + 1) * 8.0);
         HG_CK(cub::DeviceScan::ExclusiveSum(cubtmp.p, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
         ke();
-        unsigned total = 0;
+        kb("assign_chunks", double(ntiles + 1) * 16.0);
+        k_chunk_count<<<grid1(ntiles + 1, 256), 256, 0, st>>>(dp<unsigned>(cnt), ntiles, CHUNK, dp<unsigned>(nch));
+        ke();
+        kb("assign_scan", double(ntiles + 1) * 8.0);
+        HG_CK(cub::DeviceScan::ExclusiveSum(cubtmp.p, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
+        ke();
+        unsigned tot[2] = {0, 0};
         double hm[2];
-        HG_CK(cudaMemcpyAsync(&total, dp<unsigned>(off) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaMemcpyAsync(&tot[0], dp<unsigned>(off) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaMemcpyAsync(&tot[1], dp<unsigned>(choff) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaMemcpyAsync(hm, mass.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
+        const unsigned total = tot[0], nchunks = tot[1];
         HG_CK(rec.ensure(sizeof(PRec<T>) * std::max<size_t>(total, 1)));
+        HG_CK(chunks.ensure(sizeof(Chunk) * std::max<size_t>(nchunks, 1)));
+        kb("assign_chunks", double(ntiles) * 16.0);
+        k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
+                                                        dp<Chunk>(chunks));
+        ke();
         kb("assign_bin_scatter", double(src.n) * 24.0 + double(total) * sizeof(PRec<T>));
         k_bin_scatter<T><<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(off), dp<unsigned>(cursor),
                                                             dp<PRec<T>>(rec));
         ke();
-        size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2];
+        kb("assign_zero_split", 0.0);
+        k_zero_split_tiles<T, false><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), ag, out, nullptr);
+        ke();
+        size_t smem = sizeof(double) * ag.t[0] * ag.t[1] * ag.t[2];
         HG_CK(cudaFuncSetAttribute(k_tile_accum<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kb("assign_tile_accum", double(total) * sizeof(PRec<T>) + double(g.ntot) * sizeof(T));
-        k_tile_accum<T, false><<<ntiles, 256, smem, st>>>(dp<PRec<T>>(rec), dp<unsigned>(off), ag, out, nullptr);
+        k_tile_accum<T, false><<<nchunks, 256, smem, st>>>(dp<PRec<T>>(rec), dp<Chunk>(chunks), ag, out, nullptr);
         ke();
         return hm[0];
     }
@@ -464,17 +528,8 @@ struct Engine : public hg_ctx {
         if (bytes < 0) bytes = 2.0 * double(outer) * L * inner * sizeof(C);
         const C *twp = twiddles(L);
         kb(name, bytes);
-        HG_CK((launch_fft_pass<T, DIR>(L, ld, stt, pg, twp, st)));
+        HG_CK((launch_pass_any<T, DIR>(L, ld, stt, pg, twp, st)));
         ke();
-    }
-
-    // In-place 3-D c2c transform of a batch of nb arrays [nb][M0][M1][M2].
-    template <int DIR>
-    void fft3(C *p, long long nb, const int *M, const char *name) {
-        pass<DIR>(M[2], LdArr<T>{p, M[2], 1}, StArr<T>{p, M[2], 1}, nb * M[0] * M[1], 1, name);
-        pass<DIR>(M[1], LdArr<T>{p, M[1], M[2]}, StArr<T>{p, M[1], M[2]}, nb * M[0], M[2], name);
-        pass<DIR>(M[0], LdArr<T>{p, M[0], (long long)M[1] * M[2]}, StArr<T>{p, M[0], (long long)M[1] * M[2]}, nb,
-                  (long long)M[1] * M[2], name);
     }
 
     // Box density contrast, forward transformed: H = FFT[dV (rho - N/V)] (half spectrum).
@@ -534,24 +589,23 @@ struct Engine : public hg_ctx {
         rng(0, lo.x, cn.x);
         rng(1, lo.y, cn.y);
         rng(2, lo.z, cn.z);
-        DBuf acc, cnt_d;
-        HG_CK(acc.ensure(sizeof(double) * 2 * nbin * L.n));
-        HG_CK(cnt_d.ensure(sizeof(unsigned long long) * nbin));
-        HG_CK(cudaMemsetAsync(acc.p, 0, sizeof(double) * 2 * nbin * L.n, st));
-        HG_CK(cudaMemsetAsync(cnt_d.p, 0, sizeof(unsigned long long) * nbin, st));
+        HG_CK(bin_acc.ensure(sizeof(double) * 2 * nbin * L.n));
+        HG_CK(bin_cnt.ensure(sizeof(unsigned long long) * nbin));
+        HG_CK(cudaMemsetAsync(bin_acc.p, 0, sizeof(double) * 2 * nbin * L.n, st));
+        HG_CK(cudaMemsetAsync(bin_cnt.p, 0, sizeof(unsigned long long) * nbin, st));
         size_t smem = sizeof(double) * 2 * nbin * L.n + sizeof(unsigned long long) * nbin;
         HG_CK(cudaFuncSetAttribute(k_pk_bin<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         long long total = (long long)cn.x * cn.y * cn.z;
         unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 8);
         kb("pk_bin", double(total) * sizeof(C));
         k_pk_bin<T><<<blocks, 256, smem, st>>>(half_spec(), half_spec(), g, tabs, lo, cn, dp<int2>(lut), lutn, nbin, L,
-                                               S_re, S_im, cfg.assign, wpow, dp<double>(acc),
-                                               dp<unsigned long long>(cnt_d), 0, 0.0, 0.0);
+                                               S_re, S_im, cfg.assign, wpow, dp<double>(bin_acc),
+                                               dp<unsigned long long>(bin_cnt), 0, 0.0, 0.0);
         ke();
         std::vector<double> a(2 * nbin * L.n);
         nm.assign(nbin, 0);
-        HG_CK(cudaMemcpyAsync(a.data(), acc.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, st));
-        HG_CK(cudaMemcpyAsync(nm.data(), cnt_d.p, sizeof(unsigned long long) * nbin, cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaMemcpyAsync(a.data(), bin_acc.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaMemcpyAsync(nm.data(), bin_cnt.p, sizeof(unsigned long long) * nbin, cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
         avg.assign(2 * nbin * L.n, 0.0);
         for (int j = 0; j < nbin; j++)
@@ -561,20 +615,6 @@ struct Engine : public hg_ctx {
                     avg[2 * (j * L.n + q) + 1] = a[2 * (j * L.n + q) + 1] / double(nm[j]);
                 }
             }
-    }
-
-    void begin() {
-        launches = 0;
-        HG_CK(cudaEventRecord(ev0, st));
-    }
-    void end() {
-        prof_flush();
-        HG_CK(cudaEventRecord(ev1, st));
-        HG_CK(cudaEventSynchronize(ev1));
-        float ms = 0.f;
-        HG_CK(cudaEventElapsedTime(&ms, ev0, ev1));
-        last_ms = ms;
-        last_launches = launches;
     }
 
     // powerspec.hpp:273-332
@@ -601,13 +641,14 @@ struct Engine : public hg_ctx {
         S.ns = cfg.n_kbin;
         double dk_in = kbin[1] - kbin[0];  // bispec.hpp:1144
         double upper_max = kbin[S.ns - 1] + dk_in * 0.5;
-        for (int a = 0; a < 3; a++) S.s[a] = std::min((int)std::floor(upper_max / g.dk[a]) + 1, g.n[a] / 2);
+        int sx[3];
+        for (int a = 0; a < 3; a++) sx[a] = std::min((int)std::floor(upper_max / g.dk[a]) + 1, g.n[a] / 2);
         std::vector<std::vector<ShellEnt>> per(S.ns);
-        for (int nx = -S.s[0]; nx <= S.s[0]; nx++) {
+        for (int nx = -sx[0]; nx <= sx[0]; nx++) {
             if (nx >= g.n[0] / 2) continue;
-            for (int ny = -S.s[1]; ny <= S.s[1]; ny++) {
+            for (int ny = -sx[1]; ny <= sx[1]; ny++) {
                 if (ny >= g.n[1] / 2) continue;
-                for (int nz = -S.s[2]; nz <= S.s[2]; nz++) {
+                for (int nz = -sx[2]; nz <= sx[2]; nz++) {
                     if (nz >= g.n[2] / 2) continue;
                     double kmag = kmag_exact_host(kcomp(nx, g.dk[0]), kcomp(ny, g.dk[1]), kcomp(nz, g.dk[2]));
                     for (int i = 0; i < S.ns; i++) {
@@ -636,15 +677,17 @@ struct Engine : public hg_ctx {
         S.start[S.ns] = (int)S.ent.size();
         for (int a = 0; a < 3; a++) {
             S.s[a] = smax[a];
+            S.K[a] = 2 * smax[a] + 1;
             int need = 4 * smax[a] + 1;
             int m = std::max(8, next_pow2(need));
             if (m >= g.n[a]) {
                 S.M[a] = g.n[a];
-                S.gext[a] = -1;
+                S.gs[a] = g.n[a] / 2;  // whole axis
             } else {
                 S.M[a] = m;
-                S.gext[a] = 2 * smax[a];
+                S.gs[a] = 2 * smax[a];
             }
+            S.KG[a] = 2 * S.gs[a] + 1;
         }
         HG_CK(S.d_ent.ensure(sizeof(ShellEnt) * std::max<size_t>(S.ent.size(), 1)));
         if (!S.ent.empty())
@@ -659,124 +702,141 @@ struct Engine : public hg_ctx {
     }
 
     long long n_ent() const { return (long long)shells.ent.size(); }
+    long long cube_vol() const { return (long long)shells.K[0] * shells.K[1] * shells.K[2]; }
 
-    const double2 *family_A(const Fam &f) {
-        auto it = famA.find(f);
-        if (it != famA.end()) return dp<double2>(*it->second);
-        auto b = std::make_unique<DBuf>();
-        HG_CK(b->ensure(sizeof(double2) * std::max<long long>(n_ent(), 1)));
-        if (n_ent() > 0) {
-            kb("shell_family_A", double(n_ent()) * 48.0);
-            k_family_A<<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), g, f.l, f.m,
-                                                            dp<double2>(shD), dp<double>(shells.d_scale),
-                                                            dp<double2>(*b));
-            ke();
-        }
-        const double2 *p = dp<double2>(*b);
-        famA[f] = std::move(b);
-        return p;
+    DBuf &map_buf(std::map<Fam, std::unique_ptr<DBuf>> &m, const Fam &f) {
+        auto &p = m[f];
+        if (!p) p = std::make_unique<DBuf>();
+        return *p;
     }
 
+    const double2 *family_A(const Fam &f) {
+        DBuf &b = map_buf(famA, f);
+        if (famA_ok.count(f)) return dp<double2>(b);
+        HG_CK(b.ensure(sizeof(double2) * std::max<long long>(n_ent(), 1)));
+        kb("shell_family_A", double(n_ent()) * 48.0);
+        k_family_A<<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), g, f.l, f.m,
+                                                        dp<double2>(shD), dp<double>(shells.d_scale), dp<double2>(b));
+        ke();
+        famA_ok.insert(f);
+        return dp<double2>(b);
+    }
+
+    void ensure_chain_tmp(long long t1, long long t2) {
+        HG_CK(T1.ensure(sizeof(C) * std::max<long long>(t1, 1)));
+        HG_CK(T2.ensure(sizeof(C) * std::max<long long>(t2, 1)));
+    }
+
+    // G(x) = IFFT[delta/W]/V on the reduced grid, from the cube |n_a| <= gs_a (pruned passes)
     void ensure_G() {
         if (G_valid) return;
         const ShellSet &S = shells;
-        long long vol = (long long)S.M[0] * S.M[1] * S.M[2];
+        const long long vol = (long long)S.M[0] * S.M[1] * S.M[2];
+        const long long kg = (long long)S.KG[0] * S.KG[1] * S.KG[2];
+        HG_CK(Gc.ensure(sizeof(C) * kg));
         HG_CK(Gbuf.ensure(sizeof(C) * vol));
-        HG_CK(cudaMemsetAsync(Gbuf.p, 0, sizeof(C) * vol, st));
-        int3 lo, cn;
-        int *lop[3] = {&lo.x, &lo.y, &lo.z};
-        int *cnp[3] = {&cn.x, &cn.y, &cn.z};
-        for (int a = 0; a < 3; a++) {
-            if (S.gext[a] < 0) {
-                *lop[a] = -g.n[a] / 2;
-                *cnp[a] = g.n[a];
-            } else {
-                *lop[a] = -S.gext[a];
-                *cnp[a] = 2 * S.gext[a] + 1;
-            }
-        }
-        long long total = (long long)cn.x * cn.y * cn.z;
-        unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 16);
-        kb("scatter_G", double(total) * (sizeof(C) * 2));
-        k_scatter_G<T><<<blocks, 256, 0, st>>>(half_spec(), g, tabs, wpow, lo, cn,
-                                               make_int3(S.M[0], S.M[1], S.M[2]), delta0, 0.0, dp<C>(Gbuf));
+        ensure_chain_tmp((long long)S.KG[0] * S.KG[1] * S.M[2], (long long)S.KG[0] * S.M[1] * S.M[2]);
+        int3 lo = make_int3(-S.gs[0], -S.gs[1], -S.gs[2]);
+        int3 cn = make_int3(S.KG[0], S.KG[1], S.KG[2]);
+        unsigned blocks = (unsigned)std::min<long long>(grid1(kg, 256), 148 * 16);
+        kb("scatter_G", double(kg) * (sizeof(C) * 2));
+        k_scatter_G<T><<<blocks, 256, 0, st>>>(half_spec(), g, tabs, wpow, lo, cn, delta0, 0.0, dp<C>(Gc));
         ke();
-        fft3<+1>(dp<C>(Gbuf), 1, S.M, "fft_G_inv");
+        const int M0 = S.M[0], M1 = S.M[1], M2 = S.M[2];
+        pass<+1>(M2, LdCube<T>{dp<C>(Gc), S.KG[2], M2, S.gs[2]}, StArr<T>{dp<C>(T1), M2, 1},
+                 (long long)S.KG[0] * S.KG[1], 1, "fft_G_inv",
+                 double(kg + (long long)S.KG[0] * S.KG[1] * M2) * sizeof(C));
+        pass<+1>(M1, LdRowsCompact<T>{dp<C>(T1), S.KG[1], M1, S.gs[1], M2}, StArr<T>{dp<C>(T2), M1, M2}, S.KG[0], M2,
+                 "fft_G_inv", double((long long)S.KG[0] * S.KG[1] * M2 + (long long)S.KG[0] * M1 * M2) * sizeof(C));
+        pass<+1>(M0, LdRowsCompact<T>{dp<C>(T2), S.KG[0], M0, S.gs[0], (long long)M1 * M2},
+                 StArr<T>{dp<C>(Gbuf), M0, (long long)M1 * M2}, 1, (long long)M1 * M2, "fft_G_inv",
+                 double((long long)S.KG[0] * M1 * M2 + vol) * sizeof(C));
         G_valid = true;
     }
 
-    // QE_b[j][e] = Qhat_b,j(-n_e),  Qhat_b,j = FFT[IFFT[A_b,j] * G] on the reduced grid.
-    const double2 *family_Q(const Fam &b) {
-        auto it = famQ.find(b);
-        if (it != famQ.end()) return dp<double2>(*it->second);
+    // Q_b[j] = FFT[IFFT[A_b,j] * G] on the shell cube (hg_chain.cuh)
+    const C *family_Q(const Fam &b) {
+        DBuf &Q = map_buf(famQ, b);
+        if (famQ_ok.count(b)) return dp<C>(Q);
         const ShellSet &S = shells;
         ensure_G();
         const double2 *A = family_A(b);
-        long long vol = (long long)S.M[0] * S.M[1] * S.M[2];
-        HG_CK(chain.ensure(sizeof(C) * vol * S.ns));
-        HG_CK(cudaMemsetAsync(chain.p, 0, sizeof(C) * vol * S.ns, st));
-        int3 M3 = make_int3(S.M[0], S.M[1], S.M[2]);
+        const int ns = S.ns;
+        const int Kx = S.K[0], Ky = S.K[1], Kz = S.K[2];
+        const int Mx = S.M[0], My = S.M[1], Mz = S.M[2];
+        const long long cv = cube_vol();
+        HG_CK(Ac.ensure(sizeof(C) * cv * ns));
+        HG_CK(Q.ensure(sizeof(C) * cv * ns));
+        ensure_chain_tmp((long long)ns * Kx * Ky * Mz, (long long)ns * Kx * My * Mz);
+        HG_CK(cudaMemsetAsync(Ac.p, 0, sizeof(C) * cv * ns, st));
         kb("scatter_entries", double(n_ent()) * (16.0 + sizeof(C)));
-        k_scatter_entries<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), A, M3,
-                                                                  dp<C>(chain));
+        k_scatter_cube<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), A,
+                                                               make_int3(Kx, Ky, Kz), make_int3(S.s[0], S.s[1], S.s[2]),
+                                                               dp<C>(Ac));
         ke();
-        fft3<+1>(dp<C>(chain), S.ns, S.M, "fft_chain_inv");
-        // forward: first pass multiplies by G
-        C *p = dp<C>(chain);
-        pass<-1>(S.M[2], LdMulG<T>{p, dp<C>(Gbuf), S.M[2], (long long)S.M[0] * S.M[1]}, StArr<T>{p, S.M[2], 1},
-                 (long long)S.ns * S.M[0] * S.M[1], 1, "fft_chain_fwd_mulG");
-        pass<-1>(S.M[1], LdArr<T>{p, S.M[1], S.M[2]}, StArr<T>{p, S.M[1], S.M[2]}, (long long)S.ns * S.M[0], S.M[2],
-                 "fft_chain_fwd");
-        pass<-1>(S.M[0], LdArr<T>{p, S.M[0], (long long)S.M[1] * S.M[2]},
-                 StArr<T>{p, S.M[0], (long long)S.M[1] * S.M[2]}, S.ns, (long long)S.M[1] * S.M[2], "fft_chain_fwd");
-        auto q = std::make_unique<DBuf>();
-        HG_CK(q->ensure(sizeof(double2) * std::max<long long>(n_ent(), 1) * S.ns));
-        dim3 gr(grid1(n_ent(), 256), S.ns);
-        kb("extract_neg", double(n_ent()) * S.ns * (16.0 + sizeof(C)));
-        k_extract_neg<T><<<gr, 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), S.ns, M3, p, dp<double2>(*q));
+        const long long o1 = (long long)ns * Kx * Ky;
+        const long long o2 = (long long)ns * Kx;
+        pass<+1>(Mz, LdCube<T>{dp<C>(Ac), Kz, Mz, S.s[2]}, StArr<T>{dp<C>(T1), Mz, 1}, o1, 1, "chain_z",
+                 double(o1) * (Kz + Mz) * sizeof(C));
+        pass<+1>(My, LdRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, StArr<T>{dp<C>(T2), My, Mz}, o2, Mz, "chain_y",
+                 double(o2) * (Ky + My) * Mz * sizeof(C));
+        kb("chain_x_fused", double(ns) * 2.0 * Kx * My * Mz * sizeof(C) + double(Mx) * My * Mz * sizeof(C));
+        if (Mx == 256)
+            HG_CK((launch_chain_x_reg_L<T, 256>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
+                                                st)));
+        else if (Mx == 128)
+            HG_CK((launch_chain_x_reg_L<T, 128>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
+                                                st)));
+        else if (Mx == 64)
+            HG_CK((launch_chain_x_reg_L<T, 64>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
+                                               st)));
+        else if (Mx == 32)
+            HG_CK((launch_chain_x_reg_L<T, 32>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
+                                               st)));
+        else
+            HG_CK(launch_chain_x<T>(Mx, dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st));
         ke();
-        const double2 *r = dp<double2>(*q);
-        famQ[b] = std::move(q);
-        return r;
+        pass<-1>(My, LdArr<T>{dp<C>(T2), My, Mz}, StRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, o2, Mz, "chain_y",
+                 double(o2) * (Ky + My) * Mz * sizeof(C));
+        pass<-1>(Mz, LdArr<T>{dp<C>(T1), Mz, 1}, StCube<T>{dp<C>(Q), Kz, Mz, S.s[2]}, o1, 1, "chain_z",
+                 double(o1) * (Kz + Mz) * sizeof(C));
+        famQ_ok.insert(b);
+        return dp<C>(Q);
     }
 
-    // pair matrix P[i][j] = sum_{e in shell i} A_a[e] QE_b[j][e]  (complex, [ns][ns])
+    // pair matrix P[i][j] = sum_{e in shell i} A_a[e] Q_b,j(-n_e)  (complex, [ns][ns])
     const std::vector<double> &pair_matrix(const Fam &a, const Fam &b) {
         auto key = std::make_pair(a, b);
         auto it = pairs.find(key);
         if (it != pairs.end()) return it->second;
         const ShellSet &S = shells;
         const double2 *A = family_A(a);
-        const double2 *Q = family_Q(b);
-        DBuf out;
-        HG_CK(out.ensure(sizeof(double2) * S.ns * S.ns));
+        const C *Q = family_Q(b);
+        HG_CK(pair_out.ensure(sizeof(double2) * S.ns * S.ns));
         dim3 gr(S.ns, S.ns);
         kb("pair_dot", double(n_ent()) * (S.ns + 1) * 16.0);
-        k_pair_dot<<<gr, 256, 0, st>>>(dp<int>(shells.d_start), S.ns, A, Q, n_ent(), S.ns, dp<double2>(out));
+        k_pair_dot_cube<T><<<gr, 256, 0, st>>>(dp<int>(shells.d_start), dp<ShellEnt>(shells.d_ent), A, Q,
+                                               make_int3(S.K[0], S.K[1], S.K[2]), make_int3(S.M[0], S.M[1], S.M[2]),
+                                               make_int3(S.s[0], S.s[1], S.s[2]), S.ns, dp<double2>(pair_out));
         ke();
         std::vector<double> h(2 * S.ns * S.ns);
-        HG_CK(cudaMemcpyAsync(h.data(), out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaMemcpyAsync(h.data(), pair_out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
         pairs[key] = h;
         return pairs[key];
     }
 
-    // sum_x F_a,i F_b,j G  (without dV) for all (i, j): uses a chain on b, or on a transposed.
-    std::vector<double> triple_sum(const Fam &a, const Fam &b) {
+    // sum_x F_a,i F_b,j G (without dV) for all (i, j): chain on b, or on a transposed.
+    std::vector<double> triple_sum(const Fam &a, const Fam &b, const std::set<Fam> &chains) {
         const int ns = shells.ns;
+        if (chains.count(b)) return pair_matrix(a, b);
+        const auto &P = pair_matrix(b, a);
         std::vector<double> r(2 * ns * ns);
-        bool use_b = famQ.count(b) || !famQ.count(a);
-        if (use_b) {
-            const auto &P = pair_matrix(a, b);
-            r = P;
-        } else {
-            const auto &P = pair_matrix(b, a);
-            for (int i = 0; i < ns; i++)
-                for (int j = 0; j < ns; j++) {
-                    r[2 * (i * ns + j)] = P[2 * (j * ns + i)];
-                    r[2 * (i * ns + j) + 1] = P[2 * (j * ns + i) + 1];
-                }
-        }
+        for (int i = 0; i < ns; i++)
+            for (int j = 0; j < ns; j++) {
+                r[2 * (i * ns + j)] = P[2 * (j * ns + i)];
+                r[2 * (i * ns + j) + 1] = P[2 * (j * ns + i) + 1];
+            }
         return r;
     }
 
@@ -784,12 +844,13 @@ struct Engine : public hg_ctx {
         box_density();
         build_shells();
         HG_REQUIRE(n_ent() > 0, "no Fourier modes fall inside the k shells");
-        if (!shD.p || shD.n < sizeof(double2) * n_ent() || famA.empty()) {
+        if (!shD_valid) {
             HG_CK(shD.ensure(sizeof(double2) * n_ent()));
             kb("shell_D", double(n_ent()) * (16.0 + sizeof(C)));
-            k_shell_D<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), half_spec(), g,
-                                                              tabs, wpow, dp<double2>(shD));
+            k_shell_D<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), half_spec(), g, tabs,
+                                                              wpow, dp<double2>(shD));
             ke();
+            shD_valid = true;
         }
     }
 
@@ -825,45 +886,99 @@ struct Engine : public hg_ctx {
         n2dim += 1;
     }
 
-    // hist[h][n2] = sum over cells with |x/dr|^2 = n2 of xi(x) f_h(x_hat)
-    void xi_histograms(const HistSpec &hs, double S) {
+    // xi after its x and y inverse passes (cached per catalogue)
+    void ensure_xi() {
         HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
                    "bispectrum / 3PCF shot noise needs equal cell sizes on all axes");
         build_orbits();
+        if (xi_valid) return;
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
+        const double S = double(slot[0].n);
         LdXiHat<T> ld{half_spec(), g, tabs, cfg.assign, wpow, S, 0.0, delta0 * N0, 0.0, invV};
         long long yz = (long long)g.n[1] * g.n[2];
         pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
                  double(g.ntot) * sizeof(C) * 1.5);
         pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
                  "fft_xi_y");
-        HG_CK(hist.ensure(sizeof(double) * 2 * n2dim * hs.nh));
-        HG_CK(cudaMemsetAsync(hist.p, 0, sizeof(double) * 2 * n2dim * hs.nh, st));
-        int n_orb = (int)orbit_n2xy.size();
-        launch_orbit(g.n[2], hs, n_orb);
+        xi_valid = true;
     }
 
     template <int L>
-    void launch_orbit_L(const HistSpec &hs, int n_orb) {
+    void launch_orbit_L(const HistSpec &hs, int n_orb, double *hist) {
         size_t smem = sizeof(C) * 8 * (L + 1);
         HG_CK(cudaFuncSetAttribute(k_xi_orbit_hist<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kb("xi_orbit_hist", double(g.ntot) * sizeof(C));
-        k_xi_orbit_hist<T, L><<<n_orb, L, smem, st>>>(dp<C>(xi), dp<int>(d_orbit_lines), dp<int>(d_orbit_n2xy),
-                                                     n_orb, twiddles(L), hs, n2dim, dp<double>(hist));
+        k_xi_orbit_hist<T, L><<<n_orb, L, smem, st>>>(dp<C>(xi), dp<int>(d_orbit_lines), dp<int>(d_orbit_n2xy), n_orb,
+                                                     twiddles(L), hs, n2dim, hist);
         ke();
     }
-    void launch_orbit(int L, const HistSpec &hs, int n_orb) {
+    void launch_orbit(int L, const HistSpec &hs, int n_orb, double *hist) {
         switch (L) {
-            case 8: launch_orbit_L<8>(hs, n_orb); break;
-            case 16: launch_orbit_L<16>(hs, n_orb); break;
-            case 32: launch_orbit_L<32>(hs, n_orb); break;
-            case 64: launch_orbit_L<64>(hs, n_orb); break;
-            case 128: launch_orbit_L<128>(hs, n_orb); break;
-            case 256: launch_orbit_L<256>(hs, n_orb); break;
-            case 512: launch_orbit_L<512>(hs, n_orb); break;
-            case 1024: launch_orbit_L<1024>(hs, n_orb); break;
+            case 8: launch_orbit_L<8>(hs, n_orb, hist); break;
+            case 16: launch_orbit_L<16>(hs, n_orb, hist); break;
+            case 32: launch_orbit_L<32>(hs, n_orb, hist); break;
+            case 64: launch_orbit_L<64>(hs, n_orb, hist); break;
+            case 128: launch_orbit_L<128>(hs, n_orb, hist); break;
+            case 256: launch_orbit_L<256>(hs, n_orb, hist); break;
+            case 512: launch_orbit_L<512>(hs, n_orb, hist); break;
+            case 1024: launch_orbit_L<1024>(hs, n_orb, hist); break;
             default: throw HgError{"unsupported n_mesh_z"};
+        }
+    }
+
+    // (m1, m2) combinations with M = 0 and |w| >= 1e-10 (bispec.hpp:923-931)
+    struct Combo {
+        int m1, m2;
+        double w;
+    };
+    static std::vector<Combo> combos_of(const MP &mp) {
+        std::vector<Combo> out;
+        double w000 = wigner3j(mp.l1, mp.l2, mp.L, 0, 0, 0);
+        for (int m1 = -mp.l1; m1 <= mp.l1; m1++)
+            for (int m2 = -mp.l2; m2 <= mp.l2; m2++) {
+                double w = w000 * wigner3j(mp.l1, mp.l2, mp.L, m1, m2, 0);
+                w *= double(2 * mp.L + 1) * double(2 * mp.l1 + 1) * double(2 * mp.l2 + 1);
+                if (std::fabs(w) < 1.0e-10) continue;
+                out.push_back({m1, m2, w});
+            }
+        return out;
+    }
+
+    // hist_mp[mp][n2] = sum over cells with |x/dr|^2 = n2 of xi(x) sum_combos w Yhat1 Yhat2
+    void ensure_histograms(const std::vector<MP> &mps) {
+        ensure_xi();
+        std::vector<MP> todo;
+        for (const auto &mp : mps) {
+            std::array<int, 3> key{mp.l1, mp.l2, mp.L};
+            bool queued = false;
+            for (const auto &q : todo) queued |= (q.l1 == mp.l1 && q.l2 == mp.l2 && q.L == mp.L);
+            if (!hist_ok.count(key) && !queued) todo.push_back(mp);
+        }
+        for (size_t t0 = 0; t0 < todo.size(); t0 += HG_MAX_HIST) {
+            HistSpec hs;
+            memset(&hs, 0, sizeof(hs));
+            hs.nh = (int)std::min<size_t>(HG_MAX_HIST, todo.size() - t0);
+            for (int h = 0; h < hs.nh; h++) {
+                const MP &mp = todo[t0 + h];
+                hs.parity[h] = ((mp.l1 + mp.l2) % 2 == 0) ? 1 : -1;
+                auto cs = combos_of(mp);
+                HG_REQUIRE(cs.size() <= 12, "too many (m1, m2) terms in one multipole");
+                for (const auto &c : cs) hs.term[h][hs.nterm[h]++] = YTerm{mp.l1, c.m1, mp.l2, c.m2, c.w};
+            }
+            HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim * hs.nh));
+            HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim * hs.nh, st));
+            launch_orbit(g.n[2], hs, (int)orbit_n2xy.size(), dp<double>(hist_tmp));
+            for (int h = 0; h < hs.nh; h++) {
+                const MP &mp = todo[t0 + h];
+                std::array<int, 3> key{mp.l1, mp.l2, mp.L};
+                auto &p = hist_mp[key];
+                if (!p) p = std::make_unique<DBuf>();
+                HG_CK(p->ensure(sizeof(double) * 2 * n2dim));
+                HG_CK(cudaMemcpyAsync(p->p, dp<double>(hist_tmp) + 2 * n2dim * h, sizeof(double) * 2 * n2dim,
+                                      cudaMemcpyDeviceToDevice, st));
+                hist_ok.insert(key);
+            }
         }
     }
 
@@ -883,28 +998,37 @@ struct Engine : public hg_ctx {
         return r;
     }
 
-    // J[i][n2] = j_l(kv[i] * dr sqrt(n2))
-    void bessel_table(int l, const std::vector<double> &kv, DBuf &J) {
+    // J_l[i][n2] = j_l(kbin[i] * dr sqrt(n2)) (geometry only: cached for the context)
+    const double *jtab(int l) {
+        auto it = jtab_k.find(l);
+        if (it != jtab_k.end()) return dp<double>(*it->second);
         const BesselSpline &s = spline(l);
         auto &sp = d_splines[l];
-        HG_CK(d_kv.ensure(sizeof(double) * kv.size()));
-        HG_CK(cudaMemcpyAsync(d_kv.p, kv.data(), sizeof(double) * kv.size(), cudaMemcpyHostToDevice, st));
-        HG_CK(J.ensure(sizeof(double) * kv.size() * n2dim));
-        long long tot = (long long)kv.size() * n2dim;
+        HG_CK(d_kv.ensure(sizeof(double) * kbin.size()));
+        HG_CK(cudaMemcpyAsync(d_kv.p, kbin.data(), sizeof(double) * kbin.size(), cudaMemcpyHostToDevice, st));
+        auto J = std::make_unique<DBuf>();
+        HG_CK(J->ensure(sizeof(double) * kbin.size() * n2dim));
+        long long tot = (long long)kbin.size() * n2dim;
         kb("bessel_table", double(tot) * 8.0);
-        k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second),
-                                                        s.n, s.xmin, s.dx, dp<double>(d_kv), (int)kv.size(), g.dr[0],
-                                                        n2dim, dp<double>(J));
+        k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n, s.xmin,
+                                                        s.dx, dp<double>(d_kv), (int)kbin.size(), g.dr[0], n2dim,
+                                                        dp<double>(*J));
         ke();
         HG_CK(cudaStreamSynchronize(st));
+        const double *p = dp<double>(*J);
+        jtab_k[l] = std::move(J);
+        return p;
     }
 
     // ------------------------------------------------------------------ bispectrum (box)
-    // bispec.hpp:877-1203 for all k1 rows at once.
-    void bk_box(int l1, int l2, int L, int ith, double *bk_save, double *sn_save, double *norm) override {
-        HG_REQUIRE(l1 >= 0 && l2 >= 0 && L >= 0, "ell1, ell2, ELL must be >= 0");
-        double w000 = wigner3j(l1, l2, L, 0, 0, 0);
-        HG_REQUIRE(std::fabs(w000) >= 1.0e-10, "This multipole combination is not allowed: wigner_3j(ell1, ell2, ELL, 0,0,0) == 0");
+    // bispec.hpp:877-1203 for all k1 rows of several multipoles at once.
+    void bk_box_multi(const std::vector<MP> &mps, int ith, double *bk_save, double *sn_save, double *norm) override {
+        HG_REQUIRE(!mps.empty(), "no multipoles requested");
+        for (const auto &mp : mps) {
+            HG_REQUIRE(mp.l1 >= 0 && mp.l2 >= 0 && mp.L >= 0, "ell1, ell2, ELL must be >= 0");
+            HG_REQUIRE(std::fabs(wigner3j(mp.l1, mp.l2, mp.L, 0, 0, 0)) >= 1.0e-10,
+                       "This multipole combination is not allowed: wigner_3j(ell1, ell2, ELL, 0,0,0) == 0");
+        }
         HG_REQUIRE(ith >= -1 && ith < cfg.n_kbin, "ith_kbin out of range");
         begin();
         prepare_shells();
@@ -912,93 +1036,142 @@ struct Engine : public hg_ctx {
         const double Np = double(slot[0].n);
         const double dV = g.volume / double(g.ntot);
         const double red = double(g.ntot) / (double(shells.M[0]) * shells.M[1] * shells.M[2]);
-        // (m1, m2) combinations with M = 0 (bispec.hpp:1123-1133)
-        struct Combo {
-            int m1, m2;
-            double w;
-        };
-        std::vector<Combo> combos;
-        for (int m1 = -l1; m1 <= l1; m1++)
-            for (int m2 = -l2; m2 <= l2; m2++) {
-                double w = w000 * wigner3j(l1, l2, L, m1, m2, 0);
-                w *= double(2 * L + 1) * double(2 * l1 + 1) * double(2 * l2 + 1);
-                if (std::fabs(w) < 1.0e-10) continue;
-                combos.push_back({m1, m2, w});
+        // chain families: every self-paired family, then a greedy cover of the remaining pairs
+        std::vector<std::vector<Combo>> cmb;
+        std::set<std::pair<Fam, Fam>> upairs;
+        for (const auto &mp : mps) {
+            cmb.push_back(combos_of(mp));
+            for (const auto &c : cmb.back()) {
+                Fam a{mp.l1, c.m1}, b{mp.l2, c.m2};
+                upairs.insert(b < a ? std::make_pair(b, a) : std::make_pair(a, b));
             }
-        std::vector<double> B(2 * ns * ns, 0.0), SN(2 * ns * ns, 0.0);
-        for (const auto &c : combos) {
-            std::vector<double> t = triple_sum(Fam{l1, c.m1}, Fam{l2, c.m2});
-            for (int q = 0; q < 2 * ns * ns; q++) B[q] += c.w * (dV * red * t[q]);
         }
-        // shot noise, bispec.hpp:909-1078
-        std::vector<LM> lms;
-        for (const auto &c : combos) {
-            if (l2 == 0) lms.push_back(LM{l1, c.m1});
-            if (l1 == 0) lms.push_back(LM{l2, c.m2});
-        }
-        std::vector<double> avg;
-        std::vector<unsigned long long> nm;
-        if (!lms.empty()) pk_bin(lms, Np, 0.0, avg, nm);
-        int q = 0;
-        for (const auto &c : combos) {
-            for (int i1 = 0; i1 < ns; i1++)
-                for (int i2 = 0; i2 < ns; i2++) {
-                    double sr = 0.0, si = 0.0;
-                    if (l1 == 0 && l2 == 0) sr += c.w * Np;
-                    int qq = q;
-                    if (l2 == 0) {
-                        sr += c.w * avg[2 * (i1 * (int)lms.size() + qq)];
-                        si += c.w * avg[2 * (i1 * (int)lms.size() + qq) + 1];
-                        qq++;
-                    }
-                    if (l1 == 0) {
-                        sr += c.w * avg[2 * (i2 * (int)lms.size() + qq)];
-                        si += c.w * avg[2 * (i2 * (int)lms.size() + qq) + 1];
-                    }
-                    SN[2 * (i1 * ns + i2)] += sr;
-                    SN[2 * (i1 * ns + i2) + 1] += si;
+        std::set<Fam> chains(famQ_ok.begin(), famQ_ok.end());
+        for (const auto &p : upairs)
+            if (!(p.first < p.second) && !(p.second < p.first)) chains.insert(p.first);
+        while (true) {
+            std::map<Fam, int> score;
+            for (const auto &p : upairs) {
+                if (chains.count(p.first) || chains.count(p.second)) continue;
+                score[p.first]++;
+                score[p.second]++;
+            }
+            if (score.empty()) break;
+            Fam best = score.begin()->first;
+            int bs = -1;
+            for (const auto &kv : score)
+                if (kv.second > bs) {
+                    bs = kv.second;
+                    best = kv.first;
                 }
-            q += (l2 == 0) + (l1 == 0);
+            chains.insert(best);
         }
-        // xi term: hist of xi * sum_combos w Yhat_l1m1 Yhat_l2m2, then j_l1 j_l2 sums
-        HistSpec hs;
-        memset(&hs, 0, sizeof(hs));
-        hs.nh = 1;
-        hs.parity[0] = ((l1 + l2) % 2 == 0) ? 1 : -1;
-        HG_REQUIRE(combos.size() <= 12, "too many (m1, m2) terms");
-        for (const auto &c : combos) hs.term[0][hs.nterm[0]++] = YTerm{l1, c.m1, l2, c.m2, c.w};
-        xi_histograms(hs, Np);
-        bessel_table(l1, kbin, Jtab1);
-        bessel_table(l2, kbin, Jtab2);
-        HG_CK(snmat.ensure(sizeof(double2) * ns * ns));
-        kb("sn_matrix", double(ns) * ns * n2dim * 24.0);
-        k_sn_matrix<<<dim3(ns, ns), 256, 0, st>>>(dp<double>(Jtab1), dp<double>(Jtab2), dp<double>(hist), n2dim, ns,
-                                                 dp<double2>(snmat));
-        ke();
-        std::vector<double> sd(2 * ns * ns);
-        HG_CK(cudaMemcpyAsync(sd.data(), snmat.p, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, st));
-        HG_CK(cudaStreamSynchronize(st));
-        // * i^(l1+l2) * dV   (bispec.hpp:1053-1055)
-        int p4 = (l1 + l2) % 4;
-        for (int e = 0; e < ns * ns; e++) {
-            double re = sd[2 * e] * dV, im = sd[2 * e + 1] * dV;
-            double rr, ii;
-            if (p4 == 0) { rr = re; ii = im; }
-            else if (p4 == 1) { rr = -im; ii = re; }
-            else if (p4 == 2) { rr = -re; ii = -im; }
-            else { rr = im; ii = -re; }
-            SN[2 * e] += rr;
-            SN[2 * e + 1] += ii;
-        }
-        int r0 = (ith < 0) ? 0 : ith, r1 = (ith < 0) ? ns : ith + 1;
-        for (int i1 = r0; i1 < r1; i1++)
-            for (int i2 = 0; i2 < ns; i2++) {
-                int o = (i1 - r0) * ns + i2;
-                bk_save[2 * o] = B[2 * (i1 * ns + i2)];
-                bk_save[2 * o + 1] = B[2 * (i1 * ns + i2) + 1];
-                sn_save[2 * o] = SN[2 * (i1 * ns + i2)];
-                sn_save[2 * o + 1] = SN[2 * (i1 * ns + i2) + 1];
+        std::vector<std::vector<double>> B(mps.size(), std::vector<double>(2 * ns * ns, 0.0));
+        for (size_t q = 0; q < mps.size(); q++)
+            for (const auto &c : cmb[q]) {
+                std::vector<double> t = triple_sum(Fam{mps[q].l1, c.m1}, Fam{mps[q].l2, c.m2}, chains);
+                for (int e = 0; e < 2 * ns * ns; e++) B[q][e] += c.w * (dV * red * t[e]);
             }
+        // shot noise (bispec.hpp:909-1078): P terms, constant term, xi term
+        std::vector<LM> lms;
+        std::vector<std::vector<int>> lm_idx(mps.size());
+        for (size_t q = 0; q < mps.size(); q++)
+            for (const auto &c : cmb[q]) {
+                if (mps[q].l2 == 0) {
+                    lm_idx[q].push_back((int)lms.size());
+                    lms.push_back(LM{mps[q].l1, c.m1});
+                }
+                if (mps[q].l1 == 0) {
+                    lm_idx[q].push_back((int)lms.size());
+                    lms.push_back(LM{mps[q].l2, c.m2});
+                }
+            }
+        const int nl = (int)lms.size();
+        std::vector<double> avg(2 * ns * std::max(nl, 1), 0.0);
+        std::vector<unsigned long long> nm;
+        for (int b0 = 0; b0 < nl; b0 += HG_MAX_LM) {
+            int b1 = std::min(nl, b0 + HG_MAX_LM);
+            std::vector<LM> part(lms.begin() + b0, lms.begin() + b1);
+            std::vector<double> a;
+            pk_bin(part, Np, 0.0, a, nm);
+            const int np_ = b1 - b0;
+            for (int j = 0; j < ns; j++)
+                for (int u = 0; u < np_; u++) {
+                    avg[2 * (j * nl + b0 + u)] = a[2 * (j * np_ + u)];
+                    avg[2 * (j * nl + b0 + u) + 1] = a[2 * (j * np_ + u) + 1];
+                }
+        }
+        std::vector<std::vector<double>> SN(mps.size(), std::vector<double>(2 * ns * ns, 0.0));
+        for (size_t q = 0; q < mps.size(); q++) {
+            const MP &mp = mps[q];
+            int u = 0;
+            for (const auto &c : cmb[q]) {
+                int iu1 = -1, iu2 = -1;
+                if (mp.l2 == 0) iu1 = lm_idx[q][u++];
+                if (mp.l1 == 0) iu2 = lm_idx[q][u++];
+                for (int i1 = 0; i1 < ns; i1++)
+                    for (int i2 = 0; i2 < ns; i2++) {
+                        double sr = 0.0, si = 0.0;
+                        if (mp.l1 == 0 && mp.l2 == 0) sr += c.w * Np;
+                        if (iu1 >= 0) {
+                            sr += c.w * avg[2 * (i1 * nl + iu1)];
+                            si += c.w * avg[2 * (i1 * nl + iu1) + 1];
+                        }
+                        if (iu2 >= 0) {
+                            sr += c.w * avg[2 * (i2 * nl + iu2)];
+                            si += c.w * avg[2 * (i2 * nl + iu2) + 1];
+                        }
+                        SN[q][2 * (i1 * ns + i2)] += sr;
+                        SN[q][2 * (i1 * ns + i2) + 1] += si;
+                    }
+            }
+        }
+        ensure_histograms(mps);
+        HG_CK(snmat.ensure(sizeof(double2) * ns * ns));
+        for (size_t q = 0; q < mps.size(); q++) {
+            const MP &mp = mps[q];
+            const double *J1 = jtab(mp.l1);
+            const double *J2 = jtab(mp.l2);
+            const double *hq = dp<double>(*hist_mp[{mp.l1, mp.l2, mp.L}]);
+            kb("sn_matrix", double(ns) * ns * n2dim * 24.0);
+            k_sn_matrix<<<dim3(ns, ns), 256, 0, st>>>(J1, J2, hq, n2dim, ns, dp<double2>(snmat));
+            ke();
+            std::vector<double> sd(2 * ns * ns);
+            HG_CK(cudaMemcpyAsync(sd.data(), snmat.p, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, st));
+            HG_CK(cudaStreamSynchronize(st));
+            // * i^(l1+l2) * dV   (bispec.hpp:1053-1055)
+            int p4 = (mp.l1 + mp.l2) % 4;
+            for (int e = 0; e < ns * ns; e++) {
+                double re = sd[2 * e] * dV, im = sd[2 * e + 1] * dV;
+                double rr, ii;
+                if (p4 == 0) {
+                    rr = re;
+                    ii = im;
+                } else if (p4 == 1) {
+                    rr = -im;
+                    ii = re;
+                } else if (p4 == 2) {
+                    rr = -re;
+                    ii = -im;
+                } else {
+                    rr = im;
+                    ii = -re;
+                }
+                SN[q][2 * e] += rr;
+                SN[q][2 * e + 1] += ii;
+            }
+        }
+        const int r0 = (ith < 0) ? 0 : ith, r1 = (ith < 0) ? ns : ith + 1;
+        const int rows = r1 - r0;
+        for (size_t q = 0; q < mps.size(); q++)
+            for (int i1 = r0; i1 < r1; i1++)
+                for (int i2 = 0; i2 < ns; i2++) {
+                    long long o = ((long long)q * rows + (i1 - r0)) * ns + i2;
+                    bk_save[2 * o] = B[q][2 * (i1 * ns + i2)];
+                    bk_save[2 * o + 1] = B[q][2 * (i1 * ns + i2) + 1];
+                    sn_save[2 * o] = SN[q][2 * (i1 * ns + i2)];
+                    sn_save[2 * o + 1] = SN[q][2 * (i1 * ns + i2) + 1];
+                }
         if (norm) {
             double nv = g.volume / Np / Np;
             nv *= (g.volume / Np);
@@ -1052,20 +1225,20 @@ const char *hg_last_error(const hg_ctx *ctx) {
     return ctx->err.c_str();
 }
 
-#define HG_GUARD(ctx, body)                  \
-    do {                                     \
-        if (!(ctx)) return -1;               \
-        try {                                \
-            body;                            \
-            (ctx)->err.clear();              \
-            return 0;                        \
-        } catch (const HgError &e) {         \
-            (ctx)->err = e.msg;              \
-            return -1;                       \
-        } catch (const std::exception &e) {  \
-            (ctx)->err = e.what();           \
-            return -1;                       \
-        }                                    \
+#define HG_GUARD(ctx, body)                 \
+    do {                                    \
+        if (!(ctx)) return -1;              \
+        try {                               \
+            body;                           \
+            (ctx)->err.clear();             \
+            return 0;                       \
+        } catch (const HgError &e) {        \
+            (ctx)->err = e.msg;             \
+            return -1;                      \
+        } catch (const std::exception &e) { \
+            (ctx)->err = e.what();          \
+            return -1;                      \
+        }                                   \
     } while (0)
 
 int hg_set_particles(hg_ctx *ctx, int slot, const double *base, long long n, long long stride_bytes, int pos_off,
@@ -1102,7 +1275,15 @@ int hg_pk_box(hg_ctx *ctx, int ell, double *pk_save, int *n_mode, double *norm) 
 
 int hg_bk_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_kbin, double *bk_save, double *sn_save, double *norm) {
     if (!bk_save || !sn_save) return -1;
-    HG_GUARD(ctx, ctx->bk_box(ell1, ell2, ELL, ith_kbin, bk_save, sn_save, norm));
+    HG_GUARD(ctx, ctx->bk_box_multi({MP{ell1, ell2, ELL}}, ith_kbin, bk_save, sn_save, norm));
+}
+
+int hg_bk_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double *bk_save, double *sn_save,
+                    double *norm) {
+    if (!bk_save || !sn_save || !ells || n_multipoles <= 0) return -1;
+    std::vector<MP> mps;
+    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
+    HG_GUARD(ctx, ctx->bk_box_multi(mps, ith_kbin, bk_save, sn_save, norm));
 }
 
 int hg_zeta_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double *zeta_save, double *sn_save,

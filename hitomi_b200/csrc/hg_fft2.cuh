@@ -1,0 +1,386 @@
+// hg_fft2.cuh -- register-resident two-level line FFTs for lengths L = R1 * R2 <= 256.
+//
+// A line of L points is handled by R2 threads that each hold R1 values (R1 = R2 or 2 R2):
+//   step A  thread t loads x[R2 n1 + t], n1 < R1, does a DFT of size R1 in registers and
+//           multiplies by the twiddle w_L^(t k1);
+//   one exchange through shared memory (conflict-free layouts below);
+//   step B  thread t takes k1 in {t, t + R2} (R1 = 2 R2) or {t}, does a DFT of size R2
+//           over n2 and ends up holding X[k1 + R1 k2].
+// The positions a thread holds after step B are {t + R2 m, m < R1}: exactly its step-A
+// input set.  So an inverse transform can be followed by a pointwise product and a
+// forward transform without any data movement in between (k_chain_x_reg).
+//
+// Global <-> register traffic is direct and coalesced: for a tile of B columns of a
+// strided axis ("COLS") thread = t B + b, so a warp reads 32 consecutive columns of one
+// row; for B contiguous lines ("ROWS") thread = b R2 + t, so a warp reads R2-element runs.
+// Shared memory is touched twice per element per transform (vs twice per radix pass).
+#pragma once
+
+#include "hg_common.cuh"
+#include "hg_fft.cuh"
+
+namespace hg {
+
+// exp(-2 pi i k / 32), k = 0..31 (correctly rounded doubles), as compile-time constants
+__host__ __device__ constexpr double tw32_re(int k) {
+    switch (k) {
+        case 0: return 1.0;
+        case 1: return 0.9807852804032304;
+        case 2: return 0.9238795325112867;
+        case 3: return 0.8314696123025452;
+        case 4: return 0.7071067811865476;
+        case 5: return 0.5555702330196022;
+        case 6: return 0.3826834323650898;
+        case 7: return 0.19509032201612828;
+        case 8: return 0.0;
+        case 9: return -0.19509032201612828;
+        case 10: return -0.3826834323650898;
+        case 11: return -0.5555702330196022;
+        case 12: return -0.7071067811865476;
+        case 13: return -0.8314696123025452;
+        case 14: return -0.9238795325112867;
+        case 15: return -0.9807852804032304;
+        case 16: return -1.0;
+        case 17: return -0.9807852804032304;
+        case 18: return -0.9238795325112867;
+        case 19: return -0.8314696123025452;
+        case 20: return -0.7071067811865476;
+        case 21: return -0.5555702330196022;
+        case 22: return -0.3826834323650898;
+        case 23: return -0.19509032201612828;
+        case 24: return 0.0;
+        case 25: return 0.19509032201612828;
+        case 26: return 0.3826834323650898;
+        case 27: return 0.5555702330196022;
+        case 28: return 0.7071067811865476;
+        case 29: return 0.8314696123025452;
+        case 30: return 0.9238795325112867;
+        case 31: return 0.9807852804032304;
+        default: return 0.0;
+    }
+}
+__host__ __device__ constexpr double tw32_im(int k) {
+    switch (k) {
+        case 0: return 0.0;
+        case 1: return -0.19509032201612828;
+        case 2: return -0.3826834323650898;
+        case 3: return -0.5555702330196022;
+        case 4: return -0.7071067811865476;
+        case 5: return -0.8314696123025452;
+        case 6: return -0.9238795325112867;
+        case 7: return -0.9807852804032304;
+        case 8: return -1.0;
+        case 9: return -0.9807852804032304;
+        case 10: return -0.9238795325112867;
+        case 11: return -0.8314696123025452;
+        case 12: return -0.7071067811865476;
+        case 13: return -0.5555702330196022;
+        case 14: return -0.3826834323650898;
+        case 15: return -0.19509032201612828;
+        case 16: return 0.0;
+        case 17: return 0.19509032201612828;
+        case 18: return 0.3826834323650898;
+        case 19: return 0.5555702330196022;
+        case 20: return 0.7071067811865476;
+        case 21: return 0.8314696123025452;
+        case 22: return 0.9238795325112867;
+        case 23: return 0.9807852804032304;
+        case 24: return 1.0;
+        case 25: return 0.9807852804032304;
+        case 26: return 0.9238795325112867;
+        case 27: return 0.8314696123025452;
+        case 28: return 0.7071067811865476;
+        case 29: return 0.5555702330196022;
+        case 30: return 0.3826834323650898;
+        case 31: return 0.19509032201612828;
+        default: return 0.0;
+    }
+}
+
+__host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
+__host__ __device__ constexpr int brevc(int i, int bits) { return bits == 0 ? 0 : ((i & 1) << (bits - 1)) | brevc(i >> 1, bits - 1); }
+
+// v * exp(DIR 2 pi i K / 32)
+template <typename T, int DIR, int K>
+__device__ __forceinline__ cplx<T> tw32_mul(cplx<T> v) {
+    constexpr T c = (T)tw32_re(K), s = (T)tw32_im(K);  // exp(-2 pi i K/32)
+    if constexpr (DIR < 0) return mk<T>(v.x * c - v.y * s, v.x * s + v.y * c);
+    else return mk<T>(v.x * c + v.y * s, v.y * c - v.x * s);
+}
+
+template <typename T, int R, int I>
+__device__ __forceinline__ void brev_swaps(cplx<T> *v) {
+    if constexpr (I < R) {
+        constexpr int J = brevc(I, ilog2c(R));
+        if constexpr (J > I) {
+            cplx<T> t = v[I];
+            v[I] = v[J];
+            v[J] = t;
+        }
+        brev_swaps<T, R, I + 1>(v);
+    }
+}
+
+template <typename T, int R, int DIR, int LEN, int J>
+__device__ __forceinline__ void bfly_stage(cplx<T> *v) {
+    if constexpr (J < LEN / 2) {
+        constexpr int K = J * (32 / LEN);  // w_LEN^J = w_32^K
+#pragma unroll
+        for (int i = 0; i < R; i += LEN) {
+            cplx<T> u = v[i + J];
+            cplx<T> t = v[i + J + LEN / 2];
+            if constexpr (K == 8) t = mul_i<T, DIR>(t);
+            else if constexpr (K != 0) t = tw32_mul<T, DIR, K>(t);
+            v[i + J] = u + t;
+            v[i + J + LEN / 2] = u - t;
+        }
+        bfly_stage<T, R, DIR, LEN, J + 1>(v);
+    }
+}
+
+template <typename T, int R, int DIR, int LEN>
+__device__ __forceinline__ void bfly_stages(cplx<T> *v) {
+    if constexpr (LEN <= R) {
+        bfly_stage<T, R, DIR, LEN, 0>(v);
+        bfly_stages<T, R, DIR, LEN * 2>(v);
+    }
+}
+
+// In-register DFT of size R (power of two <= 32), natural-order output,
+// X[q] = sum_r v[r] exp(DIR 2 pi i r q / R): bit-reversal permutation, then radix-2
+// decimation-in-time stages; every index and twiddle is a compile-time constant.
+template <typename T, int R, int DIR>
+__device__ __forceinline__ void dft_reg(cplx<T> *v) {
+    brev_swaps<T, R, 0>(v);
+    bfly_stages<T, R, DIR, 2>(v);
+}
+
+template <int L>
+struct Split;
+template <> struct Split<8> { static constexpr int R1 = 4, R2 = 2; };
+template <> struct Split<16> { static constexpr int R1 = 4, R2 = 4; };
+template <> struct Split<32> { static constexpr int R1 = 8, R2 = 4; };
+template <> struct Split<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct Split<128> { static constexpr int R1 = 16, R2 = 8; };
+template <> struct Split<256> { static constexpr int R1 = 16, R2 = 16; };
+
+// Shared-memory exchange buffers for B lines.  COLS: S[(k1 R2 + t) B + b].
+// ROWS: S[b LP + k1 (R2 + 1) + t] with LP = R1 (R2 + 1).
+template <int L, bool COLS, int B>
+struct XchgLayout {
+    static constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    static constexpr int LP = R1 * (R2 + 1);
+    static constexpr int ELEMS = COLS ? L * B : LP * B;
+    __device__ static __forceinline__ int at(int b, int k1, int t) {
+        return COLS ? (k1 * R2 + t) * B + b : b * LP + k1 * (R2 + 1) + t;
+    }
+};
+
+// One full line transform on values already in registers (v[n1] = x[R2 n1 + t]).
+// On return v holds X at positions t + R2 m in the order of `pos_of_reg`.
+template <typename T, int L, int DIR, bool COLS, int B>
+__device__ __forceinline__ void line_fft2(cplx<T> *v, cplx<T> *S, int t, int b, const cplx<T> *__restrict__ tw) {
+    using X = XchgLayout<L, COLS, B>;
+    constexpr int R1 = X::R1, R2 = X::R2;
+    dft_reg<T, R1, DIR>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; k1++) v[k1] = mul_tw<T, DIR>(v[k1], tw[(t * k1) & (L - 1)]);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; k1++) S[X::at(b, k1, t)] = v[k1];
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < R1 / R2; d++) {
+        const int k1 = t + d * R2;
+#pragma unroll
+        for (int n2 = 0; n2 < R2; n2++) v[d * R2 + n2] = S[X::at(b, k1, n2)];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < R1 / R2; d++) dft_reg<T, R2, DIR>(&v[d * R2]);
+}
+
+// Register slot r = d R2 + k2 holds position k1 + R1 k2 with k1 = t + d R2.
+template <int L>
+__device__ __forceinline__ int pos_of_reg(int t, int r) {
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    const int d = r / R2, k2 = r % R2;
+    return t + d * R2 + R1 * k2;
+}
+// Step-A register n1 holds position R2 n1 + t.  The register holding a given step-A index
+// n1 after a step B: n1 = d + (R1/R2) k2 -> r = d R2 + k2.
+template <int L>
+__device__ __forceinline__ int reg_of_n1(int n1) {
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    constexpr int Q = R1 / R2;
+    const int d = n1 % Q, k2 = n1 / Q;
+    return d * R2 + k2;
+}
+
+template <typename T, int L, bool COLS>
+struct Fft2Cfg {
+    static constexpr int R2 = Split<L>::R2;
+    // lines per CTA: columns (strided axes) or whole lines (contiguous axis)
+    static constexpr int B = COLS ? ((sizeof(T) == 4) ? 32 : 16) : (256 / R2 > 64 ? 64 : 256 / R2);
+    static constexpr int NT = R2 * B;
+};
+
+// Generic pass: same tile geometry and loader/storer functors as k_fft_pass.
+template <typename T, int L, int DIR, bool COLS, class LD, class ST>
+__global__ void __launch_bounds__(Fft2Cfg<T, L, COLS>::NT)
+    k_fft2_pass(LD ld, ST st, PassGeom g, const cplx<T> *__restrict__ tw) {
+    using CF = Fft2Cfg<T, L, COLS>;
+    using X = XchgLayout<L, COLS, CF::B>;
+    constexpr int R1 = X::R1, R2 = X::R2, B = CF::B;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
+    int t, b;
+    if (COLS) {
+        t = threadIdx.x / B;
+        b = threadIdx.x % B;
+    } else {
+        b = threadIdx.x / R2;
+        t = threadIdx.x % R2;
+    }
+    long long o, i;
+    bool ok;
+    if (COLS) {
+        long long tiles_per_outer = (g.n_inner + B - 1) / B;
+        o = (long long)blockIdx.x / tiles_per_outer;
+        i = ((long long)blockIdx.x - o * tiles_per_outer) * B + b;
+        ok = i < g.n_inner;
+    } else {
+        o = (long long)blockIdx.x * B + b;
+        i = 0;
+        ok = o < g.n_outer;
+    }
+    cplx<T> v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; n1++) v[n1] = ok ? ld(o, R2 * n1 + t, i) : mk<T>(0, 0);
+    line_fft2<T, L, DIR, COLS, B>(v, S, t, b, tw);
+    if (ok) {
+#pragma unroll
+        for (int r = 0; r < R1; r++) st(o, pos_of_reg<L>(t, r), i, v[r]);
+    }
+}
+
+template <typename T, int L, bool COLS>
+inline size_t fft2_smem() {
+    using CF = Fft2Cfg<T, L, COLS>;
+    return (size_t)XchgLayout<L, COLS, CF::B>::ELEMS * sizeof(cplx<T>);
+}
+
+template <typename T, int L, int DIR, class LD, class ST>
+inline cudaError_t launch_fft2_L(LD ld, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
+    if (g.n_inner == 1) {
+        using CF = Fft2Cfg<T, L, false>;
+        size_t smem = fft2_smem<T, L, false>();
+        auto kern = k_fft2_pass<T, L, DIR, false, LD, ST>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        long long tiles = (g.n_outer + CF::B - 1) / CF::B;
+        if (tiles <= 0) return cudaSuccess;
+        kern<<<(unsigned)tiles, CF::NT, smem, stream>>>(ld, st, g, tw);
+    } else {
+        using CF = Fft2Cfg<T, L, true>;
+        size_t smem = fft2_smem<T, L, true>();
+        auto kern = k_fft2_pass<T, L, DIR, true, LD, ST>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        long long tiles = g.n_outer * ((g.n_inner + CF::B - 1) / CF::B);
+        if (tiles <= 0) return cudaSuccess;
+        kern<<<(unsigned)tiles, CF::NT, smem, stream>>>(ld, st, g, tw);
+    }
+    return cudaGetLastError();
+}
+
+// Any supported length: two-level register FFT up to 256, Stockham beyond.
+template <typename T, int DIR, class LD, class ST>
+inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
+    switch (L) {
+        case 8: return launch_fft2_L<T, 8, DIR>(ld, st, g, tw, stream);
+        case 16: return launch_fft2_L<T, 16, DIR>(ld, st, g, tw, stream);
+        case 32: return launch_fft2_L<T, 32, DIR>(ld, st, g, tw, stream);
+        case 64: return launch_fft2_L<T, 64, DIR>(ld, st, g, tw, stream);
+        case 128: return launch_fft2_L<T, 128, DIR>(ld, st, g, tw, stream);
+        case 256: return launch_fft2_L<T, 256, DIR>(ld, st, g, tw, stream);
+        default: return launch_fft_pass<T, DIR>(L, ld, st, g, tw, stream);
+    }
+}
+
+// The chain kernel keeps G and two register tiles live: 16 columns per CTA (256 threads).
+template <typename T, int L>
+struct ChainCfg {
+    static constexpr int R2 = Split<L>::R2;
+    static constexpr int B = 16;
+    static constexpr int NT = R2 * B;
+};
+
+// Fused chain x-pass with the register FFT: T2 layout [j][cx][y][z] (rows of `plane`
+// columns), G [x][y][z].  Thread (t, b) keeps its R1 values of G in registers for all
+// shells j; per shell: load the K kept rows, inverse FFT, * G, forward FFT, store K rows.
+template <typename T, int L>
+__global__ void __launch_bounds__(ChainCfg<T, L>::NT)
+    k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
+                  const cplx<T> *__restrict__ tw) {
+    using CF = ChainCfg<T, L>;
+    using X = XchgLayout<L, true, CF::B>;
+    constexpr int R1 = X::R1, R2 = X::R2, B = CF::B;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
+    const int t = threadIdx.x / B, b = threadIdx.x % B;
+    const long long i = (long long)blockIdx.x * B + b;
+    const bool ok = i < plane;
+    // G at the positions this thread holds after an inverse transform (register order);
+    // kept in registers across shells in FP32, re-read (L2-resident) per shell in FP64
+    constexpr bool kCacheG = (sizeof(T) == 4);
+    cplx<T> gr[kCacheG ? R1 : 1];
+    if (kCacheG) {
+#pragma unroll
+        for (int r = 0; r < (kCacheG ? R1 : 1); r++) {
+            const int x = pos_of_reg<L>(t, r);
+            gr[r] = ok ? G[(long long)x * plane + i] : mk<T>(0, 0);
+        }
+    }
+    for (int j = 0; j < ns; j++) {
+        cplx<T> *tj = t2 + (long long)j * K * plane;
+        cplx<T> v[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) {
+            const int p = R2 * n1 + t;
+            const int n = (p < L / 2) ? p : p - L;
+            const int c = n + s;
+            v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)c * plane + i] : mk<T>(0, 0);
+        }
+        line_fft2<T, L, +1, true, B>(v, S, t, b, tw);
+        // product with G, then regroup to step-A order of the forward transform
+        cplx<T> u[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) {
+            const int r = reg_of_n1<L>(n1);
+            cplx<T> gv;
+            if (kCacheG) gv = gr[kCacheG ? r : 0];
+            else gv = ok ? G[(long long)pos_of_reg<L>(t, r) * plane + i] : mk<T>(0, 0);
+            u[n1] = v[r] * gv;
+        }
+        line_fft2<T, L, -1, true, B>(u, S, t, b, tw);
+        if (ok) {
+#pragma unroll
+            for (int r = 0; r < R1; r++) {
+                const int p = pos_of_reg<L>(t, r);
+                const int n = (p < L / 2) ? p : p - L;
+                if (n >= -s && n <= s) tj[(long long)(n + s) * plane + i] = u[r];
+            }
+        }
+    }
+}
+
+template <typename T, int L>
+inline cudaError_t launch_chain_x_reg_L(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
+                                        const cplx<T> *tw, cudaStream_t st) {
+    using CF = ChainCfg<T, L>;
+    size_t smem = (size_t)XchgLayout<L, true, CF::B>::ELEMS * sizeof(cplx<T>);
+    cudaFuncSetAttribute(k_chain_x_reg<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    unsigned tiles = (unsigned)((plane + CF::B - 1) / CF::B);
+    k_chain_x_reg<T, L><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);
+    return cudaGetLastError();
+}
+
+}  // namespace hg

@@ -4,9 +4,8 @@
 //   k_pk_bin        binned  (f1 conj f2 - S C(k)) / W^2 * Yhat_lm(k)  (field.hpp:765-852)
 //   k_shell_D       delta(k)/W(k) for every (shell, mode) entry      (field.hpp:346-401)
 //   k_family_A      A_f,i(k) = Yhat_f(k) delta/W / n_i
-//   k_scatter_*     place k-space inputs on the (reduced) transform grid
-//   k_extract_neg   gather Qhat(-k) at the shell entries
-//   k_pair_dot      sum over a shell of A_a(k) Qhat_b(-k)
+//   k_scatter_*     place k-space inputs on the compact shell / G cubes
+//   k_pair_dot_cube sum over a shell of A_a(k) Qhat_b(-k)
 //   k_xi_orbit_hist last inverse-FFT pass of the shot-noise correlation field fused with
 //                   its radial histogram over integer n^2 = |x/dr|^2
 //   k_bessel_table, k_sn_matrix   spline-evaluated j_l products summed over n^2
@@ -179,22 +178,22 @@ __global__ void k_family_A(const ShellEnt *ent, long long ne, Grid g, int l, int
     A[e] = make_double2(v.x * sc, v.y * sc);
 }
 
-// Scatter A[e] into batch slot shell(e) of a [ns][M0][M1][M2] transform buffer.
+// Scatter A[e] into the compact cube of its shell: buf[shell][nx+s][ny+s][nz+s].
 template <typename T>
-__global__ void k_scatter_entries(const ShellEnt *ent, long long ne, const double2 *A, int3 M, cplx<T> *buf) {
+__global__ void k_scatter_cube(const ShellEnt *ent, long long ne, const double2 *A, int3 K, int3 s, cplx<T> *buf) {
     long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= ne) return;
-    ShellEnt s = ent[e];
-    long long vol = (long long)M.x * M.y * M.z;
-    long long idx = (long long)s.shell * vol +
-                    ((long long)mod_idx(s.nx, M.x) * M.y + mod_idx(s.ny, M.y)) * M.z + mod_idx(s.nz, M.z);
+    ShellEnt q = ent[e];
+    long long vol = (long long)K.x * K.y * K.z;
+    long long idx = (long long)q.shell * vol + ((long long)(q.nx + s.x) * K.y + (q.ny + s.y)) * K.z + (q.nz + s.z);
     buf[idx] = mk<T>((T)A[e].x, (T)A[e].y);
 }
 
-// G input: g(k) = (delta(k)/W(k)) / V on the cube |n_a| <= ext_a of the M grid.
+// G input on the compact cube [lo, lo+cnt): g(k) = (delta(k)/W(k)) / V  (field.hpp:636-637,
+// 332-335), with the k = 0 mode from the FP64 field integral.
 template <typename T>
-__global__ void k_scatter_G(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int3 lo, int3 cnt, int3 M, double k0_re,
-                            double k0_im, cplx<T> *buf) {
+__global__ void k_scatter_G(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int3 lo, int3 cnt, double k0_re, double k0_im,
+                            cplx<T> *buf) {
     long long total = (long long)cnt.x * cnt.y * cnt.z;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
@@ -205,35 +204,34 @@ __global__ void k_scatter_G(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int3 lo,
         zd d = (ix == 0 && iy == 0 && iz == 0) ? mk<double>(k0_re, k0_im) : f.at(ix, iy, iz);
         double wf = window_tab(tabs, ix, iy, iz, wpow);
         double re = d.x / wf / g.volume, im = d.y / wf / g.volume;
-        long long o = ((long long)mod_idx(nx, M.x) * M.y + mod_idx(ny, M.y)) * M.z + mod_idx(nz, M.z);
-        buf[o] = mk<T>((T)re, (T)im);
+        buf[idx] = mk<T>((T)re, (T)im);
     }
 }
 
-// QE[j][e] = Qhat_j(-n_e)
-template <typename T>
-__global__ void k_extract_neg(const ShellEnt *ent, long long ne, int ns, int3 M, const cplx<T> *buf, double2 *QE) {
-    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y;
-    if (e >= ne) return;
-    ShellEnt s = ent[e];
-    long long vol = (long long)M.x * M.y * M.z;
-    long long idx = (long long)j * vol +
-                    ((long long)mod_idx(-s.nx, M.x) * M.y + mod_idx(-s.ny, M.y)) * M.z + mod_idx(-s.nz, M.z);
-    cplx<T> v = buf[idx];
-    QE[(long long)j * ne + e] = make_double2((double)v.x, (double)v.y);
+__device__ __forceinline__ int neg_c(int n, int M, int s) {
+    int m = -n;
+    if (m >= M / 2) m -= M;  // a whole (unreduced) axis: -(-M/2) is the same mode as -M/2
+    return m + s;
 }
 
-// out[i][j] = sum_{e in shell i} A[e] * QE[j][e]; one block per (i, j); deterministic.
-__global__ void k_pair_dot(const int *start, int ns_i, const double2 *A, const double2 *QE, long long ne, int ns_j,
-                           double2 *out) {
+// out[i][j] = sum_{e in shell i} A[e] * Q[j](-n_e), Q the compact cubes of a chain family;
+// one block per (i, j); deterministic.
+template <typename T>
+__global__ void k_pair_dot_cube(const int *start, const ShellEnt *ent, const double2 *A, const cplx<T> *Q, int3 K,
+                                int3 M, int3 s, int ns_j, double2 *out) {
     int i = blockIdx.x, j = blockIdx.y;
     __shared__ double red[2][32];
+    const long long vol = (long long)K.x * K.y * K.z;
+    const cplx<T> *Qj = Q + (long long)j * vol;
     double sr = 0.0, si = 0.0;
     for (int e = start[i] + threadIdx.x; e < start[i + 1]; e += blockDim.x) {
-        double2 a = A[e], q = QE[(long long)j * ne + e];
-        sr += a.x * q.x - a.y * q.y;
-        si += a.x * q.y + a.y * q.x;
+        ShellEnt q = ent[e];
+        long long idx = ((long long)neg_c(q.nx, M.x, s.x) * K.y + neg_c(q.ny, M.y, s.y)) * K.z + neg_c(q.nz, M.z, s.z);
+        cplx<T> v = Qj[idx];
+        double2 a = A[e];
+        double qx = (double)v.x, qy = (double)v.y;
+        sr += a.x * qx - a.y * qy;
+        si += a.x * qy + a.y * qx;
     }
     for (int o = 16; o > 0; o >>= 1) {
         sr += __shfl_down_sync(0xffffffffu, sr, o);
@@ -442,16 +440,6 @@ struct StHalf {  // keep the non-negative half of the last axis
         if (l < hz) H[o * hz + l] = v;
     }
 };
-template <typename T>
-struct LdMulG {  // chain[o][l] * G[(o mod plane)][l]
-    const cplx<T> *p;
-    const cplx<T> *G;
-    long long L, plane;
-    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
-        cplx<T> a = p[o * L + l];
-        cplx<T> b = G[(o % plane) * L + l];
-        return a * b;
-    }
-};
+
 
 }  // namespace hg

@@ -97,6 +97,14 @@ int hg_pk_box(hg_ctx *ctx, int ell, double *pk_save, int *n_mode, double *norm);
 int hg_bk_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_kbin, double *bk_save, double *sn_save,
               double *norm);
 
+/* Several periodic-box bispectrum multipoles in one call, sharing the density transform,
+ * the shell-field chains and the shot-noise correlation field.  ells = n_multipoles
+ * (ell1, ell2, ELL) triples; outputs are n_multipoles consecutive blocks laid out as in
+ * hg_bk_box.  Each block equals what calcBiSpectrumForBOX (bispec.hpp:877-1203) computes
+ * for that multipole. */
+int hg_bk_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double *bk_save, double *sn_save,
+                    double *norm);
+
 /* Periodic-box 3PCF multipole.  Replaces calcThreePointCorrelationFunctionForBOX
  * (bispec.hpp:1205-1424).  Layout as hg_bk_box with r bins; output file value =
  * norm * Re(zeta_save - sn_save) (bispec.hpp:1409-1416). */

@@ -125,3 +125,16 @@ def test_repeated_calls_are_stable():
         c.set_particles(0, d["pos"])
         a2 = c.bk_box(0, 0, 0)
         assert relerr(a2[2] * (a2[0] - a2[1]), a1[2] * (a1[0] - a1[1])) < 1e-12
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_bk_box_multi_matches_single(form):
+    """hg_bk_box_multi gives each multipole what hg_bk_box gives it alone."""
+    d = load_golden("box_bk.npz")
+    b = binning_from(d["binning"])
+    with ctx(int(d["n_mesh"]), float(d["boxsize"]), b, "TSC", form) as c:
+        c.set_particles(0, d["pos"])
+        bk, sn, norm = c.bk_box_multi(MULTIPOLES)
+        for q, mp in enumerate(MULTIPOLES):
+            ref = d["bk_TSC_" + "".join(map(str, mp))]
+            assert relerr(norm * (bk[q] - sn[q]), ref, FLOOR[form]) < TOL[form], mp
