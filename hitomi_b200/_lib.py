@@ -26,6 +26,7 @@ SYMBOLS = (
     "hg_pk_survey",
     "hg_set_profiling",
     "hg_kernel_stats",
+    "hg_pk_box_spectrum_static",
     "hg_last_timing",
 )
 
@@ -93,6 +94,9 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_survey_scalars.restype = ctypes.c_int
     lib.hg_pk_survey.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, c_dp, c_ip, c_dp]
     lib.hg_pk_survey.restype = ctypes.c_int
+    lib.hg_pk_box_spectrum_static.argtypes = [ctypes.POINTER(HgConfig), ctypes.c_void_p, ctypes.c_longlong,
+                                              ctypes.c_int, c_dp, c_ip, c_dp, ctypes.c_void_p]
+    lib.hg_pk_box_spectrum_static.restype = ctypes.c_int
     lib.hg_last_timing.argtypes = [vp, c_dp, ctypes.POINTER(ctypes.c_longlong)]
     lib.hg_last_timing.restype = ctypes.c_int
     _lib = lib

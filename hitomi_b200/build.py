@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhitomi_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "hg_engine.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "hg_engine.cu"), os.path.join(HERE, "csrc", "hg_static.cu")]
 HEADERS = [
     os.path.join(HERE, "csrc", f)
     for f in os.listdir(os.path.join(HERE, "csrc"))

@@ -1195,6 +1195,11 @@ thread_local std::string g_create_error;
 
 }  // namespace
 
+namespace hg {
+// Error text returned by hg_last_error(NULL) for entry points that have no context.
+void set_contextless_error(const std::string &m) { g_create_error = m; }
+}  // namespace hg
+
 extern "C" {
 
 int hg_create(hg_ctx **out, const hg_config *cfg) {

@@ -13,16 +13,9 @@
 
 #include "hg_common.cuh"
 #include "hg_fft.cuh"
+#include "hg_bin.cuh"
 
 namespace hg {
-
-// Per-axis tables indexed by array index i (mode n = wrap(i)):
-//   tw[i] = sinc(pi w / n)   with w = (int)(n dk / dk + 1e-5)   (window, field.hpp:664-675)
-//   ts[i] = sin(pi w / n)    (0 when w == 0)                   (shot noise, field.hpp:1261-1272)
-struct AxisTabs {
-    const double *tw[3];
-    const double *ts[3];
-};
 
 __global__ void k_axis_tables(Grid g, int axis, double *tw, double *ts) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -32,120 +25,6 @@ __global__ void k_axis_tables(Grid g, int axis, double *tw, double *ts) {
     int w = window_index(kv, g.dk[axis]);
     tw[i] = sinc_axis(w, n);
     ts[i] = (w != 0) ? sin(HG_PI * (double)w / (double)n) : 0.0;
-}
-
-__device__ __forceinline__ double window_tab(const AxisTabs &t, int ix, int iy, int iz, int p) {
-    double ret = t.tw[0][ix] * t.tw[1][iy] * t.tw[2][iz];
-    double w = ret;
-    for (int q = 1; q < p; q++) w *= ret;
-    return w;
-}
-
-__device__ __forceinline__ double shot_tab(const AxisTabs &t, int ix, int iy, int iz, int assign) {
-    if (assign == 0) return 1.0;
-    const double s[3] = {t.ts[0][ix], t.ts[1][iy], t.ts[2][iz]};
-    double ret = 1.0;
-    for (int a = 0; a < 3; a++) {
-        double s2 = s[a] * s[a];
-        double f;
-        if (assign == 1) f = 1.0 - (2.0 / 3.0) * s2;
-        else if (assign == 2) f = 1.0 - s2 + 2.0 * (s2 * s2) / 15.0;
-        else f = 1.0 - (4.0 / 3.0) * s2 + (2.0 / 5.0) * s2 * s2 - (4.0 / 315.0) * s2 * s2 * s2;
-        ret *= f;
-    }
-    return ret;
-}
-
-// Read access to a transformed field, either a half spectrum [n0][n1][n2/2+1] of a real
-// input (negative kz by Hermitian symmetry) or a full [n0][n1][n2] spectrum.
-template <typename T>
-struct Spec {
-    const cplx<T> *p;
-    int n0, n1, n2;
-    int half;
-    __device__ __forceinline__ zd at(int ix, int iy, int iz) const {
-        if (!half) {
-            cplx<T> v = p[((long long)ix * n1 + iy) * n2 + iz];
-            return mk<double>((double)v.x, (double)v.y);
-        }
-        int hz = n2 / 2 + 1;
-        if (iz < hz) {
-            cplx<T> v = p[((long long)ix * n1 + iy) * hz + iz];
-            return mk<double>((double)v.x, (double)v.y);
-        }
-        int jx = (n0 - ix) % n0, jy = (n1 - iy) % n1, jz = n2 - iz;
-        cplx<T> v = p[((long long)jx * n1 + jy) * hz + jz];
-        return mk<double>((double)v.x, -(double)v.y);
-    }
-};
-
-struct LM {
-    int l, m;
-};
-
-#define HG_MAX_LM 16
-
-struct LMList {
-    int n;
-    LM lm[HG_MAX_LM];
-};
-
-// P-binning over the mode cube [lo, lo+cnt) (wrapped modes).  acc: [nbin][nlm] complex,
-// nmode: [nbin].  lut maps the fine index int(|k|/1e-4 + 0.5) to up to two coarse bins.
-template <typename T>
-__global__ void k_pk_bin(Spec<T> f1, Spec<T> f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt, const int2 *lut, int lutn,
-                         int nbin, LMList lms, double S_re, double S_im, int assign, int wpow, double *acc,
-                         unsigned long long *nmode, int k0_special, double k0_re, double k0_im) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sacc = reinterpret_cast<double *>(smem_raw);
-    unsigned long long *scnt = reinterpret_cast<unsigned long long *>(sacc + 2 * nbin * lms.n);
-    for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x) sacc[q] = 0.0;
-    for (int q = threadIdx.x; q < nbin; q += blockDim.x) scnt[q] = 0ull;
-    __syncthreads();
-    const long long total = (long long)cnt.x * cnt.y * cnt.z;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        int nz = lo.z + (int)(idx % cnt.z);
-        int ny = lo.y + (int)((idx / cnt.z) % cnt.y);
-        int nx = lo.x + (int)(idx / ((long long)cnt.z * cnt.y));
-        int ix = (nx + g.n[0]) % g.n[0], iy = (ny + g.n[1]) % g.n[1], iz = (nz + g.n[2]) % g.n[2];
-        double kv[3] = {kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
-                        kcomp(wrap_index(iz, g.n[2]), g.dk[2])};
-        double kmag = kmag_exact(kv[0], kv[1], kv[2]);
-        int kindex = (int)__dadd_rn(__ddiv_rn(kmag, 0.0001), 0.5);
-        if (kindex >= lutn) continue;
-        int2 b = lut[kindex];
-        if (b.x < 0) continue;
-        zd d1 = f1.at(ix, iy, iz), d2 = f2.at(ix, iy, iz);
-        zd pk2;
-        if (k0_special && ix == 0 && iy == 0 && iz == 0) {
-            pk2 = mk<double>(k0_re, k0_im);
-        } else {
-            pk2 = d1 * conjg(d2);
-        }
-        double C = shot_tab(tabs, ix, iy, iz, assign);
-        pk2 = pk2 - mk<double>(S_re * C, S_im * C);
-        double wf = window_tab(tabs, ix, iy, iz, wpow);
-        double w2 = wf * wf;
-        pk2 = mk<double>(pk2.x / w2, pk2.y / w2);
-        for (int q = 0; q < lms.n; q++) {
-            zd y = ylm_reduced(lms.lm[q].l, lms.lm[q].m, kv[0], kv[1], kv[2]);
-            zd v = pk2 * y;
-            atomicAdd(&sacc[2 * (b.x * lms.n + q)], v.x);
-            atomicAdd(&sacc[2 * (b.x * lms.n + q) + 1], v.y);
-            if (b.y >= 0) {
-                atomicAdd(&sacc[2 * (b.y * lms.n + q)], v.x);
-                atomicAdd(&sacc[2 * (b.y * lms.n + q) + 1], v.y);
-            }
-        }
-        atomicAdd(&scnt[b.x], 1ull);
-        if (b.y >= 0) atomicAdd(&scnt[b.y], 1ull);
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x)
-        if (sacc[q] != 0.0) atomicAdd(&acc[q], sacc[q]);
-    for (int q = threadIdx.x; q < nbin; q += blockDim.x)
-        if (scnt[q]) atomicAdd(&nmode[q], scnt[q]);
 }
 
 // Shell entries: wrapped mode (nx, ny, nz) and shell index.

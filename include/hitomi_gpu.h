@@ -132,6 +132,23 @@ int hg_pk_survey(hg_ctx *ctx, int ell, double alpha, double vsurvey, double *pk_
 int hg_set_profiling(hg_ctx *ctx, int on);
 int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen);
 
+/* Allocation-free periodic-box power-spectrum multipole, for callers that cannot call
+ * cudaMalloc (work captured into a CUDA graph, or an application whose allocator owns all
+ * device memory).  No counterpart in the reference: it is the binning step of hg_pk_box
+ * run on a density spectrum the caller already holds on the device.
+ *   d_half_spectrum : device array [n0][n1][n2/2+1] of complex (double pairs for HG_FP64,
+ *                     float pairs for HG_FP32, per cfg->precision) holding
+ *                     FFT[dV (rho - N/V)], the non-negative-kz half of the reference's
+ *                     calcFourierTransform output (field.hpp:310-325) for a real field.
+ *   outputs as hg_pk_box; stream is a cudaStream_t (NULL: the default stream).
+ * All scratch sits in a 1 MiB file-scope __device__ array that every GPU loading this
+ * library keeps until exit.  Limits: n_kbin <= 256, n_mesh <= 1024 per axis, k bins
+ * below |k| = 10; larger requests fail with an error and launch nothing.  The first call
+ * on a device looks up that array's address (make it before any stream capture).  Calls
+ * share the array: calls overlapping on the GPU race.  Errors: hg_last_error(NULL). */
+int hg_pk_box_spectrum_static(const hg_config *cfg, const void *d_half_spectrum, long long n_particles, int ell,
+                              double *pk_save, int *n_mode, double *norm, void *stream);
+
 /* Device-side time of the last statistic call in milliseconds (CUDA events on the
  * context's stream), and the number of kernels it launched. */
 int hg_last_timing(const hg_ctx *ctx, double *device_ms, long long *kernel_launches);
