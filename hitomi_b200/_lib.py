@@ -22,6 +22,7 @@ SYMBOLS = (
     "hg_bk_box",
     "hg_bk_box_multi",
     "hg_zeta_box",
+    "hg_zeta_box_multi",
     "hg_survey_scalars",
     "hg_pk_survey",
     "hg_set_profiling",
@@ -90,6 +91,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_bk_box_multi.restype = ctypes.c_int
     lib.hg_zeta_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, c_dp]
     lib.hg_zeta_box.restype = ctypes.c_int
+    lib.hg_zeta_box_multi.argtypes = [vp, ctypes.c_int, c_ip, ctypes.c_int, c_dp, c_dp, c_dp]
+    lib.hg_zeta_box_multi.restype = ctypes.c_int
     lib.hg_survey_scalars.argtypes = [vp, c_dp, c_dp, c_dp, c_dp, c_dp]
     lib.hg_survey_scalars.restype = ctypes.c_int
     lib.hg_pk_survey.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, c_dp, c_ip, c_dp]

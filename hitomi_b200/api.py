@@ -173,6 +173,20 @@ class Context:
         c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(rows, nr)
         return c(z), c(sn), norm.value
 
+    def zeta_box_multi(self, multipoles, ith_rbin: int = -1):
+        """Several (ell1, ell2, ELL) 3PCF multipoles at once: arrays [m][rows][n_rbin] and norm."""
+        nr = self.binning.n_rbin
+        rows = nr if ith_rbin < 0 else 1
+        m = len(multipoles)
+        ells = np.array([v for mp in multipoles for v in mp], dtype=np.int32)
+        z = np.zeros(2 * m * rows * nr)
+        sn = np.zeros(2 * m * rows * nr)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_zeta_box_multi(self._h, m, ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                ith_rbin, _dp(z), _dp(sn), ctypes.byref(norm)))
+        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nr)
+        return c(z), c(sn), norm.value
+
     def survey_scalars(self):
         vals = [ctypes.c_double() for _ in range(5)]
         self._check(self._lib.hg_survey_scalars(self._h, *[ctypes.byref(v) for v in vals]))

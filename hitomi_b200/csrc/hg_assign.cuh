@@ -34,7 +34,8 @@ struct AssignGeom {
     double shift;     // added to the scaled position (0, or 0.5 for the interlaced copy)
     int t[3];         // tile extent per axis
     int nt[3];        // tiles per axis
-    double factor;    // 1/dV (field.hpp:76-77)
+    double factor;      // 1/dV (field.hpp:76-77), used for the FP64 in-bounds mass
+    double acc_factor;  // factor applied in the mesh accumulation (1/dV, or 1 for a mass mesh)
 };
 
 __host__ __device__ __forceinline__ int stencil_width(int scheme) { return scheme + 1; }
@@ -195,18 +196,27 @@ __global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double
         double d[3];
         for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
         nt = particle_tiles(g, anc, tiles);
-        // in-bounds mass in the reference's product order
         const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
-        double w[3][4];
-        for (int a = 0; a < 3; a++) axis_weights<double>(g.scheme, d[a], w[a]);
-        for (int a = 0; a < W; a++)
-            for (int b = 0; b < W; b++)
-                for (int c = 0; c < W; c++) {
-                    int cx, cy, cz;
-                    if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
-                    m_re += wr * g.factor * w[0][a] * w[1][b] * w[2][c];
-                    m_im += wi * g.factor * w[0][a] * w[1][b] * w[2][c];
-                }
+        bool inside = true;
+        for (int a = 0; a < 3; a++) inside &= (anc[a] + s0 >= 0) && (anc[a] + s0 + W - 1 < g.n[a]);
+        if (inside || g.periodic) {
+            // every stencil point lands: the weights sum to one per axis
+            m_re += wr * g.factor;
+            m_im += wi * g.factor;
+        } else {
+            // in-bounds mass in the reference's product order
+            double w[3][4];
+            for (int a = 0; a < 3; a++) axis_weights<double>(g.scheme, d[a], w[a]);
+            for (int a = 0; a < W; a++)
+                for (int b = 0; b < W; b++)
+                    for (int c = 0; c < W; c++) {
+                        int cx, cy, cz;
+                        if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz))
+                            continue;
+                        m_re += wr * g.factor * w[0][a] * w[1][b] * w[2][c];
+                        m_im += wi * g.factor * w[0][a] * w[1][b] * w[2][c];
+                    }
+        }
     }
     const int lane = threadIdx.x & 31;
     int maxnt = __reduce_max_sync(0xffffffffu, nt);
@@ -313,15 +323,16 @@ __global__ void k_zero_split_tiles(const Chunk *ch, AssignGeom g, T *mesh_re, T 
     }
 }
 
-// One CTA per chunk.  FP64 shared-memory accumulator (both forms); the mesh stores the
-// density rho = sum_p w_p (1/dV) prod(w_axis) like the reference, in T.
+// One CTA per chunk.  Shared-memory accumulator in the form's precision (a chunk holds at
+// most 2048 records, which bounds the FP32 summation error); the mesh stores the density
+// rho = sum_p w_p (1/dV) prod(w_axis) like the reference, in T.
 template <typename T, bool CPLX>
 __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *acc = reinterpret_cast<double *>(smem_raw);
+    T *acc = reinterpret_cast<T *>(smem_raw);
     const int tcells = g.t[0] * g.t[1] * g.t[2];
-    double *acc_im = acc + tcells;
-    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = 0.0;
+    T *acc_im = acc + tcells;
+    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
     __syncthreads();
     const Chunk k = ch[blockIdx.x];
     const int tile = k.tile;
@@ -330,12 +341,12 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     const int tx = tile / (g.nt[2] * g.nt[1]);
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
     const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
-    const double factor = g.factor;
+    const T factor = (T)g.acc_factor;
     for (unsigned r = k.r0 + threadIdx.x; r < k.r1; r += blockDim.x) {
         PRec<T> pr = rec[r];
-        double w[3][4];
-        for (int a = 0; a < 3; a++) axis_weights<double>(g.scheme, (double)pr.d[a], w[a]);
-        const double wr = (double)pr.wr, wi = (double)pr.wi;
+        T w[3][4];
+        for (int a = 0; a < 3; a++) axis_weights<T>(g.scheme, pr.d[a], w[a]);
+        const T wr = pr.wr, wi = pr.wi;
         for (int a = 0; a < W; a++)
             for (int b = 0; b < W; b++)
                 for (int c = 0; c < W; c++) {
@@ -355,11 +366,11 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
         int lx, ly, lz;
         long long cell = tile_cell(g, tile, li, lx, ly, lz);
         if (k.multi == 0) {
-            mesh_re[cell] = (T)acc[li];
-            if (CPLX) mesh_im[cell] = (T)acc_im[li];
+            mesh_re[cell] = acc[li];
+            if (CPLX) mesh_im[cell] = acc_im[li];
         } else {
-            if (acc[li] != 0.0) atomicAdd(&mesh_re[cell], (T)acc[li]);
-            if (CPLX && acc_im[li] != 0.0) atomicAdd(&mesh_im[cell], (T)acc_im[li]);
+            if (acc[li] != (T)0) atomicAdd(&mesh_re[cell], acc[li]);
+            if (CPLX && acc_im[li] != (T)0) atomicAdd(&mesh_im[cell], acc_im[li]);
         }
     }
 }

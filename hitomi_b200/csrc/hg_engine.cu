@@ -41,6 +41,7 @@
 #include <memory>
 #include <set>
 #include <string>
+#include <tuple>
 #include <vector>
 
 using namespace hg;
@@ -125,7 +126,8 @@ struct hg_ctx {
     virtual void pk_box(int ell, double *pk_save, int *n_mode, double *norm) = 0;
     virtual void bk_box_multi(const std::vector<MP> &mps, int ith, double *bk_save, double *sn_save,
                               double *norm) = 0;
-    virtual void zeta_box(int l1, int l2, int L, int ith, double *zeta_save, double *sn_save, double *norm) = 0;
+    virtual void zeta_box_multi(const std::vector<MP> &mps, int ith, double *zeta_save, double *sn_save,
+                                double *norm) = 0;
     virtual void survey_scalars(double *alpha, double *vs, double *nbar, double *wd, double *wr) = 0;
     virtual void pk_survey(int ell, double alpha, double vs, double *pk_save, int *n_mode, double *norm) = 0;
 };
@@ -205,7 +207,24 @@ struct Engine : public hg_ctx {
     std::map<int, std::unique_ptr<DBuf>> jtab_k;  // J_l[i][n2] at the k bins (geometry only)
     std::map<std::array<int, 3>, std::unique_ptr<DBuf>> hist_mp;  // per multipole (catalogue)
     std::set<std::array<int, 3>> hist_ok;
-    DBuf hist_tmp, snmat, d_kv;
+    DBuf hist_tmp, snmat, sn_part, d_kv;
+
+    // 3PCF state: geometry tables (per context) and filtered fields (per catalogue)
+    std::map<int, std::unique_ptr<DBuf>> jtab_r;  // J_l[j][n2] = j_l(dk r_j sqrt(n2))
+    DBuf d_rv, Uz, Gz, zpart, zout;
+    bool Gz_valid = false;
+    std::vector<int> zfine;                  // fine r index of each n2 (field.hpp:1044-1050), -1 if >= 10^4
+    std::vector<std::vector<int>> zcoarse;   // coarse r bins of each fine index (field.hpp:1064-1085)
+    std::vector<double> zcount;              // cells per coarse r bin
+    struct ZKey {
+        int l, m, r0, nr;
+        bool operator<(const ZKey &o) const {
+            return std::tie(l, m, r0, nr) < std::tie(o.l, o.m, o.r0, o.nr);
+        }
+    };
+    std::map<ZKey, std::unique_ptr<DBuf>> zf;  // F_lm[r0 .. r0+nr) on the full grid
+    std::set<ZKey> zf_ok;
+    std::map<std::tuple<int, int, int, int, int>, std::vector<double>> zpairs;  // (la, ma, lb, mb, row)
 
     long long launches = 0;
 
@@ -443,6 +462,9 @@ struct Engine : public hg_ctx {
         famQ_ok.clear();
         hist_ok.clear();
         pairs.clear();
+        Gz_valid = false;
+        zf_ok.clear();
+        zpairs.clear();
     }
 
     // ------------------------------------------------------------------ assignment
@@ -462,6 +484,10 @@ struct Engine : public hg_ctx {
             a.nt[q] = g.n[q] / a.t[q];
         }
         a.factor = 1.0 / (g.volume / double(g.ntot));
+        // FP64 form: the reference's density rho = sum w (1/dV) prod(w_axis).  FP32 form: the
+        // mass per cell (rho dV), which removes the float rounding of 1/dV and dV from every
+        // cell; the FFT input (rho - N/V) dV is then mass - N/Ncells (same quantity).
+        a.acc_factor = (sizeof(T) == 8) ? a.factor : 1.0;
         return a;
     }
 
@@ -513,12 +539,23 @@ struct Engine : public hg_ctx {
         kb("assign_zero_split", 0.0);
         k_zero_split_tiles<T, false><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), ag, out, nullptr);
         ke();
-        size_t smem = sizeof(double) * ag.t[0] * ag.t[1] * ag.t[2];
+        size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2];
         HG_CK(cudaFuncSetAttribute(k_tile_accum<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kb("assign_tile_accum", double(total) * sizeof(PRec<T>) + double(g.ntot) * sizeof(T));
         k_tile_accum<T, false><<<nchunks, 256, smem, st>>>(dp<PRec<T>>(rec), dp<Chunk>(chunks), ag, out, nullptr);
         ke();
         return hm[0];
+    }
+
+    // Stockham shared-memory engine: for loaders that compute their input (8 values per
+    // thread and a separate load loop keep register pressure low)
+    template <int DIR, class LD, class ST>
+    void pass_smem(int L, LD ld, ST stt, long long outer, long long inner, const char *name, double bytes) {
+        PassGeom pg{outer, inner};
+        const C *twp = twiddles(L);
+        kb(name, bytes);
+        HG_CK((launch_fft_pass<T, DIR>(L, ld, stt, pg, twp, st)));
+        ke();
     }
 
     template <int DIR, class LD, class ST>
@@ -545,7 +582,10 @@ struct Engine : public hg_ctx {
         HG_CK(H.ensure(sizeof(C) * (size_t)g.n[0] * g.n[1] * hz));
         const double dV = g.volume / double(g.ntot);
         const double nbar = double(S.n) / g.volume;  // field.hpp:521
-        pass<-1>(g.n[2], LdMeshDelta<T>{dp<T>(mesh), g.n[2], (T)nbar, (T)dV}, StHalf<T>{dp<C>(H), g.n[2], hz},
+        const bool mass_mesh = (sizeof(T) == 4);
+        const T sub = mass_mesh ? (T)(double(S.n) / double(g.ntot)) : (T)nbar;
+        const T scl = mass_mesh ? (T)1 : (T)dV;
+        pass<-1>(g.n[2], LdMeshDelta<T>{dp<T>(mesh), g.n[2], sub, scl}, StHalf<T>{dp<C>(H), g.n[2], hz},
                  (long long)g.n[0] * g.n[1], 1, "fft_density_r2c_z",
                  double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
         pass<-1>(g.n[1], LdArr<T>{dp<C>(H), g.n[1], hz}, StArr<T>{dp<C>(H), g.n[1], hz}, g.n[0], hz, "fft_density_yx");
@@ -727,14 +767,31 @@ struct Engine : public hg_ctx {
         HG_CK(T2.ensure(sizeof(C) * std::max<long long>(t2, 1)));
     }
 
-    // G(x) = IFFT[delta/W]/V on the reduced grid, from the cube |n_a| <= gs_a (pruned passes)
-    void ensure_G() {
-        if (G_valid) return;
-        const ShellSet &S = shells;
+    // Transform-grid geometry of a set of chains: kept modes |n_a| <= s_a (compact side
+    // K = 2s+1), transform grid M, and the cube |n_a| <= gs_a of G's input.
+    struct ChainGeo {
+        int ns;
+        int s[3], K[3], M[3], gs[3], KG[3];
+    };
+    ChainGeo bk_geo() const {
+        ChainGeo q;
+        q.ns = shells.ns;
+        for (int a = 0; a < 3; a++) {
+            q.s[a] = shells.s[a];
+            q.K[a] = shells.K[a];
+            q.M[a] = shells.M[a];
+            q.gs[a] = shells.gs[a];
+            q.KG[a] = shells.KG[a];
+        }
+        return q;
+    }
+
+    // G(x) = IFFT[delta/W]/V on the geometry's grid, from the cube |n_a| <= gs_a (pruned passes)
+    void build_G(const ChainGeo &S, DBuf &Gout) {
         const long long vol = (long long)S.M[0] * S.M[1] * S.M[2];
         const long long kg = (long long)S.KG[0] * S.KG[1] * S.KG[2];
         HG_CK(Gc.ensure(sizeof(C) * kg));
-        HG_CK(Gbuf.ensure(sizeof(C) * vol));
+        HG_CK(Gout.ensure(sizeof(C) * vol));
         ensure_chain_tmp((long long)S.KG[0] * S.KG[1] * S.M[2], (long long)S.KG[0] * S.M[1] * S.M[2]);
         int3 lo = make_int3(-S.gs[0], -S.gs[1], -S.gs[2]);
         int3 cn = make_int3(S.KG[0], S.KG[1], S.KG[2]);
@@ -749,31 +806,22 @@ struct Engine : public hg_ctx {
         pass<+1>(M1, LdRowsCompact<T>{dp<C>(T1), S.KG[1], M1, S.gs[1], M2}, StArr<T>{dp<C>(T2), M1, M2}, S.KG[0], M2,
                  "fft_G_inv", double((long long)S.KG[0] * S.KG[1] * M2 + (long long)S.KG[0] * M1 * M2) * sizeof(C));
         pass<+1>(M0, LdRowsCompact<T>{dp<C>(T2), S.KG[0], M0, S.gs[0], (long long)M1 * M2},
-                 StArr<T>{dp<C>(Gbuf), M0, (long long)M1 * M2}, 1, (long long)M1 * M2, "fft_G_inv",
+                 StArr<T>{dp<C>(Gout), M0, (long long)M1 * M2}, 1, (long long)M1 * M2, "fft_G_inv",
                  double((long long)S.KG[0] * M1 * M2 + vol) * sizeof(C));
+    }
+
+    void ensure_G() {
+        if (G_valid) return;
+        build_G(bk_geo(), Gbuf);
         G_valid = true;
     }
 
-    // Q_b[j] = FFT[IFFT[A_b,j] * G] on the shell cube (hg_chain.cuh)
-    const C *family_Q(const Fam &b) {
-        DBuf &Q = map_buf(famQ, b);
-        if (famQ_ok.count(b)) return dp<C>(Q);
-        const ShellSet &S = shells;
-        ensure_G();
-        const double2 *A = family_A(b);
+    // Q[j] = FFT[IFFT[Ac[j]] * G] on the geometry's compact cube (hg_chain.cuh); Ac is filled.
+    void run_chain(const ChainGeo &S, const DBuf &Gsrc, C *Q) {
         const int ns = S.ns;
         const int Kx = S.K[0], Ky = S.K[1], Kz = S.K[2];
         const int Mx = S.M[0], My = S.M[1], Mz = S.M[2];
-        const long long cv = cube_vol();
-        HG_CK(Ac.ensure(sizeof(C) * cv * ns));
-        HG_CK(Q.ensure(sizeof(C) * cv * ns));
         ensure_chain_tmp((long long)ns * Kx * Ky * Mz, (long long)ns * Kx * My * Mz);
-        HG_CK(cudaMemsetAsync(Ac.p, 0, sizeof(C) * cv * ns, st));
-        kb("scatter_entries", double(n_ent()) * (16.0 + sizeof(C)));
-        k_scatter_cube<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), A,
-                                                               make_int3(Kx, Ky, Kz), make_int3(S.s[0], S.s[1], S.s[2]),
-                                                               dp<C>(Ac));
-        ke();
         const long long o1 = (long long)ns * Kx * Ky;
         const long long o2 = (long long)ns * Kx;
         pass<+1>(Mz, LdCube<T>{dp<C>(Ac), Kz, Mz, S.s[2]}, StArr<T>{dp<C>(T1), Mz, 1}, o1, 1, "chain_z",
@@ -781,25 +829,41 @@ struct Engine : public hg_ctx {
         pass<+1>(My, LdRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, StArr<T>{dp<C>(T2), My, Mz}, o2, Mz, "chain_y",
                  double(o2) * (Ky + My) * Mz * sizeof(C));
         kb("chain_x_fused", double(ns) * 2.0 * Kx * My * Mz * sizeof(C) + double(Mx) * My * Mz * sizeof(C));
+        const C *Gp = dp<C>(Gsrc);
         if (Mx == 256)
-            HG_CK((launch_chain_x_reg_L<T, 256>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
-                                                st)));
+            HG_CK((launch_chain_x_reg_L<T, 256>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
         else if (Mx == 128)
-            HG_CK((launch_chain_x_reg_L<T, 128>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
-                                                st)));
+            HG_CK((launch_chain_x_reg_L<T, 128>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
         else if (Mx == 64)
-            HG_CK((launch_chain_x_reg_L<T, 64>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
-                                               st)));
+            HG_CK((launch_chain_x_reg_L<T, 64>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
         else if (Mx == 32)
-            HG_CK((launch_chain_x_reg_L<T, 32>(dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx),
-                                               st)));
+            HG_CK((launch_chain_x_reg_L<T, 32>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
         else
-            HG_CK(launch_chain_x<T>(Mx, dp<C>(T2), dp<C>(Gbuf), ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st));
+            HG_CK(launch_chain_x<T>(Mx, dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st));
         ke();
         pass<-1>(My, LdArr<T>{dp<C>(T2), My, Mz}, StRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, o2, Mz, "chain_y",
                  double(o2) * (Ky + My) * Mz * sizeof(C));
-        pass<-1>(Mz, LdArr<T>{dp<C>(T1), Mz, 1}, StCube<T>{dp<C>(Q), Kz, Mz, S.s[2]}, o1, 1, "chain_z",
+        pass<-1>(Mz, LdArr<T>{dp<C>(T1), Mz, 1}, StCube<T>{Q, Kz, Mz, S.s[2]}, o1, 1, "chain_z",
                  double(o1) * (Kz + Mz) * sizeof(C));
+    }
+
+    // Q_b[j] for the bispectrum shells
+    const C *family_Q(const Fam &b) {
+        DBuf &Q = map_buf(famQ, b);
+        if (famQ_ok.count(b)) return dp<C>(Q);
+        const ChainGeo S = bk_geo();
+        ensure_G();
+        const double2 *A = family_A(b);
+        const long long cv = cube_vol();
+        HG_CK(Ac.ensure(sizeof(C) * cv * S.ns));
+        HG_CK(Q.ensure(sizeof(C) * cv * S.ns));
+        HG_CK(cudaMemsetAsync(Ac.p, 0, sizeof(C) * cv * S.ns, st));
+        kb("scatter_entries", double(n_ent()) * (16.0 + sizeof(C)));
+        k_scatter_cube<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), A,
+                                                               make_int3(S.K[0], S.K[1], S.K[2]),
+                                                               make_int3(S.s[0], S.s[1], S.s[2]), dp<C>(Ac));
+        ke();
+        run_chain(S, Gbuf, dp<C>(Q));
         famQ_ok.insert(b);
         return dp<C>(Q);
     }
@@ -897,8 +961,8 @@ struct Engine : public hg_ctx {
         const double S = double(slot[0].n);
         LdXiHat<T> ld{half_spec(), g, tabs, cfg.assign, wpow, S, 0.0, delta0 * N0, 0.0, invV};
         long long yz = (long long)g.n[1] * g.n[2];
-        pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
-                 double(g.ntot) * sizeof(C) * 1.5);
+        pass_smem<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
+                      double(g.ntot) * sizeof(C) * 1.5);
         pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
                  "fft_xi_y");
         xi_valid = true;
@@ -906,11 +970,13 @@ struct Engine : public hg_ctx {
 
     template <int L>
     void launch_orbit_L(const HistSpec &hs, int n_orb, double *hist) {
-        size_t smem = sizeof(C) * 8 * (L + 1);
+        size_t smem = OrbitCfg<T, L>::smem();
         HG_CK(cudaFuncSetAttribute(k_xi_orbit_hist<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const C *twp = twiddles(L);
         kb("xi_orbit_hist", double(g.ntot) * sizeof(C));
-        k_xi_orbit_hist<T, L><<<n_orb, L, smem, st>>>(dp<C>(xi), dp<int>(d_orbit_lines), dp<int>(d_orbit_n2xy), n_orb,
-                                                     twiddles(L), hs, n2dim, hist);
+        k_xi_orbit_hist<T, L><<<n_orb, OrbitCfg<T, L>::NT, smem, st>>>(dp<C>(xi), dp<int>(d_orbit_lines),
+                                                                       dp<int>(d_orbit_n2xy), n_orb, twp, hs, n2dim,
+                                                                       hist);
         ke();
     }
     void launch_orbit(int L, const HistSpec &hs, int n_orb, double *hist) {
@@ -1133,8 +1199,15 @@ struct Engine : public hg_ctx {
             const double *J1 = jtab(mp.l1);
             const double *J2 = jtab(mp.l2);
             const double *hq = dp<double>(*hist_mp[{mp.l1, mp.l2, mp.L}]);
-            kb("sn_matrix", double(ns) * ns * n2dim * 24.0);
-            k_sn_matrix<<<dim3(ns, ns), 256, 0, st>>>(J1, J2, hq, n2dim, ns, dp<double2>(snmat));
+            const int nblk = (int)((n2dim + HG_SN_CHUNK - 1) / HG_SN_CHUNK);
+            HG_CK(sn_part.ensure(sizeof(double) * 2 * (size_t)nblk * ns * ns));
+            const size_t smem = sn_partial_smem(ns);
+            HG_CK(cudaFuncSetAttribute(k_sn_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            kb("sn_matrix", double(2 * ns + 2) * n2dim * 8.0);
+            k_sn_partial<<<nblk, 256, smem, st>>>(J1, J2, hq, n2dim, ns, dp<double>(sn_part));
+            ke();
+            kb("sn_matrix", double(nblk) * ns * ns * 16.0);
+            k_sn_reduce<<<grid1(ns * ns, 128), 128, 0, st>>>(dp<double>(sn_part), nblk, ns, dp<double2>(snmat));
             ke();
             std::vector<double> sd(2 * ns * ns);
             HG_CK(cudaMemcpyAsync(sd.data(), snmat.p, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, st));
@@ -1180,8 +1253,289 @@ struct Engine : public hg_ctx {
         end();
     }
 
-    void zeta_box(int, int, int, int, double *, double *, double *) override {
-        throw HgError{"hg_zeta_box is not available in this build"};
+    // ------------------------------------------------------------------ 3PCF (box)
+    void zeta_geometry() {
+        HG_REQUIRE(g.n[0] == g.n[1] && g.n[0] == g.n[2] && cfg.boxsize[0] == cfg.boxsize[1] &&
+                       cfg.boxsize[0] == cfg.boxsize[2],
+                   "the 3PCF needs a cubic box and mesh (j_l(|k| r) is tabulated on integer |n|^2)");
+        build_orbits();
+        if (!zfine.empty()) return;
+        const int n = g.n[0], h = n / 2;
+        // cells per n2 = |w|^2 (w the wrapped cell offset, field.hpp:1040-1043)
+        std::vector<long long> c1(h * h + 1, 0);
+        for (int i = 0; i < n; i++) {
+            int w = wrap_index(i, n);
+            c1[w * w]++;
+        }
+        std::vector<int> sq;
+        for (int v = 0; v <= h; v++) sq.push_back(v * v);
+        std::vector<double> cnt(n2dim, 0.0);
+        for (int a : sq)
+            for (int b : sq)
+                for (int c : sq) cnt[a + b + c] += double(c1[a]) * double(c1[b]) * double(c1[c]);
+        // rindex = int(|r| / 0.5 + 0.5), kept if < 10000 (field.hpp:1030-1053).  |r|^2 = n2 dr^2 is the
+        // reference's sum of (i dr)^2 exactly when those squares are exact (dyadic dr, e.g. an integer
+        // box over a power-of-two mesh).
+        const double dr = g.dr[0];
+        zfine.assign(n2dim, -1);
+        for (long long q = 0; q < n2dim; q++) {
+            double rmag = std::sqrt(double(q) * (dr * dr));
+            int ri = (int)(rmag / 0.5 + 0.5);
+            if (ri < 10000) zfine[q] = ri;
+        }
+        // coarse bins from neighbouring half widths (field.hpp:1058-1085)
+        const int nr = cfg.n_rbin;
+        std::vector<double> drb(nr - 1);
+        for (int j = 0; j < nr - 1; j++) drb[j] = rbin[j + 1] - rbin[j];
+        zcoarse.assign(10000, {});
+        for (int j = 0; j < nr; j++) {
+            double lower = (j == 0) ? ((rbin[j] > drb[j] * 0.5) ? (rbin[j] - drb[j] * 0.5) : 0.0)
+                                    : rbin[j] - drb[j - 1] * 0.5;
+            double upper = (j == nr - 1) ? (rbin[j] + drb[j - 1] * 0.5) : (rbin[j] + drb[j] * 0.5);
+            for (int i = 0; i < 10000; i++) {
+                double rt = double(i) * 0.5;
+                if (rt > lower && rt <= upper) zcoarse[i].push_back(j);
+            }
+        }
+        zcount.assign(nr, 0.0);
+        for (long long q = 0; q < n2dim; q++)
+            if (zfine[q] >= 0)
+                for (int j : zcoarse[zfine[q]]) zcount[j] += cnt[q];
+    }
+
+    // J_l[j][n2] = j_l(r_j dk sqrt(n2)) at the r bins (geometry only: cached for the context)
+    const double *jtab_rbins(int l) {
+        auto it = jtab_r.find(l);
+        if (it != jtab_r.end()) return dp<double>(*it->second);
+        const BesselSpline &s = spline(l);
+        auto &sp = d_splines[l];
+        HG_CK(d_rv.ensure(sizeof(double) * rbin.size()));
+        HG_CK(cudaMemcpyAsync(d_rv.p, rbin.data(), sizeof(double) * rbin.size(), cudaMemcpyHostToDevice, st));
+        auto J = std::make_unique<DBuf>();
+        HG_CK(J->ensure(sizeof(double) * rbin.size() * n2dim));
+        long long tot = (long long)rbin.size() * n2dim;
+        kb("bessel_table", double(tot) * 8.0);
+        k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n, s.xmin,
+                                                        s.dx, dp<double>(d_rv), (int)rbin.size(), g.dk[0], n2dim,
+                                                        dp<double>(*J));
+        ke();
+        HG_CK(cudaStreamSynchronize(st));
+        const double *p = dp<double>(*J);
+        jtab_r[l] = std::move(J);
+        return p;
+    }
+
+    // U = Yhat_lm delta / W / V on the full grid
+    void zeta_U(int l, int m) {
+        HG_CK(Uz.ensure(sizeof(C) * g.ntot));
+        unsigned blocks = (unsigned)std::min<long long>(grid1(g.ntot, 256), 148 * 16);
+        kb("zeta_U", double(g.ntot) * (sizeof(C) * 1.5));
+        k_zeta_U<T><<<blocks, 256, 0, st>>>(half_spec(), g, tabs, wpow, l, m, delta0, dp<C>(Uz));
+        ke();
+    }
+
+    // inverse transform of nr fields on the full grid; the x pass reads through `ld`
+    template <class LD>
+    void full_inverse(LD ld, C *out, int nr, const char *name) {
+        const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+        const long long yz = (long long)n1 * n2;
+        const double fb = double(g.ntot) * sizeof(C) * nr;
+        pass<+1>(n0, ld, StArr<T>{out, n0, yz}, nr, yz, name, fb * 1.5);
+        pass<+1>(n1, LdArr<T>{out, n1, n2}, StArr<T>{out, n1, n2}, (long long)nr * n0, n2, name, fb * 2.0);
+        pass<+1>(n2, LdArr<T>{out, n2, 1}, StArr<T>{out, n2, 1}, (long long)nr * n0 * n1, 1, name, fb * 2.0);
+    }
+
+    // G(x) = IFFT[delta / W] / V on the full grid (field.hpp:326-344 after the window correction)
+    void ensure_Gz() {
+        if (Gz_valid) return;
+        zeta_U(0, 0);
+        HG_CK(Gz.ensure(sizeof(C) * g.ntot));
+        full_inverse(LdArr<T>{dp<C>(Uz), g.n[0], (long long)g.n[1] * g.n[2]}, dp<C>(Gz), 1, "zeta_G");
+        Gz_valid = true;
+    }
+
+    size_t zf_bytes() const {
+        size_t b = 0;
+        for (const auto &kv : zf) b += kv.second->n;
+        return b;
+    }
+
+    // F_lm[r] = IFFT[j_l(|k| r) U_lm] for r in [r0, r0+nr) (field.hpp:403-445), cached per catalogue
+    const C *zeta_fields(const Fam &f, int r0, int nr, const ZKey *keep) {
+        ZKey key{f.l, f.m, r0, nr};
+        auto it = zf.find(key);
+        if (it != zf.end() && zf_ok.count(key)) return dp<C>(*it->second);
+        const size_t need = sizeof(C) * (size_t)g.ntot * nr;
+        size_t fr = 0, tot = 0;
+        HG_CK(cudaMemGetInfo(&fr, &tot));
+        if (need + (size_t(1) << 30) > fr) {  // release cached fields other than `keep`
+            for (auto i = zf.begin(); i != zf.end();) {
+                if (keep && !(i->first < *keep) && !(*keep < i->first)) {
+                    ++i;
+                    continue;
+                }
+                zf_ok.erase(i->first);
+                i = zf.erase(i);
+            }
+        }
+        auto &p = zf[key];
+        if (!p) p = std::make_unique<DBuf>();
+        HG_CK(p->ensure(need));
+        zeta_U(f.l, f.m);
+        const double *J = jtab_rbins(f.l) + (size_t)r0 * n2dim;
+        LdZetaField<T> ld{dp<C>(Uz), J, n2dim, g.n[0], g.n[1], g.n[2]};
+        full_inverse(ld, dp<C>(*p), nr, "zeta_fields");
+        zf_ok.insert(key);
+        return dp<C>(*p);
+    }
+
+    // P[i1][i2] = sum_x Fa[i1](x) Fb[i2](x) G(x), complex [na][nb]
+    std::vector<double> zeta_pairsum(const C *Fa, int na, const C *Fb, int nb) {
+        const int nblk = 2 * 148;
+        const size_t smem = zeta_pairsum_smem(na, nb);
+        HG_CK(zpart.ensure(sizeof(double) * 2 * (size_t)nblk * na * nb));
+        HG_CK(zout.ensure(sizeof(double2) * (size_t)na * nb));
+        HG_CK(cudaFuncSetAttribute(k_zeta_pairsum<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kb("zeta_pairsum", double(g.ntot) * sizeof(C) * double(na + (Fa == Fb ? 0 : nb) + 1));
+        k_zeta_pairsum<T><<<nblk, HG_ZR_THREADS, smem, st>>>(Fa, na, Fb, nb, dp<C>(Gz), g.ntot, dp<double>(zpart));
+        ke();
+        kb("zeta_pairsum", double(nblk) * na * nb * 16.0);
+        k_sum_parts<<<grid1((long long)na * nb, 128), 128, 0, st>>>(dp<double>(zpart), nblk, na * nb,
+                                                                      dp<double2>(zout));
+        ke();
+        std::vector<double> h(2 * (size_t)na * nb);
+        HG_CK(cudaMemcpyAsync(h.data(), zout.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        return h;
+    }
+
+    // sum_x F_a[i1] F_b[i2] G for the requested rows i1 (all, or `row`) and every i2:
+    // [rows][ns] complex.  All rows come from the unordered pair (transposed when needed).
+    std::vector<double> zeta_pair(const Fam &a, const Fam &b, int row) {
+        const int ns = cfg.n_rbin;
+        const bool all = (row < 0);
+        Fam p = a, q = b;
+        bool swap = false;
+        if (all && b < a) {
+            std::swap(p, q);
+            swap = true;
+        }
+        auto key = std::make_tuple(p.l, p.m, q.l, q.m, row);
+        auto it = zpairs.find(key);
+        if (it == zpairs.end()) {
+            const int rows = all ? ns : 1;
+            std::vector<double> out(2 * (size_t)rows * ns, 0.0);
+            // radius tiles that fit next to the cached fields (one tile when memory allows)
+            size_t fr = 0, tot = 0;
+            HG_CK(cudaMemGetInfo(&fr, &tot));
+            const double fb = double(sizeof(C)) * double(g.ntot);
+            double avail = double(fr) + double(zf_bytes()) - double(size_t(2) << 30);
+            int tile = (int)std::min<double>(64.0, std::floor(avail / (2.0 * fb)));
+            HG_REQUIRE(tile >= 1, "not enough device memory for two 3PCF fields");
+            tile = std::min(tile, ns);
+            const int pr0 = all ? 0 : row, prn = all ? ns : 1;
+            for (int a0 = pr0; a0 < pr0 + prn; a0 += tile) {
+                const int an = std::min(tile, pr0 + prn - a0);
+                for (int b0 = 0; b0 < ns; b0 += tile) {
+                    const int bn = std::min(tile, ns - b0);
+                    ZKey ka{p.l, p.m, a0, an};
+                    const C *Fa = zeta_fields(p, a0, an, nullptr);
+                    const C *Fb = (p.l == q.l && p.m == q.m && a0 == b0 && an == bn) ? Fa
+                                                                                       : zeta_fields(q, b0, bn, &ka);
+                    std::vector<double> t = zeta_pairsum(Fa, an, Fb, bn);
+                    for (int i1 = 0; i1 < an; i1++)
+                        for (int i2 = 0; i2 < bn; i2++) {
+                            size_t o = (size_t)(a0 - pr0 + i1) * ns + (b0 + i2);
+                            out[2 * o] = t[2 * ((size_t)i1 * bn + i2)];
+                            out[2 * o + 1] = t[2 * ((size_t)i1 * bn + i2) + 1];
+                        }
+                }
+            }
+            it = zpairs.emplace(key, std::move(out)).first;
+        }
+        if (!swap) return it->second;
+        const auto &P = it->second;
+        std::vector<double> r(2 * (size_t)ns * ns);
+        for (int i = 0; i < ns; i++)
+            for (int j = 0; j < ns; j++) {
+                r[2 * ((size_t)i * ns + j)] = P[2 * ((size_t)j * ns + i)];
+                r[2 * ((size_t)i * ns + j) + 1] = P[2 * ((size_t)j * ns + i) + 1];
+            }
+        return r;
+    }
+
+    // bispec.hpp:1205-1424 for all r1 rows (ith = -1) or one, for several multipoles.
+    void zeta_box_multi(const std::vector<MP> &mps, int ith, double *zeta_save, double *sn_save,
+                        double *norm) override {
+        HG_REQUIRE(!mps.empty(), "no multipoles requested");
+        for (const auto &mp : mps) {
+            HG_REQUIRE(mp.l1 >= 0 && mp.l2 >= 0 && mp.L >= 0, "ell1, ell2, ELL must be >= 0");
+            HG_REQUIRE(std::fabs(wigner3j(mp.l1, mp.l2, mp.L, 0, 0, 0)) >= 1.0e-10,
+                       "This multipole combination is not allowed: wigner_3j(ell1, ell2, ELL, 0,0,0) == 0");
+        }
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_rbin, "ith_rbin out of range");
+        begin();
+        zeta_geometry();
+        box_density();
+        ensure_Gz();
+        const int ns = cfg.n_rbin;
+        const double Np = double(slot[0].n);
+        const double dV = g.volume / double(g.ntot);
+        const int r0 = (ith < 0) ? 0 : ith, rows = (ith < 0) ? ns : 1;
+        // zeta_raw = sum_combos w i^(l1+l2) dV sum_x F1 F2 G  (bispec.hpp:1354-1378)
+        std::vector<std::vector<double>> Z(mps.size(), std::vector<double>(2 * (size_t)rows * ns, 0.0));
+        for (size_t q = 0; q < mps.size(); q++) {
+            const MP &mp = mps[q];
+            const int p4 = (mp.l1 + mp.l2) % 4;
+            for (const auto &c : combos_of(mp)) {
+                std::vector<double> t = zeta_pair(Fam{mp.l1, c.m1}, Fam{mp.l2, c.m2}, ith);
+                for (size_t e = 0; e < (size_t)rows * ns; e++) {
+                    double re = c.w * (dV * t[2 * e]), im = c.w * (dV * t[2 * e + 1]);
+                    double rr = p4 == 0 ? re : p4 == 1 ? -im : p4 == 2 ? -re : im;
+                    double ii = p4 == 0 ? im : p4 == 1 ? re : p4 == 2 ? -im : -re;
+                    Z[q][2 * e] += rr;
+                    Z[q][2 * e + 1] += ii;
+                }
+            }
+        }
+        // shot noise on the diagonal (bispec.hpp:1236-1298, field.hpp:979-1113)
+        ensure_histograms(mps);
+        std::fill(sn_save, sn_save + 2 * mps.size() * (size_t)rows * ns, 0.0);
+        std::vector<double> hist(2 * n2dim);
+        for (size_t q = 0; q < mps.size(); q++) {
+            const MP &mp = mps[q];
+            HG_CK(cudaMemcpyAsync(hist.data(), dp<double>(*hist_mp[{mp.l1, mp.l2, mp.L}]),
+                                  sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, st));
+            HG_CK(cudaStreamSynchronize(st));
+            std::vector<double> xr(ns, 0.0), xim(ns, 0.0);
+            for (long long n2 = 0; n2 < n2dim; n2++) {
+                if (zfine[n2] < 0) continue;
+                for (int j : zcoarse[zfine[n2]]) {
+                    xr[j] += hist[2 * n2];
+                    xim[j] += hist[2 * n2 + 1];
+                }
+            }
+            const double sg = ((mp.l1 + mp.l2) % 2 == 0) ? 1.0 : -1.0;
+            for (int i = r0; i < r0 + rows; i++) {
+                double s = zcount[i] != 0.0 ? sg / zcount[i] / zcount[i] / dV : 0.0;
+                size_t o = (size_t)q * rows * ns + (size_t)(i - r0) * ns + i;
+                // rows other than the diagonal carry no shot noise (bispec.hpp:1279-1285)
+                sn_save[2 * o] = xr[i] * s;
+                sn_save[2 * o + 1] = xim[i] * s;
+            }
+        }
+        for (size_t q = 0; q < mps.size(); q++)
+            for (size_t e = 0; e < (size_t)rows * ns; e++) {
+                size_t o = q * (size_t)rows * ns + e;
+                zeta_save[2 * o] = Z[q][2 * e];
+                zeta_save[2 * o + 1] = Z[q][2 * e + 1];
+            }
+        if (norm) {
+            double nv = g.volume / Np / Np;
+            nv *= (g.volume / Np);
+            *norm = nv;
+        }
+        end();
     }
     void survey_scalars(double *, double *, double *, double *, double *) override {
         throw HgError{"hg_survey_scalars is not available in this build"};
@@ -1294,7 +1648,15 @@ int hg_bk_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin
 int hg_zeta_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double *zeta_save, double *sn_save,
                 double *norm) {
     if (!zeta_save || !sn_save) return -1;
-    HG_GUARD(ctx, ctx->zeta_box(ell1, ell2, ELL, ith_rbin, zeta_save, sn_save, norm));
+    HG_GUARD(ctx, ctx->zeta_box_multi({MP{ell1, ell2, ELL}}, ith_rbin, zeta_save, sn_save, norm));
+}
+
+int hg_zeta_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double *zeta_save,
+                      double *sn_save, double *norm) {
+    if (!zeta_save || !sn_save || !ells || n_multipoles <= 0) return -1;
+    std::vector<MP> mps;
+    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
+    HG_GUARD(ctx, ctx->zeta_box_multi(mps, ith_rbin, zeta_save, sn_save, norm));
 }
 
 int hg_survey_scalars(hg_ctx *ctx, double *alpha, double *vsurvey, double *nbar, double *wsum_data,

@@ -1,4 +1,4 @@
-// hg_fft2.cuh -- register-resident two-level line FFTs for lengths L = R1 * R2 <= 256.
+// hg_fft2.cuh -- register-resident two-level line FFTs for lengths L = R1 * R2 <= 1024.
 //
 // A line of L points is handled by R2 threads that each hold R1 values (R1 = R2 or 2 R2):
 //   step A  thread t loads x[R2 n1 + t], n1 < R1, does a DFT of size R1 in registers and
@@ -163,6 +163,8 @@ template <> struct Split<32> { static constexpr int R1 = 8, R2 = 4; };
 template <> struct Split<64> { static constexpr int R1 = 8, R2 = 8; };
 template <> struct Split<128> { static constexpr int R1 = 16, R2 = 8; };
 template <> struct Split<256> { static constexpr int R1 = 16, R2 = 16; };
+template <> struct Split<512> { static constexpr int R1 = 32, R2 = 16; };
+template <> struct Split<1024> { static constexpr int R1 = 32, R2 = 32; };
 
 // Shared-memory exchange buffers for B lines.  COLS: S[(k1 R2 + t) B + b].
 // ROWS: S[b LP + k1 (R2 + 1) + t] with LP = R1 (R2 + 1).
@@ -219,8 +221,10 @@ __device__ __forceinline__ int reg_of_n1(int n1) {
 template <typename T, int L, bool COLS>
 struct Fft2Cfg {
     static constexpr int R2 = Split<L>::R2;
-    // lines per CTA: columns (strided axes) or whole lines (contiguous axis)
-    static constexpr int B = COLS ? ((sizeof(T) == 4) ? 32 : 16) : (256 / R2 > 64 ? 64 : 256 / R2);
+    // lines per CTA: columns (strided axes) or whole lines (contiguous axis); lengths
+    // >= 512 hold 32 values per thread, so their CTAs are capped at 256 threads
+    static constexpr int B = COLS ? ((L >= 512) ? 256 / R2 : ((sizeof(T) == 4) ? 32 : 16))
+                                  : (256 / R2 > 64 ? 64 : 256 / R2);
     static constexpr int NT = R2 * B;
 };
 
@@ -301,23 +305,30 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
         case 64: return launch_fft2_L<T, 64, DIR>(ld, st, g, tw, stream);
         case 128: return launch_fft2_L<T, 128, DIR>(ld, st, g, tw, stream);
         case 256: return launch_fft2_L<T, 256, DIR>(ld, st, g, tw, stream);
+        case 512: return launch_fft2_L<T, 512, DIR>(ld, st, g, tw, stream);
+        case 1024: return launch_fft2_L<T, 1024, DIR>(ld, st, g, tw, stream);
         default: return launch_fft_pass<T, DIR>(L, ld, st, g, tw, stream);
     }
 }
 
-// The chain kernel keeps G and two register tiles live: 16 columns per CTA (256 threads).
+// The chain kernel: 16 columns per CTA (256 threads); the CTA's G tile (L x 16) is staged
+// once in shared memory next to the exchange buffer and reused by every shell.
 template <typename T, int L>
 struct ChainCfg {
     static constexpr int R2 = Split<L>::R2;
     static constexpr int B = 16;
     static constexpr int NT = R2 * B;
+    static constexpr size_t smem() {
+        return sizeof(cplx<T>) * ((size_t)XchgLayout<L, true, B>::ELEMS + (size_t)L * B);
+    }
 };
 
 // Fused chain x-pass with the register FFT: T2 layout [j][cx][y][z] (rows of `plane`
-// columns), G [x][y][z].  Thread (t, b) keeps its R1 values of G in registers for all
-// shells j; per shell: load the K kept rows, inverse FFT, * G, forward FFT, store K rows.
+// columns), G [x][y][z].  Per shell j: load the K kept rows, inverse FFT, * G, forward FFT,
+// store the K kept rows.  The product happens in the positions a thread holds after the
+// inverse transform, which are its step-A positions of the forward transform.
 template <typename T, int L>
-__global__ void __launch_bounds__(ChainCfg<T, L>::NT)
+__global__ void __launch_bounds__(ChainCfg<T, L>::NT, (sizeof(T) == 4) ? 2 : 1)
     k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
                   const cplx<T> *__restrict__ tw) {
     using CF = ChainCfg<T, L>;
@@ -325,20 +336,16 @@ __global__ void __launch_bounds__(ChainCfg<T, L>::NT)
     constexpr int R1 = X::R1, R2 = X::R2, B = CF::B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *Gs = S + X::ELEMS;  // [x][b]
     const int t = threadIdx.x / B, b = threadIdx.x % B;
     const long long i = (long long)blockIdx.x * B + b;
     const bool ok = i < plane;
-    // G at the positions this thread holds after an inverse transform (register order);
-    // kept in registers across shells in FP32, re-read (L2-resident) per shell in FP64
-    constexpr bool kCacheG = (sizeof(T) == 4);
-    cplx<T> gr[kCacheG ? R1 : 1];
-    if (kCacheG) {
-#pragma unroll
-        for (int r = 0; r < (kCacheG ? R1 : 1); r++) {
-            const int x = pos_of_reg<L>(t, r);
-            gr[r] = ok ? G[(long long)x * plane + i] : mk<T>(0, 0);
-        }
+    for (int e = threadIdx.x; e < L * B; e += CF::NT) {
+        const int x = e / B, bb = e % B;
+        const long long ii = (long long)blockIdx.x * B + bb;
+        Gs[e] = (ii < plane) ? G[(long long)x * plane + ii] : mk<T>(0, 0);
     }
+    // (the first exchange inside line_fft2 synchronises before Gs is read)
     for (int j = 0; j < ns; j++) {
         cplx<T> *tj = t2 + (long long)j * K * plane;
         cplx<T> v[R1];
@@ -350,23 +357,26 @@ __global__ void __launch_bounds__(ChainCfg<T, L>::NT)
             v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)c * plane + i] : mk<T>(0, 0);
         }
         line_fft2<T, L, +1, true, B>(v, S, t, b, tw);
-        // product with G, then regroup to step-A order of the forward transform
-        cplx<T> u[R1];
+        if constexpr (R1 == R2) {
 #pragma unroll
-        for (int n1 = 0; n1 < R1; n1++) {
-            const int r = reg_of_n1<L>(n1);
-            cplx<T> gv;
-            if (kCacheG) gv = gr[kCacheG ? r : 0];
-            else gv = ok ? G[(long long)pos_of_reg<L>(t, r) * plane + i] : mk<T>(0, 0);
-            u[n1] = v[r] * gv;
+            for (int r = 0; r < R1; r++) v[r] = v[r] * Gs[pos_of_reg<L>(t, r) * B + b];
+        } else {
+            cplx<T> u[R1];
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++) {
+                const int r = reg_of_n1<L>(n1);
+                u[n1] = v[r] * Gs[pos_of_reg<L>(t, r) * B + b];
+            }
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++) v[n1] = u[n1];
         }
-        line_fft2<T, L, -1, true, B>(u, S, t, b, tw);
+        line_fft2<T, L, -1, true, B>(v, S, t, b, tw);
         if (ok) {
 #pragma unroll
             for (int r = 0; r < R1; r++) {
                 const int p = pos_of_reg<L>(t, r);
                 const int n = (p < L / 2) ? p : p - L;
-                if (n >= -s && n <= s) tj[(long long)(n + s) * plane + i] = u[r];
+                if (n >= -s && n <= s) tj[(long long)(n + s) * plane + i] = v[r];
             }
         }
     }
@@ -376,7 +386,7 @@ template <typename T, int L>
 inline cudaError_t launch_chain_x_reg_L(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
                                         const cplx<T> *tw, cudaStream_t st) {
     using CF = ChainCfg<T, L>;
-    size_t smem = (size_t)XchgLayout<L, true, CF::B>::ELEMS * sizeof(cplx<T>);
+    size_t smem = CF::smem();
     cudaFuncSetAttribute(k_chain_x_reg<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     unsigned tiles = (unsigned)((plane + CF::B - 1) / CF::B);
     k_chain_x_reg<T, L><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);

@@ -14,6 +14,7 @@
 #include "hg_common.cuh"
 #include "hg_fft.cuh"
 #include "hg_bin.cuh"
+#include "hg_fft2.cuh"
 
 namespace hg {
 
@@ -183,37 +184,54 @@ struct HistSpec {
 // Last inverse pass (along z) over one symmetry orbit of (x, y) lines, fused with
 //   T_h(n^2) += sum over the orbit and z <-> -z of xi(x) f_h(theta)
 // where f_h = sum_terms w Yhat_l1m1 Yhat_l2m2 depends only on the polar angle (m1+m2 = 0),
-// and n^2 = wx^2 + wy^2 + wz^2 in cell units (cubic cells).
+// and n^2 = wx^2 + wy^2 + wz^2 in cell units (cubic cells).  The 8 lines are transformed
+// with the register two-level FFT (R2 threads per line), then laid out in shared memory
+// for the histogram.
 template <typename T, int L>
-__global__ void __launch_bounds__(L) k_xi_orbit_hist(const cplx<T> *xi, const int *orbit_lines, const int *orbit_n2xy,
-                                                    int n_orbits, const cplx<T> *tw, HistSpec hs, long long n2dim,
-                                                    double *hist) {
-    constexpr int B = 8;
-    constexpr int LP = L + 1;
+struct OrbitCfg {
+    static constexpr int B = 8;
+    static constexpr int NT = Split<L>::R2 * B;
+    static constexpr int LP = L + 1;
+    static constexpr size_t smem() {
+        return sizeof(cplx<T>) * ((size_t)B * LP > (size_t)XchgLayout<L, false, B>::ELEMS
+                                      ? (size_t)B * LP
+                                      : (size_t)XchgLayout<L, false, B>::ELEMS);
+    }
+};
+
+template <typename T, int L>
+__global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
+    k_xi_orbit_hist(const cplx<T> *xi, const int *orbit_lines, const int *orbit_n2xy, int n_orbits,
+                    const cplx<T> *tw, HistSpec hs, long long n2dim, double *hist) {
+    using OC = OrbitCfg<T, L>;
+    constexpr int B = OC::B, LP = OC::LP, NT = OC::NT;
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *s = reinterpret_cast<cplx<T> *>(smem_raw);
     const int orb = blockIdx.x;
     const int *lines = orbit_lines + 8 * orb;
-    for (int e = threadIdx.x; e < B * L; e += L) {
-        int b = e / L, z = e - b * L;
-        int line = lines[b];
-        s[b * LP + z] = (line >= 0) ? xi[(long long)line * L + z] : mk<T>(0, 0);
-    }
+    const int b = threadIdx.x / R2, t = threadIdx.x % R2;
+    const int line = lines[b];
+    cplx<T> v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; n1++) v[n1] = (line >= 0) ? xi[(long long)line * L + R2 * n1 + t] : mk<T>(0, 0);
+    line_fft2<T, L, +1, false, B>(v, s, t, b, tw);
+#pragma unroll
+    for (int r = 0; r < R1; r++) s[b * LP + pos_of_reg<L>(t, r)] = v[r];
     __syncthreads();
-    smem_fft<T, L, +1, L>(s, LP, B, tw);
     const int n2xy = orbit_n2xy[orb];
     const double rho = sqrt((double)n2xy);
-    for (int iz = threadIdx.x; iz <= L / 2; iz += L) {
+    for (int iz = threadIdx.x; iz <= L / 2; iz += NT) {
         int iz2 = (L - iz) % L;
         double er = 0, ei = 0, orr = 0, oi = 0;
-        for (int b = 0; b < B; b++) {
-            if (lines[b] < 0) continue;
-            cplx<T> a = s[b * LP + iz];
+        for (int bb = 0; bb < B; bb++) {
+            if (lines[bb] < 0) continue;
+            cplx<T> a = s[bb * LP + iz];
             if (iz2 == iz) {
                 er += (double)a.x;
                 ei += (double)a.y;
             } else {
-                cplx<T> c = s[b * LP + iz2];
+                cplx<T> c = s[bb * LP + iz2];
                 er += (double)a.x + (double)c.x;
                 ei += (double)a.y + (double)c.y;
                 orr += (double)a.x - (double)c.x;
@@ -224,16 +242,16 @@ __global__ void __launch_bounds__(L) k_xi_orbit_hist(const cplx<T> *xi, const in
         long long n2 = (long long)n2xy + (long long)wz * wz;
         for (int h = 0; h < hs.nh; h++) {
             zd f = mk<double>(0.0, 0.0);
-            for (int t = 0; t < hs.nterm[h]; t++) {
-                const YTerm &yt = hs.term[h][t];
+            for (int q = 0; q < hs.nterm[h]; q++) {
+                const YTerm &yt = hs.term[h][q];
                 zd y1 = ylm_reduced(yt.l1, yt.m1, rho, 0.0, (double)wz);
                 zd y2 = ylm_reduced(yt.l2, yt.m2, rho, 0.0, (double)wz);
                 f = f + (y1 * y2) * yt.w;
             }
             zd src = (hs.parity[h] > 0) ? mk<double>(er, ei) : mk<double>(orr, oi);
-            zd v = f * src;
-            if (v.x != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2)], v.x);
-            if (v.y != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2) + 1], v.y);
+            zd val = f * src;
+            if (val.x != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2)], val.x);
+            if (val.y != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2) + 1], val.y);
         }
     }
 }
@@ -265,40 +283,211 @@ __global__ void k_bessel_table(const double *sy, const double *sc, int sn, doubl
     J[q] = (x <= xmax) ? spline_eval(sy, sc, sn, xmin, dx, x) : 0.0;
 }
 
-// out[i1][i2] = sum_n2 J1[i1][n2] J2[i2][n2] hist[n2]; one block per (i1, i2).
-__global__ void k_sn_matrix(const double *J1, const double *J2, const double *hist, long long n2dim, int nk,
-                            double2 *out) {
-    int i1 = blockIdx.x, i2 = blockIdx.y;
-    __shared__ double red[2][32];
-    double sr = 0.0, si = 0.0;
-    const double *a = J1 + (long long)i1 * n2dim, *b = J2 + (long long)i2 * n2dim;
-    for (long long n2 = threadIdx.x; n2 < n2dim; n2 += blockDim.x) {
-        double hr = hist[2 * n2], hi = hist[2 * n2 + 1];
-        if (hr == 0.0 && hi == 0.0) continue;
-        double jj = a[n2] * b[n2];
-        sr += jj * hr;
-        si += jj * hi;
+// out[i1][i2] = sum_n2 J1[i1][n2] J2[i2][n2] hist[n2], as a skinny product J1 diag(h) J2^T:
+// each block stages a chunk of n2 for all rows of J1, J2 and h in shared memory and writes
+// its nk x nk partial sums; k_sn_reduce adds the partials in a fixed order (deterministic).
+#define HG_SN_CHUNK 128
+__global__ void k_sn_partial(const double *J1, const double *J2, const double *hist, long long n2dim, int nk,
+                             double *part) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int CP = HG_SN_CHUNK + 1;  // padded row: rows of J land in different banks
+    double *j1 = reinterpret_cast<double *>(smem_raw);
+    double *j2 = j1 + (size_t)nk * CP;
+    double *hr = j2 + (size_t)nk * CP;
+    double *hi = hr + CP;
+    const long long n0 = (long long)blockIdx.x * HG_SN_CHUNK;
+    const int len = (int)min((long long)HG_SN_CHUNK, n2dim - n0);
+    for (int e = threadIdx.x; e < nk * HG_SN_CHUNK; e += blockDim.x) {
+        int r = e / HG_SN_CHUNK, n = e % HG_SN_CHUNK;
+        bool ok = n < len;
+        j1[r * CP + n] = ok ? J1[(long long)r * n2dim + n0 + n] : 0.0;
+        j2[r * CP + n] = ok ? J2[(long long)r * n2dim + n0 + n] : 0.0;
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        sr += __shfl_down_sync(0xffffffffu, sr, o);
-        si += __shfl_down_sync(0xffffffffu, si, o);
-    }
-    int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    if (ln == 0) {
-        red[0][w] = sr;
-        red[1][w] = si;
+    for (int n = threadIdx.x; n < HG_SN_CHUNK; n += blockDim.x) {
+        bool ok = n < len;
+        hr[n] = ok ? hist[2 * (n0 + n)] : 0.0;
+        hi[n] = ok ? hist[2 * (n0 + n) + 1] : 0.0;
     }
     __syncthreads();
-    if (w == 0) {
-        int nw = blockDim.x >> 5;
-        sr = (ln < nw) ? red[0][ln] : 0.0;
-        si = (ln < nw) ? red[1][ln] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) {
-            sr += __shfl_down_sync(0xffffffffu, sr, o);
-            si += __shfl_down_sync(0xffffffffu, si, o);
+    for (int o = threadIdx.x; o < nk * nk; o += blockDim.x) {
+        const int i1 = o / nk, i2 = o % nk;
+        const double *a = j1 + i1 * CP, *c = j2 + i2 * CP;
+        double sr = 0.0, si = 0.0;
+        for (int n = 0; n < len; n++) {
+            double jj = a[n] * c[n];
+            sr += jj * hr[n];
+            si += jj * hi[n];
         }
-        if (ln == 0) out[(long long)i1 * nk + i2] = make_double2(sr, si);
+        part[2 * ((long long)blockIdx.x * nk * nk + o)] = sr;
+        part[2 * ((long long)blockIdx.x * nk * nk + o) + 1] = si;
     }
+}
+
+__global__ void k_sn_reduce(const double *part, int nblk, int nk, double2 *out) {
+    int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nk * nk) return;
+    double sr = 0.0, si = 0.0;
+    for (int b = 0; b < nblk; b++) {
+        sr += part[2 * ((long long)b * nk * nk + o)];
+        si += part[2 * ((long long)b * nk * nk + o) + 1];
+    }
+    out[o] = make_double2(sr, si);
+}
+
+inline size_t sn_partial_smem(int nk) { return sizeof(double) * ((size_t)2 * nk * (HG_SN_CHUNK + 1) + 2 * (HG_SN_CHUNK + 1)); }
+
+// ---------------------------------------------------------------- 3PCF (zeta)
+// Per-mode factor of the 3PCF filtered fields (field.hpp:403-445) without the Bessel weight:
+//   U(k) = Yhat_lm(k) delta(k) / W(k) / V        over the full grid, delta(0) = k0_re.
+template <typename T>
+__global__ void k_zeta_U(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int l, int m, double k0_re, cplx<T> *U) {
+    const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int iz = (int)(idx % g.n[2]);
+        int iy = (int)((idx / g.n[2]) % g.n[1]);
+        int ix = (int)(idx / ((long long)g.n[2] * g.n[1]));
+        zd d = (ix == 0 && iy == 0 && iz == 0) ? mk<double>(k0_re, 0.0) : f.at(ix, iy, iz);
+        double wf = window_tab(tabs, ix, iy, iz, wpow);
+        zd y = ylm_reduced(l, m, kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
+                           kcomp(wrap_index(iz, g.n[2]), g.dk[2]));
+        zd v = y * mk<double>(d.x / wf, d.y / wf);
+        U[idx] = mk<T>((T)(v.x / g.volume), (T)(v.y / g.volume));
+    }
+}
+
+// Loader of the first inverse pass (along x) of the fields F_r = IFFT[j_l(|k| r) U(k)]
+// for a block of radii: o = radius within the block, l = ix, i = iy * nz + iz.
+// J[r][n2] = j_l(dk r sqrt(n2)) with n2 = |n|^2 of the wrapped mode (cubic box).
+template <typename T>
+struct LdZetaField {
+    const cplx<T> *U;
+    const double *J;  // rows of the block's radii
+    long long n2dim;
+    int n0, n1, n2;
+    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
+        int iy = (int)(i / n2);
+        int iz = (int)(i - (long long)iy * n2);
+        int wx = wrap_index(l, n0), wy = wrap_index(iy, n1), wz = wrap_index(iz, n2);
+        long long q = (long long)wx * wx + (long long)wy * wy + (long long)wz * wz;
+        double j = J[o * n2dim + q];
+        cplx<T> u = U[(long long)l * n1 * n2 + i];
+        return mk<T>((T)(j * (double)u.x), (T)(j * (double)u.y));
+    }
+};
+
+// part[block][i1][i2] = sum over this block's cells x of Fa[i1](x) Fb[i2](x) G(x)
+// (complex, FP64 accumulation).  Per chunk of HG_ZR_CHUNK cells the fields are staged in
+// shared memory (as FP64, Fb premultiplied by G); a thread owns a 4 x 4 tile of (i1, i2)
+// and one residue class of the chunk's cells; the residue groups are summed at the end.
+#define HG_ZR_CHUNK 64
+#define HG_ZR_THREADS 256
+template <typename T>
+__global__ void __launch_bounds__(HG_ZR_THREADS)
+    k_zeta_pairsum(const cplx<T> *__restrict__ Fa, int na, const cplx<T> *__restrict__ Fb, int nb,
+                   const cplx<T> *__restrict__ G, long long ntot, double *part) {
+    constexpr int CH = HG_ZR_CHUNK, CHP = HG_ZR_CHUNK + 1;  // padded rows: distinct rows, distinct banks
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int na4 = (na + 3) / 4, nb4 = (nb + 3) / 4;
+    const int ntile = na4 * nb4;
+    const int ngroup = max(1, HG_ZR_THREADS / ntile);
+    double2 *sa = reinterpret_cast<double2 *>(smem_raw);  // [4 na4][CHP]
+    double2 *sb = sa + (size_t)4 * na4 * CHP;             // [4 nb4][CHP]
+    const int t = threadIdx.x;
+    const int tile = t % ntile, grp = t / ntile;
+    const bool active = (t < ntile * ngroup);
+    const int ta = tile / nb4, tb = tile % nb4;
+    double acc[4][4][2];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[u][v][0] = acc[u][v][1] = 0.0;
+    const long long nchunk = (ntot + CH - 1) / CH;
+    for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+        const long long x0 = ch * CH;
+        __syncthreads();
+        for (int e = t; e < 4 * na4 * CH; e += blockDim.x) {
+            int r = e / CH, c = e % CH;
+            double2 v = make_double2(0.0, 0.0);
+            if (r < na && x0 + c < ntot) {
+                cplx<T> a = Fa[(long long)r * ntot + x0 + c];
+                v = make_double2((double)a.x, (double)a.y);
+            }
+            sa[r * CHP + c] = v;
+        }
+        for (int e = t; e < 4 * nb4 * CH; e += blockDim.x) {
+            int r = e / CH, c = e % CH;
+            double2 v = make_double2(0.0, 0.0);
+            if (r < nb && x0 + c < ntot) {
+                cplx<T> b = Fb[(long long)r * ntot + x0 + c];
+                cplx<T> gg = G[x0 + c];
+                double br = (double)b.x, bi = (double)b.y, gr = (double)gg.x, gi = (double)gg.y;
+                v = make_double2(br * gr - bi * gi, br * gi + bi * gr);
+            }
+            sb[r * CHP + c] = v;
+        }
+        __syncthreads();
+        if (active) {
+            for (int c = grp; c < CH; c += ngroup) {
+                double2 av[4], bv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) av[u] = sa[(4 * ta + u) * CHP + c];
+#pragma unroll
+                for (int v = 0; v < 4; v++) bv[v] = sb[(4 * tb + v) * CHP + c];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int v = 0; v < 4; v++) {
+                        acc[u][v][0] += av[u].x * bv[v].x - av[u].y * bv[v].y;
+                        acc[u][v][1] += av[u].x * bv[v].y + av[u].y * bv[v].x;
+                    }
+            }
+        }
+    }
+    // sum the residue groups through shared memory: red[tile][u][v] (complex)
+    __syncthreads();
+    double2 *red = reinterpret_cast<double2 *>(smem_raw);
+    const int nred = ntile * 16;
+    for (int e = t; e < nred; e += blockDim.x) red[e] = make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int g = 0; g < ngroup; g++) {
+        if (active && grp == g) {
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    double2 &r = red[tile * 16 + u * 4 + v];
+                    r.x += acc[u][v][0];
+                    r.y += acc[u][v][1];
+                }
+        }
+        __syncthreads();
+    }
+    for (int e = t; e < na * nb; e += blockDim.x) {
+        int i1 = e / nb, i2 = e % nb;
+        int tl = (i1 / 4) * nb4 + (i2 / 4);
+        double2 r = red[tl * 16 + (i1 % 4) * 4 + (i2 % 4)];
+        part[2 * ((long long)blockIdx.x * na * nb + e)] = r.x;
+        part[2 * ((long long)blockIdx.x * na * nb + e) + 1] = r.y;
+    }
+}
+
+inline size_t zeta_pairsum_smem(int na, int nb) {
+    size_t stage = sizeof(double2) * 4 * (size_t)((na + 3) / 4 + (nb + 3) / 4) * (HG_ZR_CHUNK + 1);
+    size_t red = sizeof(double2) * 16 * (size_t)((na + 3) / 4) * ((nb + 3) / 4);
+    return stage > red ? stage : red;
+}
+
+// out[o] = sum_b part[b][o] in block order (deterministic), complex.
+__global__ void k_sum_parts(const double *part, int nblk, int nout, double2 *out) {
+    int o = blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= nout) return;
+    double re = 0.0, im = 0.0;
+    for (int b = 0; b < nblk; b++) {
+        re += part[2 * ((long long)b * nout + o)];
+        im += part[2 * ((long long)b * nout + o) + 1];
+    }
+    out[o] = make_double2(re, im);
 }
 
 // Functors used by the transform passes.

@@ -106,10 +106,20 @@ int hg_bk_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin
                     double *norm);
 
 /* Periodic-box 3PCF multipole.  Replaces calcThreePointCorrelationFunctionForBOX
- * (bispec.hpp:1205-1424).  Layout as hg_bk_box with r bins; output file value =
- * norm * Re(zeta_save - sn_save) (bispec.hpp:1409-1416). */
+ * (bispec.hpp:1205-1424).  ith_rbin >= 0 computes that r1 row, -1 all n_rbin rows;
+ * zeta_save, sn_save: [rows][n_rbin] complex.  The shot noise sits only on the diagonal
+ * r1 = r2 (bispec.hpp:1279-1285).  Output file value = norm * Re(zeta_save - sn_save)
+ * (bispec.hpp:1402-1416), norm = V^3 / N^3.  Needs a cubic box and mesh. */
 int hg_zeta_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double *zeta_save, double *sn_save,
                 double *norm);
+
+/* Several periodic-box 3PCF multipoles in one call, sharing the density transform, the
+ * filtered fields F_lm(r) and the shot-noise correlation field.  ells = n_multipoles
+ * (ell1, ell2, ELL) triples; outputs are n_multipoles consecutive blocks laid out as in
+ * hg_zeta_box.  Each block equals what calcThreePointCorrelationFunctionForBOX
+ * (bispec.hpp:1205-1424) computes for that multipole. */
+int hg_zeta_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double *zeta_save,
+                      double *sn_save, double *norm);
 
 /* Survey-geometry scalars on the current data (slot 0) and randoms (slot 1):
  * alpha = sum w_D / sum w_R (particle.hpp:268-282), V_survey = (sum w_R)^2 /

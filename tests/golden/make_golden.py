@@ -5,7 +5,8 @@ The values come from oracle/_ref/ref_harness: the reference's own estimator head
 with 17-significant-digit output.  Inputs are stored in the fixture next to the outputs
 so the GPU tests need neither the reference sources nor the harness.
 
-    python tests/golden/make_golden.py        (needs `make -C oracle` first)
+    python tests/golden/make_golden.py          (needs `make -C oracle` first)
+    python tests/golden/make_golden.py --zeta   (only box_zeta.npz)
 """
 from __future__ import annotations
 
@@ -23,6 +24,7 @@ from hitomi_b200.synthetic import lognormal_box, uniform_box  # noqa: E402
 from oracle import ref_runner  # noqa: E402
 
 MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2))
+ZETA_MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2), (1, 1, 2))
 
 
 def binning_arr(b: Binning):
@@ -65,9 +67,42 @@ def run_bk(pos, n_mesh, boxsize, b, assign, mps=MULTIPOLES):
     return out
 
 
+def run_zeta(pos, n_mesh, boxsize, b, assign, mps=ZETA_MULTIPOLES):
+    out = {}
+    for mp in mps:
+        with ref_runner.RefRun() as r:
+            r.run("3PCF", pos, *mp, n_mesh, boxsize, b, assign=assign)
+            out[mp] = r.zeta(*mp, b.n_rbin)
+    return out
+
+
+def make_zeta():
+    """3PCF multipoles, all rows: file values norm * Re(zeta - sn) (bispec.hpp:1402-1416)."""
+    pos = lognormal_box(10000, 400.0, ngrid=32, seed=15, exact_n=10000)
+    bz = Binning(0.02, 0.1, 5, 20.0, 140.0, 7)
+    d = dict(pos=pos, boxsize=400.0, n_mesh=32, binning=binning_arr(bz))
+    for mp, v in run_zeta(pos, 32, 400.0, bz, "TSC").items():
+        d["zeta_TSC_" + "".join(map(str, mp))] = v
+    for assign in ("NGP", "CIC"):
+        for mp, v in run_zeta(pos, 32, 400.0, bz, assign, mps=((0, 0, 0),)).items():
+            d[f"zeta_{assign}_" + "".join(map(str, mp))] = v
+    # r bins reaching past half the box and below one cell, on the boundary-stress catalogue
+    pe = edge_catalogue(16, 400.0, 6000, seed=13)
+    be = Binning(0.02, 0.1, 5, 10.0, 250.0, 9)
+    d["edge_pos"] = pe
+    d["edge_binning"] = binning_arr(be)
+    d["edge_zeta_TSC_000"] = run_zeta(pe, 16, 400.0, be, "TSC", mps=((0, 0, 0),))[(0, 0, 0)]
+    d["edge_zeta_TSC_110"] = run_zeta(pe, 16, 400.0, be, "TSC", mps=((1, 1, 0),))[(1, 1, 0)]
+    np.savez_compressed(os.path.join(HERE, "box_zeta.npz"), **d)
+
+
 def main():
     if not ref_runner.available():
         raise SystemExit("build the oracle first: make -C oracle")
+    if "--zeta" in sys.argv:
+        make_zeta()
+        print("fixtures written")
+        return
     # smoke case
     pos = lognormal_box(20000, 1000.0, ngrid=32, seed=5, exact_n=20000)
     b = Binning(0.02, 0.08, 4, 4.0, 156.0, 20)
@@ -117,6 +152,7 @@ def main():
             r.run("pk", pos, ell, 0, ell, [16, 32, 64], 1000.0, bn)
             d[f"pk_{ell}"] = r.pk(ell)[1]
     np.savez_compressed(os.path.join(HERE, "box_noncubic.npz"), **d)
+    make_zeta()
     print("fixtures written")
 
 
