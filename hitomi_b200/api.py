@@ -109,6 +109,12 @@ class Context:
         self._check(self._lib.hg_set_particles(self._h, slot, _dp(a), a.shape[0], a.shape[1] * 8, pos_off, los_off,
                                                w_off))
 
+    def set_survey(self, data: np.ndarray, randoms: np.ndarray):
+        """Data and randoms as (n, 7) {pos, los, w} records (hitomi_b200.survey.prepare)."""
+        from . import survey
+        for slot, arr in ((0, data), (1, randoms)):
+            self.set_particles(slot, arr, pos_off=survey.POS_OFF, los_off=survey.LOS_OFF, w_off=survey.W_OFF)
+
     def set_particles_device(self, slot: int, ptr: int, n: int, stride_bytes: int, pos_off: int = 0,
                              los_off: int = -1, w_off: int = -1, keep=None):
         """Use a caller-owned device array (e.g. a torch CUDA tensor's data_ptr()) in place."""

@@ -7,8 +7,8 @@
 //                      the FP64 in-bounds mass;
 //   2. exclusive scan of the per-tile counts; tiles cut into chunks of <= CH records;
 //   3. k_bin_scatter : one compact record per (particle, tile) in tile order;
-//   4. k_tile_accum  : one CTA per chunk accumulates its records in an FP64 shared-memory
-//                      tile; a tile with a single chunk is written once, coalesced; the
+//   4. k_tile_accum  : one CTA per chunk accumulates its records in a shared-memory tile
+//                      (the mesh's precision); a tile with a single chunk is written once, coalesced; the
 //                      chunks of a densely populated tile (clustered catalogues) are
 //                      zeroed first and add their partial tiles (one add per cell per
 //                      chunk, not per particle).
@@ -115,25 +115,46 @@ struct PartSrc {
     long long stride;           // bytes
     int pos_off;                // doubles
     int w_off;                  // doubles, < 0: weight 1
-    const double2 *cw;          // optional per-particle complex weight (Y_lm-weighted), overrides w
+    const double2 *cw;          // optional per-particle complex weight, overrides w
     double scale;               // multiplies the weight (e.g. -alpha for randoms)
+    int ylm_on;                 // weight *= Yhat_lm(los) (field.hpp:199-216)
+    int ylm_l, ylm_m;
+    int los_off;                // doubles
 };
 
-__device__ __forceinline__ void load_particle(const PartSrc &s, long long p, double pos[3], double &wr, double &wi) {
+__device__ __forceinline__ void load_pos(const PartSrc &s, long long p, double pos[3]) {
     const double *rec = reinterpret_cast<const double *>(s.base + p * s.stride);
     pos[0] = rec[s.pos_off + 0];
     pos[1] = rec[s.pos_off + 1];
     pos[2] = rec[s.pos_off + 2];
+}
+
+// The particle's assignment weight: w (or 1), times Yhat_lm(los) when requested, times
+// the source's scale; (Yhat.re w, Yhat.im w) as in field.hpp:199-216.
+__device__ __forceinline__ void load_weight(const PartSrc &s, long long p, double &wr, double &wi) {
+    const double *rec = reinterpret_cast<const double *>(s.base + p * s.stride);
     if (s.cw) {
         double2 c = s.cw[p];
         wr = c.x;
         wi = c.y;
     } else {
-        wr = (s.w_off >= 0) ? rec[s.w_off] : 1.0;
-        wi = 0.0;
+        double w = (s.w_off >= 0) ? rec[s.w_off] : 1.0;
+        if (s.ylm_on) {
+            zd y = ylm_reduced(s.ylm_l, s.ylm_m, rec[s.los_off], rec[s.los_off + 1], rec[s.los_off + 2]);
+            wr = y.x * w;
+            wi = y.y * w;
+        } else {
+            wr = w;
+            wi = 0.0;
+        }
     }
     wr *= s.scale;
     wi *= s.scale;
+}
+
+__device__ __forceinline__ void load_particle(const PartSrc &s, long long p, double pos[3], double &wr, double &wi) {
+    load_pos(s, p, pos);
+    load_weight(s, p, wr, wi);
 }
 
 template <typename T>
@@ -181,17 +202,19 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-// Pass 1: tile counts + FP64 in-bounds mass  sum_p w_p factor prod(w_axis)  (the field's
-// exact integral, needed for the k = 0 mode since boundary drops lose mass).  Clustered
-// catalogues put many lanes of a warp on the same tile, so the count is warp-aggregated.
+// Pass 1: tile counts + (when mass != null) the FP64 in-bounds mass
+// sum_p w_p factor prod(w_axis)  (the field's exact integral, needed for the k = 0 mode
+// since boundary drops lose mass).  Clustered catalogues put many lanes of a warp on the
+// same tile, so the count is warp-aggregated.
 __global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double *mass) {
     long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double m_re = 0.0, m_im = 0.0;
     int tiles[64];
     int nt = 0;
     if (p < src.n) {
-        double pos[3], wr, wi;
-        load_particle(src, p, pos, wr, wi);
+        double pos[3], wr = 0.0, wi = 0.0;
+        load_pos(src, p, pos);
+        if (mass) load_weight(src, p, wr, wi);
         int anc[3];
         double d[3];
         for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
@@ -199,7 +222,8 @@ __global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double
         const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
         bool inside = true;
         for (int a = 0; a < 3; a++) inside &= (anc[a] + s0 >= 0) && (anc[a] + s0 + W - 1 < g.n[a]);
-        if (inside || g.periodic) {
+        if (!mass) {
+        } else if (inside || g.periodic) {
             // every stencil point lands: the weights sum to one per axis
             m_re += wr * g.factor;
             m_im += wi * g.factor;
@@ -225,6 +249,7 @@ __global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double
         unsigned grp = __match_any_sync(0xffffffffu, t);
         if (t >= 0 && lane == __ffs(grp) - 1) atomicAdd(&cnt[t], (unsigned)__popc(grp));
     }
+    if (!mass) return;
     m_re = warp_sum_d(m_re);
     m_im = warp_sum_d(m_im);
     if (lane == 0 && (m_re != 0.0 || m_im != 0.0)) {
@@ -266,6 +291,67 @@ __global__ void k_bin_scatter(PartSrc src, AssignGeom g, const unsigned int *off
             base = __shfl_sync(grp, base, leader);
             rec[off[t] + base + __popc(grp & lt)] = r;
         }
+    }
+}
+
+// Per-particle FP64 sums  out[q] = sum_p scale w_p^pw[q] Yhat_{l_q m_q}(los_p)  (complex), as
+// block partials part[block][q] summed on the host in block order (deterministic):
+// sum w (particle.hpp:336-352), sum w^2 (particle.hpp:255-258), and the shot-noise sums
+// sum w^2 Yhat_LM (field.hpp:1164-1185).
+#define HG_PSUM_MAX 16
+struct PSumSpec {
+    int n;
+    int pw[HG_PSUM_MAX];
+    int l[HG_PSUM_MAX], m[HG_PSUM_MAX];  // l < 0: no harmonic (weight only)
+};
+__global__ void k_particle_sums(PartSrc src, PSumSpec q, double *part) {
+    __shared__ double red[HG_PSUM_MAX][2][32];
+    double acc[HG_PSUM_MAX][2];
+    for (int j = 0; j < HG_PSUM_MAX; j++) acc[j][0] = acc[j][1] = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < src.n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const double *rec = reinterpret_cast<const double *>(src.base + p * src.stride);
+        const double w = (src.w_off >= 0) ? rec[src.w_off] : 1.0;
+        for (int j = 0; j < q.n; j++) {
+            double wp = w;
+            for (int e = 1; e < q.pw[j]; e++) wp *= w;
+            if (q.l[j] < 0) {
+                acc[j][0] += wp;
+            } else {
+                zd y = ylm_reduced(q.l[j], q.m[j], rec[src.los_off], rec[src.los_off + 1], rec[src.los_off + 2]);
+                acc[j][0] += wp * y.x;
+                acc[j][1] += wp * y.y;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int j = 0; j < q.n; j++)
+        for (int c = 0; c < 2; c++) {
+            double v = warp_sum_d(acc[j][c]);
+            if (lane == 0) red[j][c][wid] = v;
+        }
+    __syncthreads();
+    if (threadIdx.x < 2 * q.n) {
+        const int j = threadIdx.x >> 1, c = threadIdx.x & 1;
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[j][c][w];
+        part[(long long)blockIdx.x * 2 * HG_PSUM_MAX + 2 * j + c] = v * src.scale;
+    }
+}
+
+// sum_c m[c]^2 per block (FP64), for V_survey = (sum w_R)^2 / (sum_c rho_R^2 dV) (field.hpp:449-503)
+__global__ void k_sum_squares(const double *m, long long n, double *part) {
+    __shared__ double red[32];
+    double a = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a += m[i] * m[i];
+    a = warp_sum_d(a);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[w];
+        part[blockIdx.x] = v;
     }
 }
 

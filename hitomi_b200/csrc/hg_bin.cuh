@@ -41,13 +41,23 @@ __device__ __forceinline__ double shot_tab(const AxisTabs &t, int ix, int iy, in
 }
 
 // Read access to a transformed field, either a half spectrum [n0][n1][n2/2+1] of a real
-// input (negative kz by Hermitian symmetry) or a full [n0][n1][n2] spectrum.
+// input (negative kz by Hermitian symmetry) or a full [n0][n1][n2] spectrum.  With
+// mirror = 1 it reads sgn * conj(F(-k)): the field of the conjugate weights, e.g.
+// F_{l,-m}(k) = (-1)^m conj(F_{l,m}(-k)) since Yhat_{l,-m} = (-1)^m conj(Yhat_{l,m}).
 template <typename T>
 struct Spec {
     const cplx<T> *p;
     int n0, n1, n2;
     int half;
+    int mirror;
+    double sgn;
     __device__ __forceinline__ zd at(int ix, int iy, int iz) const {
+        if (mirror) {
+            Spec<T> d = *this;
+            d.mirror = 0;
+            zd v = d.at((n0 - ix) % n0, (n1 - iy) % n1, (n2 - iz) % n2);
+            return mk<double>(sgn * v.x, -sgn * v.y);
+        }
         if (!half) {
             cplx<T> v = p[((long long)ix * n1 + iy) * n2 + iz];
             return mk<double>((double)v.x, (double)v.y);

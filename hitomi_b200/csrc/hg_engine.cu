@@ -207,7 +207,13 @@ struct Engine : public hg_ctx {
     std::map<int, std::unique_ptr<DBuf>> jtab_k;  // J_l[i][n2] at the k bins (geometry only)
     std::map<std::array<int, 3>, std::unique_ptr<DBuf>> hist_mp;  // per multipole (catalogue)
     std::set<std::array<int, 3>> hist_ok;
-    DBuf hist_tmp, snmat, sn_part, d_kv;
+    DBuf hist_tmp, snmat, snblk, sn_part, d_kv;
+
+    // survey state (per pair of catalogues)
+    DBuf smesh_re, smesh_im, dmesh, psum_part;
+    std::map<std::pair<int, int>, std::unique_ptr<DBuf>> sfield;  // (l, m >= 0) -> spectrum of D - alpha R
+    std::set<std::pair<int, int>> sfield_ok;
+    double sfield_alpha = 0.0;
 
     // 3PCF state: geometry tables (per context) and filtered fields (per catalogue)
     std::map<int, std::unique_ptr<DBuf>> jtab_r;  // J_l[j][n2] = j_l(dk r_j sqrt(n2))
@@ -465,6 +471,7 @@ struct Engine : public hg_ctx {
         Gz_valid = false;
         zf_ok.clear();
         zpairs.clear();
+        sfield_ok.clear();
     }
 
     // ------------------------------------------------------------------ assignment
@@ -491,8 +498,12 @@ struct Engine : public hg_ctx {
         return a;
     }
 
-    // Assign one catalogue into the real mesh (rho); returns the FP64 in-bounds sum of rho.
-    double assign_real(const PartSrc &src, const AssignGeom &ag, T *out) {
+    // Assign one or more particle sources into one mesh of type U (real, or complex as
+    // planar re/im arrays): tile binning of every source, scan, chunking, scatter of
+    // compact records, tile accumulation.  Returns the FP64 in-bounds mass (real part)
+    // when want_mass.
+    template <typename U, bool CPLX>
+    double assign_mesh(const std::vector<PartSrc> &srcs, const AssignGeom &ag, U *out_re, U *out_im, bool want_mass) {
         const int ntiles = ag.nt[0] * ag.nt[1] * ag.nt[2];
         HG_CK(cnt.ensure(sizeof(unsigned) * (ntiles + 1)));
         HG_CK(off.ensure(sizeof(unsigned) * (ntiles + 1)));
@@ -503,9 +514,14 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(mass.p, 0, sizeof(double) * 2, st));
-        kb("assign_bin_count", double(src.n) * 24.0);
-        k_bin_count<<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(cnt), dp<double>(mass));
-        ke();
+        long long nsum = 0;
+        for (const auto &src : srcs) {
+            nsum += src.n;
+            kb("assign_bin_count", double(src.n) * 24.0);
+            k_bin_count<<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(cnt),
+                                                           want_mass ? dp<double>(mass) : nullptr);
+            ke();
+        }
         size_t tb = 0, tb2 = 0;
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
@@ -526,25 +542,31 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemcpyAsync(hm, mass.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
         const unsigned total = tot[0], nchunks = tot[1];
-        HG_CK(rec.ensure(sizeof(PRec<T>) * std::max<size_t>(total, 1)));
+        HG_CK(rec.ensure(sizeof(PRec<U>) * std::max<size_t>(total, 1)));
         HG_CK(chunks.ensure(sizeof(Chunk) * std::max<size_t>(nchunks, 1)));
         kb("assign_chunks", double(ntiles) * 16.0);
         k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
                                                         dp<Chunk>(chunks));
         ke();
-        kb("assign_bin_scatter", double(src.n) * 24.0 + double(total) * sizeof(PRec<T>));
-        k_bin_scatter<T><<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(off), dp<unsigned>(cursor),
-                                                            dp<PRec<T>>(rec));
-        ke();
+        for (const auto &src : srcs) {
+            kb("assign_bin_scatter", double(src.n) * 24.0 + double(total) * sizeof(PRec<U>) * double(src.n) / nsum);
+            k_bin_scatter<U><<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(off), dp<unsigned>(cursor),
+                                                                dp<PRec<U>>(rec));
+            ke();
+        }
         kb("assign_zero_split", 0.0);
-        k_zero_split_tiles<T, false><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), ag, out, nullptr);
+        k_zero_split_tiles<U, CPLX><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), ag, out_re, out_im);
         ke();
-        size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2];
-        HG_CK(cudaFuncSetAttribute(k_tile_accum<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kb("assign_tile_accum", double(total) * sizeof(PRec<T>) + double(g.ntot) * sizeof(T));
-        k_tile_accum<T, false><<<nchunks, 256, smem, st>>>(dp<PRec<T>>(rec), dp<Chunk>(chunks), ag, out, nullptr);
+        size_t smem = sizeof(U) * ag.t[0] * ag.t[1] * ag.t[2] * (CPLX ? 2 : 1);
+        HG_CK(cudaFuncSetAttribute(k_tile_accum<U, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kb("assign_tile_accum", double(total) * sizeof(PRec<U>) + double(g.ntot) * sizeof(U) * (CPLX ? 2 : 1));
+        k_tile_accum<U, CPLX><<<nchunks, 256, smem, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
         ke();
         return hm[0];
+    }
+
+    double assign_real(const PartSrc &src, const AssignGeom &ag, T *out) {
+        return assign_mesh<T, false>({src}, ag, out, nullptr, true);
     }
 
     // Stockham shared-memory engine: for loaders that compute their input (8 values per
@@ -609,6 +631,10 @@ struct Engine : public hg_ctx {
     // (TwoPointStatisticsClass::calcPowerSpectrum, field.hpp:765-852).  avg: [nbin][nlm] complex.
     void pk_bin(const std::vector<LM> &lm, double S_re, double S_im, std::vector<double> &avg,
                 std::vector<unsigned long long> &nm) {
+        pk_bin2(half_spec(), half_spec(), lm, S_re, S_im, avg, nm);
+    }
+    void pk_bin2(const Spec<T> &f1, const Spec<T> &f2, const std::vector<LM> &lm, double S_re, double S_im,
+                 std::vector<double> &avg, std::vector<unsigned long long> &nm) {
         const int nbin = cfg.n_kbin;
         HG_REQUIRE((int)lm.size() <= HG_MAX_LM, "too many multipoles in one binning call");
         LMList L;
@@ -638,7 +664,7 @@ struct Engine : public hg_ctx {
         long long total = (long long)cn.x * cn.y * cn.z;
         unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 8);
         kb("pk_bin", double(total) * sizeof(C));
-        k_pk_bin<T><<<blocks, 256, smem, st>>>(half_spec(), half_spec(), g, tabs, lo, cn, dp<int2>(lut), lutn, nbin, L,
+        k_pk_bin<T><<<blocks, 256, smem, st>>>(f1, f2, g, tabs, lo, cn, dp<int2>(lut), lutn, nbin, L,
                                                S_re, S_im, cfg.assign, wpow, dp<double>(bin_acc),
                                                dp<unsigned long long>(bin_cnt), 0, 0.0, 0.0);
         ke();
@@ -1199,16 +1225,29 @@ struct Engine : public hg_ctx {
             const double *J1 = jtab(mp.l1);
             const double *J2 = jtab(mp.l2);
             const double *hq = dp<double>(*hist_mp[{mp.l1, mp.l2, mp.L}]);
-            const int nblk = (int)((n2dim + HG_SN_CHUNK - 1) / HG_SN_CHUNK);
-            HG_CK(sn_part.ensure(sizeof(double) * 2 * (size_t)nblk * ns * ns));
-            const size_t smem = sn_partial_smem(ns);
-            HG_CK(cudaFuncSetAttribute(k_sn_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            kb("sn_matrix", double(2 * ns + 2) * n2dim * 8.0);
-            k_sn_partial<<<nblk, 256, smem, st>>>(J1, J2, hq, n2dim, ns, dp<double>(sn_part));
-            ke();
-            kb("sn_matrix", double(nblk) * ns * ns * 16.0);
-            k_sn_reduce<<<grid1(ns * ns, 128), 128, 0, st>>>(dp<double>(sn_part), nblk, ns, dp<double2>(snmat));
-            ke();
+            const int nblk = sn_partial_blocks(n2dim);
+            const int rb = std::min(ns, HG_SN_MAXROWS);
+            HG_CK(sn_part.ensure(sizeof(double) * 2 * (size_t)nblk * rb * rb));
+            HG_CK(snblk.ensure(sizeof(double2) * (size_t)rb * rb));
+            for (int a0 = 0; a0 < ns; a0 += rb)
+                for (int b0 = 0; b0 < ns; b0 += rb) {
+                    const int na = std::min(rb, ns - a0), nb = std::min(rb, ns - b0);
+                    const size_t smem = sn_partial_smem(na, nb);
+                    HG_CK(cudaFuncSetAttribute(k_sn_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                    kb("sn_matrix", double(na + 2 * nb + 2) * n2dim * 8.0);
+                    k_sn_partial<<<nblk, HG_SN_THREADS, smem, st>>>(J1 + (size_t)a0 * n2dim, na,
+                                                                    J2 + (size_t)b0 * n2dim, nb, hq, n2dim,
+                                                                    dp<double>(sn_part));
+                    ke();
+                    kb("sn_matrix", double(nblk) * na * nb * 16.0);
+                    k_sum_parts<<<grid1((long long)na * nb, 128), 128, 0, st>>>(dp<double>(sn_part), nblk, na * nb,
+                                                                                  dp<double2>(snblk));
+                    ke();
+                    // place the (a0, b0) block into the ns x ns matrix
+                    HG_CK(cudaMemcpy2DAsync(dp<double2>(snmat) + (size_t)a0 * ns + b0, sizeof(double2) * ns,
+                                            snblk.p, sizeof(double2) * nb, sizeof(double2) * nb, na,
+                                            cudaMemcpyDeviceToDevice, st));
+                }
             std::vector<double> sd(2 * ns * ns);
             HG_CK(cudaMemcpyAsync(sd.data(), snmat.p, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, st));
             HG_CK(cudaStreamSynchronize(st));
@@ -1537,11 +1576,191 @@ struct Engine : public hg_ctx {
         }
         end();
     }
-    void survey_scalars(double *, double *, double *, double *, double *) override {
-        throw HgError{"hg_survey_scalars is not available in this build"};
+    // ------------------------------------------------------------------ survey geometry
+    PartSrc survey_src(int s, bool ylm, int l, int m, double scale) const {
+        const Slot &S = slot[s];
+        PartSrc p{};
+        p.base = S.base();
+        p.n = S.n;
+        p.stride = S.stride;
+        p.pos_off = S.pos_off;
+        p.w_off = S.w_off;
+        p.cw = nullptr;
+        p.scale = scale;
+        p.ylm_on = ylm ? 1 : 0;
+        p.ylm_l = l;
+        p.ylm_m = m;
+        p.los_off = S.los_off;
+        return p;
     }
-    void pk_survey(int, double, double, double *, int *, double *) override {
-        throw HgError{"hg_pk_survey is not available in this build"};
+
+    void require_survey(bool need_los) const {
+        HG_REQUIRE(slot[0].set && slot[1].set,
+                   "survey statistics need data (slot 0) and randoms (slot 1): call hg_set_particles for both");
+        if (need_los)
+            HG_REQUIRE(slot[0].los_off >= 0 && slot[1].los_off >= 0,
+                       "survey multipoles need line-of-sight vectors: pass los_off for both catalogues");
+    }
+
+    // FP64 particle sums (block partials added on the host in block order)
+    std::vector<double> particle_sums(int s, const PSumSpec &q) {
+        const PartSrc src = survey_src(s, false, 0, 0, 1.0);
+        const int nb = (int)std::min<long long>(grid1(src.n, 256), 148 * 8);
+        HG_CK(psum_part.ensure(sizeof(double) * 2 * HG_PSUM_MAX * nb));
+        kb("particle_sums", double(src.n) * 32.0);
+        k_particle_sums<<<nb, 256, 0, st>>>(src, q, dp<double>(psum_part));
+        ke();
+        std::vector<double> h(2 * HG_PSUM_MAX * (size_t)nb);
+        HG_CK(cudaMemcpyAsync(h.data(), psum_part.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        std::vector<double> out(2 * q.n, 0.0);
+        for (int b = 0; b < nb; b++)
+            for (int j = 0; j < 2 * q.n; j++) out[j] += h[(size_t)b * 2 * HG_PSUM_MAX + j];
+        return out;
+    }
+
+    // alpha = sum w_D / sum w_R (particle.hpp:268-282); V_survey = (sum w_R)^2 / sum_c rho_R^2 dV
+    // on an FP64 mesh in both forms (field.hpp:449-503); nbar = (sum w_D)^2 / V / sum w_D^2
+    // (particle.hpp:284-300).
+    void survey_scalars(double *alpha, double *vs, double *nbar, double *wd, double *wr) override {
+        require_survey(false);
+        begin();
+        PSumSpec q{};
+        q.n = 2;
+        q.pw[0] = 1;
+        q.l[0] = -1;
+        q.pw[1] = 2;
+        q.l[1] = -1;
+        std::vector<double> sd = particle_sums(0, q);
+        q.n = 1;
+        std::vector<double> sr = particle_sums(1, q);
+        const double wD = sd[0], w2D = sd[2], wR = sr[0];
+        HG_REQUIRE(wD != 0.0 && wR != 0.0, "the summed weights of data and randoms must be non-zero");
+        const double a = wD / wR;
+        AssignGeom ag = make_geom(0.0);
+        ag.acc_factor = ag.factor;  // rho = sum w (1/dV) prod(w_axis), FP64
+        HG_CK(dmesh.ensure(sizeof(double) * g.ntot));
+        assign_mesh<double, false>({survey_src(1, false, 0, 0, 1.0)}, ag, dp<double>(dmesh), nullptr, false);
+        const int nb = 148 * 8;
+        HG_CK(psum_part.ensure(sizeof(double) * nb));
+        kb("survey_volume", double(g.ntot) * 8.0);
+        k_sum_squares<<<nb, 256, 0, st>>>(dp<double>(dmesh), g.ntot, dp<double>(psum_part));
+        ke();
+        std::vector<double> h(nb);
+        HG_CK(cudaMemcpyAsync(h.data(), psum_part.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        double s2 = 0.0;
+        for (int b = 0; b < nb; b++) s2 += h[b];
+        const double dV = g.volume / double(g.ntot);
+        const double V = wR * wR / (s2 * dV);
+        dmesh.release();
+        if (alpha) *alpha = a;
+        if (vs) *vs = V;
+        if (nbar) *nbar = wD * wD / V / w2D;
+        if (wd) *wd = wD;
+        if (wr) *wr = wR;
+        end();
+    }
+
+    // FFT[dV (n_D - alpha n_R)] of the Yhat_lm(los)-weighted fields, m >= 0
+    // (calcYlmWeightedDensityFluctuation field.hpp:186-228, then field.hpp:310-325).  m = 0 is
+    // a real field (half spectrum); m > 0 is complex (full spectrum).
+    Spec<T> survey_field(int l, int m, double alpha) {
+        if (alpha != sfield_alpha) {
+            sfield_ok.clear();
+            sfield_alpha = alpha;
+        }
+        const int hz = g.n[2] / 2 + 1;
+        const bool real = (m == 0);
+        auto key = std::make_pair(l, m);
+        auto &pb = sfield[key];
+        if (!pb) pb = std::make_unique<DBuf>();
+        Spec<T> sp{dp<C>(*pb), g.n[0], g.n[1], g.n[2], real ? 1 : 0, 0, 1.0};
+        if (sfield_ok.count(key)) return sp;
+        const long long fsz = real ? (long long)g.n[0] * g.n[1] * hz : g.ntot;
+        HG_CK(pb->ensure(sizeof(C) * fsz));
+        sp.p = dp<C>(*pb);
+        AssignGeom ag = make_geom(0.0);
+        ag.acc_factor = 1.0;  // mass units: dV rho, the transform's input
+        const bool ylm = !(l == 0 && m == 0);
+        std::vector<PartSrc> srcs{survey_src(0, ylm, l, m, 1.0), survey_src(1, ylm, l, m, -alpha)};
+        HG_CK(smesh_re.ensure(sizeof(T) * g.ntot));
+        C *F = dp<C>(*pb);
+        if (real) {
+            assign_mesh<T, false>(srcs, ag, dp<T>(smesh_re), nullptr, false);
+            pass<-1>(g.n[2], LdMeshDelta<T>{dp<T>(smesh_re), g.n[2], (T)0, (T)1}, StHalf<T>{F, g.n[2], hz},
+                     (long long)g.n[0] * g.n[1], 1, "fft_survey",
+                     double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
+            pass<-1>(g.n[1], LdArr<T>{F, g.n[1], hz}, StArr<T>{F, g.n[1], hz}, g.n[0], hz, "fft_survey");
+            pass<-1>(g.n[0], LdArr<T>{F, g.n[0], (long long)g.n[1] * hz}, StArr<T>{F, g.n[0], (long long)g.n[1] * hz},
+                     1, (long long)g.n[1] * hz, "fft_survey");
+        } else {
+            HG_CK(smesh_im.ensure(sizeof(T) * g.ntot));
+            assign_mesh<T, true>(srcs, ag, dp<T>(smesh_re), dp<T>(smesh_im), false);
+            const long long yz = (long long)g.n[1] * g.n[2];
+            pass<-1>(g.n[2], LdPlanar<T>{dp<T>(smesh_re), dp<T>(smesh_im), g.n[2]}, StArr<T>{F, g.n[2], 1},
+                     (long long)g.n[0] * g.n[1], 1, "fft_survey", double(g.ntot) * (2 * sizeof(T) + sizeof(C)));
+            pass<-1>(g.n[1], LdArr<T>{F, g.n[1], g.n[2]}, StArr<T>{F, g.n[1], g.n[2]}, g.n[0], g.n[2], "fft_survey");
+            pass<-1>(g.n[0], LdArr<T>{F, g.n[0], yz}, StArr<T>{F, g.n[0], yz}, 1, yz, "fft_survey");
+        }
+        sfield_ok.insert(key);
+        return sp;
+    }
+
+    // calcPowerSpectrum (powerspec.hpp:4-91): sum over M of w3j-weighted binned
+    // (dn_LM conj dn_00 - S_LM C) / W^2 Yhat_{l m1}(k), S_LM = sum_D w^2 Yhat_LM + alpha^2 sum_R
+    // w^2 Yhat_LM (field.hpp:1164-1185).  Fields for M < 0 are mirrors of M > 0.
+    void pk_survey(int ell, double alpha, double vs, double *pk_save, int *n_mode, double *norm) override {
+        HG_REQUIRE(ell >= 0, "ell must be >= 0");
+        require_survey(ell > 0);
+        begin();
+        const int nb = cfg.n_kbin;
+        PSumSpec q{};
+        q.n = ell + 1;
+        HG_REQUIRE(q.n <= HG_PSUM_MAX, "ell too large");
+        for (int M = 0; M <= ell; M++) {
+            q.pw[M] = 2;
+            q.l[M] = ell;
+            q.m[M] = M;
+        }
+        std::vector<double> sD = particle_sums(0, q), sR = particle_sums(1, q);
+        q.n = 1;
+        q.pw[0] = 1;
+        q.l[0] = -1;
+        const double wD = particle_sums(0, q)[0];
+        HG_REQUIRE(wD != 0.0, "the summed data weights must be non-zero");
+        const Spec<T> f00 = survey_field(0, 0, alpha);
+        std::vector<double> acc(2 * nb, 0.0);
+        std::vector<unsigned long long> nm;
+        for (int M = -ell; M <= ell; M++) {
+            const int am = M < 0 ? -M : M;
+            double Sr = sD[2 * am] + alpha * alpha * sR[2 * am];
+            double Si = sD[2 * am + 1] + alpha * alpha * sR[2 * am + 1];
+            Spec<T> f1 = survey_field(ell, am, alpha);
+            if (M < 0) {  // dn_{l,-|M|}(k) = (-1)^|M| conj(dn_{l,|M|}(-k)); likewise S
+                const double sg = (am % 2) ? -1.0 : 1.0;
+                f1.mirror = 1;
+                f1.sgn = sg;
+                Sr = sg * Sr;
+                Si = -sg * Si;
+            }
+            for (int m1 = -ell; m1 <= ell; m1++) {
+                double w = wigner3j(ell, 0, ell, 0, 0, 0) * wigner3j(ell, 0, ell, m1, 0, M);
+                w *= double(2 * ell + 1) * double(2 * ell + 1);
+                if (std::fabs(w) < 1.0e-10) continue;
+                std::vector<double> avg;
+                pk_bin2(f1, f00, {LM{ell, m1}}, Sr, Si, avg, nm);
+                for (int i = 0; i < nb; i++) {
+                    acc[2 * i] += w * avg[2 * i];
+                    acc[2 * i + 1] += w * avg[2 * i + 1];
+                }
+            }
+        }
+        for (int i = 0; i < 2 * nb; i++) pk_save[i] = acc[i];
+        if (n_mode)
+            for (int i = 0; i < nb; i++) n_mode[i] = (int)nm[i];
+        if (norm) *norm = vs / wD / wD;  // particle.hpp:303-316
+        end();
     }
 };
 

@@ -11,6 +11,8 @@
 //   k_bessel_table, k_sn_matrix   spline-evaluated j_l products summed over n^2
 #pragma once
 
+#include <algorithm>
+
 #include "hg_common.cuh"
 #include "hg_fft.cuh"
 #include "hg_bin.cuh"
@@ -283,58 +285,106 @@ __global__ void k_bessel_table(const double *sy, const double *sc, int sn, doubl
     J[q] = (x <= xmax) ? spline_eval(sy, sc, sn, xmin, dx, x) : 0.0;
 }
 
-// out[i1][i2] = sum_n2 J1[i1][n2] J2[i2][n2] hist[n2], as a skinny product J1 diag(h) J2^T:
-// each block stages a chunk of n2 for all rows of J1, J2 and h in shared memory and writes
-// its nk x nk partial sums; k_sn_reduce adds the partials in a fixed order (deterministic).
-#define HG_SN_CHUNK 128
-__global__ void k_sn_partial(const double *J1, const double *J2, const double *hist, long long n2dim, int nk,
-                             double *part) {
+// out[i1][i2] = sum_n2 J1[i1][n2] J2[i2][n2] hist[n2], as a skinny product J1 diag(h) J2^T.
+// Persistent blocks walk chunks of HG_SN_CHUNK values of n2; each chunk stages J1 and
+// J2 * hist (complex) in shared memory; a thread owns a 4 x 4 register tile of (i1, i2)
+// and one residue class of the chunk; residue groups are summed in shared memory and
+// each block writes its na x nb partial sums; k_sum_parts adds the partials in a fixed
+// order (deterministic).
+#define HG_SN_CHUNK 64
+#define HG_SN_THREADS 256
+__global__ void __launch_bounds__(HG_SN_THREADS)
+    k_sn_partial(const double *__restrict__ J1, int na, const double *__restrict__ J2, int nb,
+                 const double *__restrict__ hist, long long n2dim, double *part) {
+    constexpr int CH = HG_SN_CHUNK, CHP = HG_SN_CHUNK + 1;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int CP = HG_SN_CHUNK + 1;  // padded row: rows of J land in different banks
-    double *j1 = reinterpret_cast<double *>(smem_raw);
-    double *j2 = j1 + (size_t)nk * CP;
-    double *hr = j2 + (size_t)nk * CP;
-    double *hi = hr + CP;
-    const long long n0 = (long long)blockIdx.x * HG_SN_CHUNK;
-    const int len = (int)min((long long)HG_SN_CHUNK, n2dim - n0);
-    for (int e = threadIdx.x; e < nk * HG_SN_CHUNK; e += blockDim.x) {
-        int r = e / HG_SN_CHUNK, n = e % HG_SN_CHUNK;
-        bool ok = n < len;
-        j1[r * CP + n] = ok ? J1[(long long)r * n2dim + n0 + n] : 0.0;
-        j2[r * CP + n] = ok ? J2[(long long)r * n2dim + n0 + n] : 0.0;
-    }
-    for (int n = threadIdx.x; n < HG_SN_CHUNK; n += blockDim.x) {
-        bool ok = n < len;
-        hr[n] = ok ? hist[2 * (n0 + n)] : 0.0;
-        hi[n] = ok ? hist[2 * (n0 + n) + 1] : 0.0;
+    const int na4 = (na + 3) / 4, nb4 = (nb + 3) / 4;
+    const int ntile = na4 * nb4;
+    const int ngroup = max(1, HG_SN_THREADS / ntile);
+    double2 *sb = reinterpret_cast<double2 *>(smem_raw);  // [4 nb4][CHP]  J2 * h
+    double *sa = reinterpret_cast<double *>(sb + (size_t)4 * nb4 * CHP);  // [4 na4][CHP]  J1
+    const int t = threadIdx.x;
+    const int tile = t % ntile, grp = t / ntile;
+    const bool active = (t < ntile * ngroup);
+    const int ta = tile / nb4, tb = tile % nb4;
+    double acc[4][4][2];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[u][v][0] = acc[u][v][1] = 0.0;
+    const long long nchunk = (n2dim + CH - 1) / CH;
+    for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+        const long long n0 = ch * CH;
+        __syncthreads();
+        for (int e = t; e < 4 * na4 * CH; e += blockDim.x) {
+            int r = e / CH, c = e % CH;
+            bool ok = (r < na) && (n0 + c < n2dim);
+            sa[r * CHP + c] = ok ? J1[(long long)r * n2dim + n0 + c] : 0.0;
+        }
+        for (int e = t; e < 4 * nb4 * CH; e += blockDim.x) {
+            int r = e / CH, c = e % CH;
+            bool ok = (r < nb) && (n0 + c < n2dim);
+            double b = ok ? J2[(long long)r * n2dim + n0 + c] : 0.0;
+            double hr = ok ? hist[2 * (n0 + c)] : 0.0;
+            double hi = ok ? hist[2 * (n0 + c) + 1] : 0.0;
+            sb[r * CHP + c] = make_double2(b * hr, b * hi);
+        }
+        __syncthreads();
+        if (active) {
+            for (int c = grp; c < CH; c += ngroup) {
+                double av[4];
+                double2 bv[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) av[u] = sa[(4 * ta + u) * CHP + c];
+#pragma unroll
+                for (int v = 0; v < 4; v++) bv[v] = sb[(4 * tb + v) * CHP + c];
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int v = 0; v < 4; v++) {
+                        acc[u][v][0] += av[u] * bv[v].x;
+                        acc[u][v][1] += av[u] * bv[v].y;
+                    }
+            }
+        }
     }
     __syncthreads();
-    for (int o = threadIdx.x; o < nk * nk; o += blockDim.x) {
-        const int i1 = o / nk, i2 = o % nk;
-        const double *a = j1 + i1 * CP, *c = j2 + i2 * CP;
-        double sr = 0.0, si = 0.0;
-        for (int n = 0; n < len; n++) {
-            double jj = a[n] * c[n];
-            sr += jj * hr[n];
-            si += jj * hi[n];
+    double2 *red = reinterpret_cast<double2 *>(smem_raw);
+    for (int e = t; e < ntile * 16; e += blockDim.x) red[e] = make_double2(0.0, 0.0);
+    __syncthreads();
+    for (int g = 0; g < ngroup; g++) {
+        if (active && grp == g) {
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    double2 &r = red[tile * 16 + u * 4 + v];
+                    r.x += acc[u][v][0];
+                    r.y += acc[u][v][1];
+                }
         }
-        part[2 * ((long long)blockIdx.x * nk * nk + o)] = sr;
-        part[2 * ((long long)blockIdx.x * nk * nk + o) + 1] = si;
+        __syncthreads();
+    }
+    for (int e = t; e < na * nb; e += blockDim.x) {
+        int i1 = e / nb, i2 = e % nb;
+        double2 r = red[((i1 / 4) * nb4 + (i2 / 4)) * 16 + (i1 % 4) * 4 + (i2 % 4)];
+        part[2 * ((long long)blockIdx.x * na * nb + e)] = r.x;
+        part[2 * ((long long)blockIdx.x * na * nb + e) + 1] = r.y;
     }
 }
 
-__global__ void k_sn_reduce(const double *part, int nblk, int nk, double2 *out) {
-    int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= nk * nk) return;
-    double sr = 0.0, si = 0.0;
-    for (int b = 0; b < nblk; b++) {
-        sr += part[2 * ((long long)b * nk * nk + o)];
-        si += part[2 * ((long long)b * nk * nk + o) + 1];
-    }
-    out[o] = make_double2(sr, si);
-}
 
-inline size_t sn_partial_smem(int nk) { return sizeof(double) * ((size_t)2 * nk * (HG_SN_CHUNK + 1) + 2 * (HG_SN_CHUNK + 1)); }
+#define HG_SN_MAXROWS 64  // rows per operand and launch (4 x 4 tiles, at most 256 of them)
+inline size_t sn_partial_smem(int na, int nb) {
+    const size_t na4 = (size_t)(na + 3) / 4, nb4 = (size_t)(nb + 3) / 4;
+    size_t stage = (sizeof(double2) * nb4 + sizeof(double) * na4) * 4 * (HG_SN_CHUNK + 1);
+    size_t red = sizeof(double2) * 16 * na4 * nb4;
+    return stage > red ? stage : red;
+}
+inline int sn_partial_blocks(long long n2dim) {
+    long long nchunk = (n2dim + HG_SN_CHUNK - 1) / HG_SN_CHUNK;
+    return (int)std::min<long long>(nchunk, 2 * 148);
+}
 
 // ---------------------------------------------------------------- 3PCF (zeta)
 // Per-mode factor of the 3PCF filtered fields (field.hpp:403-445) without the Bessel weight:
@@ -498,6 +548,14 @@ struct LdMeshDelta {  // real density rho -> (rho - nbar) dV  (field.hpp:520-523
     T nbar, dV;
     __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
         return mk<T>((mesh[o * L + l] - nbar) * dV, (T)0);
+    }
+};
+template <typename T>
+struct LdPlanar {  // complex mesh held as separate re / im arrays (rows of L along the last axis)
+    const T *re, *im;
+    long long L;
+    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
+        return mk<T>(re[o * L + l], im[o * L + l]);
     }
 };
 template <typename T>

@@ -7,6 +7,7 @@ so the GPU tests need neither the reference sources nor the harness.
 
     python tests/golden/make_golden.py          (needs `make -C oracle` first)
     python tests/golden/make_golden.py --zeta   (only box_zeta.npz)
+    python tests/golden/make_golden.py --survey (only survey_pk.npz)
 """
 from __future__ import annotations
 
@@ -20,7 +21,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from hitomi_b200.api import Binning  # noqa: E402
-from hitomi_b200.synthetic import lognormal_box, uniform_box  # noqa: E402
+from hitomi_b200.synthetic import lognormal_box, survey_shell, uniform_box  # noqa: E402
 from oracle import ref_runner  # noqa: E402
 
 MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2))
@@ -96,11 +97,31 @@ def make_zeta():
     np.savez_compressed(os.path.join(HERE, "box_zeta.npz"), **d)
 
 
+def make_survey():
+    """Survey-geometry P_l (powerspec.hpp:4-91) and the survey scalars (main.cpp:150-200),
+    on a shell-and-cap catalogue; every assignment for l = 0, 2 and one scheme for all l."""
+    data, rand = survey_shell(3000, 60000, seed=16)
+    bs = Binning(0.004, 0.048, 12, 20.0, 140.0, 7)
+    d = dict(data=data, rand=rand, boxsize=3500.0, n_mesh=64, binning=binning_arr(bs))
+    for assign, ells in (("TSC", (0, 1, 2, 3, 4)), ("CIC", (0, 2)), ("NGP", (0, 2))):
+        for ell in ells:
+            with ref_runner.RefRun() as r:
+                r.run("pk", data, ell, 0, ell, 64, 3500.0, bs, assign=assign, randoms=rand)
+                d[f"pk_{assign}_{ell}"] = r.pk(ell)[1]
+                sc = r.survey_scalars()
+        for k, v in sc.items():
+            d[f"scalars_{assign}_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "survey_pk.npz"), **d)
+
+
 def main():
     if not ref_runner.available():
         raise SystemExit("build the oracle first: make -C oracle")
-    if "--zeta" in sys.argv:
-        make_zeta()
+    if "--zeta" in sys.argv or "--survey" in sys.argv:
+        if "--zeta" in sys.argv:
+            make_zeta()
+        if "--survey" in sys.argv:
+            make_survey()
         print("fixtures written")
         return
     # smoke case
@@ -153,6 +174,7 @@ def main():
             d[f"pk_{ell}"] = r.pk(ell)[1]
     np.savez_compressed(os.path.join(HERE, "box_noncubic.npz"), **d)
     make_zeta()
+    make_survey()
     print("fixtures written")
 
 
