@@ -11,6 +11,7 @@ the results back.  Both forms are measured: the chosen FP32 form (the headline) 
 plain FP64 form, with the per-bin relative difference between them.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--small]
+  python bench.py --lean --forms fp32 [--n-mesh M --n-particles P]   (profiling runs)
 Under torchrun every rank runs its own mocks (weak scaling, no data-path collective).
 """
 from __future__ import annotations
@@ -34,11 +35,15 @@ PK_ELLS = (0, 2, 4)
 MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2))
 
 
-def workload(small: bool):
+def workload(small: bool, n_mesh: int = 0, n_part: int = 0):
     from hitomi_b200.api import Binning
     if small:
         return dict(name="box P_l+B_l, 64^3 mesh, 2e5 particles (reduced check size)", n_mesh=64, boxsize=1000.0,
                     n_part=200_000, ngrid=64, binning=Binning(0.015, 0.255, 25))
+    if n_mesh or n_part:  # profiling cases: same statistics, other sizes (never the headline)
+        nm, npart = n_mesh or 512, n_part or 10_000_000
+        return dict(name=f"box P_l+B_l, {nm}^3 mesh, {npart} particles (profiling size)", n_mesh=nm,
+                    boxsize=1000.0, n_part=npart, ngrid=min(256, nm), binning=Binning(0.015, 0.255, 25))
     return dict(name="box P_l(l=0,2,4)+B_l(000,110,202,022), all k1,k2; 512^3 mesh, 1e7 particles, TSC", n_mesh=512,
                 boxsize=1000.0, n_part=10_000_000, ngrid=256, binning=Binning(0.015, 0.255, 25))
 
@@ -211,9 +216,14 @@ def main():
     ap.add_argument("--small", action="store_true", help="64^3 / 2e5-particle case for quick checks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--forms", default="fp32,fp64")
+    ap.add_argument("--lean", action="store_true",
+                    help="profiling runs: device-resident steps only (no e2e, per-kernel or CPU legs)")
+    ap.add_argument("--n-mesh", type=int, default=0, help="profiling size (not the headline workload)")
+    ap.add_argument("--n-particles", type=float, default=0, help="profiling size (not the headline workload)")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-    wl = workload(args.small)
+    if not args.lean:
+        args.warmup = max(args.warmup, 3)
+    wl = workload(args.small, args.n_mesh, int(args.n_particles))
     world, rank, local = dist_setup()
     if args.impl == "reference":
         rc = run_reference(args, wl, world, rank)
@@ -258,6 +268,10 @@ def main():
         barrier(world)
         ms = reduce_max(ev0.elapsed_time(ev1) / args.steps, world)
         results[form] = res
+        if args.lean:
+            timing[form] = dict(ms=ms, e2e_ms=ms, launches=launches // args.steps, clocks=clocks, stats={}, d2h=0)
+            ctx.close()
+            continue
         # ---- end to end through the public API with host buffers
         barrier(world)
         torch.cuda.synchronize()
@@ -325,7 +339,9 @@ def main():
     if os.environ.get("HG_BENCH_DUMP"):
         np.savez_compressed(os.environ["HG_BENCH_DUMP"], **{f"{form}:{'_'.join(map(str, k))}": v
                                                             for form in results for k, v in results[form].items()})
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if args.lean:
+        line["lean"] = "profiling run: e2e, per-kernel and CPU legs skipped"
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.lean:
         try:
             from oracle import cpu_baseline
             cb = cpu_baseline.baseline(pos, wl["n_mesh"], wl["boxsize"], wl["binning"], PK_ELLS, MULTIPOLES)

@@ -17,6 +17,14 @@ struct AxisTabs {
     const double *ts[3];
 };
 
+// Per-axis factors of the separable weights of the shot-noise correlation field:
+//   cf[i]  = the axis factor of C(k) for the assignment scheme (shot_tab's per-axis f),
+//   iw2[i] = 1 / (tw[i]^p)^2, so that 1 / W(k)^2 = iw2[x] iw2[y] iw2[z].
+struct XiTabs {
+    const double *cf[3];
+    const double *iw2[3];
+};
+
 
 __device__ __forceinline__ double window_tab(const AxisTabs &t, int ix, int iy, int iz, int p) {
     double ret = t.tw[0][ix] * t.tw[1][iy] * t.tw[2][iz];
@@ -41,23 +49,13 @@ __device__ __forceinline__ double shot_tab(const AxisTabs &t, int ix, int iy, in
 }
 
 // Read access to a transformed field, either a half spectrum [n0][n1][n2/2+1] of a real
-// input (negative kz by Hermitian symmetry) or a full [n0][n1][n2] spectrum.  With
-// mirror = 1 it reads sgn * conj(F(-k)): the field of the conjugate weights, e.g.
-// F_{l,-m}(k) = (-1)^m conj(F_{l,m}(-k)) since Yhat_{l,-m} = (-1)^m conj(Yhat_{l,m}).
+// input (negative kz by Hermitian symmetry) or a full [n0][n1][n2] spectrum.
 template <typename T>
 struct Spec {
     const cplx<T> *p;
     int n0, n1, n2;
     int half;
-    int mirror;
-    double sgn;
     __device__ __forceinline__ zd at(int ix, int iy, int iz) const {
-        if (mirror) {
-            Spec<T> d = *this;
-            d.mirror = 0;
-            zd v = d.at((n0 - ix) % n0, (n1 - iy) % n1, (n2 - iz) % n2);
-            return mk<double>(sgn * v.x, -sgn * v.y);
-        }
         if (!half) {
             cplx<T> v = p[((long long)ix * n1 + iy) * n2 + iz];
             return mk<double>((double)v.x, (double)v.y);
@@ -70,6 +68,18 @@ struct Spec {
         int jx = (n0 - ix) % n0, jy = (n1 - iy) % n1, jz = n2 - iz;
         cplx<T> v = p[((long long)jx * n1 + jy) * hz + jz];
         return mk<double>((double)v.x, -(double)v.y);
+    }
+};
+
+// sgn * conj(F(-k)): the transform of the conjugated weights, e.g.
+// F_{l,-m}(k) = (-1)^m conj(F_{l,m}(-k)) since Yhat_{l,-m} = (-1)^m conj(Yhat_{l,m}).
+template <typename T>
+struct SpecMirror {
+    Spec<T> s;
+    double sgn;
+    __device__ __forceinline__ zd at(int ix, int iy, int iz) const {
+        zd v = s.at((s.n0 - ix) % s.n0, (s.n1 - iy) % s.n1, (s.n2 - iz) % s.n2);
+        return mk<double>(sgn * v.x, -sgn * v.y);
     }
 };
 
@@ -86,8 +96,8 @@ struct LMList {
 
 // P-binning over the mode cube [lo, lo+cnt) (wrapped modes).  acc: [nbin][nlm] complex,
 // nmode: [nbin].  lut maps the fine index int(|k|/1e-4 + 0.5) to up to two coarse bins.
-template <typename T>
-__global__ void k_pk_bin(Spec<T> f1, Spec<T> f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt, const int2 *lut, int lutn,
+template <typename T, class F1, class F2>
+__global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt, const int2 *lut, int lutn,
                          int nbin, LMList lms, double S_re, double S_im, int assign, int wpow, double *acc,
                          unsigned long long *nmode, int k0_special, double k0_re, double k0_im) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -157,6 +157,8 @@ struct Engine : public hg_ctx {
     std::map<int, std::unique_ptr<DBuf>> tw;  // per line length
     DBuf tab_w[3], tab_s[3];
     AxisTabs tabs;
+    XiTabs xtabs;
+    DBuf tab_cf[3], tab_iw2[3];
     DBuf lut;
     int lutn = 0;
 
@@ -282,6 +284,13 @@ struct Engine : public hg_ctx {
             HG_CK(cudaGetLastError());
             tabs.tw[a] = dp<double>(tab_w[a]);
             tabs.ts[a] = dp<double>(tab_s[a]);
+            HG_CK(tab_cf[a].ensure(sizeof(double) * g.n[a]));
+            HG_CK(tab_iw2[a].ensure(sizeof(double) * g.n[a]));
+            k_xi_tables<<<grid1(g.n[a], 128), 128, 0, st>>>(g.n[a], tabs.tw[a], tabs.ts[a], c.assign, wpow,
+                                                            dp<double>(tab_cf[a]), dp<double>(tab_iw2[a]));
+            HG_CK(cudaGetLastError());
+            xtabs.cf[a] = dp<double>(tab_cf[a]);
+            xtabs.iw2[a] = dp<double>(tab_iw2[a]);
         }
         build_lut();
         HG_CK(cudaStreamSynchronize(st));
@@ -633,7 +642,8 @@ struct Engine : public hg_ctx {
                 std::vector<unsigned long long> &nm) {
         pk_bin2(half_spec(), half_spec(), lm, S_re, S_im, avg, nm);
     }
-    void pk_bin2(const Spec<T> &f1, const Spec<T> &f2, const std::vector<LM> &lm, double S_re, double S_im,
+    template <class F1>
+    void pk_bin2(const F1 &f1, const Spec<T> &f2, const std::vector<LM> &lm, double S_re, double S_im,
                  std::vector<double> &avg, std::vector<unsigned long long> &nm) {
         const int nbin = cfg.n_kbin;
         HG_REQUIRE((int)lm.size() <= HG_MAX_LM, "too many multipoles in one binning call");
@@ -660,11 +670,11 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(bin_acc.p, 0, sizeof(double) * 2 * nbin * L.n, st));
         HG_CK(cudaMemsetAsync(bin_cnt.p, 0, sizeof(unsigned long long) * nbin, st));
         size_t smem = sizeof(double) * 2 * nbin * L.n + sizeof(unsigned long long) * nbin;
-        HG_CK(cudaFuncSetAttribute(k_pk_bin<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        HG_CK(cudaFuncSetAttribute(k_pk_bin<T, F1, Spec<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         long long total = (long long)cn.x * cn.y * cn.z;
         unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 8);
         kb("pk_bin", double(total) * sizeof(C));
-        k_pk_bin<T><<<blocks, 256, smem, st>>>(f1, f2, g, tabs, lo, cn, dp<int2>(lut), lutn, nbin, L,
+        k_pk_bin<T, F1, Spec<T>><<<blocks, 256, smem, st>>>(f1, f2, g, tabs, lo, cn, dp<int2>(lut), lutn, nbin, L,
                                                S_re, S_im, cfg.assign, wpow, dp<double>(bin_acc),
                                                dp<unsigned long long>(bin_cnt), 0, 0.0, 0.0);
         ke();
@@ -985,10 +995,10 @@ struct Engine : public hg_ctx {
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
         const double S = double(slot[0].n);
-        LdXiHat<T> ld{half_spec(), g, tabs, cfg.assign, wpow, S, 0.0, delta0 * N0, 0.0, invV};
+        LdXiHat<T> ld{half_spec(), g.n[2], xtabs, S, delta0 * N0, invV};
         long long yz = (long long)g.n[1] * g.n[2];
-        pass_smem<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
-                      double(g.ntot) * sizeof(C) * 1.5);
+        pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
+                 double(g.ntot) * sizeof(C) * 1.5);
         pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
                  "fft_xi_y");
         xi_valid = true;
@@ -1675,7 +1685,7 @@ struct Engine : public hg_ctx {
         auto key = std::make_pair(l, m);
         auto &pb = sfield[key];
         if (!pb) pb = std::make_unique<DBuf>();
-        Spec<T> sp{dp<C>(*pb), g.n[0], g.n[1], g.n[2], real ? 1 : 0, 0, 1.0};
+        Spec<T> sp{dp<C>(*pb), g.n[0], g.n[1], g.n[2], real ? 1 : 0};
         if (sfield_ok.count(key)) return sp;
         const long long fsz = real ? (long long)g.n[0] * g.n[1] * hz : g.ntot;
         HG_CK(pb->ensure(sizeof(C) * fsz));
@@ -1736,11 +1746,9 @@ struct Engine : public hg_ctx {
             const int am = M < 0 ? -M : M;
             double Sr = sD[2 * am] + alpha * alpha * sR[2 * am];
             double Si = sD[2 * am + 1] + alpha * alpha * sR[2 * am + 1];
-            Spec<T> f1 = survey_field(ell, am, alpha);
+            const Spec<T> f1 = survey_field(ell, am, alpha);
+            const double sg = (am % 2) ? -1.0 : 1.0;
             if (M < 0) {  // dn_{l,-|M|}(k) = (-1)^|M| conj(dn_{l,|M|}(-k)); likewise S
-                const double sg = (am % 2) ? -1.0 : 1.0;
-                f1.mirror = 1;
-                f1.sgn = sg;
                 Sr = sg * Sr;
                 Si = -sg * Si;
             }
@@ -1749,7 +1757,10 @@ struct Engine : public hg_ctx {
                 w *= double(2 * ell + 1) * double(2 * ell + 1);
                 if (std::fabs(w) < 1.0e-10) continue;
                 std::vector<double> avg;
-                pk_bin2(f1, f00, {LM{ell, m1}}, Sr, Si, avg, nm);
+                if (M < 0)
+                    pk_bin2(SpecMirror<T>{f1, sg}, f00, {LM{ell, m1}}, Sr, Si, avg, nm);
+                else
+                    pk_bin2(f1, f00, {LM{ell, m1}}, Sr, Si, avg, nm);
                 for (int i = 0; i < nb; i++) {
                     acc[2 * i] += w * avg[2 * i];
                     acc[2 * i + 1] += w * avg[2 * i + 1];

@@ -20,6 +20,21 @@
 
 namespace hg {
 
+__global__ void k_xi_tables(int n, const double *tw, const double *ts, int assign, int wpow, double *cf,
+                            double *iw2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s2 = ts[i] * ts[i];
+    double f = 1.0;
+    if (assign == 1) f = 1.0 - (2.0 / 3.0) * s2;
+    else if (assign == 2) f = 1.0 - s2 + 2.0 * (s2 * s2) / 15.0;
+    else if (assign == 3) f = 1.0 - (4.0 / 3.0) * s2 + (2.0 / 5.0) * s2 * s2 - (4.0 / 315.0) * s2 * s2 * s2;
+    cf[i] = f;
+    double w = tw[i];
+    for (int q = 1; q < wpow; q++) w *= tw[i];
+    iw2[i] = 1.0 / (w * w);
+}
+
 __global__ void k_axis_tables(Grid g, int axis, double *tw, double *ts) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = g.n[axis];
@@ -142,30 +157,27 @@ __global__ void k_pair_dot_cube(const int *start, const ShellEnt *ent, const dou
 //   xi(x) = (1/V) sum_k (f1 conj f2 - S C(k)) / W(k)^2 e^{ikx}   (field.hpp:1116-1160)
 // synthesising the k-space input from the half spectrum on the fly.
 template <typename T>
-struct LdXiHat {
+struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), separable tables
     Spec<T> f;
-    Grid g;
-    AxisTabs tabs;
-    int assign, wpow;
-    double S_re, S_im;
-    double k0_re, k0_im;  // (f1 conj f2)(k = 0) from the FP64 field integrals
+    int n2;
+    XiTabs xt;
+    double S;
+    double k0;  // (f1 conj f2)(k = 0) from the FP64 field integrals
     double invV;
     __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
         int ix = l;
-        int iy = (int)(i / g.n[2]);
-        int iz = (int)(i - (long long)iy * g.n[2]);
-        zd pk2;
+        int iy = (int)(i / n2);
+        int iz = (int)(i - (long long)iy * n2);
+        double p2;
         if (ix == 0 && iy == 0 && iz == 0) {
-            pk2 = mk<double>(k0_re, k0_im);
+            p2 = k0;
         } else {
             zd d = f.at(ix, iy, iz);
-            pk2 = d * conjg(d);
+            p2 = d.x * d.x + d.y * d.y;
         }
-        double C = shot_tab(tabs, ix, iy, iz, assign);
-        pk2 = pk2 - mk<double>(S_re * C, S_im * C);
-        double wf = window_tab(tabs, ix, iy, iz, wpow);
-        double w2 = wf * wf;
-        return mk<T>((T)(invV * (pk2.x / w2)), (T)(invV * (pk2.y / w2)));
+        double C = xt.cf[0][ix] * xt.cf[1][iy] * xt.cf[2][iz];
+        double iw = xt.iw2[0][ix] * xt.iw2[1][iy] * xt.iw2[2][iz];
+        return mk<T>((T)(invV * ((p2 - S * C) * iw)), (T)0);
     }
 };
 

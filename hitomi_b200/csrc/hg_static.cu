@@ -161,11 +161,11 @@ int run(const hg_config &c, const void *spec, long long n_particles, int ell, do
     lms.lm[0] = LM{ell, 0};
     Spec<T> f{reinterpret_cast<const cplx<T> *>(spec), g.n[0], g.n[1], g.n[2], 1};
     size_t smem = sizeof(double) * 2 * nbin + sizeof(unsigned long long) * nbin;
-    cudaFuncSetAttribute(k_pk_bin<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_pk_bin<T, Spec<T>, Spec<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     long long total = (long long)cn.x * cn.y * cn.z;
     unsigned blocks = (unsigned)std::min<long long>((total + 255) / 256, 148 * 8);
     const int wpow = c.assign + 1;
-    k_pk_bin<T><<<blocks, 256, smem, st>>>(f, f, g, tabs, lo, cn, lut, n_fine, nbin, lms, double(n_particles), 0.0,
+    k_pk_bin<T, Spec<T>, Spec<T>><<<blocks, 256, smem, st>>>(f, f, g, tabs, lo, cn, lut, n_fine, nbin, lms, double(n_particles), 0.0,
                                            c.assign, wpow, acc, cnt, 0, 0.0, 0.0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(std::string("binning launch: ") + cudaGetErrorString(e));
