@@ -15,15 +15,42 @@ namespace hg {
 struct AxisTabs {
     const double *tw[3];
     const double *ts[3];
+    const double *tc[3];  // cos(pi w / n); needed only when interlace != 0
+    int interlace;
 };
 
 // Per-axis factors of the separable weights of the shot-noise correlation field:
 //   cf[i]  = the axis factor of C(k) for the assignment scheme (shot_tab's per-axis f),
+//   df[i]  = the axis factor of the alternating image sum (interlacing only),
 //   iw2[i] = 1 / (tw[i]^p)^2, so that 1 / W(k)^2 = iw2[x] iw2[y] iw2[z].
 struct XiTabs {
     const double *cf[3];
+    const double *df[3];
     const double *iw2[3];
+    int interlace;
 };
+
+// Per-axis aliasing sums of W^2 over the images k + 2 k_N n (s = sin, c = cos of pi k / 2 k_N):
+//   C_p = sum_n W_p^2        (Jing 2005 eq. 20; PCS from the same sum):
+//         1, 1 - 2/3 s^2, 1 - s^2 + 2/15 s^4, 1 - 4/3 s^2 + 2/5 s^4 - 4/315 s^6
+//   D_p = sum_n (-1)^n W_p^2 (closed form of the alternating sum of sinc^2p):
+//         c, c (c^2 + 5) / 6, c (c^4 + 58 c^2 + 61) / 120, c (c^6 + 543 c^4 + 3111 c^2 + 1385) / 5040
+// Interlacing two fields offset by half a cell keeps only the images with even n_x+n_y+n_z,
+// so its shot-noise function is C_int = (prod_a C_a + prod_a D_a) / 2.
+__host__ __device__ __forceinline__ double alias_c(int assign, double sn) {
+    double s2 = sn * sn;
+    if (assign == 0) return 1.0;
+    if (assign == 1) return 1.0 - (2.0 / 3.0) * s2;
+    if (assign == 2) return 1.0 - s2 + 2.0 * (s2 * s2) / 15.0;
+    return 1.0 - (4.0 / 3.0) * s2 + (2.0 / 5.0) * s2 * s2 - (4.0 / 315.0) * s2 * s2 * s2;
+}
+__host__ __device__ __forceinline__ double alias_d(int assign, double c) {
+    double c2 = c * c;
+    if (assign == 0) return c;
+    if (assign == 1) return c * (c2 + 5.0) / 6.0;
+    if (assign == 2) return c * (c2 * c2 + 58.0 * c2 + 61.0) / 120.0;
+    return c * (c2 * c2 * c2 + 543.0 * c2 * c2 + 3111.0 * c2 + 1385.0) / 5040.0;
+}
 
 
 __device__ __forceinline__ double window_tab(const AxisTabs &t, int ix, int iy, int iz, int p) {
@@ -34,6 +61,9 @@ __device__ __forceinline__ double window_tab(const AxisTabs &t, int ix, int iy, 
 }
 
 __device__ __forceinline__ double shot_tab(const AxisTabs &t, int ix, int iy, int iz, int assign) {
+    if (t.interlace)
+        return 0.5 * (alias_c(assign, t.ts[0][ix]) * alias_c(assign, t.ts[1][iy]) * alias_c(assign, t.ts[2][iz]) +
+                      alias_d(assign, t.tc[0][ix]) * alias_d(assign, t.tc[1][iy]) * alias_d(assign, t.tc[2][iz]));
     if (assign == 0) return 1.0;
     const double s[3] = {t.ts[0][ix], t.ts[1][iy], t.ts[2][iz]};
     double ret = 1.0;

@@ -155,10 +155,10 @@ struct Engine : public hg_ctx {
 
     // tables
     std::map<int, std::unique_ptr<DBuf>> tw;  // per line length
-    DBuf tab_w[3], tab_s[3];
+    DBuf tab_w[3], tab_s[3], tab_c[3];
     AxisTabs tabs;
     XiTabs xtabs;
-    DBuf tab_cf[3], tab_iw2[3];
+    DBuf tab_cf[3], tab_df[3], tab_iw2[3];
     DBuf lut;
     int lutn = 0;
 
@@ -168,6 +168,7 @@ struct Engine : public hg_ctx {
     // fields
     DBuf mesh;  // real density rho (box)
     DBuf H;     // half spectrum of dV (rho - nbar)
+    DBuf H2;    // half spectrum of the half-cell shifted assignment (interlacing)
     bool dens_valid = false;
     double dens_mass = 0.0;  // sum_cells rho  (FP64)
     double delta0 = 0.0, N0 = 0.0;
@@ -212,7 +213,7 @@ struct Engine : public hg_ctx {
     DBuf hist_tmp, snmat, snblk, sn_part, d_kv;
 
     // survey state (per pair of catalogues)
-    DBuf smesh_re, smesh_im, dmesh, psum_part;
+    DBuf smesh_re, smesh_im, dmesh, psum_part, sfield_tmp;
     std::map<std::pair<int, int>, std::unique_ptr<DBuf>> sfield;  // (l, m >= 0) -> spectrum of D - alpha R
     std::set<std::pair<int, int>> sfield_ok;
     double sfield_alpha = 0.0;
@@ -264,7 +265,6 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(c.assign >= 0 && c.assign <= 3, "assignment must be NGP, CIC, TSC or PCS");
         HG_REQUIRE(c.n_kbin >= 2 && c.kmax > c.kmin && c.kmin > 0.0, "need n_kbin >= 2 and 0 < kmin < kmax");
         HG_REQUIRE(c.n_rbin >= 2 && c.rmax > c.rmin && c.rmin > 0.0, "need n_rbin >= 2 and 0 < rmin < rmax");
-        HG_REQUIRE(c.interlace == 0, "interlacing is not available in this build");
         g.volume = c.boxsize[0] * c.boxsize[1] * c.boxsize[2];
         g.ntot = (long long)c.n_mesh[0] * c.n_mesh[1] * c.n_mesh[2];
         wpow = c.assign + 1;
@@ -277,19 +277,29 @@ struct Engine : public hg_ctx {
         HG_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         HG_CK(cudaEventCreate(&ev0));
         HG_CK(cudaEventCreate(&ev1));
+        // the schemes the reference does not have use the exact window index and periodic wrap
+        const int exact = (c.interlace || c.assign == HG_PCS) ? 1 : 0;
+        tabs.interlace = c.interlace ? 1 : 0;
+        xtabs.interlace = tabs.interlace;
         for (int a = 0; a < 3; a++) {
             HG_CK(tab_w[a].ensure(sizeof(double) * g.n[a]));
             HG_CK(tab_s[a].ensure(sizeof(double) * g.n[a]));
-            k_axis_tables<<<grid1(g.n[a], 128), 128, 0, st>>>(g, a, dp<double>(tab_w[a]), dp<double>(tab_s[a]));
+            HG_CK(tab_c[a].ensure(sizeof(double) * g.n[a]));
+            k_axis_tables<<<grid1(g.n[a], 128), 128, 0, st>>>(g, a, exact, dp<double>(tab_w[a]), dp<double>(tab_s[a]),
+                                                              dp<double>(tab_c[a]));
             HG_CK(cudaGetLastError());
             tabs.tw[a] = dp<double>(tab_w[a]);
             tabs.ts[a] = dp<double>(tab_s[a]);
+            tabs.tc[a] = dp<double>(tab_c[a]);
             HG_CK(tab_cf[a].ensure(sizeof(double) * g.n[a]));
+            HG_CK(tab_df[a].ensure(sizeof(double) * g.n[a]));
             HG_CK(tab_iw2[a].ensure(sizeof(double) * g.n[a]));
-            k_xi_tables<<<grid1(g.n[a], 128), 128, 0, st>>>(g.n[a], tabs.tw[a], tabs.ts[a], c.assign, wpow,
-                                                            dp<double>(tab_cf[a]), dp<double>(tab_iw2[a]));
+            k_xi_tables<<<grid1(g.n[a], 128), 128, 0, st>>>(g.n[a], tabs.tw[a], tabs.ts[a], tabs.tc[a], c.assign, wpow,
+                                                            dp<double>(tab_cf[a]), dp<double>(tab_df[a]),
+                                                            dp<double>(tab_iw2[a]));
             HG_CK(cudaGetLastError());
             xtabs.cf[a] = dp<double>(tab_cf[a]);
+            xtabs.df[a] = dp<double>(tab_df[a]);
             xtabs.iw2[a] = dp<double>(tab_iw2[a]);
         }
         build_lut();
@@ -492,7 +502,7 @@ struct Engine : public hg_ctx {
         }
         a.ntot = g.ntot;
         a.scheme = cfg.assign;
-        a.periodic = (cfg.periodic || cfg.assign == HG_PCS) ? 1 : 0;
+        a.periodic = (cfg.periodic || cfg.assign == HG_PCS || cfg.interlace) ? 1 : 0;
         a.shift = shift;
         const int tdef[3] = {8, 16, 32};
         for (int q = 0; q < 3; q++) {
@@ -601,6 +611,26 @@ struct Engine : public hg_ctx {
     }
 
     // Box density contrast, forward transformed: H = FFT[dV (rho - N/V)] (half spectrum).
+    // r2c transform of a real mesh into the half spectrum Hd: FFT[(mesh - sub) scl]
+    void forward_real(const T *m, C *Hd, T sub, T scl, const char *name) {
+        const int hz = g.n[2] / 2 + 1;
+        pass<-1>(g.n[2], LdMeshDelta<T>{m, g.n[2], sub, scl}, StHalf<T>{Hd, g.n[2], hz}, (long long)g.n[0] * g.n[1], 1,
+                 name, double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
+        pass<-1>(g.n[1], LdArr<T>{Hd, g.n[1], hz}, StArr<T>{Hd, g.n[1], hz}, g.n[0], hz, name);
+        pass<-1>(g.n[0], LdArr<T>{Hd, g.n[0], (long long)g.n[1] * hz}, StArr<T>{Hd, g.n[0], (long long)g.n[1] * hz}, 1,
+                 (long long)g.n[1] * hz, name);
+    }
+
+    // F = (F + phase * Fs) / 2 over a half (half = 1) or full spectrum
+    void interlace_combine(C *F, const C *Fs, bool half) {
+        const int nzs = half ? g.n[2] / 2 + 1 : g.n[2];
+        const long long tot = (long long)g.n[0] * g.n[1] * nzs;
+        unsigned blocks = (unsigned)std::min<long long>(grid1(tot, 256), 148 * 16);
+        kb("interlace_combine", double(tot) * sizeof(C) * 3.0);
+        k_interlace<T><<<blocks, 256, 0, st>>>(F, Fs, g.n[0], g.n[1], g.n[2], nzs, half ? 1 : 0);
+        ke();
+    }
+
     void box_density() {
         if (dens_valid) return;
         Slot &S = slot[0];
@@ -616,12 +646,14 @@ struct Engine : public hg_ctx {
         const bool mass_mesh = (sizeof(T) == 4);
         const T sub = mass_mesh ? (T)(double(S.n) / double(g.ntot)) : (T)nbar;
         const T scl = mass_mesh ? (T)1 : (T)dV;
-        pass<-1>(g.n[2], LdMeshDelta<T>{dp<T>(mesh), g.n[2], sub, scl}, StHalf<T>{dp<C>(H), g.n[2], hz},
-                 (long long)g.n[0] * g.n[1], 1, "fft_density_r2c_z",
-                 double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
-        pass<-1>(g.n[1], LdArr<T>{dp<C>(H), g.n[1], hz}, StArr<T>{dp<C>(H), g.n[1], hz}, g.n[0], hz, "fft_density_yx");
-        pass<-1>(g.n[0], LdArr<T>{dp<C>(H), g.n[0], (long long)g.n[1] * hz},
-                 StArr<T>{dp<C>(H), g.n[0], (long long)g.n[1] * hz}, 1, (long long)g.n[1] * hz, "fft_density_yx");
+        forward_real(dp<T>(mesh), dp<C>(H), sub, scl, "fft_density");
+        if (cfg.interlace) {  // second assignment half a cell along every axis, combined in k space
+            const double m1 = assign_real(src, make_geom(0.5), dp<T>(mesh));
+            HG_CK(H2.ensure(sizeof(C) * (size_t)g.n[0] * g.n[1] * hz));
+            forward_real(dp<T>(mesh), dp<C>(H2), sub, scl, "fft_density");
+            interlace_combine(dp<C>(H), dp<C>(H2), true);
+            dens_mass = 0.5 * (dens_mass + m1);
+        }
         // k = 0 from the FP64 integral: sum_c (rho_c - nbar) dV
         delta0 = (dens_mass - nbar * double(g.ntot)) * dV;
         N0 = dens_mass * dV;
@@ -1690,28 +1722,31 @@ struct Engine : public hg_ctx {
         const long long fsz = real ? (long long)g.n[0] * g.n[1] * hz : g.ntot;
         HG_CK(pb->ensure(sizeof(C) * fsz));
         sp.p = dp<C>(*pb);
-        AssignGeom ag = make_geom(0.0);
-        ag.acc_factor = 1.0;  // mass units: dV rho, the transform's input
         const bool ylm = !(l == 0 && m == 0);
         std::vector<PartSrc> srcs{survey_src(0, ylm, l, m, 1.0), survey_src(1, ylm, l, m, -alpha)};
         HG_CK(smesh_re.ensure(sizeof(T) * g.ntot));
-        C *F = dp<C>(*pb);
-        if (real) {
-            assign_mesh<T, false>(srcs, ag, dp<T>(smesh_re), nullptr, false);
-            pass<-1>(g.n[2], LdMeshDelta<T>{dp<T>(smesh_re), g.n[2], (T)0, (T)1}, StHalf<T>{F, g.n[2], hz},
-                     (long long)g.n[0] * g.n[1], 1, "fft_survey",
-                     double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
-            pass<-1>(g.n[1], LdArr<T>{F, g.n[1], hz}, StArr<T>{F, g.n[1], hz}, g.n[0], hz, "fft_survey");
-            pass<-1>(g.n[0], LdArr<T>{F, g.n[0], (long long)g.n[1] * hz}, StArr<T>{F, g.n[0], (long long)g.n[1] * hz},
-                     1, (long long)g.n[1] * hz, "fft_survey");
-        } else {
-            HG_CK(smesh_im.ensure(sizeof(T) * g.ntot));
-            assign_mesh<T, true>(srcs, ag, dp<T>(smesh_re), dp<T>(smesh_im), false);
-            const long long yz = (long long)g.n[1] * g.n[2];
-            pass<-1>(g.n[2], LdPlanar<T>{dp<T>(smesh_re), dp<T>(smesh_im), g.n[2]}, StArr<T>{F, g.n[2], 1},
-                     (long long)g.n[0] * g.n[1], 1, "fft_survey", double(g.ntot) * (2 * sizeof(T) + sizeof(C)));
-            pass<-1>(g.n[1], LdArr<T>{F, g.n[1], g.n[2]}, StArr<T>{F, g.n[1], g.n[2]}, g.n[0], g.n[2], "fft_survey");
-            pass<-1>(g.n[0], LdArr<T>{F, g.n[0], yz}, StArr<T>{F, g.n[0], yz}, 1, yz, "fft_survey");
+        if (!real) HG_CK(smesh_im.ensure(sizeof(T) * g.ntot));
+        // assign (mass units: dV rho, the transform's input) with a shift, transform into F
+        auto build = [&](double shift, C *F) {
+            AssignGeom ag = make_geom(shift);
+            ag.acc_factor = 1.0;
+            if (real) {
+                assign_mesh<T, false>(srcs, ag, dp<T>(smesh_re), nullptr, false);
+                forward_real(dp<T>(smesh_re), F, (T)0, (T)1, "fft_survey");
+            } else {
+                assign_mesh<T, true>(srcs, ag, dp<T>(smesh_re), dp<T>(smesh_im), false);
+                const long long yz = (long long)g.n[1] * g.n[2];
+                pass<-1>(g.n[2], LdPlanar<T>{dp<T>(smesh_re), dp<T>(smesh_im), g.n[2]}, StArr<T>{F, g.n[2], 1},
+                         (long long)g.n[0] * g.n[1], 1, "fft_survey", double(g.ntot) * (2 * sizeof(T) + sizeof(C)));
+                pass<-1>(g.n[1], LdArr<T>{F, g.n[1], g.n[2]}, StArr<T>{F, g.n[1], g.n[2]}, g.n[0], g.n[2], "fft_survey");
+                pass<-1>(g.n[0], LdArr<T>{F, g.n[0], yz}, StArr<T>{F, g.n[0], yz}, 1, yz, "fft_survey");
+            }
+        };
+        build(0.0, dp<C>(*pb));
+        if (cfg.interlace) {
+            HG_CK(sfield_tmp.ensure(sizeof(C) * fsz));
+            build(0.5, dp<C>(sfield_tmp));
+            interlace_combine(dp<C>(*pb), dp<C>(sfield_tmp), real);
         }
         sfield_ok.insert(key);
         return sp;

@@ -20,29 +20,52 @@
 
 namespace hg {
 
-__global__ void k_xi_tables(int n, const double *tw, const double *ts, int assign, int wpow, double *cf,
-                            double *iw2) {
+__global__ void k_xi_tables(int n, const double *tw, const double *ts, const double *tc, int assign, int wpow,
+                            double *cf, double *df, double *iw2) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    double s2 = ts[i] * ts[i];
-    double f = 1.0;
-    if (assign == 1) f = 1.0 - (2.0 / 3.0) * s2;
-    else if (assign == 2) f = 1.0 - s2 + 2.0 * (s2 * s2) / 15.0;
-    else if (assign == 3) f = 1.0 - (4.0 / 3.0) * s2 + (2.0 / 5.0) * s2 * s2 - (4.0 / 315.0) * s2 * s2 * s2;
-    cf[i] = f;
+    cf[i] = alias_c(assign, ts[i]);
+    df[i] = alias_d(assign, tc[i]);
     double w = tw[i];
     for (int q = 1; q < wpow; q++) w *= tw[i];
     iw2[i] = 1.0 / (w * w);
 }
 
-__global__ void k_axis_tables(Grid g, int axis, double *tw, double *ts) {
+// Per-axis window / shot-noise tables.  exact = 0: the reference's window index (n + 1 for
+// negative modes, field.hpp:667-669); exact = 1: the mode index itself, used by the schemes
+// the reference does not have (PCS, interlacing).
+__global__ void k_axis_tables(Grid g, int axis, int exact, double *tw, double *ts, double *tc) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int n = g.n[axis];
     if (i >= n) return;
     double kv = kcomp(wrap_index(i, n), g.dk[axis]);
-    int w = window_index(kv, g.dk[axis]);
+    int w = exact ? wrap_index(i, n) : window_index(kv, g.dk[axis]);
     tw[i] = sinc_axis(w, n);
     ts[i] = (w != 0) ? sin(HG_PI * (double)w / (double)n) : 0.0;
+    tc[i] = (w != 0) ? cos(HG_PI * (double)w / (double)n) : 1.0;
+}
+
+// Interlacing (half-cell shifted second assignment): F = (F_0 + e^{i pi (nx/Nx + ny/Ny + nz/Nz)} F_s) / 2
+// over a half spectrum (nz = iz) or a full one (nz wrapped).  The shifted catalogue sits at
+// x + dr/2, so its transform carries e^{-i k dr/2}; the phase undoes it.
+template <typename T>
+__global__ void k_interlace(cplx<T> *F, const cplx<T> *Fs, int n0, int n1, int n2, int nzs, int half) {
+    const long long total = (long long)n0 * n1 * nzs;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int iz = (int)(idx % nzs);
+        int iy = (int)((idx / nzs) % n1);
+        int ix = (int)(idx / ((long long)nzs * n1));
+        int nz = half ? iz : wrap_index(iz, n2);
+        double q = (double)wrap_index(ix, n0) / n0 + (double)wrap_index(iy, n1) / n1 + (double)nz / n2;
+        double sn, cs;
+        sincospi(q, &sn, &cs);
+        cplx<T> a = F[idx], b = Fs[idx];
+        double br = (double)b.x, bi = (double)b.y;
+        double re = 0.5 * ((double)a.x + (cs * br - sn * bi));
+        double im = 0.5 * ((double)a.y + (cs * bi + sn * br));
+        F[idx] = mk<T>((T)re, (T)im);
+    }
 }
 
 // Shell entries: wrapped mode (nx, ny, nz) and shell index.
@@ -176,6 +199,7 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
             p2 = d.x * d.x + d.y * d.y;
         }
         double C = xt.cf[0][ix] * xt.cf[1][iy] * xt.cf[2][iz];
+        if (xt.interlace) C = 0.5 * (C + xt.df[0][ix] * xt.df[1][iy] * xt.df[2][iz]);
         double iw = xt.iw2[0][ix] * xt.iw2[1][iy] * xt.iw2[2][iz];
         return mk<T>((T)(invV * ((p2 - S * C) * iw)), (T)0);
     }

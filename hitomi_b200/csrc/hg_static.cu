@@ -137,7 +137,9 @@ int run(const hg_config &c, const void *spec, long long n_particles, int ell, do
     double *tab = reinterpret_cast<double *>(base + kOffTab);
     int2 *lut = reinterpret_cast<int2 *>(base + kOffLut);
     AxisTabs tabs;
+    tabs.interlace = 0;
     for (int a = 0; a < 3; a++) {
+        tabs.tc[a] = nullptr;
         tabs.tw[a] = tab + (2 * a) * HG_STATIC_MAX_MESH;
         tabs.ts[a] = tab + (2 * a + 1) * HG_STATIC_MAX_MESH;
         k_static_axis_tables<<<(g.n[a] + 127) / 128, 128, 0, st>>>(g, a, tab + (2 * a) * HG_STATIC_MAX_MESH,
@@ -203,7 +205,8 @@ extern "C" int hg_pk_box_spectrum_static(const hg_config *cfg, const void *d_hal
             return fail("hg_pk_box_spectrum_static: n_mesh must be in [2, 1024] on every axis");
         if (!(c.boxsize[a] > 0.0)) return fail("hg_pk_box_spectrum_static: boxsize must be > 0");
     }
-    if (c.assign < 0 || c.assign > 3) return fail("hg_pk_box_spectrum_static: unknown assignment");
+    if (c.assign < 0 || c.assign > 2 || c.interlace)
+        return fail("hg_pk_box_spectrum_static: assignment must be NGP, CIC or TSC without interlacing");
     if (n_particles <= 0) return fail("hg_pk_box_spectrum_static: n_particles must be > 0");
     if (ell < 0) return fail("hg_pk_box_spectrum_static: ell must be >= 0");
     {

@@ -8,6 +8,8 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py          (needs `make -C oracle` first)
     python tests/golden/make_golden.py --zeta   (only box_zeta.npz)
     python tests/golden/make_golden.py --survey (only survey_pk.npz)
+    python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
+        interlacing, from the numpy restatement oracle/restate.py; no harness needed)
 """
 from __future__ import annotations
 
@@ -114,7 +116,36 @@ def make_survey():
     np.savez_compressed(os.path.join(HERE, "survey_pk.npz"), **d)
 
 
+def make_extensions():
+    """PCS assignment and interlacing are not in the reference: their fixtures come from
+    the numpy restatement oracle/restate.py, which tests/test_oracle_restate.py pins to the
+    reference's own outputs for NGP/CIC/TSC."""
+    from oracle import restate as R
+    pos = lognormal_box(15000, 1000.0, ngrid=32, seed=17, exact_n=15000)
+    bp = Binning(0.005, 0.295, 30, 4.0, 156.0, 20)
+    kb = R.bins(bp.kmin, bp.kmax, bp.n_kbin)
+    d = dict(pos=pos, boxsize=1000.0, n_mesh=32, binning=binning_arr(bp))
+    cases = (("PCS", False), ("PCS", True), ("TSC", True), ("CIC", True), ("NGP", True))
+    for assign, il in cases:
+        for ell in (0, 2, 4):
+            pk, nm, norm = R.pk_box(pos, 32, 1000.0, kb, ell, R.SCHEMES[assign], interlace=il)
+            d[f"pk_{assign}_{int(il)}_{ell}"] = norm * pk
+            d[f"nmode_{assign}_{int(il)}"] = nm
+    bb = Binning(0.015, 0.075, 7, 4.0, 156.0, 20)
+    kb = R.bins(bb.kmin, bb.kmax, bb.n_kbin)
+    d["bk_binning"] = binning_arr(bb)
+    for assign, il in (("PCS", True), ("TSC", True), ("PCS", False)):
+        for mp in ((0, 0, 0), (1, 1, 0), (2, 0, 2)):
+            bk, sn, norm = R.bk_box(pos, 32, 1000.0, kb, *mp, R.SCHEMES[assign], interlace=il)
+            d[f"bk_{assign}_{int(il)}_" + "".join(map(str, mp))] = norm * (bk - sn)
+    np.savez_compressed(os.path.join(HERE, "box_extensions.npz"), **d)
+
+
 def main():
+    if "--extensions" in sys.argv:
+        make_extensions()
+        print("fixtures written")
+        return
     if not ref_runner.available():
         raise SystemExit("build the oracle first: make -C oracle")
     if "--zeta" in sys.argv or "--survey" in sys.argv:
@@ -175,6 +206,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "box_noncubic.npz"), **d)
     make_zeta()
     make_survey()
+    make_extensions()
     print("fixtures written")
 
 
