@@ -23,6 +23,10 @@ SYMBOLS = (
     "hg_bk_box_multi",
     "hg_zeta_box",
     "hg_zeta_box_multi",
+    "hg_bk_survey",
+    "hg_bk_survey_multi",
+    "hg_zeta_survey",
+    "hg_zeta_survey_multi",
     "hg_survey_scalars",
     "hg_pk_survey",
     "hg_set_profiling",
@@ -93,6 +97,15 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_zeta_box.restype = ctypes.c_int
     lib.hg_zeta_box_multi.argtypes = [vp, ctypes.c_int, c_ip, ctypes.c_int, c_dp, c_dp, c_dp]
     lib.hg_zeta_box_multi.restype = ctypes.c_int
+    i_, d_ = ctypes.c_int, ctypes.c_double
+    lib.hg_bk_survey.argtypes = [vp, i_, i_, i_, i_, d_, d_, c_dp, c_dp, c_dp]
+    lib.hg_bk_survey.restype = ctypes.c_int
+    lib.hg_bk_survey_multi.argtypes = [vp, i_, c_ip, i_, d_, d_, c_dp, c_dp, c_dp]
+    lib.hg_bk_survey_multi.restype = ctypes.c_int
+    lib.hg_zeta_survey.argtypes = lib.hg_bk_survey.argtypes
+    lib.hg_zeta_survey.restype = ctypes.c_int
+    lib.hg_zeta_survey_multi.argtypes = lib.hg_bk_survey_multi.argtypes
+    lib.hg_zeta_survey_multi.restype = ctypes.c_int
     lib.hg_survey_scalars.argtypes = [vp, c_dp, c_dp, c_dp, c_dp, c_dp]
     lib.hg_survey_scalars.restype = ctypes.c_int
     lib.hg_pk_survey.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, c_dp, c_ip, c_dp]

@@ -193,6 +193,36 @@ class Context:
         c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nr)
         return c(z), c(sn), norm.value
 
+    def _survey_three_point(self, fn, nbins, multipoles, ith, alpha, vsurvey):
+        rows = nbins if ith < 0 else 1
+        m = len(multipoles)
+        ells = np.array([v for mp in multipoles for v in mp], dtype=np.int32)
+        a = np.zeros(2 * m * rows * nbins)
+        sn = np.zeros(2 * m * rows * nbins)
+        norm = ctypes.c_double()
+        self._check(fn(self._h, m, ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ith, float(alpha),
+                       float(vsurvey), _dp(a), _dp(sn), ctypes.byref(norm)))
+        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nbins)
+        return c(a), c(sn), norm.value
+
+    def bk_survey_multi(self, multipoles, alpha: float, vsurvey: float, ith_kbin: int = -1):
+        """Survey bispectrum multipoles: arrays [m][rows][n_kbin] and norm."""
+        return self._survey_three_point(self._lib.hg_bk_survey_multi, self.binning.n_kbin, multipoles, ith_kbin,
+                                        alpha, vsurvey)
+
+    def bk_survey(self, ell1: int, ell2: int, ELL: int, alpha: float, vsurvey: float, ith_kbin: int = -1):
+        bk, sn, norm = self.bk_survey_multi(((ell1, ell2, ELL),), alpha, vsurvey, ith_kbin)
+        return bk[0], sn[0], norm
+
+    def zeta_survey_multi(self, multipoles, alpha: float, vsurvey: float, ith_rbin: int = -1):
+        """Survey 3PCF multipoles: arrays [m][rows][n_rbin] and norm."""
+        return self._survey_three_point(self._lib.hg_zeta_survey_multi, self.binning.n_rbin, multipoles, ith_rbin,
+                                        alpha, vsurvey)
+
+    def zeta_survey(self, ell1: int, ell2: int, ELL: int, alpha: float, vsurvey: float, ith_rbin: int = -1):
+        z, sn, norm = self.zeta_survey_multi(((ell1, ell2, ELL),), alpha, vsurvey, ith_rbin)
+        return z[0], sn[0], norm
+
     def survey_scalars(self):
         vals = [ctypes.c_double() for _ in range(5)]
         self._check(self._lib.hg_survey_scalars(self._h, *[ctypes.byref(v) for v in vals]))

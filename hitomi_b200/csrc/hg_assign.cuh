@@ -117,9 +117,11 @@ struct PartSrc {
     int w_off;                  // doubles, < 0: weight 1
     const double2 *cw;          // optional per-particle complex weight, overrides w
     double scale;               // multiplies the weight (e.g. -alpha for randoms)
-    int ylm_on;                 // weight *= Yhat_lm(los) (field.hpp:199-216)
+    int ylm_on;                 // weight *= Yhat_lm(los) (field.hpp:199-216), or conj(Yhat_lm) when ylm_conj
     int ylm_l, ylm_m;
     int los_off;                // doubles
+    int wpow;                   // the weight enters as w^wpow (0 or 1: w; 2: the shot-noise fields, field.hpp:249-306)
+    int ylm_conj;
 };
 
 __device__ __forceinline__ void load_pos(const PartSrc &s, long long p, double pos[3]) {
@@ -139,8 +141,13 @@ __device__ __forceinline__ void load_weight(const PartSrc &s, long long p, doubl
         wi = c.y;
     } else {
         double w = (s.w_off >= 0) ? rec[s.w_off] : 1.0;
+        if (s.wpow > 1) {  // pow(w, 2) in the reference: w * w
+            double w1 = w;
+            for (int q = 1; q < s.wpow; q++) w *= w1;
+        }
         if (s.ylm_on) {
             zd y = ylm_reduced(s.ylm_l, s.ylm_m, rec[s.los_off], rec[s.los_off + 1], rec[s.los_off + 2]);
+            if (s.ylm_conj) y.y = -y.y;
             wr = y.x * w;
             wi = y.y * w;
         } else {

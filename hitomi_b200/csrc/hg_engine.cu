@@ -130,6 +130,10 @@ struct hg_ctx {
                                 double *norm) = 0;
     virtual void survey_scalars(double *alpha, double *vs, double *nbar, double *wd, double *wr) = 0;
     virtual void pk_survey(int ell, double alpha, double vs, double *pk_save, int *n_mode, double *norm) = 0;
+    virtual void bk_survey_multi(const std::vector<MP> &mps, int ith, double alpha, double vs, double *bk_save,
+                                 double *sn_save, double *norm) = 0;
+    virtual void zeta_survey_multi(const std::vector<MP> &mps, int ith, double alpha, double vs, double *zeta_save,
+                                   double *sn_save, double *norm) = 0;
 };
 
 namespace {
@@ -189,15 +193,29 @@ struct Engine : public hg_ctx {
         int KG[3] = {0, 0, 0};
         DBuf d_ent, d_start, d_scale;
     } shells;
+    // The catalogue the bispectrum and 3PCF read: the box density (kind 0) or the survey's
+    // D - alpha R field (kind 1).  G fields are keyed by GK = (L, M): the Yhat_LM-weighted
+    // field of the survey drivers (bispec.hpp:268-283), (0, 0) for the box.
+    struct SpecK {
+        Spec<T> s;
+        double k0r, k0i;  // FP64 value of the k = 0 mode
+    };
+    using GK = std::pair<int, int>;
+    using FQ = std::tuple<int, int, int, int>;  // chain family (l, m) with its G key (L, M)
+    int src_kind = -1;
+    double src_alpha = 0.0;
+    SpecK dsrc{};
     // per-catalogue bispectrum state
     DBuf shD;                                   // delta/W per entry
     std::map<Fam, std::unique_ptr<DBuf>> famA;  // A_f per entry (memory kept across catalogues)
     std::set<Fam> famA_ok;
-    std::map<Fam, std::unique_ptr<DBuf>> famQ;  // Q cube per chain family
-    std::set<Fam> famQ_ok;
-    DBuf Gc, Gbuf, Ac, T1, T2, pair_out;
-    bool G_valid = false, shD_valid = false;
-    std::map<std::pair<Fam, Fam>, std::vector<double>> pairs;  // key (a, b): sum_e A_a[e] Q_b,j(-n_e)
+    std::map<FQ, std::unique_ptr<DBuf>> famQ;  // Q cube per chain family and G
+    std::set<FQ> famQ_ok;
+    std::map<GK, std::unique_ptr<DBuf>> Gm;    // G on the reduced grid per G key
+    std::set<GK> Gm_ok;
+    DBuf Gc, Ac, T1, T2, pair_out;
+    bool shD_valid = false;
+    std::map<std::tuple<int, int, int, int, int, int>, std::vector<double>> pairs;  // (a, b, L, M)
 
     // shot-noise state
     DBuf xi;
@@ -212,16 +230,25 @@ struct Engine : public hg_ctx {
     std::set<std::array<int, 3>> hist_ok;
     DBuf hist_tmp, snmat, snblk, sn_part, d_kv;
 
-    // survey state (per pair of catalogues)
+    // survey state (per pair of catalogues): transformed Yhat_lm-weighted fields of two kinds,
+    // SF_DELTA = n_D - alpha n_R with weights Yhat w (field.hpp:186-228) and SF_SN = n_D +
+    // alpha^2 n_R with weights conj(Yhat) w^2 (field.hpp:249-284); m = 0 half spectra, m != 0
+    // full ones (m < 0 as mirrors of m > 0); keyed (kind, l, m), valid for sf_alpha.
+    enum { SF_DELTA = 0, SF_SN = 1 };
     DBuf smesh_re, smesh_im, dmesh, psum_part, sfield_tmp;
-    std::map<std::pair<int, int>, std::unique_ptr<DBuf>> sfield;  // (l, m >= 0) -> spectrum of D - alpha R
-    std::set<std::pair<int, int>> sfield_ok;
-    double sfield_alpha = 0.0;
+    std::map<std::array<int, 3>, std::unique_ptr<DBuf>> sfbuf;
+    std::map<std::array<int, 3>, std::array<double, 2>> sfk0;
+    std::set<std::array<int, 3>> sf_ok;
+    double sf_alpha = 0.0;
 
     // 3PCF state: geometry tables (per context) and filtered fields (per catalogue)
     std::map<int, std::unique_ptr<DBuf>> jtab_r;  // J_l[j][n2] = j_l(dk r_j sqrt(n2))
-    DBuf d_rv, Uz, Gz, zpart, zout;
-    bool Gz_valid = false;
+    DBuf d_rv, Uz, zpart, zout;
+    std::map<GK, std::unique_ptr<DBuf>> Gz;  // G on the full grid per G key
+    std::set<GK> Gz_ok;
+    // survey shot-noise histograms per multipole: sum_M sum_(m1,m2) w sum_{|x|^2 = n2} xi_LM Yhat1 Yhat2
+    std::map<std::array<int, 3>, std::unique_ptr<DBuf>> hist_sv;
+    std::set<std::array<int, 3>> hist_sv_ok;
     std::vector<int> zfine;                  // fine r index of each n2 (field.hpp:1044-1050), -1 if >= 10^4
     std::vector<std::vector<int>> zcoarse;   // coarse r bins of each fine index (field.hpp:1064-1085)
     std::vector<double> zcount;              // cells per coarse r bin
@@ -233,7 +260,7 @@ struct Engine : public hg_ctx {
     };
     std::map<ZKey, std::unique_ptr<DBuf>> zf;  // F_lm[r0 .. r0+nr) on the full grid
     std::set<ZKey> zf_ok;
-    std::map<std::tuple<int, int, int, int, int>, std::vector<double>> zpairs;  // (la, ma, lb, mb, row)
+    std::map<std::tuple<int, int, int, int, int, int, int>, std::vector<double>> zpairs;  // (a, b, row, L, M)
 
     long long launches = 0;
 
@@ -478,19 +505,57 @@ struct Engine : public hg_ctx {
         invalidate();
     }
 
-    void invalidate() {
-        dens_valid = false;
-        G_valid = false;
+    // statistics state derived from the current source (the catalogue itself is unchanged)
+    void invalidate_stats() {
+        Gm_ok.clear();
         shD_valid = false;
         xi_valid = false;
         famA_ok.clear();
         famQ_ok.clear();
         hist_ok.clear();
         pairs.clear();
-        Gz_valid = false;
+        Gz_ok.clear();
         zf_ok.clear();
         zpairs.clear();
-        sfield_ok.clear();
+        hist_sv_ok.clear();
+    }
+
+    // select the box (kind 0) or the survey with a given alpha (kind 1) as the source
+    void set_source(int kind, double alpha) {
+        if (kind != src_kind || (kind == 1 && alpha != src_alpha)) {
+            invalidate_stats();
+            src_kind = kind;
+            src_alpha = alpha;
+        }
+        if (kind == 0) {
+            box_density();
+            dsrc = SpecK{half_spec(), delta0, 0.0};
+        } else {
+            dsrc = sfield(SF_DELTA, 0, 0, alpha);
+        }
+    }
+
+    // the spectrum whose IFFT / W / V is G for a G key
+    SpecK g_source(const GK &gk) {
+        if (src_kind == 0) return SpecK{half_spec(), delta0, 0.0};
+        return sfield(SF_DELTA, gk.first, gk.second, src_alpha);
+    }
+
+    void invalidate() {
+        src_kind = -1;
+        dens_valid = false;
+        Gm_ok.clear();
+        shD_valid = false;
+        xi_valid = false;
+        famA_ok.clear();
+        famQ_ok.clear();
+        hist_ok.clear();
+        pairs.clear();
+        Gz_ok.clear();
+        zf_ok.clear();
+        zpairs.clear();
+        sf_ok.clear();
+        hist_sv_ok.clear();
     }
 
     // ------------------------------------------------------------------ assignment
@@ -522,7 +587,8 @@ struct Engine : public hg_ctx {
     // compact records, tile accumulation.  Returns the FP64 in-bounds mass (real part)
     // when want_mass.
     template <typename U, bool CPLX>
-    double assign_mesh(const std::vector<PartSrc> &srcs, const AssignGeom &ag, U *out_re, U *out_im, bool want_mass) {
+    double assign_mesh(const std::vector<PartSrc> &srcs, const AssignGeom &ag, U *out_re, U *out_im, bool want_mass,
+                       double *mass_im = nullptr) {
         const int ntiles = ag.nt[0] * ag.nt[1] * ag.nt[2];
         HG_CK(cnt.ensure(sizeof(unsigned) * (ntiles + 1)));
         HG_CK(off.ensure(sizeof(unsigned) * (ntiles + 1)));
@@ -581,6 +647,7 @@ struct Engine : public hg_ctx {
         kb("assign_tile_accum", double(total) * sizeof(PRec<U>) + double(g.ntot) * sizeof(U) * (CPLX ? 2 : 1));
         k_tile_accum<U, CPLX><<<nchunks, 256, smem, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
         ke();
+        if (mass_im) *mass_im = hm[1];
         return hm[0];
     }
 
@@ -855,7 +922,7 @@ struct Engine : public hg_ctx {
     }
 
     // G(x) = IFFT[delta/W]/V on the geometry's grid, from the cube |n_a| <= gs_a (pruned passes)
-    void build_G(const ChainGeo &S, DBuf &Gout) {
+    void build_G(const ChainGeo &S, DBuf &Gout, const SpecK &src) {
         const long long vol = (long long)S.M[0] * S.M[1] * S.M[2];
         const long long kg = (long long)S.KG[0] * S.KG[1] * S.KG[2];
         HG_CK(Gc.ensure(sizeof(C) * kg));
@@ -865,7 +932,7 @@ struct Engine : public hg_ctx {
         int3 cn = make_int3(S.KG[0], S.KG[1], S.KG[2]);
         unsigned blocks = (unsigned)std::min<long long>(grid1(kg, 256), 148 * 16);
         kb("scatter_G", double(kg) * (sizeof(C) * 2));
-        k_scatter_G<T><<<blocks, 256, 0, st>>>(half_spec(), g, tabs, wpow, lo, cn, delta0, 0.0, dp<C>(Gc));
+        k_scatter_G<T><<<blocks, 256, 0, st>>>(src.s, g, tabs, wpow, lo, cn, src.k0r, src.k0i, dp<C>(Gc));
         ke();
         const int M0 = S.M[0], M1 = S.M[1], M2 = S.M[2];
         pass<+1>(M2, LdCube<T>{dp<C>(Gc), S.KG[2], M2, S.gs[2]}, StArr<T>{dp<C>(T1), M2, 1},
@@ -878,10 +945,14 @@ struct Engine : public hg_ctx {
                  double((long long)S.KG[0] * M1 * M2 + vol) * sizeof(C));
     }
 
-    void ensure_G() {
-        if (G_valid) return;
-        build_G(bk_geo(), Gbuf);
-        G_valid = true;
+    const DBuf &ensure_G(const GK &gk) {
+        auto &p = Gm[gk];
+        if (!p) p = std::make_unique<DBuf>();
+        if (!Gm_ok.count(gk)) {
+            build_G(bk_geo(), *p, g_source(gk));
+            Gm_ok.insert(gk);
+        }
+        return *p;
     }
 
     // Q[j] = FFT[IFFT[Ac[j]] * G] on the geometry's compact cube (hg_chain.cuh); Ac is filled.
@@ -915,12 +986,15 @@ struct Engine : public hg_ctx {
                  double(o1) * (Kz + Mz) * sizeof(C));
     }
 
-    // Q_b[j] for the bispectrum shells
-    const C *family_Q(const Fam &b) {
-        DBuf &Q = map_buf(famQ, b);
-        if (famQ_ok.count(b)) return dp<C>(Q);
+    // Q_b[j] for the bispectrum shells with the G of key gk
+    const C *family_Q(const Fam &b, const GK &gk) {
+        const FQ key{b.l, b.m, gk.first, gk.second};
+        auto &qp = famQ[key];
+        if (!qp) qp = std::make_unique<DBuf>();
+        DBuf &Q = *qp;
+        if (famQ_ok.count(key)) return dp<C>(Q);
         const ChainGeo S = bk_geo();
-        ensure_G();
+        const DBuf &Gsrc = ensure_G(gk);
         const double2 *A = family_A(b);
         const long long cv = cube_vol();
         HG_CK(Ac.ensure(sizeof(C) * cv * S.ns));
@@ -931,19 +1005,19 @@ struct Engine : public hg_ctx {
                                                                make_int3(S.K[0], S.K[1], S.K[2]),
                                                                make_int3(S.s[0], S.s[1], S.s[2]), dp<C>(Ac));
         ke();
-        run_chain(S, Gbuf, dp<C>(Q));
-        famQ_ok.insert(b);
+        run_chain(S, Gsrc, dp<C>(Q));
+        famQ_ok.insert(key);
         return dp<C>(Q);
     }
 
     // pair matrix P[i][j] = sum_{e in shell i} A_a[e] Q_b,j(-n_e)  (complex, [ns][ns])
-    const std::vector<double> &pair_matrix(const Fam &a, const Fam &b) {
-        auto key = std::make_pair(a, b);
+    const std::vector<double> &pair_matrix(const Fam &a, const Fam &b, const GK &gk) {
+        auto key = std::make_tuple(a.l, a.m, b.l, b.m, gk.first, gk.second);
         auto it = pairs.find(key);
         if (it != pairs.end()) return it->second;
         const ShellSet &S = shells;
         const double2 *A = family_A(a);
-        const C *Q = family_Q(b);
+        const C *Q = family_Q(b, gk);
         HG_CK(pair_out.ensure(sizeof(double2) * S.ns * S.ns));
         dim3 gr(S.ns, S.ns);
         kb("pair_dot", double(n_ent()) * (S.ns + 1) * 16.0);
@@ -959,10 +1033,10 @@ struct Engine : public hg_ctx {
     }
 
     // sum_x F_a,i F_b,j G (without dV) for all (i, j): chain on b, or on a transposed.
-    std::vector<double> triple_sum(const Fam &a, const Fam &b, const std::set<Fam> &chains) {
+    std::vector<double> triple_sum(const Fam &a, const Fam &b, const GK &gk, const std::set<FQ> &chains) {
         const int ns = shells.ns;
-        if (chains.count(b)) return pair_matrix(a, b);
-        const auto &P = pair_matrix(b, a);
+        if (chains.count(FQ{b.l, b.m, gk.first, gk.second})) return pair_matrix(a, b, gk);
+        const auto &P = pair_matrix(b, a, gk);
         std::vector<double> r(2 * ns * ns);
         for (int i = 0; i < ns; i++)
             for (int j = 0; j < ns; j++) {
@@ -973,13 +1047,12 @@ struct Engine : public hg_ctx {
     }
 
     void prepare_shells() {
-        box_density();
         build_shells();
         HG_REQUIRE(n_ent() > 0, "no Fourier modes fall inside the k shells");
         if (!shD_valid) {
             HG_CK(shD.ensure(sizeof(double2) * n_ent()));
             kb("shell_D", double(n_ent()) * (16.0 + sizeof(C)));
-            k_shell_D<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), half_spec(), g, tabs,
+            k_shell_D<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), dsrc.s, g, tabs,
                                                               wpow, dp<double2>(shD));
             ke();
             shD_valid = true;
@@ -1156,56 +1229,143 @@ struct Engine : public hg_ctx {
 
     // ------------------------------------------------------------------ bispectrum (box)
     // bispec.hpp:877-1203 for all k1 rows of several multipoles at once.
-    void bk_box_multi(const std::vector<MP> &mps, int ith, double *bk_save, double *sn_save, double *norm) override {
+    // (m1, m2, M) combinations with |w| >= 1e-10, w = (2L+1)(2l1+1)(2l2+1) w3j(l1 l2 L; 0 0 0)
+    // w3j(l1 l2 L; m1 m2 M): M = 0 only for the box (bispec.hpp:1129-1136), every M for the
+    // survey (bispec.hpp:255-270).
+    struct Combo3 {
+        int m1, m2, M;
+        double w;
+    };
+    static std::vector<Combo3> combos3(const MP &mp, bool all_M) {
+        std::vector<Combo3> out;
+        const double w000 = wigner3j(mp.l1, mp.l2, mp.L, 0, 0, 0);
+        for (int m1 = -mp.l1; m1 <= mp.l1; m1++)
+            for (int m2 = -mp.l2; m2 <= mp.l2; m2++)
+                for (int M = all_M ? -mp.L : 0; M <= (all_M ? mp.L : 0); M++) {
+                    double w = w000 * wigner3j(mp.l1, mp.l2, mp.L, m1, m2, M);
+                    w *= double(2 * mp.L + 1) * double(2 * mp.l1 + 1) * double(2 * mp.l2 + 1);
+                    if (std::fabs(w) < 1.0e-10) continue;
+                    out.push_back({m1, m2, M, w});
+                }
+        return out;
+    }
+
+    static void check_multipoles(const std::vector<MP> &mps) {
         HG_REQUIRE(!mps.empty(), "no multipoles requested");
         for (const auto &mp : mps) {
             HG_REQUIRE(mp.l1 >= 0 && mp.l2 >= 0 && mp.L >= 0, "ell1, ell2, ELL must be >= 0");
             HG_REQUIRE(std::fabs(wigner3j(mp.l1, mp.l2, mp.L, 0, 0, 0)) >= 1.0e-10,
                        "This multipole combination is not allowed: wigner_3j(ell1, ell2, ELL, 0,0,0) == 0");
         }
-        HG_REQUIRE(ith >= -1 && ith < cfg.n_kbin, "ith_kbin out of range");
-        begin();
+    }
+
+    // B_raw[q] for every (k1, k2): sum over (m1, m2, M) of w dV sum_x F1 F2 G_LM
+    // (bispec.hpp:1118-1170 box, 255-320 survey), [q][ns][ns] complex.  Chain families:
+    // every self-paired family per G key, then a greedy cover of the remaining pairs.
+    std::vector<std::vector<double>> bk_main(const std::vector<MP> &mps) {
+        const bool survey = (src_kind == 1);
         prepare_shells();
         const int ns = shells.ns;
-        const double Np = double(slot[0].n);
         const double dV = g.volume / double(g.ntot);
         const double red = double(g.ntot) / (double(shells.M[0]) * shells.M[1] * shells.M[2]);
-        // chain families: every self-paired family, then a greedy cover of the remaining pairs
-        std::vector<std::vector<Combo>> cmb;
-        std::set<std::pair<Fam, Fam>> upairs;
+        std::vector<std::vector<Combo3>> cmb;
+        std::map<GK, std::set<std::pair<Fam, Fam>>> upairs;
         for (const auto &mp : mps) {
-            cmb.push_back(combos_of(mp));
+            cmb.push_back(combos3(mp, survey));
             for (const auto &c : cmb.back()) {
                 Fam a{mp.l1, c.m1}, b{mp.l2, c.m2};
-                upairs.insert(b < a ? std::make_pair(b, a) : std::make_pair(a, b));
+                GK gk = survey ? GK{mp.L, c.M} : GK{0, 0};
+                upairs[gk].insert(b < a ? std::make_pair(b, a) : std::make_pair(a, b));
             }
         }
-        std::set<Fam> chains(famQ_ok.begin(), famQ_ok.end());
-        for (const auto &p : upairs)
-            if (!(p.first < p.second) && !(p.second < p.first)) chains.insert(p.first);
-        while (true) {
-            std::map<Fam, int> score;
-            for (const auto &p : upairs) {
-                if (chains.count(p.first) || chains.count(p.second)) continue;
-                score[p.first]++;
-                score[p.second]++;
-            }
-            if (score.empty()) break;
-            Fam best = score.begin()->first;
-            int bs = -1;
-            for (const auto &kv : score)
-                if (kv.second > bs) {
-                    bs = kv.second;
-                    best = kv.first;
+        std::set<FQ> chains(famQ_ok.begin(), famQ_ok.end());
+        for (const auto &kv : upairs) {
+            const GK &gk = kv.first;
+            auto has = [&](const Fam &f) { return chains.count(FQ{f.l, f.m, gk.first, gk.second}) > 0; };
+            for (const auto &p : kv.second)
+                if (!(p.first < p.second) && !(p.second < p.first))
+                    chains.insert(FQ{p.first.l, p.first.m, gk.first, gk.second});
+            while (true) {
+                std::map<Fam, int> score;
+                for (const auto &p : kv.second) {
+                    if (has(p.first) || has(p.second)) continue;
+                    score[p.first]++;
+                    score[p.second]++;
                 }
-            chains.insert(best);
+                if (score.empty()) break;
+                Fam best = score.begin()->first;
+                int bs = -1;
+                for (const auto &sc : score)
+                    if (sc.second > bs) {
+                        bs = sc.second;
+                        best = sc.first;
+                    }
+                chains.insert(FQ{best.l, best.m, gk.first, gk.second});
+            }
         }
         std::vector<std::vector<double>> B(mps.size(), std::vector<double>(2 * ns * ns, 0.0));
         for (size_t q = 0; q < mps.size(); q++)
             for (const auto &c : cmb[q]) {
-                std::vector<double> t = triple_sum(Fam{mps[q].l1, c.m1}, Fam{mps[q].l2, c.m2}, chains);
+                GK gk = survey ? GK{mps[q].L, c.M} : GK{0, 0};
+                std::vector<double> t = triple_sum(Fam{mps[q].l1, c.m1}, Fam{mps[q].l2, c.m2}, gk, chains);
                 for (int e = 0; e < 2 * ns * ns; e++) B[q][e] += c.w * (dV * red * t[e]);
             }
+        return B;
+    }
+
+    // SN += i^(l1+l2) dV sum_n2 J_l1(k1 r) J_l2(k2 r) hist(n2)  (bispec.hpp:1036-1060): the
+    // skinny product J1 diag(hist) J2^T in row blocks, [ns][ns] complex
+    void bk_sn_xi(const MP &mp, const double *hq, std::vector<double> &SNq) {
+        const int ns = cfg.n_kbin;
+        const double dV = g.volume / double(g.ntot);
+        HG_CK(snmat.ensure(sizeof(double2) * ns * ns));
+        const double *J1 = jtab(mp.l1);
+        const double *J2 = jtab(mp.l2);
+        const int nblk = sn_partial_blocks(n2dim);
+        const int rb = std::min(ns, HG_SN_MAXROWS);
+        HG_CK(sn_part.ensure(sizeof(double) * 2 * (size_t)nblk * rb * rb));
+        HG_CK(snblk.ensure(sizeof(double2) * (size_t)rb * rb));
+        for (int a0 = 0; a0 < ns; a0 += rb)
+            for (int b0 = 0; b0 < ns; b0 += rb) {
+                const int na = std::min(rb, ns - a0), nb = std::min(rb, ns - b0);
+                const size_t smem = sn_partial_smem(na, nb);
+                HG_CK(cudaFuncSetAttribute(k_sn_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                kb("sn_matrix", double(na + 2 * nb + 2) * n2dim * 8.0);
+                k_sn_partial<<<nblk, HG_SN_THREADS, smem, st>>>(J1 + (size_t)a0 * n2dim, na, J2 + (size_t)b0 * n2dim,
+                                                                nb, hq, n2dim, dp<double>(sn_part));
+                ke();
+                kb("sn_matrix", double(nblk) * na * nb * 16.0);
+                k_sum_parts<<<grid1((long long)na * nb, 128), 128, 0, st>>>(dp<double>(sn_part), nblk, na * nb,
+                                                                              dp<double2>(snblk));
+                ke();
+                // place the (a0, b0) block into the ns x ns matrix
+                HG_CK(cudaMemcpy2DAsync(dp<double2>(snmat) + (size_t)a0 * ns + b0, sizeof(double2) * ns, snblk.p,
+                                        sizeof(double2) * nb, sizeof(double2) * nb, na, cudaMemcpyDeviceToDevice, st));
+            }
+        std::vector<double> sd(2 * ns * ns);
+        HG_CK(cudaMemcpyAsync(sd.data(), snmat.p, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        const int p4 = (mp.l1 + mp.l2) % 4;
+        for (int e = 0; e < ns * ns; e++) {
+            double re = sd[2 * e] * dV, im = sd[2 * e + 1] * dV;
+            double rr = p4 == 0 ? re : p4 == 1 ? -im : p4 == 2 ? -re : im;
+            double ii = p4 == 0 ? im : p4 == 1 ? re : p4 == 2 ? -im : -re;
+            SNq[2 * e] += rr;
+            SNq[2 * e + 1] += ii;
+        }
+    }
+
+    void bk_box_multi(const std::vector<MP> &mps, int ith, double *bk_save, double *sn_save, double *norm) override {
+        check_multipoles(mps);
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_kbin, "ith_kbin out of range");
+        begin();
+        set_source(0, 0.0);
+        const int ns = cfg.n_kbin;
+        const double Np = double(slot[0].n);
+        const double dV = g.volume / double(g.ntot);
+        std::vector<std::vector<double>> B = bk_main(mps);
+        std::vector<std::vector<Combo>> cmb;
+        for (const auto &mp : mps) cmb.push_back(combos_of(mp));
         // shot noise (bispec.hpp:909-1078): P terms, constant term, xi term
         std::vector<LM> lms;
         std::vector<std::vector<int>> lm_idx(mps.size());
@@ -1261,60 +1421,8 @@ struct Engine : public hg_ctx {
             }
         }
         ensure_histograms(mps);
-        HG_CK(snmat.ensure(sizeof(double2) * ns * ns));
-        for (size_t q = 0; q < mps.size(); q++) {
-            const MP &mp = mps[q];
-            const double *J1 = jtab(mp.l1);
-            const double *J2 = jtab(mp.l2);
-            const double *hq = dp<double>(*hist_mp[{mp.l1, mp.l2, mp.L}]);
-            const int nblk = sn_partial_blocks(n2dim);
-            const int rb = std::min(ns, HG_SN_MAXROWS);
-            HG_CK(sn_part.ensure(sizeof(double) * 2 * (size_t)nblk * rb * rb));
-            HG_CK(snblk.ensure(sizeof(double2) * (size_t)rb * rb));
-            for (int a0 = 0; a0 < ns; a0 += rb)
-                for (int b0 = 0; b0 < ns; b0 += rb) {
-                    const int na = std::min(rb, ns - a0), nb = std::min(rb, ns - b0);
-                    const size_t smem = sn_partial_smem(na, nb);
-                    HG_CK(cudaFuncSetAttribute(k_sn_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                    kb("sn_matrix", double(na + 2 * nb + 2) * n2dim * 8.0);
-                    k_sn_partial<<<nblk, HG_SN_THREADS, smem, st>>>(J1 + (size_t)a0 * n2dim, na,
-                                                                    J2 + (size_t)b0 * n2dim, nb, hq, n2dim,
-                                                                    dp<double>(sn_part));
-                    ke();
-                    kb("sn_matrix", double(nblk) * na * nb * 16.0);
-                    k_sum_parts<<<grid1((long long)na * nb, 128), 128, 0, st>>>(dp<double>(sn_part), nblk, na * nb,
-                                                                                  dp<double2>(snblk));
-                    ke();
-                    // place the (a0, b0) block into the ns x ns matrix
-                    HG_CK(cudaMemcpy2DAsync(dp<double2>(snmat) + (size_t)a0 * ns + b0, sizeof(double2) * ns,
-                                            snblk.p, sizeof(double2) * nb, sizeof(double2) * nb, na,
-                                            cudaMemcpyDeviceToDevice, st));
-                }
-            std::vector<double> sd(2 * ns * ns);
-            HG_CK(cudaMemcpyAsync(sd.data(), snmat.p, sizeof(double) * sd.size(), cudaMemcpyDeviceToHost, st));
-            HG_CK(cudaStreamSynchronize(st));
-            // * i^(l1+l2) * dV   (bispec.hpp:1053-1055)
-            int p4 = (mp.l1 + mp.l2) % 4;
-            for (int e = 0; e < ns * ns; e++) {
-                double re = sd[2 * e] * dV, im = sd[2 * e + 1] * dV;
-                double rr, ii;
-                if (p4 == 0) {
-                    rr = re;
-                    ii = im;
-                } else if (p4 == 1) {
-                    rr = -im;
-                    ii = re;
-                } else if (p4 == 2) {
-                    rr = -re;
-                    ii = -im;
-                } else {
-                    rr = im;
-                    ii = -re;
-                }
-                SN[q][2 * e] += rr;
-                SN[q][2 * e + 1] += ii;
-            }
-        }
+        for (size_t q = 0; q < mps.size(); q++)
+            bk_sn_xi(mps[q], dp<double>(*hist_mp[{mps[q].l1, mps[q].l2, mps[q].L}]), SN[q]);
         const int r0 = (ith < 0) ? 0 : ith, r1 = (ith < 0) ? ns : ith + 1;
         const int rows = r1 - r0;
         for (size_t q = 0; q < mps.size(); q++)
@@ -1406,12 +1514,13 @@ struct Engine : public hg_ctx {
         return p;
     }
 
-    // U = Yhat_lm delta / W / V on the full grid
-    void zeta_U(int l, int m) {
+    // U = Yhat_lm F / W / V on the full grid, F the given spectrum (the density by default)
+    void zeta_U(int l, int m) { zeta_U_of(dsrc, l, m); }
+    void zeta_U_of(const SpecK &src, int l, int m) {
         HG_CK(Uz.ensure(sizeof(C) * g.ntot));
         unsigned blocks = (unsigned)std::min<long long>(grid1(g.ntot, 256), 148 * 16);
         kb("zeta_U", double(g.ntot) * (sizeof(C) * 1.5));
-        k_zeta_U<T><<<blocks, 256, 0, st>>>(half_spec(), g, tabs, wpow, l, m, delta0, dp<C>(Uz));
+        k_zeta_U<T><<<blocks, 256, 0, st>>>(src.s, g, tabs, wpow, l, m, src.k0r, src.k0i, dp<C>(Uz));
         ke();
     }
 
@@ -1427,12 +1536,15 @@ struct Engine : public hg_ctx {
     }
 
     // G(x) = IFFT[delta / W] / V on the full grid (field.hpp:326-344 after the window correction)
-    void ensure_Gz() {
-        if (Gz_valid) return;
-        zeta_U(0, 0);
-        HG_CK(Gz.ensure(sizeof(C) * g.ntot));
-        full_inverse(LdArr<T>{dp<C>(Uz), g.n[0], (long long)g.n[1] * g.n[2]}, dp<C>(Gz), 1, "zeta_G");
-        Gz_valid = true;
+    const C *ensure_Gz(const GK &gk) {
+        auto &p = Gz[gk];
+        if (!p) p = std::make_unique<DBuf>();
+        if (Gz_ok.count(gk)) return dp<C>(*p);
+        zeta_U_of(g_source(gk), 0, 0);
+        HG_CK(p->ensure(sizeof(C) * g.ntot));
+        full_inverse(LdArr<T>{dp<C>(Uz), g.n[0], (long long)g.n[1] * g.n[2]}, dp<C>(*p), 1, "zeta_G");
+        Gz_ok.insert(gk);
+        return dp<C>(*p);
     }
 
     size_t zf_bytes() const {
@@ -1471,14 +1583,14 @@ struct Engine : public hg_ctx {
     }
 
     // P[i1][i2] = sum_x Fa[i1](x) Fb[i2](x) G(x), complex [na][nb]
-    std::vector<double> zeta_pairsum(const C *Fa, int na, const C *Fb, int nb) {
+    std::vector<double> zeta_pairsum(const C *Fa, int na, const C *Fb, int nb, const C *G) {
         const int nblk = 2 * 148;
         const size_t smem = zeta_pairsum_smem(na, nb);
         HG_CK(zpart.ensure(sizeof(double) * 2 * (size_t)nblk * na * nb));
         HG_CK(zout.ensure(sizeof(double2) * (size_t)na * nb));
         HG_CK(cudaFuncSetAttribute(k_zeta_pairsum<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kb("zeta_pairsum", double(g.ntot) * sizeof(C) * double(na + (Fa == Fb ? 0 : nb) + 1));
-        k_zeta_pairsum<T><<<nblk, HG_ZR_THREADS, smem, st>>>(Fa, na, Fb, nb, dp<C>(Gz), g.ntot, dp<double>(zpart));
+        k_zeta_pairsum<T><<<nblk, HG_ZR_THREADS, smem, st>>>(Fa, na, Fb, nb, G, g.ntot, dp<double>(zpart));
         ke();
         kb("zeta_pairsum", double(nblk) * na * nb * 16.0);
         k_sum_parts<<<grid1((long long)na * nb, 128), 128, 0, st>>>(dp<double>(zpart), nblk, na * nb,
@@ -1492,7 +1604,7 @@ struct Engine : public hg_ctx {
 
     // sum_x F_a[i1] F_b[i2] G for the requested rows i1 (all, or `row`) and every i2:
     // [rows][ns] complex.  All rows come from the unordered pair (transposed when needed).
-    std::vector<double> zeta_pair(const Fam &a, const Fam &b, int row) {
+    std::vector<double> zeta_pair(const Fam &a, const Fam &b, int row, const GK &gk) {
         const int ns = cfg.n_rbin;
         const bool all = (row < 0);
         Fam p = a, q = b;
@@ -1501,7 +1613,7 @@ struct Engine : public hg_ctx {
             std::swap(p, q);
             swap = true;
         }
-        auto key = std::make_tuple(p.l, p.m, q.l, q.m, row);
+        auto key = std::make_tuple(p.l, p.m, q.l, q.m, row, gk.first, gk.second);
         auto it = zpairs.find(key);
         if (it == zpairs.end()) {
             const int rows = all ? ns : 1;
@@ -1523,7 +1635,7 @@ struct Engine : public hg_ctx {
                     const C *Fa = zeta_fields(p, a0, an, nullptr);
                     const C *Fb = (p.l == q.l && p.m == q.m && a0 == b0 && an == bn) ? Fa
                                                                                        : zeta_fields(q, b0, bn, &ka);
-                    std::vector<double> t = zeta_pairsum(Fa, an, Fb, bn);
+                    std::vector<double> t = zeta_pairsum(Fa, an, Fb, bn, ensure_Gz(gk));
                     for (int i1 = 0; i1 < an; i1++)
                         for (int i2 = 0; i2 < bn; i2++) {
                             size_t o = (size_t)(a0 - pr0 + i1) * ns + (b0 + i2);
@@ -1546,30 +1658,20 @@ struct Engine : public hg_ctx {
     }
 
     // bispec.hpp:1205-1424 for all r1 rows (ith = -1) or one, for several multipoles.
-    void zeta_box_multi(const std::vector<MP> &mps, int ith, double *zeta_save, double *sn_save,
-                        double *norm) override {
-        HG_REQUIRE(!mps.empty(), "no multipoles requested");
-        for (const auto &mp : mps) {
-            HG_REQUIRE(mp.l1 >= 0 && mp.l2 >= 0 && mp.L >= 0, "ell1, ell2, ELL must be >= 0");
-            HG_REQUIRE(std::fabs(wigner3j(mp.l1, mp.l2, mp.L, 0, 0, 0)) >= 1.0e-10,
-                       "This multipole combination is not allowed: wigner_3j(ell1, ell2, ELL, 0,0,0) == 0");
-        }
-        HG_REQUIRE(ith >= -1 && ith < cfg.n_rbin, "ith_rbin out of range");
-        begin();
-        zeta_geometry();
-        box_density();
-        ensure_Gz();
+    // zeta_raw = sum_(m1,m2,M) w i^(l1+l2) dV sum_x F1 F2 G_LM  (bispec.hpp:1354-1378 box,
+    // 545-575 survey): [q][rows][ns] complex
+    std::vector<std::vector<double>> zeta_main(const std::vector<MP> &mps, int ith) {
+        const bool survey = (src_kind == 1);
         const int ns = cfg.n_rbin;
-        const double Np = double(slot[0].n);
         const double dV = g.volume / double(g.ntot);
-        const int r0 = (ith < 0) ? 0 : ith, rows = (ith < 0) ? ns : 1;
-        // zeta_raw = sum_combos w i^(l1+l2) dV sum_x F1 F2 G  (bispec.hpp:1354-1378)
+        const int rows = (ith < 0) ? ns : 1;
         std::vector<std::vector<double>> Z(mps.size(), std::vector<double>(2 * (size_t)rows * ns, 0.0));
         for (size_t q = 0; q < mps.size(); q++) {
             const MP &mp = mps[q];
             const int p4 = (mp.l1 + mp.l2) % 4;
-            for (const auto &c : combos_of(mp)) {
-                std::vector<double> t = zeta_pair(Fam{mp.l1, c.m1}, Fam{mp.l2, c.m2}, ith);
+            for (const auto &c : combos3(mp, survey)) {
+                GK gk = survey ? GK{mp.L, c.M} : GK{0, 0};
+                std::vector<double> t = zeta_pair(Fam{mp.l1, c.m1}, Fam{mp.l2, c.m2}, ith, gk);
                 for (size_t e = 0; e < (size_t)rows * ns; e++) {
                     double re = c.w * (dV * t[2 * e]), im = c.w * (dV * t[2 * e + 1]);
                     double rr = p4 == 0 ? re : p4 == 1 ? -im : p4 == 2 ? -re : im;
@@ -1579,14 +1681,21 @@ struct Engine : public hg_ctx {
                 }
             }
         }
-        // shot noise on the diagonal (bispec.hpp:1236-1298, field.hpp:979-1113)
-        ensure_histograms(mps);
+        return Z;
+    }
+
+    // shot noise on the diagonal from a multipole's n^2 histogram (field.hpp:1030-1105,
+    // bispec.hpp:1279-1285), written with the results
+    void zeta_finish(const std::vector<MP> &mps, int ith, const std::vector<std::vector<double>> &Z,
+                     const std::vector<const double *> &hists, double *zeta_save, double *sn_save) {
+        const int ns = cfg.n_rbin;
+        const double dV = g.volume / double(g.ntot);
+        const int r0 = (ith < 0) ? 0 : ith, rows = (ith < 0) ? ns : 1;
         std::fill(sn_save, sn_save + 2 * mps.size() * (size_t)rows * ns, 0.0);
         std::vector<double> hist(2 * n2dim);
         for (size_t q = 0; q < mps.size(); q++) {
             const MP &mp = mps[q];
-            HG_CK(cudaMemcpyAsync(hist.data(), dp<double>(*hist_mp[{mp.l1, mp.l2, mp.L}]),
-                                  sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, st));
+            HG_CK(cudaMemcpyAsync(hist.data(), hists[q], sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, st));
             HG_CK(cudaStreamSynchronize(st));
             std::vector<double> xr(ns, 0.0), xim(ns, 0.0);
             for (long long n2 = 0; n2 < n2dim; n2++) {
@@ -1598,11 +1707,10 @@ struct Engine : public hg_ctx {
             }
             const double sg = ((mp.l1 + mp.l2) % 2 == 0) ? 1.0 : -1.0;
             for (int i = r0; i < r0 + rows; i++) {
-                double s = zcount[i] != 0.0 ? sg / zcount[i] / zcount[i] / dV : 0.0;
+                double sc = zcount[i] != 0.0 ? sg / zcount[i] / zcount[i] / dV : 0.0;
                 size_t o = (size_t)q * rows * ns + (size_t)(i - r0) * ns + i;
-                // rows other than the diagonal carry no shot noise (bispec.hpp:1279-1285)
-                sn_save[2 * o] = xr[i] * s;
-                sn_save[2 * o + 1] = xim[i] * s;
+                sn_save[2 * o] = xr[i] * sc;
+                sn_save[2 * o + 1] = xim[i] * sc;
             }
         }
         for (size_t q = 0; q < mps.size(); q++)
@@ -1611,15 +1719,32 @@ struct Engine : public hg_ctx {
                 zeta_save[2 * o] = Z[q][2 * e];
                 zeta_save[2 * o + 1] = Z[q][2 * e + 1];
             }
+    }
+
+    // bispec.hpp:1205-1424 for all r1 rows (ith = -1) or one, for several multipoles.
+    void zeta_box_multi(const std::vector<MP> &mps, int ith, double *zeta_save, double *sn_save,
+                        double *norm) override {
+        check_multipoles(mps);
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_rbin, "ith_rbin out of range");
+        begin();
+        zeta_geometry();
+        set_source(0, 0.0);
+        std::vector<std::vector<double>> Z = zeta_main(mps, ith);
+        ensure_histograms(mps);
+        std::vector<const double *> hs;
+        for (const auto &mp : mps) hs.push_back(dp<double>(*hist_mp[{mp.l1, mp.l2, mp.L}]));
+        zeta_finish(mps, ith, Z, hs, zeta_save, sn_save);
         if (norm) {
+            const double Np = double(slot[0].n);
             double nv = g.volume / Np / Np;
             nv *= (g.volume / Np);
             *norm = nv;
         }
         end();
     }
+
     // ------------------------------------------------------------------ survey geometry
-    PartSrc survey_src(int s, bool ylm, int l, int m, double scale) const {
+    PartSrc survey_src(int s, bool ylm, int l, int m, double scale, int wp = 1, bool conj = false) const {
         const Slot &S = slot[s];
         PartSrc p{};
         p.base = S.base();
@@ -1633,6 +1758,8 @@ struct Engine : public hg_ctx {
         p.ylm_l = l;
         p.ylm_m = m;
         p.los_off = S.los_off;
+        p.wpow = wp;
+        p.ylm_conj = conj ? 1 : 0;
         return p;
     }
 
@@ -1707,49 +1834,312 @@ struct Engine : public hg_ctx {
     // FFT[dV (n_D - alpha n_R)] of the Yhat_lm(los)-weighted fields, m >= 0
     // (calcYlmWeightedDensityFluctuation field.hpp:186-228, then field.hpp:310-325).  m = 0 is
     // a real field (half spectrum); m > 0 is complex (full spectrum).
-    Spec<T> survey_field(int l, int m, double alpha) {
-        if (alpha != sfield_alpha) {
-            sfield_ok.clear();
-            sfield_alpha = alpha;
+    SpecK sfield(int kind, int l, int m, double alpha) {
+        if (alpha != sf_alpha) {
+            sf_ok.clear();
+            sf_alpha = alpha;
         }
         const int hz = g.n[2] / 2 + 1;
         const bool real = (m == 0);
-        auto key = std::make_pair(l, m);
-        auto &pb = sfield[key];
+        const std::array<int, 3> key{kind, l, m};
+        auto &pb = sfbuf[key];
         if (!pb) pb = std::make_unique<DBuf>();
-        Spec<T> sp{dp<C>(*pb), g.n[0], g.n[1], g.n[2], real ? 1 : 0};
-        if (sfield_ok.count(key)) return sp;
+        if (sf_ok.count(key)) {
+            const auto &k0 = sfk0[key];
+            return SpecK{Spec<T>{dp<C>(*pb), g.n[0], g.n[1], g.n[2], real ? 1 : 0}, k0[0], k0[1]};
+        }
         const long long fsz = real ? (long long)g.n[0] * g.n[1] * hz : g.ntot;
+        if (m < 0) {  // sgn conj(F_{l,|m|}(-k)), sgn = (-1)^m
+            SpecK pos = sfield(kind, l, -m, alpha);
+            const double sg = ((-m) % 2) ? -1.0 : 1.0;
+            HG_CK(pb->ensure(sizeof(C) * fsz));
+            unsigned blocks = (unsigned)std::min<long long>(grid1(g.ntot, 256), 148 * 16);
+            kb("survey_mirror", double(g.ntot) * sizeof(C) * 2.0);
+            k_mirror<T><<<blocks, 256, 0, st>>>(pos.s.p, dp<C>(*pb), g.n[0], g.n[1], g.n[2], (T)sg);
+            ke();
+            sfk0[key] = {sg * pos.k0r, -sg * pos.k0i};
+            sf_ok.insert(key);
+            return SpecK{Spec<T>{dp<C>(*pb), g.n[0], g.n[1], g.n[2], 0}, sg * pos.k0r, -sg * pos.k0i};
+        }
         HG_CK(pb->ensure(sizeof(C) * fsz));
-        sp.p = dp<C>(*pb);
         const bool ylm = !(l == 0 && m == 0);
-        std::vector<PartSrc> srcs{survey_src(0, ylm, l, m, 1.0), survey_src(1, ylm, l, m, -alpha)};
+        std::vector<PartSrc> srcs;
+        if (kind == SF_DELTA)
+            srcs = {survey_src(0, ylm, l, m, 1.0), survey_src(1, ylm, l, m, -alpha)};
+        else
+            srcs = {survey_src(0, ylm, l, m, 1.0, 2, true), survey_src(1, ylm, l, m, alpha * alpha, 2, true)};
         HG_CK(smesh_re.ensure(sizeof(T) * g.ntot));
         if (!real) HG_CK(smesh_im.ensure(sizeof(T) * g.ntot));
-        // assign (mass units: dV rho, the transform's input) with a shift, transform into F
+        const double dV = g.volume / double(g.ntot);
+        // assign (mass units: dV rho, the transform's input) with a shift, transform into F;
+        // returns the FP64 in-bounds mass, the transform's exact k = 0 value
         auto build = [&](double shift, C *F) {
             AssignGeom ag = make_geom(shift);
             ag.acc_factor = 1.0;
+            double mi = 0.0, mr;
             if (real) {
-                assign_mesh<T, false>(srcs, ag, dp<T>(smesh_re), nullptr, false);
+                mr = assign_mesh<T, false>(srcs, ag, dp<T>(smesh_re), nullptr, true, &mi);
                 forward_real(dp<T>(smesh_re), F, (T)0, (T)1, "fft_survey");
             } else {
-                assign_mesh<T, true>(srcs, ag, dp<T>(smesh_re), dp<T>(smesh_im), false);
+                mr = assign_mesh<T, true>(srcs, ag, dp<T>(smesh_re), dp<T>(smesh_im), true, &mi);
                 const long long yz = (long long)g.n[1] * g.n[2];
                 pass<-1>(g.n[2], LdPlanar<T>{dp<T>(smesh_re), dp<T>(smesh_im), g.n[2]}, StArr<T>{F, g.n[2], 1},
                          (long long)g.n[0] * g.n[1], 1, "fft_survey", double(g.ntot) * (2 * sizeof(T) + sizeof(C)));
                 pass<-1>(g.n[1], LdArr<T>{F, g.n[1], g.n[2]}, StArr<T>{F, g.n[1], g.n[2]}, g.n[0], g.n[2], "fft_survey");
                 pass<-1>(g.n[0], LdArr<T>{F, g.n[0], yz}, StArr<T>{F, g.n[0], yz}, 1, yz, "fft_survey");
             }
+            return std::array<double, 2>{mr * dV, real ? 0.0 : mi * dV};
         };
-        build(0.0, dp<C>(*pb));
+        std::array<double, 2> k0 = build(0.0, dp<C>(*pb));
         if (cfg.interlace) {
             HG_CK(sfield_tmp.ensure(sizeof(C) * fsz));
-            build(0.5, dp<C>(sfield_tmp));
+            std::array<double, 2> k1 = build(0.5, dp<C>(sfield_tmp));
             interlace_combine(dp<C>(*pb), dp<C>(sfield_tmp), real);
+            k0 = {0.5 * (k0[0] + k1[0]), 0.5 * (k0[1] + k1[1])};
         }
-        sfield_ok.insert(key);
-        return sp;
+        C z0;
+        z0.x = (T)k0[0];
+        z0.y = (T)k0[1];
+        HG_CK(cudaMemcpyAsync(pb->p, &z0, sizeof(C), cudaMemcpyHostToDevice, st));
+        HG_CK(cudaStreamSynchronize(st));
+        sfk0[key] = k0;
+        sf_ok.insert(key);
+        return SpecK{Spec<T>{dp<C>(*pb), g.n[0], g.n[1], g.n[2], real ? 1 : 0}, k0[0], k0[1]};
+    }
+
+    // S3_LM = sum_D w^3 Yhat_LM - alpha^3 sum_R w^3 Yhat_LM for M = -L..L (field.hpp:1212-1232);
+    // M < 0 from Yhat_{L,-M} = (-1)^M conj Yhat_{L,M}
+    std::map<int, std::vector<double>> s3_cache;  // per L: [M + L] complex, for s3_alpha
+    double s3_alpha = 0.0;
+    std::array<double, 2> survey_s3(int L, int M, double alpha) {
+        if (alpha != s3_alpha) {
+            s3_cache.clear();
+            s3_alpha = alpha;
+        }
+        auto it = s3_cache.find(L);
+        if (it == s3_cache.end()) {
+            PSumSpec q{};
+            q.n = L + 1;
+            HG_REQUIRE(q.n <= HG_PSUM_MAX, "ELL too large");
+            for (int m = 0; m <= L; m++) {
+                q.pw[m] = 3;
+                q.l[m] = L;
+                q.m[m] = m;
+            }
+            std::vector<double> sD = particle_sums(0, q), sR = particle_sums(1, q);
+            const double a3 = alpha * alpha * alpha;
+            std::vector<double> v(2 * (2 * L + 1));
+            for (int m = 0; m <= L; m++) {
+                const double re = sD[2 * m] - a3 * sR[2 * m], im = sD[2 * m + 1] - a3 * sR[2 * m + 1];
+                const double sg = (m % 2) ? -1.0 : 1.0;
+                v[2 * (L + m)] = re;
+                v[2 * (L + m) + 1] = im;
+                v[2 * (L - m)] = sg * re;
+                v[2 * (L - m) + 1] = -sg * im;
+            }
+            it = s3_cache.emplace(L, std::move(v)).first;
+        }
+        return {it->second[2 * (L + M)], it->second[2 * (L + M) + 1]};
+    }
+
+    template <int LZ>
+    void launch_line_L(const HistSpec &hs, double *hist) {
+        size_t smem = OrbitCfg<T, LZ>::smem();
+        HG_CK(cudaFuncSetAttribute(k_xi_line_hist<T, LZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const long long nl = (long long)g.n[0] * g.n[1];
+        const unsigned blocks = (unsigned)((nl + OrbitCfg<T, LZ>::B - 1) / OrbitCfg<T, LZ>::B);
+        kb("xi_line_hist", double(g.ntot) * sizeof(C));
+        k_xi_line_hist<T, LZ><<<blocks, OrbitCfg<T, LZ>::NT, smem, st>>>(dp<C>(xi), g.n[0], g.n[1], twiddles(LZ), hs,
+                                                                         n2dim, hist);
+        ke();
+    }
+    void launch_line(const HistSpec &hs, double *hist) {
+        switch (g.n[2]) {
+            case 8: launch_line_L<8>(hs, hist); break;
+            case 16: launch_line_L<16>(hs, hist); break;
+            case 32: launch_line_L<32>(hs, hist); break;
+            case 64: launch_line_L<64>(hs, hist); break;
+            case 128: launch_line_L<128>(hs, hist); break;
+            case 256: launch_line_L<256>(hs, hist); break;
+            case 512: launch_line_L<512>(hs, hist); break;
+            case 1024: launch_line_L<1024>(hs, hist); break;
+            default: throw HgError{"unsupported n_mesh_z"};
+        }
+    }
+
+    // hist_sv[mp][n2] = sum over M and the (m1, m2) of that M of w sum_{|x|^2 = n2} xi_LM(x)
+    // Yhat_l1m1(x) Yhat_l2m2(x), with xi_LM = FFT_+[(dn_LM conj N_00 - S3_LM C) / W^2 / V]
+    // (calcShotNoiseForBispectrum_ijk field.hpp:1116-1160; bispec.hpp:124-196, 400-460)
+    void survey_histograms(const std::vector<MP> &mps) {
+        HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
+                   "bispectrum / 3PCF shot noise needs equal cell sizes on all axes");
+        build_orbits();
+        std::vector<MP> todo;
+        for (const auto &mp : mps) {
+            std::array<int, 3> key{mp.l1, mp.l2, mp.L};
+            bool queued = false;
+            for (const auto &q : todo) queued |= (q.l1 == mp.l1 && q.l2 == mp.l2 && q.L == mp.L);
+            if (!hist_sv_ok.count(key) && !queued) todo.push_back(mp);
+        }
+        if (todo.empty()) return;
+        for (const auto &mp : todo) {
+            auto &p = hist_sv[{mp.l1, mp.l2, mp.L}];
+            if (!p) p = std::make_unique<DBuf>();
+            HG_CK(p->ensure(sizeof(double) * 2 * n2dim));
+            HG_CK(cudaMemsetAsync(p->p, 0, sizeof(double) * 2 * n2dim, st));
+        }
+        const double alpha = src_alpha;
+        const SpecK n00 = sfield(SF_SN, 0, 0, alpha);
+        std::set<int> Ls;
+        for (const auto &mp : todo) Ls.insert(mp.L);
+        HG_CK(xi.ensure(sizeof(C) * g.ntot));
+        xi_valid = false;  // the box correlation field is overwritten
+        for (int L : Ls)
+            for (int M = -L; M <= L; M++) {
+                std::vector<std::pair<MP, std::vector<Combo3>>> hm;
+                for (const auto &mp : todo) {
+                    if (mp.L != L) continue;
+                    std::vector<Combo3> cs;
+                    for (const auto &c : combos3(mp, true))
+                        if (c.M == M) cs.push_back(c);
+                    if (!cs.empty()) hm.push_back({mp, cs});
+                }
+                if (hm.empty()) continue;
+                const SpecK f1 = sfield(SF_DELTA, L, M, alpha);
+                const std::array<double, 2> S3 = survey_s3(L, M, alpha);
+                // (f1 conj f2)(0) from the exact k = 0 values
+                const double k0r = f1.k0r * n00.k0r + f1.k0i * n00.k0i, k0i = f1.k0i * n00.k0r - f1.k0r * n00.k0i;
+                LdXiCross<T> ld{f1.s, n00.s, g.n[2], xtabs, S3[0], S3[1], k0r, k0i, 1.0 / g.volume};
+                const long long yz = (long long)g.n[1] * g.n[2];
+                pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
+                         double(g.ntot) * sizeof(C) * 2.0);
+                pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0],
+                         g.n[2], "fft_xi_y");
+                for (size_t h0 = 0; h0 < hm.size(); h0 += HG_MAX_HIST) {
+                    HistSpec hs;
+                    memset(&hs, 0, sizeof(hs));
+                    hs.nh = (int)std::min<size_t>(HG_MAX_HIST, hm.size() - h0);
+                    for (int h = 0; h < hs.nh; h++) {
+                        const auto &e = hm[h0 + h];
+                        HG_REQUIRE(e.second.size() <= 12, "too many (m1, m2) terms in one multipole");
+                        hs.parity[h] = 1;
+                        for (const auto &c : e.second)
+                            hs.term[h][hs.nterm[h]++] = YTerm{e.first.l1, c.m1, e.first.l2, c.m2, c.w};
+                    }
+                    HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim * hs.nh));
+                    HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim * hs.nh, st));
+                    launch_line(hs, dp<double>(hist_tmp));
+                    for (int h = 0; h < hs.nh; h++) {
+                        const MP &mp = hm[h0 + h].first;
+                        double *dst = dp<double>(*hist_sv[{mp.l1, mp.l2, mp.L}]);
+                        k_axpy<<<grid1(2 * n2dim, 256), 256, 0, st>>>(dst, dp<double>(hist_tmp) + 2 * n2dim * h,
+                                                                      2 * n2dim);
+                        HG_CK(cudaGetLastError());
+                    }
+                }
+            }
+        for (const auto &mp : todo) hist_sv_ok.insert({mp.l1, mp.l2, mp.L});
+    }
+
+    static bool needs_los(const std::vector<MP> &mps) {
+        for (const auto &mp : mps)
+            if (mp.l1 || mp.l2 || mp.L) return true;
+        return false;
+    }
+
+    // calcNormalizationForBiSpectrum (particle.hpp:319-332): V_s^2 / (sum w_D)^3
+    double survey_bk_norm(double vs) {
+        PSumSpec q{};
+        q.n = 1;
+        q.pw[0] = 1;
+        q.l[0] = -1;
+        const double wD = particle_sums(0, q)[0];
+        HG_REQUIRE(wD != 0.0, "the summed data weights must be non-zero");
+        double nv = vs / wD / wD;
+        nv *= (vs / wD);
+        return nv;
+    }
+
+    // calcBiSpectrum (bispec.hpp:4-352) for all k1 rows (ith = -1) or one, several multipoles
+    void bk_survey_multi(const std::vector<MP> &mps, int ith, double alpha, double vs, double *bk_save,
+                         double *sn_save, double *norm) override {
+        check_multipoles(mps);
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_kbin, "ith_kbin out of range");
+        require_survey(needs_los(mps));
+        begin();
+        set_source(1, alpha);
+        const int ns = cfg.n_kbin;
+        std::vector<std::vector<double>> B = bk_main(mps);
+        // shot noise (bispec.hpp:20-214): S3 term, P terms, xi term
+        const SpecK dn00 = sfield(SF_DELTA, 0, 0, alpha);
+        std::vector<std::vector<double>> SN(mps.size(), std::vector<double>(2 * ns * ns, 0.0));
+        std::vector<unsigned long long> nm;
+        for (size_t q = 0; q < mps.size(); q++) {
+            const MP &mp = mps[q];
+            for (const auto &c : combos3(mp, true)) {
+                const std::array<double, 2> S3 = survey_s3(mp.L, c.M, alpha);
+                if (mp.l1 == 0 && mp.l2 == 0)
+                    for (int e = 0; e < ns * ns; e++) {
+                        SN[q][2 * e] += c.w * S3[0];
+                        SN[q][2 * e + 1] += c.w * S3[1];
+                    }
+                if (mp.l2 == 0 || mp.l1 == 0) {
+                    const SpecK nlm = sfield(SF_SN, mp.L, c.M, alpha);
+                    if (mp.l2 == 0) {  // the k1 row's value on every k2
+                        std::vector<double> avg;
+                        pk_bin2(dn00.s, nlm.s, {LM{mp.l1, c.m1}}, S3[0], S3[1], avg, nm);
+                        for (int i1 = 0; i1 < ns; i1++)
+                            for (int i2 = 0; i2 < ns; i2++) {
+                                SN[q][2 * (i1 * ns + i2)] += c.w * avg[2 * i1];
+                                SN[q][2 * (i1 * ns + i2) + 1] += c.w * avg[2 * i1 + 1];
+                            }
+                    }
+                    if (mp.l1 == 0) {
+                        std::vector<double> avg;
+                        pk_bin2(dn00.s, nlm.s, {LM{mp.l2, c.m2}}, S3[0], S3[1], avg, nm);
+                        for (int i1 = 0; i1 < ns; i1++)
+                            for (int i2 = 0; i2 < ns; i2++) {
+                                SN[q][2 * (i1 * ns + i2)] += c.w * avg[2 * i2];
+                                SN[q][2 * (i1 * ns + i2) + 1] += c.w * avg[2 * i2 + 1];
+                            }
+                    }
+                }
+            }
+        }
+        survey_histograms(mps);
+        for (size_t q = 0; q < mps.size(); q++)
+            bk_sn_xi(mps[q], dp<double>(*hist_sv[{mps[q].l1, mps[q].l2, mps[q].L}]), SN[q]);
+        const int r0 = (ith < 0) ? 0 : ith, r1 = (ith < 0) ? ns : ith + 1;
+        const int rows = r1 - r0;
+        for (size_t q = 0; q < mps.size(); q++)
+            for (int i1 = r0; i1 < r1; i1++)
+                for (int i2 = 0; i2 < ns; i2++) {
+                    long long o = ((long long)q * rows + (i1 - r0)) * ns + i2;
+                    bk_save[2 * o] = B[q][2 * (i1 * ns + i2)];
+                    bk_save[2 * o + 1] = B[q][2 * (i1 * ns + i2) + 1];
+                    sn_save[2 * o] = SN[q][2 * (i1 * ns + i2)];
+                    sn_save[2 * o + 1] = SN[q][2 * (i1 * ns + i2) + 1];
+                }
+        if (norm) *norm = survey_bk_norm(vs);
+        end();
+    }
+
+    // calcThreePointCorrelationFunction (bispec.hpp:355-614), all r1 rows or one
+    void zeta_survey_multi(const std::vector<MP> &mps, int ith, double alpha, double vs, double *zeta_save,
+                           double *sn_save, double *norm) override {
+        check_multipoles(mps);
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_rbin, "ith_rbin out of range");
+        require_survey(needs_los(mps));
+        begin();
+        zeta_geometry();
+        set_source(1, alpha);
+        std::vector<std::vector<double>> Z = zeta_main(mps, ith);
+        survey_histograms(mps);
+        std::vector<const double *> hs;
+        for (const auto &mp : mps) hs.push_back(dp<double>(*hist_sv[{mp.l1, mp.l2, mp.L}]));
+        zeta_finish(mps, ith, Z, hs, zeta_save, sn_save);
+        if (norm) *norm = survey_bk_norm(vs);
+        end();
     }
 
     // calcPowerSpectrum (powerspec.hpp:4-91): sum over M of w3j-weighted binned
@@ -1774,14 +2164,14 @@ struct Engine : public hg_ctx {
         q.l[0] = -1;
         const double wD = particle_sums(0, q)[0];
         HG_REQUIRE(wD != 0.0, "the summed data weights must be non-zero");
-        const Spec<T> f00 = survey_field(0, 0, alpha);
+        const Spec<T> f00 = sfield(SF_DELTA, 0, 0, alpha).s;
         std::vector<double> acc(2 * nb, 0.0);
         std::vector<unsigned long long> nm;
         for (int M = -ell; M <= ell; M++) {
             const int am = M < 0 ? -M : M;
             double Sr = sD[2 * am] + alpha * alpha * sR[2 * am];
             double Si = sD[2 * am + 1] + alpha * alpha * sR[2 * am + 1];
-            const Spec<T> f1 = survey_field(ell, am, alpha);
+            const Spec<T> f1 = sfield(SF_DELTA, ell, am, alpha).s;
             const double sg = (am % 2) ? -1.0 : 1.0;
             if (M < 0) {  // dn_{l,-|M|}(k) = (-1)^|M| conj(dn_{l,|M|}(-k)); likewise S
                 Sr = sg * Sr;
@@ -1922,6 +2312,34 @@ int hg_zeta_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rb
     std::vector<MP> mps;
     for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
     HG_GUARD(ctx, ctx->zeta_box_multi(mps, ith_rbin, zeta_save, sn_save, norm));
+}
+
+int hg_bk_survey(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_kbin, double alpha, double vsurvey,
+                 double *bk_save, double *sn_save, double *norm) {
+    if (!bk_save || !sn_save) return -1;
+    HG_GUARD(ctx, ctx->bk_survey_multi({MP{ell1, ell2, ELL}}, ith_kbin, alpha, vsurvey, bk_save, sn_save, norm));
+}
+
+int hg_bk_survey_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double alpha, double vsurvey,
+                       double *bk_save, double *sn_save, double *norm) {
+    if (!bk_save || !sn_save || !ells || n_multipoles <= 0) return -1;
+    std::vector<MP> mps;
+    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
+    HG_GUARD(ctx, ctx->bk_survey_multi(mps, ith_kbin, alpha, vsurvey, bk_save, sn_save, norm));
+}
+
+int hg_zeta_survey(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double alpha, double vsurvey,
+                   double *zeta_save, double *sn_save, double *norm) {
+    if (!zeta_save || !sn_save) return -1;
+    HG_GUARD(ctx, ctx->zeta_survey_multi({MP{ell1, ell2, ELL}}, ith_rbin, alpha, vsurvey, zeta_save, sn_save, norm));
+}
+
+int hg_zeta_survey_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double alpha, double vsurvey,
+                         double *zeta_save, double *sn_save, double *norm) {
+    if (!zeta_save || !sn_save || !ells || n_multipoles <= 0) return -1;
+    std::vector<MP> mps;
+    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
+    HG_GUARD(ctx, ctx->zeta_survey_multi(mps, ith_rbin, alpha, vsurvey, zeta_save, sn_save, norm));
 }
 
 int hg_survey_scalars(hg_ctx *ctx, double *alpha, double *vsurvey, double *nbar, double *wsum_data,

@@ -68,6 +68,21 @@ __global__ void k_interlace(cplx<T> *F, const cplx<T> *Fs, int n0, int n1, int n
     }
 }
 
+// out[k] = sgn conj(in[-k]) over a full spectrum: the transform of the conjugated weights
+// (F_{l,-m} = (-1)^m conj F_{l,m}(-k) since Yhat_{l,-m} = (-1)^m conj Yhat_{l,m}).
+template <typename T>
+__global__ void k_mirror(const cplx<T> *in, cplx<T> *out, int n0, int n1, int n2, T sgn) {
+    const long long total = (long long)n0 * n1 * n2;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int iz = (int)(idx % n2);
+        int iy = (int)((idx / n2) % n1);
+        int ix = (int)(idx / ((long long)n2 * n1));
+        cplx<T> v = in[((long long)((n0 - ix) % n0) * n1 + (n1 - iy) % n1) * n2 + (n2 - iz) % n2];
+        out[idx] = mk<T>(sgn * v.x, -sgn * v.y);
+    }
+}
+
 // Shell entries: wrapped mode (nx, ny, nz) and shell index.
 struct ShellEnt {
     int nx, ny, nz, shell;
@@ -205,6 +220,33 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
     }
 };
 
+// Cross-spectrum version for the survey (field.hpp:1116-1160): (f1 conj f2 - S C(k)) / W^2 / V
+// with complex S, f1 = the Yhat_LM-weighted D - alpha R field, f2 = the w^2 D + alpha^2 R field.
+template <typename T>
+struct LdXiCross {
+    Spec<T> f1, f2;
+    int n2;
+    XiTabs xt;
+    double S_re, S_im;
+    double k0_re, k0_im;  // (f1 conj f2)(k = 0) from the FP64 field integrals
+    double invV;
+    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
+        int ix = l;
+        int iy = (int)(i / n2);
+        int iz = (int)(i - (long long)iy * n2);
+        zd p2;
+        if (ix == 0 && iy == 0 && iz == 0) {
+            p2 = mk<double>(k0_re, k0_im);
+        } else {
+            p2 = f1.at(ix, iy, iz) * conjg(f2.at(ix, iy, iz));
+        }
+        double C = xt.cf[0][ix] * xt.cf[1][iy] * xt.cf[2][iz];
+        if (xt.interlace) C = 0.5 * (C + xt.df[0][ix] * xt.df[1][iy] * xt.df[2][iz]);
+        double iw = xt.iw2[0][ix] * xt.iw2[1][iy] * xt.iw2[2][iz];
+        return mk<T>((T)(invV * ((p2.x - S_re * C) * iw)), (T)(invV * ((p2.y - S_im * C) * iw)));
+    }
+};
+
 // One product of reduced harmonics with its Wigner weight: w Yhat_l1m1 Yhat_l2m2.
 struct YTerm {
     int l1, m1, l2, m2;
@@ -292,6 +334,60 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
             if (val.y != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2) + 1], val.y);
         }
     }
+}
+
+// The same histogram for weights that also depend on the azimuth (the survey's M != 0
+// terms, m1 + m2 = -M): every (x, y) line on its own, B lines per CTA; the z <-> -z pair of
+// a line shares n^2 and is added once.  f_h = sum_terms w Yhat_l1m1 Yhat_l2m2 at the cell.
+template <typename T, int L>
+__global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
+    k_xi_line_hist(const cplx<T> *xi, int n0, int n1, const cplx<T> *tw, HistSpec hs, long long n2dim, double *hist) {
+    using OC = OrbitCfg<T, L>;
+    constexpr int B = OC::B, LP = OC::LP, NT = OC::NT;
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *s = reinterpret_cast<cplx<T> *>(smem_raw);
+    const long long nlines = (long long)n0 * n1;
+    const int b = threadIdx.x / R2, t = threadIdx.x % R2;
+    const long long line = (long long)blockIdx.x * B + b;
+    cplx<T> v[R1];
+#pragma unroll
+    for (int n1_ = 0; n1_ < R1; n1_++) v[n1_] = (line < nlines) ? xi[line * L + R2 * n1_ + t] : mk<T>(0, 0);
+    line_fft2<T, L, +1, false, B>(v, s, t, b, tw);
+#pragma unroll
+    for (int r = 0; r < R1; r++) s[b * LP + pos_of_reg<L>(t, r)] = v[r];
+    __syncthreads();
+    for (int q = threadIdx.x; q < B * (L / 2 + 1); q += NT) {
+        const int bb = q / (L / 2 + 1), iz = q % (L / 2 + 1);
+        const long long ln = (long long)blockIdx.x * B + bb;
+        if (ln >= nlines) continue;
+        const int wx = wrap_index((int)(ln / n1), n0), wy = wrap_index((int)(ln % n1), n1);
+        const int iz2 = (L - iz) % L;
+        const int wz = wrap_index(iz, L);
+        const cplx<T> a = s[bb * LP + iz], c = s[bb * LP + iz2];
+        const long long n2 = (long long)wx * wx + (long long)wy * wy + (long long)wz * wz;
+        for (int h = 0; h < hs.nh; h++) {
+            zd fp = mk<double>(0.0, 0.0), fm = mk<double>(0.0, 0.0);
+            for (int k = 0; k < hs.nterm[h]; k++) {
+                const YTerm &yt = hs.term[h][k];
+                fp = fp + (ylm_reduced(yt.l1, yt.m1, (double)wx, (double)wy, (double)wz) *
+                           ylm_reduced(yt.l2, yt.m2, (double)wx, (double)wy, (double)wz)) * yt.w;
+                if (iz2 != iz)
+                    fm = fm + (ylm_reduced(yt.l1, yt.m1, (double)wx, (double)wy, (double)(-wz)) *
+                               ylm_reduced(yt.l2, yt.m2, (double)wx, (double)wy, (double)(-wz))) * yt.w;
+            }
+            zd val = fp * mk<double>((double)a.x, (double)a.y);
+            if (iz2 != iz) val = val + fm * mk<double>((double)c.x, (double)c.y);
+            if (val.x != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2)], val.x);
+            if (val.y != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2) + 1], val.y);
+        }
+    }
+}
+
+// y += x (n doubles)
+__global__ void k_axpy(double *y, const double *x, long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += x[i];
 }
 
 // Natural-spline evaluation of j_l at x (knots xmin + dx i, bessel.hpp:14-25).
@@ -426,14 +522,15 @@ inline int sn_partial_blocks(long long n2dim) {
 // Per-mode factor of the 3PCF filtered fields (field.hpp:403-445) without the Bessel weight:
 //   U(k) = Yhat_lm(k) delta(k) / W(k) / V        over the full grid, delta(0) = k0_re.
 template <typename T>
-__global__ void k_zeta_U(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int l, int m, double k0_re, cplx<T> *U) {
+__global__ void k_zeta_U(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int l, int m, double k0_re, double k0_im,
+                         cplx<T> *U) {
     const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         int iz = (int)(idx % g.n[2]);
         int iy = (int)((idx / g.n[2]) % g.n[1]);
         int ix = (int)(idx / ((long long)g.n[2] * g.n[1]));
-        zd d = (ix == 0 && iy == 0 && iz == 0) ? mk<double>(k0_re, 0.0) : f.at(ix, iy, iz);
+        zd d = (ix == 0 && iy == 0 && iz == 0) ? mk<double>(k0_re, k0_im) : f.at(ix, iy, iz);
         double wf = window_tab(tabs, ix, iy, iz, wpow);
         zd y = ylm_reduced(l, m, kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
                            kcomp(wrap_index(iz, g.n[2]), g.dk[2]));

@@ -121,6 +121,30 @@ int hg_zeta_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double *
 int hg_zeta_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double *zeta_save,
                       double *sn_save, double *norm);
 
+/* Survey-geometry bispectrum multipole with local line of sight.  Replaces calcBiSpectrum
+ * (bispec.hpp:4-352): shell fields of the data-minus-randoms field, the Yhat_LM-weighted
+ * G_LM fields for every M, the (m1, m2, M) sums with Wigner-3j weights, and the shot
+ * noise (S3, P and correlation-field terms, bispec.hpp:20-214).  alpha and vsurvey as
+ * for hg_pk_survey.  Layout as hg_bk_box; *norm = V_survey^2 / (sum w_D)^3
+ * (particle.hpp:319-332).  Needs equal cell sizes on all axes. */
+int hg_bk_survey(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_kbin, double alpha, double vsurvey,
+                 double *bk_save, double *sn_save, double *norm);
+
+/* Several survey bispectrum multipoles in one call (layout as hg_bk_box_multi); each block
+ * equals what calcBiSpectrum (bispec.hpp:4-352) computes for that multipole. */
+int hg_bk_survey_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double alpha, double vsurvey,
+                       double *bk_save, double *sn_save, double *norm);
+
+/* Survey-geometry 3PCF multipole.  Replaces calcThreePointCorrelationFunction
+ * (bispec.hpp:355-614).  Layout as hg_zeta_box; the shot noise sits on the diagonal;
+ * *norm = V_survey^2 / (sum w_D)^3.  Needs a cubic box and mesh. */
+int hg_zeta_survey(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double alpha, double vsurvey,
+                   double *zeta_save, double *sn_save, double *norm);
+
+/* Several survey 3PCF multipoles in one call (layout as hg_zeta_box_multi). */
+int hg_zeta_survey_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double alpha, double vsurvey,
+                         double *zeta_save, double *sn_save, double *norm);
+
 /* Survey-geometry scalars on the current data (slot 0) and randoms (slot 1):
  * alpha = sum w_D / sum w_R (particle.hpp:268-282), V_survey = (sum w_R)^2 /
  * sum_cells n_R^2 dV (field.hpp:449-503), nbar (particle.hpp:284-300), and the summed

@@ -8,6 +8,7 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py          (needs `make -C oracle` first)
     python tests/golden/make_golden.py --zeta   (only box_zeta.npz)
     python tests/golden/make_golden.py --survey (only survey_pk.npz)
+    python tests/golden/make_golden.py --survey3 (only survey_bk_zeta.npz)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
 """
@@ -28,6 +29,7 @@ from oracle import ref_runner  # noqa: E402
 
 MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2))
 ZETA_MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (0, 2, 2), (1, 1, 2))
+SURVEY_MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (1, 1, 2))
 
 
 def binning_arr(b: Binning):
@@ -116,6 +118,23 @@ def make_survey():
     np.savez_compressed(os.path.join(HERE, "survey_pk.npz"), **d)
 
 
+def make_survey_three_point():
+    """Survey-geometry bispectrum (bispec.hpp:4-352) and 3PCF (bispec.hpp:355-614)
+    multipoles, all rows; (202) and (112) have M != 0 terms."""
+    data, rand = survey_shell(2000, 30000, seed=18)
+    b = Binning(0.004, 0.02, 5, 150.0, 750.0, 5)
+    d = dict(data=data, rand=rand, boxsize=3500.0, n_mesh=32, binning=binning_arr(b))
+    for mp in SURVEY_MULTIPOLES:
+        tag = "".join(map(str, mp))
+        with ref_runner.RefRun() as r:
+            r.run("bk", data, *mp, 32, 3500.0, b, assign="TSC", randoms=rand)
+            d["bk_" + tag] = r.bk(*mp, b.n_kbin)
+        with ref_runner.RefRun() as r:
+            r.run("3PCF", data, *mp, 32, 3500.0, b, assign="TSC", randoms=rand)
+            d["zeta_" + tag] = r.zeta(*mp, b.n_rbin)
+    np.savez_compressed(os.path.join(HERE, "survey_bk_zeta.npz"), **d)
+
+
 def make_extensions():
     """PCS assignment and interlacing are not in the reference: their fixtures come from
     the numpy restatement oracle/restate.py, which tests/test_oracle_restate.py pins to the
@@ -148,11 +167,13 @@ def main():
         return
     if not ref_runner.available():
         raise SystemExit("build the oracle first: make -C oracle")
-    if "--zeta" in sys.argv or "--survey" in sys.argv:
+    if "--zeta" in sys.argv or "--survey" in sys.argv or "--survey3" in sys.argv:
         if "--zeta" in sys.argv:
             make_zeta()
         if "--survey" in sys.argv:
             make_survey()
+        if "--survey3" in sys.argv:
+            make_survey_three_point()
         print("fixtures written")
         return
     # smoke case
@@ -206,6 +227,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "box_noncubic.npz"), **d)
     make_zeta()
     make_survey()
+    make_survey_three_point()
     make_extensions()
     print("fixtures written")
 
