@@ -12,6 +12,7 @@ plain FP64 form, with the per-bin relative difference between them.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--small]
   python bench.py --lean --forms fp32 [--n-mesh M --n-particles P]   (profiling runs)
+  python bench.py --config {1,2,3,5} [--cpu]   (the other configurations; not the headline)
 Under torchrun every rank runs its own mocks (weak scaling, no data-path collective).
 """
 from __future__ import annotations
@@ -207,6 +208,151 @@ def run_reference(args, wl, world, rank):
     return 0
 
 
+def run_config(args) -> int:
+    """The other BASELINE configurations, measured end to end through the public API (the
+    catalogue copied from host memory every mock), both forms, FP32-vs-FP64 error per
+    statistic; with --cpu also the reference's own code (oracle/_ref) timed on this host:
+    directly where a mock takes seconds, else extrapolated from timed parts (stated)."""
+    import torch
+    from hitomi_b200.api import Binning, Context
+    from hitomi_b200.synthetic import lognormal_box, survey_shell, uniform_box
+    from hitomi_b200 import survey
+    cfg = args.config
+    stats = {}
+    if cfg == 1:
+        name = "box P_l l=0,2,4: 2e5 uniform, 128^3, TSC+interlacing, k 0.005-0.295 (30 bins)"
+        mocks = [uniform_box(200_000, 1000.0, seed=1 + i) for i in range(4)]
+        setup = dict(n_mesh=128, boxsize=1000.0, b=Binning(0.005, 0.295, 30), assign="TSC", interlace=True)
+    elif cfg == 2:
+        name = "box P_l l=0,2,4: lognormal 1e7 (RSD f=0.7), 512^3, PCS+interlacing"
+        mocks = [catalogue(workload(False), 2 + i) for i in range(2)]
+        setup = dict(n_mesh=512, boxsize=1000.0, b=Binning(0.005, 0.295, 30), assign="PCS", interlace=True)
+    elif cfg == 3:
+        name = "survey P_l l=0,2,4 (local LOS): 1e6 data + 5e7 randoms, shell 1000-1800, 60x60 deg cap, 512^3, box 3500, TSC"
+        d, r = survey_shell(1_000_000, 50_000_000, seed=3)
+        mocks = [survey.prepare(d, r, 512, 3500.0)]
+        setup = dict(n_mesh=512, boxsize=3500.0, b=Binning(0.005, 0.295, 30), assign="TSC", interlace=False)
+    elif cfg == 5:
+        name = "batched covariance: P_l l=0,2,4 + zeta (000,110,202), 20 r bins 4-156, 256^3, N_p ~ N(2e6, 4e5)"
+        rng = np.random.default_rng(1000)
+        mocks = [lognormal_box(max(int(rng.normal(2e6, 4e5)), 100_000), 1000.0, ngrid=128, seed=1000 + i)
+                 for i in range(args.n_mocks)]
+        setup = dict(n_mesh=256, boxsize=1000.0, b=Binning(0.015, 0.255, 25, 4.0, 156.0, 20), assign="TSC",
+                     interlace=False)
+    else:
+        raise SystemExit("--config takes 1, 2, 3 or 5 (4 is the default headline run)")
+    zmps = ((0, 0, 0), (1, 1, 0), (2, 0, 2))
+
+    def load(ctx, m, dev):
+        """host arrays through hg_set_particles, or device copies through hg_set_particles_device"""
+        if cfg == 3:
+            if dev is None:
+                ctx.set_survey(*m)
+            else:
+                for slot, t in ((0, dev[0]), (1, dev[1])):
+                    ctx.set_particles_device(slot, t.data_ptr(), t.shape[0], 56, 0, 3, 6, keep=t)
+        elif dev is None:
+            ctx.set_particles(0, m)
+        else:
+            ctx.set_particles_device(0, dev.data_ptr(), dev.shape[0], 24, keep=dev)
+
+    def one(ctx, m, dev=None):
+        out = {}
+        load(ctx, m, dev)
+        if cfg == 3:
+            a, vs, *_ = ctx.survey_scalars()
+            for ell in PK_ELLS:
+                pk, _, norm = ctx.pk_survey(ell, a, vs)
+                out[f"pk{ell}"] = norm * pk
+            return out
+        for ell in PK_ELLS:
+            pk, _, norm = ctx.pk_box(ell)
+            out[f"pk{ell}"] = norm * pk
+        if cfg == 5:
+            z, sn, norm = ctx.zeta_box_multi(zmps)
+            for q, mp in enumerate(zmps):
+                out["zeta" + "".join(map(str, mp))] = norm * (z[q] - sn[q]).real
+        return out
+
+    line = {"config": cfg, "workload": name, "unit": UNIT,
+            "timing": "per mock; *_mocks_per_s with the catalogue resident on the device, *_e2e_mocks_per_s "
+                      "copying it from (pageable) host arrays through hg_set_particles every mock",
+            "n_mocks": len(mocks), "data": "synthetic"}
+    devs = []
+    for m in mocks:
+        if cfg == 3:
+            devs.append(tuple(torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in m))
+        else:
+            devs.append(torch.from_numpy(np.ascontiguousarray(m)).cuda())
+    res = {}
+    for form in ("fp64", "fp32"):
+        with Context(setup["n_mesh"], setup["boxsize"], setup["b"], setup["assign"], form,
+                     interlace=setup["interlace"]) as ctx:
+            one(ctx, mocks[0])  # warm-up: tables, splines, buffers
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            outs = [one(ctx, m, d) for m, d in zip(mocks, devs)]
+            torch.cuda.synchronize()
+            dt = (time.perf_counter() - t0) / len(mocks)
+            t0 = time.perf_counter()
+            for m in mocks:
+                one(ctx, m)
+            torch.cuda.synchronize()
+            de = (time.perf_counter() - t0) / len(mocks)
+        res[form] = outs
+        line[f"{form}_mocks_per_s"] = 1.0 / dt
+        line[f"{form}_ms_per_mock"] = 1000.0 * dt
+        line[f"{form}_e2e_mocks_per_s"] = 1.0 / de
+    line["fp32_over_fp64"] = line["fp32_mocks_per_s"] / line["fp64_mocks_per_s"]
+    errs = {}
+    for k in res["fp64"][0]:
+        errs[k] = max(max_rel_err(a[k], b[k]) for a, b in zip(res["fp32"], res["fp64"]))
+        scale = max(float(np.max(np.abs(b[k]))) for b in res["fp64"])
+        errs[k + "_rel_to_max"] = max(float(np.max(np.abs(a[k] - b[k]))) for a, b in zip(res["fp32"], res["fp64"])) / scale
+    line["rel_err_fp32_vs_fp64"] = errs
+    if args.cpu:
+        line["cpu_reference"] = cpu_config(cfg, mocks, setup, zmps)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_config(cfg, mocks, setup, zmps):
+    """The reference's own code (oracle/_ref/ref_harness) on this host's cores."""
+    from oracle import cpu_baseline, ref_runner
+    if not ref_runner.available():
+        return {"unavailable": "oracle/_ref/ref_harness was not built on this machine"}
+    cores = cpu_baseline.host_cores()
+    b = setup["b"]
+    if cfg in (1, 2):
+        # the reference has neither PCS nor interlacing: its TSC path, one process per l
+        t = 0.0
+        for ell in PK_ELLS:
+            with ref_runner.RefRun() as r:
+                r.run("pk", mocks[0], ell, 0, ell, setup["n_mesh"], setup["boxsize"], b, assign="TSC")
+                t += r.wall
+        return {"mocks_per_s": cores / t, "per_mock_seconds": t, "cores": cores, "kind": "reference",
+                "sample": "direct: P_0, P_2, P_4 of one mock, TSC without interlacing (the reference has neither PCS "
+                          "nor interlacing), one single-core process per mock as in main.cpp:64-76"}
+    if cfg == 5:
+        # P_l directly; zeta from one timed row of (000) scaled by rows and (m1, m2) terms
+        m = mocks[0]
+        t = 0.0
+        for ell in PK_ELLS:
+            with ref_runner.RefRun() as r:
+                r.run("pk", m, ell, 0, ell, setup["n_mesh"], setup["boxsize"], b, assign="TSC")
+                t += r.wall
+        with ref_runner.RefRun() as r:
+            r.run("3PCF", m, 0, 0, 0, setup["n_mesh"], setup["boxsize"], b, assign="TSC", all_rows=False, ith=0)
+            trow = r.wall
+        terms = 1 + 3 + 1  # (m1, m2) terms of (000), (110), (202)
+        tz = trow * b.n_rbin * terms
+        return {"mocks_per_s": cores / (t + tz), "per_mock_seconds": t + tz, "cores": cores, "kind": "reference",
+                "sample": f"P_0,2,4 direct ({t:.1f} s); zeta extrapolated from one ith_rbin row of (000) "
+                          f"({trow:.1f} s) x {b.n_rbin} rows x {terms} (m1, m2) terms"}
+    return {"unavailable": "survey P at 512^3 with 5e7 randoms takes many minutes per l in the reference; "
+                           "not timed in the bench"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,7 +366,12 @@ def main():
                     help="profiling runs: device-resident steps only (no e2e, per-kernel or CPU legs)")
     ap.add_argument("--n-mesh", type=int, default=0, help="profiling size (not the headline workload)")
     ap.add_argument("--n-particles", type=float, default=0, help="profiling size (not the headline workload)")
+    ap.add_argument("--config", type=int, default=0, help="measure another BASELINE configuration (1, 2, 3, 5)")
+    ap.add_argument("--n-mocks", type=int, default=8, help="mocks timed for --config 5")
+    ap.add_argument("--cpu", action="store_true", help="with --config: also time the reference's CPU code")
     args = ap.parse_args()
+    if args.config:
+        return run_config(args)
     if not args.lean:
         args.warmup = max(args.warmup, 3)
     wl = workload(args.small, args.n_mesh, int(args.n_particles))

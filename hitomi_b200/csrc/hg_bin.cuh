@@ -95,7 +95,7 @@ struct Spec {
             cplx<T> v = p[((long long)ix * n1 + iy) * hz + iz];
             return mk<double>((double)v.x, (double)v.y);
         }
-        int jx = (n0 - ix) % n0, jy = (n1 - iy) % n1, jz = n2 - iz;
+        int jx = neg_index(ix, n0), jy = neg_index(iy, n1), jz = n2 - iz;
         cplx<T> v = p[((long long)jx * n1 + jy) * hz + jz];
         return mk<double>((double)v.x, -(double)v.y);
     }
@@ -108,7 +108,7 @@ struct SpecMirror {
     Spec<T> s;
     double sgn;
     __device__ __forceinline__ zd at(int ix, int iy, int iz) const {
-        zd v = s.at((s.n0 - ix) % s.n0, (s.n1 - iy) % s.n1, (s.n2 - iz) % s.n2);
+        zd v = s.at(neg_index(ix, s.n0), neg_index(iy, s.n1), neg_index(iz, s.n2));
         return mk<double>(sgn * v.x, -sgn * v.y);
     }
 };
@@ -139,10 +139,12 @@ __global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt,
     const long long total = (long long)cnt.x * cnt.y * cnt.z;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        int nz = lo.z + (int)(idx % cnt.z);
-        int ny = lo.y + (int)((idx / cnt.z) % cnt.y);
-        int nx = lo.x + (int)(idx / ((long long)cnt.z * cnt.y));
-        int ix = (nx + g.n[0]) % g.n[0], iy = (ny + g.n[1]) % g.n[1], iz = (nz + g.n[2]) % g.n[2];
+        int nx, ny, nz;
+        split3((unsigned)idx, (unsigned)cnt.y, (unsigned)cnt.z, nx, ny, nz);
+        nx += lo.x;
+        ny += lo.y;
+        nz += lo.z;
+        const int ix = nx < 0 ? nx + g.n[0] : nx, iy = ny < 0 ? ny + g.n[1] : ny, iz = nz < 0 ? nz + g.n[2] : nz;
         double kv[3] = {kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
                         kcomp(wrap_index(iz, g.n[2]), g.dk[2])};
         double kmag = kmag_exact(kv[0], kv[1], kv[2]);

@@ -48,6 +48,19 @@ typedef cplx<float> zf;
 // of field.hpp:363-365: index i < n/2 is i, otherwise i - n.
 __host__ __device__ __forceinline__ int wrap_index(int i, int n) { return (i < n / 2) ? i : i - n; }
 
+// (a, b, c) with idx = (a * nb + b) * nc + c, in 32-bit unsigned arithmetic (every linear
+// index of a supported mesh is below 2^31; 64-bit division costs several times more)
+__device__ __forceinline__ void split3(unsigned idx, unsigned nb, unsigned nc, int &a, int &b, int &c) {
+    const unsigned q = idx / nc;
+    c = (int)(idx - q * nc);
+    const unsigned r = q / nb;
+    b = (int)(q - r * nb);
+    a = (int)r;
+}
+
+// (n - i) mod n for 0 <= i < n: the index of -k
+__host__ __device__ __forceinline__ int neg_index(int i, int n) { return i ? n - i : 0; }
+
 // Axis constants shared by the k-space kernels (all FP64).
 struct Grid {
     int n[3];          // mesh cells per axis

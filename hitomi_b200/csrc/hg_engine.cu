@@ -1092,6 +1092,17 @@ struct Engine : public hg_ctx {
     }
 
     // xi after its x and y inverse passes (cached per catalogue)
+    // the correlation-field spectrum synthesised into xi, then its x pass in place
+    template <class LD>
+    void xi_x_pass(const LD &ld) {
+        const long long yz = (long long)g.n[1] * g.n[2];
+        unsigned blocks = (unsigned)std::min<long long>(grid1(g.ntot, 256), 148 * 16);
+        kb("xi_synth", double(g.ntot) * sizeof(C) * 1.5);
+        k_synth<T, LD><<<blocks, 256, 0, st>>>(ld, g.n[0], yz, dp<C>(xi));
+        ke();
+        pass<+1>(g.n[0], LdArr<T>{dp<C>(xi), g.n[0], yz}, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x");
+    }
+
     void ensure_xi() {
         HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
                    "bispectrum / 3PCF shot noise needs equal cell sizes on all axes");
@@ -1101,9 +1112,7 @@ struct Engine : public hg_ctx {
         const double invV = 1.0 / g.volume;  // field.hpp:1122
         const double S = double(slot[0].n);
         LdXiHat<T> ld{half_spec(), g.n[2], xtabs, S, delta0 * N0, invV};
-        long long yz = (long long)g.n[1] * g.n[2];
-        pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
-                 double(g.ntot) * sizeof(C) * 1.5);
+        xi_x_pass(ld);
         pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
                  "fft_xi_y");
         xi_valid = true;
@@ -2010,9 +2019,7 @@ struct Engine : public hg_ctx {
                 // (f1 conj f2)(0) from the exact k = 0 values
                 const double k0r = f1.k0r * n00.k0r + f1.k0i * n00.k0i, k0i = f1.k0i * n00.k0r - f1.k0r * n00.k0i;
                 LdXiCross<T> ld{f1.s, n00.s, g.n[2], xtabs, S3[0], S3[1], k0r, k0i, 1.0 / g.volume};
-                const long long yz = (long long)g.n[1] * g.n[2];
-                pass<+1>(g.n[0], ld, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x_synth",
-                         double(g.ntot) * sizeof(C) * 2.0);
+                xi_x_pass(ld);
                 pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0],
                          g.n[2], "fft_xi_y");
                 for (size_t h0 = 0; h0 < hm.size(); h0 += HG_MAX_HIST) {

@@ -53,9 +53,8 @@ __global__ void k_interlace(cplx<T> *F, const cplx<T> *Fs, int n0, int n1, int n
     const long long total = (long long)n0 * n1 * nzs;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        int iz = (int)(idx % nzs);
-        int iy = (int)((idx / nzs) % n1);
-        int ix = (int)(idx / ((long long)nzs * n1));
+        int ix, iy, iz;
+        split3((unsigned)idx, (unsigned)n1, (unsigned)nzs, ix, iy, iz);
         int nz = half ? iz : wrap_index(iz, n2);
         double q = (double)wrap_index(ix, n0) / n0 + (double)wrap_index(iy, n1) / n1 + (double)nz / n2;
         double sn, cs;
@@ -75,10 +74,9 @@ __global__ void k_mirror(const cplx<T> *in, cplx<T> *out, int n0, int n1, int n2
     const long long total = (long long)n0 * n1 * n2;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        int iz = (int)(idx % n2);
-        int iy = (int)((idx / n2) % n1);
-        int ix = (int)(idx / ((long long)n2 * n1));
-        cplx<T> v = in[((long long)((n0 - ix) % n0) * n1 + (n1 - iy) % n1) * n2 + (n2 - iz) % n2];
+        int ix, iy, iz;
+        split3((unsigned)idx, (unsigned)n1, (unsigned)n2, ix, iy, iz);
+        cplx<T> v = in[((long long)neg_index(ix, n0) * n1 + neg_index(iy, n1)) * n2 + neg_index(iz, n2)];
         out[idx] = mk<T>(sgn * v.x, -sgn * v.y);
     }
 }
@@ -132,9 +130,11 @@ __global__ void k_scatter_G(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int3 lo,
     long long total = (long long)cnt.x * cnt.y * cnt.z;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        int nz = lo.z + (int)(idx % cnt.z);
-        int ny = lo.y + (int)((idx / cnt.z) % cnt.y);
-        int nx = lo.x + (int)(idx / ((long long)cnt.z * cnt.y));
+        int nx, ny, nz;
+        split3((unsigned)idx, (unsigned)cnt.y, (unsigned)cnt.z, nx, ny, nz);
+        nx += lo.x;
+        ny += lo.y;
+        nz += lo.z;
         int ix = mod_idx(nx, g.n[0]), iy = mod_idx(ny, g.n[1]), iz = mod_idx(nz, g.n[2]);
         zd d = (ix == 0 && iy == 0 && iz == 0) ? mk<double>(k0_re, k0_im) : f.at(ix, iy, iz);
         double wf = window_tab(tabs, ix, iy, iz, wpow);
@@ -204,8 +204,9 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
     double invV;
     __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
         int ix = l;
-        int iy = (int)(i / n2);
-        int iz = (int)(i - (long long)iy * n2);
+        const unsigned ui = (unsigned)i;
+        const int iy = (int)(ui / (unsigned)n2);
+        const int iz = (int)(ui - (unsigned)iy * (unsigned)n2);
         double p2;
         if (ix == 0 && iy == 0 && iz == 0) {
             p2 = k0;
@@ -232,8 +233,9 @@ struct LdXiCross {
     double invV;
     __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
         int ix = l;
-        int iy = (int)(i / n2);
-        int iz = (int)(i - (long long)iy * n2);
+        const unsigned ui = (unsigned)i;
+        const int iy = (int)(ui / (unsigned)n2);
+        const int iz = (int)(ui - (unsigned)iy * (unsigned)n2);
         zd p2;
         if (ix == 0 && iy == 0 && iz == 0) {
             p2 = mk<double>(k0_re, k0_im);
@@ -246,6 +248,19 @@ struct LdXiCross {
         return mk<T>((T)(invV * ((p2.x - S_re * C) * iw)), (T)(invV * ((p2.y - S_im * C) * iw)));
     }
 };
+
+// out[ix][i] = ld(0, ix, i) over the full grid (i = iy * nz + iz): the correlation-field
+// spectrum materialised by a grid-stride elementwise pass, so that the transform passes
+// that follow are plain loads.
+template <typename T, class LD>
+__global__ void k_synth(LD ld, int n0, long long yz, cplx<T> *out) {
+    const long long total = (long long)n0 * yz;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const unsigned u = (unsigned)idx, q = u / (unsigned)yz;
+        out[idx] = ld(0, (int)q, (long long)(u - q * (unsigned)yz));
+    }
+}
 
 // One product of reduced harmonics with its Wigner weight: w Yhat_l1m1 Yhat_l2m2.
 struct YTerm {
@@ -527,9 +542,8 @@ __global__ void k_zeta_U(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int l, int 
     const long long total = (long long)g.n[0] * g.n[1] * g.n[2];
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
-        int iz = (int)(idx % g.n[2]);
-        int iy = (int)((idx / g.n[2]) % g.n[1]);
-        int ix = (int)(idx / ((long long)g.n[2] * g.n[1]));
+        int ix, iy, iz;
+        split3((unsigned)idx, (unsigned)g.n[1], (unsigned)g.n[2], ix, iy, iz);
         zd d = (ix == 0 && iy == 0 && iz == 0) ? mk<double>(k0_re, k0_im) : f.at(ix, iy, iz);
         double wf = window_tab(tabs, ix, iy, iz, wpow);
         zd y = ylm_reduced(l, m, kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
@@ -549,8 +563,9 @@ struct LdZetaField {
     long long n2dim;
     int n0, n1, n2;
     __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
-        int iy = (int)(i / n2);
-        int iz = (int)(i - (long long)iy * n2);
+        const unsigned ui = (unsigned)i;
+        const int iy = (int)(ui / (unsigned)n2);
+        const int iz = (int)(ui - (unsigned)iy * (unsigned)n2);
         int wx = wrap_index(l, n0), wy = wrap_index(iy, n1), wz = wrap_index(iz, n2);
         long long q = (long long)wx * wx + (long long)wy * wy + (long long)wz * wz;
         double j = J[o * n2dim + q];
