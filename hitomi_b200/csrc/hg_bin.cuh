@@ -126,6 +126,19 @@ struct LMList {
 
 // P-binning over the mode cube [lo, lo+cnt) (wrapped modes).  acc: [nbin][nlm] complex,
 // nmode: [nbin].  lut maps the fine index int(|k|/1e-4 + 0.5) to up to two coarse bins.
+// Sum of v over the lanes of `grp` (a match_any group), valid in every member; all members
+// call it together.
+__device__ __forceinline__ double group_sum(double v, unsigned grp) {
+    double s = 0.0;
+    for (unsigned m = grp; m; m &= m - 1) s += __shfl_sync(grp, v, __ffs(m) - 1);
+    return s;
+}
+
+// Whole warps walk the mode cube together (every lane runs every iteration, so full-warp
+// intrinsics are safe); lanes whose modes fall in the same bin pool their values through
+// shuffles and one of them adds the pooled value to the block's shared-memory bins, which
+// keeps the number of (serialising) FP64 shared-memory atomics near one per bin per warp
+// step instead of one per mode.
 template <typename T, class F1, class F2>
 __global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt, const int2 *lut, int lutn,
                          int nbin, LMList lms, double S_re, double S_im, int assign, int wpow, double *acc,
@@ -137,45 +150,60 @@ __global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt,
     for (int q = threadIdx.x; q < nbin; q += blockDim.x) scnt[q] = 0ull;
     __syncthreads();
     const long long total = (long long)cnt.x * cnt.y * cnt.z;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        int nx, ny, nz;
-        split3((unsigned)idx, (unsigned)cnt.y, (unsigned)cnt.z, nx, ny, nz);
-        nx += lo.x;
-        ny += lo.y;
-        nz += lo.z;
-        const int ix = nx < 0 ? nx + g.n[0] : nx, iy = ny < 0 ? ny + g.n[1] : ny, iz = nz < 0 ? nz + g.n[2] : nz;
-        double kv[3] = {kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
-                        kcomp(wrap_index(iz, g.n[2]), g.dk[2])};
-        double kmag = kmag_exact(kv[0], kv[1], kv[2]);
-        int kindex = (int)__dadd_rn(__ddiv_rn(kmag, 0.0001), 0.5);
-        if (kindex >= lutn) continue;
-        int2 b = lut[kindex];
-        if (b.x < 0) continue;
-        zd d1 = f1.at(ix, iy, iz), d2 = f2.at(ix, iy, iz);
-        zd pk2;
-        if (k0_special && ix == 0 && iy == 0 && iz == 0) {
-            pk2 = mk<double>(k0_re, k0_im);
-        } else {
-            pk2 = d1 * conjg(d2);
-        }
-        double C = shot_tab(tabs, ix, iy, iz, assign);
-        pk2 = pk2 - mk<double>(S_re * C, S_im * C);
-        double wf = window_tab(tabs, ix, iy, iz, wpow);
-        double w2 = wf * wf;
-        pk2 = mk<double>(pk2.x / w2, pk2.y / w2);
-        for (int q = 0; q < lms.n; q++) {
-            zd y = ylm_reduced(lms.lm[q].l, lms.lm[q].m, kv[0], kv[1], kv[2]);
-            zd v = pk2 * y;
-            atomicAdd(&sacc[2 * (b.x * lms.n + q)], v.x);
-            atomicAdd(&sacc[2 * (b.x * lms.n + q) + 1], v.y);
-            if (b.y >= 0) {
-                atomicAdd(&sacc[2 * (b.y * lms.n + q)], v.x);
-                atomicAdd(&sacc[2 * (b.y * lms.n + q) + 1], v.y);
+    const int lane = threadIdx.x & 31;
+    const long long wstride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wbase < total; wbase += wstride) {
+        const long long idx = wbase + lane;
+        int2 b = make_int2(-1, -1);
+        zd pk2 = mk<double>(0.0, 0.0);
+        double kv[3] = {0.0, 0.0, 0.0};
+        if (idx < total) {
+            int nx, ny, nz;
+            split3((unsigned)idx, (unsigned)cnt.y, (unsigned)cnt.z, nx, ny, nz);
+            nx += lo.x;
+            ny += lo.y;
+            nz += lo.z;
+            const int ix = nx < 0 ? nx + g.n[0] : nx, iy = ny < 0 ? ny + g.n[1] : ny, iz = nz < 0 ? nz + g.n[2] : nz;
+            kv[0] = kcomp(wrap_index(ix, g.n[0]), g.dk[0]);
+            kv[1] = kcomp(wrap_index(iy, g.n[1]), g.dk[1]);
+            kv[2] = kcomp(wrap_index(iz, g.n[2]), g.dk[2]);
+            double kmag = kmag_exact(kv[0], kv[1], kv[2]);
+            int kindex = (int)__dadd_rn(__ddiv_rn(kmag, 0.0001), 0.5);
+            if (kindex < lutn) b = lut[kindex];
+            if (b.x >= 0) {
+                zd d1 = f1.at(ix, iy, iz), d2 = f2.at(ix, iy, iz);
+                if (k0_special && ix == 0 && iy == 0 && iz == 0) {
+                    pk2 = mk<double>(k0_re, k0_im);
+                } else {
+                    pk2 = d1 * conjg(d2);
+                }
+                double C = shot_tab(tabs, ix, iy, iz, assign);
+                pk2 = pk2 - mk<double>(S_re * C, S_im * C);
+                double wf = window_tab(tabs, ix, iy, iz, wpow);
+                double w2 = wf * wf;
+                pk2 = mk<double>(pk2.x / w2, pk2.y / w2);
             }
         }
-        atomicAdd(&scnt[b.x], 1ull);
-        if (b.y >= 0) atomicAdd(&scnt[b.y], 1ull);
+        if (__all_sync(0xffffffffu, b.x < 0)) continue;
+        const unsigned gx = __match_any_sync(0xffffffffu, b.x);
+        const unsigned gy = __match_any_sync(0xffffffffu, b.y);
+        const bool lx = (lane == __ffs(gx) - 1), ly = (lane == __ffs(gy) - 1);
+        for (int q = 0; q < lms.n; q++) {
+            zd v = mk<double>(0.0, 0.0);
+            if (b.x >= 0) v = pk2 * ylm_reduced(lms.lm[q].l, lms.lm[q].m, kv[0], kv[1], kv[2]);
+            const double sxr = group_sum(v.x, gx), sxi = group_sum(v.y, gx);
+            if (b.x >= 0 && lx) {
+                atomicAdd(&sacc[2 * (b.x * lms.n + q)], sxr);
+                atomicAdd(&sacc[2 * (b.x * lms.n + q) + 1], sxi);
+            }
+            const double syr = group_sum(v.x, gy), syi = group_sum(v.y, gy);
+            if (b.y >= 0 && ly) {
+                atomicAdd(&sacc[2 * (b.y * lms.n + q)], syr);
+                atomicAdd(&sacc[2 * (b.y * lms.n + q) + 1], syi);
+            }
+        }
+        if (b.x >= 0 && lx) atomicAdd(&scnt[b.x], (unsigned long long)__popc(gx));
+        if (b.y >= 0 && ly) atomicAdd(&scnt[b.y], (unsigned long long)__popc(gy));
     }
     __syncthreads();
     for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x)

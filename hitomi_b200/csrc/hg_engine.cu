@@ -855,6 +855,7 @@ struct Engine : public hg_ctx {
             S.K[a] = 2 * smax[a] + 1;
             int need = 4 * smax[a] + 1;
             int m = std::max(8, next_pow2(need));
+            if (need > 128 && need <= 192) m = 192;  // 3 x 64: the register FFT's 24 x 8 split
             if (m >= g.n[a]) {
                 S.M[a] = g.n[a];
                 S.gs[a] = g.n[a] / 2;  // whole axis
@@ -971,6 +972,8 @@ struct Engine : public hg_ctx {
         const C *Gp = dp<C>(Gsrc);
         if (Mx == 256)
             HG_CK((launch_chain_x_reg_L<T, 256>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
+        else if (Mx == 192)
+            HG_CK((launch_chain_x_reg_L<T, 192>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
         else if (Mx == 128)
             HG_CK((launch_chain_x_reg_L<T, 128>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
         else if (Mx == 64)

@@ -1,10 +1,11 @@
 // hg_fft2.cuh -- register-resident two-level line FFTs for lengths L = R1 * R2 <= 1024.
 //
-// A line of L points is handled by R2 threads that each hold R1 values (R1 = R2 or 2 R2):
+// A line of L points is handled by R2 threads that each hold R1 values (R1 = Q R2, Q = 1, 2
+// or 3; L = 192 is 24 x 8 with a prime-factor 24-point register DFT):
 //   step A  thread t loads x[R2 n1 + t], n1 < R1, does a DFT of size R1 in registers and
 //           multiplies by the twiddle w_L^(t k1);
 //   one exchange through shared memory (conflict-free layouts below);
-//   step B  thread t takes k1 in {t, t + R2} (R1 = 2 R2) or {t}, does a DFT of size R2
+//   step B  thread t takes k1 in {t + d R2, d < Q}, does a DFT of size R2
 //           over n2 and ends up holding X[k1 + R1 k2].
 // The positions a thread holds after step B are {t + R2 m, m < R1}: exactly its step-A
 // input set.  So an inverse transform can be followed by a pointwise product and a
@@ -146,13 +147,53 @@ __device__ __forceinline__ void bfly_stages(cplx<T> *v) {
     }
 }
 
-// In-register DFT of size R (power of two <= 32), natural-order output,
-// X[q] = sum_r v[r] exp(DIR 2 pi i r q / R): bit-reversal permutation, then radix-2
-// decimation-in-time stages; every index and twiddle is a compile-time constant.
+// 3-point DFT in place, X[q] = sum_r v[r] exp(DIR 2 pi i r q / 3):
+// X0 = a + b + c, X1,2 = a - (b + c)/2 +- DIR i (sqrt(3)/2) (b - c).
+template <typename T, int DIR>
+__device__ __forceinline__ void dft3(cplx<T> &a, cplx<T> &b, cplx<T> &c) {
+    constexpr T h = (T)0.8660254037844386;  // sqrt(3) / 2
+    const cplx<T> sum = b + c, dif = b - c;
+    const cplx<T> m = mk<T>(a.x - (T)0.5 * sum.x, a.y - (T)0.5 * sum.y);
+    const cplx<T> u = (DIR > 0) ? mk<T>(-h * dif.y, h * dif.x) : mk<T>(h * dif.y, -h * dif.x);
+    a = a + sum;
+    b = m + u;
+    c = m - u;
+}
+
+template <typename T, int R, int DIR>
+__device__ __forceinline__ void dft_reg(cplx<T> *v);
+
+// 24-point DFT as 8 x 3 with the prime-factor (Good-Thomas) maps: input n = (3 n1 + 8 n2)
+// mod 24, output k = (9 k1 + 16 k2) mod 24, so that W24^(n k) = W8^(n1 k1) W3^(n2 k2) and
+// no twiddles sit between the 3-point and the 8-point transforms.
+template <typename T, int DIR>
+__device__ __forceinline__ void dft24(cplx<T> *v) {
+    cplx<T> a[3][8];
+#pragma unroll
+    for (int n1 = 0; n1 < 8; n1++)
+#pragma unroll
+        for (int n2 = 0; n2 < 3; n2++) a[n2][n1] = v[(3 * n1 + 8 * n2) % 24];
+#pragma unroll
+    for (int n1 = 0; n1 < 8; n1++) dft3<T, DIR>(a[0][n1], a[1][n1], a[2][n1]);
+#pragma unroll
+    for (int k2 = 0; k2 < 3; k2++) dft_reg<T, 8, DIR>(a[k2]);
+#pragma unroll
+    for (int k1 = 0; k1 < 8; k1++)
+#pragma unroll
+        for (int k2 = 0; k2 < 3; k2++) v[(9 * k1 + 16 * k2) % 24] = a[k2][k1];
+}
+
+// In-register DFT of size R, natural-order output, X[q] = sum_r v[r] exp(DIR 2 pi i r q / R):
+// for a power of two <= 32, bit-reversal permutation then radix-2 decimation-in-time
+// stages; R = 24 by the prime-factor form.  Every index and twiddle is a compile-time constant.
 template <typename T, int R, int DIR>
 __device__ __forceinline__ void dft_reg(cplx<T> *v) {
-    brev_swaps<T, R, 0>(v);
-    bfly_stages<T, R, DIR, 2>(v);
+    if constexpr (R == 24) {
+        dft24<T, DIR>(v);
+    } else {
+        brev_swaps<T, R, 0>(v);
+        bfly_stages<T, R, DIR, 2>(v);
+    }
 }
 
 template <int L>
@@ -162,6 +203,7 @@ template <> struct Split<16> { static constexpr int R1 = 4, R2 = 4; };
 template <> struct Split<32> { static constexpr int R1 = 8, R2 = 4; };
 template <> struct Split<64> { static constexpr int R1 = 8, R2 = 8; };
 template <> struct Split<128> { static constexpr int R1 = 16, R2 = 8; };
+template <> struct Split<192> { static constexpr int R1 = 24, R2 = 8; };
 template <> struct Split<256> { static constexpr int R1 = 16, R2 = 16; };
 template <> struct Split<512> { static constexpr int R1 = 32, R2 = 16; };
 template <> struct Split<1024> { static constexpr int R1 = 32, R2 = 32; };
@@ -186,7 +228,7 @@ __device__ __forceinline__ void line_fft2(cplx<T> *v, cplx<T> *S, int t, int b, 
     constexpr int R1 = X::R1, R2 = X::R2;
     dft_reg<T, R1, DIR>(v);
 #pragma unroll
-    for (int k1 = 1; k1 < R1; k1++) v[k1] = mul_tw<T, DIR>(v[k1], tw[(t * k1) & (L - 1)]);
+    for (int k1 = 1; k1 < R1; k1++) v[k1] = mul_tw<T, DIR>(v[k1], tw[t * k1]);  // t k1 < R1 R2 = L
 #pragma unroll
     for (int k1 = 0; k1 < R1; k1++) S[X::at(b, k1, t)] = v[k1];
     __syncthreads();
@@ -304,6 +346,7 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
         case 32: return launch_fft2_L<T, 32, DIR>(ld, st, g, tw, stream);
         case 64: return launch_fft2_L<T, 64, DIR>(ld, st, g, tw, stream);
         case 128: return launch_fft2_L<T, 128, DIR>(ld, st, g, tw, stream);
+        case 192: return launch_fft2_L<T, 192, DIR>(ld, st, g, tw, stream);
         case 256: return launch_fft2_L<T, 256, DIR>(ld, st, g, tw, stream);
         case 512: return launch_fft2_L<T, 512, DIR>(ld, st, g, tw, stream);
         case 1024: return launch_fft2_L<T, 1024, DIR>(ld, st, g, tw, stream);

