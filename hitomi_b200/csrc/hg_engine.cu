@@ -1164,6 +1164,37 @@ struct Engine : public hg_ctx {
         return out;
     }
 
+    // Chebyshev coefficients of f_h(mu) = sum_terms w Yhat_l1m1 Yhat_l2m2 at (sqrt(1 - mu^2), 0, mu)
+    // (real for m1 + m2 = 0, a polynomial of degree l1 + l2): interpolation at deg + 1 nodes
+    static void orbit_weight_poly(HistSpec &hs, int h) {
+        int D = 0;
+        double f0 = 0.0;
+        for (int q = 0; q < hs.nterm[h]; q++) {
+            D = std::max(D, hs.term[h][q].l1 + hs.term[h][q].l2);
+            if (hs.term[h][q].l1 == 0 && hs.term[h][q].l2 == 0) f0 += hs.term[h][q].w;
+        }
+        HG_REQUIRE(D < HG_CHEB, "multipole degree too large for the shot-noise weight polynomial");
+        std::vector<double> fk(D + 1);
+        for (int k = 0; k <= D; k++) {
+            const double mu = std::cos(HG_PI * (k + 0.5) / double(D + 1));
+            const double sx = std::sqrt(std::max(0.0, 1.0 - mu * mu));
+            double f = 0.0;
+            for (int q = 0; q < hs.nterm[h]; q++) {
+                const YTerm &yt = hs.term[h][q];
+                zd y1 = ylm_reduced(yt.l1, yt.m1, sx, 0.0, mu), y2 = ylm_reduced(yt.l2, yt.m2, sx, 0.0, mu);
+                f += yt.w * (y1.x * y2.x - y1.y * y2.y);
+            }
+            fk[k] = f;
+        }
+        for (int j = 0; j <= D; j++) {
+            double c = 0.0;
+            for (int k = 0; k <= D; k++) c += fk[k] * std::cos(HG_PI * j * (k + 0.5) / double(D + 1));
+            hs.cheb[h][j] = c * 2.0 / double(D + 1) * (j == 0 ? 0.5 : 1.0);
+        }
+        hs.deg[h] = D;
+        hs.f0[h] = f0;
+    }
+
     // hist_mp[mp][n2] = sum over cells with |x/dr|^2 = n2 of xi(x) sum_combos w Yhat1 Yhat2
     void ensure_histograms(const std::vector<MP> &mps) {
         ensure_xi();
@@ -1184,6 +1215,7 @@ struct Engine : public hg_ctx {
                 auto cs = combos_of(mp);
                 HG_REQUIRE(cs.size() <= 12, "too many (m1, m2) terms in one multipole");
                 for (const auto &c : cs) hs.term[h][hs.nterm[h]++] = YTerm{mp.l1, c.m1, mp.l2, c.m2, c.w};
+                orbit_weight_poly(hs, h);
             }
             HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim * hs.nh));
             HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim * hs.nh, st));

@@ -269,12 +269,30 @@ struct YTerm {
 };
 #define HG_MAX_TERMS 24
 #define HG_MAX_HIST 8
+#define HG_CHEB 17
 struct HistSpec {
     int nh;                      // number of histograms
     int nterm[HG_MAX_HIST];      // terms per histogram
     int parity[HG_MAX_HIST];     // (-1)^(l1+l2) of the histogram's terms
     YTerm term[HG_MAX_HIST][12];
+    // m1 + m2 = 0: f_h is a real polynomial in mu = cos(theta) of degree l1 + l2, kept as
+    // Chebyshev coefficients (exact interpolation at l1 + l2 + 1 Chebyshev nodes); f0 is
+    // its value at r = 0, where Yhat_lm = 0 unless l = m = 0 (tools.hpp:12-68)
+    int deg[HG_MAX_HIST];
+    double cheb[HG_MAX_HIST][HG_CHEB];
+    double f0[HG_MAX_HIST];
 };
+
+// sum_j c_j T_j(mu), Clenshaw recurrence
+__device__ __forceinline__ double cheb_eval(const double *c, int deg, double mu) {
+    double b1 = 0.0, b2 = 0.0;
+    for (int j = deg; j >= 1; j--) {
+        const double b0 = 2.0 * mu * b1 - b2 + c[j];
+        b2 = b1;
+        b1 = b0;
+    }
+    return mu * b1 - b2 + c[0];
+}
 
 // Last inverse pass (along z) over one symmetry orbit of (x, y) lines, fused with
 //   T_h(n^2) += sum over the orbit and z <-> -z of xi(x) f_h(theta)
@@ -315,7 +333,6 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
     for (int r = 0; r < R1; r++) s[b * LP + pos_of_reg<L>(t, r)] = v[r];
     __syncthreads();
     const int n2xy = orbit_n2xy[orb];
-    const double rho = sqrt((double)n2xy);
     for (int iz = threadIdx.x; iz <= L / 2; iz += NT) {
         int iz2 = (L - iz) % L;
         double er = 0, ei = 0, orr = 0, oi = 0;
@@ -335,16 +352,12 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
         }
         int wz = wrap_index(iz, L);
         long long n2 = (long long)n2xy + (long long)wz * wz;
+        const double r = sqrt((double)n2);
+        const double mu = (n2 > 0) ? (double)wz / r : 0.0;
         for (int h = 0; h < hs.nh; h++) {
-            zd f = mk<double>(0.0, 0.0);
-            for (int q = 0; q < hs.nterm[h]; q++) {
-                const YTerm &yt = hs.term[h][q];
-                zd y1 = ylm_reduced(yt.l1, yt.m1, rho, 0.0, (double)wz);
-                zd y2 = ylm_reduced(yt.l2, yt.m2, rho, 0.0, (double)wz);
-                f = f + (y1 * y2) * yt.w;
-            }
+            const double f = (n2 > 0) ? cheb_eval(hs.cheb[h], hs.deg[h], mu) : hs.f0[h];
             zd src = (hs.parity[h] > 0) ? mk<double>(er, ei) : mk<double>(orr, oi);
-            zd val = f * src;
+            zd val = mk<double>(f * src.x, f * src.y);
             if (val.x != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2)], val.x);
             if (val.y != 0.0) atomicAdd(&hist[2 * ((long long)h * n2dim + n2) + 1], val.y);
         }
