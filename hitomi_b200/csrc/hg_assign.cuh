@@ -301,6 +301,54 @@ __global__ void k_bin_scatter(PartSrc src, AssignGeom g, const unsigned int *off
     }
 }
 
+// Records that keep the particle instead of its weight, so that one binning serves every
+// weighting of the same catalogues (the survey's Yhat_lm-weighted fields): the weight is
+// evaluated in the accumulation from the particle's own record.
+template <typename T>
+struct PRecS {
+    int i[3];
+    int src;  // which source (0 data, 1 randoms)
+    T d[3];
+    int p;    // particle index within its source
+};
+
+template <typename T>
+__global__ void k_bin_scatter_idx(PartSrc src, int srcid, AssignGeom g, const unsigned int *off, unsigned int *cursor,
+                                  PRecS<T> *rec) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int tiles[64];
+    int nt = 0;
+    PRecS<T> r;
+    if (p < src.n) {
+        double pos[3];
+        load_pos(src, p, pos);
+        int anc[3];
+        double d[3];
+        for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
+        nt = particle_tiles(g, anc, tiles);
+        for (int a = 0; a < 3; a++) {
+            r.i[a] = anc[a];
+            r.d[a] = (T)d[a];
+        }
+        r.src = srcid;
+        r.p = (int)p;
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    int maxnt = __reduce_max_sync(0xffffffffu, nt);
+    for (int q = 0; q < maxnt; q++) {
+        int t = (q < nt) ? tiles[q] : -1;
+        unsigned grp = __match_any_sync(0xffffffffu, t);
+        if (t >= 0) {
+            int leader = __ffs(grp) - 1;
+            unsigned base = 0;
+            if (lane == leader) base = atomicAdd(&cursor[t], (unsigned)__popc(grp));
+            base = __shfl_sync(grp, base, leader);
+            rec[off[t] + base + __popc(grp & lt)] = r;
+        }
+    }
+}
+
 // Per-particle FP64 sums  out[q] = sum_p scale w_p^pw[q] Yhat_{l_q m_q}(los_p)  (complex), as
 // block partials part[block][q] summed on the host in block order (deterministic):
 // sum w (particle.hpp:336-352), sum w^2 (particle.hpp:255-258), and the shot-noise sums
@@ -455,6 +503,90 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
                 }
     }
     __syncthreads();
+    for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
+        int lx, ly, lz;
+        long long cell = tile_cell(g, tile, li, lx, ly, lz);
+        if (k.multi == 0) {
+            mesh_re[cell] = acc[li];
+            if (CPLX) mesh_im[cell] = acc_im[li];
+        } else {
+            if (acc[li] != (T)0) atomicAdd(&mesh_re[cell], acc[li]);
+            if (CPLX && acc_im[li] != (T)0) atomicAdd(&mesh_im[cell], acc_im[li]);
+        }
+    }
+}
+
+// Weighting of a field: one PartSrc (weight recipe: w^wpow, Yhat_lm(los), scale) per source.
+struct FieldW {
+    PartSrc s[2];
+};
+
+// k_tile_accum on particle-index records: the weight comes from the particle
+// (load_weight, the same FP64 expression as the weight-carrying records), and the FP64
+// in-bounds mass sum of w factor prod(w_axis) is reduced on the way (each in-bounds stencil
+// point is accumulated by exactly one record), for the transform's exact k = 0 value.
+template <typename T, bool CPLX>
+__global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeom g, FieldW fw, T *mesh_re, T *mesh_im,
+                                 double *mass) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *acc = reinterpret_cast<T *>(smem_raw);
+    const int tcells = g.t[0] * g.t[1] * g.t[2];
+    T *acc_im = acc + tcells;
+    __shared__ double red[2][32];
+    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
+    __syncthreads();
+    const Chunk k = ch[blockIdx.x];
+    const int tile = k.tile;
+    const int tz = tile % g.nt[2];
+    const int ty = (tile / g.nt[2]) % g.nt[1];
+    const int tx = tile / (g.nt[2] * g.nt[1]);
+    const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
+    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+    double mr = 0.0, mi = 0.0;
+    for (unsigned r = k.r0 + threadIdx.x; r < k.r1; r += blockDim.x) {
+        const PRecS<T> pr = rec[r];
+        double wr64, wi64;
+        load_weight(fw.s[pr.src], pr.p, wr64, wi64);
+        T w[3][4];
+        double w64[3][4];
+        for (int a = 0; a < 3; a++) {
+            axis_weights<T>(g.scheme, pr.d[a], w[a]);
+            axis_weights<double>(g.scheme, (double)pr.d[a], w64[a]);
+        }
+        const T wr = (T)wr64, wi = (T)wi64;
+        const T factor = (T)g.acc_factor;
+        for (int a = 0; a < W; a++)
+            for (int b = 0; b < W; b++)
+                for (int c = 0; c < W; c++) {
+                    int cx, cy, cz;
+                    if (!effective_cell(g, pr.i[0] + s0 + a, pr.i[1] + s0 + b, pr.i[2] + s0 + c, cx, cy, cz)) continue;
+                    int lx = cx - ox, ly = cy - oy, lz = cz - oz;
+                    if ((unsigned)lx >= (unsigned)g.t[0] || (unsigned)ly >= (unsigned)g.t[1] ||
+                        (unsigned)lz >= (unsigned)g.t[2])
+                        continue;
+                    int li = (lx * g.t[1] + ly) * g.t[2] + lz;
+                    atomicAdd(&acc[li], wr * factor * w[0][a] * w[1][b] * w[2][c]);
+                    if (CPLX) atomicAdd(&acc_im[li], wi * factor * w[0][a] * w[1][b] * w[2][c]);
+                    mr += wr64 * g.factor * w64[0][a] * w64[1][b] * w64[2][c];
+                    mi += wi64 * g.factor * w64[0][a] * w64[1][b] * w64[2][c];
+                }
+    }
+    mr = warp_sum_d(mr);
+    mi = warp_sum_d(mi);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = mr;
+        red[1][threadIdx.x >> 5] = mi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sr = 0.0, si = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            sr += red[0][w];
+            si += red[1][w];
+        }
+        if (sr != 0.0) atomicAdd(&mass[0], sr);
+        if (si != 0.0) atomicAdd(&mass[1], si);
+    }
     for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
         int lx, ly, lz;
         long long cell = tile_cell(g, tile, li, lx, ly, lz);

@@ -236,6 +236,13 @@ struct Engine : public hg_ctx {
     // full ones (m < 0 as mirrors of m > 0); keyed (kind, l, m), valid for sf_alpha.
     enum { SF_DELTA = 0, SF_SN = 1 };
     DBuf smesh_re, smesh_im, dmesh, psum_part, sfield_tmp;
+    // both catalogues binned once per assignment offset (0, and 1/2 cell for interlacing);
+    // every weighting reuses them
+    struct SurveyBins {
+        DBuf rec, chunks;
+        unsigned total = 0, nchunks = 0;
+        bool ok = false;
+    } sbins[2];
     std::map<std::array<int, 3>, std::unique_ptr<DBuf>> sfbuf;
     std::map<std::array<int, 3>, std::array<double, 2>> sfk0;
     std::set<std::array<int, 3>> sf_ok;
@@ -259,6 +266,7 @@ struct Engine : public hg_ctx {
         }
     };
     std::map<ZKey, std::unique_ptr<DBuf>> zf;  // F_lm[r0 .. r0+nr) on the full grid
+    size_t zfree0 = 0;                         // device memory available to the field cache
     std::set<ZKey> zf_ok;
     std::map<std::tuple<int, int, int, int, int, int, int>, std::vector<double>> zpairs;  // (a, b, row, L, M)
 
@@ -556,6 +564,7 @@ struct Engine : public hg_ctx {
         zpairs.clear();
         sf_ok.clear();
         hist_sv_ok.clear();
+        sbins[0].ok = sbins[1].ok = false;
     }
 
     // ------------------------------------------------------------------ assignment
@@ -627,8 +636,11 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemcpyAsync(hm, mass.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
         const unsigned total = tot[0], nchunks = tot[1];
-        HG_CK(rec.ensure(sizeof(PRec<U>) * std::max<size_t>(total, 1)));
-        HG_CK(chunks.ensure(sizeof(Chunk) * std::max<size_t>(nchunks, 1)));
+        // 25 % headroom: catalogues of varying size reuse the buffers without reallocating
+        if (rec.n < sizeof(PRec<U>) * std::max<size_t>(total, 1))
+            HG_CK(rec.ensure(sizeof(PRec<U>) * (std::max<size_t>(total, 1) * 5 / 4)));
+        if (chunks.n < sizeof(Chunk) * std::max<size_t>(nchunks, 1))
+            HG_CK(chunks.ensure(sizeof(Chunk) * (std::max<size_t>(nchunks, 1) * 5 / 4)));
         kb("assign_chunks", double(ntiles) * 16.0);
         k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
                                                         dp<Chunk>(chunks));
@@ -1603,21 +1615,20 @@ struct Engine : public hg_ctx {
         auto it = zf.find(key);
         if (it != zf.end() && zf_ok.count(key)) return dp<C>(*it->second);
         const size_t need = sizeof(C) * (size_t)g.ntot * nr;
-        size_t fr = 0, tot = 0;
-        HG_CK(cudaMemGetInfo(&fr, &tot));
-        if (need + (size_t(1) << 30) > fr) {  // release cached fields other than `keep`
+        auto &p = zf[key];
+        if (!p) p = std::make_unique<DBuf>();
+        if (p->ensure(need) != cudaSuccess) {  // out of memory: release cached fields other than `keep`, retry
+            cudaGetLastError();
             for (auto i = zf.begin(); i != zf.end();) {
-                if (keep && !(i->first < *keep) && !(*keep < i->first)) {
+                if ((keep && !(i->first < *keep) && !(*keep < i->first)) || !(i->first < key || key < i->first)) {
                     ++i;
                     continue;
                 }
                 zf_ok.erase(i->first);
                 i = zf.erase(i);
             }
+            HG_CK(zf[key]->ensure(need));
         }
-        auto &p = zf[key];
-        if (!p) p = std::make_unique<DBuf>();
-        HG_CK(p->ensure(need));
         zeta_U(f.l, f.m);
         const double *J = jtab_rbins(f.l) + (size_t)r0 * n2dim;
         LdZetaField<T> ld{dp<C>(Uz), J, n2dim, g.n[0], g.n[1], g.n[2]};
@@ -1662,11 +1673,15 @@ struct Engine : public hg_ctx {
         if (it == zpairs.end()) {
             const int rows = all ? ns : 1;
             std::vector<double> out(2 * (size_t)rows * ns, 0.0);
-            // radius tiles that fit next to the cached fields (one tile when memory allows)
-            size_t fr = 0, tot = 0;
-            HG_CK(cudaMemGetInfo(&fr, &tot));
+            // radius tiles that fit next to the cached fields (one tile when memory allows);
+            // the free memory is read once per context, then tracked by what the cache holds
             const double fb = double(sizeof(C)) * double(g.ntot);
-            double avail = double(fr) + double(zf_bytes()) - double(size_t(2) << 30);
+            if (zfree0 == 0) {
+                size_t fr = 0, tot = 0;
+                HG_CK(cudaMemGetInfo(&fr, &tot));
+                zfree0 = fr + zf_bytes();
+            }
+            double avail = double(zfree0) - double(size_t(4) << 30);
             int tile = (int)std::min<double>(64.0, std::floor(avail / (2.0 * fb)));
             HG_REQUIRE(tile >= 1, "not enough device memory for two 3PCF fields");
             tile = std::min(tile, ns);
@@ -1878,6 +1893,79 @@ struct Engine : public hg_ctx {
     // FFT[dV (n_D - alpha n_R)] of the Yhat_lm(los)-weighted fields, m >= 0
     // (calcYlmWeightedDensityFluctuation field.hpp:186-228, then field.hpp:310-325).  m = 0 is
     // a real field (half spectrum); m > 0 is complex (full spectrum).
+    // tile binning of data and randoms (positions only) for one assignment offset
+    SurveyBins &survey_bins(int k) {
+        SurveyBins &B = sbins[k];
+        if (B.ok) return B;
+        const AssignGeom ag = make_geom(k ? 0.5 : 0.0);
+        const int ntiles = ag.nt[0] * ag.nt[1] * ag.nt[2];
+        HG_CK(cnt.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(off.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(cursor.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(nch.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(choff.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (ntiles + 1), st));
+        HG_CK(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned) * (ntiles + 1), st));
+        const PartSrc src[2] = {survey_src(0, false, 0, 0, 1.0), survey_src(1, false, 0, 0, 1.0)};
+        for (int q = 0; q < 2; q++) {
+            kb("assign_bin_count", double(src[q].n) * 24.0);
+            k_bin_count<<<grid1(src[q].n, 256), 256, 0, st>>>(src[q], ag, dp<unsigned>(cnt), nullptr);
+            ke();
+        }
+        size_t tb = 0, tb2 = 0;
+        HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
+        HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
+        HG_CK(cubtmp.ensure(std::max(tb, tb2)));
+        HG_CK(cub::DeviceScan::ExclusiveSum(cubtmp.p, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
+        k_chunk_count<<<grid1(ntiles + 1, 256), 256, 0, st>>>(dp<unsigned>(cnt), ntiles, CHUNK, dp<unsigned>(nch));
+        HG_CK(cub::DeviceScan::ExclusiveSum(cubtmp.p, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
+        unsigned tot[2] = {0, 0};
+        HG_CK(cudaMemcpyAsync(&tot[0], dp<unsigned>(off) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaMemcpyAsync(&tot[1], dp<unsigned>(choff) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        B.total = tot[0];
+        B.nchunks = tot[1];
+        HG_CK(B.rec.ensure(sizeof(PRecS<T>) * std::max<size_t>(B.total, 1)));
+        HG_CK(B.chunks.ensure(sizeof(Chunk) * std::max<size_t>(B.nchunks, 1)));
+        k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
+                                                        dp<Chunk>(B.chunks));
+        for (int q = 0; q < 2; q++) {
+            kb("assign_bin_scatter", double(src[q].n) * 24.0 + double(B.total) * sizeof(PRecS<T>) / 2);
+            k_bin_scatter_idx<T><<<grid1(src[q].n, 256), 256, 0, st>>>(src[q], q, ag, dp<unsigned>(off),
+                                                                       dp<unsigned>(cursor), dp<PRecS<T>>(B.rec));
+            ke();
+        }
+        HG_CK(cudaGetLastError());
+        B.ok = true;
+        return B;
+    }
+
+    // accumulate one weighting of the binned catalogues; returns the FP64 in-bounds mass
+    template <bool CPLX>
+    std::array<double, 2> survey_accumulate(int k, const PartSrc srcs[2], T *re, T *im) {
+        SurveyBins &B = survey_bins(k);
+        AssignGeom ag = make_geom(k ? 0.5 : 0.0);
+        ag.acc_factor = 1.0;
+        FieldW fw;
+        fw.s[0] = srcs[0];
+        fw.s[1] = srcs[1];
+        HG_CK(mass.ensure(sizeof(double) * 2));
+        HG_CK(cudaMemsetAsync(mass.p, 0, sizeof(double) * 2, st));
+        kb("assign_zero_split", 0.0);
+        k_zero_split_tiles<T, CPLX><<<B.nchunks, 256, 0, st>>>(dp<Chunk>(B.chunks), ag, re, im);
+        ke();
+        const size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2] * (CPLX ? 2 : 1);
+        HG_CK(cudaFuncSetAttribute(k_tile_accum_src<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kb("assign_tile_accum", double(B.total) * sizeof(PRecS<T>) + double(g.ntot) * sizeof(T) * (CPLX ? 2 : 1));
+        k_tile_accum_src<T, CPLX><<<B.nchunks, 256, smem, st>>>(dp<PRecS<T>>(B.rec), dp<Chunk>(B.chunks), ag, fw, re, im,
+                                                                dp<double>(mass));
+        ke();
+        double hm[2];
+        HG_CK(cudaMemcpyAsync(hm, mass.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        return {hm[0], hm[1]};
+    }
+
     SpecK sfield(int kind, int l, int m, double alpha) {
         if (alpha != sf_alpha) {
             sf_ok.clear();
@@ -1918,14 +2006,18 @@ struct Engine : public hg_ctx {
         // assign (mass units: dV rho, the transform's input) with a shift, transform into F;
         // returns the FP64 in-bounds mass, the transform's exact k = 0 value
         auto build = [&](double shift, C *F) {
-            AssignGeom ag = make_geom(shift);
-            ag.acc_factor = 1.0;
+            const int kb_ = shift != 0.0 ? 1 : 0;
             double mi = 0.0, mr;
             if (real) {
-                mr = assign_mesh<T, false>(srcs, ag, dp<T>(smesh_re), nullptr, true, &mi);
+                const std::array<double, 2> mm = survey_accumulate<false>(kb_, srcs.data(), dp<T>(smesh_re), nullptr);
+                mr = mm[0];
+                mi = mm[1];
                 forward_real(dp<T>(smesh_re), F, (T)0, (T)1, "fft_survey");
             } else {
-                mr = assign_mesh<T, true>(srcs, ag, dp<T>(smesh_re), dp<T>(smesh_im), true, &mi);
+                const std::array<double, 2> mm =
+                    survey_accumulate<true>(kb_, srcs.data(), dp<T>(smesh_re), dp<T>(smesh_im));
+                mr = mm[0];
+                mi = mm[1];
                 const long long yz = (long long)g.n[1] * g.n[2];
                 pass<-1>(g.n[2], LdPlanar<T>{dp<T>(smesh_re), dp<T>(smesh_im), g.n[2]}, StArr<T>{F, g.n[2], 1},
                          (long long)g.n[0] * g.n[1], 1, "fft_survey", double(g.ntot) * (2 * sizeof(T) + sizeof(C)));
