@@ -487,6 +487,10 @@ def main():
     for form in timing:
         line.setdefault("kernel_ms", {})[form] = {k: round(v["ms"], 4) for k, v in
                                                   sorted(timing[form]["stats"].items(), key=lambda kv: -kv[1]["ms"])}
+        # algorithmic bytes (the library's per-launch model) over the measured time
+        line.setdefault("kernel_gbs", {})[form] = {k: round(v["bytes"] / v["ms"] / 1e6, 1) for k, v in
+                                                   sorted(timing[form]["stats"].items(), key=lambda kv: -kv[1]["ms"])
+                                                   if v["ms"] > 0 and v["bytes"] > 0}
     if os.environ.get("HG_BENCH_DUMP"):
         np.savez_compressed(os.environ["HG_BENCH_DUMP"], **{f"{form}:{'_'.join(map(str, k))}": v
                                                             for form in results for k, v in results[form].items()})
