@@ -36,6 +36,7 @@ struct AssignGeom {
     int nt[3];        // tiles per axis
     double factor;      // 1/dV (field.hpp:76-77), used for the FP64 in-bounds mass
     double acc_factor;  // factor applied in the mesh accumulation (1/dV, or 1 for a mass mesh)
+    float fix_bound;    // bound on |w acc_factor prod(w_axis)| per record (fixed-point accumulation)
 };
 
 __host__ __device__ __forceinline__ int stencil_width(int scheme) { return scheme + 1; }
@@ -81,15 +82,65 @@ __device__ __forceinline__ void axis_weights(int scheme, T d, T *w) {
     }
 }
 
-// Effective cell of stencil point (ix, iy, iz); false if the reference drops it.
+// i mod n for i within one period of [0, n) (stencil indices of particles inside the
+// box), the general remainder otherwise.
+__device__ __forceinline__ int wrap_cell(int i, int n) {
+    if (i >= -n && i < 2 * n) return i < 0 ? i + n : (i >= n ? i - n : i);
+    const int c = i % n;
+    return c < 0 ? c + n : c;
+}
+
+// Stencil weight j of one axis: the same expressions as axis_weights, without an array
+// (for loops whose index is not known at compile time).
+template <typename T>
+__device__ __forceinline__ T axis_weight_at(int scheme, T d, int j) {
+    if (scheme == 0) return (T)1;
+    if (scheme == 1) return j == 0 ? (T)1 - d : d;
+    if (scheme == 2) {
+        if (j == 1) return (T)0.75 - d * d;
+        const T e = (j == 0) ? (T)0.5 - d : (T)0.5 + d;
+        return (T)0.5 * e * e;
+    }
+    const T t = d, u = (T)1 - d;
+    if (j == 0) return u * u * u / (T)6;
+    if (j == 1) return ((T)4 - (T)6 * t * t + (T)3 * t * t * t) / (T)6;
+    if (j == 2) return ((T)1 + (T)3 * t + (T)3 * t * t - (T)3 * t * t * t) / (T)6;
+    return t * t * t / (T)6;
+}
+
+// Effective cell of stencil point (ix, iy, iz); false if the reference drops it.  The
+// non-periodic rule decomposes the flat index (ix n1 + iy) n2 + iz: with iz and iy within
+// one period of their ranges this is a carry from z into y and from y into x (then
+// 0 <= flat < N exactly when the carried ix is in range); a 64-bit division otherwise.
 __device__ __forceinline__ bool effective_cell(const AssignGeom &g, int ix, int iy, int iz, int &cx, int &cy, int &cz) {
     if (g.periodic) {
-        cx = ((ix % g.n[0]) + g.n[0]) % g.n[0];
-        cy = ((iy % g.n[1]) + g.n[1]) % g.n[1];
-        cz = ((iz % g.n[2]) + g.n[2]) % g.n[2];
+        cx = wrap_cell(ix, g.n[0]);
+        cy = wrap_cell(iy, g.n[1]);
+        cz = wrap_cell(iz, g.n[2]);
         return true;
     }
     if (ix >= 0 && ix < g.n[0] && iy >= 0 && iy < g.n[1] && iz >= 0 && iz < g.n[2]) {
+        cx = ix;
+        cy = iy;
+        cz = iz;
+        return true;
+    }
+    if (iz >= -g.n[2] && iz < 2 * g.n[2] && iy > -g.n[1] && iy < 2 * g.n[1] - 1) {
+        if (iz < 0) {
+            iz += g.n[2];
+            iy--;
+        } else if (iz >= g.n[2]) {
+            iz -= g.n[2];
+            iy++;
+        }
+        if (iy < 0) {
+            iy += g.n[1];
+            ix--;
+        } else if (iy >= g.n[1]) {
+            iy -= g.n[1];
+            ix++;
+        }
+        if (ix < 0 || ix >= g.n[0]) return false;
         cx = ix;
         cy = iy;
         cz = iz;
@@ -171,26 +222,47 @@ struct PRec {
     T wr, wi;
 };
 
-// Enumerate the distinct tiles a particle's stencil touches.  Returns the count.
-__device__ __forceinline__ int particle_tiles(const AssignGeom &g, const int anc[3], int *tiles) {
+// A stencil is separable when its cells follow axis by axis: on a periodic mesh (each axis
+// wraps on its own), or when every point lies inside a non-periodic mesh.  Otherwise the
+// reference's flat-index rule couples the axes (a point at iz = -1 lands in row iy - 1).
+__device__ __forceinline__ bool stencil_separable(const AssignGeom &g, const int anc[3]) {
+    if (g.periodic) return true;
     const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
-    bool inside = true;
-    for (int a = 0; a < 3; a++) {
-        int lo = anc[a] + s0, hi = anc[a] + s0 + W - 1;
-        if (g.periodic || lo < 0 || hi >= g.n[a]) inside = false;
+    bool in = true;
+    for (int a = 0; a < 3; a++) in &= (anc[a] + s0 >= 0) && (anc[a] + s0 + W - 1 < g.n[a]);
+    return in;
+}
+
+// Cell index along axis a of stencil index i in a separable stencil.
+__device__ __forceinline__ int axis_cell(const AssignGeom &g, int a, int i) {
+    return g.periodic ? wrap_cell(i, g.n[a]) : i;
+}
+
+// The distinct tiles a particle's stencil touches.  Separable stencils keep, per axis, the
+// tiles of the first and last point (the tile extent is at least the stencil width unless
+// the axis holds a single tile, so a run of W cells, wrapped or not, meets at most two
+// tiles); the q-th tile is a mixed-radix index over the three axes, in registers.  Other
+// stencils (non-periodic, straddling the mesh edge: a few per cent of particles) list
+// their tiles by deduplicating the effective cells of every point.
+struct TileList {
+    int f[3], l[3], c[3];  // first / last tile per axis, and how many (1 or 2)
+    int n;
+    bool sep;
+};
+
+__device__ __forceinline__ void tile_list(const AssignGeom &g, const int anc[3], TileList &tl, int *slow) {
+    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+    tl.sep = stencil_separable(g, anc);
+    if (tl.sep) {
+        for (int a = 0; a < 3; a++) {
+            tl.f[a] = axis_cell(g, a, anc[a] + s0) / g.t[a];
+            tl.l[a] = axis_cell(g, a, anc[a] + s0 + W - 1) / g.t[a];
+            tl.c[a] = (tl.f[a] != tl.l[a]) ? 2 : 1;
+        }
+        tl.n = tl.c[0] * tl.c[1] * tl.c[2];
+        return;
     }
     int nt = 0;
-    if (inside) {
-        int tlo[3], thi[3];
-        for (int a = 0; a < 3; a++) {
-            tlo[a] = (anc[a] + s0) / g.t[a];
-            thi[a] = (anc[a] + s0 + W - 1) / g.t[a];
-        }
-        for (int tx = tlo[0]; tx <= thi[0]; tx++)
-            for (int ty = tlo[1]; ty <= thi[1]; ty++)
-                for (int tz = tlo[2]; tz <= thi[2]; tz++) tiles[nt++] = (tx * g.nt[1] + ty) * g.nt[2] + tz;
-        return nt;
-    }
     for (int a = 0; a < W; a++)
         for (int b = 0; b < W; b++)
             for (int c = 0; c < W; c++) {
@@ -198,107 +270,26 @@ __device__ __forceinline__ int particle_tiles(const AssignGeom &g, const int anc
                 if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
                 int t = tile_of(g, cx, cy, cz);
                 bool seen = false;
-                for (int q = 0; q < nt; q++) seen |= (tiles[q] == t);
-                if (!seen) tiles[nt++] = t;
+                for (int q = 0; q < nt; q++) seen |= (slow[q] == t);
+                if (!seen) slow[nt++] = t;
             }
-    return nt;
+    tl.n = nt;
 }
+
+__device__ __forceinline__ int tile_at(const AssignGeom &g, const TileList &tl, const int *slow, int q) {
+    if (!tl.sep) return slow[q];
+    const int qc = q % tl.c[2], qb = (q / tl.c[2]) % tl.c[1], qa = q / (tl.c[2] * tl.c[1]);
+    const int tx = qa ? tl.l[0] : tl.f[0], ty = qb ? tl.l[1] : tl.f[1], tz = qc ? tl.l[2] : tl.f[2];
+    return (tx * g.nt[1] + ty) * g.nt[2] + tz;
+}
+
+// Most stencil points a non-separable stencil can have (non-periodic meshes: NGP, CIC, TSC).
+#define HG_SLOW_TILES 27
+
 
 __device__ __forceinline__ double warp_sum_d(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
-}
-
-// Pass 1: tile counts + (when mass != null) the FP64 in-bounds mass
-// sum_p w_p factor prod(w_axis)  (the field's exact integral, needed for the k = 0 mode
-// since boundary drops lose mass).  Clustered catalogues put many lanes of a warp on the
-// same tile, so the count is warp-aggregated.
-__global__ void k_bin_count(PartSrc src, AssignGeom g, unsigned int *cnt, double *mass) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    double m_re = 0.0, m_im = 0.0;
-    int tiles[64];
-    int nt = 0;
-    if (p < src.n) {
-        double pos[3], wr = 0.0, wi = 0.0;
-        load_pos(src, p, pos);
-        if (mass) load_weight(src, p, wr, wi);
-        int anc[3];
-        double d[3];
-        for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
-        nt = particle_tiles(g, anc, tiles);
-        const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
-        bool inside = true;
-        for (int a = 0; a < 3; a++) inside &= (anc[a] + s0 >= 0) && (anc[a] + s0 + W - 1 < g.n[a]);
-        if (!mass) {
-        } else if (inside || g.periodic) {
-            // every stencil point lands: the weights sum to one per axis
-            m_re += wr * g.factor;
-            m_im += wi * g.factor;
-        } else {
-            // in-bounds mass in the reference's product order
-            double w[3][4];
-            for (int a = 0; a < 3; a++) axis_weights<double>(g.scheme, d[a], w[a]);
-            for (int a = 0; a < W; a++)
-                for (int b = 0; b < W; b++)
-                    for (int c = 0; c < W; c++) {
-                        int cx, cy, cz;
-                        if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz))
-                            continue;
-                        m_re += wr * g.factor * w[0][a] * w[1][b] * w[2][c];
-                        m_im += wi * g.factor * w[0][a] * w[1][b] * w[2][c];
-                    }
-        }
-    }
-    const int lane = threadIdx.x & 31;
-    int maxnt = __reduce_max_sync(0xffffffffu, nt);
-    for (int q = 0; q < maxnt; q++) {
-        int t = (q < nt) ? tiles[q] : -1;
-        unsigned grp = __match_any_sync(0xffffffffu, t);
-        if (t >= 0 && lane == __ffs(grp) - 1) atomicAdd(&cnt[t], (unsigned)__popc(grp));
-    }
-    if (!mass) return;
-    m_re = warp_sum_d(m_re);
-    m_im = warp_sum_d(m_im);
-    if (lane == 0 && (m_re != 0.0 || m_im != 0.0)) {
-        atomicAdd(&mass[0], m_re);
-        atomicAdd(&mass[1], m_im);
-    }
-}
-
-template <typename T>
-__global__ void k_bin_scatter(PartSrc src, AssignGeom g, const unsigned int *off, unsigned int *cursor, PRec<T> *rec) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int tiles[64];
-    int nt = 0;
-    PRec<T> r;
-    if (p < src.n) {
-        double pos[3], wr, wi;
-        load_particle(src, p, pos, wr, wi);
-        int anc[3];
-        double d[3];
-        for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
-        nt = particle_tiles(g, anc, tiles);
-        for (int a = 0; a < 3; a++) {
-            r.i[a] = anc[a];
-            r.d[a] = (T)d[a];
-        }
-        r.wr = (T)wr;
-        r.wi = (T)wi;
-    }
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    int maxnt = __reduce_max_sync(0xffffffffu, nt);
-    for (int q = 0; q < maxnt; q++) {
-        int t = (q < nt) ? tiles[q] : -1;
-        unsigned grp = __match_any_sync(0xffffffffu, t);
-        if (t >= 0) {
-            int leader = __ffs(grp) - 1;
-            unsigned base = 0;
-            if (lane == leader) base = atomicAdd(&cursor[t], (unsigned)__popc(grp));
-            base = __shfl_sync(grp, base, leader);
-            rec[off[t] + base + __popc(grp & lt)] = r;
-        }
-    }
 }
 
 // Records that keep the particle instead of its weight, so that one binning serves every
@@ -312,39 +303,184 @@ struct PRecS {
     int p;    // particle index within its source
 };
 
+// Record makers for the scatter: weight-carrying records (the box), or particle-index
+// records (the survey catalogues, srcid 0 data / 1 randoms).
 template <typename T>
-__global__ void k_bin_scatter_idx(PartSrc src, int srcid, AssignGeom g, const unsigned int *off, unsigned int *cursor,
-                                  PRecS<T> *rec) {
-    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int tiles[64];
-    int nt = 0;
-    PRecS<T> r;
-    if (p < src.n) {
-        double pos[3];
-        load_pos(src, p, pos);
-        int anc[3];
-        double d[3];
-        for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
-        nt = particle_tiles(g, anc, tiles);
+struct RecWeight {
+    using R = PRec<T>;
+    __device__ __forceinline__ R make(const PartSrc &s, long long p, const int anc[3], const double d[3]) const {
+        R r;
+        double wr, wi;
+        load_weight(s, p, wr, wi);
+        for (int a = 0; a < 3; a++) {
+            r.i[a] = anc[a];
+            r.d[a] = (T)d[a];
+        }
+        r.wr = (T)wr;
+        r.wi = (T)wi;
+        return r;
+    }
+};
+template <typename T>
+struct RecIndex {
+    using R = PRecS<T>;
+    int srcid;
+    __device__ __forceinline__ R make(const PartSrc &, long long p, const int anc[3], const double d[3]) const {
+        R r;
         for (int a = 0; a < 3; a++) {
             r.i[a] = anc[a];
             r.d[a] = (T)d[a];
         }
         r.src = srcid;
         r.p = (int)p;
+        return r;
     }
+};
+
+// Particles whose stencil straddles a non-periodic mesh edge (the reference's flat-index
+// rule couples the axes there) take a longer path: deduplicated effective cells, and an
+// in-bounds mass point by point.  A warp that met one such lane would idle its other lanes
+// for that path, and a catalogue stored in spatial order has some in most warps that touch
+// a face; so the main passes hand those particles to a list (Defer) and a second launch
+// of the same kernel runs them with every lane on the long path.
+struct Defer {
+    int *list;          // particle indices, capacity n
+    unsigned *count;    // device counter
+    int pass;           // 0: main pass (append), 1: the deferred pass (read the list)
+};
+
+// Lanes of a warp with `want` set append their particle index to the list.
+__device__ __forceinline__ void defer_push(const Defer &df, bool want, long long p) {
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    unsigned base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(df.count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (want) df.list[base + __popc(m & ((1u << lane) - 1u))] = (int)p;
+}
+
+// Pass 1: tile counts + (when mass != null) the FP64 in-bounds mass
+// sum_p w_p factor prod(w_axis)  (the field's exact integral, needed for the k = 0 mode
+// since boundary drops lose mass).  Clustered catalogues put many lanes of a warp on the
+// same tile, so the count is warp-aggregated.  Whole warps stride over the catalogue (the
+// main pass) or the deferred list, and the mass is reduced per block before one atomic.
+__global__ void __launch_bounds__(256, 3) k_bin_count(PartSrc src, AssignGeom g, Defer df, unsigned int *cnt,
+                                                      double *mass) {
+    __shared__ double red[2][32];
+    double m_re = 0.0, m_im = 0.0;
+    const int lane = threadIdx.x & 31;
+    const long long wstride = (long long)gridDim.x * blockDim.x;
+    const long long total = df.pass ? (long long)*df.count : src.n;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wbase < total;
+         wbase += wstride) {
+        const long long i = wbase + lane;
+        const long long p = (i < total) ? (df.pass ? (long long)df.list[i] : i) : -1;
+        TileList tl;
+        int slow[HG_SLOW_TILES];
+        tl.n = 0;
+        bool push = false;
+        if (p >= 0) {
+            double pos[3], wr = 0.0, wi = 0.0;
+            load_pos(src, p, pos);
+            if (mass) load_weight(src, p, wr, wi);
+            int anc[3];
+            double d[3];
+            for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
+            if (!df.pass && !stencil_separable(g, anc)) {
+                push = true;
+            } else {
+                tile_list(g, anc, tl, slow);
+                if (!mass) {
+                } else if (tl.sep) {
+                    // every stencil point lands: the weights sum to one per axis
+                    m_re += wr * g.factor;
+                    m_im += wi * g.factor;
+                } else {
+                    // in-bounds mass in the reference's product order
+                    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+                    for (int q = 0; q < W * W * W; q++) {
+                        const int a = q / (W * W), b = (q / W) % W, c = q % W;
+                        int cx, cy, cz;
+                        if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
+                        const double wa = axis_weight_at<double>(g.scheme, d[0], a),
+                                     wb = axis_weight_at<double>(g.scheme, d[1], b),
+                                     wc = axis_weight_at<double>(g.scheme, d[2], c);
+                        m_re += wr * g.factor * wa * wb * wc;
+                        m_im += wi * g.factor * wa * wb * wc;
+                    }
+                }
+            }
+        }
+        if (!df.pass) defer_push(df, push, p);
+        const int maxnt = __reduce_max_sync(0xffffffffu, tl.n);
+        for (int q = 0; q < maxnt; q++) {
+            const int t = (q < tl.n) ? tile_at(g, tl, slow, q) : -1;
+            const unsigned grp = __match_any_sync(0xffffffffu, t);
+            if (t >= 0 && lane == __ffs(grp) - 1) atomicAdd(&cnt[t], (unsigned)__popc(grp));
+        }
+    }
+    if (!mass) return;
+    m_re = warp_sum_d(m_re);
+    m_im = warp_sum_d(m_im);
+    if (lane == 0) {
+        red[0][threadIdx.x >> 5] = m_re;
+        red[1][threadIdx.x >> 5] = m_im;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sr = 0.0, si = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            sr += red[0][w];
+            si += red[1][w];
+        }
+        if (sr != 0.0) atomicAdd(&mass[0], sr);
+        if (si != 0.0) atomicAdd(&mass[1], si);
+    }
+}
+
+// Pass 3: one record per (particle, tile).  The main pass fills each tile's range from the
+// front (cursor) and skips the deferred particles; the deferred pass fills it from the back
+// (cursor_back), so the records of stencils that straddle a mesh edge sit together at the
+// end of their tile's range and the accumulation's warps take one path or the other.
+template <class MK>
+__global__ void k_bin_scatter(PartSrc src, AssignGeom g, MK mk, Defer df, const unsigned int *off,
+                              unsigned int *cursor, unsigned int *cursor_back, typename MK::R *rec) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    int maxnt = __reduce_max_sync(0xffffffffu, nt);
-    for (int q = 0; q < maxnt; q++) {
-        int t = (q < nt) ? tiles[q] : -1;
-        unsigned grp = __match_any_sync(0xffffffffu, t);
-        if (t >= 0) {
-            int leader = __ffs(grp) - 1;
-            unsigned base = 0;
-            if (lane == leader) base = atomicAdd(&cursor[t], (unsigned)__popc(grp));
-            base = __shfl_sync(grp, base, leader);
-            rec[off[t] + base + __popc(grp & lt)] = r;
+    const long long wstride = (long long)gridDim.x * blockDim.x;
+    const long long total = df.pass ? (long long)*df.count : src.n;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wbase < total;
+         wbase += wstride) {
+        const long long i = wbase + lane;
+        const long long p = (i < total) ? (df.pass ? (long long)df.list[i] : i) : -1;
+        TileList tl;
+        int slow[HG_SLOW_TILES];
+        tl.n = 0;
+        typename MK::R r;
+        if (p >= 0) {
+            double pos[3];
+            load_pos(src, p, pos);
+            int anc[3];
+            double d[3];
+            for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
+            if (df.pass || stencil_separable(g, anc)) {
+                tile_list(g, anc, tl, slow);
+                r = mk.make(src, p, anc, d);
+            }
+        }
+        const int maxnt = __reduce_max_sync(0xffffffffu, tl.n);
+        for (int q = 0; q < maxnt; q++) {
+            const int t = (q < tl.n) ? tile_at(g, tl, slow, q) : -1;
+            const unsigned grp = __match_any_sync(0xffffffffu, t);
+            if (t >= 0) {
+                const int leader = __ffs(grp) - 1;
+                unsigned base = 0;
+                if (lane == leader) base = atomicAdd(df.pass ? &cursor_back[t] : &cursor[t], (unsigned)__popc(grp));
+                base = __shfl_sync(grp, base, leader);
+                const unsigned k = base + __popc(grp & lt);
+                rec[df.pass ? off[t + 1] - 1u - k : off[t] + k] = r;
+            }
         }
     }
 }
@@ -464,16 +600,65 @@ __global__ void k_zero_split_tiles(const Chunk *ch, AssignGeom g, T *mesh_re, T 
     }
 }
 
-// One CTA per chunk.  Shared-memory accumulator in the form's precision (a chunk holds at
-// most 2048 records, which bounds the FP32 summation error); the mesh stores the density
-// rho = sum_p w_p (1/dV) prod(w_axis) like the reference, in T.
-template <typename T, bool CPLX>
+// Local tile coordinates of a separable stencil along axis a: bit j of the result is set
+// when point j (index i0 + j) lies in this CTA's tile, at local index loc[j].
+__device__ __forceinline__ unsigned axis_local(const AssignGeom &g, int a, int i0, int o, int W, int loc[4]) {
+    unsigned m = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        loc[j] = 0;
+        if (j < W) {
+            const int l = axis_cell(g, a, i0 + j) - o;
+            if ((unsigned)l < (unsigned)g.t[a]) {
+                loc[j] = l;
+                m |= 1u << j;
+            }
+        }
+    }
+    return m;
+}
+
+// One CTA per chunk.  The mesh stores the density rho = sum_p w_p (1/dV) prod(w_axis)
+// like the reference (the FP32 form: the mass rho dV), in T.
+//
+// Accumulator.  FIX = false: a shared-memory tile of T with T atomics.  FIX = true (FP32
+// real meshes of sources whose per-record weight |w acc_factor| is bounded by
+// g.fix_bound, which the host knows for unweighted catalogues): an exact fixed-point sum
+// in two 32-bit integer words per cell.  Integer shared-memory atomics run about five
+// times faster than FP32 ones on this part (which emulates the latter), and the
+// accumulation is bound by them.  Per chunk every stencil weight (an FP32 product) is
+// scaled by S = 2^s, exactly, with (records) x fix_bound x S < 2^50 and
+// fix_bound x S < 2^42, and split as x = hi 2^20 + lo with hi = round(x / 2^20) and
+// |lo| <= 2^19; both parts are formed exactly with FP32 adds against 1.5 x 2^23 (valid
+// below 2^22), and lo is rounded to an integer there, the only rounding (below 2^-50 of
+// the chunk's bound).  A cell receives at most one add per record (the stencil's points
+// are distinct cells when every axis has at least W cells), so |sum hi| < 2^30 + records
+// and |sum lo| <= records 2^19 <= 2^30: neither word overflows, the sum is exact and
+// independent of the order of the atomics, and it is rounded once, to the mesh's FP32.
+//
+// Separable stencils (every point inside the mesh, or a periodic mesh) compute their local
+// coordinates axis by axis; the few that straddle a non-periodic mesh edge take the
+// reference's flat-index rule point by point.
+// x = hi 2^20 + lo exactly for |x| < 2^42, hi = round(x / 2^20), lo = round(x - hi 2^20):
+// 1.5 x 2^23 + y (|y| < 2^22) is a float of unit spacing whose low bits hold round(y).
+__device__ __forceinline__ void fix_split(float x, int &hi, int &lo) {
+    const float t = __fmaf_rn(x, 0x1p-20f, 12582912.0f);
+    hi = __float_as_int(t) - 0x4B400000;
+    const float r = __fmaf_rn(-(t - 12582912.0f), 0x1p20f, x);
+    lo = __float_as_int(__fadd_rn(r, 12582912.0f)) - 0x4B400000;
+}
+
+template <typename T, bool CPLX, bool FIX, int SCHEME>
 __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
+    static_assert(!FIX || (!CPLX && sizeof(T) == 4), "fixed-point accumulation is for real FP32 meshes");
+    constexpr int W = SCHEME + 1, s0 = (SCHEME >= 2) ? -1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *acc = reinterpret_cast<T *>(smem_raw);
     const int tcells = g.t[0] * g.t[1] * g.t[2];
     T *acc_im = acc + tcells;
-    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
+    int *acc_hi = reinterpret_cast<int *>(smem_raw);
+    int *acc_lo = acc_hi + tcells;
+    for (int c = threadIdx.x; c < tcells * ((CPLX || FIX) ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
     __syncthreads();
     const Chunk k = ch[blockIdx.x];
     const int tile = k.tile;
@@ -481,36 +666,87 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     const int ty = (tile / g.nt[2]) % g.nt[1];
     const int tx = tile / (g.nt[2] * g.nt[1]);
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
-    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+    float fscale = 1.0f;
+    double dinv = 1.0;
+    if (FIX) {
+        int e, e1;
+        frexpf(float(k.r1 - k.r0) * g.fix_bound, &e);
+        frexpf(g.fix_bound, &e1);
+        const int sc = min(50 - e, 42 - e1);
+        fscale = ldexpf(1.0f, sc);
+        dinv = ldexp(1.0, -sc);
+    }
     const T factor = (T)g.acc_factor;
+    auto add = [&](int li, T v, T vi) {
+        if (FIX) {
+            int hi, lo;
+            fix_split((float)v, hi, lo);
+            atomicAdd(&acc_hi[li], hi);
+            atomicAdd(&acc_lo[li], lo);
+        } else {
+            atomicAdd(&acc[li], v);
+            if (CPLX) atomicAdd(&acc_im[li], vi);
+        }
+    };
     for (unsigned r = k.r0 + threadIdx.x; r < k.r1; r += blockDim.x) {
-        PRec<T> pr = rec[r];
-        T w[3][4];
-        for (int a = 0; a < 3; a++) axis_weights<T>(g.scheme, pr.d[a], w[a]);
-        const T wr = pr.wr, wi = pr.wi;
-        for (int a = 0; a < W; a++)
-            for (int b = 0; b < W; b++)
-                for (int c = 0; c < W; c++) {
-                    int cx, cy, cz;
-                    if (!effective_cell(g, pr.i[0] + s0 + a, pr.i[1] + s0 + b, pr.i[2] + s0 + c, cx, cy, cz)) continue;
-                    int lx = cx - ox, ly = cy - oy, lz = cz - oz;
-                    if ((unsigned)lx >= (unsigned)g.t[0] || (unsigned)ly >= (unsigned)g.t[1] ||
-                        (unsigned)lz >= (unsigned)g.t[2])
-                        continue;
-                    int li = (lx * g.t[1] + ly) * g.t[2] + lz;
-                    atomicAdd(&acc[li], wr * factor * w[0][a] * w[1][b] * w[2][c]);
-                    if (CPLX) atomicAdd(&acc_im[li], wi * factor * w[0][a] * w[1][b] * w[2][c]);
+        const PRec<T> pr = rec[r];
+        T wr = pr.wr * factor, wi = pr.wi * factor;
+        if (FIX) wr *= (T)fscale;
+        const int anc[3] = {pr.i[0], pr.i[1], pr.i[2]};
+        if (stencil_separable(g, anc)) {
+            T w[3][W];
+            int lx[4], ly[4], lz[4];
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int j = 0; j < W; j++) w[a][j] = axis_weight_at<T>(SCHEME, pr.d[a], j);
+            const unsigned mx = axis_local(g, 0, anc[0] + s0, ox, W, lx);
+            const unsigned my = axis_local(g, 1, anc[1] + s0, oy, W, ly);
+            const unsigned mz = axis_local(g, 2, anc[2] + s0, oz, W, lz);
+#pragma unroll
+            for (int a = 0; a < W; a++) {
+                if (!((mx >> a) & 1u)) continue;
+                const T wa = wr * w[0][a], wia = wi * w[0][a];
+#pragma unroll
+                for (int b = 0; b < W; b++) {
+                    if (!((my >> b) & 1u)) continue;
+                    const T wab = wa * w[1][b], wiab = wia * w[1][b];
+                    const int lab = (lx[a] * g.t[1] + ly[b]) * g.t[2];
+#pragma unroll
+                    for (int c = 0; c < W; c++) {
+                        if (!((mz >> c) & 1u)) continue;
+                        add(lab + lz[c], wab * w[2][c], wiab * w[2][c]);
+                    }
                 }
+            }
+            continue;
+        }
+        // a stencil straddling a non-periodic mesh edge (the scatter put these records at the
+        // end of the tile's range): point by point, the reference's flat-index rule, weights
+        // evaluated per point (no arrays)
+#pragma unroll 1
+        for (int p = 0; p < W * W * W; p++) {
+            const int a = p / (W * W), b = (p / W) % W, c = p % W;
+            int cx, cy, cz;
+            if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
+            const int lx = cx - ox, ly = cy - oy, lz = cz - oz;
+            if ((unsigned)lx >= (unsigned)g.t[0] || (unsigned)ly >= (unsigned)g.t[1] || (unsigned)lz >= (unsigned)g.t[2])
+                continue;
+            const T wa = axis_weight_at<T>(SCHEME, pr.d[0], a), wb = axis_weight_at<T>(SCHEME, pr.d[1], b),
+                    wc = axis_weight_at<T>(SCHEME, pr.d[2], c);
+            add((lx * g.t[1] + ly) * g.t[2] + lz, wr * wa * wb * wc, wi * wa * wb * wc);
+        }
     }
     __syncthreads();
     for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
         int lx, ly, lz;
         long long cell = tile_cell(g, tile, li, lx, ly, lz);
+        const T v = FIX ? (T)((double)((long long)acc_hi[li] * 1048576LL + (long long)acc_lo[li]) * dinv) : acc[li];
         if (k.multi == 0) {
-            mesh_re[cell] = acc[li];
+            mesh_re[cell] = v;
             if (CPLX) mesh_im[cell] = acc_im[li];
         } else {
-            if (acc[li] != (T)0) atomicAdd(&mesh_re[cell], acc[li]);
+            if (v != (T)0) atomicAdd(&mesh_re[cell], v);
             if (CPLX && acc_im[li] != (T)0) atomicAdd(&mesh_im[cell], acc_im[li]);
         }
     }
@@ -555,9 +791,13 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
         }
         const T wr = (T)wr64, wi = (T)wi64;
         const T factor = (T)g.acc_factor;
-        for (int a = 0; a < W; a++)
-            for (int b = 0; b < W; b++)
-                for (int c = 0; c < W; c++) {
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    if (a >= W || b >= W || c >= W) continue;
                     int cx, cy, cz;
                     if (!effective_cell(g, pr.i[0] + s0 + a, pr.i[1] + s0 + b, pr.i[2] + s0 + c, cx, cy, cz)) continue;
                     int lx = cx - ox, ly = cy - oy, lz = cz - oz;

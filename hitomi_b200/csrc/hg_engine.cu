@@ -168,12 +168,18 @@ struct Engine : public hg_ctx {
 
     // assignment scratch
     DBuf cnt, off, cursor, rec, cubtmp, mass, nch, choff, chunks;
+    DBuf deflist, defcnt, cursor_back;  // particles whose stencil straddles a non-periodic edge
     static constexpr unsigned CHUNK = 2048;  // records per accumulation CTA
     // fields
     DBuf mesh;  // real density rho (box)
     DBuf H;     // half spectrum of dV (rho - nbar)
     DBuf H2;    // half spectrum of the half-cell shifted assignment (interlacing)
     bool dens_valid = false;
+    struct PkBins {
+        std::vector<double> avg;  // [nbin] complex bin averages before the (2l+1) factor
+        std::vector<unsigned long long> nm;
+    };
+    std::map<int, PkBins> pk_cache;  // box P_l bins of the current density, by l
     double dens_mass = 0.0;  // sum_cells rho  (FP64)
     double delta0 = 0.0, N0 = 0.0;
 
@@ -552,6 +558,7 @@ struct Engine : public hg_ctx {
     void invalidate() {
         src_kind = -1;
         dens_valid = false;
+        pk_cache.clear();
         Gm_ok.clear();
         shD_valid = false;
         xi_valid = false;
@@ -588,7 +595,56 @@ struct Engine : public hg_ctx {
         // mass per cell (rho dV), which removes the float rounding of 1/dV and dV from every
         // cell; the FFT input (rho - N/V) dV is then mass - N/Ncells (same quantity).
         a.acc_factor = (sizeof(T) == 8) ? a.factor : 1.0;
+        a.fix_bound = 0.0f;
         return a;
+    }
+
+    // Tile counts of several sources (pass 1).  Each source's edge-straddling particles go to
+    // its own slice of the deferred list (at the running offset of the sources' sizes) and
+    // are counted by a second launch; the scatter reads the same slices.
+    void bin_count_sources(const PartSrc *srcs, int ns, const AssignGeom &ag, double *mass_dev) {
+        long long cap = 0;
+        for (int q = 0; q < ns; q++) cap += srcs[q].n;
+        HG_CK(deflist.ensure(sizeof(int) * std::max<long long>(cap, 1)));
+        HG_CK(defcnt.ensure(sizeof(unsigned) * ns));
+        HG_CK(cudaMemsetAsync(defcnt.p, 0, sizeof(unsigned) * ns, st));
+        long long o = 0;
+        for (int q = 0; q < ns; q++) {
+            Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0};
+            kb("assign_bin_count", double(srcs[q].n) * 24.0);
+            k_bin_count<<<(unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 8), 256, 0, st>>>(
+                srcs[q], ag, df, dp<unsigned>(cnt), mass_dev);
+            ke();
+            df.pass = 1;
+            kb("assign_edge_count", 0.0);
+            k_bin_count<<<148 * 2, 256, 0, st>>>(srcs[q], ag, df, dp<unsigned>(cnt), mass_dev);
+            ke();
+            o += srcs[q].n;
+        }
+    }
+
+    // Records of several sources (pass 3), from the front of each tile's range, then the
+    // deferred particles from the back.
+    template <class MK>
+    void bin_scatter_sources(const PartSrc *srcs, const MK *mks, int ns, const AssignGeom &ag, int ntiles,
+                             typename MK::R *recp, double rec_bytes) {
+        HG_CK(cursor_back.ensure(sizeof(unsigned) * (ntiles + 1)));
+        HG_CK(cudaMemsetAsync(cursor_back.p, 0, sizeof(unsigned) * (ntiles + 1), st));
+        long long o = 0, nsum = 0;
+        for (int q = 0; q < ns; q++) nsum += srcs[q].n;
+        for (int q = 0; q < ns; q++) {
+            Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0};
+            kb("assign_bin_scatter", double(srcs[q].n) * 24.0 + rec_bytes * double(srcs[q].n) / double(nsum));
+            k_bin_scatter<MK><<<(unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 16), 256, 0, st>>>(
+                srcs[q], ag, mks[q], df, dp<unsigned>(off), dp<unsigned>(cursor), dp<unsigned>(cursor_back), recp);
+            ke();
+            df.pass = 1;
+            kb("assign_edge_scatter", 0.0);
+            k_bin_scatter<MK><<<148 * 2, 256, 0, st>>>(srcs[q], ag, mks[q], df, dp<unsigned>(off),
+                                                      dp<unsigned>(cursor), dp<unsigned>(cursor_back), recp);
+            ke();
+            o += srcs[q].n;
+        }
     }
 
     // Assign one or more particle sources into one mesh of type U (real, or complex as
@@ -608,14 +664,7 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(mass.p, 0, sizeof(double) * 2, st));
-        long long nsum = 0;
-        for (const auto &src : srcs) {
-            nsum += src.n;
-            kb("assign_bin_count", double(src.n) * 24.0);
-            k_bin_count<<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(cnt),
-                                                           want_mass ? dp<double>(mass) : nullptr);
-            ke();
-        }
+        bin_count_sources(srcs.data(), (int)srcs.size(), ag, want_mass ? dp<double>(mass) : nullptr);
         size_t tb = 0, tb2 = 0;
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
@@ -645,22 +694,58 @@ struct Engine : public hg_ctx {
         k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
                                                         dp<Chunk>(chunks));
         ke();
-        for (const auto &src : srcs) {
-            kb("assign_bin_scatter", double(src.n) * 24.0 + double(total) * sizeof(PRec<U>) * double(src.n) / nsum);
-            k_bin_scatter<U><<<grid1(src.n, 256), 256, 0, st>>>(src, ag, dp<unsigned>(off), dp<unsigned>(cursor),
-                                                                dp<PRec<U>>(rec));
-            ke();
+        {
+            std::vector<RecWeight<U>> mk(srcs.size());
+            bin_scatter_sources(srcs.data(), mk.data(), (int)srcs.size(), ag, ntiles, dp<PRec<U>>(rec),
+                                double(total) * sizeof(PRec<U>));
         }
         kb("assign_zero_split", 0.0);
         k_zero_split_tiles<U, CPLX><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), ag, out_re, out_im);
         ke();
-        size_t smem = sizeof(U) * ag.t[0] * ag.t[1] * ag.t[2] * (CPLX ? 2 : 1);
-        HG_CK(cudaFuncSetAttribute(k_tile_accum<U, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const size_t tbytes = sizeof(U) * ag.t[0] * ag.t[1] * ag.t[2];
+        // exact fixed-point accumulation for real FP32 meshes of unweighted sources, whose
+        // per-record weight |scale| acc_factor is known here (the stencil weights sum to one),
+        // on meshes with at least W cells per axis (one add per record and cell)
+        static_assert(CHUNK <= 2048, "the fixed-point lo word holds at most 2048 adds of < 2^20");
+        bool fix = false;
+        AssignGeom agx = ag;
+        if constexpr (sizeof(U) == 4 && !CPLX) {
+            fix = true;
+            double wmax = 0.0;
+            for (const auto &src : srcs) {
+                fix = fix && src.cw == nullptr && !src.ylm_on && src.w_off < 0;
+                wmax = std::max(wmax, std::fabs(src.scale));
+            }
+            for (int a = 0; a < 3; a++) fix = fix && ag.n[a] >= stencil_width(ag.scheme);
+            agx.fix_bound = (float)(wmax * std::fabs(ag.acc_factor));
+            fix = fix && agx.fix_bound > 0.0f;
+        }
         kb("assign_tile_accum", double(total) * sizeof(PRec<U>) + double(g.ntot) * sizeof(U) * (CPLX ? 2 : 1));
-        k_tile_accum<U, CPLX><<<nchunks, 256, smem, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
+        switch (ag.scheme) {
+            case HG_NGP: launch_tile_accum<U, CPLX, HG_NGP>(fix, tbytes, nchunks, agx, out_re, out_im); break;
+            case HG_CIC: launch_tile_accum<U, CPLX, HG_CIC>(fix, tbytes, nchunks, agx, out_re, out_im); break;
+            case HG_TSC: launch_tile_accum<U, CPLX, HG_TSC>(fix, tbytes, nchunks, agx, out_re, out_im); break;
+            default: launch_tile_accum<U, CPLX, HG_PCS>(fix, tbytes, nchunks, agx, out_re, out_im); break;
+        }
         ke();
         if (mass_im) *mass_im = hm[1];
         return hm[0];
+    }
+
+    template <typename U, bool CPLX, int SCHEME>
+    void launch_tile_accum(bool fix, size_t tbytes, unsigned nchunks, const AssignGeom &ag, U *out_re, U *out_im) {
+        if constexpr (sizeof(U) == 4 && !CPLX) {
+            if (fix) {
+                auto kern = k_tile_accum<U, false, true, SCHEME>;
+                HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * tbytes)));
+                kern<<<nchunks, 256, 2 * tbytes, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
+                return;
+            }
+        }
+        const size_t smem = tbytes * (CPLX ? 2 : 1);
+        auto kern = k_tile_accum<U, CPLX, false, SCHEME>;
+        HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<nchunks, 256, smem, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
     }
 
     double assign_real(const PartSrc &src, const AssignGeom &ag, T *out) {
@@ -809,13 +894,32 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(ell >= 0, "ell must be >= 0");
         begin();
         box_density();
-        std::vector<double> avg;
-        std::vector<unsigned long long> nm;
-        pk_bin({LM{ell, 0}}, double(slot[0].n), 0.0, avg, nm);
+        if (!pk_cache.count(ell)) {
+            // one pass over the modes bins the requested multipole together with the
+            // others of the usual set (0, 2, 4) not yet binned for this density: the pass
+            // is latency-bound, so the extra multipoles cost next to nothing
+            std::vector<LM> lm{LM{ell, 0}};
+            for (int e : {0, 2, 4})
+                if (e != ell && !pk_cache.count(e)) lm.push_back(LM{e, 0});
+            std::vector<double> avg;
+            std::vector<unsigned long long> nm;
+            pk_bin(lm, double(slot[0].n), 0.0, avg, nm);
+            const int nl = (int)lm.size();
+            for (int q = 0; q < nl; q++) {
+                PkBins &pb = pk_cache[lm[q].l];
+                pb.avg.resize(2 * cfg.n_kbin);
+                for (int i = 0; i < cfg.n_kbin; i++) {
+                    pb.avg[2 * i] = avg[2 * (i * nl + q)];
+                    pb.avg[2 * i + 1] = avg[2 * (i * nl + q) + 1];
+                }
+                pb.nm = nm;
+            }
+        }
+        const PkBins &pb = pk_cache[ell];
         for (int i = 0; i < cfg.n_kbin; i++) {
-            pk_save[2 * i] = double(2 * ell + 1) * avg[2 * i];
-            pk_save[2 * i + 1] = double(2 * ell + 1) * avg[2 * i + 1];
-            if (n_mode) n_mode[i] = (int)nm[i];
+            pk_save[2 * i] = double(2 * ell + 1) * pb.avg[2 * i];
+            pk_save[2 * i + 1] = double(2 * ell + 1) * pb.avg[2 * i + 1];
+            if (n_mode) n_mode[i] = (int)pb.nm[i];
         }
         if (norm) *norm = g.volume / double(slot[0].n) / double(slot[0].n);
         end();
@@ -1907,11 +2011,7 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         const PartSrc src[2] = {survey_src(0, false, 0, 0, 1.0), survey_src(1, false, 0, 0, 1.0)};
-        for (int q = 0; q < 2; q++) {
-            kb("assign_bin_count", double(src[q].n) * 24.0);
-            k_bin_count<<<grid1(src[q].n, 256), 256, 0, st>>>(src[q], ag, dp<unsigned>(cnt), nullptr);
-            ke();
-        }
+        bin_count_sources(src, 2, ag, nullptr);
         size_t tb = 0, tb2 = 0;
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
@@ -1929,11 +2029,9 @@ struct Engine : public hg_ctx {
         HG_CK(B.chunks.ensure(sizeof(Chunk) * std::max<size_t>(B.nchunks, 1)));
         k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
                                                         dp<Chunk>(B.chunks));
-        for (int q = 0; q < 2; q++) {
-            kb("assign_bin_scatter", double(src[q].n) * 24.0 + double(B.total) * sizeof(PRecS<T>) / 2);
-            k_bin_scatter_idx<T><<<grid1(src[q].n, 256), 256, 0, st>>>(src[q], q, ag, dp<unsigned>(off),
-                                                                       dp<unsigned>(cursor), dp<PRecS<T>>(B.rec));
-            ke();
+        {
+            const RecIndex<T> mk[2] = {RecIndex<T>{0}, RecIndex<T>{1}};
+            bin_scatter_sources(src, mk, 2, ag, ntiles, dp<PRecS<T>>(B.rec), double(B.total) * sizeof(PRecS<T>));
         }
         HG_CK(cudaGetLastError());
         B.ok = true;
