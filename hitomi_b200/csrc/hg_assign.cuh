@@ -470,16 +470,40 @@ __global__ void k_bin_scatter(PartSrc src, AssignGeom g, MK mk, Defer df, const 
             }
         }
         const int maxnt = __reduce_max_sync(0xffffffffu, tl.n);
+        if (!df.pass) {
+            // separable stencils meet at most 8 tiles: every counter atomic of the warp is
+            // issued before any result is used, so their round trips overlap
+            int tq[8];
+            unsigned gq[8], bq[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                tq[q] = -1;
+                gq[q] = 0u;
+                bq[q] = 0u;
+                if (q < maxnt) {
+                    tq[q] = (q < tl.n) ? tile_at(g, tl, slow, q) : -1;
+                    gq[q] = __match_any_sync(0xffffffffu, tq[q]);
+                    if (tq[q] >= 0 && lane == __ffs(gq[q]) - 1) bq[q] = atomicAdd(&cursor[tq[q]], (unsigned)__popc(gq[q]));
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (q < maxnt && tq[q] >= 0) {
+                    const unsigned base = __shfl_sync(gq[q], bq[q], __ffs(gq[q]) - 1);
+                    rec[off[tq[q]] + base + __popc(gq[q] & lt)] = r;
+                }
+            }
+            continue;
+        }
         for (int q = 0; q < maxnt; q++) {
             const int t = (q < tl.n) ? tile_at(g, tl, slow, q) : -1;
             const unsigned grp = __match_any_sync(0xffffffffu, t);
             if (t >= 0) {
                 const int leader = __ffs(grp) - 1;
                 unsigned base = 0;
-                if (lane == leader) base = atomicAdd(df.pass ? &cursor_back[t] : &cursor[t], (unsigned)__popc(grp));
+                if (lane == leader) base = atomicAdd(&cursor_back[t], (unsigned)__popc(grp));
                 base = __shfl_sync(grp, base, leader);
-                const unsigned k = base + __popc(grp & lt);
-                rec[df.pass ? off[t + 1] - 1u - k : off[t] + k] = r;
+                rec[off[t + 1] - 1u - (base + __popc(grp & lt))] = r;
             }
         }
     }
@@ -759,11 +783,15 @@ struct FieldW {
 
 // k_tile_accum on particle-index records: the weight comes from the particle
 // (load_weight, the same FP64 expression as the weight-carrying records), and the FP64
-// in-bounds mass sum of w factor prod(w_axis) is reduced on the way (each in-bounds stencil
-// point is accumulated by exactly one record), for the transform's exact k = 0 value.
-template <typename T, bool CPLX>
+// in-bounds mass sum of w factor prod(w_axis) is reduced on the way, for the transform's
+// exact k = 0 value.  A separable stencil lands whole, so its mass is w factor (the axis
+// weights sum to one), counted by the one record whose tile holds the stencil's first
+// point; an edge-straddling stencil (records at the end of the tile's range) adds its
+// in-bounds points one by one in the reference's product order.
+template <typename T, bool CPLX, int SCHEME>
 __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeom g, FieldW fw, T *mesh_re, T *mesh_im,
                                  double *mass) {
+    constexpr int W = SCHEME + 1, s0 = (SCHEME >= 2) ? -1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *acc = reinterpret_cast<T *>(smem_raw);
     const int tcells = g.t[0] * g.t[1] * g.t[2];
@@ -777,39 +805,66 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
     const int ty = (tile / g.nt[2]) % g.nt[1];
     const int tx = tile / (g.nt[2] * g.nt[1]);
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
-    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+    const T factor = (T)g.acc_factor;
     double mr = 0.0, mi = 0.0;
     for (unsigned r = k.r0 + threadIdx.x; r < k.r1; r += blockDim.x) {
         const PRecS<T> pr = rec[r];
         double wr64, wi64;
         load_weight(fw.s[pr.src], pr.p, wr64, wi64);
-        T w[3][4];
-        double w64[3][4];
-        for (int a = 0; a < 3; a++) {
-            axis_weights<T>(g.scheme, pr.d[a], w[a]);
-            axis_weights<double>(g.scheme, (double)pr.d[a], w64[a]);
-        }
-        const T wr = (T)wr64, wi = (T)wi64;
-        const T factor = (T)g.acc_factor;
+        const T wr = (T)wr64 * factor, wi = (T)wi64 * factor;
+        const int anc[3] = {pr.i[0], pr.i[1], pr.i[2]};
+        if (stencil_separable(g, anc)) {
+            T w[3][W];
+            int lx[4], ly[4], lz[4];
 #pragma unroll
-        for (int a = 0; a < 4; a++)
+            for (int a = 0; a < 3; a++)
 #pragma unroll
-            for (int b = 0; b < 4; b++)
+                for (int j = 0; j < W; j++) w[a][j] = axis_weight_at<T>(SCHEME, pr.d[a], j);
+            const unsigned mx = axis_local(g, 0, anc[0] + s0, ox, W, lx);
+            const unsigned my = axis_local(g, 1, anc[1] + s0, oy, W, ly);
+            const unsigned mz = axis_local(g, 2, anc[2] + s0, oz, W, lz);
+            if (mx & my & mz & 1u) {
+                mr += wr64 * g.factor;
+                mi += wi64 * g.factor;
+            }
 #pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    if (a >= W || b >= W || c >= W) continue;
-                    int cx, cy, cz;
-                    if (!effective_cell(g, pr.i[0] + s0 + a, pr.i[1] + s0 + b, pr.i[2] + s0 + c, cx, cy, cz)) continue;
-                    int lx = cx - ox, ly = cy - oy, lz = cz - oz;
-                    if ((unsigned)lx >= (unsigned)g.t[0] || (unsigned)ly >= (unsigned)g.t[1] ||
-                        (unsigned)lz >= (unsigned)g.t[2])
-                        continue;
-                    int li = (lx * g.t[1] + ly) * g.t[2] + lz;
-                    atomicAdd(&acc[li], wr * factor * w[0][a] * w[1][b] * w[2][c]);
-                    if (CPLX) atomicAdd(&acc_im[li], wi * factor * w[0][a] * w[1][b] * w[2][c]);
-                    mr += wr64 * g.factor * w64[0][a] * w64[1][b] * w64[2][c];
-                    mi += wi64 * g.factor * w64[0][a] * w64[1][b] * w64[2][c];
+            for (int a = 0; a < W; a++) {
+                if (!((mx >> a) & 1u)) continue;
+                const T wa = wr * w[0][a], wia = wi * w[0][a];
+#pragma unroll
+                for (int b = 0; b < W; b++) {
+                    if (!((my >> b) & 1u)) continue;
+                    const T wab = wa * w[1][b], wiab = wia * w[1][b];
+                    const int lab = (lx[a] * g.t[1] + ly[b]) * g.t[2];
+#pragma unroll
+                    for (int c = 0; c < W; c++) {
+                        if (!((mz >> c) & 1u)) continue;
+                        atomicAdd(&acc[lab + lz[c]], wab * w[2][c]);
+                        if (CPLX) atomicAdd(&acc_im[lab + lz[c]], wiab * w[2][c]);
+                    }
                 }
+            }
+            continue;
+        }
+#pragma unroll 1
+        for (int p = 0; p < W * W * W; p++) {
+            const int a = p / (W * W), b = (p / W) % W, c = p % W;
+            int cx, cy, cz;
+            if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
+            const int lx = cx - ox, ly = cy - oy, lz = cz - oz;
+            if ((unsigned)lx >= (unsigned)g.t[0] || (unsigned)ly >= (unsigned)g.t[1] || (unsigned)lz >= (unsigned)g.t[2])
+                continue;
+            const int li = (lx * g.t[1] + ly) * g.t[2] + lz;
+            const T wa = axis_weight_at<T>(SCHEME, pr.d[0], a), wb = axis_weight_at<T>(SCHEME, pr.d[1], b),
+                    wc = axis_weight_at<T>(SCHEME, pr.d[2], c);
+            atomicAdd(&acc[li], wr * wa * wb * wc);
+            if (CPLX) atomicAdd(&acc_im[li], wi * wa * wb * wc);
+            const double da = axis_weight_at<double>(SCHEME, (double)pr.d[0], a),
+                         db = axis_weight_at<double>(SCHEME, (double)pr.d[1], b),
+                         dc = axis_weight_at<double>(SCHEME, (double)pr.d[2], c);
+            mr += wr64 * g.factor * da * db * dc;
+            mi += wi64 * g.factor * da * db * dc;
+        }
     }
     mr = warp_sum_d(mr);
     mi = warp_sum_d(mi);

@@ -225,6 +225,7 @@ struct Engine : public hg_ctx {
 
     // shot-noise state
     DBuf xi;
+    DBuf xi_half;  // box correlation field after x and y passes, x = 0 .. n0/2
     bool xi_valid = false;
     std::vector<int> orbit_lines, orbit_n2xy;
     DBuf d_orbit_lines, d_orbit_n2xy;
@@ -1210,8 +1211,7 @@ struct Engine : public hg_ctx {
         n2dim += 1;
     }
 
-    // xi after its x and y inverse passes (cached per catalogue)
-    // the correlation-field spectrum synthesised into xi, then its x pass in place
+    // a survey correlation-field spectrum (complex) synthesised into xi, then its x pass in place
     template <class LD>
     void xi_x_pass(const LD &ld) {
         const long long yz = (long long)g.n[1] * g.n[2];
@@ -1222,18 +1222,30 @@ struct Engine : public hg_ctx {
         pass<+1>(g.n[0], LdArr<T>{dp<C>(xi), g.n[0], yz}, StArr<T>{dp<C>(xi), g.n[0], yz}, 1, yz, "fft_xi_x");
     }
 
+    // Box correlation field after its x and y inverse passes (cached per catalogue).  Its
+    // spectrum P is real, so the x pass transforms two kz columns per complex line
+    // (k_synth_pairs: [n0][n1][n2/2] in xi), and the y pass separates them while keeping
+    // x = 0 .. n0/2 only (LdSplitX into xi_half: [n0/2 + 1][n1][n2]); the histogram
+    // kernel takes the line (-x, y) as the conjugate of (x, -y).
     void ensure_xi() {
         HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
                    "bispectrum / 3PCF shot noise needs equal cell sizes on all axes");
         build_orbits();
         if (xi_valid) return;
+        const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], nh = n2 / 2, hx = n0 / 2 + 1;
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
+        HG_CK(xi_half.ensure(sizeof(C) * (size_t)hx * n1 * n2));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
         const double S = double(slot[0].n);
-        LdXiHat<T> ld{half_spec(), g.n[2], xtabs, S, delta0 * N0, invV};
-        xi_x_pass(ld);
-        pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
-                 "fft_xi_y");
+        LdXiHat<T> ld{half_spec(), n2, xtabs, S, delta0 * N0, invV};
+        const long long yz = (long long)n1 * nh, tot = (long long)n0 * yz;
+        unsigned blocks = (unsigned)std::min<long long>(grid1(tot, 256), 148 * 16);
+        kb("xi_synth", double(tot) * sizeof(C) * 2.0);
+        k_synth_pairs<T, LdXiHat<T>><<<blocks, 256, 0, st>>>(ld, n0, n1, nh, dp<C>(xi));
+        ke();
+        pass<+1>(n0, LdArr<T>{dp<C>(xi), n0, yz}, StArr<T>{dp<C>(xi), n0, yz}, 1, yz, "fft_xi_x");
+        pass<+1>(n1, LdSplitX<T>{dp<C>(xi), n0, n1, nh}, StArr<T>{dp<C>(xi_half), n1, n2}, hx, n2, "fft_xi_y",
+                 double(hx) * n1 * n2 * sizeof(C) * 2.0);
         xi_valid = true;
     }
 
@@ -1242,8 +1254,9 @@ struct Engine : public hg_ctx {
         size_t smem = OrbitCfg<T, L>::smem();
         HG_CK(cudaFuncSetAttribute(k_xi_orbit_hist<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const C *twp = twiddles(L);
-        kb("xi_orbit_hist", double(g.ntot) * sizeof(C));
-        k_xi_orbit_hist<T, L><<<n_orb, OrbitCfg<T, L>::NT, smem, st>>>(dp<C>(xi), dp<int>(d_orbit_lines),
+        kb("xi_orbit_hist", double(g.n[0] / 2 + 1) * g.n[1] * g.n[2] * sizeof(C));
+        k_xi_orbit_hist<T, L><<<n_orb, OrbitCfg<T, L>::NT, smem, st>>>(dp<C>(xi_half), g.n[0], g.n[1],
+                                                                       dp<int>(d_orbit_lines),
                                                                        dp<int>(d_orbit_n2xy), n_orb, twp, hs, n2dim,
                                                                        hist);
         ke();
@@ -2053,10 +2066,18 @@ struct Engine : public hg_ctx {
         k_zero_split_tiles<T, CPLX><<<B.nchunks, 256, 0, st>>>(dp<Chunk>(B.chunks), ag, re, im);
         ke();
         const size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2] * (CPLX ? 2 : 1);
-        HG_CK(cudaFuncSetAttribute(k_tile_accum_src<T, CPLX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kb("assign_tile_accum", double(B.total) * sizeof(PRecS<T>) + double(g.ntot) * sizeof(T) * (CPLX ? 2 : 1));
-        k_tile_accum_src<T, CPLX><<<B.nchunks, 256, smem, st>>>(dp<PRecS<T>>(B.rec), dp<Chunk>(B.chunks), ag, fw, re, im,
-                                                                dp<double>(mass));
+        auto launch = [&](auto kern) {
+            HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            kern<<<B.nchunks, 256, smem, st>>>(dp<PRecS<T>>(B.rec), dp<Chunk>(B.chunks), ag, fw, re, im,
+                                               dp<double>(mass));
+        };
+        switch (ag.scheme) {
+            case HG_NGP: launch(k_tile_accum_src<T, CPLX, HG_NGP>); break;
+            case HG_CIC: launch(k_tile_accum_src<T, CPLX, HG_CIC>); break;
+            case HG_TSC: launch(k_tile_accum_src<T, CPLX, HG_TSC>); break;
+            default: launch(k_tile_accum_src<T, CPLX, HG_PCS>); break;
+        }
         ke();
         double hm[2];
         HG_CK(cudaMemcpyAsync(hm, mass.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));

@@ -202,11 +202,7 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
     double S;
     double k0;  // (f1 conj f2)(k = 0) from the FP64 field integrals
     double invV;
-    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
-        int ix = l;
-        const unsigned ui = (unsigned)i;
-        const int iy = (int)(ui / (unsigned)n2);
-        const int iz = (int)(ui - (unsigned)iy * (unsigned)n2);
+    __device__ __forceinline__ T value(int ix, int iy, int iz) const {
         double p2;
         if (ix == 0 && iy == 0 && iz == 0) {
             p2 = k0;
@@ -217,7 +213,40 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
         double C = xt.cf[0][ix] * xt.cf[1][iy] * xt.cf[2][iz];
         if (xt.interlace) C = 0.5 * (C + xt.df[0][ix] * xt.df[1][iy] * xt.df[2][iz]);
         double iw = xt.iw2[0][ix] * xt.iw2[1][iy] * xt.iw2[2][iz];
-        return mk<T>((T)(invV * ((p2 - S * C) * iw)), (T)0);
+        return (T)(invV * ((p2 - S * C) * iw));
+    }
+};
+
+// The real correlation-field spectrum P of the box, two kz columns per complex value:
+// out[ix][iy][j] = P(ix, iy, 2j) + i P(ix, iy, 2j + 1)  ([n0][n1][n2/2]).  A complex
+// transform along x of these lines gives both columns' transforms at once (LdSplitX).
+template <typename T, class LD>
+__global__ void k_synth_pairs(LD ld, int n0, int n1, int nh, cplx<T> *out) {
+    const long long total = (long long)n0 * n1 * nh;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, j;
+        split3((unsigned)idx, (unsigned)n1, (unsigned)nh, ix, iy, j);
+        out[idx] = mk<T>(ld.value(ix, iy, 2 * j), ld.value(ix, iy, 2 * j + 1));
+    }
+}
+
+// y-pass loader that separates the paired columns after the x pass.  With
+// Z(x) = A(x) + i B(x) the transform of a + i b for real a, b:
+// A(x) = (Z(x) + conj Z(-x)) / 2,  B(x) = (Z(x) - conj Z(-x)) / (2 i).  Only x = 0 .. n0/2
+// is kept (the transform of a real line satisfies A(-x) = conj A(x)).  Element
+// (o = x, l = ky, i = kz) of z ([n0][n1][nh] complex).
+template <typename T>
+struct LdSplitX {
+    const cplx<T> *z;
+    int n0, n1, nh;
+    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
+        const int x = (int)o, kz = (int)i, j = kz >> 1;
+        const int xm = (x == 0) ? 0 : n0 - x;
+        const cplx<T> zp = z[((long long)x * n1 + l) * nh + j];
+        const cplx<T> zm = z[((long long)xm * n1 + l) * nh + j];
+        if ((kz & 1) == 0) return mk<T>((T)0.5 * (zp.x + zm.x), (T)0.5 * (zp.y - zm.y));
+        return mk<T>((T)0.5 * (zp.y + zm.y), (T)0.5 * (zm.x - zp.x));
     }
 };
 
@@ -314,7 +343,7 @@ struct OrbitCfg {
 
 template <typename T, int L>
 __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
-    k_xi_orbit_hist(const cplx<T> *xi, const int *orbit_lines, const int *orbit_n2xy, int n_orbits,
+    k_xi_orbit_hist(const cplx<T> *xi, int n0, int n1, const int *orbit_lines, const int *orbit_n2xy, int n_orbits,
                     const cplx<T> *tw, HistSpec hs, long long n2dim, double *hist) {
     using OC = OrbitCfg<T, L>;
     constexpr int B = OC::B, LP = OC::LP, NT = OC::NT;
@@ -325,9 +354,25 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
     const int *lines = orbit_lines + 8 * orb;
     const int b = threadIdx.x / R2, t = threadIdx.x % R2;
     const int line = lines[b];
+    // xi holds x = 0 .. n0/2 ([n0/2 + 1][n1][L]); the line (-x, y) is the conjugate of (x, -y)
+    int src = line;
+    bool cj = false;
+    if (line >= 0) {
+        const int ix = line / n1, iy = line - ix * n1;
+        if (ix > n0 / 2) {
+            src = (n0 - ix) * n1 + (iy == 0 ? 0 : n1 - iy);
+            cj = true;
+        }
+    }
     cplx<T> v[R1];
 #pragma unroll
-    for (int n1 = 0; n1 < R1; n1++) v[n1] = (line >= 0) ? xi[(long long)line * L + R2 * n1 + t] : mk<T>(0, 0);
+    for (int n1_ = 0; n1_ < R1; n1_++) {
+        v[n1_] = mk<T>(0, 0);
+        if (line >= 0) {
+            const cplx<T> c = xi[(long long)src * L + R2 * n1_ + t];
+            v[n1_] = cj ? mk<T>(c.x, -c.y) : c;
+        }
+    }
     line_fft2<T, L, +1, false, B>(v, s, t, b, tw);
 #pragma unroll
     for (int r = 0; r < R1; r++) s[b * LP + pos_of_reg<L>(t, r)] = v[r];
