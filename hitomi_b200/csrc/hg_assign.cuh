@@ -600,14 +600,30 @@ __global__ void k_chunk_fill(const unsigned int *off, const unsigned int *choff,
     }
 }
 
-__device__ __forceinline__ long long tile_cell(const AssignGeom &g, int tile, int li, int &lx, int &ly, int &lz) {
+// Visit a tile's cells row by row: warp w takes rows w, w + nwarps, ...; a row is t2
+// consecutive cells of the mesh, so a warp's stores are contiguous.  f(li, cell) with li
+// the cell's index in the tile, (lx t1 + ly) t2 + lz.
+template <class F>
+__device__ __forceinline__ void for_tile_cells(const AssignGeom &g, int tile, F f) {
     const int tz = tile % g.nt[2];
     const int ty = (tile / g.nt[2]) % g.nt[1];
     const int tx = tile / (g.nt[2] * g.nt[1]);
-    lz = li % g.t[2];
-    ly = (li / g.t[2]) % g.t[1];
-    lx = li / (g.t[2] * g.t[1]);
-    return ((long long)(tx * g.t[0] + lx) * g.n[1] + (ty * g.t[1] + ly)) * g.n[2] + (tz * g.t[2] + lz);
+    const int nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+    const int rows = g.t[0] * g.t[1];
+    for (int r = threadIdx.x >> 5; r < rows; r += nw) {
+        const int lx = r / g.t[1], ly = r - lx * g.t[1];
+        const long long base =
+            ((long long)(tx * g.t[0] + lx) * g.n[1] + (ty * g.t[1] + ly)) * g.n[2] + tz * g.t[2];
+        for (int lz = lane; lz < g.t[2]; lz += 32) f(r * g.t[2] + lz, base + lz);
+    }
+}
+
+// Zero `words` 32-bit words of shared memory (16-byte stores for the bulk).
+__device__ __forceinline__ void zero_shared(void *p, int words) {
+    int4 *q = reinterpret_cast<int4 *>(p);
+    for (int c = threadIdx.x; c < (words >> 2); c += blockDim.x) q[c] = make_int4(0, 0, 0, 0);
+    int *w = reinterpret_cast<int *>(p);
+    for (int c = (words & ~3) + threadIdx.x; c < words; c += blockDim.x) w[c] = 0;
 }
 
 // Zero the cells of every split tile (run before the accumulation).
@@ -615,13 +631,10 @@ template <typename T, bool CPLX>
 __global__ void k_zero_split_tiles(const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
     Chunk k = ch[blockIdx.x];
     if (k.multi != 1) return;
-    const int tcells = g.t[0] * g.t[1] * g.t[2];
-    for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
-        int lx, ly, lz;
-        long long cell = tile_cell(g, k.tile, li, lx, ly, lz);
+    for_tile_cells(g, k.tile, [&](int, long long cell) {
         mesh_re[cell] = (T)0;
         if (CPLX) mesh_im[cell] = (T)0;
-    }
+    });
 }
 
 // Local tile coordinates of a separable stencil along axis a: bit j of the result is set
@@ -682,7 +695,7 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     T *acc_im = acc + tcells;
     int *acc_hi = reinterpret_cast<int *>(smem_raw);
     int *acc_lo = acc_hi + tcells;
-    for (int c = threadIdx.x; c < tcells * ((CPLX || FIX) ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
+    zero_shared(smem_raw, tcells * ((CPLX || FIX) ? 2 : 1) * (int)(sizeof(T) / 4));
     __syncthreads();
     const Chunk k = ch[blockIdx.x];
     const int tile = k.tile;
@@ -690,15 +703,14 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     const int ty = (tile / g.nt[2]) % g.nt[1];
     const int tx = tile / (g.nt[2] * g.nt[1]);
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
-    float fscale = 1.0f;
-    double dinv = 1.0;
+    float fscale = 1.0f, finv = 1.0f;
     if (FIX) {
         int e, e1;
         frexpf(float(k.r1 - k.r0) * g.fix_bound, &e);
         frexpf(g.fix_bound, &e1);
-        const int sc = min(50 - e, 42 - e1);
+        const int sc = min(50 - e, 42 - e1);  // the host keeps fix_bound >= 2^-60, so sc <= 102
         fscale = ldexpf(1.0f, sc);
-        dinv = ldexp(1.0, -sc);
+        finv = ldexpf(1.0f, -sc);
     }
     const T factor = (T)g.acc_factor;
     auto add = [&](int li, T v, T vi) {
@@ -762,10 +774,10 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
         }
     }
     __syncthreads();
-    for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
-        int lx, ly, lz;
-        long long cell = tile_cell(g, tile, li, lx, ly, lz);
-        const T v = FIX ? (T)((double)((long long)acc_hi[li] * 1048576LL + (long long)acc_lo[li]) * dinv) : acc[li];
+    // FIX: the exact integer sum rounded once to FP32, then scaled by a power of two (exact)
+    for_tile_cells(g, tile, [&](int li, long long cell) {
+        const T v = FIX ? (T)(__ll2float_rn((long long)acc_hi[li] * 1048576LL + (long long)acc_lo[li]) * finv)
+                        : acc[li];
         if (k.multi == 0) {
             mesh_re[cell] = v;
             if (CPLX) mesh_im[cell] = acc_im[li];
@@ -773,7 +785,7 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
             if (v != (T)0) atomicAdd(&mesh_re[cell], v);
             if (CPLX && acc_im[li] != (T)0) atomicAdd(&mesh_im[cell], acc_im[li]);
         }
-    }
+    });
 }
 
 // Weighting of a field: one PartSrc (weight recipe: w^wpow, Yhat_lm(los), scale) per source.
@@ -797,7 +809,7 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
     const int tcells = g.t[0] * g.t[1] * g.t[2];
     T *acc_im = acc + tcells;
     __shared__ double red[2][32];
-    for (int c = threadIdx.x; c < tcells * (CPLX ? 2 : 1); c += blockDim.x) acc[c] = (T)0;
+    zero_shared(smem_raw, tcells * (CPLX ? 2 : 1) * (int)(sizeof(T) / 4));
     __syncthreads();
     const Chunk k = ch[blockIdx.x];
     const int tile = k.tile;
@@ -882,9 +894,7 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
         if (sr != 0.0) atomicAdd(&mass[0], sr);
         if (si != 0.0) atomicAdd(&mass[1], si);
     }
-    for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
-        int lx, ly, lz;
-        long long cell = tile_cell(g, tile, li, lx, ly, lz);
+    for_tile_cells(g, tile, [&](int li, long long cell) {
         if (k.multi == 0) {
             mesh_re[cell] = acc[li];
             if (CPLX) mesh_im[cell] = acc_im[li];
@@ -892,7 +902,7 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
             if (acc[li] != (T)0) atomicAdd(&mesh_re[cell], acc[li]);
             if (CPLX && acc_im[li] != (T)0) atomicAdd(&mesh_im[cell], acc_im[li]);
         }
-    }
+    });
 }
 
 }  // namespace hg

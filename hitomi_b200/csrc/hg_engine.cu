@@ -225,9 +225,8 @@ struct Engine : public hg_ctx {
 
     // shot-noise state
     DBuf xi;
-    DBuf xi_half;  // box correlation field after x and y passes, x = 0 .. n0/2
     bool xi_valid = false;
-    std::vector<int> orbit_lines, orbit_n2xy;
+    std::vector<int> orbit_lines, orbit_n2xy;  // per orbit: 4 (line, mirror) pairs; n_x^2 + n_y^2
     DBuf d_orbit_lines, d_orbit_n2xy;
     long long n2dim = 0;
     std::map<int, std::unique_ptr<BesselSpline>> splines;
@@ -719,7 +718,7 @@ struct Engine : public hg_ctx {
             }
             for (int a = 0; a < 3; a++) fix = fix && ag.n[a] >= stencil_width(ag.scheme);
             agx.fix_bound = (float)(wmax * std::fabs(ag.acc_factor));
-            fix = fix && agx.fix_bound > 0.0f;
+            fix = fix && agx.fix_bound >= 0x1p-60f;
         }
         kb("assign_tile_accum", double(total) * sizeof(PRec<U>) + double(g.ntot) * sizeof(U) * (CPLX ? 2 : 1));
         switch (ag.scheme) {
@@ -1194,12 +1193,23 @@ struct Engine : public hg_ctx {
                     int ix = ((cand[q][0] % nx) + nx) % nx, iy = ((cand[q][1] % ny) + ny) % ny;
                     ls.insert(ix * ny + iy);
                 }
+                // representatives: one line of each mirror pair (x, y) <-> (-x, -y) (the set
+                // is closed under the mirror), with its mirror
                 int k = 0;
                 for (int l : ls) {
+                    const int ix = l / ny, iy = l % ny;
+                    const int m = ((nx - ix) % nx) * ny + (ny - iy) % ny;
+                    HG_REQUIRE(ls.count(m), "orbit not closed under the mirror");
+                    if (l > m) continue;
+                    HG_REQUIRE(k < 4, "more than four representative lines in an orbit");
                     orbit_lines.push_back(l);
+                    orbit_lines.push_back(m);
                     k++;
                 }
-                for (; k < 8; k++) orbit_lines.push_back(-1);
+                for (; k < 4; k++) {
+                    orbit_lines.push_back(-1);
+                    orbit_lines.push_back(-1);
+                }
                 orbit_n2xy.push_back(wx * wx + wy * wy);
             }
         HG_CK(d_orbit_lines.ensure(sizeof(int) * orbit_lines.size()));
@@ -1223,18 +1233,16 @@ struct Engine : public hg_ctx {
     }
 
     // Box correlation field after its x and y inverse passes (cached per catalogue).  Its
-    // spectrum P is real, so the x pass transforms two kz columns per complex line
-    // (k_synth_pairs: [n0][n1][n2/2] in xi), and the y pass separates them while keeping
-    // x = 0 .. n0/2 only (LdSplitX into xi_half: [n0/2 + 1][n1][n2]); the histogram
-    // kernel takes the line (-x, y) as the conjugate of (x, -y).
+    // spectrum P is real, so the even and odd kz planes travel as the real and imaginary
+    // parts of one complex field (k_synth_pairs: [n0][n1][n2/2] in xi): half the data
+    // through the x and y passes; the histogram kernel separates them before its z pass.
     void ensure_xi() {
         HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
                    "bispectrum / 3PCF shot noise needs equal cell sizes on all axes");
         build_orbits();
         if (xi_valid) return;
-        const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], nh = n2 / 2, hx = n0 / 2 + 1;
+        const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], nh = n2 / 2;
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
-        HG_CK(xi_half.ensure(sizeof(C) * (size_t)hx * n1 * n2));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
         const double S = double(slot[0].n);
         LdXiHat<T> ld{half_spec(), n2, xtabs, S, delta0 * N0, invV};
@@ -1244,8 +1252,7 @@ struct Engine : public hg_ctx {
         k_synth_pairs<T, LdXiHat<T>><<<blocks, 256, 0, st>>>(ld, n0, n1, nh, dp<C>(xi));
         ke();
         pass<+1>(n0, LdArr<T>{dp<C>(xi), n0, yz}, StArr<T>{dp<C>(xi), n0, yz}, 1, yz, "fft_xi_x");
-        pass<+1>(n1, LdSplitX<T>{dp<C>(xi), n0, n1, nh}, StArr<T>{dp<C>(xi_half), n1, n2}, hx, n2, "fft_xi_y",
-                 double(hx) * n1 * n2 * sizeof(C) * 2.0);
+        pass<+1>(n1, LdArr<T>{dp<C>(xi), n1, nh}, StArr<T>{dp<C>(xi), n1, nh}, n0, nh, "fft_xi_y");
         xi_valid = true;
     }
 
@@ -1254,11 +1261,9 @@ struct Engine : public hg_ctx {
         size_t smem = OrbitCfg<T, L>::smem();
         HG_CK(cudaFuncSetAttribute(k_xi_orbit_hist<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const C *twp = twiddles(L);
-        kb("xi_orbit_hist", double(g.n[0] / 2 + 1) * g.n[1] * g.n[2] * sizeof(C));
-        k_xi_orbit_hist<T, L><<<n_orb, OrbitCfg<T, L>::NT, smem, st>>>(dp<C>(xi_half), g.n[0], g.n[1],
-                                                                       dp<int>(d_orbit_lines),
-                                                                       dp<int>(d_orbit_n2xy), n_orb, twp, hs, n2dim,
-                                                                       hist);
+        kb("xi_orbit_hist", double(g.ntot / 2) * sizeof(C));
+        k_xi_orbit_hist<T, L><<<(n_orb + 1) / 2, OrbitCfg<T, L>::NT, smem, st>>>(
+            dp<C>(xi), dp<int2>(d_orbit_lines), dp<int>(d_orbit_n2xy), n_orb, twp, hs, n2dim, hist);
         ke();
     }
     void launch_orbit(int L, const HistSpec &hs, int n_orb, double *hist) {

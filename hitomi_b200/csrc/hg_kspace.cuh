@@ -219,7 +219,8 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
 
 // The real correlation-field spectrum P of the box, two kz columns per complex value:
 // out[ix][iy][j] = P(ix, iy, 2j) + i P(ix, iy, 2j + 1)  ([n0][n1][n2/2]).  A complex
-// transform along x of these lines gives both columns' transforms at once (LdSplitX).
+// transform of these lines along x and y gives both planes' transforms at once; the
+// histogram kernel separates them.
 template <typename T, class LD>
 __global__ void k_synth_pairs(LD ld, int n0, int n1, int nh, cplx<T> *out) {
     const long long total = (long long)n0 * n1 * nh;
@@ -231,24 +232,6 @@ __global__ void k_synth_pairs(LD ld, int n0, int n1, int nh, cplx<T> *out) {
     }
 }
 
-// y-pass loader that separates the paired columns after the x pass.  With
-// Z(x) = A(x) + i B(x) the transform of a + i b for real a, b:
-// A(x) = (Z(x) + conj Z(-x)) / 2,  B(x) = (Z(x) - conj Z(-x)) / (2 i).  Only x = 0 .. n0/2
-// is kept (the transform of a real line satisfies A(-x) = conj A(x)).  Element
-// (o = x, l = ky, i = kz) of z ([n0][n1][nh] complex).
-template <typename T>
-struct LdSplitX {
-    const cplx<T> *z;
-    int n0, n1, nh;
-    __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
-        const int x = (int)o, kz = (int)i, j = kz >> 1;
-        const int xm = (x == 0) ? 0 : n0 - x;
-        const cplx<T> zp = z[((long long)x * n1 + l) * nh + j];
-        const cplx<T> zm = z[((long long)xm * n1 + l) * nh + j];
-        if ((kz & 1) == 0) return mk<T>((T)0.5 * (zp.x + zm.x), (T)0.5 * (zp.y - zm.y));
-        return mk<T>((T)0.5 * (zp.y + zm.y), (T)0.5 * (zm.x - zp.x));
-    }
-};
 
 // Cross-spectrum version for the survey (field.hpp:1116-1160): (f1 conj f2 - S C(k)) / W^2 / V
 // with complex S, f1 = the Yhat_LM-weighted D - alpha R field, f2 = the w^2 D + alpha^2 R field.
@@ -343,58 +326,69 @@ struct OrbitCfg {
 
 template <typename T, int L>
 __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
-    k_xi_orbit_hist(const cplx<T> *xi, int n0, int n1, const int *orbit_lines, const int *orbit_n2xy, int n_orbits,
+    k_xi_orbit_hist(const cplx<T> *xi, const int2 *orbit_reps, const int *orbit_n2xy, int n_orbits,
                     const cplx<T> *tw, HistSpec hs, long long n2dim, double *hist) {
     using OC = OrbitCfg<T, L>;
     constexpr int B = OC::B, LP = OC::LP, NT = OC::NT;
     constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    static_assert(B == 8, "two orbits of four representative lines per CTA");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *s = reinterpret_cast<cplx<T> *>(smem_raw);
-    const int orb = blockIdx.x;
-    const int *lines = orbit_lines + 8 * orb;
     const int b = threadIdx.x / R2, t = threadIdx.x % R2;
-    const int line = lines[b];
-    // xi holds x = 0 .. n0/2 ([n0/2 + 1][n1][L]); the line (-x, y) is the conjugate of (x, -y)
-    int src = line;
-    bool cj = false;
-    if (line >= 0) {
-        const int ix = line / n1, iy = line - ix * n1;
-        if (ix > n0 / 2) {
-            src = (n0 - ix) * n1 + (iy == 0 ? 0 : n1 - iy);
-            cj = true;
-        }
-    }
+    const int orb_b = 2 * blockIdx.x + (b >> 2);
+    const int2 rep = (orb_b < n_orbits) ? orbit_reps[4 * orb_b + (b & 3)] : make_int2(-1, -1);
+    const int line = rep.x, mirror = rep.y;
+    // xi holds Z = A + i B ([n0][n1][L/2]) after the x and y passes, A and B the transforms
+    // of the even and odd kz planes of the real spectrum: A(x) = (Z(x) + conj Z(-x)) / 2,
+    // B(x) = (Z(x) - conj Z(-x)) / (2 i), with -x the mirror line (-x, -y)
+    constexpr int NH = L / 2;
     cplx<T> v[R1];
 #pragma unroll
     for (int n1_ = 0; n1_ < R1; n1_++) {
         v[n1_] = mk<T>(0, 0);
         if (line >= 0) {
-            const cplx<T> c = xi[(long long)src * L + R2 * n1_ + t];
-            v[n1_] = cj ? mk<T>(c.x, -c.y) : c;
+            const int kz = R2 * n1_ + t, j = kz >> 1;
+            const cplx<T> zp = xi[(long long)line * NH + j], zm = xi[(long long)mirror * NH + j];
+            v[n1_] = (kz & 1) ? mk<T>((T)0.5 * (zp.y + zm.y), (T)0.5 * (zm.x - zp.x))
+                              : mk<T>((T)0.5 * (zp.x + zm.x), (T)0.5 * (zp.y - zm.y));
         }
     }
     line_fft2<T, L, +1, false, B>(v, s, t, b, tw);
 #pragma unroll
     for (int r = 0; r < R1; r++) s[b * LP + pos_of_reg<L>(t, r)] = v[r];
     __syncthreads();
-    const int n2xy = orbit_n2xy[orb];
-    for (int iz = threadIdx.x; iz <= L / 2; iz += NT) {
-        int iz2 = (L - iz) % L;
+    // The mirror line carries conj xi(x, y, -z): with the pair folded over +-z, its even
+    // part is the conjugate of the representative's and its odd part minus the conjugate,
+    // so a representative with a distinct mirror adds 2 Re of its even part and 2i Im of its
+    // odd part; a line that is its own mirror adds both parts as they are.  The planes z = 0
+    // and z = L/2 (the reference's coordinate -L/2, field.hpp:1050) hold one cell per line,
+    // weighted by f(mu) with mu of that sign, for either parity.
+    for (int q = threadIdx.x; q < 2 * (L / 2 + 1); q += NT) {
+        const int o = q / (L / 2 + 1), iz = q - o * (L / 2 + 1);
+        const int orb = 2 * blockIdx.x + o;
+        if (orb >= n_orbits) continue;
+        const int iz2 = (L - iz) % L;
         double er = 0, ei = 0, orr = 0, oi = 0;
-        for (int bb = 0; bb < B; bb++) {
-            if (lines[bb] < 0) continue;
-            cplx<T> a = s[bb * LP + iz];
-            if (iz2 == iz) {
-                er += (double)a.x;
-                ei += (double)a.y;
-            } else {
-                cplx<T> c = s[bb * LP + iz2];
+        for (int bb = 4 * o; bb < 4 * o + 4; bb++) {
+            const int2 rb = orbit_reps[4 * orb + (bb & 3)];
+            if (rb.x < 0) continue;
+            const cplx<T> a = s[bb * LP + iz];
+            const cplx<T> c = (iz2 == iz) ? mk<T>(0, 0) : s[bb * LP + iz2];
+            if (rb.y == rb.x) {
                 er += (double)a.x + (double)c.x;
                 ei += (double)a.y + (double)c.y;
                 orr += (double)a.x - (double)c.x;
                 oi += (double)a.y - (double)c.y;
+            } else {
+                er += 2.0 * ((double)a.x + (double)c.x);
+                oi += 2.0 * ((double)a.y - (double)c.y);
             }
         }
+        if (iz2 == iz) {  // z = 0 or the Nyquist plane (z = -L/2): the cell counts once, either parity
+            orr = er;
+            oi = ei;
+        }
+        const int n2xy = orbit_n2xy[orb];
         int wz = wrap_index(iz, L);
         long long n2 = (long long)n2xy + (long long)wz * wz;
         const double r = sqrt((double)n2);

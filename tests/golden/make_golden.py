@@ -9,6 +9,7 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --zeta   (only box_zeta.npz)
     python tests/golden/make_golden.py --survey (only survey_pk.npz)
     python tests/golden/make_golden.py --survey3 (only survey_bk_zeta.npz)
+    python tests/golden/make_golden.py --odd (only box_odd.npz: odd l1 + l2)
     python tests/golden/make_golden.py --bk256 (only box_bk_256.npz, from the restatement)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
@@ -176,6 +177,25 @@ def make_extensions():
     np.savez_compressed(os.path.join(HERE, "box_extensions.npz"), **d)
 
 
+def make_odd():
+    """Multipoles with odd l1 + l2 (odd L): their shot-noise weights are odd in cos(theta),
+    which exercises the histogram's sign handling, the Nyquist plane z = -L/2 included."""
+    mps = ((1, 0, 1), (2, 1, 1))
+    pos = lognormal_box(12000, 1000.0, ngrid=32, seed=12, exact_n=12000)
+    bb = Binning(0.015, 0.075, 7, 4.0, 156.0, 20)
+    d = dict(pos=pos, boxsize=1000.0, binning=binning_arr(bb), n_mesh=32)
+    for mp, v in run_bk(pos, 32, 1000.0, bb, "TSC", mps=mps).items():
+        d["bk_TSC_" + "".join(map(str, mp))] = v
+    pz = lognormal_box(10000, 400.0, ngrid=32, seed=15, exact_n=10000)
+    bz = Binning(0.02, 0.1, 5, 20.0, 140.0, 7)
+    d["zeta_pos"] = pz
+    d["zeta_boxsize"] = 400.0
+    d["zeta_binning"] = binning_arr(bz)
+    for mp, v in run_zeta(pz, 32, 400.0, bz, "TSC", mps=mps).items():
+        d["zeta_TSC_" + "".join(map(str, mp))] = v
+    np.savez_compressed(os.path.join(HERE, "box_odd.npz"), **d)
+
+
 def main():
     if "--extensions" in sys.argv or "--bk256" in sys.argv:
         if "--extensions" in sys.argv:
@@ -186,9 +206,11 @@ def main():
         return
     if not ref_runner.available():
         raise SystemExit("build the oracle first: make -C oracle")
-    if "--zeta" in sys.argv or "--survey" in sys.argv or "--survey3" in sys.argv:
+    if "--zeta" in sys.argv or "--survey" in sys.argv or "--survey3" in sys.argv or "--odd" in sys.argv:
         if "--zeta" in sys.argv:
             make_zeta()
+        if "--odd" in sys.argv:
+            make_odd()
         if "--survey" in sys.argv:
             make_survey()
         if "--survey3" in sys.argv:

@@ -153,3 +153,16 @@ def test_bk_reduced_grid_192(form):
         bk, sn, norm = c.bk_box_multi(mps)
         for q, mp in enumerate(mps):
             assert relerr(norm * (bk[q] - sn[q]), d["bk_" + "".join(map(str, mp))], FLOOR[form]) < TOL[form], mp
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_bk_box_odd_multipoles(form):
+    """l1 + l2 odd: shot-noise weights odd in cos(theta), the Nyquist plane z = -L/2 included."""
+    d = load_golden("box_odd.npz")
+    b = binning_from(d["binning"])
+    with ctx(int(d["n_mesh"]), float(d["boxsize"]), b, "TSC", form) as c:
+        c.set_particles(0, d["pos"])
+        for mp in ((1, 0, 1), (2, 1, 1)):
+            bk, sn, norm = c.bk_box(*mp)
+            ref = d["bk_TSC_" + "".join(map(str, mp))]
+            assert relerr(norm * (bk - sn), ref, FLOOR[form]) < TOL[form], mp

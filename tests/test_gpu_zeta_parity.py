@@ -117,3 +117,16 @@ def test_zeta_rejects_noncubic_and_bad_rows():
             c.zeta_box(0, 0, 0, 7)
         with pytest.raises(HitomiError, match="not allowed"):
             c.zeta_box(1, 0, 0)
+
+
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_zeta_box_odd_multipoles(form):
+    """l1 + l2 odd: shot-noise weights odd in cos(theta), the Nyquist plane z = -L/2 included."""
+    d = load_golden("box_odd.npz")
+    b = binning_from(d["zeta_binning"])
+    with ctx(int(d["n_mesh"]), float(d["zeta_boxsize"]), b, "TSC", form) as c:
+        c.set_particles(0, d["zeta_pos"])
+        for mp in ((1, 0, 1), (2, 1, 1)):
+            z, sn, norm = c.zeta_box(*mp)
+            ref = d["zeta_TSC_" + "".join(map(str, mp))]
+            assert relerr(file_value(z, sn, norm), ref, FLOOR[form]) < TOL[form], mp
