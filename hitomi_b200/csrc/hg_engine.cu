@@ -198,6 +198,8 @@ struct Engine : public hg_ctx {
         int gs[3] = {0, 0, 0};      // G cube half extent (2s, or n/2 when the axis is not reduced)
         int KG[3] = {0, 0, 0};
         DBuf d_ent, d_start, d_scale;
+        int nitems = 0;            // pair-sum work items (k_pair_dot_items)
+        DBuf d_items, d_istart;
     } shells;
     // The catalogue the bispectrum and 3PCF read: the box density (kind 0) or the survey's
     // D - alpha R field (kind 1).  G fields are keyed by GK = (L, M): the Yhat_LM-weighted
@@ -220,6 +222,7 @@ struct Engine : public hg_ctx {
     std::map<GK, std::unique_ptr<DBuf>> Gm;    // G on the reduced grid per G key
     std::set<GK> Gm_ok;
     DBuf Gc, Ac, T1, T2, pair_out;
+    DBuf pair_part;  // per work item partial pair sums
     bool shD_valid = false;
     std::map<std::tuple<int, int, int, int, int, int>, std::vector<double>> pairs;  // (a, b, L, M)
 
@@ -986,6 +989,22 @@ struct Engine : public hg_ctx {
             HG_CK(cudaMemcpy(S.d_ent.p, S.ent.data(), sizeof(ShellEnt) * S.ent.size(), cudaMemcpyHostToDevice));
         HG_CK(S.d_start.ensure(sizeof(int) * (S.ns + 1)));
         HG_CK(cudaMemcpy(S.d_start.p, S.start.data(), sizeof(int) * (S.ns + 1), cudaMemcpyHostToDevice));
+        {  // pair-sum work items: each shell cut into runs of at most 32 PD_LANE entries
+            std::vector<PairItem> items;
+            std::vector<int> istart(S.ns + 1, 0);
+            for (int i = 0; i < S.ns; i++) {
+                istart[i] = (int)items.size();
+                for (int e = S.start[i]; e < S.start[i + 1]; e += 32 * PD_LANE)
+                    items.push_back(PairItem{i, e, std::min(S.start[i + 1], e + 32 * PD_LANE)});
+            }
+            istart[S.ns] = (int)items.size();
+            S.nitems = (int)items.size();
+            HG_CK(S.d_items.ensure(sizeof(PairItem) * std::max(1, S.nitems)));
+            if (S.nitems)
+                HG_CK(cudaMemcpy(S.d_items.p, items.data(), sizeof(PairItem) * S.nitems, cudaMemcpyHostToDevice));
+            HG_CK(S.d_istart.ensure(sizeof(int) * (S.ns + 1)));
+            HG_CK(cudaMemcpy(S.d_istart.p, istart.data(), sizeof(int) * (S.ns + 1), cudaMemcpyHostToDevice));
+        }
         std::vector<double> inv(S.ns);
         for (int i = 0; i < S.ns; i++) inv[i] = S.nmode[i] ? 1.0 / double(S.nmode[i]) : 0.0;
         HG_CK(S.d_scale.ensure(sizeof(double) * S.ns));
@@ -1138,11 +1157,14 @@ struct Engine : public hg_ctx {
         const double2 *A = family_A(a);
         const C *Q = family_Q(b, gk);
         HG_CK(pair_out.ensure(sizeof(double2) * S.ns * S.ns));
-        dim3 gr(S.ns, S.ns);
-        kb("pair_dot", double(n_ent()) * (S.ns + 1) * 16.0);
-        k_pair_dot_cube<T><<<gr, 256, 0, st>>>(dp<int>(shells.d_start), dp<ShellEnt>(shells.d_ent), A, Q,
-                                               make_int3(S.K[0], S.K[1], S.K[2]), make_int3(S.M[0], S.M[1], S.M[2]),
-                                               make_int3(S.s[0], S.s[1], S.s[2]), S.ns, dp<double2>(pair_out));
+        HG_CK(pair_part.ensure(sizeof(double2) * (size_t)std::max(1, S.nitems) * S.ns));
+        kb("pair_dot", double(n_ent()) * (S.ns * sizeof(C) + 32.0));
+        if (S.nitems)
+            k_pair_dot_items<T><<<(unsigned)((S.nitems + 7) / 8), 256, 0, st>>>(
+                dp<PairItem>(S.d_items), S.nitems, dp<ShellEnt>(shells.d_ent), A, Q, make_int3(S.K[0], S.K[1], S.K[2]),
+                make_int3(S.M[0], S.M[1], S.M[2]), make_int3(S.s[0], S.s[1], S.s[2]), S.ns, dp<double2>(pair_part));
+        k_pair_sum_items<<<grid1((long long)S.ns * S.ns, 128), 128, 0, st>>>(dp<int>(S.d_istart), dp<double2>(pair_part),
+                                                                           S.ns, S.ns, dp<double2>(pair_out));
         ke();
         std::vector<double> h(2 * S.ns * S.ns);
         HG_CK(cudaMemcpyAsync(h.data(), pair_out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));

@@ -5,7 +5,7 @@
 //   k_shell_D       delta(k)/W(k) for every (shell, mode) entry      (field.hpp:346-401)
 //   k_family_A      A_f,i(k) = Yhat_f(k) delta/W / n_i
 //   k_scatter_*     place k-space inputs on the compact shell / G cubes
-//   k_pair_dot_cube sum over a shell of A_a(k) Qhat_b(-k)
+//   k_pair_dot_items sum over a shell of A_a(k) Qhat_b(-k)
 //   k_xi_orbit_hist last inverse-FFT pass of the shot-noise correlation field fused with
 //                   its radial histogram over integer n^2 = |x/dr|^2
 //   k_bessel_table, k_sn_matrix   spline-evaluated j_l products summed over n^2
@@ -149,45 +149,66 @@ __device__ __forceinline__ int neg_c(int n, int M, int s) {
     return m + s;
 }
 
-// out[i][j] = sum_{e in shell i} A[e] * Q[j](-n_e), Q the compact cubes of a chain family;
-// one block per (i, j); deterministic.
+// out[i][j] = sum_{e in shell i} A[e] * Q[j](-n_e), Q the compact cubes of a chain family.
+// The sums are cut into work items: a warp takes up to 32 PD_LANE entries of one shell and
+// gathers Q[j](-n_e) for every j (groups of PD_JG accumulators), so each lane keeps PD_JG
+// independent loads in flight instead of one; warp sums go to part[item][j], and
+// k_pair_sum_items adds a shell's items in a fixed order (deterministic).
+#define PD_LANE 4
+#define PD_JG 8
+struct PairItem {
+    int i, e0, e1;
+};
 template <typename T>
-__global__ void k_pair_dot_cube(const int *start, const ShellEnt *ent, const double2 *A, const cplx<T> *Q, int3 K,
-                                int3 M, int3 s, int ns_j, double2 *out) {
-    int i = blockIdx.x, j = blockIdx.y;
-    __shared__ double red[2][32];
+__global__ void k_pair_dot_items(const PairItem *items, int nitems, const ShellEnt *ent, const double2 *A,
+                                 const cplx<T> *Q, int3 K, int3 M, int3 s, int ns_j, double2 *part) {
+    const int wid = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (wid >= nitems) return;  // whole warps
+    const PairItem it = items[wid];
     const long long vol = (long long)K.x * K.y * K.z;
-    const cplx<T> *Qj = Q + (long long)j * vol;
-    double sr = 0.0, si = 0.0;
-    for (int e = start[i] + threadIdx.x; e < start[i + 1]; e += blockDim.x) {
-        ShellEnt q = ent[e];
-        long long idx = ((long long)neg_c(q.nx, M.x, s.x) * K.y + neg_c(q.ny, M.y, s.y)) * K.z + neg_c(q.nz, M.z, s.z);
-        cplx<T> v = Qj[idx];
-        double2 a = A[e];
-        double qx = (double)v.x, qy = (double)v.y;
-        sr += a.x * qx - a.y * qy;
-        si += a.x * qy + a.y * qx;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-        sr += __shfl_down_sync(0xffffffffu, sr, o);
-        si += __shfl_down_sync(0xffffffffu, si, o);
-    }
-    int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    if (ln == 0) {
-        red[0][w] = sr;
-        red[1][w] = si;
-    }
-    __syncthreads();
-    if (w == 0) {
-        int nw = blockDim.x >> 5;
-        sr = (ln < nw) ? red[0][ln] : 0.0;
-        si = (ln < nw) ? red[1][ln] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) {
-            sr += __shfl_down_sync(0xffffffffu, sr, o);
-            si += __shfl_down_sync(0xffffffffu, si, o);
+    for (int j0 = 0; j0 < ns_j; j0 += PD_JG) {
+        double ar[PD_JG], ai[PD_JG];
+#pragma unroll
+        for (int q = 0; q < PD_JG; q++) ar[q] = ai[q] = 0.0;
+        for (int e = it.e0 + lane; e < it.e1; e += 32) {
+            const ShellEnt q = ent[e];
+            const long long idx =
+                ((long long)neg_c(q.nx, M.x, s.x) * K.y + neg_c(q.ny, M.y, s.y)) * K.z + neg_c(q.nz, M.z, s.z);
+            const double2 a = A[e];
+            cplx<T> v[PD_JG];
+#pragma unroll
+            for (int jj = 0; jj < PD_JG; jj++) v[jj] = (j0 + jj < ns_j) ? Q[(long long)(j0 + jj) * vol + idx] : mk<T>(0, 0);
+#pragma unroll
+            for (int jj = 0; jj < PD_JG; jj++) {
+                const double qx = (double)v[jj].x, qy = (double)v[jj].y;
+                ar[jj] += a.x * qx - a.y * qy;
+                ai[jj] += a.x * qy + a.y * qx;
+            }
         }
-        if (ln == 0) out[(long long)i * ns_j + j] = make_double2(sr, si);
+#pragma unroll
+        for (int jj = 0; jj < PD_JG; jj++) {
+            double r = ar[jj], im = ai[jj];
+            for (int o = 16; o > 0; o >>= 1) {
+                r += __shfl_xor_sync(0xffffffffu, r, o);
+                im += __shfl_xor_sync(0xffffffffu, im, o);
+            }
+            if (lane == 0 && j0 + jj < ns_j) part[(long long)wid * ns_j + j0 + jj] = make_double2(r, im);
+        }
     }
+}
+
+// out[i][j] = sum over shell i's items (contiguous from istart[i]) of part[item][j]
+__global__ void k_pair_sum_items(const int *istart, const double2 *part, int ns_i, int ns_j, double2 *out) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ns_i * ns_j) return;
+    const int i = q / ns_j, j = q - i * ns_j;
+    double r = 0.0, im = 0.0;
+    for (int it = istart[i]; it < istart[i + 1]; it++) {
+        const double2 v = part[(long long)it * ns_j + j];
+        r += v.x;
+        im += v.y;
+    }
+    out[q] = make_double2(r, im);
 }
 
 // ---------------------------------------------------------------- shot-noise field
