@@ -1535,7 +1535,7 @@ struct Engine : public hg_ctx {
                                                                 nb, hq, n2dim, dp<double>(sn_part));
                 ke();
                 kb("sn_matrix", double(nblk) * na * nb * 16.0);
-                k_sum_parts<<<grid1((long long)na * nb, 128), 128, 0, st>>>(dp<double>(sn_part), nblk, na * nb,
+                k_sum_parts<<<grid1(sum_parts_threads((long long)na * nb), 256), 256, 0, st>>>(dp<double>(sn_part), nblk, na * nb,
                                                                               dp<double2>(snblk));
                 ke();
                 // place the (a0, b0) block into the ns x ns matrix
@@ -1792,7 +1792,7 @@ struct Engine : public hg_ctx {
         k_zeta_pairsum<T><<<nblk, HG_ZR_THREADS, smem, st>>>(Fa, na, Fb, nb, G, g.ntot, dp<double>(zpart));
         ke();
         kb("zeta_pairsum", double(nblk) * na * nb * 16.0);
-        k_sum_parts<<<grid1((long long)na * nb, 128), 128, 0, st>>>(dp<double>(zpart), nblk, na * nb,
+        k_sum_parts<<<grid1(sum_parts_threads((long long)na * nb), 256), 256, 0, st>>>(dp<double>(zpart), nblk, na * nb,
                                                                       dp<double2>(zout));
         ke();
         std::vector<double> h(2 * (size_t)na * nb);

@@ -749,17 +749,27 @@ inline size_t zeta_pairsum_smem(int na, int nb) {
     return stage > red ? stage : red;
 }
 
-// out[o] = sum_b part[b][o] in block order (deterministic), complex.
+// out[o] = sum_b part[b][o], complex: one warp per output, lane l adds b = l, l + 32, ...
+// in order, then a fixed shuffle tree (deterministic; the block partials' loads overlap).
 __global__ void k_sum_parts(const double *part, int nblk, int nout, double2 *out) {
-    int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= nout) return;
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= nout) return;  // whole warps
+    const int o = (int)w;
     double re = 0.0, im = 0.0;
-    for (int b = 0; b < nblk; b++) {
-        re += part[2 * ((long long)b * nout + o)];
-        im += part[2 * ((long long)b * nout + o) + 1];
+    for (int b = lane; b < nblk; b += 32) {
+        const double2 v = reinterpret_cast<const double2 *>(part)[(long long)b * nout + o];
+        re += v.x;
+        im += v.y;
     }
-    out[o] = make_double2(re, im);
+    for (int d = 16; d > 0; d >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, d);
+        im += __shfl_xor_sync(0xffffffffu, im, d);
+    }
+    if (lane == 0) out[o] = make_double2(re, im);
 }
+// threads for k_sum_parts over nout outputs
+inline long long sum_parts_threads(long long nout) { return nout * 32; }
 
 // Functors used by the transform passes.
 template <typename T>
