@@ -524,6 +524,7 @@ struct Engine : public hg_ctx {
 
     // statistics state derived from the current source (the catalogue itself is unchanged)
     void invalidate_stats() {
+        sn_xi_cache.clear();
         Gm_ok.clear();
         shD_valid = false;
         xi_valid = false;
@@ -562,6 +563,7 @@ struct Engine : public hg_ctx {
         src_kind = -1;
         dens_valid = false;
         pk_cache.clear();
+        sn_xi_cache.clear();
         Gm_ok.clear();
         shD_valid = false;
         xi_valid = false;
@@ -1516,6 +1518,28 @@ struct Engine : public hg_ctx {
     // SN += i^(l1+l2) dV sum_n2 J_l1(k1 r) J_l2(k2 r) hist(n2)  (bispec.hpp:1036-1060): the
     // skinny product J1 diag(hist) J2^T in row blocks, [ns][ns] complex
     void bk_sn_xi(const MP &mp, const double *hq, std::vector<double> &SNq) {
+        // (l2, l1, L) has the same shot-noise weights as (l1, l2, L) (the 3j symbols change by
+        // (-1)^(l1 + l2 + L) = 1), hence the same histogram, and its matrix is the transpose
+        const int ns = cfg.n_kbin;
+        auto sw = sn_xi_cache.find({mp.l2, mp.l1, mp.L});
+        if (src_kind == 0 && mp.l1 != mp.l2 && sw != sn_xi_cache.end() && sw->second.first == src_kind) {
+            const std::vector<double> &Tr = sw->second.second;
+            for (int i1 = 0; i1 < ns; i1++)
+                for (int i2 = 0; i2 < ns; i2++) {
+                    SNq[2 * (i1 * ns + i2)] += Tr[2 * (i2 * ns + i1)];
+                    SNq[2 * (i1 * ns + i2) + 1] += Tr[2 * (i2 * ns + i1) + 1];
+                }
+            return;
+        }
+        std::vector<double> add(2 * ns * ns, 0.0);
+        bk_sn_xi_compute(mp, hq, add);
+        for (size_t e = 0; e < add.size(); e++) SNq[e] += add[e];
+        sn_xi_cache[{mp.l1, mp.l2, mp.L}] = {src_kind, std::move(add)};
+    }
+    // xi-term matrices of this catalogue by (l1, l2, L), with the source kind they came from
+    std::map<std::array<int, 3>, std::pair<int, std::vector<double>>> sn_xi_cache;
+
+    void bk_sn_xi_compute(const MP &mp, const double *hq, std::vector<double> &SNq) {
         const int ns = cfg.n_kbin;
         const double dV = g.volume / double(g.ntot);
         HG_CK(snmat.ensure(sizeof(double2) * ns * ns));
