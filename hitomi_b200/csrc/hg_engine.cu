@@ -1165,7 +1165,7 @@ struct Engine : public hg_ctx {
             k_pair_dot_items<T><<<(unsigned)((S.nitems + 7) / 8), 256, 0, st>>>(
                 dp<PairItem>(S.d_items), S.nitems, dp<ShellEnt>(shells.d_ent), A, Q, make_int3(S.K[0], S.K[1], S.K[2]),
                 make_int3(S.M[0], S.M[1], S.M[2]), make_int3(S.s[0], S.s[1], S.s[2]), S.ns, dp<double2>(pair_part));
-        k_pair_sum_items<<<grid1((long long)S.ns * S.ns, 128), 128, 0, st>>>(dp<int>(S.d_istart), dp<double2>(pair_part),
+        k_pair_sum_items<<<grid1(32LL * S.ns * S.ns, 256), 256, 0, st>>>(dp<int>(S.d_istart), dp<double2>(pair_part),
                                                                            S.ns, S.ns, dp<double2>(pair_out));
         ke();
         std::vector<double> h(2 * S.ns * S.ns);

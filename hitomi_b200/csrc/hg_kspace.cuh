@@ -197,18 +197,24 @@ __global__ void k_pair_dot_items(const PairItem *items, int nitems, const ShellE
     }
 }
 
-// out[i][j] = sum over shell i's items (contiguous from istart[i]) of part[item][j]
+// out[i][j] = sum over shell i's items (contiguous from istart[i]) of part[item][j]: one
+// warp per output, lane l adds items l, l + 32, ... in order, then a fixed shuffle tree
 __global__ void k_pair_sum_items(const int *istart, const double2 *part, int ns_i, int ns_j, double2 *out) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= ns_i * ns_j) return;
-    const int i = q / ns_j, j = q - i * ns_j;
+    const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (long long)ns_i * ns_j) return;  // whole warps
+    const int q = (int)w, i = q / ns_j, j = q - i * ns_j;
     double r = 0.0, im = 0.0;
-    for (int it = istart[i]; it < istart[i + 1]; it++) {
+    for (int it = istart[i] + lane; it < istart[i + 1]; it += 32) {
         const double2 v = part[(long long)it * ns_j + j];
         r += v.x;
         im += v.y;
     }
-    out[q] = make_double2(r, im);
+    for (int d = 16; d > 0; d >>= 1) {
+        r += __shfl_xor_sync(0xffffffffu, r, d);
+        im += __shfl_xor_sync(0xffffffffu, im, d);
+    }
+    if (lane == 0) out[q] = make_double2(r, im);
 }
 
 // ---------------------------------------------------------------- shot-noise field

@@ -85,6 +85,9 @@ def measure_units(pos: np.ndarray, n_mesh: int, boxsize: float, binning, ops=UNI
         param = os.path.join(d, "param.ini")
         ref_runner.write_param(param, os.path.join(d, "out"), "bk", 0, 0, 0, n_mesh, boxsize, binning.kmin,
                                binning.kmax, binning.n_kbin, binning.rmin, binning.rmax, binning.n_rbin, "TSC")
+        # the concurrent processes share one output directory: made here, since each would
+        # otherwise race to create it (parameter.hpp:256-275 fails when mkdir loses)
+        os.makedirs(os.path.join(d, "out"), exist_ok=True)
         dpath = os.path.join(d, "data.f64")
         np.ascontiguousarray(pos, dtype=np.float64).tofile(dpath)
 
