@@ -315,8 +315,105 @@ inline size_t fft2_smem() {
     return (size_t)XchgLayout<L, COLS, CF::B>::ELEMS * sizeof(cplx<T>);
 }
 
+// Strided passes over plain arrays (LdArr), software-pipelined: a persistent CTA walks its
+// tiles (L rows x PB columns) and, while it transforms one tile, the next one streams into the
+// other half of a double buffer with cp.async (no registers held, no wait until the data is
+// needed).  The tile's buffer then serves as the transform's exchange buffer.  Without this
+// the pass is latency-bound: a CTA's loads are all issued at its start and nothing is in
+// flight while it computes and stores.
+template <typename T, int L>
+struct PipeCfg {
+    static constexpr int R2 = Split<L>::R2;
+    static constexpr int B = (L >= 256) ? 8 : 16;  // columns per tile
+    static constexpr int NT = R2 * B;
+    static constexpr size_t smem() { return 2 * (size_t)L * B * sizeof(cplx<T>); }
+};
+
+__device__ __forceinline__ void cp_async_elem(void *sdst, const void *gsrc, int bytes, bool ok) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(ok ? 8 : 0));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(ok ? 16 : 0));
+}
+
+template <typename T, int L, int DIR, class ST>
+__global__ void __launch_bounds__(PipeCfg<T, L>::NT)
+    k_fft2_pass_pipe(const cplx<T> *src, ST st, PassGeom g, const cplx<T> *__restrict__ tw) {
+    using PC = PipeCfg<T, L>;
+    using X = XchgLayout<L, true, PC::B>;
+    constexpr int R1 = X::R1, R2 = X::R2, B = PC::B, NT = PC::NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);  // [2][L][B]
+    const int t = threadIdx.x / B, b = threadIdx.x % B;
+    const long long tpo = (g.n_inner + B - 1) / B;
+    const long long ntiles = g.n_outer * tpo;
+    // element e of a tile (row e / B, column e % B), NT at a time
+    auto prefetch = [&](long long tile, cplx<T> *dst) {
+        const long long o = tile / tpo, i0 = (tile - o * tpo) * B;
+#pragma unroll 4
+        for (int e = threadIdx.x; e < L * B; e += NT) {
+            const int l = e / B, c = e - l * B;
+            const bool ok = (i0 + c) < g.n_inner;
+            const long long off = (o * L + l) * g.n_inner + (ok ? i0 + c : 0);
+            cp_async_elem(dst + e, src + off, (int)sizeof(cplx<T>), ok);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    int cur = 0;
+    long long tile = blockIdx.x;
+    if (tile < ntiles) prefetch(tile, buf);
+    for (; tile < ntiles; tile += gridDim.x) {
+        const long long next = tile + gridDim.x;
+        if (next < ntiles) prefetch(next, buf + (size_t)(cur ^ 1) * L * B);
+        else asm volatile("cp.async.commit_group;\n" ::);  // keep one group per iteration
+        asm volatile("cp.async.wait_group 1;\n" ::);
+        __syncthreads();
+        cplx<T> *S = buf + (size_t)cur * L * B;
+        cplx<T> v[R1];
+#pragma unroll
+        for (int n1 = 0; n1 < R1; n1++) v[n1] = S[(R2 * n1 + t) * B + b];
+        __syncthreads();  // every value is in registers: S becomes the exchange buffer
+        line_fft2<T, L, DIR, true, B>(v, S, t, b, tw);
+        const long long o = tile / tpo, i = (tile - o * tpo) * B + b;
+        if (i < g.n_inner) {
+#pragma unroll
+            for (int r = 0; r < R1; r++) st(o, pos_of_reg<L>(t, r), i, v[r]);
+        }
+        __syncthreads();  // S is the target of the prefetch two tiles on
+        cur ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+template <typename T, int L, int DIR, class ST>
+inline cudaError_t launch_fft2_pipe(const cplx<T> *src, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
+    using PC = PipeCfg<T, L>;
+    auto kern = k_fft2_pass_pipe<T, L, DIR, ST>;
+    const size_t smem = PC::smem();
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PC::NT, smem);
+    if (e != cudaSuccess) return e;
+    const long long ntiles = g.n_outer * ((g.n_inner + PC::B - 1) / PC::B);
+    const long long grid = std::min<long long>(ntiles, 148LL * std::max(per_sm, 1));
+    if (grid <= 0) return cudaSuccess;
+    kern<<<(unsigned)grid, PC::NT, smem, stream>>>(src, st, g, tw);
+    return cudaGetLastError();
+}
+
+template <class LD>
+struct IsLdArr : std::false_type {};
+template <typename U>
+struct IsLdArr<LdArr<U>> : std::true_type {};
+
 template <typename T, int L, int DIR, class LD, class ST>
 inline cudaError_t launch_fft2_L(LD ld, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
+    if constexpr (IsLdArr<LD>::value) {
+        // plain strided source: the pipelined pass (LdArr's inner stride is the pass's own)
+        if (g.n_inner > 1 && ld.inner == g.n_inner && ld.L == L) return launch_fft2_pipe<T, L, DIR>(ld.p, st, g, tw, stream);
+    }
     if (g.n_inner == 1) {
         using CF = Fft2Cfg<T, L, false>;
         size_t smem = fft2_smem<T, L, false>();
