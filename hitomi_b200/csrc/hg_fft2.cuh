@@ -458,8 +458,9 @@ struct ChainCfg {
     static constexpr int R2 = Split<L>::R2;
     static constexpr int B = 16;
     static constexpr int NT = R2 * B;
+    // exchange buffer, G tile, and the next shell's input rows (streamed in by cp.async)
     static constexpr size_t smem() {
-        return sizeof(cplx<T>) * ((size_t)XchgLayout<L, true, B>::ELEMS + (size_t)L * B);
+        return sizeof(cplx<T>) * ((size_t)XchgLayout<L, true, B>::ELEMS + 2 * (size_t)L * B);
     }
 };
 
@@ -477,6 +478,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L>::NT, (sizeof(T) == 4) ? 2 : 1)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
     cplx<T> *Gs = S + X::ELEMS;  // [x][b]
+    cplx<T> *Pb = Gs + L * B;    // next shell's input, [x][b]; rows outside |n| <= s stay zero
     const int t = threadIdx.x / B, b = threadIdx.x % B;
     const long long i = (long long)blockIdx.x * B + b;
     const bool ok = i < plane;
@@ -484,18 +486,31 @@ __global__ void __launch_bounds__(ChainCfg<T, L>::NT, (sizeof(T) == 4) ? 2 : 1)
         const int x = e / B, bb = e % B;
         const long long ii = (long long)blockIdx.x * B + bb;
         Gs[e] = (ii < plane) ? G[(long long)x * plane + ii] : mk<T>(0, 0);
+        Pb[e] = mk<T>(0, 0);
     }
-    // (the first exchange inside line_fft2 synchronises before Gs is read)
+    __syncthreads();
+    // the K kept rows of shell j into Pb (position x = n mod L of row c = n + s)
+    auto prefetch = [&](int j) {
+        const cplx<T> *tj = t2 + (long long)j * K * plane;
+        for (int e = threadIdx.x; e < K * B; e += CF::NT) {
+            const int c = e / B, bb = e - c * B;
+            const int n = c - s, x = (n < 0) ? n + L : n;
+            const long long ii = (long long)blockIdx.x * B + bb;
+            const bool in = ii < plane;
+            cp_async_elem(Pb + x * B + bb, tj + (long long)c * plane + (in ? ii : 0), (int)sizeof(cplx<T>), in);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    if (ns > 0) prefetch(0);
     for (int j = 0; j < ns; j++) {
         cplx<T> *tj = t2 + (long long)j * K * plane;
+        asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncthreads();
         cplx<T> v[R1];
 #pragma unroll
-        for (int n1 = 0; n1 < R1; n1++) {
-            const int p = R2 * n1 + t;
-            const int n = (p < L / 2) ? p : p - L;
-            const int c = n + s;
-            v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)c * plane + i] : mk<T>(0, 0);
-        }
+        for (int n1 = 0; n1 < R1; n1++) v[n1] = Pb[(R2 * n1 + t) * B + b];
+        __syncthreads();  // Pb is read: the next shell streams in while this one is transformed
+        if (j + 1 < ns) prefetch(j + 1);
         line_fft2<T, L, +1, true, B>(v, S, t, b, tw);
         if constexpr (R1 == R2) {
 #pragma unroll
