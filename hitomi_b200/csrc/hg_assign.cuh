@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(256, 3) k_bin_count(PartSrc src, AssignGeom g,
 // (cursor_back), so the records of stencils that straddle a mesh edge sit together at the
 // end of their tile's range and the accumulation's warps take one path or the other.
 template <class MK>
-__global__ void k_bin_scatter(PartSrc src, AssignGeom g, MK mk, Defer df, const unsigned int *off,
+__global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom g, MK mk, Defer df, const unsigned int *off,
                               unsigned int *cursor, unsigned int *cursor_back, typename MK::R *rec) {
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
