@@ -60,3 +60,44 @@ def covariance_measure(ctx, catalogue: Callable[[int], "object"], pk_ells=(0, 2,
                 out["zeta" + "".join(map(str, mp))] = norm * (z[q] - sn[q]).real
         return out
     return measure
+
+
+def run_pipelined(indices: Sequence[int], contexts: Sequence[object],
+                  measure_on: Callable[[object, int], dict]) -> Dict[int, dict]:
+    """Measure mocks on one GPU with several contexts, one host thread each: context c takes
+    mocks c, c + n, c + 2n, ... of `indices`.  Each context has its own CUDA stream and the
+    C ABI calls release the GIL, so one context's upload of its next catalogue
+    (hg_set_particles from pinned host memory) runs while another context computes; with
+    two contexts the host-to-device copy leaves the critical path once the compute per mock
+    is the longer of the two.  `measure_on(ctx, i)` does the whole mock (upload, statistics,
+    read-back) and returns its results.  Results are keyed by mock index; the first
+    exception of any thread is raised after all threads have stopped."""
+    import threading
+
+    out: Dict[int, dict] = {}
+    errors: List[BaseException] = []
+    lock = threading.Lock()
+    n = len(contexts)
+    if n < 1:
+        raise ValueError("need at least one context")
+
+    def worker(c: int) -> None:
+        try:
+            for k in range(c, len(indices), n):
+                if errors:
+                    return
+                r = measure_on(contexts[c], indices[k])
+                with lock:
+                    out[indices[k]] = r
+        except BaseException as e:  # noqa: BLE001 - re-raised in the caller's thread
+            with lock:
+                errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(c,), daemon=True) for c in range(n)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return out

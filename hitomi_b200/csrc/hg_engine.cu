@@ -2534,6 +2534,7 @@ int hg_create(hg_ctx **out, const hg_config *cfg) {
 
 int hg_destroy(hg_ctx *ctx) {
     if (!ctx) return -1;
+    cudaSetDevice(ctx->cfg.device);  // the buffers are freed on the context's GPU
     delete ctx;
     return 0;
 }
@@ -2543,10 +2544,13 @@ const char *hg_last_error(const hg_ctx *ctx) {
     return ctx->err.c_str();
 }
 
+// Every entry point first makes the context's GPU current on the calling host thread, so
+// that contexts can be driven from several threads (one per context).
 #define HG_GUARD(ctx, body)                 \
     do {                                    \
         if (!(ctx)) return -1;              \
         try {                               \
+            HG_CK(cudaSetDevice((ctx)->cfg.device)); \
             body;                           \
             (ctx)->err.clear();             \
             return 0;                       \

@@ -74,3 +74,32 @@ def test_gather_over_two_gloo_ranks():
     assert sorted(own0 + own1) == list(range(len(sizes))) and not set(own0) & set(own1)
     assert all0 == all1 == {i: 2.0 * i for i in range(len(sizes))}
     assert mx0 == mx1 == max(len(own0), len(own1))
+
+
+def test_run_pipelined_covers_every_mock_once_per_context():
+    from hitomi_b200.batch import run_pipelined
+
+    seen = []
+
+    def measure_on(ctx, i):
+        seen.append((ctx, i))
+        return {"i": i, "ctx": ctx}
+
+    out = run_pipelined(list(range(7)), ["a", "b"], measure_on)
+    assert sorted(out) == list(range(7))
+    assert sorted(i for _, i in seen) == list(range(7))
+    # context c takes mocks c, c + 2, c + 4, ...
+    assert all(out[i]["ctx"] == ("a" if i % 2 == 0 else "b") for i in range(7))
+
+
+def test_run_pipelined_raises_a_worker_error():
+    import pytest
+    from hitomi_b200.batch import run_pipelined
+
+    def measure_on(ctx, i):
+        if i == 3:
+            raise RuntimeError("mock 3 failed")
+        return {}
+
+    with pytest.raises(RuntimeError, match="mock 3 failed"):
+        run_pipelined(list(range(6)), [0, 1, 2], measure_on)
