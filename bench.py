@@ -76,24 +76,38 @@ def result_bytes(res) -> int:
 
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms.  The sampler starts
+    before the warm-up (nvidia-smi takes a few hundred ms to emit its first line) and the
+    timed region is marked with host times; only samples stamped inside the timed region
+    (widened by one sampling interval on each side) are summarised."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.p = None
+        self.t0 = self.t1 = None
         self.path = os.path.join("/tmp", f"hg_clocks_{os.getpid()}_{device_index}.csv")
 
     def start(self):
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                       "-lms", "200", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "100", "-i", str(self.dev)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 
+    def mark_start(self):
+        import datetime
+        self.t0 = datetime.datetime.now()
+
+    def mark_stop(self):
+        import datetime
+        self.t1 = datetime.datetime.now()
+
     def stop(self):
+        import datetime
         if self.p is None:
             return None
         time.sleep(0.25)
@@ -103,25 +117,33 @@ class ClockSampler:
         except Exception:
             self.p.kill()
         self.f.close()
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         with open(self.path) as f:
             for line in f:
                 parts = [x.strip() for x in line.split(",")]
-                if len(parts) < 9:
+                if len(parts) < 10:
                     continue
                 try:
-                    sm.append(float(parts[1]))
-                    smax = float(parts[2])
+                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+                    rows.append((ts, float(parts[2]), float(parts[3]), parts[6:10]))
                 except ValueError:
                     continue
-                for nm, v in zip(names, parts[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(nm)
         os.unlink(self.path)
-        if not sm:
+        if not rows:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        pad = datetime.timedelta(milliseconds=100)
+        inside = [r for r in rows if self.t0 is not None and self.t1 is not None and self.t0 - pad <= r[0] <= self.t1 + pad]
+        if not inside:  # the region was shorter than the sampling interval: the nearest sample after its start
+            after = [r for r in rows if self.t0 is None or r[0] >= self.t0 - pad]
+            inside = after[:1] if after else rows[-1:]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in inside:
+            for nm, v in zip(names, r[3]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median([r[1] for r in inside]), "sm_max_mhz": inside[-1][2],
+                "reasons": sorted(reasons), "samples": len(inside)}
 
 
 def measured_peaks():
@@ -399,15 +421,16 @@ def main():
     timing = {}
     for form in forms:
         ctx = Context(wl["n_mesh"], wl["boxsize"], wl["binning"], "TSC", form, device=local)
+        clk = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
+                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else local)
+        clk.start()
         for _ in range(args.warmup):
             ctx.set_particles_device(0, d_pos.data_ptr(), n, 24, keep=d_pos)
             run_mock(ctx)
         # ---- device-resident value
-        clk = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
-                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else local)
         barrier(world)
         torch.cuda.synchronize()
-        clk.start()
+        clk.mark_start()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         launches = 0
@@ -417,6 +440,7 @@ def main():
             launches += nl
         ev1.record()
         torch.cuda.synchronize()
+        clk.mark_stop()
         clocks = clk.stop()
         barrier(world)
         ms = reduce_max(ev0.elapsed_time(ev1) / args.steps, world)
