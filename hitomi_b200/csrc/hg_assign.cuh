@@ -509,6 +509,24 @@ __global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom 
     }
 }
 
+// max |w| over a catalogue (1 when it has no weights): block partials, maximum on the host
+__global__ void k_max_weight(PartSrc src, double *part) {
+    __shared__ double red[32];
+    double m = 0.0;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < src.n; p += (long long)gridDim.x * blockDim.x) {
+        const double *rec = reinterpret_cast<const double *>(src.base + p * src.stride);
+        m = fmax(m, (src.w_off >= 0) ? fabs(rec[src.w_off]) : 1.0);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v = fmax(v, red[w]);
+        part[blockIdx.x] = v;
+    }
+}
+
 // Per-particle FP64 sums  out[q] = sum_p scale w_p^pw[q] Yhat_{l_q m_q}(los_p)  (complex), as
 // block partials part[block][q] summed on the host in block order (deterministic):
 // sum w (particle.hpp:336-352), sum w^2 (particle.hpp:255-258), and the shot-noise sums
@@ -799,17 +817,23 @@ struct FieldW {
 // exact k = 0 value.  A separable stencil lands whole, so its mass is w factor (the axis
 // weights sum to one), counted by the one record whose tile holds the stencil's first
 // point; an edge-straddling stencil (records at the end of the tile's range) adds its
-// in-bounds points one by one in the reference's product order.
-template <typename T, bool CPLX, int SCHEME>
+// in-bounds points one by one in the reference's product order.  FIX (FP32 fields whose
+// per-record weight is bounded by g.fix_bound: the host takes max |w|^wpow |scale| over the
+// catalogues, |Yhat_lm| <= 1): k_tile_accum's exact two-word integer sums, for the real and
+// the imaginary part.
+template <typename T, bool CPLX, int SCHEME, bool FIX>
 __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeom g, FieldW fw, T *mesh_re, T *mesh_im,
                                  double *mass) {
+    static_assert(!FIX || sizeof(T) == 4, "fixed-point accumulation is for FP32 meshes");
     constexpr int W = SCHEME + 1, s0 = (SCHEME >= 2) ? -1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *acc = reinterpret_cast<T *>(smem_raw);
     const int tcells = g.t[0] * g.t[1] * g.t[2];
     T *acc_im = acc + tcells;
+    // FIX: (hi, lo) words of the real part, then of the imaginary part (k_tile_accum's scheme)
+    int *fx = reinterpret_cast<int *>(smem_raw);
     __shared__ double red[2][32];
-    zero_shared(smem_raw, tcells * (CPLX ? 2 : 1) * (int)(sizeof(T) / 4));
+    zero_shared(smem_raw, tcells * (CPLX ? 2 : 1) * (FIX ? 2 : 1) * (int)(sizeof(T) / 4));
     __syncthreads();
     const Chunk k = ch[blockIdx.x];
     const int tile = k.tile;
@@ -818,12 +842,41 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
     const int tx = tile / (g.nt[2] * g.nt[1]);
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
     const T factor = (T)g.acc_factor;
+    float fscale = 1.0f, finv = 1.0f;
+    if (FIX) {
+        int e, e1;
+        frexpf(float(k.r1 - k.r0) * g.fix_bound, &e);
+        frexpf(g.fix_bound, &e1);
+        const int sc = min(50 - e, 42 - e1);  // the host keeps fix_bound >= 2^-60
+        fscale = ldexpf(1.0f, sc);
+        finv = ldexpf(1.0f, -sc);
+    }
+    auto add = [&](int li, T v, T vi) {
+        if (FIX) {
+            int hi, lo;
+            fix_split((float)v, hi, lo);
+            atomicAdd(&fx[li], hi);
+            atomicAdd(&fx[tcells + li], lo);
+            if (CPLX) {
+                fix_split((float)vi, hi, lo);
+                atomicAdd(&fx[2 * tcells + li], hi);
+                atomicAdd(&fx[3 * tcells + li], lo);
+            }
+        } else {
+            atomicAdd(&acc[li], v);
+            if (CPLX) atomicAdd(&acc_im[li], vi);
+        }
+    };
     double mr = 0.0, mi = 0.0;
     for (unsigned r = k.r0 + threadIdx.x; r < k.r1; r += blockDim.x) {
         const PRecS<T> pr = rec[r];
         double wr64, wi64;
         load_weight(fw.s[pr.src], pr.p, wr64, wi64);
-        const T wr = (T)wr64 * factor, wi = (T)wi64 * factor;
+        T wr = (T)wr64 * factor, wi = (T)wi64 * factor;
+        if (FIX) {
+            wr *= (T)fscale;
+            wi *= (T)fscale;
+        }
         const int anc[3] = {pr.i[0], pr.i[1], pr.i[2]};
         if (stencil_separable(g, anc)) {
             T w[3][W];
@@ -851,8 +904,7 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
 #pragma unroll
                     for (int c = 0; c < W; c++) {
                         if (!((mz >> c) & 1u)) continue;
-                        atomicAdd(&acc[lab + lz[c]], wab * w[2][c]);
-                        if (CPLX) atomicAdd(&acc_im[lab + lz[c]], wiab * w[2][c]);
+                        add(lab + lz[c], wab * w[2][c], wiab * w[2][c]);
                     }
                 }
             }
@@ -869,8 +921,7 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
             const int li = (lx * g.t[1] + ly) * g.t[2] + lz;
             const T wa = axis_weight_at<T>(SCHEME, pr.d[0], a), wb = axis_weight_at<T>(SCHEME, pr.d[1], b),
                     wc = axis_weight_at<T>(SCHEME, pr.d[2], c);
-            atomicAdd(&acc[li], wr * wa * wb * wc);
-            if (CPLX) atomicAdd(&acc_im[li], wi * wa * wb * wc);
+            add(li, wr * wa * wb * wc, wi * wa * wb * wc);
             const double da = axis_weight_at<double>(SCHEME, (double)pr.d[0], a),
                          db = axis_weight_at<double>(SCHEME, (double)pr.d[1], b),
                          dc = axis_weight_at<double>(SCHEME, (double)pr.d[2], c);
@@ -895,12 +946,21 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
         if (si != 0.0) atomicAdd(&mass[1], si);
     }
     for_tile_cells(g, tile, [&](int li, long long cell) {
-        if (k.multi == 0) {
-            mesh_re[cell] = acc[li];
-            if (CPLX) mesh_im[cell] = acc_im[li];
+        T vr, vi = (T)0;
+        if (FIX) {
+            vr = (T)(__ll2float_rn((long long)fx[li] * 1048576LL + (long long)fx[tcells + li]) * finv);
+            if (CPLX)
+                vi = (T)(__ll2float_rn((long long)fx[2 * tcells + li] * 1048576LL + (long long)fx[3 * tcells + li]) * finv);
         } else {
-            if (acc[li] != (T)0) atomicAdd(&mesh_re[cell], acc[li]);
-            if (CPLX && acc_im[li] != (T)0) atomicAdd(&mesh_im[cell], acc_im[li]);
+            vr = acc[li];
+            if (CPLX) vi = acc_im[li];
+        }
+        if (k.multi == 0) {
+            mesh_re[cell] = vr;
+            if (CPLX) mesh_im[cell] = vi;
+        } else {
+            if (vr != (T)0) atomicAdd(&mesh_re[cell], vr);
+            if (CPLX && vi != (T)0) atomicAdd(&mesh_im[cell], vi);
         }
     });
 }

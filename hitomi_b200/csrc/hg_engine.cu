@@ -501,6 +501,7 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(w_off < 0 || (w_off + 1) * 8 <= stride, "w_off outside the record");
         HG_REQUIRE(los_off < 0 || (los_off + 3) * 8 <= stride, "los_off outside the record");
         Slot &S = slot[s];
+        wmax_cache[s] = -1.0;
         if (on_device) {
             cudaPointerAttributes at;
             HG_CK(cudaPointerGetAttributes(&at, base));
@@ -2102,6 +2103,25 @@ struct Engine : public hg_ctx {
         return B;
     }
 
+    // max |w| of catalogue s (cached until the catalogue changes)
+    double wmax_cache[2] = {-1.0, -1.0};
+    double max_weight(int s) {
+        if (wmax_cache[s] >= 0.0) return wmax_cache[s];
+        const PartSrc src = survey_src(s, false, 0, 0, 1.0);
+        const int nb = (int)std::min<long long>(grid1(src.n, 256), 148 * 8);
+        HG_CK(psum_part.ensure(sizeof(double) * nb));
+        kb("particle_sums", double(src.n) * 8.0);
+        k_max_weight<<<nb, 256, 0, st>>>(src, dp<double>(psum_part));
+        ke();
+        std::vector<double> h(nb);
+        HG_CK(cudaMemcpyAsync(h.data(), psum_part.p, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        double m = 0.0;
+        for (double v : h) m = std::max(m, v);
+        wmax_cache[s] = m;
+        return m;
+    }
+
     // accumulate one weighting of the binned catalogues; returns the FP64 in-bounds mass
     template <bool CPLX>
     std::array<double, 2> survey_accumulate(int k, const PartSrc srcs[2], T *re, T *im) {
@@ -2116,18 +2136,41 @@ struct Engine : public hg_ctx {
         kb("assign_zero_split", 0.0);
         k_zero_split_tiles<T, CPLX><<<B.nchunks, 256, 0, st>>>(dp<Chunk>(B.chunks), ag, re, im);
         ke();
-        const size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2] * (CPLX ? 2 : 1);
+        // exact fixed-point sums for FP32 fields whose per-record weight bound is known:
+        // |Yhat_lm w^wpow scale| <= max|w|^wpow |scale| (|Yhat_lm| <= 1), one add per record
+        // and cell (every axis at least W cells)
+        bool fix = (sizeof(T) == 4);
+        double wb = 0.0;
+        for (int q = 0; q < 2; q++) {
+            fix = fix && srcs[q].cw == nullptr;
+            if (!fix) break;
+            const double mw = max_weight(q);
+            wb = std::max(wb, std::pow(mw, std::max(1, srcs[q].wpow)) * std::fabs(srcs[q].scale));
+        }
+        for (int a = 0; a < 3; a++) fix = fix && ag.n[a] >= stencil_width(ag.scheme);
+        ag.fix_bound = (float)(wb * std::fabs(ag.acc_factor) * (1.0 + 1e-6));
+        fix = fix && ag.fix_bound >= 0x1p-60f && std::isfinite(ag.fix_bound);
+        const size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2] * (CPLX ? 2 : 1) * (fix ? 2 : 1);
         kb("assign_tile_accum", double(B.total) * sizeof(PRecS<T>) + double(g.ntot) * sizeof(T) * (CPLX ? 2 : 1));
         auto launch = [&](auto kern) {
             HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             kern<<<B.nchunks, 256, smem, st>>>(dp<PRecS<T>>(B.rec), dp<Chunk>(B.chunks), ag, fw, re, im,
                                                dp<double>(mass));
         };
-        switch (ag.scheme) {
-            case HG_NGP: launch(k_tile_accum_src<T, CPLX, HG_NGP>); break;
-            case HG_CIC: launch(k_tile_accum_src<T, CPLX, HG_CIC>); break;
-            case HG_TSC: launch(k_tile_accum_src<T, CPLX, HG_TSC>); break;
-            default: launch(k_tile_accum_src<T, CPLX, HG_PCS>); break;
+        auto by_scheme = [&](auto fixtag) {
+            constexpr bool F = decltype(fixtag)::value;
+            switch (ag.scheme) {
+                case HG_NGP: launch(k_tile_accum_src<T, CPLX, HG_NGP, F>); break;
+                case HG_CIC: launch(k_tile_accum_src<T, CPLX, HG_CIC, F>); break;
+                case HG_TSC: launch(k_tile_accum_src<T, CPLX, HG_TSC, F>); break;
+                default: launch(k_tile_accum_src<T, CPLX, HG_PCS, F>); break;
+            }
+        };
+        if constexpr (sizeof(T) == 4) {
+            if (fix) by_scheme(std::true_type{});
+            else by_scheme(std::false_type{});
+        } else {
+            by_scheme(std::false_type{});
         }
         ke();
         double hm[2];
