@@ -212,4 +212,100 @@ __global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt,
         if (scnt[q]) atomicAdd(&nmode[q], scnt[q]);
 }
 
+// Several spectra binned against one in a single pass (the survey P_l: every M of one l):
+// per mode, sum_q w_q ((F_q conj F2 - S_q C(k)) / W^2) Yhat_{l_q m_q}(k), binned like k_pk_bin
+// (the bin average is linear, so this equals the weighted sum of the per-term averages of
+// powerspec.hpp:36-77 with the same mode counts).  F_q is a stored spectrum, or the mirror
+// sg conj F(-k) of one.
+#define HG_MAX_PK_TERMS 9
+template <typename T>
+struct PkTerm {
+    Spec<T> f;
+    int mirror;
+    double sg;
+    double S_re, S_im;
+    int l, m;
+    double w;
+};
+template <typename T>
+struct PkTerms {
+    int n;
+    PkTerm<T> t[HG_MAX_PK_TERMS];
+};
+
+template <typename T, class F2>
+__global__ void k_pk_bin_terms(PkTerms<T> terms, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt, const int2 *lut,
+                               int lutn, int nbin, int assign, int wpow, double *acc, unsigned long long *nmode) {
+    __shared__ double sacc[2 * 256];
+    __shared__ unsigned long long scnt[256];
+    for (int q = threadIdx.x; q < 2 * nbin; q += blockDim.x) sacc[q] = 0.0;
+    for (int q = threadIdx.x; q < nbin; q += blockDim.x) scnt[q] = 0ull;
+    __syncthreads();
+    const long long total = (long long)cnt.x * cnt.y * cnt.z;
+    const int lane = threadIdx.x & 31;
+    const long long wstride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wbase < total; wbase += wstride) {
+        const long long idx = wbase + lane;
+        int2 b = make_int2(-1, -1);
+        zd v = mk<double>(0.0, 0.0);
+        if (idx < total) {
+            int nx, ny, nz;
+            split3((unsigned)idx, (unsigned)cnt.y, (unsigned)cnt.z, nx, ny, nz);
+            nx += lo.x;
+            ny += lo.y;
+            nz += lo.z;
+            const int ix = nx < 0 ? nx + g.n[0] : nx, iy = ny < 0 ? ny + g.n[1] : ny, iz = nz < 0 ? nz + g.n[2] : nz;
+            double kv[3];
+            kv[0] = kcomp(wrap_index(ix, g.n[0]), g.dk[0]);
+            kv[1] = kcomp(wrap_index(iy, g.n[1]), g.dk[1]);
+            kv[2] = kcomp(wrap_index(iz, g.n[2]), g.dk[2]);
+            const double kmag = kmag_exact(kv[0], kv[1], kv[2]);
+            const int kindex = (int)__dadd_rn(__ddiv_rn(kmag, 0.0001), 0.5);
+            if (kindex < lutn) b = lut[kindex];
+            if (b.x >= 0) {
+                const zd d2 = f2.at(ix, iy, iz);
+                const double C = shot_tab(tabs, ix, iy, iz, assign);
+                const double wf = window_tab(tabs, ix, iy, iz, wpow);
+                const double w2 = wf * wf;
+                const int jx = neg_index(ix, g.n[0]), jy = neg_index(iy, g.n[1]), jz = neg_index(iz, g.n[2]);
+                for (int q = 0; q < terms.n; q++) {
+                    const PkTerm<T> &tq = terms.t[q];
+                    zd d1;
+                    if (tq.mirror) {
+                        const zd u = tq.f.at(jx, jy, jz);
+                        d1 = mk<double>(tq.sg * u.x, -tq.sg * u.y);
+                    } else {
+                        d1 = tq.f.at(ix, iy, iz);
+                    }
+                    zd pk2 = d1 * conjg(d2) - mk<double>(tq.S_re * C, tq.S_im * C);
+                    pk2 = mk<double>(pk2.x / w2, pk2.y / w2);
+                    const zd y = ylm_reduced(tq.l, tq.m, kv[0], kv[1], kv[2]);
+                    v = v + (pk2 * y) * tq.w;
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, b.x < 0)) continue;
+        const unsigned gx = __match_any_sync(0xffffffffu, b.x);
+        const unsigned gy = __match_any_sync(0xffffffffu, b.y);
+        const bool lx = (lane == __ffs(gx) - 1), ly = (lane == __ffs(gy) - 1);
+        const double sxr = group_sum(v.x, gx), sxi = group_sum(v.y, gx);
+        if (b.x >= 0 && lx) {
+            atomicAdd(&sacc[2 * b.x], sxr);
+            atomicAdd(&sacc[2 * b.x + 1], sxi);
+            atomicAdd(&scnt[b.x], (unsigned long long)__popc(gx));
+        }
+        const double syr = group_sum(v.x, gy), syi = group_sum(v.y, gy);
+        if (b.y >= 0 && ly) {
+            atomicAdd(&sacc[2 * b.y], syr);
+            atomicAdd(&sacc[2 * b.y + 1], syi);
+            atomicAdd(&scnt[b.y], (unsigned long long)__popc(gy));
+        }
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 2 * nbin; q += blockDim.x)
+        if (sacc[q] != 0.0) atomicAdd(&acc[q], sacc[q]);
+    for (int q = threadIdx.x; q < nbin; q += blockDim.x)
+        if (scnt[q]) atomicAdd(&nmode[q], scnt[q]);
+}
+
 }  // namespace hg

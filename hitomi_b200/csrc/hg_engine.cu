@@ -895,6 +895,49 @@ struct Engine : public hg_ctx {
             }
     }
 
+    // averages over each k bin of sum_q w_q (F_q conj f2 - S_q C) / W^2 Yhat_{l_q m_q}
+    void pk_bin_terms(const PkTerms<T> &terms, const Spec<T> &f2, std::vector<double> &avg,
+                      std::vector<unsigned long long> &nm) {
+        const int nbin = cfg.n_kbin;
+        int3 lo, cn;
+        int c[3];
+        for (int a = 0; a < 3; a++) {
+            double kedge = double(lutn) * 0.0001;
+            c[a] = (int)std::floor(kedge / g.dk[a]) + 1;
+        }
+        auto rng = [&](int a, int &l0, int &cnt_) {
+            int lo_ = std::max(-c[a], -g.n[a] / 2);
+            int hi_ = std::min(c[a], g.n[a] / 2 - 1);
+            l0 = lo_;
+            cnt_ = hi_ - lo_ + 1;
+        };
+        rng(0, lo.x, cn.x);
+        rng(1, lo.y, cn.y);
+        rng(2, lo.z, cn.z);
+        HG_CK(bin_acc.ensure(sizeof(double) * 2 * nbin));
+        HG_CK(bin_cnt.ensure(sizeof(unsigned long long) * nbin));
+        HG_CK(cudaMemsetAsync(bin_acc.p, 0, sizeof(double) * 2 * nbin, st));
+        HG_CK(cudaMemsetAsync(bin_cnt.p, 0, sizeof(unsigned long long) * nbin, st));
+        long long total = (long long)cn.x * cn.y * cn.z;
+        unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 8);
+        kb("pk_bin", double(total) * sizeof(C) * (terms.n + 1));
+        k_pk_bin_terms<T, Spec<T>><<<blocks, 256, 0, st>>>(terms, f2, g, tabs, lo, cn, dp<int2>(lut), lutn, nbin,
+                                                           cfg.assign, wpow, dp<double>(bin_acc),
+                                                           dp<unsigned long long>(bin_cnt));
+        ke();
+        std::vector<double> a(2 * nbin);
+        nm.assign(nbin, 0);
+        HG_CK(cudaMemcpyAsync(a.data(), bin_acc.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaMemcpyAsync(nm.data(), bin_cnt.p, sizeof(unsigned long long) * nbin, cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        avg.assign(2 * nbin, 0.0);
+        for (int j = 0; j < nbin; j++)
+            if (nm[j] != 0) {
+                avg[2 * j] = a[2 * j] / double(nm[j]);
+                avg[2 * j + 1] = a[2 * j + 1] / double(nm[j]);
+            }
+    }
+
     // powerspec.hpp:273-332
     void pk_box(int ell, double *pk_save, int *n_mode, double *norm) override {
         HG_REQUIRE(ell >= 0, "ell must be >= 0");
@@ -2514,6 +2557,31 @@ struct Engine : public hg_ctx {
         const Spec<T> f00 = sfield(SF_DELTA, 0, 0, alpha).s;
         std::vector<double> acc(2 * nb, 0.0);
         std::vector<unsigned long long> nm;
+        if (nb <= 256 && 2 * ell + 1 <= HG_MAX_PK_TERMS) {
+            // every M of this l in one pass over the modes
+            PkTerms<T> terms{};
+            for (int M = -ell; M <= ell; M++) {
+                const int am = M < 0 ? -M : M;
+                double Sr = sD[2 * am] + alpha * alpha * sR[2 * am];
+                double Si = sD[2 * am + 1] + alpha * alpha * sR[2 * am + 1];
+                const Spec<T> f1 = sfield(SF_DELTA, ell, am, alpha).s;
+                const double sg = (am % 2) ? -1.0 : 1.0;
+                if (M < 0) {
+                    Sr = sg * Sr;
+                    Si = -sg * Si;
+                }
+                for (int m1 = -ell; m1 <= ell; m1++) {
+                    double w = wigner3j(ell, 0, ell, 0, 0, 0) * wigner3j(ell, 0, ell, m1, 0, M);
+                    w *= double(2 * ell + 1) * double(2 * ell + 1);
+                    if (std::fabs(w) < 1.0e-10) continue;
+                    HG_REQUIRE(terms.n < HG_MAX_PK_TERMS, "too many survey P terms");
+                    terms.t[terms.n++] = PkTerm<T>{f1, M < 0 ? 1 : 0, sg, Sr, Si, ell, m1, w};
+                }
+            }
+            std::vector<double> avg;
+            pk_bin_terms(terms, f00, avg, nm);
+            acc = avg;
+        } else {  // more bins or terms than the one-pass kernel holds: one pass per term
         for (int M = -ell; M <= ell; M++) {
             const int am = M < 0 ? -M : M;
             double Sr = sD[2 * am] + alpha * alpha * sR[2 * am];
@@ -2538,6 +2606,7 @@ struct Engine : public hg_ctx {
                     acc[2 * i + 1] += w * avg[2 * i + 1];
                 }
             }
+        }
         }
         for (int i = 0; i < 2 * nb; i++) pk_save[i] = acc[i];
         if (n_mode)
