@@ -509,6 +509,19 @@ __global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom 
     }
 }
 
+// The complex weight of every particle of a source before its scale (load_weight with
+// scale 1), in catalogue order: the accumulation then gathers 16 bytes per record instead of
+// the particle's weight and line of sight, and evaluates no Yhat_lm.
+__global__ void k_make_cw(PartSrc src, double2 *cw) {
+    src.scale = 1.0;
+    src.cw = nullptr;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < src.n; p += (long long)gridDim.x * blockDim.x) {
+        double wr, wi;
+        load_weight(src, p, wr, wi);
+        cw[p] = make_double2(wr, wi);
+    }
+}
+
 // max |w| over a catalogue (1 when it has no weights): block partials, maximum on the host
 __global__ void k_max_weight(PartSrc src, double *part) {
     __shared__ double red[32];

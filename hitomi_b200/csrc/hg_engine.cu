@@ -2146,6 +2146,7 @@ struct Engine : public hg_ctx {
         return B;
     }
 
+    DBuf cwbuf[2];  // per-particle complex weights of the field being accumulated
     // max |w| of catalogue s (cached until the catalogue changes)
     double wmax_cache[2] = {-1.0, -1.0};
     double max_weight(int s) {
@@ -2174,6 +2175,15 @@ struct Engine : public hg_ctx {
         FieldW fw;
         fw.s[0] = srcs[0];
         fw.s[1] = srcs[1];
+        for (int q = 0; q < 2; q++) {  // harmonic-weighted sources: weights precomputed in order
+            if (!srcs[q].ylm_on || srcs[q].cw) continue;
+            HG_CK(cwbuf[q].ensure(sizeof(double2) * std::max<long long>(srcs[q].n, 1)));
+            const unsigned nb = (unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 16);
+            kb("particle_sums", double(srcs[q].n) * (16.0 + 32.0));
+            k_make_cw<<<nb, 256, 0, st>>>(srcs[q], dp<double2>(cwbuf[q]));
+            ke();
+            fw.s[q].cw = dp<double2>(cwbuf[q]);
+        }
         HG_CK(mass.ensure(sizeof(double) * 2));
         HG_CK(cudaMemsetAsync(mass.p, 0, sizeof(double) * 2, st));
         kb("assign_zero_split", 0.0);
