@@ -312,7 +312,8 @@ def run_config(args) -> int:
     for form in ("fp64", "fp32"):
         with Context(setup["n_mesh"], setup["boxsize"], setup["b"], setup["assign"], form,
                      interlace=setup["interlace"]) as ctx:
-            one(ctx, mocks[0])  # warm-up: tables, splines, buffers
+            for m in mocks:  # warm-up over every mock: tables, splines, buffers sized for the largest
+                one(ctx, m)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             outs = [one(ctx, m, d) for m, d in zip(mocks, devs)]
