@@ -12,6 +12,7 @@
 #pragma once
 
 #include <algorithm>
+#include <type_traits>
 
 #include "hg_common.cuh"
 #include "hg_fft.cuh"
@@ -664,49 +665,63 @@ __global__ void __launch_bounds__(HG_ZR_THREADS)
     k_zeta_pairsum(const cplx<T> *__restrict__ Fa, int na, const cplx<T> *__restrict__ Fb, int nb,
                    const cplx<T> *__restrict__ G, long long ntot, double *part) {
     constexpr int CH = HG_ZR_CHUNK, CHP = HG_ZR_CHUNK + 1;  // padded rows: distinct rows, distinct banks
+    // FP32 form: operands staged and multiplied in FP32, partial sums over FLUSH chunks
+    // (a few tens of products per thread) added to the FP64 accumulators; FP64 form: FP64
+    using A = T;
+    using A2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+    constexpr int FLUSH = 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int na4 = (na + 3) / 4, nb4 = (nb + 3) / 4;
     const int ntile = na4 * nb4;
     const int ngroup = max(1, HG_ZR_THREADS / ntile);
-    double2 *sa = reinterpret_cast<double2 *>(smem_raw);  // [4 na4][CHP]
-    double2 *sb = sa + (size_t)4 * na4 * CHP;             // [4 nb4][CHP]
+    A2 *sa = reinterpret_cast<A2 *>(smem_raw);  // [4 na4][CHP]
+    A2 *sb = sa + (size_t)4 * na4 * CHP;        // [4 nb4][CHP]
     const int t = threadIdx.x;
     const int tile = t % ntile, grp = t / ntile;
     const bool active = (t < ntile * ngroup);
     const int ta = tile / nb4, tb = tile % nb4;
     double acc[4][4][2];
+    A pacc[(sizeof(T) == 4) ? 4 : 1][4][2];  // FP32 partials (unused in the FP64 form)
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) acc[u][v][0] = acc[u][v][1] = 0.0;
+        for (int v = 0; v < 4; v++) {
+            acc[u][v][0] = acc[u][v][1] = 0.0;
+            if constexpr (sizeof(T) == 4) pacc[u][v][0] = pacc[u][v][1] = (A)0;
+        }
     const long long nchunk = (ntot + CH - 1) / CH;
+    int since = 0;
     for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
         const long long x0 = ch * CH;
         __syncthreads();
         for (int e = t; e < 4 * na4 * CH; e += blockDim.x) {
             int r = e / CH, c = e % CH;
-            double2 v = make_double2(0.0, 0.0);
+            A2 v;
+            v.x = v.y = (A)0;
             if (r < na && x0 + c < ntot) {
                 cplx<T> a = Fa[(long long)r * ntot + x0 + c];
-                v = make_double2((double)a.x, (double)a.y);
+                v.x = (A)a.x;
+                v.y = (A)a.y;
             }
             sa[r * CHP + c] = v;
         }
         for (int e = t; e < 4 * nb4 * CH; e += blockDim.x) {
             int r = e / CH, c = e % CH;
-            double2 v = make_double2(0.0, 0.0);
+            A2 v;
+            v.x = v.y = (A)0;
             if (r < nb && x0 + c < ntot) {
                 cplx<T> b = Fb[(long long)r * ntot + x0 + c];
                 cplx<T> gg = G[x0 + c];
-                double br = (double)b.x, bi = (double)b.y, gr = (double)gg.x, gi = (double)gg.y;
-                v = make_double2(br * gr - bi * gi, br * gi + bi * gr);
+                const A br = (A)b.x, bi = (A)b.y, gr = (A)gg.x, gi = (A)gg.y;
+                v.x = br * gr - bi * gi;
+                v.y = br * gi + bi * gr;
             }
             sb[r * CHP + c] = v;
         }
         __syncthreads();
         if (active) {
             for (int c = grp; c < CH; c += ngroup) {
-                double2 av[4], bv[4];
+                A2 av[4], bv[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) av[u] = sa[(4 * ta + u) * CHP + c];
 #pragma unroll
@@ -715,11 +730,38 @@ __global__ void __launch_bounds__(HG_ZR_THREADS)
                 for (int u = 0; u < 4; u++)
 #pragma unroll
                     for (int v = 0; v < 4; v++) {
-                        acc[u][v][0] += av[u].x * bv[v].x - av[u].y * bv[v].y;
-                        acc[u][v][1] += av[u].x * bv[v].y + av[u].y * bv[v].x;
+                        if constexpr (sizeof(T) == 4) {
+                            pacc[u][v][0] += av[u].x * bv[v].x - av[u].y * bv[v].y;
+                            pacc[u][v][1] += av[u].x * bv[v].y + av[u].y * bv[v].x;
+                        } else {
+                            acc[u][v][0] += av[u].x * bv[v].x - av[u].y * bv[v].y;
+                            acc[u][v][1] += av[u].x * bv[v].y + av[u].y * bv[v].x;
+                        }
                     }
             }
+            if constexpr (sizeof(T) == 4) {
+                if (++since == FLUSH) {
+                    since = 0;
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+#pragma unroll
+                        for (int v = 0; v < 4; v++) {
+                            acc[u][v][0] += (double)pacc[u][v][0];
+                            acc[u][v][1] += (double)pacc[u][v][1];
+                            pacc[u][v][0] = pacc[u][v][1] = (A)0;
+                        }
+                }
+            }
         }
+    }
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                acc[u][v][0] += (double)pacc[u][v][0];
+                acc[u][v][1] += (double)pacc[u][v][1];
+            }
     }
     // sum the residue groups through shared memory: red[tile][u][v] (complex)
     __syncthreads();
