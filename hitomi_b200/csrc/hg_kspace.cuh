@@ -528,8 +528,10 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
     const int na4 = (na + 3) / 4, nb4 = (nb + 3) / 4;
     const int ntile = na4 * nb4;
     const int ngroup = max(1, HG_SN_THREADS / ntile);
-    double2 *sb = reinterpret_cast<double2 *>(smem_raw);  // [4 nb4][CHP]  J2 * h
-    double *sa = reinterpret_cast<double *>(sb + (size_t)4 * nb4 * CHP);  // [4 na4][CHP]  J1
+    // row r of a staged operand starts at r CHP + r / 4: one extra slot per tile of four rows
+    // puts the rows that a warp's tiles read at the same c on different banks
+    double2 *sb = reinterpret_cast<double2 *>(smem_raw);  // [4 nb4][CHP] (+ nb4)  J2 * h
+    double *sa = reinterpret_cast<double *>(sb + (size_t)4 * nb4 * CHP + nb4);  // [4 na4][CHP] (+ na4)  J1
     const int t = threadIdx.x;
     const int tile = t % ntile, grp = t / ntile;
     const bool active = (t < ntile * ngroup);
@@ -546,7 +548,7 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
         for (int e = t; e < 4 * na4 * CH; e += blockDim.x) {
             int r = e / CH, c = e % CH;
             bool ok = (r < na) && (n0 + c < n2dim);
-            sa[r * CHP + c] = ok ? J1[(long long)r * n2dim + n0 + c] : 0.0;
+            sa[r * CHP + (r >> 2) + c] = ok ? J1[(long long)r * n2dim + n0 + c] : 0.0;
         }
         for (int e = t; e < 4 * nb4 * CH; e += blockDim.x) {
             int r = e / CH, c = e % CH;
@@ -554,7 +556,7 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
             double b = ok ? J2[(long long)r * n2dim + n0 + c] : 0.0;
             double hr = ok ? hist[2 * (n0 + c)] : 0.0;
             double hi = ok ? hist[2 * (n0 + c) + 1] : 0.0;
-            sb[r * CHP + c] = make_double2(b * hr, b * hi);
+            sb[r * CHP + (r >> 2) + c] = make_double2(b * hr, b * hi);
         }
         __syncthreads();
         if (active) {
@@ -562,9 +564,9 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
                 double av[4];
                 double2 bv[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) av[u] = sa[(4 * ta + u) * CHP + c];
+                for (int u = 0; u < 4; u++) av[u] = sa[(4 * ta + u) * CHP + ta + c];
 #pragma unroll
-                for (int v = 0; v < 4; v++) bv[v] = sb[(4 * tb + v) * CHP + c];
+                for (int v = 0; v < 4; v++) bv[v] = sb[(4 * tb + v) * CHP + tb + c];
 #pragma unroll
                 for (int u = 0; u < 4; u++)
 #pragma unroll
@@ -604,7 +606,7 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
 #define HG_SN_MAXROWS 64  // rows per operand and launch (4 x 4 tiles, at most 256 of them)
 inline size_t sn_partial_smem(int na, int nb) {
     const size_t na4 = (size_t)(na + 3) / 4, nb4 = (size_t)(nb + 3) / 4;
-    size_t stage = (sizeof(double2) * nb4 + sizeof(double) * na4) * 4 * (HG_SN_CHUNK + 1);
+    size_t stage = (sizeof(double2) * nb4 + sizeof(double) * na4) * (4 * (HG_SN_CHUNK + 1) + 1);
     size_t red = sizeof(double2) * 16 * na4 * nb4;
     return stage > red ? stage : red;
 }
