@@ -667,20 +667,18 @@ __global__ void __launch_bounds__(HG_ZR_THREADS)
     k_zeta_pairsum(const cplx<T> *__restrict__ Fa, int na, const cplx<T> *__restrict__ Fb, int nb,
                    const cplx<T> *__restrict__ G, long long ntot, double *part) {
     constexpr int CH = HG_ZR_CHUNK, CHP = HG_ZR_CHUNK + 1;  // padded rows: distinct rows, distinct banks
-    // FP32 form: operands staged and multiplied in FP32, partial sums over FLUSH chunks
-    // (a few tens of products per thread) added to the FP64 accumulators; FP64 form: FP64
-    using A = T;
-    using A2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
-    constexpr int FLUSH = 4;
+    // operands staged in FP64 in both forms (FP32 staging and FP32 products were measured
+    // slower: 19.1 against 18.1 ms per config-5 mock)
+    using A = double;
+    using A2 = double2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int na4 = (na + 3) / 4, nb4 = (nb + 3) / 4;
     const int ntile = na4 * nb4;
     const int ngroup = max(1, HG_ZR_THREADS / ntile);
-    // FP64 form: row r of a staged operand starts at r CHP + r / 4 (one extra slot per tile
-    // of four rows: the 16-byte rows a warp's tiles read at the same c fall on different
-    // banks; measured 21.3 -> 18.1 ms per config-5 mock).  The FP32 form's 8-byte rows are
-    // faster unshifted (19.3 against 27.1 ms shifted).
-    constexpr int SH = (sizeof(T) == 8) ? 1 : 0;
+    // row r of a staged operand starts at r CHP + r / 4 (one extra slot per tile of four
+    // rows: the 16-byte rows a warp's tiles read at the same c fall on different banks;
+    // measured 21.3 -> 18.1 ms per config-5 mock)
+    constexpr int SH = 1;
     A2 *sa = reinterpret_cast<A2 *>(smem_raw);       // [4 na4][CHP] (+ na4)
     A2 *sb = sa + (size_t)4 * na4 * CHP + SH * na4;  // [4 nb4][CHP] (+ nb4)
     const int t = threadIdx.x;
@@ -688,16 +686,11 @@ __global__ void __launch_bounds__(HG_ZR_THREADS)
     const bool active = (t < ntile * ngroup);
     const int ta = tile / nb4, tb = tile % nb4;
     double acc[4][4][2];
-    A pacc[(sizeof(T) == 4) ? 4 : 1][4][2];  // FP32 partials (unused in the FP64 form)
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-            acc[u][v][0] = acc[u][v][1] = 0.0;
-            if constexpr (sizeof(T) == 4) pacc[u][v][0] = pacc[u][v][1] = (A)0;
-        }
+        for (int v = 0; v < 4; v++) acc[u][v][0] = acc[u][v][1] = 0.0;
     const long long nchunk = (ntot + CH - 1) / CH;
-    int since = 0;
     for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
         const long long x0 = ch * CH;
         __syncthreads();
@@ -737,38 +730,11 @@ __global__ void __launch_bounds__(HG_ZR_THREADS)
                 for (int u = 0; u < 4; u++)
 #pragma unroll
                     for (int v = 0; v < 4; v++) {
-                        if constexpr (sizeof(T) == 4) {
-                            pacc[u][v][0] += av[u].x * bv[v].x - av[u].y * bv[v].y;
-                            pacc[u][v][1] += av[u].x * bv[v].y + av[u].y * bv[v].x;
-                        } else {
-                            acc[u][v][0] += av[u].x * bv[v].x - av[u].y * bv[v].y;
-                            acc[u][v][1] += av[u].x * bv[v].y + av[u].y * bv[v].x;
-                        }
+                        acc[u][v][0] += av[u].x * bv[v].x - av[u].y * bv[v].y;
+                        acc[u][v][1] += av[u].x * bv[v].y + av[u].y * bv[v].x;
                     }
             }
-            if constexpr (sizeof(T) == 4) {
-                if (++since == FLUSH) {
-                    since = 0;
-#pragma unroll
-                    for (int u = 0; u < 4; u++)
-#pragma unroll
-                        for (int v = 0; v < 4; v++) {
-                            acc[u][v][0] += (double)pacc[u][v][0];
-                            acc[u][v][1] += (double)pacc[u][v][1];
-                            pacc[u][v][0] = pacc[u][v][1] = (A)0;
-                        }
-                }
-            }
         }
-    }
-    if constexpr (sizeof(T) == 4) {
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int v = 0; v < 4; v++) {
-                acc[u][v][0] += (double)pacc[u][v][0];
-                acc[u][v][1] += (double)pacc[u][v][1];
-            }
     }
     // sum the residue groups through shared memory: red[tile][u][v] (complex)
     __syncthreads();
