@@ -758,17 +758,6 @@ struct Engine : public hg_ctx {
         return assign_mesh<T, false>({src}, ag, out, nullptr, true);
     }
 
-    // Stockham shared-memory engine: for loaders that compute their input (8 values per
-    // thread and a separate load loop keep register pressure low)
-    template <int DIR, class LD, class ST>
-    void pass_smem(int L, LD ld, ST stt, long long outer, long long inner, const char *name, double bytes) {
-        PassGeom pg{outer, inner};
-        const C *twp = twiddles(L);
-        kb(name, bytes);
-        HG_CK((launch_fft_pass<T, DIR>(L, ld, stt, pg, twp, st)));
-        ke();
-    }
-
     template <int DIR, class LD, class ST>
     void pass(int L, LD ld, ST stt, long long outer, long long inner, const char *name = "fft_pass",
               double bytes = -1.0) {
