@@ -623,7 +623,7 @@ struct Engine : public hg_ctx {
             ke();
             df.pass = 1;
             kb("assign_edge_count", 0.0);
-            k_bin_count<<<148 * 2, 256, 0, st>>>(srcs[q], ag, df, dp<unsigned>(cnt), mass_dev);
+            k_bin_count<<<148 * 8, 256, 0, st>>>(srcs[q], ag, df, dp<unsigned>(cnt), mass_dev);
             ke();
             o += srcs[q].n;
         }
@@ -646,7 +646,7 @@ struct Engine : public hg_ctx {
             ke();
             df.pass = 1;
             kb("assign_edge_scatter", 0.0);
-            k_bin_scatter<MK><<<148 * 2, 256, 0, st>>>(srcs[q], ag, mks[q], df, dp<unsigned>(off),
+            k_bin_scatter<MK><<<148 * 8, 256, 0, st>>>(srcs[q], ag, mks[q], df, dp<unsigned>(off),
                                                       dp<unsigned>(cursor), dp<unsigned>(cursor_back), recp);
             ke();
             o += srcs[q].n;
