@@ -773,8 +773,16 @@ struct Engine : public hg_ctx {
     // r2c transform of a real mesh into the half spectrum Hd: FFT[(mesh - sub) scl]
     void forward_real(const T *m, C *Hd, T sub, T scl, const char *name) {
         const int hz = g.n[2] / 2 + 1;
-        pass<-1>(g.n[2], LdMeshDelta<T>{m, g.n[2], sub, scl}, StHalf<T>{Hd, g.n[2], hz}, (long long)g.n[0] * g.n[1], 1,
-                 name, double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
+        // z: two real rows per complex transform (k_fft2_r2c_pair), the plain pass otherwise
+        kb(name, double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
+        cudaError_t pe = cudaSuccess;
+        const bool paired =
+            launch_r2c_pair<T, -1>(g.n[2], m, sub, scl, Hd, (long long)g.n[0] * g.n[1], hz, twiddles(g.n[2]), st, pe);
+        HG_CK(pe);
+        ke();
+        if (!paired)
+            pass<-1>(g.n[2], LdMeshDelta<T>{m, g.n[2], sub, scl}, StHalf<T>{Hd, g.n[2], hz}, (long long)g.n[0] * g.n[1],
+                     1, name, double(g.ntot) * sizeof(T) + double(g.n[0]) * g.n[1] * hz * sizeof(C));
         pass<-1>(g.n[1], LdArr<T>{Hd, g.n[1], hz}, StArr<T>{Hd, g.n[1], hz}, g.n[0], hz, name);
         pass<-1>(g.n[0], LdArr<T>{Hd, g.n[0], (long long)g.n[1] * hz}, StArr<T>{Hd, g.n[0], (long long)g.n[1] * hz}, 1,
                  (long long)g.n[1] * hz, name);

@@ -403,6 +403,79 @@ inline cudaError_t launch_fft2_pipe(const cplx<T> *src, ST st, PassGeom g, const
     return cudaGetLastError();
 }
 
+// Real rows -> half spectra, two rows per complex transform: line b carries rows 2o (real
+// part) and 2o + 1 (imaginary part) of (mesh - sub) scl; after the transform
+// A(k) = (Z(k) + conj Z(-k)) / 2 and B(k) = (Z(k) - conj Z(-k)) / (2 i) are the two rows'
+// spectra, of which k = 0 .. hz - 1 are stored ([row][hz]).  Half the transform work of a
+// complex pass over real input.
+template <typename T, int L, int DIR>
+__global__ void __launch_bounds__(Fft2Cfg<T, L, false>::NT)
+    k_fft2_r2c_pair(const T *__restrict__ mesh, T sub, T scl, cplx<T> *__restrict__ H, long long npair, int hz,
+                    const cplx<T> *__restrict__ tw) {
+    using CF = Fft2Cfg<T, L, false>;
+    using X = XchgLayout<L, false, CF::B>;
+    constexpr int R1 = X::R1, R2 = X::R2, B = CF::B, LP = L + 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
+    const int b = threadIdx.x / R2, t = threadIdx.x % R2;
+    const long long o = (long long)blockIdx.x * B + b;
+    const bool ok = o < npair;
+    const T *ra = mesh + 2 * o * L, *rb = ra + L;
+    cplx<T> v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; n1++) {
+        const int p = R2 * n1 + t;
+        v[n1] = ok ? mk<T>((ra[p] - sub) * scl, (rb[p] - sub) * scl) : mk<T>(0, 0);
+    }
+    line_fft2<T, L, DIR, false, B>(v, S, t, b, tw);  // ends with S free
+#pragma unroll
+    for (int r = 0; r < R1; r++) S[b * LP + pos_of_reg<L>(t, r)] = v[r];
+    __syncthreads();
+    if (ok) {
+        cplx<T> *ha = H + 2 * o * hz, *hb = ha + hz;
+        for (int k = t; k < hz; k += R2) {
+            const cplx<T> z = S[b * LP + k], zm = S[b * LP + ((L - k) & (L - 1))];
+            ha[k] = mk<T>((T)0.5 * (z.x + zm.x), (T)0.5 * (z.y - zm.y));
+            hb[k] = mk<T>((T)0.5 * (z.y + zm.y), (T)0.5 * (zm.x - z.x));
+        }
+    }
+}
+
+template <typename T, int L, int DIR>
+inline cudaError_t launch_r2c_pair_L(const T *mesh, T sub, T scl, cplx<T> *H, long long nrows, int hz,
+                                     const cplx<T> *tw, cudaStream_t stream) {
+    using CF = Fft2Cfg<T, L, false>;
+    using X = XchgLayout<L, false, CF::B>;
+    const size_t elems = std::max<size_t>((size_t)X::ELEMS, (size_t)CF::B * (L + 1));
+    const size_t smem = elems * sizeof(cplx<T>);
+    auto kern = k_fft2_r2c_pair<T, L, DIR>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long long npair = nrows / 2;
+    const long long blocks = (npair + CF::B - 1) / CF::B;
+    if (blocks <= 0) return cudaSuccess;
+    kern<<<(unsigned)blocks, CF::NT, smem, stream>>>(mesh, sub, scl, H, npair, hz, tw);
+    return cudaGetLastError();
+}
+
+// false when the length has no paired kernel (the caller then runs the plain pass)
+template <typename T, int DIR>
+inline bool launch_r2c_pair(int L, const T *mesh, T sub, T scl, cplx<T> *H, long long nrows, int hz,
+                            const cplx<T> *tw, cudaStream_t stream, cudaError_t &err) {
+    if (nrows % 2) return false;
+    switch (L) {
+        case 8: err = launch_r2c_pair_L<T, 8, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        case 16: err = launch_r2c_pair_L<T, 16, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        case 32: err = launch_r2c_pair_L<T, 32, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        case 64: err = launch_r2c_pair_L<T, 64, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        case 128: err = launch_r2c_pair_L<T, 128, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        case 256: err = launch_r2c_pair_L<T, 256, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        case 512: err = launch_r2c_pair_L<T, 512, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        case 1024: err = launch_r2c_pair_L<T, 1024, DIR>(mesh, sub, scl, H, nrows, hz, tw, stream); return true;
+        default: return false;
+    }
+}
+
 template <class LD>
 struct IsLdArr : std::false_type {};
 template <typename U>
