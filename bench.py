@@ -32,6 +32,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
+CHOSEN = "fp32+density+bk_signal"
 METRIC = "mocks/sec P_ℓ+B_ℓ @512³,1e7 pts: batched FP32 vs FP64 GPU, ≤1e-5 rel err"
 UNIT = "mocks/s"
 PK_ELLS = (0, 2, 4)
@@ -378,6 +379,82 @@ def cpu_config(cfg, mocks, setup, zmps):
                            "not timed in the bench"}
 
 
+def dtype_of(form: str) -> str:
+    """The arithmetic a form computes in: FP64 stages named after the '+'."""
+    parts = form.split("+")
+    if parts[0] == "fp64":
+        return "f64"
+    if len(parts) == 1:
+        return "f32"
+    return "f64 (" + ", ".join(parts[1:]) + ") + f32 (the rest)"
+
+
+def make_context(form: str, wl, device: int):
+    """form: "fp64", "fp32", or "fp32+<stage>+..." with stages run in FP64 (density, bk_signal,
+    bk_shot: hg_config.fp64_stages)."""
+    from hitomi_b200.api import Context
+    parts = form.split("+")
+    return Context(wl["n_mesh"], wl["boxsize"], wl["binning"], "TSC", parts[0], device=device,
+                   fp64_stages=parts[1:])
+
+
+STAGE_VARIANTS = ("fp32", "fp32+density", "fp32+bk_signal", "fp32+bk_shot", "fp32+density+bk_shot",
+                  "fp32+density+bk_signal", "fp32+bk_signal+bk_shot", "fp32+density+bk_signal+bk_shot")
+
+
+def run_stage_table(args) -> int:
+    """Per-stage error attribution of the FP32 form on the headline workload: each variant
+    runs the named stages in FP64 (hg_config.fp64_stages); per statistic, the maximum over
+    bins of |x - x_fp64| / max(|x_fp64|, 1e-12 max|x_fp64|), for the printed B (bk - sn) and
+    for its signal (bk) and shot-noise (sn) parts separately; device time per mock."""
+    import torch
+    wl = workload(args.small, args.n_mesh, int(args.n_particles))
+    pos = catalogue(wl, 2)
+    n = pos.shape[0]
+    d_pos = torch.from_numpy(pos).cuda()
+
+    def mock(ctx):
+        out = {}
+        for ell in PK_ELLS:
+            pk, _, norm = ctx.pk_box(ell)
+            out[f"pk{ell}"] = norm * pk
+        bk, sn, norm = ctx.bk_box_multi(MULTIPOLES)
+        for q, mp in enumerate(MULTIPOLES):
+            t = "".join(map(str, mp))
+            out["bk" + t] = norm * (bk[q] - sn[q])
+            out["signal" + t] = norm * bk[q]
+            out["shot" + t] = norm * sn[q]
+        return out
+
+    res, ms = {}, {}
+    for form in ("fp64",) + STAGE_VARIANTS:
+        ctx = make_context(form, wl, 0)
+        for _ in range(2):
+            ctx.set_particles_device(0, d_pos.data_ptr(), n, 24, keep=d_pos)
+            mock(ctx)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            ctx.set_particles_device(0, d_pos.data_ptr(), n, 24, keep=d_pos)
+            res[form] = mock(ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        ms[form] = e0.elapsed_time(e1) / args.steps
+        ctx.close()
+    table = {}
+    for form in STAGE_VARIANTS:
+        table[form] = {"ms_per_mock": ms[form], "fp64_over_this": ms["fp64"] / ms[form],
+                       "rel_err": {k: max_rel_err(res[form][k], res["fp64"][k]) for k in res["fp64"]}}
+    line = {"stage_table": table, "fp64_ms_per_mock": ms["fp64"], "workload": wl["name"], "steps": args.steps,
+            "metric": "max over bins of |x - x_fp64| / max(|x_fp64|, 1e-12 max |x_fp64|)"}
+    if os.environ.get("HG_BENCH_DUMP"):
+        np.savez_compressed(os.environ["HG_BENCH_DUMP"], **{f"{form}:{k}": v for form in res
+                                                            for k, v in res[form].items()})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,7 +463,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="64^3 / 2e5-particle case for quick checks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--forms", default="fp32,fp64")
+    # the first form is the headline: the FP32 form with the stages that set its error floor
+    # (density, bispectrum signal) in FP64 -- the fastest setting that meets 1e-5 per bin
+    ap.add_argument("--forms", default=f"{CHOSEN},fp32,fp64")
     ap.add_argument("--lean", action="store_true",
                     help="profiling runs: device-resident steps only (no e2e, per-kernel or CPU legs)")
     ap.add_argument("--n-mesh", type=int, default=0, help="profiling size (not the headline workload)")
@@ -394,9 +473,13 @@ def main():
     ap.add_argument("--config", type=int, default=0, help="measure another BASELINE configuration (1, 2, 3, 5)")
     ap.add_argument("--n-mocks", type=int, default=8, help="mocks timed for --config 5")
     ap.add_argument("--cpu", action="store_true", help="with --config: also time the reference's CPU code")
+    ap.add_argument("--stage-table", action="store_true",
+                    help="FP32-form error and time with each set of stages run in FP64 (not a bench line)")
     args = ap.parse_args()
     if args.config:
         return run_config(args)
+    if args.stage_table:
+        return run_stage_table(args)
     if not args.lean:
         args.warmup = max(args.warmup, 3)
     wl = workload(args.small, args.n_mesh, int(args.n_particles))
@@ -421,7 +504,7 @@ def main():
     results = {}
     timing = {}
     for form in forms:
-        ctx = Context(wl["n_mesh"], wl["boxsize"], wl["binning"], "TSC", form, device=local)
+        ctx = make_context(form, wl, local)
         clk = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local)).split(",")[0])
                            if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else local)
         clk.start()
@@ -446,7 +529,7 @@ def main():
         barrier(world)
         ms = reduce_max(ev0.elapsed_time(ev1) / args.steps, world)
         results[form] = res
-        if args.lean:
+        if args.lean or form != forms[0]:  # the other forms: device-resident rate and results only
             timing[form] = dict(ms=ms, e2e_ms=ms, launches=launches // args.steps, clocks=clocks, stats={}, d2h=0)
             ctx.close()
             continue
@@ -468,7 +551,7 @@ def main():
         # statistics; every step still copies its catalogue from pinned host memory and reads
         # its results back.  Wall clock around the whole run, the device drained on both sides.
         from hitomi_b200.batch import run_pipelined
-        ctx2 = Context(wl["n_mesh"], wl["boxsize"], wl["binning"], "TSC", form, device=local)
+        ctx2 = make_context(form, wl, local)
         ctx2.set_particles(0, h_np)
         run_mock(ctx2)
 
@@ -512,7 +595,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if head == "fp32" else "f64", "data": "synthetic",
+        "dtype": dtype_of(head), "data": "synthetic",
         "config": {"workload": wl["name"], "n_mesh": wl["n_mesh"], "n_particles": n, "boxsize": wl["boxsize"],
                    "assignment": "TSC", "n_kbin": wl["binning"].n_kbin, "kmin": wl["binning"].kmin,
                    "kmax": wl["binning"].kmax, "pk_ells": list(PK_ELLS), "bk_multipoles": [list(m) for m in MULTIPOLES],
@@ -527,14 +610,23 @@ def main():
         "roofline": roof,
     }
     if "fp64" in timing and head != "fp64":
-        errs = {f"{k[0]}{''.join(map(str, k[1:]))}": max_rel_err(results[head][k], results["fp64"][k])
-                for k in results[head]}
-        line["fp64_form"] = {"value": world * 1000.0 / timing["fp64"]["ms"], "ms_per_step": timing["fp64"]["ms"],
-                             "e2e_value": world * 1000.0 / timing["fp64"]["e2e_ms"]}
+        def errs_of(form):
+            return {f"{k[0]}{''.join(map(str, k[1:]))}": max_rel_err(results[form][k], results["fp64"][k])
+                    for k in results[form]}
+        errs = errs_of(head)
+        line["fp64_form"] = {"value": world * 1000.0 / timing["fp64"]["ms"], "ms_per_step": timing["fp64"]["ms"]}
         line["fp32_over_fp64"] = timing["fp64"]["ms"] / t["ms"]
         line["max_rel_err_fp32_vs_fp64"] = max(errs.values())
         line["rel_err_by_statistic"] = errs
-    for form in timing:
+        line["rel_err_metric"] = "max over bins of |x - x_fp64| / max(|x_fp64|, 1e-12 max|x_fp64|)"
+        for other in forms[1:]:
+            if other in ("fp64", head):
+                continue
+            e = errs_of(other)
+            line.setdefault("other_forms", {})[other] = {
+                "value": world * 1000.0 / timing[other]["ms"], "ms_per_step": timing[other]["ms"],
+                "max_rel_err_vs_fp64": max(e.values()), "rel_err_by_statistic": e}
+    for form in (f for f in timing if timing[f]["stats"]):
         line.setdefault("kernel_ms", {})[form] = {k: round(v["ms"], 4) for k, v in
                                                   sorted(timing[form]["stats"].items(), key=lambda kv: -kv[1]["ms"])}
         # algorithmic bytes (the library's per-launch model) over the measured time

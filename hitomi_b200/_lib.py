@@ -29,6 +29,13 @@ SYMBOLS = (
     "hg_zeta_survey_multi",
     "hg_survey_scalars",
     "hg_pk_survey",
+    "hg_xi_box",
+    "hg_xi_survey",
+    "hg_xi_window",
+    "hg_zeta_window",
+    "hg_zeta_window_multi",
+    "hg_batch_run",
+    "hg_batch_block_len",
     "hg_set_profiling",
     "hg_kernel_stats",
     "hg_pk_box_spectrum_static",
@@ -37,6 +44,16 @@ SYMBOLS = (
 
 HG_NGP, HG_CIC, HG_TSC, HG_PCS = 0, 1, 2, 3
 HG_FP64, HG_FP32 = 0, 1
+HG_STAGE_DENSITY, HG_STAGE_BK_SIGNAL, HG_STAGE_BK_SHOT = 1, 2, 4
+
+
+class HgMock(ctypes.Structure):
+    _fields_ = [
+        ("base", ctypes.POINTER(ctypes.c_double)),
+        ("n", ctypes.c_longlong),
+        ("stride_bytes", ctypes.c_longlong),
+        ("pos_off", ctypes.c_int),
+    ]
 
 
 class HgConfig(ctypes.Structure):
@@ -54,6 +71,7 @@ class HgConfig(ctypes.Structure):
         ("n_rbin", ctypes.c_int),
         ("periodic", ctypes.c_int),
         ("device", ctypes.c_int),
+        ("fp64_stages", ctypes.c_int),
     ]
 
 
@@ -110,6 +128,20 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_survey_scalars.restype = ctypes.c_int
     lib.hg_pk_survey.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, c_dp, c_ip, c_dp]
     lib.hg_pk_survey.restype = ctypes.c_int
+    lib.hg_xi_box.argtypes = [vp, i_, c_dp, c_ip, c_dp]
+    lib.hg_xi_box.restype = ctypes.c_int
+    lib.hg_xi_survey.argtypes = [vp, i_, d_, d_, c_dp, c_ip, c_dp]
+    lib.hg_xi_survey.restype = ctypes.c_int
+    lib.hg_xi_window.argtypes = [vp, i_, d_, c_dp, c_ip, c_dp]
+    lib.hg_xi_window.restype = ctypes.c_int
+    lib.hg_zeta_window.argtypes = [vp, i_, i_, i_, i_, d_, c_dp, c_dp, c_dp]
+    lib.hg_zeta_window.restype = ctypes.c_int
+    lib.hg_zeta_window_multi.argtypes = [vp, i_, c_ip, i_, d_, c_dp, c_dp, c_dp]
+    lib.hg_zeta_window_multi.restype = ctypes.c_int
+    lib.hg_batch_run.argtypes = [vp, ctypes.POINTER(HgMock), i_, i_, c_ip, i_, c_ip, i_, c_ip, c_dp]
+    lib.hg_batch_run.restype = ctypes.c_int
+    lib.hg_batch_block_len.argtypes = [vp, i_, i_, i_]
+    lib.hg_batch_block_len.restype = ctypes.c_longlong
     lib.hg_pk_box_spectrum_static.argtypes = [ctypes.POINTER(HgConfig), ctypes.c_void_p, ctypes.c_longlong,
                                               ctypes.c_int, c_dp, c_ip, c_dp, ctypes.c_void_p]
     lib.hg_pk_box_spectrum_static.restype = ctypes.c_int

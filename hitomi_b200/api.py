@@ -20,6 +20,20 @@ from . import _lib
 
 ASSIGN = {"NGP": _lib.HG_NGP, "CIC": _lib.HG_CIC, "TSC": _lib.HG_TSC, "PCS": _lib.HG_PCS}
 PRECISION = {"fp64": _lib.HG_FP64, "fp32": _lib.HG_FP32}
+# stages of the periodic-box pipeline an FP32 context can run in FP64 (hg_config.fp64_stages)
+STAGES = {"density": _lib.HG_STAGE_DENSITY, "bk_signal": _lib.HG_STAGE_BK_SIGNAL, "bk_shot": _lib.HG_STAGE_BK_SHOT}
+
+
+def stage_bits(stages) -> int:
+    """A stage name list ("density", "bk_signal", "bk_shot") or an int bit set, as an int."""
+    if isinstance(stages, int):
+        return stages
+    bits = 0
+    for s in stages:
+        if s not in STAGES:
+            raise HitomiError(f"unknown FP64 stage {s!r}; expected one of {sorted(STAGES)}")
+        bits |= STAGES[s]
+    return bits
 
 
 class HitomiError(RuntimeError):
@@ -52,7 +66,7 @@ def _dp(a: np.ndarray):
 
 class Context:
     def __init__(self, n_mesh, boxsize, binning: Binning, assign: str = "TSC", precision: str = "fp64",
-                 periodic: bool = False, interlace: bool = False, device: int = 0):
+                 periodic: bool = False, interlace: bool = False, device: int = 0, fp64_stages=()):
         self._lib = _lib.load()
         cfg = _lib.HgConfig()
         nm = [int(n_mesh)] * 3 if np.isscalar(n_mesh) else [int(v) for v in n_mesh]
@@ -69,6 +83,7 @@ class Context:
         cfg.rmin, cfg.rmax, cfg.n_rbin = binning.rmin, binning.rmax, binning.n_rbin
         cfg.periodic = int(bool(periodic))
         cfg.device = int(device)
+        cfg.fp64_stages = stage_bits(fp64_stages)
         self.n_mesh, self.boxsize, self.binning = nm, bs, binning
         self.precision = precision
         h = ctypes.c_void_p()
@@ -236,6 +251,83 @@ class Context:
         self._check(self._lib.hg_pk_survey(self._h, ell, alpha, vsurvey, _dp(out),
                                            nmode.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(norm)))
         return out[0::2] + 1j * out[1::2], nmode, norm.value
+
+    def _xi(self, fn, *args):
+        nr = self.binning.n_rbin
+        out = np.zeros(2 * nr)
+        nmode = np.zeros(nr, dtype=np.int32)
+        norm = ctypes.c_double()
+        self._check(fn(self._h, *args, _dp(out), nmode.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                       ctypes.byref(norm)))
+        return out[0::2] + 1j * out[1::2], nmode, norm.value
+
+    def xi_box(self, ell: int):
+        """2PCF multipole of the box: (xi_save, cells per r bin, norm); the file value is
+        norm * xi_save.real (powerspec.hpp:334-393)."""
+        return self._xi(self._lib.hg_xi_box, int(ell))
+
+    def xi_survey(self, ell: int, alpha: float, vsurvey: float):
+        return self._xi(self._lib.hg_xi_survey, int(ell), float(alpha), float(vsurvey))
+
+    def xi_window(self, ell: int, vsurvey: float):
+        return self._xi(self._lib.hg_xi_window, int(ell), float(vsurvey))
+
+    def zeta_window_multi(self, multipoles, vsurvey: float, ith_rbin: int = -1):
+        """Window 3PCF multipoles of the randoms (slot 1): arrays [m][rows][n_rbin] and norm."""
+        nr = self.binning.n_rbin
+        rows = nr if ith_rbin < 0 else 1
+        m = len(multipoles)
+        ells = np.array([v for mp in multipoles for v in mp], dtype=np.int32)
+        z = np.zeros(2 * m * rows * nr)
+        sn = np.zeros(2 * m * rows * nr)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_zeta_window_multi(self._h, m, ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                   ith_rbin, float(vsurvey), _dp(z), _dp(sn), ctypes.byref(norm)))
+        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nr)
+        return c(z), c(sn), norm.value
+
+    def batch_run(self, mocks, pk_ells=(), bk_multipoles=(), zeta_multipoles=()):
+        """Box statistics of several catalogues through hg_batch_run (the next catalogue is
+        copied to the GPU while the current one is measured).  mocks: (n, fields) float64
+        arrays of structs with x y z first.  Returns one dict per mock: "pk" [n_pk][n_kbin],
+        "pk_norm" [n_pk], "bk", "bk_sn" [n_bk][n_kbin][n_kbin], "bk_norm", "zeta", "zeta_sn"
+        [n_zeta][n_rbin][n_rbin], "zeta_norm" (complex raw sums and their norms)."""
+        arrs = [np.ascontiguousarray(m, dtype=np.float64) for m in mocks]
+        ms = (_lib.HgMock * len(arrs))()
+        for i, a in enumerate(arrs):
+            ms[i].base = _dp(a)
+            ms[i].n = a.shape[0]
+            ms[i].stride_bytes = a.shape[1] * 8
+            ms[i].pos_off = 0
+        pk = np.array(list(pk_ells), dtype=np.int32)
+        bk = np.array([v for mp in bk_multipoles for v in mp], dtype=np.int32)
+        zt = np.array([v for mp in zeta_multipoles for v in mp], dtype=np.int32)
+        npk, nbk, nz = len(pk), len(bk) // 3, len(zt) // 3
+        blk = int(self._lib.hg_batch_block_len(self._h, npk, nbk, nz))
+        out = np.zeros(blk * len(arrs))
+        ip = lambda v: v.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        self._check(self._lib.hg_batch_run(self._h, ms, len(arrs), npk, ip(pk), nbk, ip(bk), nz, ip(zt), _dp(out)))
+        nk, nr = self.binning.n_kbin, self.binning.n_rbin
+        res = []
+        for i in range(len(arrs)):
+            o = out[i * blk:(i + 1) * blk]
+            r, p = {}, 0
+            c = lambda v, *shape: (v[0::2] + 1j * v[1::2]).reshape(shape)
+            r["pk"] = c(o[p:p + 2 * npk * nk], npk, nk)
+            p += 2 * npk * nk
+            r["pk_norm"] = o[p:p + npk].copy()
+            p += npk
+            if nbk:
+                sz = 2 * nbk * nk * nk
+                r["bk"], r["bk_sn"] = c(o[p:p + sz], nbk, nk, nk), c(o[p + sz:p + 2 * sz], nbk, nk, nk)
+                r["bk_norm"] = float(o[p + 2 * sz])
+                p += 2 * sz + 1
+            if nz:
+                sz = 2 * nz * nr * nr
+                r["zeta"], r["zeta_sn"] = c(o[p:p + sz], nz, nr, nr), c(o[p + sz:p + 2 * sz], nz, nr, nr)
+                r["zeta_norm"] = float(o[p + 2 * sz])
+            res.append(r)
+        return res
 
     def last_timing(self):
         ms = ctypes.c_double()

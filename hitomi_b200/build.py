@@ -12,7 +12,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhitomi_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", "hg_engine.cu"), os.path.join(HERE, "csrc", "hg_static.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in
+           ("hg_engine_fp32.cu", "hg_engine_fp64.cu", "hg_api.cu", "hg_static.cu")]
+OBJDIR = os.path.join(HERE, "_build")
 HEADERS = [
     os.path.join(HERE, "csrc", f)
     for f in os.listdir(os.path.join(HERE, "csrc"))
@@ -33,19 +35,29 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile each translation unit to an object (in parallel: the two engine precisions
+    are the long ones), then link the shared library."""
     if not force and up_to_date():
         return LIB
-    cmd = [
-        nvcc(),
+    os.makedirs(OBJDIR, exist_ok=True)
+    common = [
         "-gencode", "arch=compute_100a,code=sm_100a",
         "-O3", "-lineinfo", "-std=c++17",
-        "-Xcompiler", "-fPIC", "-shared",
+        "-Xcompiler", "-fPIC",
         "-I", os.path.join(ROOT, "include"),
-        "-o", LIB + ".tmp",
-    ] + SOURCES
+    ]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+        common.append("-Xptxas=-v")
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(OBJDIR, os.path.basename(src).replace(".cu", ".o"))
+        objs.append(obj)
+        procs.append(subprocess.Popen([nvcc()] + common + ["--split-compile=4", "-c", src, "-o", obj]))
+    bad = [src for src, p in zip(SOURCES, procs) if p.wait() != 0]
+    if bad:
+        raise subprocess.CalledProcessError(1, "nvcc " + " ".join(os.path.basename(b) for b in bad))
+    subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
+                    "-o", LIB + ".tmp"] + objs, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

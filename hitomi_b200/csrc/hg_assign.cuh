@@ -24,6 +24,9 @@
 #include "hg_common.cuh"
 
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 struct AssignGeom {
     int n[3];
@@ -978,4 +981,5 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
     });
 }
 
+}  // namespace HG_TU_NS
 }  // namespace hg

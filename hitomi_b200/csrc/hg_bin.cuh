@@ -8,6 +8,9 @@
 #include "hg_common.cuh"
 
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 // Per-axis tables indexed by array index i (mode n = wrap(i)):
 //   tw[i] = sinc(pi w / n)   with w = (int)(n dk / dk + 1e-5)   (window, field.hpp:664-675)
@@ -308,4 +311,5 @@ __global__ void k_pk_bin_terms(PkTerms<T> terms, F2 f2, Grid g, AxisTabs tabs, i
         if (scnt[q]) atomicAdd(&nmode[q], scnt[q]);
 }
 
+}  // namespace HG_TU_NS
 }  // namespace hg

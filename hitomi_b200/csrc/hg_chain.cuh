@@ -20,6 +20,9 @@
 #include "hg_fft.cuh"
 
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 // wrapped mode n of line position p on an axis of M points; compact index c = n + s
 __device__ __forceinline__ int pos_to_c(int p, int M, int s) {
@@ -157,4 +160,5 @@ inline cudaError_t launch_chain_x(int L, cplx<T> *t2, const cplx<T> *G, int ns, 
     }
 }
 
+}  // namespace HG_TU_NS
 }  // namespace hg

@@ -14,7 +14,14 @@
 #define HG_PI 3.14159265358979323846
 #endif
 
+#ifndef HG_TU_NS
+#error "define HG_TU_NS (a namespace name unique to this translation unit) before including"
+#endif
+
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 template <typename T>
 struct cplx {
@@ -180,4 +187,5 @@ __host__ __device__ inline zd ylm_reduced(int l, int m, double x, double y, doub
     return mk<double>(sgn * plm * ex * norm, -sgn * plm * ey * norm);
 }
 
+}  // namespace HG_TU_NS
 }  // namespace hg

@@ -1,8 +1,11 @@
-// hg_engine.cu -- the estimator engine behind the C ABI in include/hitomi_gpu.h.
+// hg_engine.cuh -- the estimator engine behind the C ABI in include/hitomi_gpu.h.
 //
 // One Engine<T> per context; T = double for the plain FP64 form, float for the chosen
 // FP32 form (FP32 mesh / FFT / fields; FP64 assignment accumulators, bin sums, shell
-// sums, scalars and shot-noise histograms).
+// sums, scalars and shot-noise histograms).  Each precision is instantiated in its own
+// translation unit (hg_engine_fp32.cu, hg_engine_fp64.cu); they meet only through the
+// hg_ctx interface (hg_ctx.hpp).  An FP32 context whose hg_config.fp64_stages is non-zero
+// owns an FP64 engine on the same stream and hands it the stages named there.
 //
 // Periodic-box pipeline for one catalogue (cached until the particles change):
 //   assignment (hg_assign.cuh) -> rho(x) -> r2c forward FFT (z, y, x passes) -> delta(k)
@@ -22,6 +25,7 @@
 // mesh; its last pass is fused with a histogram over integer n^2 = |x/dr|^2 (cubic cells),
 // which turns sum_x j_l1(k1 r) j_l2(k2 r) xi Yhat1 Yhat2 into a sum over distinct radii.
 #include "hitomi_gpu.h"
+#include "hg_ctx.hpp"
 #include "hg_common.cuh"
 #include "hg_fft.cuh"
 #include "hg_assign.cuh"
@@ -31,6 +35,9 @@
 #include "hg_special.hpp"
 
 #include <cub/cub.cuh>
+
+#include <exception>
+#include <thread>
 
 #include <algorithm>
 #include <array>
@@ -76,10 +83,6 @@ inline X *dp(const DBuf &b) {
     return reinterpret_cast<X *>(b.p);
 }
 
-struct HgError {
-    std::string msg;
-};
-
 #define HG_CK(x)                                                                                    \
     do {                                                                                            \
         cudaError_t e_ = (x);                                                                       \
@@ -107,36 +110,23 @@ struct Fam {
     bool operator<(const Fam &o) const { return l != o.l ? l < o.l : m < o.m; }
 };
 
-struct MP {
-    int l1, l2, L;
-};
-
 }  // namespace
 
-struct hg_ctx {
-    hg_config cfg;
-    std::string err;
-    double last_ms = 0.0;
-    long long last_launches = 0;
-    virtual ~hg_ctx() {}
-    virtual void set_particles(int slot, const double *base, long long n, long long stride, int pos_off, int los_off,
-                               int w_off, bool on_device) = 0;
-    virtual void set_profiling(bool on) = 0;
-    virtual std::string kernel_stats() = 0;
-    virtual void pk_box(int ell, double *pk_save, int *n_mode, double *norm) = 0;
-    virtual void bk_box_multi(const std::vector<MP> &mps, int ith, double *bk_save, double *sn_save,
-                              double *norm) = 0;
-    virtual void zeta_box_multi(const std::vector<MP> &mps, int ith, double *zeta_save, double *sn_save,
-                                double *norm) = 0;
-    virtual void survey_scalars(double *alpha, double *vs, double *nbar, double *wd, double *wr) = 0;
-    virtual void pk_survey(int ell, double alpha, double vs, double *pk_save, int *n_mode, double *norm) = 0;
-    virtual void bk_survey_multi(const std::vector<MP> &mps, int ith, double alpha, double vs, double *bk_save,
-                                 double *sn_save, double *norm) = 0;
-    virtual void zeta_survey_multi(const std::vector<MP> &mps, int ith, double alpha, double vs, double *zeta_save,
-                                   double *sn_save, double *norm) = 0;
-};
 
 namespace {
+
+// element-wise precision change of a complex array (the density spectrum between the
+// FP32 engine and its FP64 stages)
+template <typename S, typename D>
+__global__ void k_convert_spec(const cplx<S> *__restrict__ in, cplx<D> *__restrict__ out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const cplx<S> v = in[i];
+        cplx<D> w;
+        w.x = (D)v.x;
+        w.y = (D)v.y;
+        out[i] = w;
+    }
+}
 
 template <typename T>
 struct Engine : public hg_ctx {
@@ -229,6 +219,7 @@ struct Engine : public hg_ctx {
     // shot-noise state
     DBuf xi;
     bool xi_valid = false;
+    double xi_k0 = 0.0;  // the k = 0 product the cached box correlation field was made with
     std::vector<int> orbit_lines, orbit_n2xy;  // per orbit: 4 (line, mirror) pairs; n_x^2 + n_y^2
     DBuf d_orbit_lines, d_orbit_n2xy;
     long long n2dim = 0;
@@ -243,7 +234,10 @@ struct Engine : public hg_ctx {
     // SF_DELTA = n_D - alpha n_R with weights Yhat w (field.hpp:186-228) and SF_SN = n_D +
     // alpha^2 n_R with weights conj(Yhat) w^2 (field.hpp:249-284); m = 0 half spectra, m != 0
     // full ones (m < 0 as mirrors of m > 0); keyed (kind, l, m), valid for sf_alpha.
-    enum { SF_DELTA = 0, SF_SN = 1 };
+    // SF_WIN / SF_WIN_SN: the same fields of the randoms alone, n_R with weights Yhat w
+    // (calcYlmWeightedDensity field.hpp:230-247) and conj(Yhat) w^2
+    // (calcYlmWeightedDensityForThreePointWindowFunctionShotnoise field.hpp:286-306)
+    enum { SF_DELTA = 0, SF_SN = 1, SF_WIN = 2, SF_WIN_SN = 3 };
     DBuf smesh_re, smesh_im, dmesh, psum_part, sfield_tmp;
     // both catalogues binned once per assignment offset (0, and 1/2 cell for interlacing);
     // every weighting reuses them
@@ -280,6 +274,11 @@ struct Engine : public hg_ctx {
     std::map<std::tuple<int, int, int, int, int, int, int>, std::vector<double>> zpairs;  // (a, b, row, L, M)
 
     long long launches = 0;
+
+    // FP64 engine of the stages named in cfg.fp64_stages (FP32 form only), on this stream
+    std::unique_ptr<hg_ctx> hi;
+    int fp64_stages = 0;
+    bool own_stream = true;
 
     // per-kernel device timing (CUDA events on the context stream) and modelled bytes
     bool profiling = false;
@@ -348,9 +347,21 @@ struct Engine : public hg_ctx {
         }
         build_lut();
         HG_CK(cudaStreamSynchronize(st));
+        if (sizeof(T) == 4 && c.fp64_stages != 0) {
+            HG_REQUIRE((c.fp64_stages & ~(HG_STAGE_DENSITY | HG_STAGE_BK_SIGNAL | HG_STAGE_BK_SHOT)) == 0,
+                       "fp64_stages holds unknown HG_STAGE_* bits");
+            hg_config hc = c;
+            hc.precision = HG_FP64;
+            hc.fp64_stages = 0;
+            hi.reset(make_engine_fp64(hc));
+            hi->stage_adopt_stream(st);
+            fp64_stages = c.fp64_stages;
+        }
     }
 
     ~Engine() override {
+        hi.reset();  // it runs on this engine's stream
+        batch_release();
         if (st) cudaStreamSynchronize(st);
         for (auto e : ev_pool) cudaEventDestroy(e);
         for (auto &r : pend) {
@@ -359,7 +370,7 @@ struct Engine : public hg_ctx {
         }
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        if (st) cudaStreamDestroy(st);
+        if (st && own_stream) cudaStreamDestroy(st);
     }
 
     // ------------------------------------------------------------------ profiling
@@ -404,14 +415,26 @@ struct Engine : public hg_ctx {
     void set_profiling(bool on) override {
         profiling = on;
         if (on) kagg.clear();
+        if (hi) hi->set_profiling(on);
     }
     std::string kernel_stats() override {
+        prof_flush();
         std::string out;
         char line[256];
         for (auto &kv : kagg) {
             snprintf(line, sizeof(line), "%s\t%lld\t%.6f\t%.6e\n", kv.first.c_str(), kv.second.launches, kv.second.ms,
                      kv.second.bytes);
             out += line;
+        }
+        if (hi) {  // the FP64 stages, under their own names
+            std::string h = hi->kernel_stats();
+            size_t p0 = 0;
+            while (p0 < h.size()) {
+                size_t p1 = h.find('\n', p0);
+                if (p1 == std::string::npos) p1 = h.size();
+                if (p1 > p0) out += "fp64:" + h.substr(p0, p1 - p0) + "\n";
+                p0 = p1 + 1;
+            }
         }
         return out;
     }
@@ -521,6 +544,8 @@ struct Engine : public hg_ctx {
         S.set = true;
         HG_CK(cudaStreamSynchronize(st));
         invalidate();
+        // the FP64 stages read the same device copy in place
+        if (hi) hi->set_particles(s, reinterpret_cast<const double *>(S.base()), n, stride, pos_off, los_off, w_off, true);
     }
 
     // statistics state derived from the current source (the catalogue itself is unchanged)
@@ -541,7 +566,7 @@ struct Engine : public hg_ctx {
 
     // select the box (kind 0) or the survey with a given alpha (kind 1) as the source
     void set_source(int kind, double alpha) {
-        if (kind != src_kind || (kind == 1 && alpha != src_alpha)) {
+        if (kind != src_kind || (kind != 0 && alpha != src_alpha)) {
             invalidate_stats();
             src_kind = kind;
             src_alpha = alpha;
@@ -550,14 +575,18 @@ struct Engine : public hg_ctx {
             box_density();
             dsrc = SpecK{half_spec(), delta0, 0.0};
         } else {
-            dsrc = sfield(SF_DELTA, 0, 0, alpha);
+            dsrc = sfield(delta_kind(), 0, 0, alpha);
         }
     }
+    // the Yhat-weighted field the current survey source is made of: D - alpha R, or the
+    // randoms alone for the window functions (source kind 2)
+    int delta_kind() const { return src_kind == 2 ? SF_WIN : SF_DELTA; }
+    int sn_kind() const { return src_kind == 2 ? SF_WIN_SN : SF_SN; }
 
     // the spectrum whose IFFT / W / V is G for a G key
     SpecK g_source(const GK &gk) {
         if (src_kind == 0) return SpecK{half_spec(), delta0, 0.0};
-        return sfield(SF_DELTA, gk.first, gk.second, src_alpha);
+        return sfield(delta_kind(), gk.first, gk.second, src_alpha);
     }
 
     void invalidate() {
@@ -616,6 +645,7 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(defcnt.p, 0, sizeof(unsigned) * ns, st));
         long long o = 0;
         for (int q = 0; q < ns; q++) {
+            if (srcs[q].n == 0) continue;  // an empty catalogue (no data for a window function)
             Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0};
             kb("assign_bin_count", double(srcs[q].n) * 24.0);
             k_bin_count<<<(unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 8), 256, 0, st>>>(
@@ -639,6 +669,7 @@ struct Engine : public hg_ctx {
         long long o = 0, nsum = 0;
         for (int q = 0; q < ns; q++) nsum += srcs[q].n;
         for (int q = 0; q < ns; q++) {
+            if (srcs[q].n == 0) continue;
             Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0};
             kb("assign_bin_scatter", double(srcs[q].n) * 24.0 + rec_bytes * double(srcs[q].n) / double(nsum));
             k_bin_scatter<MK><<<(unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 16), 256, 0, st>>>(
@@ -800,6 +831,13 @@ struct Engine : public hg_ctx {
 
     void box_density() {
         if (dens_valid) return;
+        if (hi && (fp64_stages & HG_STAGE_DENSITY)) {  // computed by the FP64 engine, narrowed
+            double d0, n0, m0;
+            const void *Hh = hi->stage_density(&d0, &n0, &m0);
+            launches += hi->stage_take_launches();
+            stage_import_density(Hh, true, d0, n0, m0);
+            return;
+        }
         Slot &S = slot[0];
         HG_REQUIRE(S.set, "no particles: call hg_set_particles(ctx, 0, ...) first");
         AssignGeom ag = make_geom(0.0);
@@ -938,6 +976,13 @@ struct Engine : public hg_ctx {
     // powerspec.hpp:273-332
     void pk_box(int ell, double *pk_save, int *n_mode, double *norm) override {
         HG_REQUIRE(ell >= 0, "ell must be >= 0");
+        if (hi && (fp64_stages & HG_STAGE_DENSITY)) {  // binned from the FP64 spectrum
+            begin();
+            hi->pk_box(ell, pk_save, n_mode, norm);
+            launches += hi->stage_take_launches();
+            end();
+            return;
+        }
         begin();
         box_density();
         if (!pk_cache.count(ell)) {
@@ -1301,16 +1346,20 @@ struct Engine : public hg_ctx {
     // spectrum P is real, so the even and odd kz planes travel as the real and imaginary
     // parts of one complex field (k_synth_pairs: [n0][n1][n2/2] in xi): half the data
     // through the x and y passes; the histogram kernel separates them before its z pass.
-    void ensure_xi() {
+    // k0prod: (f1 conj f2)(k = 0), delta0 N0 for the bispectrum shot noise (dn against the
+    // density N, bispec.hpp:913-921), delta0^2 for the 2PCF (dn against itself)
+    void ensure_xi() { ensure_xi(delta0 * N0); }
+    void ensure_xi(double k0prod) {
         HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
-                   "bispectrum / 3PCF shot noise needs equal cell sizes on all axes");
+                   "bispectrum / 3PCF shot noise and the 2PCF need equal cell sizes on all axes");
         build_orbits();
-        if (xi_valid) return;
+        if (xi_valid && xi_k0 == k0prod) return;
+        xi_k0 = k0prod;
         const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], nh = n2 / 2;
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
         const double S = double(slot[0].n);
-        LdXiHat<T> ld{half_spec(), n2, xtabs, S, delta0 * N0, invV};
+        LdXiHat<T> ld{half_spec(), n2, xtabs, S, k0prod, invV};
         const long long yz = (long long)n1 * nh, tot = (long long)n0 * yz;
         unsigned blocks = (unsigned)std::min<long long>(grid1(tot, 256), 148 * 16);
         kb("xi_synth", double(tot) * sizeof(C) * 2.0);
@@ -1506,7 +1555,7 @@ struct Engine : public hg_ctx {
     // (bispec.hpp:1118-1170 box, 255-320 survey), [q][ns][ns] complex.  Chain families:
     // every self-paired family per G key, then a greedy cover of the remaining pairs.
     std::vector<std::vector<double>> bk_main(const std::vector<MP> &mps) {
-        const bool survey = (src_kind == 1);
+        const bool survey = (src_kind >= 1);
         prepare_shells();
         const int ns = shells.ns;
         const double dV = g.volume / double(g.ntot);
@@ -1627,8 +1676,50 @@ struct Engine : public hg_ctx {
         set_source(0, 0.0);
         const int ns = cfg.n_kbin;
         const double Np = double(slot[0].n);
-        const double dV = g.volume / double(g.ntot);
-        std::vector<std::vector<double>> B = bk_main(mps);
+        std::vector<std::vector<double>> B, SN;
+        if (hi && (fp64_stages & HG_STAGE_BK_SIGNAL)) {
+            hi_density();
+            B = hi->stage_bk_signal(mps);
+        } else {
+            B = bk_main(mps);
+        }
+        if (hi && (fp64_stages & HG_STAGE_BK_SHOT)) {
+            hi_density();
+            SN = hi->stage_bk_shot(mps);
+        } else {
+            SN = bk_shot(mps);
+        }
+        if (hi) launches += hi->stage_take_launches();
+        const int r0 = (ith < 0) ? 0 : ith, r1 = (ith < 0) ? ns : ith + 1;
+        const int rows = r1 - r0;
+        for (size_t q = 0; q < mps.size(); q++)
+            for (int i1 = r0; i1 < r1; i1++)
+                for (int i2 = 0; i2 < ns; i2++) {
+                    long long o = ((long long)q * rows + (i1 - r0)) * ns + i2;
+                    bk_save[2 * o] = B[q][2 * (i1 * ns + i2)];
+                    bk_save[2 * o + 1] = B[q][2 * (i1 * ns + i2) + 1];
+                    sn_save[2 * o] = SN[q][2 * (i1 * ns + i2)];
+                    sn_save[2 * o + 1] = SN[q][2 * (i1 * ns + i2) + 1];
+                }
+        if (norm) {
+            double nv = g.volume / Np / Np;
+            nv *= (g.volume / Np);
+            *norm = nv;
+        }
+        end();
+    }
+
+    // the current box density on the FP64 engine: its own (HG_STAGE_DENSITY) or this one's
+    // spectrum widened
+    void hi_density() {
+        if (!hi->stage_density_ready()) hi->stage_import_density(H.p, sizeof(T) == 8, delta0, N0, dens_mass);
+    }
+
+    // Box bispectrum shot noise (bispec.hpp:909-1078) of the current source: constant and P
+    // terms, then the correlation-field term; [q][ns][ns] complex, all rows.
+    std::vector<std::vector<double>> bk_shot(const std::vector<MP> &mps) {
+        const int ns = cfg.n_kbin;
+        const double Np = double(slot[0].n);
         std::vector<std::vector<Combo>> cmb;
         for (const auto &mp : mps) cmb.push_back(combos_of(mp));
         // shot noise (bispec.hpp:909-1078): P terms, constant term, xi term
@@ -1688,23 +1779,166 @@ struct Engine : public hg_ctx {
         ensure_histograms(mps);
         for (size_t q = 0; q < mps.size(); q++)
             bk_sn_xi(mps[q], dp<double>(*hist_mp[{mps[q].l1, mps[q].l2, mps[q].L}]), SN[q]);
-        const int r0 = (ith < 0) ? 0 : ith, r1 = (ith < 0) ? ns : ith + 1;
-        const int rows = r1 - r0;
-        for (size_t q = 0; q < mps.size(); q++)
-            for (int i1 = r0; i1 < r1; i1++)
-                for (int i2 = 0; i2 < ns; i2++) {
-                    long long o = ((long long)q * rows + (i1 - r0)) * ns + i2;
-                    bk_save[2 * o] = B[q][2 * (i1 * ns + i2)];
-                    bk_save[2 * o + 1] = B[q][2 * (i1 * ns + i2) + 1];
-                    sn_save[2 * o] = SN[q][2 * (i1 * ns + i2)];
-                    sn_save[2 * o + 1] = SN[q][2 * (i1 * ns + i2) + 1];
-                }
-        if (norm) {
-            double nv = g.volume / Np / Np;
-            nv *= (g.volume / Np);
-            *norm = nv;
+        return SN;
+    }
+
+    // ------------------------------------------------------------------ batch (hg_batch_run)
+    // Two device catalogue buffers: mock i is measured from one while a host thread stages
+    // mock i + 1 through two pinned chunks into the other on the copy stream.
+    DBuf bcat[2];
+    cudaStream_t cst = nullptr;
+    cudaEvent_t cev[2] = {nullptr, nullptr};
+    void *pinned[2] = {nullptr, nullptr};
+    static constexpr size_t PIN_CHUNK = 32u << 20;
+
+    void batch_release() {
+        if (cst) cudaStreamSynchronize(cst);
+        for (int k = 0; k < 2; k++) {
+            if (pinned[k]) cudaFreeHost(pinned[k]);
+            if (cev[k]) cudaEventDestroy(cev[k]);
+            pinned[k] = nullptr;
+            cev[k] = nullptr;
         }
-        end();
+        if (cst) cudaStreamDestroy(cst);
+        cst = nullptr;
+    }
+
+    // copy one catalogue into a device buffer (host thread: set_device first)
+    void batch_upload(const hg_mock &m, void *dst) {
+        HG_CK(cudaSetDevice(cfg.device));
+        const size_t bytes = (size_t)m.n * (size_t)m.stride_bytes;
+        const unsigned char *src = reinterpret_cast<const unsigned char *>(m.base);
+        int k = 0;
+        for (size_t o = 0; o < bytes; o += PIN_CHUNK, k ^= 1) {
+            const size_t sz = std::min(PIN_CHUNK, bytes - o);
+            HG_CK(cudaEventSynchronize(cev[k]));  // this chunk's previous copy is done
+            memcpy(pinned[k], src + o, sz);
+            HG_CK(cudaMemcpyAsync(reinterpret_cast<unsigned char *>(dst) + o, pinned[k], sz, cudaMemcpyHostToDevice,
+                                  cst));
+            HG_CK(cudaEventRecord(cev[k], cst));
+        }
+        HG_CK(cudaStreamSynchronize(cst));
+    }
+
+    void batch_run(const hg_mock *m, int n, const std::vector<int> &pk_ells, const std::vector<MP> &bk,
+                   const std::vector<MP> &zeta, double *out) override {
+        for (int e : pk_ells) HG_REQUIRE(e >= 0, "ell must be >= 0");
+        if (!bk.empty()) check_multipoles(bk);
+        if (!zeta.empty()) check_multipoles(zeta);
+        size_t maxb = 0;
+        for (int i = 0; i < n; i++) {
+            HG_REQUIRE(m[i].base != nullptr && m[i].n > 0, "a mock has no particles");
+            HG_REQUIRE(m[i].stride_bytes >= 24 && m[i].stride_bytes % 8 == 0 && m[i].pos_off >= 0 &&
+                           (m[i].pos_off + 3) * 8 <= m[i].stride_bytes,
+                       "a mock's stride_bytes / pos_off do not describe {x, y, z} doubles");
+            maxb = std::max(maxb, (size_t)m[i].n * (size_t)m[i].stride_bytes);
+        }
+        // every allocation before the pipeline starts (no cudaMalloc beside running work)
+        HG_CK(bcat[0].ensure(maxb));
+        if (n > 1) HG_CK(bcat[1].ensure(maxb));
+        if (!cst) {
+            HG_CK(cudaStreamCreateWithFlags(&cst, cudaStreamNonBlocking));
+            for (int k = 0; k < 2; k++) {
+                HG_CK(cudaEventCreateWithFlags(&cev[k], cudaEventDisableTiming));
+                HG_CK(cudaHostAlloc(&pinned[k], PIN_CHUNK, cudaHostAllocDefault));
+            }
+        }
+        const long long blk = batch_block_len(cfg, (int)pk_ells.size(), (int)bk.size(), (int)zeta.size());
+        const int nk = cfg.n_kbin, nr = cfg.n_rbin;
+        std::exception_ptr up_err;
+        auto upload = [&](int i) {
+            try {
+                batch_upload(m[i], bcat[i & 1].p);
+            } catch (...) {
+                up_err = std::current_exception();
+            }
+        };
+        upload(0);
+        if (up_err) std::rethrow_exception(up_err);
+        double total_ms = 0.0;
+        long long total_launches = 0;
+        for (int i = 0; i < n; i++) {
+            std::thread next;
+            if (i + 1 < n) next = std::thread(upload, i + 1);
+            try {
+                set_particles(0, reinterpret_cast<const double *>(bcat[i & 1].p), m[i].n, m[i].stride_bytes,
+                              m[i].pos_off, -1, -1, true);
+                double *o = out + (long long)i * blk;
+                for (size_t q = 0; q < pk_ells.size(); q++) {
+                    pk_box(pk_ells[q], o + 2LL * q * nk, nullptr, o + 2LL * pk_ells.size() * nk + q);
+                    total_ms += last_ms;
+                    total_launches += last_launches;
+                }
+                o += 2LL * pk_ells.size() * nk + pk_ells.size();
+                if (!bk.empty()) {
+                    const long long sz = 2LL * bk.size() * nk * nk;
+                    bk_box_multi(bk, -1, o, o + sz, o + 2 * sz);
+                    total_ms += last_ms;
+                    total_launches += last_launches;
+                    o += 2 * sz + 1;
+                }
+                if (!zeta.empty()) {
+                    const long long sz = 2LL * zeta.size() * nr * nr;
+                    zeta_box_multi(zeta, -1, o, o + sz, o + 2 * sz);
+                    total_ms += last_ms;
+                    total_launches += last_launches;
+                }
+            } catch (...) {
+                if (next.joinable()) next.join();
+                throw;
+            }
+            if (next.joinable()) next.join();
+            if (up_err) std::rethrow_exception(up_err);
+        }
+        last_ms = total_ms;
+        last_launches = total_launches;
+    }
+
+    // ------------------------------------------------------------------ stages (hg_ctx.hpp)
+    void stage_adopt_stream(void *stream) override {
+        if (st && own_stream) {
+            HG_CK(cudaStreamSynchronize(st));
+            HG_CK(cudaStreamDestroy(st));
+        }
+        st = reinterpret_cast<cudaStream_t>(stream);
+        own_stream = false;
+    }
+    const void *stage_density(double *d0, double *n0, double *m0) override {
+        box_density();
+        *d0 = delta0;
+        *n0 = N0;
+        *m0 = dens_mass;
+        return H.p;
+    }
+    bool stage_density_ready() const override { return dens_valid; }
+    void stage_import_density(const void *src, bool src_fp64, double d0, double n0, double m0) override {
+        const long long n = (long long)g.n[0] * g.n[1] * (g.n[2] / 2 + 1);
+        HG_CK(H.ensure(sizeof(C) * n));
+        const unsigned blocks = (unsigned)std::min<long long>(grid1(n, 256), 148 * 16);
+        kb("stage_convert", double(n) * (sizeof(C) + (src_fp64 ? 16.0 : 8.0)));
+        if (src_fp64)
+            k_convert_spec<double, T><<<blocks, 256, 0, st>>>(reinterpret_cast<const cplx<double> *>(src), dp<C>(H), n);
+        else
+            k_convert_spec<float, T><<<blocks, 256, 0, st>>>(reinterpret_cast<const cplx<float> *>(src), dp<C>(H), n);
+        ke();
+        delta0 = d0;
+        N0 = n0;
+        dens_mass = m0;
+        dens_valid = true;  // statistics of the previous density were dropped by set_particles
+        pk_cache.clear();
+    }
+    std::vector<std::vector<double>> stage_bk_signal(const std::vector<MP> &mps) override {
+        set_source(0, 0.0);
+        return bk_main(mps);
+    }
+    std::vector<std::vector<double>> stage_bk_shot(const std::vector<MP> &mps) override {
+        set_source(0, 0.0);
+        return bk_shot(mps);
+    }
+    long long stage_take_launches() override {
+        const long long l = launches;
+        launches = 0;
+        return l;
     }
 
     // ------------------------------------------------------------------ 3PCF (box)
@@ -1929,7 +2163,7 @@ struct Engine : public hg_ctx {
     // zeta_raw = sum_(m1,m2,M) w i^(l1+l2) dV sum_x F1 F2 G_LM  (bispec.hpp:1354-1378 box,
     // 545-575 survey): [q][rows][ns] complex
     std::vector<std::vector<double>> zeta_main(const std::vector<MP> &mps, int ith) {
-        const bool survey = (src_kind == 1);
+        const bool survey = (src_kind >= 1);
         const int ns = cfg.n_rbin;
         const double dV = g.volume / double(g.ntot);
         const int rows = (ith < 0) ? ns : 1;
@@ -2042,6 +2276,7 @@ struct Engine : public hg_ctx {
     // FP64 particle sums (block partials added on the host in block order)
     std::vector<double> particle_sums(int s, const PSumSpec &q) {
         const PartSrc src = survey_src(s, false, 0, 0, 1.0);
+        if (src.n == 0) return std::vector<double>(2 * q.n, 0.0);
         const int nb = (int)std::min<long long>(grid1(src.n, 256), 148 * 8);
         HG_CK(psum_part.ensure(sizeof(double) * 2 * HG_PSUM_MAX * nb));
         kb("particle_sums", double(src.n) * 32.0);
@@ -2149,6 +2384,7 @@ struct Engine : public hg_ctx {
     double max_weight(int s) {
         if (wmax_cache[s] >= 0.0) return wmax_cache[s];
         const PartSrc src = survey_src(s, false, 0, 0, 1.0);
+        if (src.n == 0) return wmax_cache[s] = 0.0;
         const int nb = (int)std::min<long long>(grid1(src.n, 256), 148 * 8);
         HG_CK(psum_part.ensure(sizeof(double) * nb));
         kb("particle_sums", double(src.n) * 8.0);
@@ -2173,7 +2409,7 @@ struct Engine : public hg_ctx {
         fw.s[0] = srcs[0];
         fw.s[1] = srcs[1];
         for (int q = 0; q < 2; q++) {  // harmonic-weighted sources: weights precomputed in order
-            if (!srcs[q].ylm_on || srcs[q].cw) continue;
+            if (!srcs[q].ylm_on || srcs[q].cw || srcs[q].n == 0) continue;
             HG_CK(cwbuf[q].ensure(sizeof(double2) * std::max<long long>(srcs[q].n, 1)));
             const unsigned nb = (unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 16);
             kb("particle_sums", double(srcs[q].n) * (16.0 + 32.0));
@@ -2261,8 +2497,12 @@ struct Engine : public hg_ctx {
         std::vector<PartSrc> srcs;
         if (kind == SF_DELTA)
             srcs = {survey_src(0, ylm, l, m, 1.0), survey_src(1, ylm, l, m, -alpha)};
-        else
+        else if (kind == SF_SN)
             srcs = {survey_src(0, ylm, l, m, 1.0, 2, true), survey_src(1, ylm, l, m, alpha * alpha, 2, true)};
+        else if (kind == SF_WIN)  // the data (if any were binned with the randoms) weigh nothing
+            srcs = {survey_src(0, ylm, l, m, 0.0), survey_src(1, ylm, l, m, 1.0)};
+        else
+            srcs = {survey_src(0, ylm, l, m, 0.0, 2, true), survey_src(1, ylm, l, m, 1.0, 2, true)};
         HG_CK(smesh_re.ensure(sizeof(T) * g.ntot));
         if (!real) HG_CK(smesh_im.ensure(sizeof(T) * g.ntot));
         const double dV = g.volume / double(g.ntot);
@@ -2341,6 +2581,31 @@ struct Engine : public hg_ctx {
         return {it->second[2 * (L + M)], it->second[2 * (L + M) + 1]};
     }
 
+    // S_LM = sum_D w^2 Yhat_LM + alpha^2 sum_R w^2 Yhat_LM (calcShotNoiseForPowerspectrum,
+    // field.hpp:1164-1185), or sum_R w^2 Yhat_LM alone (rand_only:
+    // calcShotNoiseForTwoPointWindowCorrelationFunction, field.hpp:1202-1217); any M
+    std::array<double, 2> survey_s2(int L, int M, double alpha, bool rand_only) {
+        const int am = M < 0 ? -M : M;
+        PSumSpec q{};
+        q.n = 1;
+        q.pw[0] = 2;
+        q.l[0] = L;
+        q.m[0] = am;
+        const std::vector<double> sR = particle_sums(1, q);
+        double re = (rand_only ? 1.0 : alpha * alpha) * sR[0], im = (rand_only ? 1.0 : alpha * alpha) * sR[1];
+        if (!rand_only) {
+            const std::vector<double> sD = particle_sums(0, q);
+            re += sD[0];
+            im += sD[1];
+        }
+        if (M < 0) {  // Yhat_{L,-M} = (-1)^M conj Yhat_{L,M}
+            const double sg = (am % 2) ? -1.0 : 1.0;
+            re = sg * re;
+            im = -sg * im;
+        }
+        return {re, im};
+    }
+
     template <int LZ>
     void launch_line_L(const HistSpec &hs, double *hist) {
         size_t smem = OrbitCfg<T, LZ>::smem();
@@ -2388,7 +2653,7 @@ struct Engine : public hg_ctx {
             HG_CK(cudaMemsetAsync(p->p, 0, sizeof(double) * 2 * n2dim, st));
         }
         const double alpha = src_alpha;
-        const SpecK n00 = sfield(SF_SN, 0, 0, alpha);
+        const SpecK n00 = sfield(sn_kind(), 0, 0, alpha);
         std::set<int> Ls;
         for (const auto &mp : todo) Ls.insert(mp.L);
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
@@ -2404,8 +2669,10 @@ struct Engine : public hg_ctx {
                     if (!cs.empty()) hm.push_back({mp, cs});
                 }
                 if (hm.empty()) continue;
-                const SpecK f1 = sfield(SF_DELTA, L, M, alpha);
-                const std::array<double, 2> S3 = survey_s3(L, M, alpha);
+                const SpecK f1 = sfield(delta_kind(), L, M, alpha);
+                // the window 3PCF subtracts sum_R w^2 Yhat_LM (bispec.hpp:700), the survey
+                // S3_LM (bispec.hpp:446)
+                const std::array<double, 2> S3 = (src_kind == 2) ? survey_s2(L, M, 0.0, true) : survey_s3(L, M, alpha);
                 // (f1 conj f2)(0) from the exact k = 0 values
                 const double k0r = f1.k0r * n00.k0r + f1.k0i * n00.k0i, k0i = f1.k0i * n00.k0r - f1.k0r * n00.k0i;
                 LdXiCross<T> ld{f1.s, n00.s, g.n[2], xtabs, S3[0], S3[1], k0r, k0i, 1.0 / g.volume};
@@ -2539,6 +2806,200 @@ struct Engine : public hg_ctx {
         end();
     }
 
+    // calcThreePointWindowCorrelationFunction (bispec.hpp:617-874): the survey 3PCF of the
+    // randoms alone (Yhat w fields of n_R), its shot noise from conj(Yhat) w^2 fields of n_R
+    // with sum_R w^2 Yhat_LM subtracted; *norm = V_survey^2 / (sum w_R)^3
+    void zeta_window_multi(const std::vector<MP> &mps, int ith, double vs, double *zeta_save, double *sn_save,
+                           double *norm) override {
+        check_multipoles(mps);
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_rbin, "ith_rbin out of range");
+        require_randoms(needs_los(mps));
+        begin();
+        zeta_geometry();
+        set_source(2, 0.0);
+        std::vector<std::vector<double>> Z = zeta_main(mps, ith);
+        survey_histograms(mps);
+        std::vector<const double *> hs;
+        for (const auto &mp : mps) hs.push_back(dp<double>(*hist_sv[{mp.l1, mp.l2, mp.L}]));
+        zeta_finish(mps, ith, Z, hs, zeta_save, sn_save);
+        if (norm) {
+            const double wR = weight_sum(1);
+            HG_REQUIRE(wR != 0.0, "the summed random weights must be non-zero");
+            double nv = vs / wR / wR;
+            nv *= (vs / wR);
+            *norm = nv;
+        }
+        end();
+    }
+
+    void require_randoms(bool need_los) const {
+        HG_REQUIRE(slot[1].set, "window functions need the randoms (slot 1): call hg_set_particles(ctx, 1, ...)");
+        if (need_los)
+            HG_REQUIRE(slot[1].los_off >= 0, "window multipoles need line-of-sight vectors: pass los_off for the randoms");
+    }
+
+    double weight_sum(int s) {
+        PSumSpec q{};
+        q.n = 1;
+        q.pw[0] = 1;
+        q.l[0] = -1;
+        return particle_sums(s, q)[0];
+    }
+
+    // ------------------------------------------------------------------ 2PCF
+    // The 2PCF's r binning (calcCorrelationFunction, field.hpp:854-977): fine index
+    // int(|r| / 0.5 + 0.5) kept below 20000, coarse bin j takes fine i iff lower_j < 0.5 i <=
+    // upper_j with the uniform width rbin[1] - rbin[0], averages by cell count.  Per n2 =
+    // |x / dr|^2 (equal cell sizes; |r|^2 = n2 dr^2 is the reference's sum of (i dr)^2 exactly
+    // when those squares are exact, e.g. dyadic dr): the fine index and the cells.
+    struct Xi2Geo {
+        bool built = false;
+        std::vector<int> fine;                 // per n2; -1 past the fine table
+        std::vector<std::vector<int>> coarse;  // per fine index
+        std::vector<double> cells;             // per n2
+    } x2;
+    void xi2_geometry() {
+        build_orbits();
+        if (x2.built) return;
+        std::vector<std::vector<double>> c1(3);
+        for (int a = 0; a < 3; a++) {
+            const int h = g.n[a] / 2;
+            c1[a].assign((size_t)h * h + 1, 0.0);
+            for (int i = 0; i < g.n[a]; i++) {
+                const int w = wrap_index(i, g.n[a]);
+                c1[a][(size_t)w * w] += 1.0;
+            }
+        }
+        x2.cells.assign(n2dim, 0.0);
+        for (size_t a = 0; a < c1[0].size(); a++) {
+            if (c1[0][a] == 0.0) continue;
+            for (size_t b = 0; b < c1[1].size(); b++) {
+                if (c1[1][b] == 0.0) continue;
+                for (size_t c = 0; c < c1[2].size(); c++)
+                    if (c1[2][c] != 0.0) x2.cells[a + b + c] += c1[0][a] * c1[1][b] * c1[2][c];
+            }
+        }
+        const int n_temp = 20000;
+        const double dr_temp = 0.5, dr = g.dr[0];
+        x2.fine.assign(n2dim, -1);
+        for (long long q = 0; q < n2dim; q++) {
+            const double rmag = std::sqrt(double(q) * (dr * dr));
+            const int ri = (int)(rmag / dr_temp + 0.5);
+            if (ri < n_temp) x2.fine[q] = ri;
+        }
+        const double dr_bin = rbin[1] - rbin[0];
+        x2.coarse.assign(n_temp, {});
+        for (int j = 0; j < cfg.n_rbin; j++) {
+            const double lower = (rbin[j] > dr_bin * 0.5) ? (rbin[j] - dr_bin * 0.5) : 0.0;
+            const double upper = rbin[j] + dr_bin * 0.5;
+            for (int i = 0; i < n_temp; i++) {
+                const double rt = double(i) * dr_temp;
+                if ((rt > lower) && (rt <= upper)) x2.coarse[i].push_back(j);
+            }
+        }
+        x2.built = true;
+    }
+
+    // xi_save[j] = scale * (sum of hist over the n2 of bin j) / (cells of bin j)
+    void xi2_bin(const double *d_hist, double scale, double *xi_save, int *n_mode) {
+        std::vector<double> h(2 * n2dim);
+        HG_CK(cudaMemcpyAsync(h.data(), d_hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        const int nr = cfg.n_rbin;
+        std::vector<double> xr(nr, 0.0), xim(nr, 0.0), nm(nr, 0.0);
+        for (long long q = 0; q < n2dim; q++) {
+            const int f = x2.fine[q];
+            if (f < 0) continue;
+            for (int j : x2.coarse[f]) {
+                xr[j] += h[2 * q];
+                xim[j] += h[2 * q + 1];
+                nm[j] += x2.cells[q];
+            }
+        }
+        for (int j = 0; j < nr; j++) {
+            xi_save[2 * j] = nm[j] != 0.0 ? scale * (xr[j] / nm[j]) : 0.0;
+            xi_save[2 * j + 1] = nm[j] != 0.0 ? scale * (xim[j] / nm[j]) : 0.0;
+            if (n_mode) n_mode[j] = (int)nm[j];
+        }
+    }
+
+    // calcTwoPointCorrelationFunctionForBOX (powerspec.hpp:334-393): xi = FFT_+[(|dn|^2 - N C)
+    // / W^2] / V, r-binned with the Legendre weight L_l(mu); xi_save = (2l+1) xi, norm V / N^2
+    void xi_box(int ell, double *xi_save, int *n_mode, double *norm) override {
+        HG_REQUIRE(ell >= 0, "ell must be >= 0");
+        begin();
+        set_source(0, 0.0);
+        xi2_geometry();
+        ensure_xi(delta0 * delta0);
+        HistSpec hs;
+        memset(&hs, 0, sizeof(hs));
+        hs.nh = 1;
+        hs.parity[0] = (ell % 2 == 0) ? 1 : -1;
+        hs.term[0][hs.nterm[0]++] = YTerm{ell, 0, 0, 0, 1.0};
+        orbit_weight_poly(hs, 0);
+        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim));
+        HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim, st));
+        launch_orbit(g.n[2], hs, (int)orbit_n2xy.size(), dp<double>(hist_tmp));
+        xi2_bin(dp<double>(hist_tmp), double(2 * ell + 1), xi_save, n_mode);
+        if (norm) *norm = g.volume / double(slot[0].n) / double(slot[0].n);
+        end();
+    }
+
+    // calcTwoPointCorrelationFunction (powerspec.hpp:93-180; window: false) and
+    // calcTwoPointWindowCorrelationFunction (powerspec.hpp:182-270; window: true): sum over
+    // M and m1 of w3j-weighted r-binned xi_LM Yhat_{l m1}(r), xi_LM = FFT_+[(dn_LM conj dn_00 -
+    // S_LM C) / W^2] / V; norm V_survey / (sum w)^2 of the data (randoms for the window)
+    void xi_survey(int ell, bool window, double alpha, double vs, double *xi_save, int *n_mode,
+                   double *norm) override {
+        HG_REQUIRE(ell >= 0, "ell must be >= 0");
+        if (window) require_randoms(ell > 0);
+        else require_survey(ell > 0);
+        HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
+                   "the 2PCF needs equal cell sizes on all axes");
+        begin();
+        set_source(window ? 2 : 1, window ? 0.0 : alpha);
+        xi2_geometry();
+        const SpecK f00 = sfield(delta_kind(), 0, 0, src_alpha);
+        HG_CK(xi.ensure(sizeof(C) * g.ntot));
+        xi_valid = false;  // the box correlation field is overwritten
+        HG_CK(xi2acc.ensure(sizeof(double) * 2 * n2dim));
+        HG_CK(cudaMemsetAsync(xi2acc.p, 0, sizeof(double) * 2 * n2dim, st));
+        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim));
+        for (int M = -ell; M <= ell; M++) {
+            HistSpec hs;
+            memset(&hs, 0, sizeof(hs));
+            hs.nh = 1;
+            hs.parity[0] = 1;
+            for (int m1 = -ell; m1 <= ell; m1++) {
+                double w = wigner3j(ell, 0, ell, 0, 0, 0) * wigner3j(ell, 0, ell, m1, 0, M);
+                w *= double(2 * ell + 1) * double(2 * ell + 1);
+                if (std::fabs(w) < 1.0e-10) continue;
+                HG_REQUIRE(hs.nterm[0] < 12, "too many (m1) terms in one 2PCF multipole");
+                hs.term[0][hs.nterm[0]++] = YTerm{ell, m1, 0, 0, w};
+            }
+            if (hs.nterm[0] == 0) continue;
+            const SpecK f1 = sfield(delta_kind(), ell, M, src_alpha);
+            const std::array<double, 2> S = survey_s2(ell, M, src_alpha, window);
+            const double k0r = f1.k0r * f00.k0r + f1.k0i * f00.k0i, k0i = f1.k0i * f00.k0r - f1.k0r * f00.k0i;
+            LdXiCross<T> ld{f1.s, f00.s, g.n[2], xtabs, S[0], S[1], k0r, k0i, 1.0 / g.volume};
+            xi_x_pass(ld);
+            pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
+                     "fft_xi_y");
+            HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim, st));
+            launch_line(hs, dp<double>(hist_tmp));
+            k_axpy<<<grid1(2 * n2dim, 256), 256, 0, st>>>(dp<double>(xi2acc), dp<double>(hist_tmp), 2 * n2dim);
+            HG_CK(cudaGetLastError());
+        }
+        xi2_bin(dp<double>(xi2acc), 1.0, xi_save, n_mode);
+        if (norm) {
+            const double ws = weight_sum(window ? 1 : 0);
+            HG_REQUIRE(ws != 0.0, "the summed weights must be non-zero");
+            *norm = vs / ws / ws;
+        }
+        end();
+    }
+    DBuf xi2acc;
+
     // calcPowerSpectrum (powerspec.hpp:4-91): sum over M of w3j-weighted binned
     // (dn_LM conj dn_00 - S_LM C) / W^2 Yhat_{l m1}(k), S_LM = sum_D w^2 Yhat_LM + alpha^2 sum_R
     // w^2 Yhat_LM (field.hpp:1164-1185).  Fields for M < 0 are mirrors of M > 0.
@@ -2623,167 +3084,4 @@ struct Engine : public hg_ctx {
     }
 };
 
-thread_local std::string g_create_error;
-
 }  // namespace
-
-namespace hg {
-// Error text returned by hg_last_error(NULL) for entry points that have no context.
-void set_contextless_error(const std::string &m) { g_create_error = m; }
-}  // namespace hg
-
-extern "C" {
-
-int hg_create(hg_ctx **out, const hg_config *cfg) {
-    if (!out || !cfg) return -1;
-    *out = nullptr;
-    try {
-        if (cfg->precision == HG_FP64) *out = new Engine<double>(*cfg);
-        else if (cfg->precision == HG_FP32) *out = new Engine<float>(*cfg);
-        else throw HgError{"precision must be HG_FP64 or HG_FP32"};
-        return 0;
-    } catch (const HgError &e) {
-        g_create_error = e.msg;
-        return -1;
-    } catch (const std::exception &e) {
-        g_create_error = e.what();
-        return -1;
-    }
-}
-
-int hg_destroy(hg_ctx *ctx) {
-    if (!ctx) return -1;
-    cudaSetDevice(ctx->cfg.device);  // the buffers are freed on the context's GPU
-    delete ctx;
-    return 0;
-}
-
-const char *hg_last_error(const hg_ctx *ctx) {
-    if (!ctx) return g_create_error.c_str();
-    return ctx->err.c_str();
-}
-
-// Every entry point first makes the context's GPU current on the calling host thread, so
-// that contexts can be driven from several threads (one per context).
-#define HG_GUARD(ctx, body)                 \
-    do {                                    \
-        if (!(ctx)) return -1;              \
-        try {                               \
-            HG_CK(cudaSetDevice((ctx)->cfg.device)); \
-            body;                           \
-            (ctx)->err.clear();             \
-            return 0;                       \
-        } catch (const HgError &e) {        \
-            (ctx)->err = e.msg;             \
-            return -1;                      \
-        } catch (const std::exception &e) { \
-            (ctx)->err = e.what();          \
-            return -1;                      \
-        }                                   \
-    } while (0)
-
-int hg_set_particles(hg_ctx *ctx, int slot, const double *base, long long n, long long stride_bytes, int pos_off,
-                     int los_off, int w_off) {
-    HG_GUARD(ctx, ctx->set_particles(slot, base, n, stride_bytes, pos_off, los_off, w_off, false));
-}
-
-int hg_set_particles_device(hg_ctx *ctx, int slot, const double *dev_base, long long n, long long stride_bytes,
-                            int pos_off, int los_off, int w_off) {
-    HG_GUARD(ctx, ctx->set_particles(slot, dev_base, n, stride_bytes, pos_off, los_off, w_off, true));
-}
-
-int hg_set_profiling(hg_ctx *ctx, int on) { HG_GUARD(ctx, ctx->set_profiling(on != 0)); }
-
-int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen) {
-    if (!ctx || !buf || buflen <= 0) return -1;
-    std::string s;
-    try {
-        s = ctx->kernel_stats();
-    } catch (const HgError &e) {
-        ctx->err = e.msg;
-        return -1;
-    }
-    long long n = std::min<long long>((long long)s.size(), buflen - 1);
-    memcpy(buf, s.data(), (size_t)n);
-    buf[n] = 0;
-    return 0;
-}
-
-int hg_pk_box(hg_ctx *ctx, int ell, double *pk_save, int *n_mode, double *norm) {
-    if (!pk_save) return -1;
-    HG_GUARD(ctx, ctx->pk_box(ell, pk_save, n_mode, norm));
-}
-
-int hg_bk_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_kbin, double *bk_save, double *sn_save, double *norm) {
-    if (!bk_save || !sn_save) return -1;
-    HG_GUARD(ctx, ctx->bk_box_multi({MP{ell1, ell2, ELL}}, ith_kbin, bk_save, sn_save, norm));
-}
-
-int hg_bk_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double *bk_save, double *sn_save,
-                    double *norm) {
-    if (!bk_save || !sn_save || !ells || n_multipoles <= 0) return -1;
-    std::vector<MP> mps;
-    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
-    HG_GUARD(ctx, ctx->bk_box_multi(mps, ith_kbin, bk_save, sn_save, norm));
-}
-
-int hg_zeta_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double *zeta_save, double *sn_save,
-                double *norm) {
-    if (!zeta_save || !sn_save) return -1;
-    HG_GUARD(ctx, ctx->zeta_box_multi({MP{ell1, ell2, ELL}}, ith_rbin, zeta_save, sn_save, norm));
-}
-
-int hg_zeta_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double *zeta_save,
-                      double *sn_save, double *norm) {
-    if (!zeta_save || !sn_save || !ells || n_multipoles <= 0) return -1;
-    std::vector<MP> mps;
-    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
-    HG_GUARD(ctx, ctx->zeta_box_multi(mps, ith_rbin, zeta_save, sn_save, norm));
-}
-
-int hg_bk_survey(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_kbin, double alpha, double vsurvey,
-                 double *bk_save, double *sn_save, double *norm) {
-    if (!bk_save || !sn_save) return -1;
-    HG_GUARD(ctx, ctx->bk_survey_multi({MP{ell1, ell2, ELL}}, ith_kbin, alpha, vsurvey, bk_save, sn_save, norm));
-}
-
-int hg_bk_survey_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double alpha, double vsurvey,
-                       double *bk_save, double *sn_save, double *norm) {
-    if (!bk_save || !sn_save || !ells || n_multipoles <= 0) return -1;
-    std::vector<MP> mps;
-    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
-    HG_GUARD(ctx, ctx->bk_survey_multi(mps, ith_kbin, alpha, vsurvey, bk_save, sn_save, norm));
-}
-
-int hg_zeta_survey(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double alpha, double vsurvey,
-                   double *zeta_save, double *sn_save, double *norm) {
-    if (!zeta_save || !sn_save) return -1;
-    HG_GUARD(ctx, ctx->zeta_survey_multi({MP{ell1, ell2, ELL}}, ith_rbin, alpha, vsurvey, zeta_save, sn_save, norm));
-}
-
-int hg_zeta_survey_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double alpha, double vsurvey,
-                         double *zeta_save, double *sn_save, double *norm) {
-    if (!zeta_save || !sn_save || !ells || n_multipoles <= 0) return -1;
-    std::vector<MP> mps;
-    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
-    HG_GUARD(ctx, ctx->zeta_survey_multi(mps, ith_rbin, alpha, vsurvey, zeta_save, sn_save, norm));
-}
-
-int hg_survey_scalars(hg_ctx *ctx, double *alpha, double *vsurvey, double *nbar, double *wsum_data,
-                      double *wsum_rand) {
-    HG_GUARD(ctx, ctx->survey_scalars(alpha, vsurvey, nbar, wsum_data, wsum_rand));
-}
-
-int hg_pk_survey(hg_ctx *ctx, int ell, double alpha, double vsurvey, double *pk_save, int *n_mode, double *norm) {
-    if (!pk_save) return -1;
-    HG_GUARD(ctx, ctx->pk_survey(ell, alpha, vsurvey, pk_save, n_mode, norm));
-}
-
-int hg_last_timing(const hg_ctx *ctx, double *device_ms, long long *kernel_launches) {
-    if (!ctx) return -1;
-    if (device_ms) *device_ms = ctx->last_ms;
-    if (kernel_launches) *kernel_launches = ctx->last_launches;
-    return 0;
-}
-
-}  // extern "C"

@@ -19,6 +19,9 @@
 #include "hg_common.cuh"
 
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 template <typename T>
 struct TwTable {
@@ -273,4 +276,5 @@ inline bool fft_supported_length(int L) {
     return L >= 8 && L <= 1024 && (L & (L - 1)) == 0;
 }
 
+}  // namespace HG_TU_NS
 }  // namespace hg

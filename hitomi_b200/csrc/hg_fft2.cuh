@@ -21,6 +21,9 @@
 #include "hg_fft.cuh"
 
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 // exp(-2 pi i k / 32), k = 0..31 (correctly rounded doubles), as compile-time constants
 __host__ __device__ constexpr double tw32_re(int k) {
@@ -621,4 +624,5 @@ inline cudaError_t launch_chain_x_reg_L(cplx<T> *t2, const cplx<T> *G, int ns, i
     return cudaGetLastError();
 }
 
+}  // namespace HG_TU_NS
 }  // namespace hg

@@ -20,6 +20,9 @@
 #include "hg_fft2.cuh"
 
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 __global__ void k_xi_tables(int n, const double *tw, const double *ts, const double *tc, int assign, int wpow,
                             double *cf, double *df, double *iw2) {
@@ -820,4 +823,5 @@ struct StHalf {  // keep the non-negative half of the last axis
 };
 
 
+}  // namespace HG_TU_NS
 }  // namespace hg

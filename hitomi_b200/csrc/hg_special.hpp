@@ -16,6 +16,9 @@
 #include <vector>
 
 namespace hg {
+// one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
+// helpers of this header never collide at link time
+inline namespace HG_TU_NS {
 
 inline double lnfact(int n) { return std::lgamma((double)n + 1.0); }
 
@@ -147,4 +150,5 @@ struct BesselSpline {
     }
 };
 
+}  // namespace HG_TU_NS
 }  // namespace hg

@@ -1,25 +1,26 @@
 // hg_static.cu -- the one entry point of this library that allocates no device memory.
 //
 // hg_pk_box_spectrum_static bins a power-spectrum multipole out of a density spectrum the
-// caller already holds on the device.  It is meant for callers that cannot call
-// cudaMalloc: code that runs while a stream is being captured into a CUDA graph (where
-// allocation is not allowed), and applications whose own allocator or memory budget owns
-// every byte of the GPU, so that a library allocating behind their back would fail or
-// break their accounting.  It runs the same binning kernel as hg_pk_box, but every
-// scratch buffer (the fine-to-coarse bin table, the per-axis window and shot-noise tables
-// and the FP64 bin accumulators) lives in one file-scope __device__ array of
-// HG_STATIC_SCRATCH_BYTES, which every GPU that loads this library holds until the
-// process exits.
+// caller already holds on the device.  It is for callers that cannot call cudaMalloc:
+// applications whose own allocator or memory budget owns every byte of the GPU (a library
+// allocating behind their back would fail, or break their accounting), and loops that must
+// not pay cudaMalloc's cost or its implicit device-wide synchronisation on every call.  It
+// runs the same binning kernel as hg_pk_box, but every scratch buffer (the fine-to-coarse
+// bin table, the per-axis window and shot-noise tables and the FP64 bin accumulators) lives
+// in one file-scope __device__ array of HG_STATIC_SCRATCH_BYTES, which every GPU that loads
+// this library holds until the process exits.
 //
 // Limits (rejected with an error, nothing launched): n_kbin <= 256; n_mesh <= 1024 per
 // axis; the fine table needs at most 100000 entries (k bins up to |k| = 10, as in the
 // reference's fine histogram).
 //
 // The first call on each device looks up the array's device address with
-// cudaGetSymbolAddress (with that device current) and caches it; make that first call
-// before capturing a stream.  All calls share the one array and it keeps the last call's
-// contents: the accumulators are cleared at the start of every call, and calls whose work
-// overlaps on the GPU (different streams or threads at the same time) race on it.
+// cudaGetSymbolAddress (with that device current) and caches it.  All calls share the one
+// array and it keeps the last call's contents: the accumulators are cleared at the start of
+// every call, and calls whose work overlaps on the GPU (different streams or threads at the
+// same time) race on it.  The call waits for its stream and copies the sums into host
+// memory before it returns; it leaves the caller's current device as it found it.
+#define HG_TU_NS tu_static
 #include "hitomi_gpu.h"
 #include "hg_common.cuh"
 #include "hg_bin.cuh"
@@ -146,8 +147,12 @@ int run(const hg_config &c, const void *spec, long long n_particles, int ell, do
                                                                   tab + (2 * a + 1) * HG_STATIC_MAX_MESH);
     }
     k_static_lut<<<(n_fine + 255) / 256, 256, 0, st>>>(c.kmin, dkk, nbin, n_fine, lut);
-    cudaMemsetAsync(acc, 0, sizeof(double) * 2 * nbin, st);
-    cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * nbin, st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(std::string("table launches: ") + cudaGetErrorString(e));
+    // the previous call's sums are still in the array
+    e = cudaMemsetAsync(acc, 0, sizeof(double) * 2 * nbin, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * nbin, st);
+    if (e != cudaSuccess) return fail(std::string("clearing the static accumulators: ") + cudaGetErrorString(e));
     // the mode cube that can reach a bin (as in the context path)
     int3 lo, cn;
     int *lop[3] = {&lo.x, &lo.y, &lo.z};
@@ -163,19 +168,20 @@ int run(const hg_config &c, const void *spec, long long n_particles, int ell, do
     lms.lm[0] = LM{ell, 0};
     Spec<T> f{reinterpret_cast<const cplx<T> *>(spec), g.n[0], g.n[1], g.n[2], 1};
     size_t smem = sizeof(double) * 2 * nbin + sizeof(unsigned long long) * nbin;
-    cudaFuncSetAttribute(k_pk_bin<T, Spec<T>, Spec<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(k_pk_bin<T, Spec<T>, Spec<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fail(std::string("binning kernel attribute: ") + cudaGetErrorString(e));
     long long total = (long long)cn.x * cn.y * cn.z;
     unsigned blocks = (unsigned)std::min<long long>((total + 255) / 256, 148 * 8);
     const int wpow = c.assign + 1;
     k_pk_bin<T, Spec<T>, Spec<T>><<<blocks, 256, smem, st>>>(f, f, g, tabs, lo, cn, lut, n_fine, nbin, lms, double(n_particles), 0.0,
                                            c.assign, wpow, acc, cnt, 0, 0.0, 0.0);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return fail(std::string("binning launch: ") + cudaGetErrorString(e));
     double hacc[2 * HG_STATIC_MAX_KBIN];
     unsigned long long hcnt[HG_STATIC_MAX_KBIN];
-    cudaMemcpyAsync(hacc, acc, sizeof(double) * 2 * nbin, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(hcnt, cnt, sizeof(unsigned long long) * nbin, cudaMemcpyDeviceToHost, st);
-    e = cudaStreamSynchronize(st);
+    e = cudaMemcpyAsync(hacc, acc, sizeof(double) * 2 * nbin, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hcnt, cnt, sizeof(unsigned long long) * nbin, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(std::string("static binning: ") + cudaGetErrorString(e));
     for (int i = 0; i < nbin; i++) {
         double re = 0.0, im = 0.0;
@@ -215,17 +221,28 @@ extern "C" int hg_pk_box_spectrum_static(const hg_config *cfg, const void *d_hal
         if (std::ceil(kedge / 0.0001) + 2 > HG_STATIC_MAX_FINE)
             return fail("hg_pk_box_spectrum_static: k bins beyond |k| = 10 exceed the fine-bin table");
     }
-    cudaError_t e = cudaSetDevice(c.device);
+    if (c.precision != HG_FP64 && c.precision != HG_FP32)
+        return fail("hg_pk_box_spectrum_static: precision must be HG_FP64 or HG_FP32");
+    int prev_dev = -1;
+    cudaError_t e = cudaGetDevice(&prev_dev);
+    if (e != cudaSuccess) return fail(std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    e = cudaSetDevice(c.device);
     if (e != cudaSuccess) return fail(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
     std::string err;
+    int rc;
     void *base = scratch_address(c.device, err);
-    if (!base) return fail(err);
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    if (c.precision == HG_FP64)
-        return run<double>(c, d_half_spectrum, n_particles, ell, pk_save, n_mode, norm, st,
-                           reinterpret_cast<unsigned char *>(base));
-    if (c.precision == HG_FP32)
-        return run<float>(c, d_half_spectrum, n_particles, ell, pk_save, n_mode, norm, st,
-                          reinterpret_cast<unsigned char *>(base));
-    return fail("hg_pk_box_spectrum_static: precision must be HG_FP64 or HG_FP32");
+    if (!base) {
+        rc = fail(err);
+    } else {
+        cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+        unsigned char *b = reinterpret_cast<unsigned char *>(base);
+        rc = (c.precision == HG_FP64) ? run<double>(c, d_half_spectrum, n_particles, ell, pk_save, n_mode, norm, st, b)
+                                      : run<float>(c, d_half_spectrum, n_particles, ell, pk_save, n_mode, norm, st, b);
+    }
+    // the caller's current device, as it was
+    if (prev_dev != c.device) {
+        e = cudaSetDevice(prev_dev);
+        if (e != cudaSuccess && rc == 0) rc = fail(std::string("restoring the current device: ") + cudaGetErrorString(e));
+    }
+    return rc;
 }

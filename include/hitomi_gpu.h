@@ -11,8 +11,11 @@
  *
  * Conventions (mirroring the reference, src/hitomi_measurement/field.hpp:61,
  * powerspec.hpp:12-16): every function returns 0 on success and -1 on failure;
- * hg_last_error() gives the reason.  No exception crosses the ABI.  One context per
- * process per GPU; calls on one context are synchronous and not reentrant.
+ * hg_last_error() gives the reason.  No exception crosses the ABI.  Calls on one context
+ * are synchronous and not reentrant.  Several contexts may share a GPU (one host thread
+ * each, e.g. to overlap one catalogue's upload with another's statistics); each has its
+ * own stream and buffers, and their caches compete for the GPU's memory (a 3PCF field
+ * cache that fails to allocate is trimmed and rebuilt in smaller pieces).
  *
  * Results are the reference's RAW FP64 sums before normalisation and printing
  * (pk_save / bk_save / sn_save / zeta_save), plus the normalisation factor the
@@ -53,11 +56,26 @@ typedef struct hg_config {
     int periodic;       /* 0: the reference's flat-index bounds rule (field.hpp:92-96);
                            1: periodic wrap (forced for PCS / interlacing) */
     int device;         /* CUDA device ordinal */
+    int fp64_stages;    /* HG_FP32 form only: HG_STAGE_* bits of the periodic-box P_l / B_l
+                           pipeline to run in FP64 instead (0: none); ignored by HG_FP64 */
 } hg_config;
+
+/* Stages of the periodic-box pipeline (hg_pk_box, hg_bk_box*) that an HG_FP32 context can
+ * run in FP64 (hg_config.fp64_stages).  The context then also holds an FP64 engine on the
+ * same stream; the density spectrum crosses between the two, converted.
+ *   HG_STAGE_DENSITY   : assignment and density transform (field.hpp:67-184, 310-325);
+ *                        P_l is then binned from the FP64 spectrum
+ *   HG_STAGE_BK_SIGNAL : bispectrum signal: G, shell fields, chains, pair sums
+ *                        (bispec.hpp:1097-1168)
+ *   HG_STAGE_BK_SHOT   : bispectrum shot noise: P terms and the correlation field
+ *                        (bispec.hpp:909-1078) */
+#define HG_STAGE_DENSITY 1
+#define HG_STAGE_BK_SIGNAL 2
+#define HG_STAGE_BK_SHOT 4
 
 /* Create / destroy a context.  Replaces the per-call setup the reference does inside
  * each estimator (DensityFieldClass allocation, field.hpp:20-30; FFTW planning,
- * field.hpp:321).  The context owns all device memory, plans, tables and graphs. */
+ * field.hpp:321).  The context owns all device memory, twiddle and bin tables and caches. */
 int hg_create(hg_ctx **ctx, const hg_config *cfg);
 int hg_destroy(hg_ctx *ctx);
 const char *hg_last_error(const hg_ctx *ctx);
@@ -159,6 +177,64 @@ int hg_survey_scalars(hg_ctx *ctx, double *alpha, double *vsurvey, double *nbar,
  * reference function.  *norm = V_survey / (sum w_D)^2 (particle.hpp:303-316). */
 int hg_pk_survey(hg_ctx *ctx, int ell, double alpha, double vsurvey, double *pk_save, int *n_mode, double *norm);
 
+/* Periodic-box two-point correlation function multipole.  Replaces
+ * calcTwoPointCorrelationFunctionForBOX (powerspec.hpp:334-393): xi(x) = FFT_+[(|dn|^2 -
+ * N C(k)) / W(k)^2] / V (field.hpp:854-905) averaged over r bins with the Legendre weight
+ * L_l(mu) (field.hpp:906-977: fine bins of dr = 0.5, coarse bins (lower, upper]).
+ * xi_save[2*n_rbin]: the reference's xi_save = (2l+1) stat.xi; n_mode[n_rbin] (cells per
+ * bin) may be NULL; *norm = V / N^2.  Output file value = norm * Re(xi_save)
+ * (powerspec.hpp:380-387).  Needs equal cell sizes on all axes. */
+int hg_xi_box(hg_ctx *ctx, int ell, double *xi_save, int *n_mode, double *norm);
+
+/* Survey-geometry two-point correlation function multipole with local LOS.  Replaces
+ * calcTwoPointCorrelationFunction (powerspec.hpp:93-180): the sum over M and m1 of
+ * Wigner-3j-weighted r-binned xi_LM Yhat_{l m1}(r), xi_LM from the Yhat_LM-weighted
+ * D - alpha R field against the l = 0 one with the shot noise of field.hpp:1164-1185.
+ * *norm = V_survey / (sum w_D)^2.  Layout as hg_xi_box. */
+int hg_xi_survey(hg_ctx *ctx, int ell, double alpha, double vsurvey, double *xi_save, int *n_mode, double *norm);
+
+/* Two-point window correlation function multipole.  Replaces
+ * calcTwoPointWindowCorrelationFunction (powerspec.hpp:182-270): as hg_xi_survey on the
+ * randoms alone (slot 1; calcYlmWeightedDensity field.hpp:230-247, shot noise
+ * field.hpp:1202-1217).  *norm = V_survey / (sum w_R)^2.  No data catalogue is needed. */
+int hg_xi_window(hg_ctx *ctx, int ell, double vsurvey, double *xi_save, int *n_mode, double *norm);
+
+/* Three-point window correlation function multipole.  Replaces
+ * calcThreePointWindowCorrelationFunction (bispec.hpp:617-874): the survey 3PCF of the
+ * randoms alone, shot noise from their conj(Yhat) w^2 field minus sum_R w^2 Yhat_LM, on the
+ * diagonal.  Layout as hg_zeta_box; *norm = V_survey^2 / (sum w_R)^3.  Output file value =
+ * norm * Re(zeta_save - sn_save) (bispec.hpp:863-866).  Needs a cubic box and mesh. */
+int hg_zeta_window(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double vsurvey, double *zeta_save,
+                   double *sn_save, double *norm);
+int hg_zeta_window_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double vsurvey,
+                         double *zeta_save, double *sn_save, double *norm);
+
+/* One catalogue of a batch (hg_batch_run): an array of structs in host memory, read as
+ * hg_set_particles reads it (positions at pos_off doubles into each record, weight 1). */
+typedef struct hg_mock {
+    const double *base;
+    long long n;
+    long long stride_bytes;
+    int pos_off;
+} hg_mock;
+
+/* Periodic-box statistics of many mock catalogues in one call: the covariance workload
+ * that the reference runs as one process per realization (main.cpp:64-76,
+ * main_box.cpp:64-90), each process calling calcPowerSpectrumForBOX /
+ * calcBiSpectrumForBOX / calcThreePointCorrelationFunctionForBOX.  For every mock, in
+ * order: P_l for the n_pk ells, B for the n_bk (l1, l2, L) triples and zeta for the n_zeta
+ * triples (all rows).  While one mock is measured, the next one's catalogue is staged
+ * through pinned memory by a host thread and copied to the GPU on a second stream.
+ * out holds n_mocks blocks of hg_batch_block_len(ctx, n_pk, n_bk, n_zeta) doubles:
+ *   pk_save [n_pk][n_kbin] complex, then n_pk norms;
+ *   bk_save [n_bk][n_kbin][n_kbin] complex, sn_save likewise, then 1 norm (if n_bk > 0);
+ *   zeta_save [n_zeta][n_rbin][n_rbin] complex, sn_save likewise, then 1 norm (if n_zeta > 0).
+ * Each block equals what hg_pk_box, hg_bk_box_multi and hg_zeta_box_multi give for that
+ * catalogue. */
+int hg_batch_run(hg_ctx *ctx, const hg_mock *mocks, int n_mocks, int n_pk, const int *pk_ells, int n_bk,
+                 const int *bk_ells, int n_zeta, const int *zeta_ells, double *out);
+long long hg_batch_block_len(const hg_ctx *ctx, int n_pk, int n_bk, int n_zeta);
+
 /* Per-kernel device timing: when on, every kernel launch of this library is bracketed by
  * CUDA events on the context's stream.  hg_kernel_stats writes one line per kernel name:
  * "name<TAB>launches<TAB>total_ms<TAB>modelled_bytes".  These replace the reference's
@@ -166,20 +242,24 @@ int hg_pk_survey(hg_ctx *ctx, int ell, double alpha, double vsurvey, double *pk_
 int hg_set_profiling(hg_ctx *ctx, int on);
 int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen);
 
-/* Allocation-free periodic-box power-spectrum multipole, for callers that cannot call
- * cudaMalloc (work captured into a CUDA graph, or an application whose allocator owns all
- * device memory).  No counterpart in the reference: it is the binning step of hg_pk_box
- * run on a density spectrum the caller already holds on the device.
+/* Allocation-free periodic-box power-spectrum multipole.  No counterpart in the reference:
+ * it is the binning step of hg_pk_box run on a density spectrum the caller already holds
+ * on the device, for callers that cannot call cudaMalloc -- an application whose own
+ * allocator or memory budget owns all of the GPU's memory, or a loop that cannot afford
+ * cudaMalloc's cost and implicit synchronisation on every call.
  *   d_half_spectrum : device array [n0][n1][n2/2+1] of complex (double pairs for HG_FP64,
  *                     float pairs for HG_FP32, per cfg->precision) holding
  *                     FFT[dV (rho - N/V)], the non-negative-kz half of the reference's
  *                     calcFourierTransform output (field.hpp:310-325) for a real field.
+ *   cfg->assign     : NGP, CIC or TSC (the window and shot-noise tables), no interlacing.
  *   outputs as hg_pk_box; stream is a cudaStream_t (NULL: the default stream).
  * All scratch sits in a 1 MiB file-scope __device__ array that every GPU loading this
  * library keeps until exit.  Limits: n_kbin <= 256, n_mesh <= 1024 per axis, k bins
  * below |k| = 10; larger requests fail with an error and launch nothing.  The first call
- * on a device looks up that array's address (make it before any stream capture).  Calls
- * share the array: calls overlapping on the GPU race.  Errors: hg_last_error(NULL). */
+ * on a device looks up that array's address.  Calls share the array (each clears its
+ * accumulators first): calls overlapping on the GPU race.  The call waits for the stream,
+ * returns the sums in host memory and restores the caller's current device.
+ * Errors: hg_last_error(NULL). */
 int hg_pk_box_spectrum_static(const hg_config *cfg, const void *d_half_spectrum, long long n_particles, int ell,
                               double *pk_save, int *n_mode, double *norm, void *stream);
 

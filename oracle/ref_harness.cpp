@@ -16,6 +16,8 @@
  *   ref_harness param.ini data.f64 [random.f64] [--all-rows]
  *     box    : data.f64 holds n x 3 doubles (x y z)
  *     survey : data.f64 / random.f64 hold n x 4 doubles (x y z w)
+ *   measure = pk | 2PCF | bk | 3PCF (box and survey), window2PCF | window3PCF (survey: the
+ *   randoms only, main.cpp:252-270)
  *   --all-rows : for measure = bk / 3PCF, run every ith_kbin / ith_rbin row
  *                (the reference computes one row per process, main.cpp:78-84).
  *   --unit OP  : (box) time one building block of the reference's estimators once and
@@ -82,8 +84,14 @@ static int hx_fprintf(FILE *fp, const char *fmt, ...) {
 #include "particleGadget.hpp"
 #include "particle_reconstruction.hpp"
 #include "field.hpp"
+#ifdef HX_DROPIN
+/* the reference's estimator entry points with bodies over the B200 library: the same driver
+ * flow, the same output files (tests/test_gpu_dropin.py compares them) */
+#include "hitomi_dropin.hpp"
+#else
 #include "powerspec.hpp"
 #include "bispec.hpp"
+#endif
 
 #undef printf
 #undef fprintf
@@ -134,6 +142,7 @@ static double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+#ifndef HX_DROPIN
 static int unit_op(const std::string &op, ParticleGadgetClass &P_D, ParameterClass &param, std::vector<double> &kbin) {
     double t = 0.0;
     std::complex<double> shotnoise = double(P_D.n_tot);
@@ -258,6 +267,8 @@ static int unit_op(const std::string &op, ParticleGadgetClass &P_D, ParameterCla
     return 0;
 }
 
+#endif
+
 int main(int argc, char **argv) {
     if (argc < 3) {
         std::fprintf(stderr, "usage: ref_harness param.ini data.f64 [random.f64] [--all-rows]\n");
@@ -274,6 +285,9 @@ int main(int argc, char **argv) {
     char *pargv[2] = {argv[0], (char *)pos[0]};
     ParameterClass param;
     if (param.readParameters(pargv)) return fail("param.readParameters");
+#ifdef HX_DROPIN
+    if (hitomi_dropin_configure(pos[0])) return fail("hitomi_dropin_configure");
+#endif
     if (param.makeOutputDirectory()) return fail("param.makeOutputDirectory");
     if (param.printParameters()) return fail("param.printParameters");
     std::vector<double> kbin(param.n_kbin), rbin(param.n_rbin);
@@ -291,7 +305,9 @@ int main(int argc, char **argv) {
         for (long long i = 0; i < n; i++)
             for (int ax = 0; ax < 3; ax++) P_D[i].pos[ax] = a[3 * i + ax];
         P_D.calcMinAndMax();
+#ifndef HX_DROPIN
         if (!unit.empty()) return unit_op(unit, P_D, param, kbin);
+#endif
         t0 = std::chrono::steady_clock::now();
         if (param.measure == "pk") {
             rc = calcPowerSpectrumForBOX(P_D, param, kbin.data());
@@ -343,6 +359,14 @@ int main(int argc, char **argv) {
             rc = calcPowerSpectrum(P_D, P_R, param, alpha, kbin.data(), Vsurvey);
         } else if (param.measure == "2PCF") {
             rc = calcTwoPointCorrelationFunction(P_D, P_R, param, alpha, rbin.data(), Vsurvey);
+        } else if (param.measure == "window2PCF") {
+            rc = calcTwoPointWindowCorrelationFunction(P_R, param, rbin.data(), Vsurvey);
+        } else if (param.measure == "window3PCF") {
+            int lo = all_rows ? 0 : param.ith_rbin, hi = all_rows ? param.n_rbin : param.ith_rbin + 1;
+            for (int i = lo; i < hi && rc == 0; i++) {
+                param.ith_rbin = i;
+                rc = calcThreePointWindowCorrelationFunction(P_R, param, rbin.data(), Vsurvey);
+            }
         } else if (param.measure == "bk") {
             int lo = all_rows ? 0 : param.ith_kbin, hi = all_rows ? param.n_kbin : param.ith_kbin + 1;
             for (int i = lo; i < hi && rc == 0; i++) {

@@ -147,6 +147,19 @@ class RefRun:
             rows.append(a[:, 2])
         return np.array(rows)
 
+    def xi(self, ell: int, window: bool = False):
+        """xi{l}.dat / xi{l}_window.dat (powerspec.hpp:165-175, 254-264, 380-387): r, value."""
+        a = _read_cols(os.path.join(self.out, f"xi{ell}{'_window' if window else ''}.dat"))
+        return a[:, 0], a[:, 1]
+
+    def zeta_window(self, l1: int, l2: int, L: int, n_rows: int):
+        """zeta{l1}{l2}{L}_{ith}_window.dat (bispec.hpp:857-866)."""
+        rows = []
+        for i in range(n_rows):
+            a = _read_cols(os.path.join(self.out, f"zeta{l1}{l2}{L}_{i:02d}_window.dat"))
+            rows.append(a[:, 2])
+        return np.array(rows)
+
     def survey_scalars(self):
         v = np.loadtxt(os.path.join(self.out, "survey_scalars_full"))
         return dict(alpha=v[0], vsurvey=v[1], nbar=v[2], wsum_data=v[3], wsum_rand=v[4])

@@ -11,6 +11,8 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --survey3 (only survey_bk_zeta.npz)
     python tests/golden/make_golden.py --odd (only box_odd.npz: odd l1 + l2)
     python tests/golden/make_golden.py --bk256 (only box_bk_256.npz, from the restatement)
+    python tests/golden/make_golden.py --xi     (only xi_window.npz: 2PCF, window 2PCF / 3PCF)
+    python tests/golden/make_golden.py --configs (only box_config_sizes.npz: 128^3 and 512^3)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
 """
@@ -196,7 +198,99 @@ def make_odd():
     np.savez_compressed(os.path.join(HERE, "box_odd.npz"), **d)
 
 
+def make_xi():
+    """Two-point correlation function multipoles: box (powerspec.hpp:334-393) for every
+    scheme, survey (powerspec.hpp:93-180), window (powerspec.hpp:182-270) and the window
+    3PCF (bispec.hpp:617-874), on the catalogues of the P and survey fixtures."""
+    d = {}
+    pos = lognormal_box(15000, 1000.0, ngrid=32, seed=11, exact_n=15000)
+    bx = Binning(0.005, 0.295, 30, 4.0, 156.0, 20)
+    d.update(box_pos=pos, box_binning=binning_arr(bx), box_boxsize=1000.0, box_n_mesh=64)
+    for assign, ells in (("TSC", (0, 1, 2, 4)), ("CIC", (0, 2)), ("NGP", (0, 2))):
+        for ell in ells:
+            with ref_runner.RefRun() as r:
+                r.run("2PCF", pos, ell, 0, ell, 64, 1000.0, bx, assign=assign)
+                d[f"box_xi_{assign}_{ell}"] = r.xi(ell)[1]
+    data, rand = survey_shell(3000, 60000, seed=16)
+    bs = Binning(0.004, 0.048, 12, 100.0, 1500.0, 15)
+    d.update(sv_data=data, sv_rand=rand, sv_binning=binning_arr(bs), sv_boxsize=3500.0, sv_n_mesh=64)
+    for ell in (0, 1, 2):
+        with ref_runner.RefRun() as r:
+            r.run("2PCF", data, ell, 0, ell, 64, 3500.0, bs, assign="TSC", randoms=rand)
+            d[f"sv_xi_{ell}"] = r.xi(ell)[1]
+            sc = r.survey_scalars()
+        with ref_runner.RefRun() as r:
+            r.run("window2PCF", data, ell, 0, ell, 64, 3500.0, bs, assign="TSC", randoms=rand)
+            d[f"win_xi_{ell}"] = r.xi(ell, window=True)[1]
+    for k, v in sc.items():
+        d[f"sv_scalars_{k}"] = v
+    data3, rand3 = survey_shell(2000, 30000, seed=18)
+    b3 = Binning(0.004, 0.02, 5, 150.0, 750.0, 5)
+    d.update(w3_data=data3, w3_rand=rand3, w3_binning=binning_arr(b3), w3_boxsize=3500.0, w3_n_mesh=32)
+    for mp in ((0, 0, 0), (1, 1, 0), (2, 0, 2)):
+        with ref_runner.RefRun() as r:
+            r.run("window3PCF", data3, *mp, 32, 3500.0, b3, assign="TSC", randoms=rand3)
+            d["w3_zeta_" + "".join(map(str, mp))] = r.zeta_window(*mp, b3.n_rbin)
+            sc = r.survey_scalars()
+    for k, v in sc.items():
+        d[f"w3_scalars_{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "xi_window.npz"), **d)
+
+
+def catalogue_digest(pos: np.ndarray) -> np.ndarray:
+    """Count, coordinate sums and sums of squares: the tests regenerate the large catalogues
+    from their seeds and check these first, so a generator change cannot pass silently."""
+    return np.array([pos.shape[0], *pos.sum(axis=0), *(pos * pos).sum(axis=0)], dtype=np.float64)
+
+
+def make_config_sizes():
+    """Reference outputs at the configurations' own sizes (the catalogues are regenerated
+    from their seeds by the tests, so only outputs and a digest are stored):
+      c1: 2x10^5 uniform particles (seed 1) in a 1000 Mpc/h box, 128^3 mesh, TSC, l = 0, 2, 4,
+          kmin 0.005, kmax 0.295, 30 bins;
+      c2: the clustered lognormal catalogue of 10^7 particles (256^3 Gaussian grid, seed 2),
+          512^3 mesh, TSC, l = 0, 2, 4 on the bispectrum's 25 k bins 0.015-0.255, and the
+          B_000 row ith_kbin = 0 against every k2 (bispec.hpp:877-1203 as one run does it).
+    The 512^3 runs take minutes each on one core; they run concurrently."""
+    from concurrent.futures import ThreadPoolExecutor
+    pos1 = uniform_box(200_000, 1000.0, seed=1)
+    b1 = Binning(0.005, 0.295, 30, 4.0, 156.0, 20)
+    pos2 = lognormal_box(10_000_000, 1000.0, ngrid=256, seed=2, exact_n=10_000_000)
+    b2 = Binning(0.015, 0.255, 25, 4.0, 156.0, 20)
+
+    def pk_job(pos, nm, b, ell):
+        with ref_runner.RefRun() as r:
+            r.run("pk", pos, ell, 0, ell, nm, 1000.0, b, assign="TSC")
+            return r.pk(ell)[1], r.wall
+
+    def bk_job():
+        with ref_runner.RefRun() as r:
+            r.run("bk", pos2, 0, 0, 0, 512, 1000.0, b2, assign="TSC", all_rows=False, ith=0)
+            a = ref_runner._read_cols(os.path.join(r.out, "bk000_00.dat"))
+            return a[:, 2] + 1j * a[:, 3], r.wall
+
+    d = dict(c1_digest=catalogue_digest(pos1), c1_binning=binning_arr(b1), c2_digest=catalogue_digest(pos2),
+             c2_binning=binning_arr(b2))
+    with ThreadPoolExecutor(max_workers=4) as ex:
+        fb = ex.submit(bk_job)
+        f2 = {ell: ex.submit(pk_job, pos2, 512, b2, ell) for ell in (0, 2, 4)}
+        f1 = {ell: ex.submit(pk_job, pos1, 128, b1, ell) for ell in (0, 2, 4)}
+        for ell in (0, 2, 4):
+            d[f"c1_pk_{ell}"], d[f"c1_wall_{ell}"] = f1[ell].result()
+            d[f"c2_pk_{ell}"], d[f"c2_wall_{ell}"] = f2[ell].result()
+        d["c2_bk000_row0"], d["c2_bk_wall"] = fb.result()
+    np.savez_compressed(os.path.join(HERE, "box_config_sizes.npz"), **d)
+
+
 def main():
+    if "--xi" in sys.argv:
+        make_xi()
+        print("fixtures written")
+        return
+    if "--configs" in sys.argv:
+        make_config_sizes()
+        print("fixtures written")
+        return
     if "--extensions" in sys.argv or "--bk256" in sys.argv:
         if "--extensions" in sys.argv:
             make_extensions()
