@@ -6,11 +6,13 @@ Zel'dovich RSD), TSC assignment, 25 k shells 0.01-0.26 h/Mpc.
 
 One step = one mock through the whole pipeline (assignment, FFT, P_l binning, shell
 transforms, bispectrum sums and shot noise).  `value` has the catalogue resident in HBM;
-`e2e` copies it from pinned host memory through hg_set_particles every step and reads
-the results back, through the batch pipeline a covariance run uses (hitomi_b200.batch:
-two contexts, one host thread each, one mock's upload overlapping another's statistics);
-`e2e.sequential_value` is the same with one context, one mock after another.  Both forms are measured: the chosen FP32 form (the headline) and the
-plain FP64 form, with the per-bin relative difference between them.
+`e2e` copies it from host memory every step and reads the results back, through the
+library's batch entry point hg_batch_run (the next mock's upload overlapping the current
+one's statistics); `e2e.sequential_value` is hg_set_particles + the statistic calls, one
+mock after another.  Three forms are measured: the chosen form (the headline: FP32 with the
+density and the bispectrum signal in FP64, the fastest setting whose every bin is within
+1e-5 of the FP64 form), the plain FP32 form and the plain FP64 form, with the per-bin
+relative difference of each against FP64.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--small]
   python bench.py --lean --forms fp32 [--n-mesh M --n-particles P]   (profiling runs)
@@ -546,26 +548,18 @@ def main():
         e1.record()
         torch.cuda.synchronize()
         sms = reduce_max(e0.elapsed_time(e1) / args.steps, world)
-        # ---- the same through the batch pipeline (hitomi_b200.batch.run_pipelined): two
-        # contexts on this GPU, one host thread each, so one mock's upload overlaps the other's
-        # statistics; every step still copies its catalogue from pinned host memory and reads
-        # its results back.  Wall clock around the whole run, the device drained on both sides.
-        from hitomi_b200.batch import run_pipelined
-        ctx2 = make_context(form, wl, local)
-        ctx2.set_particles(0, h_np)
-        run_mock(ctx2)
-
-        def e2e_mock(c, i):
-            c.set_particles(0, h_np)
-            return run_mock(c)[0]
-
+        # ---- the same through the library's batch entry point (hg_batch_run): every step's
+        # catalogue is copied from host memory, the next one's upload overlapping the current
+        # one's statistics (a host thread stages it through pinned memory, a second stream
+        # copies it), and every result comes back to host memory.  Wall clock around the whole
+        # call, the device drained on both sides.
+        ctx.batch_run([h_np], pk_ells=PK_ELLS, bk_multipoles=MULTIPOLES)  # buffers sized
         barrier(world)
         torch.cuda.synchronize()
         w0 = time.perf_counter()
-        run_pipelined(list(range(args.steps)), [ctx, ctx2], e2e_mock)
+        ctx.batch_run([h_np] * args.steps, pk_ells=PK_ELLS, bk_multipoles=MULTIPOLES)
         torch.cuda.synchronize()
         ems = reduce_max((time.perf_counter() - w0) * 1000.0 / args.steps, world)
-        ctx2.close()
         # ---- one profiled step: per-kernel CUDA-event timing
         ctx.set_profiling(True)
         ctx.set_particles_device(0, d_pos.data_ptr(), n, 24, keep=d_pos)
@@ -603,8 +597,8 @@ def main():
                    "parallelism": f"mocks sharded over {world} GPU(s), no collective on the data path"},
         "clocks": t["clocks"],
         "e2e": {"value": evalue, "unit": UNIT, "h2d_bytes_per_step": int(n * 24), "d2h_bytes_per_step": int(t["d2h"]),
-                "how": "hitomi_b200.batch.run_pipelined over two contexts on the GPU (upload of one mock overlaps "
-                       "the statistics of another), wall clock",
+                "how": "hg_batch_run through the C ABI with host buffers (the next mock's upload overlaps the "
+                       "current one's statistics), wall clock around the call",
                 "sequential_value": (world * 1000.0 / t["e2e_seq_ms"]) if t.get("e2e_seq_ms") else None},
         "gpu_launches": int(t["launches"] * args.steps),
         "roofline": roof,

@@ -36,8 +36,12 @@ SYMBOLS = (
     "hg_zeta_window_multi",
     "hg_batch_run",
     "hg_batch_block_len",
+    "hg_read_ascii",
+    "hg_read_gadget",
+    "hg_free",
     "hg_set_profiling",
     "hg_kernel_stats",
+    "hg_tuning",
     "hg_pk_box_spectrum_static",
     "hg_last_timing",
 )
@@ -53,6 +57,25 @@ class HgMock(ctypes.Structure):
         ("n", ctypes.c_longlong),
         ("stride_bytes", ctypes.c_longlong),
         ("pos_off", ctypes.c_int),
+    ]
+
+
+class HgGadgetHeader(ctypes.Structure):
+    _fields_ = [
+        ("npart", ctypes.c_uint * 6),
+        ("mass", ctypes.c_double * 6),
+        ("time", ctypes.c_double),
+        ("redshift", ctypes.c_double),
+        ("flag_sfr", ctypes.c_int),
+        ("flag_feedback", ctypes.c_int),
+        ("npartTotal", ctypes.c_uint * 6),
+        ("flag_cooling", ctypes.c_int),
+        ("num_files", ctypes.c_int),
+        ("BoxSize", ctypes.c_double),
+        ("Omega0", ctypes.c_double),
+        ("OmegaLambda", ctypes.c_double),
+        ("HubbleParam", ctypes.c_double),
+        ("fill", ctypes.c_char * 96),
     ]
 
 
@@ -105,6 +128,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_set_profiling.restype = ctypes.c_int
     lib.hg_kernel_stats.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
     lib.hg_kernel_stats.restype = ctypes.c_int
+    lib.hg_tuning.argtypes = [vp, ctypes.c_char_p, ctypes.c_longlong]
+    lib.hg_tuning.restype = ctypes.c_int
     lib.hg_pk_box.argtypes = [vp, ctypes.c_int, c_dp, c_ip, c_dp]
     lib.hg_pk_box.restype = ctypes.c_int
     lib.hg_bk_box.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_dp, c_dp, c_dp]
@@ -142,6 +167,13 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_batch_run.restype = ctypes.c_int
     lib.hg_batch_block_len.argtypes = [vp, i_, i_, i_]
     lib.hg_batch_block_len.restype = ctypes.c_longlong
+    lib.hg_read_ascii.argtypes = [ctypes.c_char_p, i_, ctypes.POINTER(c_dp), ctypes.POINTER(ctypes.c_longlong)]
+    lib.hg_read_ascii.restype = ctypes.c_int
+    lib.hg_read_gadget.argtypes = [ctypes.c_char_p, ctypes.POINTER(c_dp), ctypes.POINTER(ctypes.c_longlong),
+                                   ctypes.POINTER(HgGadgetHeader)]
+    lib.hg_read_gadget.restype = ctypes.c_int
+    lib.hg_free.argtypes = [ctypes.c_void_p]
+    lib.hg_free.restype = None
     lib.hg_pk_box_spectrum_static.argtypes = [ctypes.POINTER(HgConfig), ctypes.c_void_p, ctypes.c_longlong,
                                               ctypes.c_int, c_dp, c_ip, c_dp, ctypes.c_void_p]
     lib.hg_pk_box_spectrum_static.restype = ctypes.c_int

@@ -150,6 +150,12 @@ class Context:
             out[name] = dict(launches=int(n), ms=float(ms), bytes=float(by))
         return out
 
+    def tuning(self) -> str:
+        """The launch shapes the context's autotuner picked, with the time of every variant."""
+        buf = ctypes.create_string_buffer(1 << 14)
+        self._check(self._lib.hg_tuning(self._h, buf, len(buf)))
+        return buf.value.decode()
+
     # -- statistics
     def pk_box(self, ell: int):
         nk = self.binning.n_kbin

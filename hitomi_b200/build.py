@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhitomi_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in
-           ("hg_engine_fp32.cu", "hg_engine_fp64.cu", "hg_api.cu", "hg_static.cu")]
+           ("hg_engine_fp32.cu", "hg_engine_fp64.cu", "hg_api.cu", "hg_static.cu", "hg_io.cpp")]
 OBJDIR = os.path.join(HERE, "_build")
 HEADERS = [
     os.path.join(HERE, "csrc", f)
@@ -50,7 +50,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         common.append("-Xptxas=-v")
     objs, procs = [], []
     for src in SOURCES:
-        obj = os.path.join(OBJDIR, os.path.basename(src).replace(".cu", ".o"))
+        obj = os.path.join(OBJDIR, os.path.splitext(os.path.basename(src))[0] + ".o")
         objs.append(obj)
         procs.append(subprocess.Popen([nvcc()] + common + ["--split-compile=4", "-c", src, "-o", obj]))
     bad = [src for src, p in zip(SOURCES, procs) if p.wait() != 0]

@@ -109,6 +109,21 @@ int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen) {
     return 0;
 }
 
+int hg_tuning(hg_ctx *ctx, char *buf, long long buflen) {
+    if (!ctx || !buf || buflen <= 0) return -1;
+    std::string s;
+    try {
+        s = ctx->tuning();
+    } catch (const HgError &e) {
+        ctx->err = e.msg;
+        return -1;
+    }
+    long long n = std::min<long long>((long long)s.size(), buflen - 1);
+    memcpy(buf, s.data(), (size_t)n);
+    buf[n] = 0;
+    return 0;
+}
+
 int hg_pk_box(hg_ctx *ctx, int ell, double *pk_save, int *n_mode, double *norm) {
     if (!pk_save) return -1;
     HG_GUARD(ctx, ctx->pk_box(ell, pk_save, n_mode, norm));

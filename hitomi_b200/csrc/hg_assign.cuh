@@ -719,9 +719,16 @@ __device__ __forceinline__ void fix_split(float x, int &hi, int &lo) {
     lo = __float_as_int(__fadd_rn(r, 12582912.0f)) - 0x4B400000;
 }
 
+// FIX with T = double (real FP64 meshes of weight-bounded sources): one 64-bit integer word
+// per cell.  Per chunk every stencil weight (an FP64 product) is scaled by S = 2^s, exactly,
+// with (records) x fix_bound x S < 2^62, and rounded to an integer (the only rounding, below
+// 2^-63 of the chunk's bound); at most one add per record and cell keeps |sum| < 2^62, so
+// the sum is exact and independent of the order of the 64-bit integer atomics, and it is
+// rounded once, to the mesh's FP64.
 template <typename T, bool CPLX, bool FIX, int SCHEME>
 __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
-    static_assert(!FIX || (!CPLX && sizeof(T) == 4), "fixed-point accumulation is for real FP32 meshes");
+    static_assert(!FIX || !CPLX, "fixed-point accumulation is for real meshes");
+    constexpr bool FIX64 = FIX && sizeof(T) == 8;
     constexpr int W = SCHEME + 1, s0 = (SCHEME >= 2) ? -1 : 0;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *acc = reinterpret_cast<T *>(smem_raw);
@@ -729,7 +736,8 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     T *acc_im = acc + tcells;
     int *acc_hi = reinterpret_cast<int *>(smem_raw);
     int *acc_lo = acc_hi + tcells;
-    zero_shared(smem_raw, tcells * ((CPLX || FIX) ? 2 : 1) * (int)(sizeof(T) / 4));
+    unsigned long long *acc64 = reinterpret_cast<unsigned long long *>(smem_raw);
+    zero_shared(smem_raw, tcells * ((CPLX || (FIX && !FIX64)) ? 2 : 1) * (int)(sizeof(T) / 4));
     __syncthreads();
     const Chunk k = ch[blockIdx.x];
     const int tile = k.tile;
@@ -738,7 +746,13 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     const int tx = tile / (g.nt[2] * g.nt[1]);
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
     float fscale = 1.0f, finv = 1.0f;
-    if (FIX) {
+    double dscale = 1.0, dinv = 1.0;
+    if (FIX64) {
+        int e;
+        frexp(double(k.r1 - k.r0) * (double)g.fix_bound, &e);
+        dscale = ldexp(1.0, 62 - e);
+        dinv = ldexp(1.0, e - 62);
+    } else if (FIX) {
         int e, e1;
         frexpf(float(k.r1 - k.r0) * g.fix_bound, &e);
         frexpf(g.fix_bound, &e1);
@@ -748,7 +762,9 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     }
     const T factor = (T)g.acc_factor;
     auto add = [&](int li, T v, T vi) {
-        if (FIX) {
+        if (FIX64) {
+            atomicAdd(&acc64[li], (unsigned long long)__double2ll_rn((double)v));
+        } else if (FIX) {
             int hi, lo;
             fix_split((float)v, hi, lo);
             atomicAdd(&acc_hi[li], hi);
@@ -761,7 +777,8 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     for (unsigned r = k.r0 + threadIdx.x; r < k.r1; r += blockDim.x) {
         const PRec<T> pr = rec[r];
         T wr = pr.wr * factor, wi = pr.wi * factor;
-        if (FIX) wr *= (T)fscale;
+        if (FIX64) wr = (T)((double)wr * dscale);
+        else if (FIX) wr *= (T)fscale;
         const int anc[3] = {pr.i[0], pr.i[1], pr.i[2]};
         if (stencil_separable(g, anc)) {
             T w[3][W];
@@ -810,8 +827,9 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     __syncthreads();
     // FIX: the exact integer sum rounded once to FP32, then scaled by a power of two (exact)
     for_tile_cells(g, tile, [&](int li, long long cell) {
-        const T v = FIX ? (T)(__ll2float_rn((long long)acc_hi[li] * 1048576LL + (long long)acc_lo[li]) * finv)
-                        : acc[li];
+        const T v = FIX64 ? (T)(__ll2double_rn((long long)acc64[li]) * dinv)
+                    : FIX ? (T)(__ll2float_rn((long long)acc_hi[li] * 1048576LL + (long long)acc_lo[li]) * finv)
+                          : acc[li];
         if (k.multi == 0) {
             mesh_re[cell] = v;
             if (CPLX) mesh_im[cell] = acc_im[li];

@@ -43,6 +43,7 @@ struct hg_ctx {
                                int w_off, bool on_device) = 0;
     virtual void set_profiling(bool on) = 0;
     virtual std::string kernel_stats() = 0;
+    virtual std::string tuning() = 0;
     virtual void pk_box(int ell, double *pk_save, int *n_mode, double *norm) = 0;
     virtual void bk_box_multi(const std::vector<hg::MP> &mps, int ith, double *bk_save, double *sn_save,
                               double *norm) = 0;

@@ -746,7 +746,7 @@ struct Engine : public hg_ctx {
         static_assert(CHUNK <= 2048, "the fixed-point lo word holds at most 2048 adds of < 2^20");
         bool fix = false;
         AssignGeom agx = ag;
-        if constexpr (sizeof(U) == 4 && !CPLX) {
+        if constexpr (!CPLX) {  // FP32: two 32-bit words per cell; FP64: one 64-bit word
             fix = true;
             double wmax = 0.0;
             for (const auto &src : srcs) {
@@ -771,11 +771,12 @@ struct Engine : public hg_ctx {
 
     template <typename U, bool CPLX, int SCHEME>
     void launch_tile_accum(bool fix, size_t tbytes, unsigned nchunks, const AssignGeom &ag, U *out_re, U *out_im) {
-        if constexpr (sizeof(U) == 4 && !CPLX) {
-            if (fix) {
+        if constexpr (!CPLX) {
+            if (fix) {  // FP32: two words of 4 bytes per cell; FP64: one of 8
+                const size_t sm = (sizeof(U) == 4) ? 2 * tbytes : tbytes;
                 auto kern = k_tile_accum<U, false, true, SCHEME>;
-                HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * tbytes)));
-                kern<<<nchunks, 256, 2 * tbytes, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
+                HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                kern<<<nchunks, 256, sm, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
                 return;
             }
         }
@@ -1191,25 +1192,88 @@ struct Engine : public hg_ctx {
                  double(o1) * (Kz + Mz) * sizeof(C));
         pass<+1>(My, LdRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, StArr<T>{dp<C>(T2), My, Mz}, o2, Mz, "chain_y",
                  double(o2) * (Ky + My) * Mz * sizeof(C));
-        kb("chain_x_fused", double(ns) * 2.0 * Kx * My * Mz * sizeof(C) + double(Mx) * My * Mz * sizeof(C));
         const C *Gp = dp<C>(Gsrc);
-        if (Mx == 256)
-            HG_CK((launch_chain_x_reg_L<T, 256>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
-        else if (Mx == 192)
-            HG_CK((launch_chain_x_reg_L<T, 192>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
-        else if (Mx == 128)
-            HG_CK((launch_chain_x_reg_L<T, 128>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
-        else if (Mx == 64)
-            HG_CK((launch_chain_x_reg_L<T, 64>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
-        else if (Mx == 32)
-            HG_CK((launch_chain_x_reg_L<T, 32>(dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st)));
-        else
-            HG_CK(launch_chain_x<T>(Mx, dp<C>(T2), Gp, ns, Kx, S.s[0], (long long)My * Mz, twiddles(Mx), st));
+        const long long plane = (long long)My * Mz;
+        const int var = chain_variant(Mx, Kx, S.s[0], ns, plane, Gp);  // before the timed launch
+        kb("chain_x_fused", double(ns) * 2.0 * Kx * My * Mz * sizeof(C) + double(Mx) * My * Mz * sizeof(C));
+        HG_CK(launch_chain_x_any(Mx, var, dp<C>(T2), Gp, ns, Kx, S.s[0], plane));
         ke();
         pass<-1>(My, LdArr<T>{dp<C>(T2), My, Mz}, StRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, o2, Mz, "chain_y",
                  double(o2) * (Ky + My) * Mz * sizeof(C));
         pass<-1>(Mz, LdArr<T>{dp<C>(T1), Mz, 1}, StCube<T>{Q, Kz, Mz, S.s[2]}, o1, 1, "chain_z",
                  double(o1) * (Kz + Mz) * sizeof(C));
+    }
+
+    cudaError_t launch_chain_x_any(int Mx, int var, C *t2, const C *Gp, int ns, int Kx, int s0, long long plane) {
+        switch (Mx) {
+            case 256: return launch_chain_x_reg_L<T, 256>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
+            case 192: return launch_chain_x_reg_L<T, 192>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
+            case 128: return launch_chain_x_reg_L<T, 128>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
+            case 64: return launch_chain_x_reg_L<T, 64>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
+            case 32: return launch_chain_x_reg_L<T, 32>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
+            default: return launch_chain_x<T>(Mx, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
+        }
+    }
+
+    // Launch-shape autotuning of the fused chain pass: the first time a chain runs on a given
+    // grid, every variant (kChainVariants) transforms a copy of the first two shells twice
+    // and the faster of the timed second runs is kept for the context.  The copy is restored
+    // before each run, so every variant sees the same data; the real shells are untouched.
+    struct Tuned {
+        int variant;
+        std::vector<float> ms;
+    };
+    std::map<int, Tuned> chain_tuned;  // by transform length
+    DBuf tune_buf, tune_src;
+    int chain_variant(int Mx, int Kx, int s0, int ns, long long plane, const C *Gp) {
+        if (Mx != 32 && Mx != 64 && Mx != 128 && Mx != 192 && Mx != 256) return 0;
+        auto it = chain_tuned.find(Mx);
+        if (it != chain_tuned.end()) return it->second.variant;
+        const int nsh = std::min(ns, 2);
+        const size_t bytes = sizeof(C) * (size_t)Kx * plane * nsh;
+        HG_CK(tune_src.ensure(bytes));
+        HG_CK(tune_buf.ensure(bytes));
+        HG_CK(cudaMemcpyAsync(tune_src.p, T2.p, bytes, cudaMemcpyDeviceToDevice, st));
+        Tuned tu{0, std::vector<float>(kNumChainVariants, 0.f)};
+        float best = 1e30f;
+        for (int v = 0; v < kNumChainVariants; v++) {
+            for (int rep = 0; rep < 2; rep++) {
+                HG_CK(cudaMemcpyAsync(tune_buf.p, tune_src.p, bytes, cudaMemcpyDeviceToDevice, st));
+                HG_CK(cudaEventRecord(ev0, st));
+                HG_CK(launch_chain_x_any(Mx, v, dp<C>(tune_buf), Gp, nsh, Kx, s0, plane));
+                HG_CK(cudaEventRecord(ev1, st));
+            }
+            HG_CK(cudaEventSynchronize(ev1));
+            float ms = 0.f;
+            HG_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+            tu.ms[v] = ms;
+            if (ms < best) {
+                best = ms;
+                tu.variant = v;
+            }
+        }
+        HG_CK(cudaEventRecord(ev0, st));  // begin()'s event, reused above: statistics time from here
+        tune_buf.release();
+        tune_src.release();
+        chain_tuned[Mx] = tu;
+        return tu.variant;
+    }
+    std::string tuning() override {
+        std::string out;
+        char line[256];
+        for (const auto &kv : chain_tuned) {
+            const ChainVariant &cv = kChainVariants[kv.second.variant];
+            snprintf(line, sizeof(line), "chain_x L=%d: variant %d (B=%d, G %s, %s)", kv.first, kv.second.variant,
+                     cv.B, cv.gs ? "staged in shared memory" : "read from L2", cv.pf ? "cp.async prefetch" : "no prefetch");
+            out += line;
+            for (size_t v = 0; v < kv.second.ms.size(); v++) {
+                snprintf(line, sizeof(line), "%s%.4f", v ? " " : "; ms per variant: ", kv.second.ms[v]);
+                out += line;
+            }
+            out += "\n";
+        }
+        if (hi) out += hi->tuning();
+        return out;
     }
 
     // Q_b[j] for the bispectrum shells with the G of key gk

@@ -527,16 +527,28 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
     }
 }
 
-// The chain kernel: 16 columns per CTA (256 threads); the CTA's G tile (L x 16) is staged
-// once in shared memory next to the exchange buffer and reused by every shell.
-template <typename T, int L>
+// The chain kernel's launch shape (a tunable variant): B columns per CTA; GS: the CTA's G
+// tile (L x B) staged once in shared memory for all shells, else each thread reads its G
+// values from global memory (L2-resident) per shell; PF: the next shell's input rows stream
+// into shared memory by cp.async while the current one is transformed, else each shell's
+// rows are loaded into registers when it starts.  Less shared memory per CTA means more
+// CTAs per SM; which is faster depends on the precision and the line length, so the engine
+// times the variants once per geometry and keeps the fastest.
+struct ChainVariant {
+    int B;
+    bool gs, pf;
+};
+constexpr ChainVariant kChainVariants[] = {{16, true, true}, {16, false, true}, {16, false, false},
+                                           {8, true, true},  {8, false, false}};
+constexpr int kNumChainVariants = 5;
+
+template <typename T, int L, int B, bool GS, bool PF>
 struct ChainCfg {
     static constexpr int R2 = Split<L>::R2;
-    static constexpr int B = 16;
     static constexpr int NT = R2 * B;
-    // exchange buffer, G tile, and the next shell's input rows (streamed in by cp.async)
     static constexpr size_t smem() {
-        return sizeof(cplx<T>) * ((size_t)XchgLayout<L, true, B>::ELEMS + 2 * (size_t)L * B);
+        return sizeof(cplx<T>) * ((size_t)XchgLayout<L, true, B>::ELEMS + (GS ? (size_t)L * B : 0) +
+                                  (PF ? (size_t)L * B : 0));
     }
 };
 
@@ -544,27 +556,29 @@ struct ChainCfg {
 // columns), G [x][y][z].  Per shell j: load the K kept rows, inverse FFT, * G, forward FFT,
 // store the K kept rows.  The product happens in the positions a thread holds after the
 // inverse transform, which are its step-A positions of the forward transform.
-template <typename T, int L>
-__global__ void __launch_bounds__(ChainCfg<T, L>::NT, (sizeof(T) == 4) ? 2 : 1)
+template <typename T, int L, int B, bool GS, bool PF>
+__global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, (sizeof(T) == 4) ? 2 : 1)
     k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
                   const cplx<T> *__restrict__ tw) {
-    using CF = ChainCfg<T, L>;
-    using X = XchgLayout<L, true, CF::B>;
-    constexpr int R1 = X::R1, R2 = X::R2, B = CF::B;
+    using CF = ChainCfg<T, L, B, GS, PF>;
+    using X = XchgLayout<L, true, B>;
+    constexpr int R1 = X::R1, R2 = X::R2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
-    cplx<T> *Gs = S + X::ELEMS;  // [x][b]
-    cplx<T> *Pb = Gs + L * B;    // next shell's input, [x][b]; rows outside |n| <= s stay zero
+    cplx<T> *Gs = S + X::ELEMS;              // [x][b] (GS)
+    cplx<T> *Pb = Gs + (GS ? L * B : 0);     // next shell's input, [x][b] (PF); rows outside |n| <= s stay zero
     const int t = threadIdx.x / B, b = threadIdx.x % B;
     const long long i = (long long)blockIdx.x * B + b;
     const bool ok = i < plane;
-    for (int e = threadIdx.x; e < L * B; e += CF::NT) {
-        const int x = e / B, bb = e % B;
-        const long long ii = (long long)blockIdx.x * B + bb;
-        Gs[e] = (ii < plane) ? G[(long long)x * plane + ii] : mk<T>(0, 0);
-        Pb[e] = mk<T>(0, 0);
+    if constexpr (GS || PF) {
+        for (int e = threadIdx.x; e < L * B; e += CF::NT) {
+            const int x = e / B, bb = e % B;
+            const long long ii = (long long)blockIdx.x * B + bb;
+            if constexpr (GS) Gs[e] = (ii < plane) ? G[(long long)x * plane + ii] : mk<T>(0, 0);
+            if constexpr (PF) Pb[e] = mk<T>(0, 0);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     // the K kept rows of shell j into Pb (position x = n mod L of row c = n + s)
     auto prefetch = [&](int j) {
         const cplx<T> *tj = t2 + (long long)j * K * plane;
@@ -577,26 +591,41 @@ __global__ void __launch_bounds__(ChainCfg<T, L>::NT, (sizeof(T) == 4) ? 2 : 1)
         }
         asm volatile("cp.async.commit_group;\n" ::);
     };
-    if (ns > 0) prefetch(0);
+    auto g_at = [&](int pos) -> cplx<T> {
+        if constexpr (GS) return Gs[pos * B + b];
+        else return ok ? G[(long long)pos * plane + i] : mk<T>(0, 0);
+    };
+    if constexpr (PF) {
+        if (ns > 0) prefetch(0);
+    }
     for (int j = 0; j < ns; j++) {
         cplx<T> *tj = t2 + (long long)j * K * plane;
-        asm volatile("cp.async.wait_group 0;\n" ::);
-        __syncthreads();
         cplx<T> v[R1];
+        if constexpr (PF) {
+            asm volatile("cp.async.wait_group 0;\n" ::);
+            __syncthreads();
 #pragma unroll
-        for (int n1 = 0; n1 < R1; n1++) v[n1] = Pb[(R2 * n1 + t) * B + b];
-        __syncthreads();  // Pb is read: the next shell streams in while this one is transformed
-        if (j + 1 < ns) prefetch(j + 1);
+            for (int n1 = 0; n1 < R1; n1++) v[n1] = Pb[(R2 * n1 + t) * B + b];
+            __syncthreads();  // Pb is read: the next shell streams in while this one is transformed
+            if (j + 1 < ns) prefetch(j + 1);
+        } else {
+#pragma unroll
+            for (int n1 = 0; n1 < R1; n1++) {
+                const int x = R2 * n1 + t;
+                const int n = (x < L / 2) ? x : x - L;
+                v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
+            }
+        }
         line_fft2<T, L, +1, true, B>(v, S, t, b, tw);
         if constexpr (R1 == R2) {
 #pragma unroll
-            for (int r = 0; r < R1; r++) v[r] = v[r] * Gs[pos_of_reg<L>(t, r) * B + b];
+            for (int r = 0; r < R1; r++) v[r] = v[r] * g_at(pos_of_reg<L>(t, r));
         } else {
             cplx<T> u[R1];
 #pragma unroll
             for (int n1 = 0; n1 < R1; n1++) {
                 const int r = reg_of_n1<L>(n1);
-                u[n1] = v[r] * Gs[pos_of_reg<L>(t, r) * B + b];
+                u[n1] = v[r] * g_at(pos_of_reg<L>(t, r));
             }
 #pragma unroll
             for (int n1 = 0; n1 < R1; n1++) v[n1] = u[n1];
@@ -613,15 +642,30 @@ __global__ void __launch_bounds__(ChainCfg<T, L>::NT, (sizeof(T) == 4) ? 2 : 1)
     }
 }
 
-template <typename T, int L>
-inline cudaError_t launch_chain_x_reg_L(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
-                                        const cplx<T> *tw, cudaStream_t st) {
-    using CF = ChainCfg<T, L>;
-    size_t smem = CF::smem();
-    cudaFuncSetAttribute(k_chain_x_reg<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    unsigned tiles = (unsigned)((plane + CF::B - 1) / CF::B);
-    k_chain_x_reg<T, L><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);
+template <typename T, int L, int B, bool GS, bool PF>
+inline cudaError_t launch_chain_x_v(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
+                                    const cplx<T> *tw, cudaStream_t st) {
+    using CF = ChainCfg<T, L, B, GS, PF>;
+    const size_t smem = CF::smem();
+    cudaError_t e = cudaFuncSetAttribute(k_chain_x_reg<T, L, B, GS, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    const unsigned tiles = (unsigned)((plane + B - 1) / B);
+    k_chain_x_reg<T, L, B, GS, PF><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);
     return cudaGetLastError();
+}
+
+// variant v of kChainVariants
+template <typename T, int L>
+inline cudaError_t launch_chain_x_reg_L(int v, cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
+                                        const cplx<T> *tw, cudaStream_t st) {
+    switch (v) {
+        case 1: return launch_chain_x_v<T, L, 16, false, true>(t2, G, ns, K, s, plane, tw, st);
+        case 2: return launch_chain_x_v<T, L, 16, false, false>(t2, G, ns, K, s, plane, tw, st);
+        case 3: return launch_chain_x_v<T, L, 8, true, true>(t2, G, ns, K, s, plane, tw, st);
+        case 4: return launch_chain_x_v<T, L, 8, false, false>(t2, G, ns, K, s, plane, tw, st);
+        default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, st);
+    }
 }
 
 }  // namespace HG_TU_NS

@@ -235,12 +235,52 @@ int hg_batch_run(hg_ctx *ctx, const hg_mock *mocks, int n_mocks, int n_pk, const
                  const int *bk_ells, int n_zeta, const int *zeta_ells, double *out);
 long long hg_batch_block_len(const hg_ctx *ctx, int n_pk, int n_bk, int n_zeta);
 
+/* ---- catalogue ingest (host side; the reference's readers, native and multi-threaded) */
+
+/* Gadget-2 snapshot header block: 256 bytes, the layout of ParticleGadgetClass::io_header
+ * (particleGadget.hpp:33-50), which is the file format. */
+typedef struct hg_gadget_header {
+    unsigned int npart[6];
+    double mass[6];
+    double time;
+    double redshift;
+    int flag_sfr;
+    int flag_feedback;
+    unsigned int npartTotal[6];
+    int flag_cooling;
+    int num_files;
+    double BoxSize;
+    double Omega0;
+    double OmegaLambda;
+    double HubbleParam;
+    char fill[256 - 6 * 4 - 6 * 8 - 2 * 8 - 2 * 4 - 6 * 4 - 2 * 4 - 4 * 8];
+} hg_gadget_header;
+
+/* ASCII catalogue.  Replaces ParticleBOSSClass::readParticleBOSS (particle.hpp:93-154):
+ * every line from which ncols numbers can be read (as sscanf "%lf %lf ..." reads them:
+ * x y z w for ncols = 4) is one record, other lines are skipped.  *out: n x ncols doubles,
+ * allocated here, released with hg_free.  Errors: hg_last_error(NULL). */
+int hg_read_ascii(const char *path, int ncols, double **out, long long *n);
+
+/* Gadget snapshot base.0 .. base.(num_files-1).  Replaces
+ * ParticleGadgetClass::readParticlesFromGagdetSnapshot (particleGadget.hpp:211-298):
+ * *out holds n records {pos[3], vel[3] * sqrt(a)} (the ParticleGadgetClass layout, 48-byte
+ * stride, for hg_set_particles), allocated here, released with hg_free; *hdr (may be NULL)
+ * receives base.0's header. */
+int hg_read_gadget(const char *base, double **out, long long *n, hg_gadget_header *hdr);
+void hg_free(void *p);
+
 /* Per-kernel device timing: when on, every kernel launch of this library is bracketed by
  * CUDA events on the context's stream.  hg_kernel_stats writes one line per kernel name:
  * "name<TAB>launches<TAB>total_ms<TAB>modelled_bytes".  These replace the reference's
  * clock() progress prints (bispec.hpp:1170-1171, powerspec.hpp:63-66). */
 int hg_set_profiling(hg_ctx *ctx, int on);
 int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen);
+
+/* The launch shapes the context's autotuner picked (one line per tuned kernel and grid: the
+ * chosen variant and the measured time of every variant).  No counterpart in the
+ * reference. */
+int hg_tuning(hg_ctx *ctx, char *buf, long long buflen);
 
 /* Allocation-free periodic-box power-spectrum multipole.  No counterpart in the reference:
  * it is the binning step of hg_pk_box run on a density spectrum the caller already holds

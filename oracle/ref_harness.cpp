@@ -282,6 +282,33 @@ int main(int argc, char **argv) {
         else if (!strcmp(argv[i], "--unit") && i + 1 < argc) unit = argv[++i];
         else pos.push_back(argv[i]);
     }
+    /* --read-ascii FILE OUT / --read-gadget BASE OUT: run the reference's readers
+     * (particle.hpp:93-154, particleGadget.hpp:211-298) and write what they hold as raw
+     * doubles (x y z w / x y z vx vy vz per particle) */
+    if (pos.size() == 3 && !strcmp(pos[0], "--read-ascii")) {
+        ParticleBOSSClass P;
+        std::string fn(pos[1]);
+        if (P.readParticleBOSS(fn)) return fail("readParticleBOSS");
+        FILE *fo = fopen(pos[2], "wb");
+        for (long long i = 0; i < P.n_tot; i++) {
+            double r[4] = {P[i].pos[0], P[i].pos[1], P[i].pos[2], P[i].w};
+            fwrite(r, sizeof(double), 4, fo);
+        }
+        fclose(fo);
+        return 0;
+    }
+    if (pos.size() == 3 && !strcmp(pos[0], "--read-gadget")) {
+        ParticleGadgetClass P;
+        std::string fn(pos[1]);
+        if (P.readParticlesFromGagdetSnapshot(fn)) return fail("readParticlesFromGagdetSnapshot");
+        FILE *fo = fopen(pos[2], "wb");
+        for (long long i = 0; i < P.n_tot; i++) {
+            double r[6] = {P[i].pos[0], P[i].pos[1], P[i].pos[2], P[i].vel[0], P[i].vel[1], P[i].vel[2]};
+            fwrite(r, sizeof(double), 6, fo);
+        }
+        fclose(fo);
+        return 0;
+    }
     char *pargv[2] = {argv[0], (char *)pos[0]};
     ParameterClass param;
     if (param.readParameters(pargv)) return fail("param.readParameters");

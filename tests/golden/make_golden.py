@@ -12,6 +12,7 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --odd (only box_odd.npz: odd l1 + l2)
     python tests/golden/make_golden.py --bk256 (only box_bk_256.npz, from the restatement)
     python tests/golden/make_golden.py --xi     (only xi_window.npz: 2PCF, window 2PCF / 3PCF)
+    python tests/golden/make_golden.py --ingest (only ingest.npz: the ASCII and Gadget readers)
     python tests/golden/make_golden.py --configs (only box_config_sizes.npz: 128^3 and 512^3)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
@@ -237,6 +238,55 @@ def make_xi():
     np.savez_compressed(os.path.join(HERE, "xi_window.npz"), **d)
 
 
+def gadget_files(rng, n_per_file, time=0.5, box=1000.0):
+    """Bytes of a Gadget-2 snapshot split over len(n_per_file) files (256-byte header, then
+    position, velocity and id blocks, each between Fortran record markers)."""
+    import struct
+    total = sum(n_per_file)
+    files, pos_all, vel_all = [], [], []
+    for i, npf in enumerate(n_per_file):
+        pos = rng.uniform(0.0, box, size=(npf, 3)).astype(np.float32)
+        vel = rng.normal(0.0, 300.0, size=(npf, 3)).astype(np.float32)
+        hdr = struct.pack("6I6dddii6Iii4d", 0, npf, 0, 0, 0, 0, 0.0, 1.5, 0, 0, 0, 0, time, 1.0 / time - 1.0, 0, 0,
+                          0, total, 0, 0, 0, 0, 0, len(n_per_file), box, 0.31, 0.69, 0.68)
+        hdr += b"\0" * (256 - len(hdr))
+        rec = lambda b: struct.pack("i", len(b)) + b + struct.pack("i", len(b))
+        ids = np.arange(npf, dtype=np.int64) + sum(n_per_file[:i])
+        files.append(rec(hdr) + rec(pos.tobytes()) + rec(vel.tobytes()) + rec(ids.tobytes()))
+        pos_all.append(pos)
+        vel_all.append(vel)
+    return files
+
+
+def make_ingest():
+    """The reference's own readers (readParticleBOSS particle.hpp:93-154,
+    readParticlesFromGagdetSnapshot particleGadget.hpp:211-298) run through the harness on
+    an ASCII file with lines that do and do not parse, and on a two-file Gadget snapshot."""
+    import subprocess
+    import tempfile
+    rng = np.random.default_rng(23)
+    lines = ["# x y z w", "", "1 2 3 4", "1 2 3", "1 2 3 4 5 6", "  5.5\t6.5  7.5 8.5\r", "1,2,3,4",
+             "+1 -2 .3 4.", "1e5 2E-3 -0 0x1p3", "abc 1 2 3", "1 2 3 nan", "7 8 9 1e400", "\t", "3 4 5 6 # tail"]
+    body = rng.uniform(-2000.0, 2000.0, size=(60000, 4))
+    text = "\n".join(lines) + "\n" + "\n".join(" ".join(repr(float(v)) for v in row) for row in body) + "\n9 9 9 9"
+    gfiles = gadget_files(rng, [3000, 2500])
+    with tempfile.TemporaryDirectory() as tmp:
+        ap = os.path.join(tmp, "cat.txt")
+        with open(ap, "w") as f:
+            f.write(text)
+        gb = os.path.join(tmp, "snap")
+        for i, b in enumerate(gfiles):
+            with open(f"{gb}.{i}", "wb") as f:
+                f.write(b)
+        for mode, src in (("--read-ascii", ap), ("--read-gadget", gb)):
+            subprocess.run([ref_runner.HARNESS, mode, src, os.path.join(tmp, mode + ".f64")], check=True)
+        ascii_ref = np.fromfile(os.path.join(tmp, "--read-ascii.f64")).reshape(-1, 4)
+        gadget_ref = np.fromfile(os.path.join(tmp, "--read-gadget.f64")).reshape(-1, 6)
+    np.savez_compressed(os.path.join(HERE, "ingest.npz"), ascii_text=np.frombuffer(text.encode(), dtype=np.uint8),
+                        ascii_ref=ascii_ref, gadget0=np.frombuffer(gfiles[0], dtype=np.uint8),
+                        gadget1=np.frombuffer(gfiles[1], dtype=np.uint8), gadget_ref=gadget_ref)
+
+
 def catalogue_digest(pos: np.ndarray) -> np.ndarray:
     """Count, coordinate sums and sums of squares: the tests regenerate the large catalogues
     from their seeds and check these first, so a generator change cannot pass silently."""
@@ -283,6 +333,10 @@ def make_config_sizes():
 
 
 def main():
+    if "--ingest" in sys.argv:
+        make_ingest()
+        print("fixtures written")
+        return
     if "--xi" in sys.argv:
         make_xi()
         print("fixtures written")
