@@ -34,6 +34,9 @@ SYMBOLS = (
     "hg_xi_window",
     "hg_zeta_window",
     "hg_zeta_window_multi",
+    "hg_reconstruct",
+    "hg_pk_box_recon",
+    "hg_xi_box_recon",
     "hg_batch_run",
     "hg_batch_block_len",
     "hg_read_ascii",
@@ -163,6 +166,12 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_zeta_window.restype = ctypes.c_int
     lib.hg_zeta_window_multi.argtypes = [vp, i_, c_ip, i_, d_, c_dp, c_dp, c_dp]
     lib.hg_zeta_window_multi.restype = ctypes.c_int
+    lib.hg_reconstruct.argtypes = [vp, i_, d_, d_, d_, d_, c_dp, c_dp]
+    lib.hg_reconstruct.restype = ctypes.c_int
+    lib.hg_pk_box_recon.argtypes = [vp, i_, d_, c_dp, c_ip, c_dp]
+    lib.hg_pk_box_recon.restype = ctypes.c_int
+    lib.hg_xi_box_recon.argtypes = [vp, i_, d_, c_dp, c_ip, c_dp]
+    lib.hg_xi_box_recon.restype = ctypes.c_int
     lib.hg_batch_run.argtypes = [vp, ctypes.POINTER(HgMock), i_, i_, c_ip, i_, c_ip, i_, c_ip, c_dp]
     lib.hg_batch_run.restype = ctypes.c_int
     lib.hg_batch_block_len.argtypes = [vp, i_, i_, i_]

@@ -292,6 +292,28 @@ class Context:
         c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nr)
         return c(z), c(sn), norm.value
 
+    def reconstruct(self, b1_fid: float, RG: float, box: bool = False, alpha: float = 0.0, vsurvey: float = 0.0):
+        """BAO reconstruction of the current data (slot 0) and randoms (slot 1): their shifted
+        positions as two (n, 3) arrays (particle_reconstruction.hpp:12-402)."""
+        nd = self._keep[0].shape[0]
+        nr = self._keep[1].shape[0]
+        pd, pr = np.zeros((nd, 3)), np.zeros((nr, 3))
+        self._check(self._lib.hg_reconstruct(self._h, int(bool(box)), float(b1_fid), float(RG), float(alpha),
+                                             float(vsurvey), _dp(pd), _dp(pr)))
+        return pd, pr
+
+    def pk_box_recon(self, ell: int, alpha: float):
+        nk = self.binning.n_kbin
+        out = np.zeros(2 * nk)
+        nmode = np.zeros(nk, dtype=np.int32)
+        norm = ctypes.c_double()
+        self._check(self._lib.hg_pk_box_recon(self._h, int(ell), float(alpha), _dp(out),
+                                              nmode.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(norm)))
+        return out[0::2] + 1j * out[1::2], nmode, norm.value
+
+    def xi_box_recon(self, ell: int, alpha: float):
+        return self._xi(self._lib.hg_xi_box_recon, int(ell), float(alpha))
+
     def batch_run(self, mocks, pk_ells=(), bk_multipoles=(), zeta_multipoles=()):
         """Box statistics of several catalogues through hg_batch_run (the next catalogue is
         copied to the GPU while the current one is measured).  mocks: (n, fields) float64

@@ -223,6 +223,21 @@ int hg_zeta_window_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith
     HG_GUARD(ctx, ctx->zeta_window_multi(mps, ith_rbin, vsurvey, zeta_save, sn_save, norm));
 }
 
+int hg_reconstruct(hg_ctx *ctx, int box, double b1_fid, double RG, double alpha, double vsurvey, double *pos_D,
+                   double *pos_R) {
+    HG_GUARD(ctx, ctx->reconstruct(box, b1_fid, RG, alpha, vsurvey, pos_D, pos_R));
+}
+
+int hg_pk_box_recon(hg_ctx *ctx, int ell, double alpha, double *pk_save, int *n_mode, double *norm) {
+    if (!pk_save) return -1;
+    HG_GUARD(ctx, ctx->pk_box_recon(ell, alpha, pk_save, n_mode, norm));
+}
+
+int hg_xi_box_recon(hg_ctx *ctx, int ell, double alpha, double *xi_save, int *n_mode, double *norm) {
+    if (!xi_save) return -1;
+    HG_GUARD(ctx, ctx->xi_box_recon(ell, alpha, xi_save, n_mode, norm));
+}
+
 long long hg_batch_block_len(const hg_ctx *ctx, int n_pk, int n_bk, int n_zeta) {
     if (!ctx || n_pk < 0 || n_bk < 0 || n_zeta < 0) return -1;
     return hg::batch_block_len(ctx->cfg, n_pk, n_bk, n_zeta);

@@ -178,7 +178,7 @@ __global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt,
                 if (k0_special && ix == 0 && iy == 0 && iz == 0) {
                     pk2 = mk<double>(k0_re, k0_im);
                 } else {
-                    pk2 = d1 * conjg(d2);
+                    pk2 = mul_conj_rn(d1, d2);
                 }
                 double C = shot_tab(tabs, ix, iy, iz, assign);
                 pk2 = pk2 - mk<double>(S_re * C, S_im * C);

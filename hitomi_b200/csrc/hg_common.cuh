@@ -47,6 +47,13 @@ template <typename T>
 __host__ __device__ __forceinline__ cplx<T> operator*(cplx<T> a, T s) { return mk<T>(a.x * s, a.y * s); }
 template <typename T>
 __host__ __device__ __forceinline__ cplx<T> conjg(cplx<T> a) { return mk<T>(a.x, -a.y); }
+// a conj(b) with every product and sum rounded separately, as std::complex<double> evaluates
+// it on the host: the imaginary part of a conj(a) is then exactly zero (a fused multiply-add
+// would leave the rounding error of one product in it)
+__device__ __forceinline__ cplx<double> mul_conj_rn(cplx<double> a, cplx<double> b) {
+    return mk<double>(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dsub_rn(__dmul_rn(a.y, b.x), __dmul_rn(a.x, b.y)));
+}
 
 typedef cplx<double> zd;
 typedef cplx<float> zf;

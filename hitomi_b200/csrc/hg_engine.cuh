@@ -1418,12 +1418,18 @@ struct Engine : public hg_ctx {
                    "bispectrum / 3PCF shot noise and the 2PCF need equal cell sizes on all axes");
         build_orbits();
         if (xi_valid && xi_k0 == k0prod) return;
+        build_box_xi(half_spec(), double(slot[0].n), k0prod);
         xi_k0 = k0prod;
+        xi_valid = true;
+    }
+
+    // The box correlation field of a real field's half spectrum f, (|f|^2 - S C) / W^2 / V,
+    // after its x and y inverse passes, into xi (even and odd kz planes as one complex field)
+    void build_box_xi(const Spec<T> &f, double S, double k0prod) {
         const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], nh = n2 / 2;
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
-        const double S = double(slot[0].n);
-        LdXiHat<T> ld{half_spec(), n2, xtabs, S, k0prod, invV};
+        LdXiHat<T> ld{f, n2, xtabs, S, k0prod, invV};
         const long long yz = (long long)n1 * nh, tot = (long long)n0 * yz;
         unsigned blocks = (unsigned)std::min<long long>(grid1(tot, 256), 148 * 16);
         kb("xi_synth", double(tot) * sizeof(C) * 2.0);
@@ -1431,7 +1437,6 @@ struct Engine : public hg_ctx {
         ke();
         pass<+1>(n0, LdArr<T>{dp<C>(xi), n0, yz}, StArr<T>{dp<C>(xi), n0, yz}, 1, yz, "fft_xi_x");
         pass<+1>(n1, LdArr<T>{dp<C>(xi), n1, nh}, StArr<T>{dp<C>(xi), n1, nh}, n0, nh, "fft_xi_y");
-        xi_valid = true;
     }
 
     template <int L>
@@ -2910,6 +2915,88 @@ struct Engine : public hg_ctx {
         return particle_sums(s, q)[0];
     }
 
+    // ------------------------------------------------------------------ BAO reconstruction
+    // calcReconstructionParticles (particle_reconstruction.hpp:12-208; box: :210-402) on this
+    // context's mesh (the reference's n_mesh_recon): the D - alpha R field with the
+    // context's scheme, its transform divided by W, three displacement components
+    // Psi_a = FFT_+[-i (W_G / b1) (k_a / k^2) D / W / V] scaled by V_survey / sum w_D
+    // (box: V / N_D, alpha = double(N_D / N_R) with the reference's integer division),
+    // and every particle of both catalogues shifted by their TSC interpolation.
+    DBuf psi_f[3], psi_tmp, shift_out;
+    void reconstruct(int box, double b1, double RG, double alpha, double vs, double *posD, double *posR) override {
+        HG_REQUIRE(slot[0].set && slot[1].set, "reconstruction needs data (slot 0) and randoms (slot 1)");
+        HG_REQUIRE(b1 != 0.0, "b1_fid must be non-zero");
+        begin();
+        double a = alpha, norm;
+        if (box) {
+            a = double(slot[0].n / slot[1].n);  // particle_reconstruction.hpp:221 (integer division)
+            norm = g.volume / double(slot[0].n);
+        } else {
+            const double wD = weight_sum(0);
+            HG_REQUIRE(wD != 0.0, "the summed data weights must be non-zero");
+            norm = vs / wD;
+        }
+        invalidate_stats();
+        src_kind = -1;
+        const SpecK D = sfield(SF_DELTA, 0, 0, a);
+        HG_CK(psi_tmp.ensure(sizeof(C) * g.ntot));
+        const long long yz = (long long)g.n[1] * g.n[2];
+        const unsigned blocks = (unsigned)std::min<long long>(grid1(g.ntot, 256), 148 * 16);
+        for (int ax = 0; ax < 3; ax++) {
+            kb("recon_psi", double(g.ntot) * (sizeof(C) + 0.5 * sizeof(C)));
+            k_recon_psi<T><<<blocks, 256, 0, st>>>(D.s, g, tabs, wpow, ax, RG, b1, dp<C>(psi_tmp));
+            ke();
+            pass<+1>(g.n[2], LdArr<T>{dp<C>(psi_tmp), g.n[2], 1}, StArr<T>{dp<C>(psi_tmp), g.n[2], 1},
+                     (long long)g.n[0] * g.n[1], 1, "fft_recon");
+            pass<+1>(g.n[1], LdArr<T>{dp<C>(psi_tmp), g.n[1], g.n[2]}, StArr<T>{dp<C>(psi_tmp), g.n[1], g.n[2]}, g.n[0],
+                     g.n[2], "fft_recon");
+            pass<+1>(g.n[0], LdArr<T>{dp<C>(psi_tmp), g.n[0], yz}, StArr<T>{dp<C>(psi_tmp), g.n[0], yz}, 1, yz,
+                     "fft_recon");
+            HG_CK(psi_f[ax].ensure(sizeof(T) * g.ntot));
+            kb("recon_psi", double(g.ntot) * (sizeof(C) + sizeof(T)));
+            k_real_scaled<T><<<blocks, 256, 0, st>>>(dp<C>(psi_tmp), g.ntot, norm, dp<T>(psi_f[ax]));
+            ke();
+        }
+        psi_tmp.release();
+        for (int s = 0; s < 2; s++) {
+            double *dst = s == 0 ? posD : posR;
+            if (!dst) continue;
+            const PartSrc src = survey_src(s, false, 0, 0, 1.0);
+            HG_CK(shift_out.ensure(sizeof(double) * 3 * src.n));
+            kb("recon_shift", double(src.n) * (24.0 + 24.0));
+            k_recon_shift<T><<<(unsigned)std::min<long long>(grid1(src.n, 256), 148 * 16), 256, 0, st>>>(
+                src, g, dp<T>(psi_f[0]), dp<T>(psi_f[1]), dp<T>(psi_f[2]), dp<double>(shift_out));
+            ke();
+            HG_CK(cudaMemcpyAsync(dst, shift_out.p, sizeof(double) * 3 * src.n, cudaMemcpyDeviceToHost, st));
+            HG_CK(cudaStreamSynchronize(st));
+        }
+        for (int ax = 0; ax < 3; ax++) psi_f[ax].release();
+        shift_out.release();
+        end();
+    }
+
+    // calcPowerSpectrumForBOXForReconstruction (powerspec.hpp:396-457): the box estimator on
+    // dn = n_D - alpha n_R (weights 1) with shot noise N_D + alpha^2 N_R (field.hpp:1190-1196)
+    void pk_box_recon(int ell, double alpha, double *pk_save, int *n_mode, double *norm) override {
+        HG_REQUIRE(ell >= 0, "ell must be >= 0");
+        HG_REQUIRE(slot[0].set && slot[1].set, "the reconstructed P needs data (slot 0) and randoms (slot 1)");
+        begin();
+        invalidate_stats();
+        src_kind = -1;
+        const SpecK f = sfield(SF_DELTA, 0, 0, alpha);
+        const double S = double(slot[0].n) + alpha * alpha * double(slot[1].n);
+        std::vector<double> avg;
+        std::vector<unsigned long long> nm;
+        pk_bin2(f.s, f.s, {LM{ell, 0}}, S, 0.0, avg, nm);
+        for (int i = 0; i < cfg.n_kbin; i++) {
+            pk_save[2 * i] = double(2 * ell + 1) * avg[2 * i];
+            pk_save[2 * i + 1] = double(2 * ell + 1) * avg[2 * i + 1];
+            if (n_mode) n_mode[i] = (int)nm[i];
+        }
+        if (norm) *norm = g.volume / double(slot[0].n) / double(slot[0].n);
+        end();
+    }
+
     // ------------------------------------------------------------------ 2PCF
     // The 2PCF's r binning (calcCorrelationFunction, field.hpp:854-977): fine index
     // int(|r| / 0.5 + 0.5) kept below 20000, coarse bin j takes fine i iff lower_j < 0.5 i <=
@@ -2985,6 +3072,34 @@ struct Engine : public hg_ctx {
             xi_save[2 * j + 1] = nm[j] != 0.0 ? scale * (xim[j] / nm[j]) : 0.0;
             if (n_mode) n_mode[j] = (int)nm[j];
         }
+    }
+
+    // calcTwoPointFunctionForBOXForReconstruction (powerspec.hpp:459-520): the box 2PCF of
+    // dn = n_D - alpha n_R (weights 1), shot noise N_D + alpha^2 N_R, norm V / N_D^2
+    void xi_box_recon(int ell, double alpha, double *xi_save, int *n_mode, double *norm) override {
+        HG_REQUIRE(ell >= 0, "ell must be >= 0");
+        HG_REQUIRE(slot[0].set && slot[1].set, "the reconstructed 2PCF needs data (slot 0) and randoms (slot 1)");
+        HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
+                   "the 2PCF needs equal cell sizes on all axes");
+        begin();
+        invalidate_stats();
+        src_kind = -1;
+        xi2_geometry();
+        const SpecK f = sfield(SF_DELTA, 0, 0, alpha);
+        build_box_xi(f.s, double(slot[0].n) + alpha * alpha * double(slot[1].n), f.k0r * f.k0r + f.k0i * f.k0i);
+        xi_valid = false;  // not the box density's correlation field
+        HistSpec hs;
+        memset(&hs, 0, sizeof(hs));
+        hs.nh = 1;
+        hs.parity[0] = (ell % 2 == 0) ? 1 : -1;
+        hs.term[0][hs.nterm[0]++] = YTerm{ell, 0, 0, 0, 1.0};
+        orbit_weight_poly(hs, 0);
+        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim));
+        HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim, st));
+        launch_orbit(g.n[2], hs, (int)orbit_n2xy.size(), dp<double>(hist_tmp));
+        xi2_bin(dp<double>(hist_tmp), double(2 * ell + 1), xi_save, n_mode);
+        if (norm) *norm = g.volume / double(slot[0].n) / double(slot[0].n);
+        end();
     }
 
     // calcTwoPointCorrelationFunctionForBOX (powerspec.hpp:334-393): xi = FFT_+[(|dn|^2 - N C)

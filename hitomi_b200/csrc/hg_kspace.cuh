@@ -115,6 +115,82 @@ __global__ void k_family_A(const ShellEnt *ent, long long ne, Grid g, int l, int
     A[e] = make_double2(v.x * sc, v.y * sc);
 }
 
+// BAO reconstruction (particle_reconstruction.hpp:39-94): the full complex spectrum of the
+// a-th displacement component, Psi_a(k) = -i (W_G(k) / b1) (k_a / k^2) D(k) / W(k) / V with
+// W_G = exp(-(k R_G)^2 / 2), zero at k = 0 (|k| < 1e-10); D from the half spectrum.
+template <typename T>
+__global__ void k_recon_psi(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int axis, double RG, double b1,
+                            cplx<T> *out) {
+    const long long total = g.ntot;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int iz = (int)(idx % g.n[2]);
+        const int iy = (int)((idx / g.n[2]) % g.n[1]);
+        const int ix = (int)(idx / ((long long)g.n[2] * g.n[1]));
+        const double kv[3] = {kcomp(wrap_index(ix, g.n[0]), g.dk[0]), kcomp(wrap_index(iy, g.n[1]), g.dk[1]),
+                              kcomp(wrap_index(iz, g.n[2]), g.dk[2])};
+        const double kmag = sqrt(kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2]);
+        cplx<T> r = mk<T>(0, 0);
+        if (!(kmag < 1.0e-10)) {
+            const double kr = kmag * RG;
+            const double wg = exp(-(kr * kr) / 2.0);
+            const double c = (wg / b1) * (kv[axis] / (kmag * kmag));
+            const zd d = f.at(ix, iy, iz);
+            const double wf = window_tab(tabs, ix, iy, iz, wpow);
+            // -i c (d / W) / V
+            const double dr = (d.x / wf) / g.volume, di = (d.y / wf) / g.volume;
+            r = mk<T>((T)(c * di), (T)(-c * dr));
+        }
+        out[idx] = r;
+    }
+}
+
+// psi[i] = Re(field[i]) * norm (the displacement in position units)
+template <typename T>
+__global__ void k_real_scaled(const cplx<T> *in, long long n, double norm, T *out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (T)((double)in[i].x * norm);
+}
+
+// Shift each particle by the TSC-interpolated displacement (particle_reconstruction.hpp:152-205):
+// anchor int(x n / L + 0.5), the reference's flat-index rule (only 0 <= flat < N is used),
+// the 27 terms added to the position in the reference's order.  out: [n][3] doubles.
+template <typename T>
+__global__ void k_recon_shift(PartSrc src, Grid g, const T *__restrict__ p0, const T *__restrict__ p1,
+                              const T *__restrict__ p2, double *out) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < src.n;
+         p += (long long)gridDim.x * blockDim.x) {
+        const double *rec = reinterpret_cast<const double *>(src.base + p * src.stride) + src.pos_off;
+        double pos[3] = {rec[0], rec[1], rec[2]};
+        double w[3][3];
+        long long iw[3][3];
+        for (int a = 0; a < 3; a++) {
+            const double xp = pos[a] * double(g.n[a]) / g.L[a];
+            const int i1 = (int)(xp + 0.5);
+            const double dx = xp - double(i1);
+            w[0][a] = __dmul_rn(__dmul_rn(0.5, __dsub_rn(0.5, dx)), __dsub_rn(0.5, dx));
+            w[1][a] = __dsub_rn(0.75, __dmul_rn(dx, dx));
+            w[2][a] = __dmul_rn(__dmul_rn(0.5, __dadd_rn(0.5, dx)), __dadd_rn(0.5, dx));
+            iw[0][a] = i1 - 1;
+            iw[1][a] = i1;
+            iw[2][a] = i1 + 1;
+        }
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                for (int k = 0; k < 3; k++) {
+                    const long long coord = (iw[i][0] * g.n[1] + iw[j][1]) * g.n[2] + iw[k][2];
+                    if (coord < 0 || coord >= g.ntot) continue;
+                    const double ww = __dmul_rn(__dmul_rn(w[i][0], w[j][1]), w[k][2]);
+                    pos[0] = __dadd_rn(pos[0], __dmul_rn(ww, (double)p0[coord]));
+                    pos[1] = __dadd_rn(pos[1], __dmul_rn(ww, (double)p1[coord]));
+                    pos[2] = __dadd_rn(pos[2], __dmul_rn(ww, (double)p2[coord]));
+                }
+        out[3 * p + 0] = pos[0];
+        out[3 * p + 1] = pos[1];
+        out[3 * p + 2] = pos[2];
+    }
+}
+
 // Scatter A[e] into the compact cube of its shell: buf[shell][nx+s][ny+s][nz+s].
 template <typename T>
 __global__ void k_scatter_cube(const ShellEnt *ent, long long ne, const double2 *A, int3 K, int3 s, cplx<T> *buf) {

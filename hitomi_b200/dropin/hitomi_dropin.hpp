@@ -19,6 +19,12 @@
 //   calcBiSpectrum                           bispec.hpp:4-352
 //   calcThreePointCorrelationFunction        bispec.hpp:355-614
 //   calcThreePointWindowCorrelationFunction  bispec.hpp:617-874
+//   calcPowerSpectrumForBOXForReconstruction      powerspec.hpp:396-457
+//   calcTwoPointFunctionForBOXForReconstruction   powerspec.hpp:459-520
+//   calcReconstructionParticles                   particle_reconstruction.hpp:12-208
+//   calcReconstructionParticlesForBOX             particle_reconstruction.hpp:210-402
+// (the last two in place of particle_reconstruction.hpp, which the program then does not
+// include either)
 //
 // Optional parameter-file keys (hitomi_dropin_configure, one added call after
 // ParameterClass::readParameters); absent keys keep the reference's behaviour:
@@ -68,13 +74,15 @@ struct Cached {
     }
 };
 
-inline hg_ctx *context(ParameterClass &param) {
-    static Cached cache;
+// recon: the reconstruction mesh n_mesh_recon (its own context, cached separately)
+inline hg_ctx *context(ParameterClass &param, bool recon = false) {
+    static Cached cache, cache_recon;
+    Cached &cc = recon ? cache_recon : cache;
     const Options &o = options();
     hg_config c;
     std::memset(&c, 0, sizeof(c));
     for (int a = 0; a < 3; a++) {
-        c.n_mesh[a] = param.n_mesh[a];
+        c.n_mesh[a] = recon ? param.n_mesh_recon[a] : param.n_mesh[a];
         c.boxsize[a] = param.boxsize[a];
     }
     c.assign = o.pcs ? HG_PCS : param.assign == "NGP" ? HG_NGP : param.assign == "CIC" ? HG_CIC : HG_TSC;
@@ -89,16 +97,16 @@ inline hg_ctx *context(ParameterClass &param) {
     c.n_rbin = param.n_rbin;
     c.periodic = 0;
     c.device = o.device;
-    if (cache.ctx && std::memcmp(&cache.cfg, &c, sizeof(c)) == 0) return cache.ctx;
-    if (cache.ctx) hg_destroy(cache.ctx);
-    cache.ctx = nullptr;
-    if (hg_create(&cache.ctx, &c)) {
+    if (cc.ctx && std::memcmp(&cc.cfg, &c, sizeof(c)) == 0) return cc.ctx;
+    if (cc.ctx) hg_destroy(cc.ctx);
+    cc.ctx = nullptr;
+    if (hg_create(&cc.ctx, &c)) {
         printf("hg_create fails: %s\n", hg_last_error(nullptr));
-        cache.ctx = nullptr;
+        cc.ctx = nullptr;
         return nullptr;
     }
-    cache.cfg = c;
-    return cache.ctx;
+    cc.cfg = c;
+    return cc.ctx;
 }
 
 inline int fail(hg_ctx *ctx, const char *what) {
@@ -109,6 +117,13 @@ inline int fail(hg_ctx *ctx, const char *what) {
 // {pos[3], vel[3]} records read in place (particleGadget.hpp:12-15)
 inline int set_box(hg_ctx *ctx, ParticleGadgetClass &P) {
     if (hg_set_particles(ctx, 0, &P[0].pos[0], P.n_tot, (long long)sizeof(P[0]), 0, -1, -1))
+        return fail(ctx, "hg_set_particles");
+    return 0;
+}
+
+// the same, randoms in slot 1 (the box with reconstruction)
+inline int set_box_randoms(hg_ctx *ctx, ParticleGadgetClass &P) {
+    if (hg_set_particles(ctx, 1, &P[0].pos[0], P.n_tot, (long long)sizeof(P[0]), 0, -1, -1))
         return fail(ctx, "hg_set_particles");
     return 0;
 }
@@ -365,6 +380,66 @@ inline int calcThreePointWindowCorrelationFunction(ParticleBOSSClass &P_R, Param
         return fail(ctx, "hg_zeta_window");
     const std::string tag = std::string(recon_tag(param)) + "_window";
     return write_zeta(param, tag.c_str(), rbin, z, sn, norm);
+}
+
+// ---------------------------------------------------------------------------- reconstruction
+
+namespace hitomi_dropin {
+// the shifted positions written back into the caller's particles, as the reference moves them
+template <class P>
+inline void write_back(P &part, const std::vector<double> &pos) {
+    for (long long i = 0; i < part.n_tot; i++)
+        for (int a = 0; a < 3; a++) part[i].pos[a] = pos[3 * i + a];
+}
+}  // namespace hitomi_dropin
+
+inline int calcReconstructionParticles(ParticleBOSSClass &P_D, ParticleBOSSClass &P_R, ParameterClass &param,
+                                       double alpha, double Vsurvey) {
+    using namespace hitomi_dropin;
+    hg_ctx *ctx = context(param, true);
+    if (!ctx || set_survey(ctx, 0, P_D) || set_survey(ctx, 1, P_R)) return -1;
+    std::vector<double> pd(3 * P_D.n_tot), pr(3 * P_R.n_tot);
+    if (hg_reconstruct(ctx, 0, param.b1_fid, param.RG, alpha, Vsurvey, pd.data(), pr.data()))
+        return fail(ctx, "hg_reconstruct");
+    write_back(P_D, pd);
+    write_back(P_R, pr);
+    return 0;
+}
+
+inline int calcReconstructionParticlesForBOX(ParticleGadgetClass &P_D, ParticleGadgetClass &P_R, ParameterClass &param) {
+    using namespace hitomi_dropin;
+    hg_ctx *ctx = context(param, true);
+    if (!ctx || set_box(ctx, P_D) || set_box_randoms(ctx, P_R)) return -1;
+    std::vector<double> pd(3 * P_D.n_tot), pr(3 * P_R.n_tot);
+    if (hg_reconstruct(ctx, 1, param.b1_fid, param.RG, 0.0, param.volume, pd.data(), pr.data()))
+        return fail(ctx, "hg_reconstruct");
+    write_back(P_D, pd);
+    write_back(P_R, pr);
+    return 0;
+}
+
+inline int calcPowerSpectrumForBOXForReconstruction(ParticleGadgetClass &P_D, ParticleGadgetClass &P_R,
+                                                    ParameterClass &param, double alpha, double *kbin) {
+    using namespace hitomi_dropin;
+    if (!ell_check(param)) return -1;
+    hg_ctx *ctx = context(param);
+    if (!ctx || set_box(ctx, P_D) || set_box_randoms(ctx, P_R)) return -1;
+    std::vector<std::complex<double>> pk(param.n_kbin);
+    double norm;
+    if (hg_pk_box_recon(ctx, param.ELL, alpha, dp(pk), nullptr, &norm)) return fail(ctx, "hg_pk_box_recon");
+    return write_pk(param, "_recon", kbin, pk, norm);
+}
+
+inline int calcTwoPointFunctionForBOXForReconstruction(ParticleGadgetClass &P_D, ParticleGadgetClass &P_R,
+                                                       ParameterClass &param, double alpha, double *rbin) {
+    using namespace hitomi_dropin;
+    if (!ell_check(param)) return -1;
+    hg_ctx *ctx = context(param);
+    if (!ctx || set_box(ctx, P_D) || set_box_randoms(ctx, P_R)) return -1;
+    std::vector<std::complex<double>> xi(param.n_rbin);
+    double norm;
+    if (hg_xi_box_recon(ctx, param.ELL, alpha, dp(xi), nullptr, &norm)) return fail(ctx, "hg_xi_box_recon");
+    return write_xi(param, "_recon", rbin, xi, norm);
 }
 
 #endif  // HITOMI_DROPIN_HPP

@@ -4,7 +4,9 @@ before any estimator runs (src/hitomi_measurement/main.cpp:129-180):
   * line of sight per particle, los = pos / |pos| with the observer at the origin
     (ParticleBOSSClass::calcLOS, particle.hpp:355-372);
   * both catalogues shifted so that the randoms' minimum sits `factor` cells inside the
-    FFT box (ParticleBOSSClass::resetParticleForFFT, particle.hpp:222-262).
+    FFT box (ParticleBOSSClass::resetParticleForFFT, particle.hpp:222-262; the driver
+    calls it with its default factor 1, main.cpp:171-175 and, after a reconstruction,
+    main.cpp:220).
 
 The result is the reference's array of structs {pos[3], los[3], w} (56 bytes per
 particle, particle.hpp:12-16), which the library reads in place (pos_off 0, los_off 3,
@@ -32,7 +34,7 @@ def records(xyzw: np.ndarray) -> np.ndarray:
     return out
 
 
-def shift_into_box(D: np.ndarray, R: np.ndarray, n_mesh, boxsize, factor: float = 3.0):
+def shift_into_box(D: np.ndarray, R: np.ndarray, n_mesh, boxsize, factor: float = 1.0):
     """Subtract dP = min(R.pos) - factor * boxsize / n_mesh from both catalogues' positions
     (in place); returns dP."""
     nm = np.broadcast_to(np.asarray(n_mesh, dtype=np.float64), (3,))
@@ -45,7 +47,7 @@ def shift_into_box(D: np.ndarray, R: np.ndarray, n_mesh, boxsize, factor: float 
     return dP
 
 
-def prepare(data_xyzw: np.ndarray, rand_xyzw: np.ndarray, n_mesh, boxsize, factor: float = 3.0):
+def prepare(data_xyzw: np.ndarray, rand_xyzw: np.ndarray, n_mesh, boxsize, factor: float = 1.0):
     """The reference driver's preparation of (data, randoms): records with LOS, then the shift."""
     D, R = records(data_xyzw), records(rand_xyzw)
     shift_into_box(D, R, n_mesh, boxsize, factor)

@@ -235,6 +235,30 @@ int hg_batch_run(hg_ctx *ctx, const hg_mock *mocks, int n_mocks, int n_pk, const
                  const int *bk_ells, int n_zeta, const int *zeta_ells, double *out);
 long long hg_batch_block_len(const hg_ctx *ctx, int n_pk, int n_bk, int n_zeta);
 
+/* BAO reconstruction of the current data (slot 0) and randoms (slot 1) on this context's
+ * mesh (create the context with the reference's n_mesh_recon) and assignment scheme.
+ * Replaces calcReconstructionParticles (particle_reconstruction.hpp:12-208; box = 1:
+ * calcReconstructionParticlesForBOX, :210-402): the displacement
+ * Psi = FFT_+[-i (W_G(k) / b1_fid) (k / k^2) D(k) / W(k) / V] of the D - alpha R field,
+ * W_G = exp(-(k RG)^2 / 2), scaled by vsurvey / sum w_D (box: V / N_D, with alpha taken as
+ * double(N_D / N_R) as the reference computes it), TSC-interpolated to every particle.  The
+ * shifted positions go to pos_D [n_D][3] and pos_R [n_R][3] (host; either may be NULL); the
+ * catalogues the context holds are not changed -- hand the shifted ones back with
+ * hg_set_particles, as the reference's drivers continue with the moved particles. */
+int hg_reconstruct(hg_ctx *ctx, int box, double b1_fid, double RG, double alpha, double vsurvey, double *pos_D,
+                   double *pos_R);
+
+/* Reconstructed periodic-box power-spectrum multipole.  Replaces
+ * calcPowerSpectrumForBOXForReconstruction (powerspec.hpp:396-457): dn = n_D - alpha n_R
+ * (data slot 0, randoms slot 1, weights 1), shot noise N_D + alpha^2 N_R, Legendre weight;
+ * pk_save as hg_pk_box, *norm = V / N_D^2. */
+int hg_pk_box_recon(hg_ctx *ctx, int ell, double alpha, double *pk_save, int *n_mode, double *norm);
+
+/* Reconstructed periodic-box 2PCF multipole.  Replaces
+ * calcTwoPointFunctionForBOXForReconstruction (powerspec.hpp:459-520): hg_xi_box's estimator
+ * on dn = n_D - alpha n_R (weights 1) with shot noise N_D + alpha^2 N_R; *norm = V / N_D^2. */
+int hg_xi_box_recon(hg_ctx *ctx, int ell, double alpha, double *xi_save, int *n_mode, double *norm);
+
 /* ---- catalogue ingest (host side; the reference's readers, native and multi-threaded) */
 
 /* Gadget-2 snapshot header block: 256 bytes, the layout of ParticleGadgetClass::io_header

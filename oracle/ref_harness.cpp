@@ -82,13 +82,13 @@ static int hx_fprintf(FILE *fp, const char *fmt, ...) {
 #include "bessel.hpp"
 #include "particle.hpp"
 #include "particleGadget.hpp"
-#include "particle_reconstruction.hpp"
 #include "field.hpp"
 #ifdef HX_DROPIN
 /* the reference's estimator entry points with bodies over the B200 library: the same driver
  * flow, the same output files (tests/test_gpu_dropin.py compares them) */
 #include "hitomi_dropin.hpp"
 #else
+#include "particle_reconstruction.hpp"
 #include "powerspec.hpp"
 #include "bispec.hpp"
 #endif
@@ -274,11 +274,12 @@ int main(int argc, char **argv) {
         std::fprintf(stderr, "usage: ref_harness param.ini data.f64 [random.f64] [--all-rows]\n");
         return 2;
     }
-    bool all_rows = false;
+    bool all_rows = false, box_recon = false;
     std::string unit;
     std::vector<const char *> pos;
     for (int i = 1; i < argc; i++) {
         if (!strcmp(argv[i], "--all-rows")) all_rows = true;
+        else if (!strcmp(argv[i], "--box-recon")) box_recon = true;
         else if (!strcmp(argv[i], "--unit") && i + 1 < argc) unit = argv[++i];
         else pos.push_back(argv[i]);
     }
@@ -323,7 +324,36 @@ int main(int argc, char **argv) {
 
     auto t0 = std::chrono::steady_clock::now();
     int rc = 0;
-    if (pos.size() == 2) {
+    if (box_recon && pos.size() == 3) {
+        /* periodic box with reconstruction: main_box.cpp:134-152 then the recon estimators
+         * (randoms from the second file instead of readRandomParticles); the shifted
+         * positions are also written to output_dir/recon_{D,R}.f64 */
+        std::vector<double> a = read_f64(pos[1]), b = read_f64(pos[2]);
+        ParticleGadgetClass P_D, P_R;
+        long long nd = (long long)(a.size() / 3), nr = (long long)(b.size() / 3);
+        if (P_D.initializeParticle(nd) || P_R.initializeParticle(nr)) return fail("initializeParticle");
+        for (long long i = 0; i < nd; i++)
+            for (int ax = 0; ax < 3; ax++) P_D[i].pos[ax] = a[3 * i + ax];
+        for (long long i = 0; i < nr; i++)
+            for (int ax = 0; ax < 3; ax++) P_R[i].pos[ax] = b[3 * i + ax];
+        P_D.calcMinAndMax();
+        P_R.calcMinAndMax();
+        t0 = std::chrono::steady_clock::now();
+        if (calcReconstructionParticlesForBOX(P_D, P_R, param)) return fail("calcReconstructionParticlesForBOX");
+        for (int s = 0; s < 2; s++) {
+            ParticleGadgetClass &P = s ? P_R : P_D;
+            std::string fn = param.output_dir + (s ? "/recon_R.f64" : "/recon_D.f64");
+            FILE *fo = fopen(fn.c_str(), "wb");
+            for (long long i = 0; i < P.n_tot; i++) fwrite(P[i].pos, sizeof(double), 3, fo);
+            fclose(fo);
+        }
+        P_D.calcPeriodicBoundary(param);
+        P_R.calcPeriodicBoundary(param);
+        double alpha = double(P_D.n_tot) / double(P_R.n_tot);
+        if (param.measure == "pk") rc = calcPowerSpectrumForBOXForReconstruction(P_D, P_R, param, alpha, kbin.data());
+        else if (param.measure == "2PCF") rc = calcTwoPointFunctionForBOXForReconstruction(P_D, P_R, param, alpha, rbin.data());
+        else return fail("measure");
+    } else if (pos.size() == 2) {
         /* periodic box: main_box.cpp:96-228 (reader replaced, boxsize from param) */
         std::vector<double> a = read_f64(pos[1]);
         ParticleGadgetClass P_D;
@@ -374,6 +404,18 @@ int main(int argc, char **argv) {
         double nbar = ParticleBOSSClass::calcMeanNumberDensity(P_D, Vsurvey);
         if (nbar < 0.0) return fail("calcMeanNumberDensity");
         if (ParticleBOSSClass::printParameters(param, P_D, P_R, alpha, Vsurvey, nbar)) return fail("printParameters");
+        if (param.flag_recon == "True") {
+            /* main.cpp:215-225; the shifted positions also go to output_dir/recon_{D,R}.f64 */
+            if (calcReconstructionParticles(P_D, P_R, param, alpha, Vsurvey)) return fail("calcReconstructionParticles");
+            for (int s = 0; s < 2; s++) {
+                ParticleBOSSClass &P = s ? P_R : P_D;
+                std::string fn = param.output_dir + (s ? "/recon_R.f64" : "/recon_D.f64");
+                FILE *fo = fopen(fn.c_str(), "wb");
+                for (long long i = 0; i < P.n_tot; i++) fwrite(P[i].pos, sizeof(double), 3, fo);
+                fclose(fo);
+            }
+            ParticleBOSSClass::resetParticleForFFT(P_D, P_R, param);
+        }
         {
             /* full-precision survey scalars for the parity tests */
             std::string fn = param.output_dir + "/survey_scalars_full";

@@ -28,8 +28,11 @@ def available() -> bool:
 
 def write_param(path: str, out_dir: str, measure: str, ell1: int, ell2: int, ELL: int, n_mesh, boxsize,
                 kmin: float, kmax: float, n_kbin: int, rmin: float, rmax: float, n_rbin: int, assign: str = "TSC",
-                ith_kbin: int = 0, ith_rbin: int = 0):
+                ith_kbin: int = 0, ith_rbin: int = 0, recon=None):
+    """recon: None, or (b1_fid, RG, n_mesh_recon) for flag_recon = True."""
     nm = [n_mesh] * 3 if np.isscalar(n_mesh) else list(n_mesh)
+    b1, rg, nrec = (1.0, 15.0, nm) if recon is None else (recon[0], recon[1], recon[2])
+    nrec = [nrec] * 3 if np.isscalar(nrec) else list(nrec)
     bs = [boxsize] * 3 if np.isscalar(boxsize) else list(boxsize)
     lines = [
         f"data_dir = {os.path.dirname(out_dir)}",
@@ -53,12 +56,12 @@ def write_param(path: str, out_dir: str, measure: str, ell1: int, ell2: int, ELL
         f"rmin = {rmin!r}",
         f"rmax = {rmax!r}",
         f"n_rbin = {n_rbin}",
-        "flag_recon = False",
-        "b1_fid = 1.0",
-        "RG = 15.0",
-        f"n_mesh_recon_x = {nm[0]}",
-        f"n_mesh_recon_y = {nm[1]}",
-        f"n_mesh_recon_z = {nm[2]}",
+        f"flag_recon = {'False' if recon is None else 'True'}",
+        f"b1_fid = {b1!r}",
+        f"RG = {rg!r}",
+        f"n_mesh_recon_x = {nrec[0]}",
+        f"n_mesh_recon_y = {nrec[1]}",
+        f"n_mesh_recon_z = {nrec[2]}",
         f"ith_kbin = {ith_kbin}",
         f"ith_rbin = {ith_rbin}",
         "NR = 0",
@@ -100,11 +103,11 @@ class RefRun:
 
     def run(self, measure: str, data: np.ndarray, ell1: int, ell2: int, ELL: int, n_mesh, boxsize, binning,
             assign: str = "TSC", randoms: np.ndarray | None = None, all_rows: bool = True, ith: int = 0,
-            full: bool = True, timeout: float | None = None):
+            full: bool = True, timeout: float | None = None, recon=None, box_recon: bool = False):
         param = os.path.join(self.dir, "param.ini")
         write_param(param, self.out, measure, ell1, ell2, ELL, n_mesh, boxsize, binning.kmin, binning.kmax,
                     binning.n_kbin, binning.rmin, binning.rmax, binning.n_rbin, assign,
-                    ith_kbin=ith, ith_rbin=ith)
+                    ith_kbin=ith, ith_rbin=ith, recon=recon)
         dpath = os.path.join(self.dir, "data.f64")
         np.ascontiguousarray(data, dtype=np.float64).tofile(dpath)
         args = [HARNESS, param, dpath]
@@ -114,6 +117,8 @@ class RefRun:
             args.append(rpath)
         if all_rows:
             args.append("--all-rows")
+        if box_recon:
+            args.append("--box-recon")
         env = dict(os.environ)
         if full:
             env["HX_FULL"] = "1"
@@ -159,6 +164,10 @@ class RefRun:
             a = _read_cols(os.path.join(self.out, f"zeta{l1}{l2}{L}_{i:02d}_window.dat"))
             rows.append(a[:, 2])
         return np.array(rows)
+
+    def recon_positions(self):
+        """The reconstructed positions the harness wrote (recon_D.f64, recon_R.f64): (n, 3) each."""
+        return tuple(np.fromfile(os.path.join(self.out, f"recon_{s}.f64")).reshape(-1, 3) for s in "DR")
 
     def survey_scalars(self):
         v = np.loadtxt(os.path.join(self.out, "survey_scalars_full"))

@@ -13,6 +13,7 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --bk256 (only box_bk_256.npz, from the restatement)
     python tests/golden/make_golden.py --xi     (only xi_window.npz: 2PCF, window 2PCF / 3PCF)
     python tests/golden/make_golden.py --ingest (only ingest.npz: the ASCII and Gadget readers)
+    python tests/golden/make_golden.py --recon  (only recon.npz: BAO reconstruction)
     python tests/golden/make_golden.py --configs (only box_config_sizes.npz: 128^3 and 512^3)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
@@ -287,6 +288,40 @@ def make_ingest():
                         gadget1=np.frombuffer(gfiles[1], dtype=np.uint8), gadget_ref=gadget_ref)
 
 
+def make_recon():
+    """BAO reconstruction (particle_reconstruction.hpp:12-402) through the reference's drivers:
+    the shifted positions and the reconstructed P_l, survey (main.cpp:215-225, then
+    calcPowerSpectrum with the _recon file name) and box (main_box.cpp:134-152, then
+    calcPowerSpectrumForBOXForReconstruction)."""
+    d = {}
+    data, rand = survey_shell(3000, 60000, seed=16)
+    bs = Binning(0.004, 0.048, 12, 100.0, 1500.0, 15)
+    d.update(sv_data=data, sv_rand=rand, sv_binning=binning_arr(bs), sv_boxsize=3500.0, sv_n_mesh=64,
+             sv_n_mesh_recon=32, sv_b1=2.0, sv_RG=40.0)
+    for ell in (0, 2):
+        with ref_runner.RefRun() as r:
+            r.run("pk", data, ell, 0, ell, 64, 3500.0, bs, assign="TSC", randoms=rand, recon=(2.0, 40.0, 32))
+            a = ref_runner._read_cols(os.path.join(r.out, f"pk{ell}_recon.dat"))
+            d[f"sv_pk_{ell}"] = a[:, 1] + 1j * a[:, 2]
+            d["sv_recon_D"], d["sv_recon_R"] = r.recon_positions()
+            sc = r.survey_scalars()
+    for k, v in sc.items():
+        d[f"sv_scalars_{k}"] = v
+    pos = lognormal_box(15000, 1000.0, ngrid=32, seed=11, exact_n=15000)
+    rnd = uniform_box(30000, 1000.0, seed=31)
+    bx = Binning(0.005, 0.295, 30, 4.0, 156.0, 20)
+    d.update(box_pos=pos, box_rand=rnd, box_binning=binning_arr(bx), box_boxsize=1000.0, box_n_mesh=32,
+             box_n_mesh_recon=32, box_b1=1.5, box_RG=20.0)
+    for ell in (0, 2):
+        with ref_runner.RefRun() as r:
+            r.run("pk", pos, ell, 0, ell, 32, 1000.0, bx, assign="TSC", randoms=rnd, recon=(1.5, 20.0, 32),
+                  box_recon=True, all_rows=False)
+            a = ref_runner._read_cols(os.path.join(r.out, f"pk{ell}_recon.dat"))
+            d[f"box_pk_{ell}"] = a[:, 1] + 1j * a[:, 2]
+            d["box_recon_D"], d["box_recon_R"] = r.recon_positions()
+    np.savez_compressed(os.path.join(HERE, "recon.npz"), **d)
+
+
 def catalogue_digest(pos: np.ndarray) -> np.ndarray:
     """Count, coordinate sums and sums of squares: the tests regenerate the large catalogues
     from their seeds and check these first, so a generator change cannot pass silently."""
@@ -333,6 +368,10 @@ def make_config_sizes():
 
 
 def main():
+    if "--recon" in sys.argv:
+        make_recon()
+        print("fixtures written")
+        return
     if "--ingest" in sys.argv:
         make_ingest()
         print("fixtures written")

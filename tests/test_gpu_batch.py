@@ -25,6 +25,9 @@ def test_batch_equals_single_calls(form):
     g[:, :3] = mocks[1]
     g[:, 3:] = -7.0
     mocks[1] = g
+    # two runs of the same catalogue agree to the order-dependent last bits of the FP64 atomics
+    # (FP64 form) or of the FP32 float atomics of crowded assignment tiles (FP32 form)
+    tol = {"fp64": 1e-10, "fp32": 1e-5}[form]
     with Context(32, 1000.0, b, "TSC", form) as c:
         res = c.batch_run(mocks, pk_ells=(0, 2), bk_multipoles=MULTIPOLES, zeta_multipoles=ZETA)
         assert len(res) == 3
@@ -32,11 +35,11 @@ def test_batch_equals_single_calls(form):
             c.set_particles(0, m)
             for q, ell in enumerate((0, 2)):
                 pk, _, norm = c.pk_box(ell)
-                assert relerr(r["pk"][q], pk) < 1e-12 and r["pk_norm"][q] == norm
+                assert relerr(r["pk"][q], pk, 1e-3) < tol and r["pk_norm"][q] == norm
             bk, sn, norm = c.bk_box_multi(MULTIPOLES)
-            assert relerr(r["bk"], bk) < 1e-12 and relerr(r["bk_sn"], sn) < 1e-10 and r["bk_norm"] == norm
+            assert relerr(r["bk"], bk, 1e-3) < tol and relerr(r["bk_sn"], sn, 1e-3) < tol and r["bk_norm"] == norm
             z, zs, zn = c.zeta_box_multi(ZETA)
-            assert relerr(r["zeta"], z) < 1e-10 and relerr(r["zeta_sn"], zs) < 1e-10 and r["zeta_norm"] == zn
+            assert relerr(r["zeta"], z, 1e-3) < tol and relerr(r["zeta_sn"], zs, 1e-3) < tol and r["zeta_norm"] == zn
 
 
 def test_batch_rejects_bad_mocks():

@@ -28,7 +28,7 @@ def have_harnesses():
     return all(os.path.exists(p) and os.access(p, os.X_OK) for p in (REF, DROPIN))
 
 
-def run_both(measure, data, ells, n_mesh, boxsize, b, randoms=None, ith=0, extra=""):
+def run_both(measure, data, ells, n_mesh, boxsize, b, randoms=None, ith=0, extra="", recon=None, box_recon=False):
     """Run the reference driver and the drop-in driver; return {file name: (ref, dropin) text}."""
     from oracle import ref_runner
     out = {}
@@ -40,13 +40,13 @@ def run_both(measure, data, ells, n_mesh, boxsize, b, randoms=None, ith=0, extra
             os.makedirs(os.path.dirname(od))
             param = os.path.join(tmp, name, "param.ini")
             ref_runner.write_param(param, od, measure, *ells, n_mesh, boxsize, b.kmin, b.kmax, b.n_kbin, b.rmin,
-                                   b.rmax, b.n_rbin, "TSC", ith_kbin=ith, ith_rbin=ith)
+                                   b.rmax, b.n_rbin, "TSC", ith_kbin=ith, ith_rbin=ith, recon=recon)
             if extra:
                 with open(param, "a") as f:
                     f.write(extra)
             dpath = os.path.join(tmp, name, "data.f64")
             np.ascontiguousarray(data, dtype=np.float64).tofile(dpath)
-            args = [exe, param, dpath]
+            args = [exe, param, dpath] + (["--box-recon"] if box_recon else [])
             if randoms is not None:
                 rpath = os.path.join(tmp, name, "random.f64")
                 np.ascontiguousarray(randoms, dtype=np.float64).tofile(rpath)
@@ -55,8 +55,8 @@ def run_both(measure, data, ells, n_mesh, boxsize, b, randoms=None, ith=0, extra
             p = subprocess.run(args, env=env, capture_output=True, text=True, timeout=600)
             assert p.returncode == 0, (name, p.stdout[-2000:], p.stderr[-2000:])
             outs[name] = od
-        names = sorted(os.listdir(outs["ref"]))
-        assert sorted(os.listdir(outs["dropin"])) == names
+        names = sorted(f for f in os.listdir(outs["ref"]) if not f.endswith(".f64"))
+        assert sorted(f for f in os.listdir(outs["dropin"]) if not f.endswith(".f64")) == names
         for fn in names:
             with open(os.path.join(outs["ref"], fn)) as f1, open(os.path.join(outs["dropin"], fn)) as f2:
                 out[fn] = (f1.read(), f2.read())
@@ -65,7 +65,7 @@ def run_both(measure, data, ells, n_mesh, boxsize, b, randoms=None, ith=0, extra
     return out
 
 
-def compare_files(files):
+def compare_files(files, rel=6e-8, floor_frac=1e-9):
     n_values = 0
     for fn, (a, b) in files.items():
         la, lb = a.splitlines(), b.splitlines()
@@ -83,8 +83,8 @@ def compare_files(files):
         for c in range(nlead, ncol):
             va = np.array([float(r[c]) for r in rows_a])
             vb = np.array([float(r[c]) for r in rows_b])
-            floor = 1e-9 * float(np.max(np.abs(va))) if va.size else 0.0
-            assert np.all(np.abs(vb - va) <= np.maximum(6e-8 * np.abs(va), floor)), (fn, c, va, vb)
+            floor = floor_frac * float(np.max(np.abs(va))) if va.size else 0.0
+            assert np.all(np.abs(vb - va) <= np.maximum(rel * np.abs(va), floor)), (fn, c, va, vb)
             n_values += va.size
     return n_values
 
@@ -128,9 +128,25 @@ def test_dropin_survey_files():
 
 
 def test_dropin_optional_keys():
-    """gpu_precision = chosen runs the FP32 context with FP64 density and bispectrum signal:
-    the files still agree with the reference's to the printed precision."""
+    """gpu_precision = chosen runs the FP32 context with FP64 density and bispectrum signal
+    (its shot noise in FP32): the files agree with the reference's within that form's bar,
+    1e-5 per bin."""
     d = load_golden("box_bk.npz")
     b = binning_from(d["binning"])
     files = run_both("bk", d["pos"], (0, 0, 0), 32, 1000.0, b, ith=3, extra="gpu_precision = chosen\n")
-    assert compare_files(files) > 0
+    assert compare_files(files, rel=1e-5, floor_frac=1e-5) > 0
+
+
+def test_dropin_reconstruction_files():
+    """BAO reconstruction through the drop-in (hg_reconstruct on the n_mesh_recon mesh) and
+    the estimators that follow it: the survey P with the _recon file name, the box
+    reconstructed P and 2PCF."""
+    g = load_golden("recon.npz")
+    bs = binning_from(g["sv_binning"])
+    n = compare_files(run_both("pk", g["sv_data"], (2, 0, 2), 64, 3500.0, bs, randoms=g["sv_rand"],
+                               recon=(2.0, 40.0, 32)), rel=1e-7)
+    bx = binning_from(g["box_binning"])
+    for measure in ("pk", "2PCF"):
+        n += compare_files(run_both(measure, g["box_pos"], (0, 0, 0), 32, 1000.0, bx, randoms=g["box_rand"],
+                                    recon=(1.5, 20.0, 32), box_recon=True), rel=1e-7)
+    assert n > 20

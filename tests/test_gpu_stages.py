@@ -35,8 +35,9 @@ def test_all_stages_fp64_equals_plain_form():
         np.testing.assert_array_equal(pkm[ell][1], pk64[ell][1])
     assert nm == n64
     assert relerr(bkm, bk64) < 1e-13
-    # the shot-noise histogram adds with FP64 atomics: order-dependent at the last bits
-    assert relerr(snm, sn64) < 1e-12
+    # the shot-noise histogram adds with FP64 atomics: order-dependent at the last bits,
+    # which the cancellation between its terms lifts to ~1e-12 of a bin
+    assert relerr(snm, sn64) < 1e-11
 
 
 @pytest.mark.parametrize("stages", [s for r in range(1, 3) for s in itertools.combinations(STAGES, r)])
