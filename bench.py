@@ -566,7 +566,8 @@ def main():
         run_mock(ctx)
         stats = ctx.kernel_stats()
         ctx.set_profiling(False)
-        timing[form] = dict(ms=ms, e2e_ms=ems, e2e_seq_ms=sms, launches=launches // args.steps, clocks=clocks,
+        tuned = ctx.tuning()
+        timing[form] = dict(ms=ms, e2e_ms=ems, e2e_seq_ms=sms, launches=launches // args.steps, clocks=clocks, tuned=tuned,
                             stats=stats, d2h=d2h)
         ctx.close()
 
@@ -602,6 +603,7 @@ def main():
                 "sequential_value": (world * 1000.0 / t["e2e_seq_ms"]) if t.get("e2e_seq_ms") else None},
         "gpu_launches": int(t["launches"] * args.steps),
         "roofline": roof,
+        "autotuned": t.get("tuned", "").strip().splitlines(),
     }
     if "fp64" in timing and head != "fp64":
         def errs_of(form):

@@ -367,7 +367,10 @@ __device__ __forceinline__ void defer_push(const Defer &df, bool want, long long
 // sum_p w_p factor prod(w_axis)  (the field's exact integral, needed for the k = 0 mode
 // since boundary drops lose mass).  Clustered catalogues put many lanes of a warp on the
 // same tile, so the count is warp-aggregated.  Whole warps stride over the catalogue (the
-// main pass) or the deferred list, and the mass is reduced per block before one atomic.
+// main pass) or the deferred list.  The mass is summed in the main pass only, for every
+// particle (those deferred for their tiles included), and each block writes its sum to
+// mass[2 blockIdx.x] (+1 for the imaginary part): fixed blocks over fixed particles, added
+// on the host in block order, so the integral does not depend on scheduling.
 __global__ void __launch_bounds__(256, 3) k_bin_count(PartSrc src, AssignGeom g, Defer df, unsigned int *cnt,
                                                       double *mass) {
     __shared__ double red[2][32];
@@ -392,9 +395,22 @@ __global__ void __launch_bounds__(256, 3) k_bin_count(PartSrc src, AssignGeom g,
             for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);
             if (!df.pass && !stencil_separable(g, anc)) {
                 push = true;
+                if (mass) {  // its in-bounds mass point by point, here (the deferred pass sums none)
+                    const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
+                    for (int q = 0; q < W * W * W; q++) {
+                        const int a = q / (W * W), b = (q / W) % W, c = q % W;
+                        int cx, cy, cz;
+                        if (!effective_cell(g, anc[0] + s0 + a, anc[1] + s0 + b, anc[2] + s0 + c, cx, cy, cz)) continue;
+                        const double wa = axis_weight_at<double>(g.scheme, d[0], a),
+                                     wb = axis_weight_at<double>(g.scheme, d[1], b),
+                                     wc = axis_weight_at<double>(g.scheme, d[2], c);
+                        m_re += wr * g.factor * wa * wb * wc;
+                        m_im += wi * g.factor * wa * wb * wc;
+                    }
+                }
             } else {
                 tile_list(g, anc, tl, slow);
-                if (!mass) {
+                if (!mass || df.pass) {
                 } else if (tl.sep) {
                     // every stencil point lands: the weights sum to one per axis
                     m_re += wr * g.factor;
@@ -423,7 +439,7 @@ __global__ void __launch_bounds__(256, 3) k_bin_count(PartSrc src, AssignGeom g,
             if (t >= 0 && lane == __ffs(grp) - 1) atomicAdd(&cnt[t], (unsigned)__popc(grp));
         }
     }
-    if (!mass) return;
+    if (!mass || df.pass) return;
     m_re = warp_sum_d(m_re);
     m_im = warp_sum_d(m_im);
     if (lane == 0) {
@@ -437,8 +453,8 @@ __global__ void __launch_bounds__(256, 3) k_bin_count(PartSrc src, AssignGeom g,
             sr += red[0][w];
             si += red[1][w];
         }
-        if (sr != 0.0) atomicAdd(&mass[0], sr);
-        if (si != 0.0) atomicAdd(&mass[1], si);
+        mass[2 * blockIdx.x] = sr;
+        mass[2 * blockIdx.x + 1] = si;
     }
 }
 
@@ -611,6 +627,8 @@ struct Chunk {
     int tile;
     unsigned r0, r1;
     int multi;  // 0: sole chunk; 1: first chunk of a split tile; 2: later chunk of a split tile
+    unsigned tile_n;  // records of the whole tile
+    int slot;         // split tiles: their slot in the integer staging buffer (crowd), else -1
 };
 
 __global__ void k_chunk_count(const unsigned int *cnt, int ntiles, unsigned chunk, unsigned int *nch) {
@@ -619,17 +637,22 @@ __global__ void k_chunk_count(const unsigned int *cnt, int ntiles, unsigned chun
     nch[t] = (t == ntiles) ? 0u : max(1u, (cnt[t] + chunk - 1) / chunk);
 }
 
-__global__ void k_chunk_fill(const unsigned int *off, const unsigned int *choff, int ntiles, unsigned chunk, Chunk *ch) {
+// nslots: a counter (zeroed by the host) that hands every split tile its staging slot
+__global__ void k_chunk_fill(const unsigned int *off, const unsigned int *choff, int ntiles, unsigned chunk, Chunk *ch,
+                             unsigned *nslots = nullptr) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
     unsigned b = off[t], e = off[t + 1];
     unsigned n = choff[t + 1] - choff[t];
+    const int slot = (n > 1 && nslots) ? (int)atomicAdd(nslots, 1u) : -1;
     for (unsigned c = 0; c < n; c++) {
         Chunk k;
         k.tile = t;
         k.r0 = b + c * chunk;
         k.r1 = min(e, b + (c + 1) * chunk);
         k.multi = (n == 1) ? 0 : (c == 0 ? 1 : 2);
+        k.tile_n = e - b;
+        k.slot = slot;
         ch[choff[t] + c] = k;
     }
 }
@@ -660,14 +683,59 @@ __device__ __forceinline__ void zero_shared(void *p, int words) {
     for (int c = (words & ~3) + threadIdx.x; c < words; c += blockDim.x) w[c] = 0;
 }
 
-// Zero the cells of every split tile (run before the accumulation).
+// Zero the cells of every split tile (run before the accumulation), or with crowd != null
+// its slot of the integer staging buffer (crowd_words 64-bit words per cell).
 template <typename T, bool CPLX>
-__global__ void k_zero_split_tiles(const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
+__global__ void k_zero_split_tiles(const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im,
+                                   unsigned long long *crowd = nullptr, int crowd_words = 0) {
     Chunk k = ch[blockIdx.x];
     if (k.multi != 1) return;
+    if (crowd) {
+        const int tcells = g.t[0] * g.t[1] * g.t[2];
+        unsigned long long *c = crowd + (size_t)k.slot * tcells * crowd_words;
+        for (int i = threadIdx.x; i < tcells * crowd_words; i += blockDim.x) c[i] = 0ull;
+        return;
+    }
     for_tile_cells(g, k.tile, [&](int, long long cell) {
         mesh_re[cell] = (T)0;
         if (CPLX) mesh_im[cell] = (T)0;
+    });
+}
+
+// Fixed-point scale of a tile: 2^sc with sc from the tile's record count, the same for every
+// chunk of a split tile, so their integer partial sums add exactly.  FP32 (two 32-bit
+// words): tile records x bound x 2^sc < 2^50 and bound x 2^sc < 2^42; FP64 (three words):
+// tile records x bound x 2^sc <= 2^69.
+template <typename T>
+__device__ __forceinline__ int fix_exponent(const AssignGeom &g, unsigned tile_n) {
+    if (sizeof(T) == 8) {
+        int e;
+        frexp(double(max(tile_n, 1u)) * (double)g.fix_bound, &e);
+        return 69 - e;
+    }
+    int e, e1;
+    frexpf(float(max(tile_n, 1u)) * g.fix_bound, &e);
+    frexpf(g.fix_bound, &e1);
+    return min(50 - e, 42 - e1);  // the host keeps fix_bound >= 2^-60, so sc <= 102
+}
+
+// Split tiles of a fixed-point accumulation: the integer sums their chunks added to the
+// staging slot, rounded once to the mesh's type and written (one CTA per split tile).
+template <typename T>
+__global__ void k_crowd_writeout(const Chunk *ch, AssignGeom g, const unsigned long long *crowd, T *mesh) {
+    const Chunk k = ch[blockIdx.x];
+    if (k.multi != 1) return;
+    const int tcells = g.t[0] * g.t[1] * g.t[2];
+    const double inv = ldexp(1.0, -fix_exponent<T>(g, k.tile_n));
+    for_tile_cells(g, k.tile, [&](int li, long long cell) {
+        if (sizeof(T) == 8) {
+            const unsigned long long *c = crowd + (size_t)k.slot * tcells * 2;
+            const double hi = (double)(long long)c[li] * 0x1p40;
+            mesh[cell] = (T)(__dadd_rn(hi, (double)(long long)c[tcells + li]) * inv);
+        } else {
+            const unsigned long long *c = crowd + (size_t)k.slot * tcells;
+            mesh[cell] = (T)(__ll2float_rn((long long)c[li]) * (float)inv);
+        }
     });
 }
 
@@ -719,14 +787,18 @@ __device__ __forceinline__ void fix_split(float x, int &hi, int &lo) {
     lo = __float_as_int(__fadd_rn(r, 12582912.0f)) - 0x4B400000;
 }
 
-// FIX with T = double (real FP64 meshes of weight-bounded sources): one 64-bit integer word
-// per cell.  Per chunk every stencil weight (an FP64 product) is scaled by S = 2^s, exactly,
-// with (records) x fix_bound x S < 2^62, and rounded to an integer (the only rounding, below
-// 2^-63 of the chunk's bound); at most one add per record and cell keeps |sum| < 2^62, so
-// the sum is exact and independent of the order of the 64-bit integer atomics, and it is
-// rounded once, to the mesh's FP64.
+// FIX with T = double (real FP64 meshes of weight-bounded sources): three 32-bit integer
+// words per cell (64-bit shared-memory atomics measured no faster than FP64 ones here, the
+// 32-bit ones are native).  Per chunk every stencil weight (an FP64 product) is scaled by
+// S = 2^s, exactly, with (records) x fix_bound x S <= 2^69, and split as
+// x = hi 2^40 + mid 2^20 + lo with hi = round(x / 2^40), mid = round((x - hi 2^40) / 2^20);
+// both differences are exact, and lo = round(x - hi 2^40 - mid 2^20) is the only rounding
+// (below 2^-70 of the chunk's bound, finer than FP64).  |sum lo|, |sum mid| <= records 2^19
+// and |sum hi| <= 2^29 + records stay inside 32 bits, so the sum is exact, independent of the
+// order of the atomics, and rounded once to the mesh's FP64.
 template <typename T, bool CPLX, bool FIX, int SCHEME>
-__global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im) {
+__global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, T *mesh_re, T *mesh_im,
+                             unsigned long long *crowd = nullptr) {
     static_assert(!FIX || !CPLX, "fixed-point accumulation is for real meshes");
     constexpr bool FIX64 = FIX && sizeof(T) == 8;
     constexpr int W = SCHEME + 1, s0 = (SCHEME >= 2) ? -1 : 0;
@@ -736,8 +808,8 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     T *acc_im = acc + tcells;
     int *acc_hi = reinterpret_cast<int *>(smem_raw);
     int *acc_lo = acc_hi + tcells;
-    unsigned long long *acc64 = reinterpret_cast<unsigned long long *>(smem_raw);
-    zero_shared(smem_raw, tcells * ((CPLX || (FIX && !FIX64)) ? 2 : 1) * (int)(sizeof(T) / 4));
+    int *acc_w3 = reinterpret_cast<int *>(smem_raw);  // FIX64: hi, mid, lo words
+    zero_shared(smem_raw, FIX64 ? 3 * tcells : tcells * ((CPLX || FIX) ? 2 : 1) * (int)(sizeof(T) / 4));
     __syncthreads();
     const Chunk k = ch[blockIdx.x];
     const int tile = k.tile;
@@ -747,23 +819,24 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     const int ox = tx * g.t[0], oy = ty * g.t[1], oz = tz * g.t[2];
     float fscale = 1.0f, finv = 1.0f;
     double dscale = 1.0, dinv = 1.0;
-    if (FIX64) {
-        int e;
-        frexp(double(k.r1 - k.r0) * (double)g.fix_bound, &e);
-        dscale = ldexp(1.0, 62 - e);
-        dinv = ldexp(1.0, e - 62);
-    } else if (FIX) {
-        int e, e1;
-        frexpf(float(k.r1 - k.r0) * g.fix_bound, &e);
-        frexpf(g.fix_bound, &e1);
-        const int sc = min(50 - e, 42 - e1);  // the host keeps fix_bound >= 2^-60, so sc <= 102
+    if (FIX) {  // one scale for the whole tile (all its chunks)
+        const int sc = fix_exponent<T>(g, k.tile_n);
+        dscale = ldexp(1.0, sc);
+        dinv = ldexp(1.0, -sc);
         fscale = ldexpf(1.0f, sc);
         finv = ldexpf(1.0f, -sc);
     }
     const T factor = (T)g.acc_factor;
     auto add = [&](int li, T v, T vi) {
         if (FIX64) {
-            atomicAdd(&acc64[li], (unsigned long long)__double2ll_rn((double)v));
+            const double x = (double)v;
+            const double hi = rint(x * 0x1p-40);
+            const double r1 = x - hi * 0x1p40;  // exact
+            const double mid = rint(r1 * 0x1p-20);
+            const double r2 = r1 - mid * 0x1p20;  // exact
+            atomicAdd(&acc_w3[li], (int)hi);
+            atomicAdd(&acc_w3[tcells + li], (int)mid);
+            atomicAdd(&acc_w3[2 * tcells + li], __double2int_rn(r2));
         } else if (FIX) {
             int hi, lo;
             fix_split((float)v, hi, lo);
@@ -825,9 +898,27 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
         }
     }
     __syncthreads();
+    if (FIX && k.multi != 0 && crowd) {  // a split tile: this chunk's exact partial sums, added as integers
+        for (int li = threadIdx.x; li < tcells; li += blockDim.x) {
+            if (FIX64) {
+                unsigned long long *c = crowd + (size_t)k.slot * tcells * 2;
+                const long long hi = acc_w3[li];
+                const long long ml = (long long)acc_w3[tcells + li] * 1048576LL + (long long)acc_w3[2 * tcells + li];
+                if (hi) atomicAdd(&c[li], (unsigned long long)hi);
+                if (ml) atomicAdd(&c[tcells + li], (unsigned long long)ml);
+            } else {
+                unsigned long long *c = crowd + (size_t)k.slot * tcells;
+                const long long v = (long long)acc_hi[li] * 1048576LL + (long long)acc_lo[li];
+                if (v) atomicAdd(&c[li], (unsigned long long)v);
+            }
+        }
+        return;
+    }
     // FIX: the exact integer sum rounded once to FP32, then scaled by a power of two (exact)
     for_tile_cells(g, tile, [&](int li, long long cell) {
-        const T v = FIX64 ? (T)(__ll2double_rn((long long)acc64[li]) * dinv)
+        const T v = FIX64 ? (T)(__dadd_rn((double)acc_w3[li] * 0x1p40,
+                                          (double)((long long)acc_w3[tcells + li] * 1048576LL +
+                                                   (long long)acc_w3[2 * tcells + li])) * dinv)
                     : FIX ? (T)(__ll2float_rn((long long)acc_hi[li] * 1048576LL + (long long)acc_lo[li]) * finv)
                           : acc[li];
         if (k.multi == 0) {

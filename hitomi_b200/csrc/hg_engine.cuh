@@ -637,7 +637,11 @@ struct Engine : public hg_ctx {
     // Tile counts of several sources (pass 1).  Each source's edge-straddling particles go to
     // its own slice of the deferred list (at the running offset of the sources' sizes) and
     // are counted by a second launch; the scatter reads the same slices.
-    void bin_count_sources(const PartSrc *srcs, int ns, const AssignGeom &ag, double *mass_dev) {
+    // mass_part (when not null): room for ns x MASS_BLOCKS x 2 doubles; source q's blocks write
+    // theirs at q MASS_BLOCKS 2 (see k_bin_count), mass_blocks[q] of them
+    static constexpr int MASS_BLOCKS = 148 * 8;
+    int mass_blocks[2] = {0, 0};
+    void bin_count_sources(const PartSrc *srcs, int ns, const AssignGeom &ag, double *mass_part) {
         long long cap = 0;
         for (int q = 0; q < ns; q++) cap += srcs[q].n;
         HG_CK(deflist.ensure(sizeof(int) * std::max<long long>(cap, 1)));
@@ -645,15 +649,18 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(defcnt.p, 0, sizeof(unsigned) * ns, st));
         long long o = 0;
         for (int q = 0; q < ns; q++) {
+            if (q < 2) mass_blocks[q] = 0;
             if (srcs[q].n == 0) continue;  // an empty catalogue (no data for a window function)
             Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0};
+            const unsigned nb = (unsigned)std::min<long long>(grid1(srcs[q].n, 256), MASS_BLOCKS);
+            if (q < 2) mass_blocks[q] = (int)nb;
             kb("assign_bin_count", double(srcs[q].n) * 24.0);
-            k_bin_count<<<(unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 8), 256, 0, st>>>(
-                srcs[q], ag, df, dp<unsigned>(cnt), mass_dev);
+            k_bin_count<<<nb, 256, 0, st>>>(srcs[q], ag, df, dp<unsigned>(cnt),
+                                            mass_part ? mass_part + (size_t)q * MASS_BLOCKS * 2 : nullptr);
             ke();
             df.pass = 1;
             kb("assign_edge_count", 0.0);
-            k_bin_count<<<148 * 8, 256, 0, st>>>(srcs[q], ag, df, dp<unsigned>(cnt), mass_dev);
+            k_bin_count<<<148 * 8, 256, 0, st>>>(srcs[q], ag, df, dp<unsigned>(cnt), nullptr);
             ke();
             o += srcs[q].n;
         }
@@ -697,10 +704,10 @@ struct Engine : public hg_ctx {
         HG_CK(cursor.ensure(sizeof(unsigned) * (ntiles + 1)));
         HG_CK(nch.ensure(sizeof(unsigned) * (ntiles + 1)));
         HG_CK(choff.ensure(sizeof(unsigned) * (ntiles + 1)));
-        HG_CK(mass.ensure(sizeof(double) * 2));
+        HG_REQUIRE(srcs.size() <= 2, "at most two sources per assignment");
+        HG_CK(mass.ensure(sizeof(double) * 2 * MASS_BLOCKS * 2));
         HG_CK(cudaMemsetAsync(cnt.p, 0, sizeof(unsigned) * (ntiles + 1), st));
         HG_CK(cudaMemsetAsync(cursor.p, 0, sizeof(unsigned) * (ntiles + 1), st));
-        HG_CK(cudaMemsetAsync(mass.p, 0, sizeof(double) * 2, st));
         bin_count_sources(srcs.data(), (int)srcs.size(), ag, want_mass ? dp<double>(mass) : nullptr);
         size_t tb = 0, tb2 = 0;
         HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(cnt), dp<unsigned>(off), ntiles + 1, st));
@@ -716,37 +723,32 @@ struct Engine : public hg_ctx {
         HG_CK(cub::DeviceScan::ExclusiveSum(cubtmp.p, tb2, dp<unsigned>(nch), dp<unsigned>(choff), ntiles + 1, st));
         ke();
         unsigned tot[2] = {0, 0};
-        double hm[2];
+        double hm[2] = {0.0, 0.0};
+        std::vector<double> mp(want_mass ? 2 * MASS_BLOCKS * 2 : 0);
         HG_CK(cudaMemcpyAsync(&tot[0], dp<unsigned>(off) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaMemcpyAsync(&tot[1], dp<unsigned>(choff) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-        HG_CK(cudaMemcpyAsync(hm, mass.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, st));
+        if (want_mass)
+            HG_CK(cudaMemcpyAsync(mp.data(), mass.p, sizeof(double) * mp.size(), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
+        if (want_mass)  // block partials in a fixed order
+            for (size_t q = 0; q < srcs.size(); q++)
+                for (int b = 0; b < mass_blocks[q]; b++) {
+                    hm[0] += mp[(q * MASS_BLOCKS + b) * 2];
+                    hm[1] += mp[(q * MASS_BLOCKS + b) * 2 + 1];
+                }
         const unsigned total = tot[0], nchunks = tot[1];
         // 25 % headroom: catalogues of varying size reuse the buffers without reallocating
         if (rec.n < sizeof(PRec<U>) * std::max<size_t>(total, 1))
             HG_CK(rec.ensure(sizeof(PRec<U>) * (std::max<size_t>(total, 1) * 5 / 4)));
         if (chunks.n < sizeof(Chunk) * std::max<size_t>(nchunks, 1))
             HG_CK(chunks.ensure(sizeof(Chunk) * (std::max<size_t>(nchunks, 1) * 5 / 4)));
-        kb("assign_chunks", double(ntiles) * 16.0);
-        k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
-                                                        dp<Chunk>(chunks));
-        ke();
-        {
-            std::vector<RecWeight<U>> mk(srcs.size());
-            bin_scatter_sources(srcs.data(), mk.data(), (int)srcs.size(), ag, ntiles, dp<PRec<U>>(rec),
-                                double(total) * sizeof(PRec<U>));
-        }
-        kb("assign_zero_split", 0.0);
-        k_zero_split_tiles<U, CPLX><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), ag, out_re, out_im);
-        ke();
-        const size_t tbytes = sizeof(U) * ag.t[0] * ag.t[1] * ag.t[2];
-        // exact fixed-point accumulation for real FP32 meshes of unweighted sources, whose
+        // exact fixed-point accumulation for real meshes of unweighted sources, whose
         // per-record weight |scale| acc_factor is known here (the stencil weights sum to one),
         // on meshes with at least W cells per axis (one add per record and cell)
         static_assert(CHUNK <= 2048, "the fixed-point lo word holds at most 2048 adds of < 2^20");
         bool fix = false;
         AssignGeom agx = ag;
-        if constexpr (!CPLX) {  // FP32: two 32-bit words per cell; FP64: one 64-bit word
+        if constexpr (!CPLX) {  // FP32: two 32-bit words per cell; FP64: three
             fix = true;
             double wmax = 0.0;
             for (const auto &src : srcs) {
@@ -757,33 +759,68 @@ struct Engine : public hg_ctx {
             agx.fix_bound = (float)(wmax * std::fabs(ag.acc_factor));
             fix = fix && agx.fix_bound >= 0x1p-60f;
         }
+        // split tiles of a fixed-point accumulation add their chunks' exact partial sums as
+        // 64-bit integers in a staging slot (at most nchunks - ntiles split tiles), written
+        // out once: the mesh does not depend on the order the chunks finish in
+        const int cwords = sizeof(U) == 8 ? 2 : 1;
+        const size_t tcells = (size_t)ag.t[0] * ag.t[1] * ag.t[2];
+        const size_t nsplit_max = nchunks > (unsigned)ntiles ? nchunks - (unsigned)ntiles : 0;
+        unsigned long long *crowd_p = nullptr;
+        if (fix && nsplit_max > 0) {
+            HG_CK(crowd.ensure(sizeof(unsigned long long) * cwords * tcells * nsplit_max));
+            crowd_p = dp<unsigned long long>(crowd);
+        }
+        HG_CK(nslots.ensure(sizeof(unsigned)));
+        HG_CK(cudaMemsetAsync(nslots.p, 0, sizeof(unsigned), st));
+        kb("assign_chunks", double(ntiles) * 16.0);
+        k_chunk_fill<<<grid1(ntiles, 256), 256, 0, st>>>(dp<unsigned>(off), dp<unsigned>(choff), ntiles, CHUNK,
+                                                        dp<Chunk>(chunks), dp<unsigned>(nslots));
+        ke();
+        {
+            std::vector<RecWeight<U>> mk(srcs.size());
+            bin_scatter_sources(srcs.data(), mk.data(), (int)srcs.size(), ag, ntiles, dp<PRec<U>>(rec),
+                                double(total) * sizeof(PRec<U>));
+        }
+        kb("assign_zero_split", 0.0);
+        k_zero_split_tiles<U, CPLX><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), ag, out_re, out_im, crowd_p, cwords);
+        ke();
+        const size_t tbytes = sizeof(U) * tcells;
         kb("assign_tile_accum", double(total) * sizeof(PRec<U>) + double(g.ntot) * sizeof(U) * (CPLX ? 2 : 1));
         switch (ag.scheme) {
-            case HG_NGP: launch_tile_accum<U, CPLX, HG_NGP>(fix, tbytes, nchunks, agx, out_re, out_im); break;
-            case HG_CIC: launch_tile_accum<U, CPLX, HG_CIC>(fix, tbytes, nchunks, agx, out_re, out_im); break;
-            case HG_TSC: launch_tile_accum<U, CPLX, HG_TSC>(fix, tbytes, nchunks, agx, out_re, out_im); break;
-            default: launch_tile_accum<U, CPLX, HG_PCS>(fix, tbytes, nchunks, agx, out_re, out_im); break;
+            case HG_NGP: launch_tile_accum<U, CPLX, HG_NGP>(fix, tbytes, nchunks, agx, out_re, out_im, crowd_p); break;
+            case HG_CIC: launch_tile_accum<U, CPLX, HG_CIC>(fix, tbytes, nchunks, agx, out_re, out_im, crowd_p); break;
+            case HG_TSC: launch_tile_accum<U, CPLX, HG_TSC>(fix, tbytes, nchunks, agx, out_re, out_im, crowd_p); break;
+            default: launch_tile_accum<U, CPLX, HG_PCS>(fix, tbytes, nchunks, agx, out_re, out_im, crowd_p); break;
         }
         ke();
+        if constexpr (!CPLX) {
+            if (crowd_p) {
+                kb("assign_split_writeout", 0.0);
+                k_crowd_writeout<U><<<nchunks, 256, 0, st>>>(dp<Chunk>(chunks), agx, crowd_p, out_re);
+                ke();
+            }
+        }
         if (mass_im) *mass_im = hm[1];
         return hm[0];
     }
+    DBuf crowd, nslots;  // split-tile staging of the fixed-point accumulation
 
     template <typename U, bool CPLX, int SCHEME>
-    void launch_tile_accum(bool fix, size_t tbytes, unsigned nchunks, const AssignGeom &ag, U *out_re, U *out_im) {
+    void launch_tile_accum(bool fix, size_t tbytes, unsigned nchunks, const AssignGeom &ag, U *out_re, U *out_im,
+                           unsigned long long *crowd_p) {
         if constexpr (!CPLX) {
-            if (fix) {  // FP32: two words of 4 bytes per cell; FP64: one of 8
-                const size_t sm = (sizeof(U) == 4) ? 2 * tbytes : tbytes;
+            if (fix) {  // FP32: two words of 4 bytes per cell; FP64: three
+                const size_t sm = (sizeof(U) == 4) ? 2 * tbytes : (3 * tbytes) / 2;
                 auto kern = k_tile_accum<U, false, true, SCHEME>;
                 HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                kern<<<nchunks, 256, sm, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
+                kern<<<nchunks, 256, sm, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im, crowd_p);
                 return;
             }
         }
         const size_t smem = tbytes * (CPLX ? 2 : 1);
         auto kern = k_tile_accum<U, CPLX, false, SCHEME>;
         HG_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<nchunks, 256, smem, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im);
+        kern<<<nchunks, 256, smem, st>>>(dp<PRec<U>>(rec), dp<Chunk>(chunks), ag, out_re, out_im, nullptr);
     }
 
     double assign_real(const PartSrc &src, const AssignGeom &ag, T *out) {
@@ -1216,9 +1253,11 @@ struct Engine : public hg_ctx {
     }
 
     // Launch-shape autotuning of the fused chain pass: the first time a chain runs on a given
-    // grid, every variant (kChainVariants) transforms a copy of the first two shells twice
-    // and the faster of the timed second runs is kept for the context.  The copy is restored
-    // before each run, so every variant sees the same data; the real shells are untouched.
+    // grid, every variant (kChainVariants) transforms a copy of the chain's shells (all of
+    // them, up to 2 GB: staging G once per CTA pays off over many shells, so fewer would
+    // favour the variants that do not stage it) twice, and the variant with the fastest
+    // second run is kept for the context.  The copy is restored before each run, so every
+    // variant sees the same data; the real shells are untouched.
     struct Tuned {
         int variant;
         std::vector<float> ms;
@@ -1229,8 +1268,9 @@ struct Engine : public hg_ctx {
         if (Mx != 32 && Mx != 64 && Mx != 128 && Mx != 192 && Mx != 256) return 0;
         auto it = chain_tuned.find(Mx);
         if (it != chain_tuned.end()) return it->second.variant;
-        const int nsh = std::min(ns, 2);
-        const size_t bytes = sizeof(C) * (size_t)Kx * plane * nsh;
+        const size_t per_shell = sizeof(C) * (size_t)Kx * plane;
+        const int nsh = (int)std::max<size_t>(1, std::min<size_t>((size_t)ns, (2ull << 30) / per_shell));
+        const size_t bytes = per_shell * nsh;
         HG_CK(tune_src.ensure(bytes));
         HG_CK(tune_buf.ensure(bytes));
         HG_CK(cudaMemcpyAsync(tune_src.p, T2.p, bytes, cudaMemcpyDeviceToDevice, st));
@@ -1263,8 +1303,11 @@ struct Engine : public hg_ctx {
         char line[256];
         for (const auto &kv : chain_tuned) {
             const ChainVariant &cv = kChainVariants[kv.second.variant];
-            snprintf(line, sizeof(line), "chain_x L=%d: variant %d (B=%d, G %s, %s)", kv.first, kv.second.variant,
-                     cv.B, cv.gs ? "staged in shared memory" : "read from L2", cv.pf ? "cp.async prefetch" : "no prefetch");
+            snprintf(line, sizeof(line), "chain_x L=%d %s: variant %d (B=%d, G %s, %s, %s)", kv.first,
+                     sizeof(T) == 8 ? "fp64" : "fp32", kv.second.variant, cv.B,
+                     cv.gs ? "staged in shared memory" : "read from L2", cv.pf ? "cp.async prefetch" : "no prefetch",
+                     cv.minb ? ("register cap for " + std::to_string(cv.minb) + " CTAs per SM").c_str()
+                             : "default register budget");
             out += line;
             for (size_t v = 0; v < kv.second.ms.size(); v++) {
                 snprintf(line, sizeof(line), "%s%.4f", v ? " " : "; ms per variant: ", kv.second.ms[v]);
@@ -1858,7 +1901,7 @@ struct Engine : public hg_ctx {
     cudaStream_t cst = nullptr;
     cudaEvent_t cev[2] = {nullptr, nullptr};
     void *pinned[2] = {nullptr, nullptr};
-    static constexpr size_t PIN_CHUNK = 32u << 20;
+    static constexpr size_t PIN_CHUNK = 64u << 20;
 
     void batch_release() {
         if (cst) cudaStreamSynchronize(cst);
@@ -1872,16 +1915,35 @@ struct Engine : public hg_ctx {
         cst = nullptr;
     }
 
-    // copy one catalogue into a device buffer (host thread: set_device first)
+    // copy one catalogue into a device buffer (host thread: set_device first).  Page-locked
+    // host memory is copied directly; pageable memory through the two pinned chunks, each
+    // filled by several host threads.
     void batch_upload(const hg_mock &m, void *dst) {
         HG_CK(cudaSetDevice(cfg.device));
         const size_t bytes = (size_t)m.n * (size_t)m.stride_bytes;
         const unsigned char *src = reinterpret_cast<const unsigned char *>(m.base);
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost) {
+            HG_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, cst));
+            HG_CK(cudaStreamSynchronize(cst));
+            return;
+        }
+        cudaGetLastError();  // a pageable pointer may leave an error behind on older runtimes
+        const unsigned nthr = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
         int k = 0;
         for (size_t o = 0; o < bytes; o += PIN_CHUNK, k ^= 1) {
             const size_t sz = std::min(PIN_CHUNK, bytes - o);
             HG_CK(cudaEventSynchronize(cev[k]));  // this chunk's previous copy is done
-            memcpy(pinned[k], src + o, sz);
+            {
+                std::vector<std::thread> th;
+                const size_t part = (sz + nthr - 1) / nthr;
+                for (unsigned t = 0; t < nthr; t++) {
+                    const size_t a = std::min(sz, t * part), b = std::min(sz, a + part);
+                    if (b > a)
+                        th.emplace_back([=] { memcpy(static_cast<unsigned char *>(pinned[k]) + a, src + o + a, b - a); });
+                }
+                for (auto &x : th) x.join();
+            }
             HG_CK(cudaMemcpyAsync(reinterpret_cast<unsigned char *>(dst) + o, pinned[k], sz, cudaMemcpyHostToDevice,
                                   cst));
             HG_CK(cudaEventRecord(cev[k], cst));

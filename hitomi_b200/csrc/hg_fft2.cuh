@@ -534,13 +534,19 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
 // rows are loaded into registers when it starts.  Less shared memory per CTA means more
 // CTAs per SM; which is faster depends on the precision and the line length, so the engine
 // times the variants once per geometry and keeps the fastest.
+// MINB: CTAs per SM the compiler must fit (the register cap: 65536 / (MINB x threads);
+// 0 keeps the default, 2 CTAs for FP32 and 1 for FP64).  The FP64 transform holds 24 complex
+// values per thread and is latency-bound at the two CTAs of 128 threads its 255 registers
+// allow; the capped variants trade spills for more warps in flight.
 struct ChainVariant {
     int B;
     bool gs, pf;
+    int minb;
 };
-constexpr ChainVariant kChainVariants[] = {{16, true, true}, {16, false, true}, {16, false, false},
-                                           {8, true, true},  {8, false, false}};
-constexpr int kNumChainVariants = 5;
+constexpr ChainVariant kChainVariants[] = {{16, true, true, 0},  {16, false, true, 0}, {16, false, false, 0},
+                                           {8, true, true, 0},   {8, false, false, 0}, {16, false, false, 3},
+                                           {16, false, false, 4}, {8, false, false, 8}};
+constexpr int kNumChainVariants = 8;
 
 template <typename T, int L, int B, bool GS, bool PF>
 struct ChainCfg {
@@ -556,8 +562,8 @@ struct ChainCfg {
 // columns), G [x][y][z].  Per shell j: load the K kept rows, inverse FFT, * G, forward FFT,
 // store the K kept rows.  The product happens in the positions a thread holds after the
 // inverse transform, which are its step-A positions of the forward transform.
-template <typename T, int L, int B, bool GS, bool PF>
-__global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, (sizeof(T) == 4) ? 2 : 1)
+template <typename T, int L, int B, bool GS, bool PF, int MINB>
+__global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : ((sizeof(T) == 4) ? 2 : 1))
     k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
                   const cplx<T> *__restrict__ tw) {
     using CF = ChainCfg<T, L, B, GS, PF>;
@@ -642,16 +648,16 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, (sizeof(T) == 4
     }
 }
 
-template <typename T, int L, int B, bool GS, bool PF>
+template <typename T, int L, int B, bool GS, bool PF, int MINB = 0>
 inline cudaError_t launch_chain_x_v(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
                                     const cplx<T> *tw, cudaStream_t st) {
     using CF = ChainCfg<T, L, B, GS, PF>;
     const size_t smem = CF::smem();
-    cudaError_t e = cudaFuncSetAttribute(k_chain_x_reg<T, L, B, GS, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_chain_x_reg<T, L, B, GS, PF, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned tiles = (unsigned)((plane + B - 1) / B);
-    k_chain_x_reg<T, L, B, GS, PF><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);
+    k_chain_x_reg<T, L, B, GS, PF, MINB><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);
     return cudaGetLastError();
 }
 
@@ -664,6 +670,9 @@ inline cudaError_t launch_chain_x_reg_L(int v, cplx<T> *t2, const cplx<T> *G, in
         case 2: return launch_chain_x_v<T, L, 16, false, false>(t2, G, ns, K, s, plane, tw, st);
         case 3: return launch_chain_x_v<T, L, 8, true, true>(t2, G, ns, K, s, plane, tw, st);
         case 4: return launch_chain_x_v<T, L, 8, false, false>(t2, G, ns, K, s, plane, tw, st);
+        case 5: return launch_chain_x_v<T, L, 16, false, false, 3>(t2, G, ns, K, s, plane, tw, st);
+        case 6: return launch_chain_x_v<T, L, 16, false, false, 4>(t2, G, ns, K, s, plane, tw, st);
+        case 7: return launch_chain_x_v<T, L, 8, false, false, 8>(t2, G, ns, K, s, plane, tw, st);
         default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, st);
     }
 }

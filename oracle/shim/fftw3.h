@@ -40,9 +40,16 @@ struct hx_fftw_plan_s {
 };
 typedef hx_fftw_plan_s *fftw_plan;
 
+/* Zero-filled, unlike FFTW's allocator: the reference's reconstruction skips the k = 0
+ * element of its displacement arrays without writing it (particle_reconstruction.hpp:64-71)
+ * and then transforms it, so with an uninitialised block its result depends on what the heap
+ * held (a uniform shift of one coordinate).  Zero is what a fresh page gives and what the
+ * method intends (no displacement from the mean density). */
 static inline fftw_complex *fftw_alloc_complex(size_t n) {
     void *p = nullptr;
-    if (posix_memalign(&p, 64, (n ? n : 1) * sizeof(fftw_complex)) != 0) return nullptr;
+    const size_t bytes = (n ? n : 1) * sizeof(fftw_complex);
+    if (posix_memalign(&p, 64, bytes) != 0) return nullptr;
+    memset(p, 0, bytes);
     return (fftw_complex *)p;
 }
 static inline void fftw_free(void *p) { free(p); }
