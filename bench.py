@@ -54,6 +54,18 @@ def workload(small: bool, n_mesh: int = 0, n_part: int = 0):
                 boxsize=1000.0, n_part=10_000_000, ngrid=256, binning=Binning(0.015, 0.255, 25))
 
 
+def workload_config(wl, world):
+    """The bench line's `config`: the workload alone, identical in both arms (the precision
+    form of our arm is reported beside it, in `form`)."""
+    b = wl["binning"]
+    return {"workload": wl["name"], "n_mesh": wl["n_mesh"], "n_particles": wl["n_part"], "boxsize": wl["boxsize"],
+            "assignment": "TSC", "n_kbin": b.n_kbin, "kmin": b.kmin, "kmax": b.kmax, "pk_ells": list(PK_ELLS),
+            "bk_multipoles": [list(m) for m in MULTIPOLES],
+            "l2": ("inputs larger than L2 (mesh and catalogue > 126 MB)" if wl["n_mesh"] ** 3 * 4 > 126e6
+                   else "inputs smaller than L2 (reduced check size)"),
+            "parallelism": f"mocks sharded over {world} rank(s), one catalogue each, no collective on the data path"}
+
+
 def catalogue(wl, seed):
     from hitomi_b200.synthetic import lognormal_box
     return lognormal_box(wl["n_part"], wl["boxsize"], ngrid=wl["ngrid"], seed=seed, exact_n=wl["n_part"])
@@ -222,17 +234,48 @@ def run_reference(args, wl, world, rank):
     line.update({
         "value": v,
         "ms_per_step": 1000.0 * statistics.median(per),
-        "config": {"workload": wl["name"], "n_mesh": wl["n_mesh"], "n_particles": wl["n_part"],
-                   "n_kbin": wl["binning"].n_kbin},
+        "config": workload_config(wl, world),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "reference",
                          "sample": "each step: every building block of the reference's box P/B drivers timed once "
-                                   "at 512^3 / 1e7 particles (one single-core process per block, concurrently); "
+                                   f"at {wl['n_mesh']}^3 / {wl['n_part']} particles (one single-core process per "
+                                   "block, concurrently); "
                                    "per-mock time extrapolated by the drivers' call counts; FFT is the project "
                                    "shim, not FFTW"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     })
     print(json.dumps(line), flush=True)
     return 0
+
+
+def cufft_reference(n_mesh, timing):
+    """cuFFT (through torch.fft.rfftn) on the density transform's shape, timed beside the
+    library's own transform as a reference point only: the real n^3 mesh to its
+    [n][n][n/2+1] half spectrum, FP32 and FP64, CUDA events over 5 runs after 3 warm-ups.
+    `ours_ms` is the library's fft_density (the same transform, its input scaled and
+    offset on the fly) from the profiled step of each form."""
+    import torch
+    out = {"shape": [n_mesh] * 3, "what": "real-to-complex 3-D transform, mean ms per transform"}
+    for name, dt in (("fp32", torch.float32), ("fp64", torch.float64)):
+        x = torch.randn((n_mesh,) * 3, dtype=dt, device="cuda")
+        for _ in range(3):
+            y = torch.fft.rfftn(x)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(5):
+            y = torch.fft.rfftn(x)
+        e1.record()
+        torch.cuda.synchronize()
+        out[f"cufft_{name}_ms"] = e0.elapsed_time(e1) / 5
+        del x, y
+    torch.cuda.empty_cache()
+    for form, t in timing.items():
+        st = t.get("stats") or {}
+        for key in ("fft_density", "fp64:fft_density"):
+            if key in st and st[key]["launches"]:
+                prec = "fp64" if (key.startswith("fp64:") or form == "fp64") else "fp32"
+                out[f"ours_{prec}_ms"] = st[key]["ms"]
+    return out
 
 
 def run_config(args) -> int:
@@ -450,6 +493,8 @@ def run_stage_table(args) -> int:
                        "rel_err": {k: max_rel_err(res[form][k], res["fp64"][k]) for k in res["fp64"]}}
     line = {"stage_table": table, "fp64_ms_per_mock": ms["fp64"], "workload": wl["name"], "steps": args.steps,
             "metric": "max over bins of |x - x_fp64| / max(|x_fp64|, 1e-12 max |x_fp64|)"}
+    if rank == 0 and not args.lean:
+        line["cufft_reference"] = cufft_reference(wl["n_mesh"], timing)
     if os.environ.get("HG_BENCH_DUMP"):
         np.savez_compressed(os.environ["HG_BENCH_DUMP"], **{f"{form}:{k}": v for form in res
                                                             for k, v in res[form].items()})
@@ -591,11 +636,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": dtype_of(head), "data": "synthetic",
-        "config": {"workload": wl["name"], "n_mesh": wl["n_mesh"], "n_particles": n, "boxsize": wl["boxsize"],
-                   "assignment": "TSC", "n_kbin": wl["binning"].n_kbin, "kmin": wl["binning"].kmin,
-                   "kmax": wl["binning"].kmax, "pk_ells": list(PK_ELLS), "bk_multipoles": [list(m) for m in MULTIPOLES],
-                   "form": head, "l2": "inputs larger than L2 (mesh and catalogue > 126 MB)",
-                   "parallelism": f"mocks sharded over {world} GPU(s), no collective on the data path"},
+        "config": workload_config(wl, world), "form": head,
         "clocks": t["clocks"],
         "e2e": {"value": evalue, "unit": UNIT, "h2d_bytes_per_step": int(n * 24), "d2h_bytes_per_step": int(t["d2h"]),
                 "how": "hg_batch_run through the C ABI with host buffers (the next mock's upload overlaps the "

@@ -39,6 +39,9 @@ SYMBOLS = (
     "hg_xi_box_recon",
     "hg_batch_run",
     "hg_batch_block_len",
+    "hg_batch_done",
+    "hg_set_memory_limit",
+    "hg_memory_in_use",
     "hg_read_ascii",
     "hg_read_gadget",
     "hg_free",
@@ -176,6 +179,12 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_batch_run.restype = ctypes.c_int
     lib.hg_batch_block_len.argtypes = [vp, i_, i_, i_]
     lib.hg_batch_block_len.restype = ctypes.c_longlong
+    lib.hg_batch_done.argtypes = [vp]
+    lib.hg_batch_done.restype = ctypes.c_int
+    lib.hg_set_memory_limit.argtypes = [vp, ctypes.c_longlong]
+    lib.hg_set_memory_limit.restype = ctypes.c_int
+    lib.hg_memory_in_use.argtypes = [vp]
+    lib.hg_memory_in_use.restype = ctypes.c_longlong
     lib.hg_read_ascii.argtypes = [ctypes.c_char_p, i_, ctypes.POINTER(c_dp), ctypes.POINTER(ctypes.c_longlong)]
     lib.hg_read_ascii.restype = ctypes.c_int
     lib.hg_read_gadget.argtypes = [ctypes.c_char_p, ctypes.POINTER(c_dp), ctypes.POINTER(ctypes.c_longlong),

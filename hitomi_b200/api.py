@@ -40,6 +40,16 @@ class HitomiError(RuntimeError):
     pass
 
 
+class BatchError(HitomiError):
+    """A batch stopped at a failing mock: `done` mocks completed, their results in `results`
+    (the same dicts batch_run returns), so a caller resumes from mock `done`."""
+
+    def __init__(self, msg, done, results):
+        super().__init__(msg)
+        self.done = done
+        self.results = results
+
+
 @dataclass
 class Binning:
     kmin: float
@@ -149,6 +159,14 @@ class Context:
             name, n, ms, by = line.split("\t")
             out[name] = dict(launches=int(n), ms=float(ms), bytes=float(by))
         return out
+
+    def set_memory_limit(self, nbytes: int):
+        """Cap the device memory this context's buffers may hold (0: no cap)."""
+        self._check(self._lib.hg_set_memory_limit(self._h, int(nbytes)))
+
+    def memory_in_use(self) -> int:
+        """Bytes of device memory the context's buffers hold now."""
+        return int(self._lib.hg_memory_in_use(self._h))
 
     def tuning(self) -> str:
         """The launch shapes the context's autotuner picked, with the time of every variant."""
@@ -334,10 +352,11 @@ class Context:
         blk = int(self._lib.hg_batch_block_len(self._h, npk, nbk, nz))
         out = np.zeros(blk * len(arrs))
         ip = lambda v: v.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
-        self._check(self._lib.hg_batch_run(self._h, ms, len(arrs), npk, ip(pk), nbk, ip(bk), nz, ip(zt), _dp(out)))
+        rc = self._lib.hg_batch_run(self._h, ms, len(arrs), npk, ip(pk), nbk, ip(bk), nz, ip(zt), _dp(out))
+        done = len(arrs) if rc == 0 else int(self._lib.hg_batch_done(self._h))
         nk, nr = self.binning.n_kbin, self.binning.n_rbin
         res = []
-        for i in range(len(arrs)):
+        for i in range(done):
             o = out[i * blk:(i + 1) * blk]
             r, p = {}, 0
             c = lambda v, *shape: (v[0::2] + 1j * v[1::2]).reshape(shape)
@@ -355,6 +374,8 @@ class Context:
                 r["zeta"], r["zeta_sn"] = c(o[p:p + sz], nz, nr, nr), c(o[p + sz:p + 2 * sz], nz, nr, nr)
                 r["zeta_norm"] = float(o[p + 2 * sz])
             res.append(r)
+        if rc != 0:
+            raise BatchError(self._lib.hg_last_error(self._h).decode(), done, res)
         return res
 
     def last_timing(self):

@@ -22,7 +22,29 @@ thread_local std::string g_create_error;
 namespace hg {
 void set_contextless_error(const std::string &m) { g_create_error = m; }
 const std::string &contextless_error() { return g_create_error; }
+MemBudget *&current_budget() {
+    thread_local MemBudget *b = nullptr;
+    return b;
+}
 }  // namespace hg
+
+namespace {
+// charges the allocations of one API call to its context
+struct BudgetScope {
+    hg::MemBudget *prev;
+    explicit BudgetScope(hg::MemBudget *b) : prev(hg::current_budget()) {
+        b->hit = false;
+        hg::current_budget() = b;
+    }
+    ~BudgetScope() { hg::current_budget() = prev; }
+};
+
+std::string with_budget_note(const hg_ctx *ctx, const std::string &m) {
+    if (!ctx->budget.hit) return m;
+    return m + " [the context's device memory limit of " + std::to_string(ctx->budget.limit) +
+           " bytes (hg_set_memory_limit) was reached; it holds " + std::to_string(ctx->budget.used) + " bytes]";
+}
+}  // namespace
 
 #define HG_CK(x)                                                                                    \
     do {                                                                                            \
@@ -65,21 +87,22 @@ const char *hg_last_error(const hg_ctx *ctx) {
 
 // Every entry point first makes the context's GPU current on the calling host thread, so
 // that contexts can be driven from several threads (one per context).
-#define HG_GUARD(ctx, body)                 \
-    do {                                    \
-        if (!(ctx)) return -1;              \
-        try {                               \
-            HG_CK(cudaSetDevice((ctx)->cfg.device)); \
-            body;                           \
-            (ctx)->err.clear();             \
-            return 0;                       \
-        } catch (const HgError &e) {        \
-            (ctx)->err = e.msg;             \
-            return -1;                      \
-        } catch (const std::exception &e) { \
-            (ctx)->err = e.what();          \
-            return -1;                      \
-        }                                   \
+#define HG_GUARD(ctx, body)                                  \
+    do {                                                     \
+        if (!(ctx)) return -1;                               \
+        try {                                                \
+            BudgetScope bs_(&(ctx)->budget);                 \
+            HG_CK(cudaSetDevice((ctx)->cfg.device));         \
+            body;                                            \
+            (ctx)->err.clear();                              \
+            return 0;                                        \
+        } catch (const HgError &e) {                         \
+            (ctx)->err = with_budget_note((ctx), e.msg);     \
+            return -1;                                       \
+        } catch (const std::exception &e) {                  \
+            (ctx)->err = with_budget_note((ctx), e.what());  \
+            return -1;                                       \
+        }                                                    \
     } while (0)
 
 int hg_set_particles(hg_ctx *ctx, int slot, const double *base, long long n, long long stride_bytes, int pos_off,
@@ -91,6 +114,21 @@ int hg_set_particles_device(hg_ctx *ctx, int slot, const double *dev_base, long 
                             int pos_off, int los_off, int w_off) {
     HG_GUARD(ctx, ctx->set_particles(slot, dev_base, n, stride_bytes, pos_off, los_off, w_off, true));
 }
+
+int hg_set_memory_limit(hg_ctx *ctx, long long bytes) {
+    if (!ctx) return -1;
+    if (bytes < 0) {
+        ctx->err = "the memory limit must be >= 0 bytes (0: none)";
+        return -1;
+    }
+    ctx->budget.limit = (size_t)bytes;
+    ctx->err.clear();
+    return 0;
+}
+
+long long hg_memory_in_use(const hg_ctx *ctx) { return ctx ? (long long)ctx->budget.used : -1; }
+
+int hg_batch_done(const hg_ctx *ctx) { return ctx ? ctx->batch_done : -1; }
 
 int hg_set_profiling(hg_ctx *ctx, int on) { HG_GUARD(ctx, ctx->set_profiling(on != 0)); }
 

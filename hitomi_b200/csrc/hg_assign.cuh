@@ -350,7 +350,40 @@ struct Defer {
     int *list;          // particle indices, capacity n
     unsigned *count;    // device counter
     int pass;           // 0: main pass (append), 1: the deferred pass (read the list)
+    unsigned *bad;      // main pass: counts particles with a non-finite position, weight or line
+                        // of sight; they get no tiles and no records (the host rejects the
+                        // catalogue when the count is not zero)
+    unsigned *neg;      // main pass: set to 1 when some particle has a negative coordinate; the
+                        // reference's int() truncates toward zero there, so a CIC or TSC stencil
+                        // weight can reach 2 per axis instead of at most 1 (the fixed-point
+                        // accumulation then takes 3 more bits of headroom)
 };
+
+// A particle whose scaled coordinate n x / L lies 2^30 cells or more from the mesh origin on
+// some axis (far outside the box, where the reference's int anchors overflow): on a
+// non-periodic mesh it lands in no cell and is dropped (returns true); on a periodic mesh
+// (PCS, interlacing) that coordinate is first reduced into [0, L].  Within 2^30 cells every
+// anchor and stencil index of the assignment is exact in int.
+__device__ __forceinline__ bool far_reduce(const AssignGeom &g, double pos[3]) {
+    bool drop = false;
+    for (int a = 0; a < 3; a++) {
+        if (fabs(pos[a] * double(g.n[a]) / g.L[a]) < 0x1p30) continue;
+        // separately rounded operations (no fused multiply-add): x - L floor(x / L)
+        if (g.periodic) pos[a] = __dsub_rn(pos[a], __dmul_rn(g.L[a], floor(__ddiv_rn(pos[a], g.L[a]))));
+        else drop = true;
+    }
+    return drop;
+}
+
+// Position, weight (when the source has one) and line of sight (when it has one) all finite.
+// The count and scatter passes apply the same test, so a skipped particle has no records.
+__device__ __forceinline__ bool particle_finite(const PartSrc &s, long long p, const double pos[3]) {
+    bool ok = isfinite(pos[0]) && isfinite(pos[1]) && isfinite(pos[2]);
+    const double *rec = reinterpret_cast<const double *>(s.base + p * s.stride);
+    if (s.w_off >= 0) ok = ok && isfinite(rec[s.w_off]);
+    if (s.los_off >= 0) ok = ok && isfinite(rec[s.los_off]) && isfinite(rec[s.los_off + 1]) && isfinite(rec[s.los_off + 2]);
+    return ok;
+}
 
 // Lanes of a warp with `want` set append their particle index to the list.
 __device__ __forceinline__ void defer_push(const Defer &df, bool want, long long p) {
@@ -381,14 +414,24 @@ __global__ void __launch_bounds__(256, 3) k_bin_count(PartSrc src, AssignGeom g,
     for (long long wbase = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wbase < total;
          wbase += wstride) {
         const long long i = wbase + lane;
-        const long long p = (i < total) ? (df.pass ? (long long)df.list[i] : i) : -1;
+        long long p = (i < total) ? (df.pass ? (long long)df.list[i] : i) : -1;
         TileList tl;
         int slow[HG_SLOW_TILES];
         tl.n = 0;
         bool push = false;
+        double pos[3];
+        if (p >= 0) load_pos(src, p, pos);
+        if (p >= 0 && !df.pass && !particle_finite(src, p, pos)) {
+            atomicAdd(df.bad, 1u);
+            p = -1;
+        }
+        if (p >= 0 && far_reduce(g, pos)) p = -1;
+        if (!df.pass) {  // warp-uniform point: every lane of the warp is here
+            const bool negc = p >= 0 && (pos[0] < 0.0 || pos[1] < 0.0 || pos[2] < 0.0);
+            if (__any_sync(0xffffffffu, negc) && lane == 0) atomicOr(df.neg, 1u);
+        }
         if (p >= 0) {
-            double pos[3], wr = 0.0, wi = 0.0;
-            load_pos(src, p, pos);
+            double wr = 0.0, wi = 0.0;
             if (mass) load_weight(src, p, wr, wi);
             int anc[3];
             double d[3];
@@ -472,14 +515,16 @@ __global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom 
     for (long long wbase = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wbase < total;
          wbase += wstride) {
         const long long i = wbase + lane;
-        const long long p = (i < total) ? (df.pass ? (long long)df.list[i] : i) : -1;
+        long long p = (i < total) ? (df.pass ? (long long)df.list[i] : i) : -1;
         TileList tl;
         int slow[HG_SLOW_TILES];
         tl.n = 0;
         typename MK::R r;
+        double pos[3];
+        if (p >= 0) load_pos(src, p, pos);
+        if (p >= 0 && !df.pass && !particle_finite(src, p, pos)) p = -1;
+        if (p >= 0 && far_reduce(g, pos)) p = -1;
         if (p >= 0) {
-            double pos[3];
-            load_pos(src, p, pos);
             int anc[3];
             double d[3];
             for (int a = 0; a < 3; a++) anchor(pos[a], g.n[a], g.L[a], g.scheme, g.shift, anc[a], d[a]);

@@ -31,13 +31,27 @@ struct HgError {
     std::string msg;
 };
 
+// Device memory held by one context's buffers, and the limit set by hg_set_memory_limit
+// (0: none).  Every engine allocation made during an API call is charged to the calling
+// context (current_budget), and returned to it when the buffer is freed; an allocation that
+// would pass the limit fails as cudaMalloc's out-of-memory does, with `hit` set.
+struct MemBudget {
+    size_t limit = 0;
+    size_t used = 0;
+    bool hit = false;
+};
+// the budget of the API call running on this thread (null outside API calls)
+MemBudget *&current_budget();
+
 }  // namespace hg
 
 struct hg_ctx {
     hg_config cfg;
     std::string err;
+    hg::MemBudget budget;
     double last_ms = 0.0;
     long long last_launches = 0;
+    int batch_done = 0;  // mocks completed by the last batch_run
     virtual ~hg_ctx() {}
     virtual void set_particles(int slot, const double *base, long long n, long long stride, int pos_off, int los_off,
                                int w_off, bool on_device) = 0;

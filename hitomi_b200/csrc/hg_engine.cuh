@@ -58,22 +58,36 @@ namespace {
 struct DBuf {
     void *p = nullptr;
     size_t n = 0;
+    MemBudget *owner = nullptr;  // the context charged for this buffer
     DBuf() = default;
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
     ~DBuf() { release(); }
     void release() {
         if (p) cudaFree(p);
+        if (p && owner) owner->used -= n;
         p = nullptr;
         n = 0;
+        owner = nullptr;
     }
     // grows only; contents are not preserved across a growth
     cudaError_t ensure(size_t bytes) {
         if (bytes <= n && p) return cudaSuccess;
         release();
-        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
-        if (e == cudaSuccess) n = bytes ? bytes : 16;
-        else p = nullptr;
+        const size_t want = bytes ? bytes : 16;
+        MemBudget *b = current_budget();
+        if (b && b->limit && b->used + want > b->limit) {
+            b->hit = true;
+            return cudaErrorMemoryAllocation;
+        }
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return e;
+        }
+        n = want;
+        owner = b;
+        if (b) b->used += want;
         return e;
     }
 };
@@ -245,6 +259,7 @@ struct Engine : public hg_ctx {
         DBuf rec, chunks;
         unsigned total = 0, nchunks = 0;
         bool ok = false;
+        bool neg = false;  // some particle has a negative coordinate (stencil_weight_bound)
     } sbins[2];
     std::map<std::array<int, 3>, std::unique_ptr<DBuf>> sfbuf;
     std::map<std::array<int, 3>, std::array<double, 2>> sfk0;
@@ -645,13 +660,15 @@ struct Engine : public hg_ctx {
         long long cap = 0;
         for (int q = 0; q < ns; q++) cap += srcs[q].n;
         HG_CK(deflist.ensure(sizeof(int) * std::max<long long>(cap, 1)));
-        HG_CK(defcnt.ensure(sizeof(unsigned) * ns));
-        HG_CK(cudaMemsetAsync(defcnt.p, 0, sizeof(unsigned) * ns, st));
+        // + the non-finite particle count and the negative-coordinate flag
+        HG_CK(defcnt.ensure(sizeof(unsigned) * (ns + 2)));
+        HG_CK(cudaMemsetAsync(defcnt.p, 0, sizeof(unsigned) * (ns + 2), st));
         long long o = 0;
         for (int q = 0; q < ns; q++) {
             if (q < 2) mass_blocks[q] = 0;
             if (srcs[q].n == 0) continue;  // an empty catalogue (no data for a window function)
-            Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0};
+            Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0, dp<unsigned>(defcnt) + ns,
+                     dp<unsigned>(defcnt) + ns + 1};
             const unsigned nb = (unsigned)std::min<long long>(grid1(srcs[q].n, 256), MASS_BLOCKS);
             if (q < 2) mass_blocks[q] = (int)nb;
             kb("assign_bin_count", double(srcs[q].n) * 24.0);
@@ -666,6 +683,22 @@ struct Engine : public hg_ctx {
         }
     }
 
+    // After bin_count_sources(ns sources): queue the read-back of its non-finite particle
+    // count and negative-coordinate flag into flags[0..1] (checked by check_finite once the
+    // stream has been synchronised).
+    void read_bad_count(int ns, unsigned *flags) {
+        HG_CK(cudaMemcpyAsync(flags, dp<unsigned>(defcnt) + ns, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    }
+    static void check_finite(const unsigned *flags) {
+        HG_REQUIRE(flags[0] == 0, "the catalogue holds " + std::to_string(flags[0]) +
+                                      " particle(s) with a non-finite position, weight or line of sight");
+    }
+    // the largest product of the three axis weights of one stencil point: 1 for coordinates
+    // >= 0 (and for NGP and PCS), 8 for CIC and TSC when a coordinate is negative
+    float stencil_weight_bound(bool neg) const {
+        return (neg && (cfg.assign == HG_CIC || cfg.assign == HG_TSC)) ? 8.0f : 1.0f;
+    }
+
     // Records of several sources (pass 3), from the front of each tile's range, then the
     // deferred particles from the back.
     template <class MK>
@@ -677,7 +710,8 @@ struct Engine : public hg_ctx {
         for (int q = 0; q < ns; q++) nsum += srcs[q].n;
         for (int q = 0; q < ns; q++) {
             if (srcs[q].n == 0) continue;
-            Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0};
+            Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0, dp<unsigned>(defcnt) + ns,
+                     dp<unsigned>(defcnt) + ns + 1};
             kb("assign_bin_scatter", double(srcs[q].n) * 24.0 + rec_bytes * double(srcs[q].n) / double(nsum));
             k_bin_scatter<MK><<<(unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 16), 256, 0, st>>>(
                 srcs[q], ag, mks[q], df, dp<unsigned>(off), dp<unsigned>(cursor), dp<unsigned>(cursor_back), recp);
@@ -729,7 +763,10 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemcpyAsync(&tot[1], dp<unsigned>(choff) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         if (want_mass)
             HG_CK(cudaMemcpyAsync(mp.data(), mass.p, sizeof(double) * mp.size(), cudaMemcpyDeviceToHost, st));
+        unsigned flags[2] = {0, 0};
+        read_bad_count((int)srcs.size(), flags);
         HG_CK(cudaStreamSynchronize(st));
+        check_finite(flags);
         if (want_mass)  // block partials in a fixed order
             for (size_t q = 0; q < srcs.size(); q++)
                 for (int b = 0; b < mass_blocks[q]; b++) {
@@ -756,7 +793,7 @@ struct Engine : public hg_ctx {
                 wmax = std::max(wmax, std::fabs(src.scale));
             }
             for (int a = 0; a < 3; a++) fix = fix && ag.n[a] >= stencil_width(ag.scheme);
-            agx.fix_bound = (float)(wmax * std::fabs(ag.acc_factor));
+            agx.fix_bound = (float)(wmax * std::fabs(ag.acc_factor)) * stencil_weight_bound(flags[1] != 0);
             fix = fix && agx.fix_bound >= 0x1p-60f;
         }
         // split tiles of a fixed-point accumulation add their chunks' exact partial sums as
@@ -1277,6 +1314,10 @@ struct Engine : public hg_ctx {
         Tuned tu{0, std::vector<float>(kNumChainVariants, 0.f)};
         float best = 1e30f;
         for (int v = 0; v < kNumChainVariants; v++) {
+            if (!chain_variant_exists(Mx, v)) {
+                tu.ms[v] = 0.f;
+                continue;
+            }
             for (int rep = 0; rep < 2; rep++) {
                 HG_CK(cudaMemcpyAsync(tune_buf.p, tune_src.p, bytes, cudaMemcpyDeviceToDevice, st));
                 HG_CK(cudaEventRecord(ev0, st));
@@ -1303,8 +1344,9 @@ struct Engine : public hg_ctx {
         char line[256];
         for (const auto &kv : chain_tuned) {
             const ChainVariant &cv = kChainVariants[kv.second.variant];
-            snprintf(line, sizeof(line), "chain_x L=%d %s: variant %d (B=%d, G %s, %s, %s)", kv.first,
-                     sizeof(T) == 8 ? "fp64" : "fp32", kv.second.variant, cv.B,
+            snprintf(line, sizeof(line), "chain_x L=%d %s: variant %d (%s, B=%d, G %s, %s, %s)", kv.first,
+                     sizeof(T) == 8 ? "fp64" : "fp32", kv.second.variant,
+                     cv.v12 ? "12 values per thread" : "two-level register transform", cv.B,
                      cv.gs ? "staged in shared memory" : "read from L2", cv.pf ? "cp.async prefetch" : "no prefetch",
                      cv.minb ? ("register cap for " + std::to_string(cv.minb) + " CTAs per SM").c_str()
                              : "default register budget");
@@ -1984,8 +2026,16 @@ struct Engine : public hg_ctx {
                 up_err = std::current_exception();
             }
         };
+        batch_done = 0;
+        auto mock_error = [](int i, const std::string &m) { return HgError{"mock " + std::to_string(i) + ": " + m}; };
         upload(0);
-        if (up_err) std::rethrow_exception(up_err);
+        if (up_err) {
+            try {
+                std::rethrow_exception(up_err);
+            } catch (const HgError &e) {
+                throw mock_error(0, e.msg);
+            }
+        }
         double total_ms = 0.0;
         long long total_launches = 0;
         for (int i = 0; i < n; i++) {
@@ -2014,12 +2064,22 @@ struct Engine : public hg_ctx {
                     total_ms += last_ms;
                     total_launches += last_launches;
                 }
+            } catch (const HgError &e) {
+                if (next.joinable()) next.join();
+                throw mock_error(i, e.msg);
             } catch (...) {
                 if (next.joinable()) next.join();
                 throw;
             }
             if (next.joinable()) next.join();
-            if (up_err) std::rethrow_exception(up_err);
+            batch_done = i + 1;
+            if (up_err) {
+                try {
+                    std::rethrow_exception(up_err);
+                } catch (const HgError &e) {
+                    throw mock_error(i + 1, e.msg);
+                }
+            }
         }
         last_ms = total_ms;
         last_launches = total_launches;
@@ -2438,6 +2498,8 @@ struct Engine : public hg_ctx {
         q.n = 1;
         std::vector<double> sr = particle_sums(1, q);
         const double wD = sd[0], w2D = sd[2], wR = sr[0];
+        HG_REQUIRE(std::isfinite(wD) && std::isfinite(w2D) && std::isfinite(wR),
+                   "the catalogue holds particle(s) with a non-finite weight");
         HG_REQUIRE(wD != 0.0 && wR != 0.0, "the summed weights of data and randoms must be non-zero");
         const double a = wD / wR;
         AssignGeom ag = make_geom(0.0);
@@ -2493,7 +2555,11 @@ struct Engine : public hg_ctx {
         unsigned tot[2] = {0, 0};
         HG_CK(cudaMemcpyAsync(&tot[0], dp<unsigned>(off) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaMemcpyAsync(&tot[1], dp<unsigned>(choff) + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        unsigned flags[2] = {0, 0};
+        read_bad_count(2, flags);
         HG_CK(cudaStreamSynchronize(st));
+        check_finite(flags);
+        B.neg = flags[1] != 0;
         B.total = tot[0];
         B.nchunks = tot[1];
         HG_CK(B.rec.ensure(sizeof(PRecS<T>) * std::max<size_t>(B.total, 1)));
@@ -2565,7 +2631,7 @@ struct Engine : public hg_ctx {
             wb = std::max(wb, std::pow(mw, std::max(1, srcs[q].wpow)) * std::fabs(srcs[q].scale));
         }
         for (int a = 0; a < 3; a++) fix = fix && ag.n[a] >= stencil_width(ag.scheme);
-        ag.fix_bound = (float)(wb * std::fabs(ag.acc_factor) * (1.0 + 1e-6));
+        ag.fix_bound = (float)(wb * std::fabs(ag.acc_factor) * (1.0 + 1e-6)) * stencil_weight_bound(B.neg);
         fix = fix && ag.fix_bound >= 0x1p-60f && std::isfinite(ag.fix_bound);
         const size_t smem = sizeof(T) * ag.t[0] * ag.t[1] * ag.t[2] * (CPLX ? 2 : 1) * (fix ? 2 : 1);
         kb("assign_tile_accum", double(B.total) * sizeof(PRecS<T>) + double(g.ntot) * sizeof(T) * (CPLX ? 2 : 1));

@@ -302,10 +302,13 @@ __global__ void __launch_bounds__(Fft2Cfg<T, L, COLS>::NT)
         i = 0;
         ok = o < g.n_outer;
     }
+    cplx<T> *Tw = S + X::ELEMS;  // twiddles, staged for the whole CTA (barrier below)
+    for (int e = threadIdx.x; e < L; e += CF::NT) Tw[e] = tw[e];
     cplx<T> v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; n1++) v[n1] = ok ? ld(o, R2 * n1 + t, i) : mk<T>(0, 0);
-    line_fft2<T, L, DIR, COLS, B>(v, S, t, b, tw);
+    __syncthreads();
+    line_fft2<T, L, DIR, COLS, B>(v, S, t, b, Tw);
     if (ok) {
 #pragma unroll
         for (int r = 0; r < R1; r++) st(o, pos_of_reg<L>(t, r), i, v[r]);
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(Fft2Cfg<T, L, COLS>::NT)
 template <typename T, int L, bool COLS>
 inline size_t fft2_smem() {
     using CF = Fft2Cfg<T, L, COLS>;
-    return (size_t)XchgLayout<L, COLS, CF::B>::ELEMS * sizeof(cplx<T>);
+    return ((size_t)XchgLayout<L, COLS, CF::B>::ELEMS + L) * sizeof(cplx<T>);  // exchange buffer, twiddles
 }
 
 // Strided passes over plain arrays (LdArr), software-pipelined: a persistent CTA walks its
@@ -327,9 +330,12 @@ inline size_t fft2_smem() {
 template <typename T, int L>
 struct PipeCfg {
     static constexpr int R2 = Split<L>::R2;
-    static constexpr int B = (L >= 256) ? 8 : 16;  // columns per tile
+    // columns per tile: the double buffer of FP64 1024-point tiles takes 4 columns to stay
+    // within the 227 KB a CTA may hold
+    static constexpr int B = (L >= 1024 && sizeof(T) == 8) ? 4 : ((L >= 256) ? 8 : 16);
     static constexpr int NT = R2 * B;
-    static constexpr size_t smem() { return 2 * (size_t)L * B * sizeof(cplx<T>); }
+    // double buffer, then the L twiddles (staged once per persistent CTA)
+    static constexpr size_t smem() { return (2 * (size_t)L * B + L) * sizeof(cplx<T>); }
 };
 
 __device__ __forceinline__ void cp_async_elem(void *sdst, const void *gsrc, int bytes, bool ok) {
@@ -348,6 +354,8 @@ __global__ void __launch_bounds__(PipeCfg<T, L>::NT)
     constexpr int R1 = X::R1, R2 = X::R2, B = PC::B, NT = PC::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *buf = reinterpret_cast<cplx<T> *>(smem_raw);  // [2][L][B]
+    cplx<T> *Tw = buf + 2 * L * B;                          // [L]
+    for (int e = threadIdx.x; e < L; e += NT) Tw[e] = tw[e];  // first read after the loop's first barrier
     const int t = threadIdx.x / B, b = threadIdx.x % B;
     const long long tpo = (g.n_inner + B - 1) / B;
     const long long ntiles = g.n_outer * tpo;
@@ -377,7 +385,7 @@ __global__ void __launch_bounds__(PipeCfg<T, L>::NT)
 #pragma unroll
         for (int n1 = 0; n1 < R1; n1++) v[n1] = S[(R2 * n1 + t) * B + b];
         __syncthreads();  // every value is in registers: S becomes the exchange buffer
-        line_fft2<T, L, DIR, true, B>(v, S, t, b, tw);
+        line_fft2<T, L, DIR, true, B>(v, S, t, b, Tw);
         const long long o = tile / tpo, i = (tile - o * tpo) * B + b;
         if (i < g.n_inner) {
 #pragma unroll
@@ -424,13 +432,17 @@ __global__ void __launch_bounds__(Fft2Cfg<T, L, false>::NT)
     const long long o = (long long)blockIdx.x * B + b;
     const bool ok = o < npair;
     const T *ra = mesh + 2 * o * L, *rb = ra + L;
+    constexpr int ELEMS = (X::ELEMS > B * LP) ? X::ELEMS : B * LP;
+    cplx<T> *Tw = S + ELEMS;  // twiddles, staged for the whole CTA (barrier below)
+    for (int e = threadIdx.x; e < L; e += CF::NT) Tw[e] = tw[e];
     cplx<T> v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; n1++) {
         const int p = R2 * n1 + t;
         v[n1] = ok ? mk<T>((ra[p] - sub) * scl, (rb[p] - sub) * scl) : mk<T>(0, 0);
     }
-    line_fft2<T, L, DIR, false, B>(v, S, t, b, tw);  // ends with S free
+    __syncthreads();
+    line_fft2<T, L, DIR, false, B>(v, S, t, b, Tw);  // ends with S free
 #pragma unroll
     for (int r = 0; r < R1; r++) S[b * LP + pos_of_reg<L>(t, r)] = v[r];
     __syncthreads();
@@ -450,7 +462,7 @@ inline cudaError_t launch_r2c_pair_L(const T *mesh, T sub, T scl, cplx<T> *H, lo
     using CF = Fft2Cfg<T, L, false>;
     using X = XchgLayout<L, false, CF::B>;
     const size_t elems = std::max<size_t>((size_t)X::ELEMS, (size_t)CF::B * (L + 1));
-    const size_t smem = elems * sizeof(cplx<T>);
+    const size_t smem = (elems + L) * sizeof(cplx<T>);  // exchange / row buffer, twiddles
     auto kern = k_fft2_r2c_pair<T, L, DIR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -538,30 +550,38 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
 // 0 keeps the default, 2 CTAs for FP32 and 1 for FP64).  The FP64 transform holds 24 complex
 // values per thread and is latency-bound at the two CTAs of 128 threads its 255 registers
 // allow; the capped variants trade spills for more warps in flight.
+// v12: the 192-point kernel with 12 values per thread (k_chain_x_192).
 struct ChainVariant {
     int B;
     bool gs, pf;
     int minb;
+    bool v12;
 };
-constexpr ChainVariant kChainVariants[] = {{16, true, true, 0},  {16, false, true, 0}, {16, false, false, 0},
-                                           {8, true, true, 0},   {8, false, false, 0}, {16, false, false, 3},
-                                           {16, false, false, 4}, {8, false, false, 8}};
-constexpr int kNumChainVariants = 8;
+constexpr ChainVariant kChainVariants[] = {
+    {16, true, true, 0, false},  {16, false, true, 0, false},  {16, false, false, 0, false},
+    {8, true, true, 0, false},   {8, false, false, 0, false},  {16, false, false, 3, false},
+    {16, false, false, 4, false}, {8, false, false, 8, false}, {8, false, false, 4, true},
+    {16, false, false, 2, true},  {8, true, false, 4, true},   {8, false, false, 3, true}};
+constexpr int kNumChainVariants = 12;
 
 template <typename T, int L, int B, bool GS, bool PF>
 struct ChainCfg {
     static constexpr int R2 = Split<L>::R2;
     static constexpr int NT = R2 * B;
-    static constexpr size_t smem() {
+    // exchange buffer, G tile (GS), the next shell's K kept rows (PF), the L twiddles
+    static size_t smem(int K) {
         return sizeof(cplx<T>) * ((size_t)XchgLayout<L, true, B>::ELEMS + (GS ? (size_t)L * B : 0) +
-                                  (PF ? (size_t)L * B : 0));
+                                  (PF ? (size_t)K * B : 0) + (size_t)L);
     }
 };
 
 // Fused chain x-pass with the register FFT: T2 layout [j][cx][y][z] (rows of `plane`
 // columns), G [x][y][z].  Per shell j: load the K kept rows, inverse FFT, * G, forward FFT,
 // store the K kept rows.  The product happens in the positions a thread holds after the
-// inverse transform, which are its step-A positions of the forward transform.
+// inverse transform, which are its step-A positions of the forward transform.  The twiddle
+// table is staged in shared memory once per CTA (the transforms read it on every shell; from
+// shared memory those reads wait less than L1 hits do), and the prefetch buffer holds only
+// the K kept rows, so that three FP64 CTAs of the staged variants fit on an SM.
 template <typename T, int L, int B, bool GS, bool PF, int MINB>
 __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : ((sizeof(T) == 4) ? 2 : 1))
     k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
@@ -572,28 +592,29 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
     cplx<T> *Gs = S + X::ELEMS;              // [x][b] (GS)
-    cplx<T> *Pb = Gs + (GS ? L * B : 0);     // next shell's input, [x][b] (PF); rows outside |n| <= s stay zero
+    cplx<T> *Pb = Gs + (GS ? L * B : 0);     // next shell's K kept rows, [c][b] (PF)
+    cplx<T> *Tw = Pb + (PF ? K * B : 0);     // twiddles [L]
     const int t = threadIdx.x / B, b = threadIdx.x % B;
     const long long i = (long long)blockIdx.x * B + b;
     const bool ok = i < plane;
-    if constexpr (GS || PF) {
+    for (int e = threadIdx.x; e < L; e += CF::NT) Tw[e] = tw[e];
+    if constexpr (GS) {
         for (int e = threadIdx.x; e < L * B; e += CF::NT) {
             const int x = e / B, bb = e % B;
             const long long ii = (long long)blockIdx.x * B + bb;
-            if constexpr (GS) Gs[e] = (ii < plane) ? G[(long long)x * plane + ii] : mk<T>(0, 0);
-            if constexpr (PF) Pb[e] = mk<T>(0, 0);
+            Gs[e] = (ii < plane) ? G[(long long)x * plane + ii] : mk<T>(0, 0);
         }
-        __syncthreads();
     }
-    // the K kept rows of shell j into Pb (position x = n mod L of row c = n + s)
+    __syncthreads();
+    // the K kept rows of shell j into Pb (row c = n + s; rows of columns past the plane
+    // are zero-filled)
     auto prefetch = [&](int j) {
         const cplx<T> *tj = t2 + (long long)j * K * plane;
         for (int e = threadIdx.x; e < K * B; e += CF::NT) {
             const int c = e / B, bb = e - c * B;
-            const int n = c - s, x = (n < 0) ? n + L : n;
             const long long ii = (long long)blockIdx.x * B + bb;
             const bool in = ii < plane;
-            cp_async_elem(Pb + x * B + bb, tj + (long long)c * plane + (in ? ii : 0), (int)sizeof(cplx<T>), in);
+            cp_async_elem(Pb + c * B + bb, tj + (long long)c * plane + (in ? ii : 0), (int)sizeof(cplx<T>), in);
         }
         asm volatile("cp.async.commit_group;\n" ::);
     };
@@ -611,7 +632,11 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
             asm volatile("cp.async.wait_group 0;\n" ::);
             __syncthreads();
 #pragma unroll
-            for (int n1 = 0; n1 < R1; n1++) v[n1] = Pb[(R2 * n1 + t) * B + b];
+            for (int n1 = 0; n1 < R1; n1++) {
+                const int x = R2 * n1 + t;
+                const int n = (x < L / 2) ? x : x - L;
+                v[n1] = (n >= -s && n <= s) ? Pb[(n + s) * B + b] : mk<T>(0, 0);
+            }
             __syncthreads();  // Pb is read: the next shell streams in while this one is transformed
             if (j + 1 < ns) prefetch(j + 1);
         } else {
@@ -622,7 +647,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
                 v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
             }
         }
-        line_fft2<T, L, +1, true, B>(v, S, t, b, tw);
+        line_fft2<T, L, +1, true, B>(v, S, t, b, Tw);
         if constexpr (R1 == R2) {
 #pragma unroll
             for (int r = 0; r < R1; r++) v[r] = v[r] * g_at(pos_of_reg<L>(t, r));
@@ -636,7 +661,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
 #pragma unroll
             for (int n1 = 0; n1 < R1; n1++) v[n1] = u[n1];
         }
-        line_fft2<T, L, -1, true, B>(v, S, t, b, tw);
+        line_fft2<T, L, -1, true, B>(v, S, t, b, Tw);
         if (ok) {
 #pragma unroll
             for (int r = 0; r < R1; r++) {
@@ -648,11 +673,162 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
     }
 }
 
+// ---- 192-point lines with 12 values per thread (16 threads per line): 192 = 12 x 4 x 4.
+// The two-level transform above holds 24 complex values per thread for this length; in FP64
+// that needs 255 registers and leaves two CTAs of 128 threads per SM, too few warps to hide
+// the memory latency.  Here: stage A, thread t takes x[16 n1 + t] (n1 < 12), their 12-point
+// DFT (prime-factor 3 x 4: input index (4 na + 3 nb) mod 12, output (4 ka + 9 kb) mod 12,
+// no twiddles inside) and multiplies output k1 by W_192^(t k1).  One 16-point DFT over t per
+// k1 remains, done as 4 x 4 (t = a + 4 c, k2 = q + 4 r): stage B, per item (k1, a), the
+// 4-point DFT over c of S[k1][a + 4c] times W_16^(a q); stage C, per item (k1, q), the
+// 4-point DFT over a, giving X[k1 + 12 (q + 4 r)].  Items are 0..47; thread t takes t,
+// t + 16 and t + 32 in stages B and C.
+
+template <typename T, int DIR>
+__device__ __forceinline__ void dft12(cplx<T> *v) {
+    cplx<T> a[3][4];
+#pragma unroll
+    for (int nb = 0; nb < 4; nb++)
+#pragma unroll
+        for (int na = 0; na < 3; na++) a[na][nb] = v[(4 * na + 3 * nb) % 12];
+#pragma unroll
+    for (int nb = 0; nb < 4; nb++) dft3<T, DIR>(a[0][nb], a[1][nb], a[2][nb]);
+#pragma unroll
+    for (int ka = 0; ka < 3; ka++) dft4<T, DIR>(a[ka][0], a[ka][1], a[ka][2], a[ka][3]);
+#pragma unroll
+    for (int ka = 0; ka < 3; ka++)
+#pragma unroll
+        for (int kb = 0; kb < 4; kb++) v[(4 * ka + 9 * kb) % 12] = a[ka][kb];
+}
+
+// line position held in register 4 j + r after line_fft192_12
+__device__ __forceinline__ int l192_pos(int t, int j, int r) { return ((t >> 2) + 4 * j) + 12 * ((t & 3) + 4 * r); }
+
+// One 192-point transform of B lines; S: [192][B] exchange buffer (column layout).  On entry
+// v[n1] = x[16 n1 + t]; on return v[4 j + r] = X[l192_pos(t, j, r)], S free for reuse.
+template <typename T, int DIR, int B>
+__device__ __forceinline__ void line_fft192_12(cplx<T> *v, cplx<T> *S, int t, int b, const cplx<T> *__restrict__ tw) {
+    dft12<T, DIR>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < 12; k1++) v[k1] = mul_tw<T, DIR>(v[k1], tw[t * k1]);  // W_192^(t k1)
+#pragma unroll
+    for (int k1 = 0; k1 < 12; k1++) S[(k1 * 16 + t) * B + b] = v[k1];
+    __syncthreads();
+    const int a = t & 3;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {  // stage B: item (k1, a)
+        const int k1 = (t >> 2) + 4 * j;
+        cplx<T> u0 = S[(k1 * 16 + a) * B + b], u1 = S[(k1 * 16 + a + 4) * B + b];
+        cplx<T> u2 = S[(k1 * 16 + a + 8) * B + b], u3 = S[(k1 * 16 + a + 12) * B + b];
+        dft4<T, DIR>(u0, u1, u2, u3);
+        v[4 * j] = u0;
+        v[4 * j + 1] = mul_tw<T, DIR>(u1, tw[12 * a]);  // W_16^(a q) = W_192^(12 a q)
+        v[4 * j + 2] = mul_tw<T, DIR>(u2, tw[24 * a]);
+        v[4 * j + 3] = mul_tw<T, DIR>(u3, tw[36 * a]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int k1 = (t >> 2) + 4 * j;
+#pragma unroll
+        for (int q = 0; q < 4; q++) S[(k1 * 16 + q * 4 + a) * B + b] = v[4 * j + q];
+    }
+    __syncthreads();
+    const int q = t & 3;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {  // stage C: item (k1, q)
+        const int k1 = (t >> 2) + 4 * j;
+        cplx<T> w0 = S[(k1 * 16 + q * 4) * B + b], w1 = S[(k1 * 16 + q * 4 + 1) * B + b];
+        cplx<T> w2 = S[(k1 * 16 + q * 4 + 2) * B + b], w3 = S[(k1 * 16 + q * 4 + 3) * B + b];
+        dft4<T, DIR>(w0, w1, w2, w3);
+        v[4 * j] = w0;
+        v[4 * j + 1] = w1;
+        v[4 * j + 2] = w2;
+        v[4 * j + 3] = w3;
+    }
+    __syncthreads();
+}
+
+// The fused chain x-pass (as k_chain_x_reg) on 192-point lines with line_fft192_12.  The
+// inverse transform leaves the positions l192_pos, which are not the forward transform's
+// step-A positions, so the product with G goes through the exchange buffer.  MINB CTAs per SM
+// set the register cap (4 x 128 threads: 128 registers).
+template <typename T, int B, bool GS, int MINB>
+__global__ void __launch_bounds__(16 * B, MINB)
+    k_chain_x_192(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
+                  const cplx<T> *__restrict__ tw) {
+    constexpr int L = 192;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);  // [192][B]
+    cplx<T> *Gs = S + L * B;                               // [192][B] (GS)
+    cplx<T> *Tw = Gs + (GS ? L * B : 0);                   // twiddles [192]
+    const int t = threadIdx.x / B, b = threadIdx.x % B;
+    const long long i = (long long)blockIdx.x * B + b;
+    const bool ok = i < plane;
+    for (int e = threadIdx.x; e < L; e += 16 * B) Tw[e] = tw[e];
+    if constexpr (GS) {
+        for (int e = threadIdx.x; e < L * B; e += 16 * B) {
+            const int x = e / B, bb = e % B;
+            const long long ii = (long long)blockIdx.x * B + bb;
+            Gs[e] = (ii < plane) ? G[(long long)x * plane + ii] : mk<T>(0, 0);
+        }
+    }
+    __syncthreads();
+    for (int j = 0; j < ns; j++) {
+        cplx<T> *tj = t2 + (long long)j * K * plane;
+        cplx<T> v[12];
+#pragma unroll
+        for (int n1 = 0; n1 < 12; n1++) {
+            const int x = 16 * n1 + t;
+            const int n = (x < L / 2) ? x : x - L;
+            v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
+        }
+        line_fft192_12<T, +1, B>(v, S, t, b, Tw);
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int p = l192_pos(t, jj, r);
+                cplx<T> gv;
+                if constexpr (GS) gv = Gs[p * B + b];
+                else gv = ok ? G[(long long)p * plane + i] : mk<T>(0, 0);
+                S[p * B + b] = v[4 * jj + r] * gv;
+            }
+        __syncthreads();
+#pragma unroll
+        for (int n1 = 0; n1 < 12; n1++) v[n1] = S[(16 * n1 + t) * B + b];
+        __syncthreads();
+        line_fft192_12<T, -1, B>(v, S, t, b, Tw);
+        if (ok) {
+#pragma unroll
+            for (int jj = 0; jj < 3; jj++)
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    const int p = l192_pos(t, jj, r);
+                    const int n = (p < L / 2) ? p : p - L;
+                    if (n >= -s && n <= s) tj[(long long)(n + s) * plane + i] = v[4 * jj + r];
+                }
+        }
+    }
+}
+
+template <typename T, int B, bool GS, int MINB>
+inline cudaError_t launch_chain_x_192(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
+                                      const cplx<T> *tw, cudaStream_t st) {
+    const size_t smem = sizeof(cplx<T>) * (192 * B * (GS ? 2 : 1) + 192);
+    cudaError_t e = cudaFuncSetAttribute(k_chain_x_192<T, B, GS, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const unsigned tiles = (unsigned)((plane + B - 1) / B);
+    k_chain_x_192<T, B, GS, MINB><<<tiles, 16 * B, smem, st>>>(t2, G, ns, K, s, plane, tw);
+    return cudaGetLastError();
+}
+
 template <typename T, int L, int B, bool GS, bool PF, int MINB = 0>
 inline cudaError_t launch_chain_x_v(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
                                     const cplx<T> *tw, cudaStream_t st) {
     using CF = ChainCfg<T, L, B, GS, PF>;
-    const size_t smem = CF::smem();
+    const size_t smem = CF::smem(K);
     cudaError_t e = cudaFuncSetAttribute(k_chain_x_reg<T, L, B, GS, PF, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -673,9 +849,24 @@ inline cudaError_t launch_chain_x_reg_L(int v, cplx<T> *t2, const cplx<T> *G, in
         case 5: return launch_chain_x_v<T, L, 16, false, false, 3>(t2, G, ns, K, s, plane, tw, st);
         case 6: return launch_chain_x_v<T, L, 16, false, false, 4>(t2, G, ns, K, s, plane, tw, st);
         case 7: return launch_chain_x_v<T, L, 8, false, false, 8>(t2, G, ns, K, s, plane, tw, st);
+        case 8:
+            if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 4>(t2, G, ns, K, s, plane, tw, st);
+            return cudaErrorInvalidValue;
+        case 9:
+            if constexpr (L == 192) return launch_chain_x_192<T, 16, false, 2>(t2, G, ns, K, s, plane, tw, st);
+            return cudaErrorInvalidValue;
+        case 10:
+            if constexpr (L == 192) return launch_chain_x_192<T, 8, true, 4>(t2, G, ns, K, s, plane, tw, st);
+            return cudaErrorInvalidValue;
+        case 11:
+            if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 3>(t2, G, ns, K, s, plane, tw, st);
+            return cudaErrorInvalidValue;
         default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, st);
     }
 }
+
+// whether variant v exists for line length L (8 .. 11: the 12-values-per-thread 192 kernel)
+inline bool chain_variant_exists(int L, int v) { return v < 8 || L == 192; }
 
 }  // namespace HG_TU_NS
 }  // namespace hg

@@ -230,10 +230,15 @@ typedef struct hg_mock {
  *   bk_save [n_bk][n_kbin][n_kbin] complex, sn_save likewise, then 1 norm (if n_bk > 0);
  *   zeta_save [n_zeta][n_rbin][n_rbin] complex, sn_save likewise, then 1 norm (if n_zeta > 0).
  * Each block equals what hg_pk_box, hg_bk_box_multi and hg_zeta_box_multi give for that
- * catalogue. */
+ * catalogue.  When a mock fails (a catalogue with non-finite positions, a memory limit),
+ * the call returns -1 with the mock's index in hg_last_error; the blocks of the mocks
+ * before it are complete (hg_batch_done), so a caller resumes from there. */
 int hg_batch_run(hg_ctx *ctx, const hg_mock *mocks, int n_mocks, int n_pk, const int *pk_ells, int n_bk,
                  const int *bk_ells, int n_zeta, const int *zeta_ells, double *out);
 long long hg_batch_block_len(const hg_ctx *ctx, int n_pk, int n_bk, int n_zeta);
+/* How many mocks the last hg_batch_run on this context completed (all of them after a
+ * return of 0). */
+int hg_batch_done(const hg_ctx *ctx);
 
 /* BAO reconstruction of the current data (slot 0) and randoms (slot 1) on this context's
  * mesh (create the context with the reference's n_mesh_recon) and assignment scheme.
@@ -300,6 +305,16 @@ void hg_free(void *p);
  * clock() progress prints (bispec.hpp:1170-1171, powerspec.hpp:63-66). */
 int hg_set_profiling(hg_ctx *ctx, int on);
 int hg_kernel_stats(hg_ctx *ctx, char *buf, long long buflen);
+
+/* Device memory of a context.  hg_set_memory_limit caps what the context's buffers may hold
+ * (bytes; 0 removes the cap): a statistic that would need more fails with -1 and a message
+ * naming the limit, without launching past the failed allocation, and the context stays
+ * usable (raise the limit and call again).  Buffers are kept between calls and grow only, so
+ * the cap also bounds what a long-lived context keeps.  hg_memory_in_use returns the bytes
+ * the context's buffers hold now.  The reference has no counterpart (its global `byte`
+ * counter, common.hpp:36, only prints). */
+int hg_set_memory_limit(hg_ctx *ctx, long long bytes);
+long long hg_memory_in_use(const hg_ctx *ctx);
 
 /* The launch shapes the context's autotuner picked (one line per tuned kernel and grid: the
  * chosen variant and the measured time of every variant).  No counterpart in the

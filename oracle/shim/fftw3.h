@@ -14,8 +14,11 @@
  * Algorithm: power-of-two lengths use an iterative Stockham autosort FFT (radix 4,
  * one radix-2 stage when log2 n is odd); other lengths a recursive Cooley-Tukey over
  * their prime factors with direct DFTs of the odd primes.  Twiddles come from sincos
- * of an exactly reduced angle.  Nothing here is FFTW's code; results
- * agree with FFTW-double to ~1e-15 relative, far inside the oracle's 1e-10 budget.
+ * of an exactly reduced angle.  Nothing here is FFTW's code.  tests/test_oracle_shims.py
+ * checks it against numpy.fft (pocketfft) for power-of-two, mixed and prime lengths, both
+ * signs: <= 6e-16 of the largest output.  FFTW itself is not in this image, so the distance
+ * to FFTW's own rounding is not measured; two correctly rounded double FFTs differ at the
+ * same ~1e-16 level, far inside the oracle's 1e-10 budget.
  */
 #ifndef HITOMI_ORACLE_FFTW3_SHIM_H
 #define HITOMI_ORACLE_FFTW3_SHIM_H

@@ -16,7 +16,8 @@
  *   - natural cubic spline: c_i = s''(x_i)/2 from the symmetric tridiagonal system
  *     h_{i-1} c_{i-1} + 2 (h_{i-1}+h_i) c_i + h_i c_{i+1} = 3 (dy_i/h_i - dy_{i-1}/h_{i-1}),
  *     c_0 = c_{n-1} = 0, evaluated as y_i + dx (b_i + dx (c_i + dx d_i)).
- * tests/test_oracle_shims.py checks each against scipy.special / sympy.
+ * tests/test_oracle_shims.py checks each against scipy.special, scipy.interpolate and
+ * sympy's exact 3j symbols.
  */
 #ifndef HITOMI_ORACLE_GSL_IMPL_H
 #define HITOMI_ORACLE_GSL_IMPL_H

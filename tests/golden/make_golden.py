@@ -14,6 +14,8 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --xi     (only xi_window.npz: 2PCF, window 2PCF / 3PCF)
     python tests/golden/make_golden.py --ingest (only ingest.npz: the ASCII and Gadget readers)
     python tests/golden/make_golden.py --recon  (only recon.npz: BAO reconstruction)
+    python tests/golden/make_golden.py --outside (only box_outside.npz: particles outside the box)
+    python tests/golden/make_golden.py --long   (only box_long_axes.npz: 1024-point axes)
     python tests/golden/make_golden.py --configs (only box_config_sizes.npz: 128^3 and 512^3)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
@@ -288,6 +290,53 @@ def make_ingest():
                         gadget1=np.frombuffer(gfiles[1], dtype=np.uint8), gadget_ref=gadget_ref)
 
 
+def outside_catalogue(n_mesh: int, boxsize: float, n: int, seed: int) -> np.ndarray:
+    """Particles partly outside the box: a quarter within 1.6 cells beyond a face (where the
+    reference's int() truncation toward zero gives CIC/TSC weights above 1 for negative
+    coordinates and the flat-index rule bleeds into neighbouring rows), and a few at up to
+    three box lengths away on one axis (dropped, or landed elsewhere by the flat-index rule)."""
+    rng = np.random.default_rng(seed)
+    dr = boxsize / n_mesh
+    pos = lognormal_box(n, boxsize, ngrid=n_mesh, seed=seed, exact_n=n)
+    k = n // 4
+    axis = rng.integers(0, 3, size=k)
+    side = rng.random(k) < 0.5
+    off = rng.uniform(0.0, 1.6 * dr, size=k)
+    pos[np.arange(k), axis] = np.where(side, -off, boxsize + off)
+    m = 40
+    axis = rng.integers(0, 3, size=m)
+    pos[k + np.arange(m), axis] = rng.uniform(-3.0 * boxsize, 4.0 * boxsize, size=m)
+    return np.ascontiguousarray(pos)
+
+
+def make_outside():
+    """P_l and B_000 of a catalogue with particles outside the box (outside_catalogue), every
+    assignment scheme of the reference: its bounds rule (field.hpp:92-96) applied to the
+    anchors its int() truncation gives."""
+    pos = outside_catalogue(32, 1000.0, 12000, seed=21)
+    b = Binning(0.015, 0.095, 9, 4.0, 156.0, 20)  # below the 32^3 Nyquist k = 0.1
+    d = dict(pos=pos, boxsize=1000.0, n_mesh=32, binning=binning_arr(b))
+    for assign in ("NGP", "CIC", "TSC"):
+        for ell, v in run_pk(pos, 32, 1000.0, b, assign, ells=(0, 2)).items():
+            d[f"pk_{assign}_{ell}"] = v
+        d[f"bk_{assign}_000"] = run_bk(pos, 32, 1000.0, b, assign, mps=((0, 0, 0),))[(0, 0, 0)]
+    np.savez_compressed(os.path.join(HERE, "box_outside.npz"), **d)
+
+
+def make_long_axes():
+    """P_l on a [1024, 16, 1024] mesh: the longest line length the transforms support, on
+    the strided (x) and the contiguous (z) axis."""
+    pos = uniform_box(20000, 1000.0, seed=22)
+    b = Binning(0.01, 0.15, 8, 4.0, 156.0, 20)
+    nm = [1024, 16, 1024]
+    d = dict(pos=pos, boxsize=np.array([1000.0, 1000.0, 1000.0]), n_mesh=np.array(nm), binning=binning_arr(b))
+    for ell in (0, 2):
+        with ref_runner.RefRun() as r:
+            r.run("pk", pos, ell, 0, ell, nm, 1000.0, b)
+            d[f"pk_{ell}"] = r.pk(ell)[1]
+    np.savez_compressed(os.path.join(HERE, "box_long_axes.npz"), **d)
+
+
 def make_recon():
     """BAO reconstruction (particle_reconstruction.hpp:12-402) through the reference's drivers:
     the shifted positions and the reconstructed P_l, survey (main.cpp:215-225, then
@@ -368,6 +417,13 @@ def make_config_sizes():
 
 
 def main():
+    if "--outside" in sys.argv or "--long" in sys.argv:
+        if "--outside" in sys.argv:
+            make_outside()
+        if "--long" in sys.argv:
+            make_long_axes()
+        print("fixtures written")
+        return
     if "--recon" in sys.argv:
         make_recon()
         print("fixtures written")
@@ -458,6 +514,8 @@ def main():
     make_survey_three_point()
     make_extensions()
     make_bk_256()
+    make_outside()
+    make_long_axes()
     print("fixtures written")
 
 

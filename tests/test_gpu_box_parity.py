@@ -102,6 +102,19 @@ def test_pk_noncubic_mesh(form):
             assert relerr(norm * pk, d[f"pk_{ell}"], FLOOR[form]) < TOL[form], ell
 
 
+@pytest.mark.parametrize("form", ["fp64", "fp32"])
+def test_pk_1024_point_axes(form):
+    """[1024, 16, 1024] mesh: 1024-point lines on the strided axis (the pipelined pass, whose
+    FP64 tiles are 4 columns wide) and on the contiguous axis (the paired real transform)."""
+    d = load_golden("box_long_axes.npz")
+    b = binning_from(d["binning"])
+    with ctx([int(v) for v in d["n_mesh"]], [float(v) for v in d["boxsize"]], b, "TSC", form) as c:
+        c.set_particles(0, d["pos"])
+        for ell in (0, 2):
+            pk, _, norm = c.pk_box(ell)
+            assert relerr(norm * pk, d[f"pk_{ell}"], FLOOR[form]) < TOL[form], ell
+
+
 def test_gadget_record_stride():
     """Positions read in place from the reference's {pos[3], vel[3]} records (48-byte stride)."""
     d = load_golden("box_pk.npz")
@@ -166,3 +179,49 @@ def test_bk_box_odd_multipoles(form):
             bk, sn, norm = c.bk_box(*mp)
             ref = d["bk_TSC_" + "".join(map(str, mp))]
             assert relerr(norm * (bk - sn), ref, FLOOR[form]) < TOL[form], mp
+
+
+# The headline form: FP32 context with FP64 density and bispectrum signal, shot noise FP32.
+CHOSEN = ("density", "bk_signal")
+
+
+def test_chosen_form_pk_meets_bar():
+    """P_l of the headline form against the reference at the path's bar, 1e-5 relative per
+    bin with only the 1e-12 max|bins| floor (P is binned from the FP64 density spectrum)."""
+    from hitomi_b200.api import Context
+    d = load_golden("box_pk.npz")
+    b = binning_from(d["binning"])
+    for n_mesh in (32, 64):
+        with Context(n_mesh, float(d["boxsize"]), b, "TSC", "fp32", fp64_stages=CHOSEN) as c:
+            c.set_particles(0, d["pos"])
+            for ell in (0, 2, 4):
+                pk, nmode, norm = c.pk_box(ell)
+                assert relerr(norm * pk, d[f"pk_{n_mesh}_TSC_{ell}"], 1e-12) < 1e-5, (n_mesh, ell)
+
+
+@pytest.mark.parametrize("name,n_mesh", [("box_bk.npz", 32), ("box_bk_256.npz", 256)])
+def test_chosen_form_bk_against_fp64(name, n_mesh):
+    """B_l of the headline form against the FP64 form on the same catalogue, per bin with the
+    1e-12 max|bins| floor: within 1e-5 wherever the shot noise is not most of the bin.  The
+    shot-noise half stays FP32 (4e-4 of itself), so the bar applies to bins where
+    |B - S| >= |S|, the rest are held to 1e-4 of |S|."""
+    from hitomi_b200.api import Context
+    d = load_golden(name)
+    b = binning_from(d["binning"])
+    mps = MULTIPOLES if name == "box_bk.npz" else ((0, 0, 0), (2, 0, 2))
+    out = {}
+    for form, stages in (("fp64", ()), ("fp32", CHOSEN)):
+        with Context(n_mesh, float(d["boxsize"]), b, "TSC", form, fp64_stages=stages) as c:
+            c.set_particles(0, d["pos"])
+            out[form] = c.bk_box_multi(mps)
+    bk64, sn64, n64 = out["fp64"]
+    bkc, snc, nc = out["fp32"]
+    assert n64 == nc
+    for q, mp in enumerate(mps):
+        assert relerr(bkc[q], bk64[q], 1e-12) < 1e-10, mp  # signal in FP64: the FP64 form's value
+        full64, fullc = n64 * (bk64[q] - sn64[q]), nc * (bkc[q] - snc[q])
+        err = np.abs(fullc - full64)
+        scale = np.maximum(np.abs(full64), 1e-12 * np.max(np.abs(full64)))
+        shot_dom = np.abs(n64 * sn64[q]) > np.abs(full64)
+        assert np.all((err / scale < 1e-5) | shot_dom), mp
+        assert np.all(err[shot_dom] <= 1e-4 * np.abs(n64 * sn64[q])[shot_dom]), mp
