@@ -73,6 +73,51 @@ struct StRowsCompact {  // output [o][K][inner], keep compact rows only
     }
 };
 
+// Shell-extent pruning of B1 and B2.  Shell j's modes reach |n_a| <= e_j,a only (e_j grows
+// with k_j; the cube side K = 2s+1 is set by the largest shell), so B1 transforms only the
+// lines (j, cx, cy) with |cx - s_x| <= e_j,x and |cy - s_y| <= e_j,y, and B2 only the lines
+// (j, cx) with |cx - s_x| <= e_j,x: pass line q is line lines[q] of the full layout.  T1 and
+// T2 lines outside those sets are never written, and their readers (B2's rows, X's rows)
+// treat them as zero by the same extents.
+template <typename T>
+struct LdCubeL {  // B1: compact cube line lines[q], kept modes |n_z| <= e_j,z
+    const cplx<T> *p;
+    int K, M, s;
+    const int *lines;
+    const int4 *ext;  // per shell (e_x, e_y, e_z, -)
+    int kxky;         // Kx Ky: lines per shell
+    __device__ __forceinline__ cplx<T> operator()(long long q, int l, long long i) const {
+        const int o = lines[q];
+        const int e = ext[o / kxky].z;
+        const int n = (l < M / 2) ? l : l - M;
+        return (n >= -e && n <= e) ? p[(long long)o * K + n + s] : mk<T>(0, 0);
+    }
+};
+template <typename T>
+struct LdRowsCompactL {  // B2: [o][K][inner] at line lines[q], rows |n_y| <= e_j,y
+    const cplx<T> *p;
+    int K, M, s;
+    long long inner;
+    const int *lines;
+    const int4 *ext;
+    int kx;  // lines per shell
+    __device__ __forceinline__ cplx<T> operator()(long long q, int l, long long i) const {
+        const int o = lines[q];
+        const int e = ext[o / kx].y;
+        const int n = (l < M / 2) ? l : l - M;
+        return (n >= -e && n <= e) ? p[((long long)o * K + n + s) * inner + i] : mk<T>(0, 0);
+    }
+};
+template <typename T>
+struct StArrL {  // [o][L][inner] at line lines[q]
+    cplx<T> *p;
+    long long L, inner;
+    const int *lines;
+    __device__ __forceinline__ void operator()(long long q, int l, long long i, cplx<T> v) const {
+        p[((long long)lines[q] * L + l) * inner + i] = v;
+    }
+};
+
 // X: fused  inverse FFT (x) -> * G -> forward FFT (x)  over all shells of a family.
 // T2 layout [j][cx][y][z] (K rows of M*M); G layout [x][y][z].  One CTA per tile of
 // B consecutive (y,z) columns; shells processed in a loop.  Shared memory: the G tile
@@ -88,7 +133,7 @@ struct XTile {
 template <typename T, int L>
 __global__ void __launch_bounds__(XTile<T, L>::NT)
     k_chain_x(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
-              const cplx<T> *__restrict__ tw) {
+              const cplx<T> *__restrict__ tw, const int *__restrict__ ext_x) {
     using X = XTile<T, L>;
     constexpr int B = X::B, LP = X::LP, NT = X::NT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -103,12 +148,13 @@ __global__ void __launch_bounds__(XTile<T, L>::NT)
     }
     for (int j = 0; j < ns; j++) {
         cplx<T> *tj = t2 + (long long)j * K * plane;
+        const int ej = ext_x ? ext_x[j] : s;  // rows of shell j that B2 wrote
         __syncthreads();
         for (int e = threadIdx.x; e < B * L; e += NT) {
             int x = e / B, b = e - x * B;
             long long i = i0 + b;
-            int c = pos_to_c(x, L, s);
-            w[b * LP + x] = (c >= 0 && i < plane) ? tj[(long long)c * plane + i] : mk<T>(0, 0);
+            const int n = (x < L / 2) ? x : x - L;
+            w[b * LP + x] = (n >= -ej && n <= ej && i < plane) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
         }
         __syncthreads();
         smem_fft<T, L, +1, NT>(w, LP, B, tw);
@@ -135,27 +181,27 @@ inline size_t chain_x_smem() {
 
 template <typename T, int L>
 inline cudaError_t launch_chain_x_L(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
-                                    const cplx<T> *tw, cudaStream_t st) {
+                                    const cplx<T> *tw, const int *ext, cudaStream_t st) {
     using X = XTile<T, L>;
     size_t smem = chain_x_smem<T, L>();
     cudaFuncSetAttribute(k_chain_x<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     unsigned tiles = (unsigned)((plane + X::B - 1) / X::B);
-    k_chain_x<T, L><<<tiles, X::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);
+    k_chain_x<T, L><<<tiles, X::NT, smem, st>>>(t2, G, ns, K, s, plane, tw, ext);
     return cudaGetLastError();
 }
 
 template <typename T>
 inline cudaError_t launch_chain_x(int L, cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
-                                  const cplx<T> *tw, cudaStream_t st) {
+                                  const cplx<T> *tw, const int *ext, cudaStream_t st) {
     switch (L) {
-        case 8: return launch_chain_x_L<T, 8>(t2, G, ns, K, s, plane, tw, st);
-        case 16: return launch_chain_x_L<T, 16>(t2, G, ns, K, s, plane, tw, st);
-        case 32: return launch_chain_x_L<T, 32>(t2, G, ns, K, s, plane, tw, st);
-        case 64: return launch_chain_x_L<T, 64>(t2, G, ns, K, s, plane, tw, st);
-        case 128: return launch_chain_x_L<T, 128>(t2, G, ns, K, s, plane, tw, st);
-        case 256: return launch_chain_x_L<T, 256>(t2, G, ns, K, s, plane, tw, st);
-        case 512: return launch_chain_x_L<T, 512>(t2, G, ns, K, s, plane, tw, st);
-        case 1024: return launch_chain_x_L<T, 1024>(t2, G, ns, K, s, plane, tw, st);
+        case 8: return launch_chain_x_L<T, 8>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 16: return launch_chain_x_L<T, 16>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 32: return launch_chain_x_L<T, 32>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 64: return launch_chain_x_L<T, 64>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 128: return launch_chain_x_L<T, 128>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 256: return launch_chain_x_L<T, 256>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 512: return launch_chain_x_L<T, 512>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 1024: return launch_chain_x_L<T, 1024>(t2, G, ns, K, s, plane, tw, ext, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -204,6 +204,13 @@ struct Engine : public hg_ctx {
         DBuf d_ent, d_start, d_scale;
         int nitems = 0;            // pair-sum work items (k_pair_dot_items)
         DBuf d_items, d_istart;
+        // shell-extent pruning of the chains' inverse passes: per shell j, e_j,a = max |n_a|
+        // of its modes (-1 for an empty shell); the B1 lines (j, cx, cy) and B2 lines (j, cx)
+        // inside those extents, as indices into the full layouts
+        std::vector<int> ext;       // [ns][3]
+        DBuf d_ext4, d_extx;        // int4 per shell (e_x, e_y, e_z, 0); e_x per shell
+        DBuf d_lines1, d_lines2;
+        long long nl1 = 0, nl2 = 0;
     } shells;
     // The catalogue the bispectrum and 3PCF read: the box density (kind 0) or the survey's
     // D - alpha R field (kind 1).  G fields are keyed by GK = (L, M): the Yhat_LM-weighted
@@ -1168,6 +1175,38 @@ struct Engine : public hg_ctx {
             HG_CK(S.d_istart.ensure(sizeof(int) * (S.ns + 1)));
             HG_CK(cudaMemcpy(S.d_istart.p, istart.data(), sizeof(int) * (S.ns + 1), cudaMemcpyHostToDevice));
         }
+        {  // shell extents and the pruned line lists
+            S.ext.assign(3 * S.ns, -1);
+            for (int i = 0; i < S.ns; i++)
+                for (int e = S.start[i]; e < S.start[i + 1]; e++) {
+                    const ShellEnt &q = S.ent[e];
+                    S.ext[3 * i] = std::max(S.ext[3 * i], std::abs(q.nx));
+                    S.ext[3 * i + 1] = std::max(S.ext[3 * i + 1], std::abs(q.ny));
+                    S.ext[3 * i + 2] = std::max(S.ext[3 * i + 2], std::abs(q.nz));
+                }
+            std::vector<int4> e4(S.ns);
+            std::vector<int> ex(S.ns), l1, l2;
+            for (int i = 0; i < S.ns; i++) {
+                e4[i] = make_int4(S.ext[3 * i], S.ext[3 * i + 1], S.ext[3 * i + 2], 0);
+                ex[i] = S.ext[3 * i];
+                for (int cx = S.s[0] - ex[i]; cx <= S.s[0] + ex[i]; cx++) {
+                    l2.push_back(i * S.K[0] + cx);
+                    for (int cy = S.s[1] - S.ext[3 * i + 1]; cy <= S.s[1] + S.ext[3 * i + 1]; cy++)
+                        l1.push_back((i * S.K[0] + cx) * S.K[1] + cy);
+                }
+            }
+            HG_REQUIRE((long long)S.ns * S.K[0] * S.K[1] < (1LL << 31), "too many chain lines");
+            S.nl1 = (long long)l1.size();
+            S.nl2 = (long long)l2.size();
+            HG_CK(S.d_ext4.ensure(sizeof(int4) * S.ns));
+            HG_CK(cudaMemcpy(S.d_ext4.p, e4.data(), sizeof(int4) * S.ns, cudaMemcpyHostToDevice));
+            HG_CK(S.d_extx.ensure(sizeof(int) * S.ns));
+            HG_CK(cudaMemcpy(S.d_extx.p, ex.data(), sizeof(int) * S.ns, cudaMemcpyHostToDevice));
+            HG_CK(S.d_lines1.ensure(sizeof(int) * std::max<size_t>(l1.size(), 1)));
+            if (!l1.empty()) HG_CK(cudaMemcpy(S.d_lines1.p, l1.data(), sizeof(int) * l1.size(), cudaMemcpyHostToDevice));
+            HG_CK(S.d_lines2.ensure(sizeof(int) * std::max<size_t>(l2.size(), 1)));
+            if (!l2.empty()) HG_CK(cudaMemcpy(S.d_lines2.p, l2.data(), sizeof(int) * l2.size(), cudaMemcpyHostToDevice));
+        }
         std::vector<double> inv(S.ns);
         for (int i = 0; i < S.ns; i++) inv[i] = S.nmode[i] ? 1.0 / double(S.nmode[i]) : 0.0;
         HG_CK(S.d_scale.ensure(sizeof(double) * S.ns));
@@ -1262,15 +1301,23 @@ struct Engine : public hg_ctx {
         ensure_chain_tmp((long long)ns * Kx * Ky * Mz, (long long)ns * Kx * My * Mz);
         const long long o1 = (long long)ns * Kx * Ky;
         const long long o2 = (long long)ns * Kx;
-        pass<+1>(Mz, LdCube<T>{dp<C>(Ac), Kz, Mz, S.s[2]}, StArr<T>{dp<C>(T1), Mz, 1}, o1, 1, "chain_z",
-                 double(o1) * (Kz + Mz) * sizeof(C));
-        pass<+1>(My, LdRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, StArr<T>{dp<C>(T2), My, Mz}, o2, Mz, "chain_y",
-                 double(o2) * (Ky + My) * Mz * sizeof(C));
+        // inverse z and y passes over the lines inside each shell's extents only
+        const ShellSet &SH = shells;
+        const int *lines1 = dp<int>(SH.d_lines1), *lines2 = dp<int>(SH.d_lines2);
+        const int4 *ext4 = dp<int4>(SH.d_ext4);
+        double in_rows_x = 0.0;  // input rows of the fused x pass, summed over shells
+        for (int j = 0; j < ns; j++) in_rows_x += double(2 * SH.ext[3 * j] + 1);
+        pass<+1>(Mz, LdCubeL<T>{dp<C>(Ac), Kz, Mz, S.s[2], lines1, ext4, Kx * Ky}, StArrL<T>{dp<C>(T1), Mz, 1, lines1},
+                 SH.nl1, 1, "chain_z", double(SH.nl1) * (Kz + Mz) * sizeof(C));
+        pass<+1>(My, LdRowsCompactL<T>{dp<C>(T1), Ky, My, S.s[1], Mz, lines2, ext4, Kx},
+                 StArrL<T>{dp<C>(T2), My, Mz, lines2}, SH.nl2, Mz, "chain_y",
+                 double(SH.nl2) * (Ky + My) * Mz * sizeof(C));
         const C *Gp = dp<C>(Gsrc);
         const long long plane = (long long)My * Mz;
-        const int var = chain_variant(Mx, Kx, S.s[0], ns, plane, Gp);  // before the timed launch
-        kb("chain_x_fused", double(ns) * 2.0 * Kx * My * Mz * sizeof(C) + double(Mx) * My * Mz * sizeof(C));
-        HG_CK(launch_chain_x_any(Mx, var, dp<C>(T2), Gp, ns, Kx, S.s[0], plane));
+        const int *extx = dp<int>(SH.d_extx);
+        const int var = chain_variant(Mx, Kx, S.s[0], ns, plane, Gp, extx);  // before the timed launch
+        kb("chain_x_fused", (in_rows_x + double(ns) * Kx) * My * Mz * sizeof(C) + double(Mx) * My * Mz * sizeof(C));
+        HG_CK(launch_chain_x_any(Mx, var, dp<C>(T2), Gp, ns, Kx, S.s[0], plane, extx));
         ke();
         pass<-1>(My, LdArr<T>{dp<C>(T2), My, Mz}, StRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, o2, Mz, "chain_y",
                  double(o2) * (Ky + My) * Mz * sizeof(C));
@@ -1278,14 +1325,15 @@ struct Engine : public hg_ctx {
                  double(o1) * (Kz + Mz) * sizeof(C));
     }
 
-    cudaError_t launch_chain_x_any(int Mx, int var, C *t2, const C *Gp, int ns, int Kx, int s0, long long plane) {
+    cudaError_t launch_chain_x_any(int Mx, int var, C *t2, const C *Gp, int ns, int Kx, int s0, long long plane,
+                                   const int *extx) {
         switch (Mx) {
-            case 256: return launch_chain_x_reg_L<T, 256>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
-            case 192: return launch_chain_x_reg_L<T, 192>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
-            case 128: return launch_chain_x_reg_L<T, 128>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
-            case 64: return launch_chain_x_reg_L<T, 64>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
-            case 32: return launch_chain_x_reg_L<T, 32>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
-            default: return launch_chain_x<T>(Mx, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), st);
+            case 256: return launch_chain_x_reg_L<T, 256>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), extx, st);
+            case 192: return launch_chain_x_reg_L<T, 192>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), extx, st);
+            case 128: return launch_chain_x_reg_L<T, 128>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), extx, st);
+            case 64: return launch_chain_x_reg_L<T, 64>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), extx, st);
+            case 32: return launch_chain_x_reg_L<T, 32>(var, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), extx, st);
+            default: return launch_chain_x<T>(Mx, t2, Gp, ns, Kx, s0, plane, twiddles(Mx), extx, st);
         }
     }
 
@@ -1301,7 +1349,7 @@ struct Engine : public hg_ctx {
     };
     std::map<int, Tuned> chain_tuned;  // by transform length
     DBuf tune_buf, tune_src;
-    int chain_variant(int Mx, int Kx, int s0, int ns, long long plane, const C *Gp) {
+    int chain_variant(int Mx, int Kx, int s0, int ns, long long plane, const C *Gp, const int *extx) {
         if (Mx != 32 && Mx != 64 && Mx != 128 && Mx != 192 && Mx != 256) return 0;
         auto it = chain_tuned.find(Mx);
         if (it != chain_tuned.end()) return it->second.variant;
@@ -1321,7 +1369,7 @@ struct Engine : public hg_ctx {
             for (int rep = 0; rep < 2; rep++) {
                 HG_CK(cudaMemcpyAsync(tune_buf.p, tune_src.p, bytes, cudaMemcpyDeviceToDevice, st));
                 HG_CK(cudaEventRecord(ev0, st));
-                HG_CK(launch_chain_x_any(Mx, v, dp<C>(tune_buf), Gp, nsh, Kx, s0, plane));
+                HG_CK(launch_chain_x_any(Mx, v, dp<C>(tune_buf), Gp, nsh, Kx, s0, plane, extx));
                 HG_CK(cudaEventRecord(ev1, st));
             }
             HG_CK(cudaEventSynchronize(ev1));

@@ -585,7 +585,7 @@ struct ChainCfg {
 template <typename T, int L, int B, bool GS, bool PF, int MINB>
 __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : ((sizeof(T) == 4) ? 2 : 1))
     k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
-                  const cplx<T> *__restrict__ tw) {
+                  const cplx<T> *__restrict__ tw, const int *__restrict__ ext) {
     using CF = ChainCfg<T, L, B, GS, PF>;
     using X = XchgLayout<L, true, B>;
     constexpr int R1 = X::R1, R2 = X::R2;
@@ -606,12 +606,14 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
         }
     }
     __syncthreads();
-    // the K kept rows of shell j into Pb (row c = n + s; rows of columns past the plane
-    // are zero-filled)
+    // shell j's input rows |n| <= e_j (the rows the pruned y pass wrote; ext null: all K)
+    auto ext_of = [&](int j) { return ext ? ext[j] : s; };
+    // those rows of shell j into Pb (row c = n + s; columns past the plane zero-filled)
     auto prefetch = [&](int j) {
         const cplx<T> *tj = t2 + (long long)j * K * plane;
-        for (int e = threadIdx.x; e < K * B; e += CF::NT) {
-            const int c = e / B, bb = e - c * B;
+        const int e0 = s - ext_of(j), nr = 2 * ext_of(j) + 1;
+        for (int e = threadIdx.x; e < nr * B; e += CF::NT) {
+            const int c = e0 + e / B, bb = e % B;
             const long long ii = (long long)blockIdx.x * B + bb;
             const bool in = ii < plane;
             cp_async_elem(Pb + c * B + bb, tj + (long long)c * plane + (in ? ii : 0), (int)sizeof(cplx<T>), in);
@@ -627,6 +629,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
     }
     for (int j = 0; j < ns; j++) {
         cplx<T> *tj = t2 + (long long)j * K * plane;
+        const int ej = ext_of(j);
         cplx<T> v[R1];
         if constexpr (PF) {
             asm volatile("cp.async.wait_group 0;\n" ::);
@@ -635,7 +638,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
             for (int n1 = 0; n1 < R1; n1++) {
                 const int x = R2 * n1 + t;
                 const int n = (x < L / 2) ? x : x - L;
-                v[n1] = (n >= -s && n <= s) ? Pb[(n + s) * B + b] : mk<T>(0, 0);
+                v[n1] = (n >= -ej && n <= ej) ? Pb[(n + s) * B + b] : mk<T>(0, 0);
             }
             __syncthreads();  // Pb is read: the next shell streams in while this one is transformed
             if (j + 1 < ns) prefetch(j + 1);
@@ -644,7 +647,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
             for (int n1 = 0; n1 < R1; n1++) {
                 const int x = R2 * n1 + t;
                 const int n = (x < L / 2) ? x : x - L;
-                v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
+                v[n1] = (ok && n >= -ej && n <= ej) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
             }
         }
         line_fft2<T, L, +1, true, B>(v, S, t, b, Tw);
@@ -756,7 +759,7 @@ __device__ __forceinline__ void line_fft192_12(cplx<T> *v, cplx<T> *S, int t, in
 template <typename T, int B, bool GS, int MINB>
 __global__ void __launch_bounds__(16 * B, MINB)
     k_chain_x_192(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
-                  const cplx<T> *__restrict__ tw) {
+                  const cplx<T> *__restrict__ tw, const int *__restrict__ ext) {
     constexpr int L = 192;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);  // [192][B]
@@ -776,12 +779,13 @@ __global__ void __launch_bounds__(16 * B, MINB)
     __syncthreads();
     for (int j = 0; j < ns; j++) {
         cplx<T> *tj = t2 + (long long)j * K * plane;
+        const int ej = ext ? ext[j] : s;  // shell j's input rows |n| <= e_j
         cplx<T> v[12];
 #pragma unroll
         for (int n1 = 0; n1 < 12; n1++) {
             const int x = 16 * n1 + t;
             const int n = (x < L / 2) ? x : x - L;
-            v[n1] = (ok && n >= -s && n <= s) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
+            v[n1] = (ok && n >= -ej && n <= ej) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
         }
         line_fft192_12<T, +1, B>(v, S, t, b, Tw);
 #pragma unroll
@@ -814,54 +818,54 @@ __global__ void __launch_bounds__(16 * B, MINB)
 
 template <typename T, int B, bool GS, int MINB>
 inline cudaError_t launch_chain_x_192(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
-                                      const cplx<T> *tw, cudaStream_t st) {
+                                      const cplx<T> *tw, const int *ext, cudaStream_t st) {
     const size_t smem = sizeof(cplx<T>) * (192 * B * (GS ? 2 : 1) + 192);
     cudaError_t e = cudaFuncSetAttribute(k_chain_x_192<T, B, GS, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned tiles = (unsigned)((plane + B - 1) / B);
-    k_chain_x_192<T, B, GS, MINB><<<tiles, 16 * B, smem, st>>>(t2, G, ns, K, s, plane, tw);
+    k_chain_x_192<T, B, GS, MINB><<<tiles, 16 * B, smem, st>>>(t2, G, ns, K, s, plane, tw, ext);
     return cudaGetLastError();
 }
 
 template <typename T, int L, int B, bool GS, bool PF, int MINB = 0>
 inline cudaError_t launch_chain_x_v(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
-                                    const cplx<T> *tw, cudaStream_t st) {
+                                    const cplx<T> *tw, const int *ext, cudaStream_t st) {
     using CF = ChainCfg<T, L, B, GS, PF>;
     const size_t smem = CF::smem(K);
     cudaError_t e = cudaFuncSetAttribute(k_chain_x_reg<T, L, B, GS, PF, MINB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned tiles = (unsigned)((plane + B - 1) / B);
-    k_chain_x_reg<T, L, B, GS, PF, MINB><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw);
+    k_chain_x_reg<T, L, B, GS, PF, MINB><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw, ext);
     return cudaGetLastError();
 }
 
 // variant v of kChainVariants
 template <typename T, int L>
 inline cudaError_t launch_chain_x_reg_L(int v, cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
-                                        const cplx<T> *tw, cudaStream_t st) {
+                                        const cplx<T> *tw, const int *ext, cudaStream_t st) {
     switch (v) {
-        case 1: return launch_chain_x_v<T, L, 16, false, true>(t2, G, ns, K, s, plane, tw, st);
-        case 2: return launch_chain_x_v<T, L, 16, false, false>(t2, G, ns, K, s, plane, tw, st);
-        case 3: return launch_chain_x_v<T, L, 8, true, true>(t2, G, ns, K, s, plane, tw, st);
-        case 4: return launch_chain_x_v<T, L, 8, false, false>(t2, G, ns, K, s, plane, tw, st);
-        case 5: return launch_chain_x_v<T, L, 16, false, false, 3>(t2, G, ns, K, s, plane, tw, st);
-        case 6: return launch_chain_x_v<T, L, 16, false, false, 4>(t2, G, ns, K, s, plane, tw, st);
-        case 7: return launch_chain_x_v<T, L, 8, false, false, 8>(t2, G, ns, K, s, plane, tw, st);
+        case 1: return launch_chain_x_v<T, L, 16, false, true>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 2: return launch_chain_x_v<T, L, 16, false, false>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 3: return launch_chain_x_v<T, L, 8, true, true>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 4: return launch_chain_x_v<T, L, 8, false, false>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 5: return launch_chain_x_v<T, L, 16, false, false, 3>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 6: return launch_chain_x_v<T, L, 16, false, false, 4>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 7: return launch_chain_x_v<T, L, 8, false, false, 8>(t2, G, ns, K, s, plane, tw, ext, st);
         case 8:
-            if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 4>(t2, G, ns, K, s, plane, tw, st);
+            if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 4>(t2, G, ns, K, s, plane, tw, ext, st);
             return cudaErrorInvalidValue;
         case 9:
-            if constexpr (L == 192) return launch_chain_x_192<T, 16, false, 2>(t2, G, ns, K, s, plane, tw, st);
+            if constexpr (L == 192) return launch_chain_x_192<T, 16, false, 2>(t2, G, ns, K, s, plane, tw, ext, st);
             return cudaErrorInvalidValue;
         case 10:
-            if constexpr (L == 192) return launch_chain_x_192<T, 8, true, 4>(t2, G, ns, K, s, plane, tw, st);
+            if constexpr (L == 192) return launch_chain_x_192<T, 8, true, 4>(t2, G, ns, K, s, plane, tw, ext, st);
             return cudaErrorInvalidValue;
         case 11:
-            if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 3>(t2, G, ns, K, s, plane, tw, st);
+            if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 3>(t2, G, ns, K, s, plane, tw, ext, st);
             return cudaErrorInvalidValue;
-        default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, st);
+        default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, ext, st);
     }
 }
 

@@ -38,7 +38,8 @@ def test_nonfinite_position_rejected_and_context_usable(form, bad):
         c.set_particles(0, d["pos"])
         pk2, nm2, norm2 = c.pk_box(0)
         bk2, sn2, _ = c.bk_box_multi(((0, 0, 0),))
-    np.testing.assert_array_equal(pk, pk2)
+    # P's bin sums add with FP64 atomics (last-bit order dependence); the signal is exact
+    assert relerr(pk, pk2) < 1e-14
     np.testing.assert_array_equal(nm, nm2)
     np.testing.assert_array_equal(bk, bk2)
 
@@ -90,9 +91,10 @@ def test_far_positions_are_dropped(assign):
             c.set_particles(0, pos)
             out[far] = (c.pk_box(0), c.bk_box_multi(((0, 0, 0),)))
     (pa, ba), (pb, bb) = out.values()
-    np.testing.assert_array_equal(pa[0], pb[0])
+    assert relerr(pa[0], pb[0]) < 1e-14
+    np.testing.assert_array_equal(pa[1], pb[1])
     np.testing.assert_array_equal(ba[0], bb[0])
-    np.testing.assert_array_equal(ba[1], bb[1])
+    assert relerr(ba[1], bb[1]) < 1e-12
 
 
 def test_far_positions_wrap_on_periodic_mesh():
@@ -109,7 +111,7 @@ def test_far_positions_wrap_on_periodic_mesh():
         with ctx_for(d, "fp64", "PCS") as c:
             c.set_particles(0, p)
             res.append(c.pk_box(0)[0])
-    np.testing.assert_array_equal(res[0], res[1])
+    assert relerr(res[0], res[1]) < 1e-14
 
 
 @pytest.mark.parametrize("form", ["fp64", "fp32"])
@@ -156,9 +158,9 @@ def test_batch_stops_at_failing_mock():
         bk0 = c.bk_box_multi(((0, 0, 0),))[0]
         c.set_particles(0, other)
         pko = c.pk_box(0)[0]
-    np.testing.assert_array_equal(r0["pk"][0], pk0)
+    assert relerr(r0["pk"][0], pk0) < 1e-14
     np.testing.assert_array_equal(r0["bk"], bk0)
-    np.testing.assert_array_equal(rest[0]["pk"][0], pko)
+    assert relerr(rest[0]["pk"][0], pko) < 1e-14
 
 
 def test_empty_catalogue_rejected():
