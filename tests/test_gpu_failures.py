@@ -78,15 +78,21 @@ def test_outside_box_matches_reference(form, assign):
 
 @pytest.mark.parametrize("assign", ["CIC", "TSC"])
 def test_far_positions_are_dropped(assign):
-    """Coordinates 10^12 box lengths away (beyond the int range of the anchor) give exactly
-    what coordinates 10^2 box lengths away give: no cell, the same particle count."""
+    """Coordinates 10^12 box lengths away on one axis (beyond the int range of the anchor)
+    give exactly what particles 100 box lengths away on every axis give -- a flat index far
+    past the mesh under the reference's rule, so no cell -- with the same particle count.
+    (100 box lengths on the z axis alone would not do: the flat-index rule carries z into
+    y and x, and such a particle lands in the mesh.)"""
     d = load_golden("box_bk.npz")
     L = float(d["boxsize"])
     out = {}
-    for far in (1e2 * L, 1e12 * L):
+    for far in (None, 1e12 * L):
         pos = d["pos"].copy()
-        pos[:6] = [[far, 10.0, 10.0], [-far, 10.0, 10.0], [10.0, far, 10.0], [10.0, -far, 10.0],
-                   [10.0, 10.0, far], [10.0, 10.0, -far]]
+        if far is None:
+            pos[:6] = 100.0 * L
+        else:
+            pos[:6] = [[far, 10.0, 10.0], [-far, 10.0, 10.0], [10.0, far, 10.0], [10.0, -far, 10.0],
+                       [10.0, 10.0, far], [10.0, 10.0, -far]]
         with ctx_for(d, "fp64", assign) as c:
             c.set_particles(0, pos)
             out[far] = (c.pk_box(0), c.bk_box_multi(((0, 0, 0),)))
