@@ -37,6 +37,8 @@ SYMBOLS = (
     "hg_reconstruct",
     "hg_pk_box_recon",
     "hg_xi_box_recon",
+    "hg_bk_box_recon_multi",
+    "hg_zeta_box_recon_multi",
     "hg_batch_run",
     "hg_batch_block_len",
     "hg_batch_done",
@@ -175,6 +177,10 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_pk_box_recon.restype = ctypes.c_int
     lib.hg_xi_box_recon.argtypes = [vp, i_, d_, c_dp, c_ip, c_dp]
     lib.hg_xi_box_recon.restype = ctypes.c_int
+    lib.hg_bk_box_recon_multi.argtypes = [vp, i_, c_ip, i_, d_, c_dp, c_dp, c_dp]
+    lib.hg_bk_box_recon_multi.restype = ctypes.c_int
+    lib.hg_zeta_box_recon_multi.argtypes = lib.hg_bk_box_recon_multi.argtypes
+    lib.hg_zeta_box_recon_multi.restype = ctypes.c_int
     lib.hg_batch_run.argtypes = [vp, ctypes.POINTER(HgMock), i_, i_, c_ip, i_, c_ip, i_, c_ip, c_dp]
     lib.hg_batch_run.restype = ctypes.c_int
     lib.hg_batch_block_len.argtypes = [vp, i_, i_, i_]

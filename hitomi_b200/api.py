@@ -296,19 +296,33 @@ class Context:
     def xi_window(self, ell: int, vsurvey: float):
         return self._xi(self._lib.hg_xi_window, int(ell), float(vsurvey))
 
-    def zeta_window_multi(self, multipoles, vsurvey: float, ith_rbin: int = -1):
-        """Window 3PCF multipoles of the randoms (slot 1): arrays [m][rows][n_rbin] and norm."""
-        nr = self.binning.n_rbin
-        rows = nr if ith_rbin < 0 else 1
+    def _one_scalar_three_point(self, fn, nbins, multipoles, ith, scalar):
+        rows = nbins if ith < 0 else 1
         m = len(multipoles)
         ells = np.array([v for mp in multipoles for v in mp], dtype=np.int32)
-        z = np.zeros(2 * m * rows * nr)
-        sn = np.zeros(2 * m * rows * nr)
+        z = np.zeros(2 * m * rows * nbins)
+        sn = np.zeros(2 * m * rows * nbins)
         norm = ctypes.c_double()
-        self._check(self._lib.hg_zeta_window_multi(self._h, m, ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                                   ith_rbin, float(vsurvey), _dp(z), _dp(sn), ctypes.byref(norm)))
-        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nr)
+        self._check(fn(self._h, m, ells.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ith, float(scalar), _dp(z),
+                       _dp(sn), ctypes.byref(norm)))
+        c = lambda v: (v[0::2] + 1j * v[1::2]).reshape(m, rows, nbins)
         return c(z), c(sn), norm.value
+
+    def zeta_window_multi(self, multipoles, vsurvey: float, ith_rbin: int = -1):
+        """Window 3PCF multipoles of the randoms (slot 1): arrays [m][rows][n_rbin] and norm."""
+        return self._one_scalar_three_point(self._lib.hg_zeta_window_multi, self.binning.n_rbin, multipoles,
+                                            ith_rbin, vsurvey)
+
+    def bk_box_recon_multi(self, multipoles, alpha: float, ith_kbin: int = -1):
+        """Reconstructed-box bispectrum multipoles of data (slot 0) and randoms (slot 1):
+        arrays [m][rows][n_kbin] and norm (V^2 / N_D^3)."""
+        return self._one_scalar_three_point(self._lib.hg_bk_box_recon_multi, self.binning.n_kbin, multipoles,
+                                            ith_kbin, alpha)
+
+    def zeta_box_recon_multi(self, multipoles, alpha: float, ith_rbin: int = -1):
+        """Reconstructed-box 3PCF multipoles: arrays [m][rows][n_rbin] and norm (V^2 / N_D^3)."""
+        return self._one_scalar_three_point(self._lib.hg_zeta_box_recon_multi, self.binning.n_rbin, multipoles,
+                                            ith_rbin, alpha)
 
     def reconstruct(self, b1_fid: float, RG: float, box: bool = False, alpha: float = 0.0, vsurvey: float = 0.0):
         """BAO reconstruction of the current data (slot 0) and randoms (slot 1): their shifted

@@ -276,6 +276,22 @@ int hg_xi_box_recon(hg_ctx *ctx, int ell, double alpha, double *xi_save, int *n_
     HG_GUARD(ctx, ctx->xi_box_recon(ell, alpha, xi_save, n_mode, norm));
 }
 
+int hg_bk_box_recon_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double alpha,
+                          double *bk_save, double *sn_save, double *norm) {
+    if (!bk_save || !sn_save || !ells || n_multipoles <= 0) return -1;
+    std::vector<MP> mps;
+    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
+    HG_GUARD(ctx, ctx->bk_box_recon_multi(mps, ith_kbin, alpha, bk_save, sn_save, norm));
+}
+
+int hg_zeta_box_recon_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double alpha,
+                            double *zeta_save, double *sn_save, double *norm) {
+    if (!zeta_save || !sn_save || !ells || n_multipoles <= 0) return -1;
+    std::vector<MP> mps;
+    for (int q = 0; q < n_multipoles; q++) mps.push_back(MP{ells[3 * q], ells[3 * q + 1], ells[3 * q + 2]});
+    HG_GUARD(ctx, ctx->zeta_box_recon_multi(mps, ith_rbin, alpha, zeta_save, sn_save, norm));
+}
+
 long long hg_batch_block_len(const hg_ctx *ctx, int n_pk, int n_bk, int n_zeta) {
     if (!ctx || n_pk < 0 || n_bk < 0 || n_zeta < 0) return -1;
     return hg::batch_block_len(ctx->cfg, n_pk, n_bk, n_zeta);

@@ -75,6 +75,10 @@ struct hg_ctx {
     virtual void reconstruct(int box, double b1, double RG, double alpha, double vs, double *posD, double *posR) = 0;
     virtual void pk_box_recon(int ell, double alpha, double *pk_save, int *n_mode, double *norm) = 0;
     virtual void xi_box_recon(int ell, double alpha, double *xi_save, int *n_mode, double *norm) = 0;
+    virtual void bk_box_recon_multi(const std::vector<hg::MP> &mps, int ith, double alpha, double *bk_save,
+                                    double *sn_save, double *norm) = 0;
+    virtual void zeta_box_recon_multi(const std::vector<hg::MP> &mps, int ith, double alpha, double *zeta_save,
+                                      double *sn_save, double *norm) = 0;
     virtual void batch_run(const hg_mock *mocks, int n_mocks, const std::vector<int> &pk_ells,
                            const std::vector<hg::MP> &bk, const std::vector<hg::MP> &zeta, double *out) = 0;
     virtual void xi_survey(int ell, bool window, double alpha, double vs, double *xi_save, int *n_mode,

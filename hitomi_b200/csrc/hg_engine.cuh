@@ -221,6 +221,10 @@ struct Engine : public hg_ctx {
     };
     using GK = std::pair<int, int>;
     using FQ = std::tuple<int, int, int, int>;  // chain family (l, m) with its G key (L, M)
+    // 0 box density; 1 survey D - alpha R; 2 randoms alone (window functions); 3 the
+    // reconstructed box, D - alpha R of two box catalogues with the line of sight along z
+    // (bispec.hpp:1426-1753): every particle's Yhat_LM(z) is 1 for M = 0 and 0 otherwise, so
+    // only M = 0 terms remain and every (L, 0) field is the (0, 0) one
     int src_kind = -1;
     double src_alpha = 0.0;
     SpecK dsrc{};
@@ -1744,6 +1748,13 @@ struct Engine : public hg_ctx {
         return out;
     }
 
+    // (m1, m2, M) terms over every M for the survey sources, M = 0 for the box ones (the
+    // reconstructed box included: its particles' Yhat_LM(z) vanish for M != 0)
+    bool all_M() const { return src_kind == 1 || src_kind == 2; }
+    // the G field of an (L, M) term: G_LM for the survey sources, the one G of the box
+    // (and of the reconstructed box, whose (L, 0) fields are all the (0, 0) one)
+    GK g_key(int L, int M) const { return all_M() ? GK{L, M} : GK{0, 0}; }
+
     static void check_multipoles(const std::vector<MP> &mps) {
         HG_REQUIRE(!mps.empty(), "no multipoles requested");
         for (const auto &mp : mps) {
@@ -1757,7 +1768,6 @@ struct Engine : public hg_ctx {
     // (bispec.hpp:1118-1170 box, 255-320 survey), [q][ns][ns] complex.  Chain families:
     // every self-paired family per G key, then a greedy cover of the remaining pairs.
     std::vector<std::vector<double>> bk_main(const std::vector<MP> &mps) {
-        const bool survey = (src_kind >= 1);
         prepare_shells();
         const int ns = shells.ns;
         const double dV = g.volume / double(g.ntot);
@@ -1765,10 +1775,10 @@ struct Engine : public hg_ctx {
         std::vector<std::vector<Combo3>> cmb;
         std::map<GK, std::set<std::pair<Fam, Fam>>> upairs;
         for (const auto &mp : mps) {
-            cmb.push_back(combos3(mp, survey));
+            cmb.push_back(combos3(mp, all_M()));
             for (const auto &c : cmb.back()) {
                 Fam a{mp.l1, c.m1}, b{mp.l2, c.m2};
-                GK gk = survey ? GK{mp.L, c.M} : GK{0, 0};
+                GK gk = g_key(mp.L, c.M);
                 upairs[gk].insert(b < a ? std::make_pair(b, a) : std::make_pair(a, b));
             }
         }
@@ -1800,7 +1810,7 @@ struct Engine : public hg_ctx {
         std::vector<std::vector<double>> B(mps.size(), std::vector<double>(2 * ns * ns, 0.0));
         for (size_t q = 0; q < mps.size(); q++)
             for (const auto &c : cmb[q]) {
-                GK gk = survey ? GK{mps[q].L, c.M} : GK{0, 0};
+                GK gk = g_key(mps[q].L, c.M);
                 std::vector<double> t = triple_sum(Fam{mps[q].l1, c.m1}, Fam{mps[q].l2, c.m2}, gk, chains);
                 for (int e = 0; e < 2 * ns * ns; e++) B[q][e] += c.w * (dV * red * t[e]);
             }
@@ -2402,7 +2412,6 @@ struct Engine : public hg_ctx {
     // zeta_raw = sum_(m1,m2,M) w i^(l1+l2) dV sum_x F1 F2 G_LM  (bispec.hpp:1354-1378 box,
     // 545-575 survey): [q][rows][ns] complex
     std::vector<std::vector<double>> zeta_main(const std::vector<MP> &mps, int ith) {
-        const bool survey = (src_kind >= 1);
         const int ns = cfg.n_rbin;
         const double dV = g.volume / double(g.ntot);
         const int rows = (ith < 0) ? ns : 1;
@@ -2410,8 +2419,8 @@ struct Engine : public hg_ctx {
         for (size_t q = 0; q < mps.size(); q++) {
             const MP &mp = mps[q];
             const int p4 = (mp.l1 + mp.l2) % 4;
-            for (const auto &c : combos3(mp, survey)) {
-                GK gk = survey ? GK{mp.L, c.M} : GK{0, 0};
+            for (const auto &c : combos3(mp, all_M())) {
+                GK gk = g_key(mp.L, c.M);
                 std::vector<double> t = zeta_pair(Fam{mp.l1, c.m1}, Fam{mp.l2, c.m2}, ith, gk);
                 for (size_t e = 0; e < (size_t)rows * ns; e++) {
                     double re = c.w * (dV * t[2 * e]), im = c.w * (dV * t[2 * e + 1]);
@@ -2711,6 +2720,10 @@ struct Engine : public hg_ctx {
     }
 
     SpecK sfield(int kind, int l, int m, double alpha) {
+        if (src_kind == 3) {  // line of sight z: Yhat_{l,0} = 1 per particle (see src_kind)
+            HG_REQUIRE(m == 0, "the reconstructed box has M = 0 fields only");
+            l = 0;
+        }
         if (alpha != sf_alpha) {
             sf_ok.clear();
             sf_alpha = alpha;
@@ -2796,6 +2809,10 @@ struct Engine : public hg_ctx {
     std::map<int, std::vector<double>> s3_cache;  // per L: [M + L] complex, for s3_alpha
     double s3_alpha = 0.0;
     std::array<double, 2> survey_s3(int L, int M, double alpha) {
+        if (src_kind == 3) {  // N_D - alpha^3 N_R (field.hpp:1242-1250): unit weights, Yhat_L0(z) = 1
+            HG_REQUIRE(M == 0, "the reconstructed box has M = 0 terms only");
+            return {double(slot[0].n) - alpha * alpha * alpha * double(slot[1].n), 0.0};
+        }
         if (alpha != s3_alpha) {
             s3_cache.clear();
             s3_alpha = alpha;
@@ -2909,7 +2926,7 @@ struct Engine : public hg_ctx {
                 for (const auto &mp : todo) {
                     if (mp.L != L) continue;
                     std::vector<Combo3> cs;
-                    for (const auto &c : combos3(mp, true))
+                    for (const auto &c : combos3(mp, all_M()))
                         if (c.M == M) cs.push_back(c);
                     if (!cs.empty()) hm.push_back({mp, cs});
                 }
@@ -2977,6 +2994,36 @@ struct Engine : public hg_ctx {
         require_survey(needs_los(mps));
         begin();
         set_source(1, alpha);
+        bk_two_catalogues(mps, ith, alpha, bk_save, sn_save);
+        if (norm) *norm = survey_bk_norm(vs);
+        end();
+    }
+
+    // calcBiSpectrumForBOXForReconstruction (bispec.hpp:1426-1753): the survey estimator's
+    // structure on the reconstructed box catalogues (source kind 3); norm V^2 / N_D^3
+    void bk_box_recon_multi(const std::vector<MP> &mps, int ith, double alpha, double *bk_save, double *sn_save,
+                            double *norm) override {
+        check_multipoles(mps);
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_kbin, "ith_kbin out of range");
+        require_box_recon();
+        begin();
+        set_source(3, alpha);
+        bk_two_catalogues(mps, ith, alpha, bk_save, sn_save);
+        if (norm) *norm = box_recon_norm();
+        end();
+    }
+    void require_box_recon() const {
+        HG_REQUIRE(slot[0].set && slot[1].set,
+                   "the reconstructed box needs data (slot 0) and randoms (slot 1): call hg_set_particles for both");
+    }
+    double box_recon_norm() const {
+        const double nd = double(slot[0].n);
+        return g.volume / nd / nd * (g.volume / nd);
+    }
+
+    // B and its shot noise of a two-catalogue source (survey, reconstructed box): S3 term,
+    // P terms, xi term (bispec.hpp:20-214, 1443-1616)
+    void bk_two_catalogues(const std::vector<MP> &mps, int ith, double alpha, double *bk_save, double *sn_save) {
         const int ns = cfg.n_kbin;
         std::vector<std::vector<double>> B = bk_main(mps);
         // shot noise (bispec.hpp:20-214): S3 term, P terms, xi term
@@ -2985,7 +3032,7 @@ struct Engine : public hg_ctx {
         std::vector<unsigned long long> nm;
         for (size_t q = 0; q < mps.size(); q++) {
             const MP &mp = mps[q];
-            for (const auto &c : combos3(mp, true)) {
+            for (const auto &c : combos3(mp, all_M())) {
                 const std::array<double, 2> S3 = survey_s3(mp.L, c.M, alpha);
                 if (mp.l1 == 0 && mp.l2 == 0)
                     for (int e = 0; e < ns * ns; e++) {
@@ -3029,7 +3076,24 @@ struct Engine : public hg_ctx {
                     sn_save[2 * o] = SN[q][2 * (i1 * ns + i2)];
                     sn_save[2 * o + 1] = SN[q][2 * (i1 * ns + i2) + 1];
                 }
-        if (norm) *norm = survey_bk_norm(vs);
+    }
+
+    // calcThreePointCorrelationFunctionForBOXForReconstruction (bispec.hpp:1755-1990): as
+    // the survey 3PCF on the reconstructed box catalogues (source kind 3); norm V^2 / N_D^3
+    void zeta_box_recon_multi(const std::vector<MP> &mps, int ith, double alpha, double *zeta_save,
+                              double *sn_save, double *norm) override {
+        check_multipoles(mps);
+        HG_REQUIRE(ith >= -1 && ith < cfg.n_rbin, "ith_rbin out of range");
+        require_box_recon();
+        begin();
+        zeta_geometry();
+        set_source(3, alpha);
+        std::vector<std::vector<double>> Z = zeta_main(mps, ith);
+        survey_histograms(mps);
+        std::vector<const double *> hs;
+        for (const auto &mp : mps) hs.push_back(dp<double>(*hist_sv[{mp.l1, mp.l2, mp.L}]));
+        zeta_finish(mps, ith, Z, hs, zeta_save, sn_save);
+        if (norm) *norm = box_recon_norm();
         end();
     }
 

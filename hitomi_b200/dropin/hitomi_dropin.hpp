@@ -21,6 +21,8 @@
 //   calcThreePointWindowCorrelationFunction  bispec.hpp:617-874
 //   calcPowerSpectrumForBOXForReconstruction      powerspec.hpp:396-457
 //   calcTwoPointFunctionForBOXForReconstruction   powerspec.hpp:459-520
+//   calcBiSpectrumForBOXForReconstruction         bispec.hpp:1426-1753
+//   calcThreePointCorrelationFunctionForBOXForReconstruction  bispec.hpp:1755-1990
 //   calcReconstructionParticles                   particle_reconstruction.hpp:12-208
 //   calcReconstructionParticlesForBOX             particle_reconstruction.hpp:210-402
 // (the last two in place of particle_reconstruction.hpp, which the program then does not
@@ -440,6 +442,35 @@ inline int calcTwoPointFunctionForBOXForReconstruction(ParticleGadgetClass &P_D,
     double norm;
     if (hg_xi_box_recon(ctx, param.ELL, alpha, dp(xi), nullptr, &norm)) return fail(ctx, "hg_xi_box_recon");
     return write_xi(param, "_recon", rbin, xi, norm);
+}
+
+inline int calcBiSpectrumForBOXForReconstruction(ParticleGadgetClass &P_D, ParticleGadgetClass &P_R,
+                                                 ParameterClass &param, double alpha, double *kbin) {
+    using namespace hitomi_dropin;
+    if (!triple_check(param)) return -1;
+    hg_ctx *ctx = context(param);
+    if (!ctx || set_box(ctx, P_D) || set_box_randoms(ctx, P_R)) return -1;
+    std::vector<std::complex<double>> bk(param.n_kbin), sn(param.n_kbin);
+    const int ells[3] = {param.ell1, param.ell2, param.ELL};
+    double norm;
+    if (hg_bk_box_recon_multi(ctx, 1, ells, param.ith_kbin, alpha, dp(bk), dp(sn), &norm))
+        return fail(ctx, "hg_bk_box_recon_multi");
+    return write_bk(param, "_recon", kbin, bk, sn, norm);
+}
+
+inline int calcThreePointCorrelationFunctionForBOXForReconstruction(ParticleGadgetClass &P_D, ParticleGadgetClass &P_R,
+                                                                    ParameterClass &param, double alpha,
+                                                                    double *rbin) {
+    using namespace hitomi_dropin;
+    if (!triple_check(param)) return -1;
+    hg_ctx *ctx = context(param);
+    if (!ctx || set_box(ctx, P_D) || set_box_randoms(ctx, P_R)) return -1;
+    std::vector<std::complex<double>> z(param.n_rbin), sn(param.n_rbin);
+    const int ells[3] = {param.ell1, param.ell2, param.ELL};
+    double norm;
+    if (hg_zeta_box_recon_multi(ctx, 1, ells, param.ith_rbin, alpha, dp(z), dp(sn), &norm))
+        return fail(ctx, "hg_zeta_box_recon_multi");
+    return write_zeta(param, "_recon", rbin, z, sn, norm);
 }
 
 #endif  // HITOMI_DROPIN_HPP

@@ -264,6 +264,24 @@ int hg_pk_box_recon(hg_ctx *ctx, int ell, double alpha, double *pk_save, int *n_
  * on dn = n_D - alpha n_R (weights 1) with shot noise N_D + alpha^2 N_R; *norm = V / N_D^2. */
 int hg_xi_box_recon(hg_ctx *ctx, int ell, double alpha, double *xi_save, int *n_mode, double *norm);
 
+/* Reconstructed periodic-box bispectrum multipoles.  Replaces
+ * calcBiSpectrumForBOXForReconstruction (bispec.hpp:1426-1753): the estimator of
+ * hg_bk_box_multi on dn = n_D - alpha n_R (data slot 0, randoms slot 1, weights 1), its shot
+ * noise from the fields dn and n_D + alpha^2 n_R with S3 = N_D - alpha^3 N_R
+ * (field.hpp:1242-1250); M = 0 terms only (global line of sight).  ells as
+ * hg_bk_box_multi (n_multipoles triples), ith_kbin one row or -1 for all; outputs
+ * [n_multipoles][rows][n_kbin] complex; *norm = V^2 / N_D^3.  Output file value =
+ * norm * (bk_save - sn_save) (bispec.hpp:1735-1748, file bk{l1}{l2}{L}_{ith}_recon.dat). */
+int hg_bk_box_recon_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin, double alpha,
+                          double *bk_save, double *sn_save, double *norm);
+
+/* Reconstructed periodic-box 3PCF multipoles.  Replaces
+ * calcThreePointCorrelationFunctionForBOXForReconstruction (bispec.hpp:1755-1990): as
+ * hg_bk_box_recon_multi for zeta (r bins, shot noise on the diagonal); *norm = V^2 / N_D^3;
+ * output file value = norm * Re(zeta_save - sn_save). */
+int hg_zeta_box_recon_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double alpha,
+                            double *zeta_save, double *sn_save, double *norm);
+
 /* ---- catalogue ingest (host side; the reference's readers, native and multi-threaded) */
 
 /* Gadget-2 snapshot header block: 256 bytes, the layout of ParticleGadgetClass::io_header

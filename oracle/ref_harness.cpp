@@ -352,7 +352,19 @@ int main(int argc, char **argv) {
         double alpha = double(P_D.n_tot) / double(P_R.n_tot);
         if (param.measure == "pk") rc = calcPowerSpectrumForBOXForReconstruction(P_D, P_R, param, alpha, kbin.data());
         else if (param.measure == "2PCF") rc = calcTwoPointFunctionForBOXForReconstruction(P_D, P_R, param, alpha, rbin.data());
-        else return fail("measure");
+        else if (param.measure == "bk") {  /* main_box.cpp:211-215, one ith_kbin row per run */
+            int lo = all_rows ? 0 : param.ith_kbin, hi = all_rows ? param.n_kbin : param.ith_kbin + 1;
+            for (int i = lo; i < hi && rc == 0; i++) {
+                param.ith_kbin = i;
+                rc = calcBiSpectrumForBOXForReconstruction(P_D, P_R, param, alpha, kbin.data());
+            }
+        } else if (param.measure == "3PCF") {  /* main_box.cpp:216-220 */
+            int lo = all_rows ? 0 : param.ith_rbin, hi = all_rows ? param.n_rbin : param.ith_rbin + 1;
+            for (int i = lo; i < hi && rc == 0; i++) {
+                param.ith_rbin = i;
+                rc = calcThreePointCorrelationFunctionForBOXForReconstruction(P_D, P_R, param, alpha, rbin.data());
+            }
+        } else return fail("measure");
     } else if (pos.size() == 2) {
         /* periodic box: main_box.cpp:96-228 (reader replaced, boxsize from param) */
         std::vector<double> a = read_f64(pos[1]);

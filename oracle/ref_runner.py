@@ -138,17 +138,17 @@ class RefRun:
         a = _read_cols(os.path.join(self.out, f"pk{ell}.dat"))
         return a[:, 0], a[:, 1] + 1j * a[:, 2]
 
-    def bk(self, l1: int, l2: int, L: int, n_rows: int):
+    def bk(self, l1: int, l2: int, L: int, n_rows: int, tag: str = ""):
         rows = []
         for i in range(n_rows):
-            a = _read_cols(os.path.join(self.out, f"bk{l1}{l2}{L}_{i:02d}.dat"))
+            a = _read_cols(os.path.join(self.out, f"bk{l1}{l2}{L}_{i:02d}{tag}.dat"))
             rows.append(a[:, 2] + 1j * a[:, 3])
         return np.array(rows)
 
-    def zeta(self, l1: int, l2: int, L: int, n_rows: int):
+    def zeta(self, l1: int, l2: int, L: int, n_rows: int, tag: str = ""):
         rows = []
         for i in range(n_rows):
-            a = _read_cols(os.path.join(self.out, f"zeta{l1}{l2}{L}_{i:02d}.dat"))
+            a = _read_cols(os.path.join(self.out, f"zeta{l1}{l2}{L}_{i:02d}{tag}.dat"))
             rows.append(a[:, 2])
         return np.array(rows)
 

@@ -341,7 +341,7 @@ def make_recon():
     """BAO reconstruction (particle_reconstruction.hpp:12-402) through the reference's drivers:
     the shifted positions and the reconstructed P_l, survey (main.cpp:215-225, then
     calcPowerSpectrum with the _recon file name) and box (main_box.cpp:134-152, then
-    calcPowerSpectrumForBOXForReconstruction)."""
+    calcPowerSpectrumForBOXForReconstruction, the bispectrum and the 3PCF)."""
     d = {}
     data, rand = survey_shell(3000, 60000, seed=16)
     bs = Binning(0.004, 0.048, 12, 100.0, 1500.0, 15)
@@ -368,6 +368,19 @@ def make_recon():
             a = ref_runner._read_cols(os.path.join(r.out, f"pk{ell}_recon.dat"))
             d[f"box_pk_{ell}"] = a[:, 1] + 1j * a[:, 2]
             d["box_recon_D"], d["box_recon_R"] = r.recon_positions()
+    # reconstructed-box bispectrum and 3PCF (bispec.hpp:1426-1990): a coarser binning so
+    # that the reference's per-row runs stay short
+    bb = Binning(0.02, 0.08, 4, 20.0, 140.0, 7)
+    d["box_bk_binning"] = binning_arr(bb)
+    for mp in ((0, 0, 0), (2, 0, 2)):
+        with ref_runner.RefRun() as r:
+            r.run("bk", pos, *mp, 32, 1000.0, bb, assign="TSC", randoms=rnd, recon=(1.5, 20.0, 32), box_recon=True)
+            d["box_bk_" + "".join(map(str, mp))] = r.bk(*mp, bb.n_kbin, tag="_recon")
+    for mp in ((0, 0, 0), (1, 1, 0)):
+        with ref_runner.RefRun() as r:
+            r.run("3PCF", pos, *mp, 32, 1000.0, bb, assign="TSC", randoms=rnd, recon=(1.5, 20.0, 32),
+                  box_recon=True)
+            d["box_zeta_" + "".join(map(str, mp))] = r.zeta(*mp, bb.n_rbin, tag="_recon")
     np.savez_compressed(os.path.join(HERE, "recon.npz"), **d)
 
 

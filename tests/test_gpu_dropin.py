@@ -140,7 +140,7 @@ def test_dropin_optional_keys():
 def test_dropin_reconstruction_files():
     """BAO reconstruction through the drop-in (hg_reconstruct on the n_mesh_recon mesh) and
     the estimators that follow it: the survey P with the _recon file name, the box
-    reconstructed P and 2PCF."""
+    reconstructed P, 2PCF, bispectrum and 3PCF."""
     g = load_golden("recon.npz")
     bs = binning_from(g["sv_binning"])
     n = compare_files(run_both("pk", g["sv_data"], (2, 0, 2), 64, 3500.0, bs, randoms=g["sv_rand"],
@@ -149,4 +149,8 @@ def test_dropin_reconstruction_files():
     for measure in ("pk", "2PCF"):
         n += compare_files(run_both(measure, g["box_pos"], (0, 0, 0), 32, 1000.0, bx, randoms=g["box_rand"],
                                     recon=(1.5, 20.0, 32), box_recon=True), rel=1e-7)
-    assert n > 20
+    bb = binning_from(g["box_bk_binning"])
+    for measure, mp in (("bk", (2, 0, 2)), ("3PCF", (1, 1, 0))):
+        n += compare_files(run_both(measure, g["box_pos"], mp, 32, 1000.0, bb, randoms=g["box_rand"],
+                                    recon=(1.5, 20.0, 32), box_recon=True, ith=1), rel=1e-7)
+    assert n > 30
