@@ -324,7 +324,8 @@ struct Engine : public hg_ctx {
     explicit Engine(const hg_config &c) {
         cfg = c;
         for (int a = 0; a < 3; a++) {
-            HG_REQUIRE(fft_supported_length(c.n_mesh[a]), "n_mesh must be a power of two in [8, 1024] on every axis");
+            HG_REQUIRE(fft_any_length(c.n_mesh[a]) && c.n_mesh[a] % 2 == 0,
+                       "n_mesh must be even, in [8, 2048] and a product of primes <= 31 on every axis");
             HG_REQUIRE(c.boxsize[a] > 0.0, "boxsize must be > 0");
             g.n[a] = c.n_mesh[a];
             g.L[a] = c.boxsize[a];
@@ -336,6 +337,7 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(c.n_rbin >= 2 && c.rmax > c.rmin && c.rmin > 0.0, "need n_rbin >= 2 and 0 < rmin < rmax");
         g.volume = c.boxsize[0] * c.boxsize[1] * c.boxsize[2];
         g.ntot = (long long)c.n_mesh[0] * c.n_mesh[1] * c.n_mesh[2];
+        choose_tiles();
         wpow = c.assign + 1;
         // tools.hpp:118-134
         double dk = (c.kmax - c.kmin) / double(c.n_kbin - 1);
@@ -636,6 +638,40 @@ struct Engine : public hg_ctx {
     }
 
     // ------------------------------------------------------------------ assignment
+    // Assignment tile extents: 8 x 16 x 32 cells (or the whole axis when shorter) where those
+    // divide the mesh; otherwise, per axis, divisors of n between 4 (the widest stencil)
+    // and 32, the combination with the most cells up to 4096 (the shared-memory tile).
+    int tile_t[3] = {8, 16, 32};
+    void choose_tiles() {
+        const int tdef[3] = {8, 16, 32};
+        bool plain = true;
+        for (int a = 0; a < 3; a++) plain = plain && g.n[a] % std::min(tdef[a], g.n[a]) == 0;
+        if (plain) {
+            for (int a = 0; a < 3; a++) tile_t[a] = std::min(tdef[a], g.n[a]);
+            return;
+        }
+        std::vector<int> dv[3];
+        for (int a = 0; a < 3; a++) {
+            for (int d = 4; d <= 32; d++)
+                if (g.n[a] % d == 0) dv[a].push_back(d);
+            HG_REQUIRE(!dv[a].empty(), "n_mesh: every axis needs a divisor between 4 and 32 (the assignment tiles)");
+        }
+        long long best = -1;
+        for (int x : dv[0])
+            for (int y : dv[1])
+                for (int z : dv[2]) {
+                    const long long v = (long long)x * y * z;
+                    // most cells, then the longest rows (z), then y
+                    const long long key = v * 4096 + z * 64 + y;
+                    if (v <= 4096 && key > best) {
+                        best = key;
+                        tile_t[0] = x;
+                        tile_t[1] = y;
+                        tile_t[2] = z;
+                    }
+                }
+        HG_REQUIRE(best >= 0, "n_mesh: no assignment tile of at most 4096 cells");
+    }
     AssignGeom make_geom(double shift) const {
         AssignGeom a;
         for (int q = 0; q < 3; q++) {
@@ -646,9 +682,8 @@ struct Engine : public hg_ctx {
         a.scheme = cfg.assign;
         a.periodic = (cfg.periodic || cfg.assign == HG_PCS || cfg.interlace) ? 1 : 0;
         a.shift = shift;
-        const int tdef[3] = {8, 16, 32};
         for (int q = 0; q < 3; q++) {
-            a.t[q] = std::min(tdef[q], g.n[q]);
+            a.t[q] = tile_t[q];
             a.nt[q] = g.n[q] / a.t[q];
         }
         a.factor = 1.0 / (g.volume / double(g.ntot));
@@ -1150,6 +1185,8 @@ struct Engine : public hg_ctx {
             int m = std::max(8, next_pow2(need));
             if (need > 128 && need <= 192) m = 192;  // 3 x 64: the register FFT's 24 x 8 split
             if (m >= g.n[a]) {
+                HG_REQUIRE(fft_supported_length(g.n[a]),
+                           "the bispectrum's shells reach the whole of a mesh axis that is not a power of two");
                 S.M[a] = g.n[a];
                 S.gs[a] = g.n[a] / 2;  // whole axis
             } else {
@@ -1492,6 +1529,9 @@ struct Engine : public hg_ctx {
     // ------------------------------------------------------------------ shot noise (xi)
     void build_orbits() {
         if (!orbit_lines.empty()) return;
+        HG_REQUIRE(fft_supported_length(g.n[2]),
+                   "the correlation-field histograms (2PCF, bispectrum and 3PCF shot noise) need a power-of-two "
+                   "n_mesh_z in [8, 1024]");
         const int nx = g.n[0], ny = g.n[1];
         const bool swap = (nx == ny);
         for (int wx = 0; wx <= nx / 2; wx++)

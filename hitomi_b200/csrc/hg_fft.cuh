@@ -18,6 +18,8 @@
 
 #include "hg_common.cuh"
 
+#include <algorithm>
+
 namespace hg {
 // one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
 // helpers of this header never collide at link time
@@ -274,6 +276,141 @@ inline cudaError_t launch_fft_pass(int L, LD ld, ST st, PassGeom g, const cplx<T
 
 inline bool fft_supported_length(int L) {
     return L >= 8 && L <= 1024 && (L & (L - 1)) == 0;
+}
+
+// ---------------------------------------------------------------- mixed-radix lengths
+// Lines whose length is not a power of two (the reference transforms any n_mesh with
+// FFTW, e.g. its survey meshes 250 x 460 x 260): a Stockham autosort transform over the
+// factors of L (4s, then 2, then odd primes up to HG_MAX_RADIX), computed output by output
+// between two shared-memory buffers.  Pass s with radix R after Ns = R_0 ... R_{s-1}: output
+// o = (j / Ns) Ns R + k + q Ns (k = j mod Ns, q < R) is
+//   sum_r in[j + r L / R] exp(DIR 2 pi i r (k + q Ns) / (Ns R)),
+// the twiddle and the R-point DFT in one sum (every exponent is a multiple of 1 / L, read
+// from the context's L-point table).  A pass costs L R complex products per line; the
+// supported meshes' lines keep R <= 23.
+#define HG_MAX_RADIX 31
+#define HG_MAX_STAGES 16
+struct MixedPlan {
+    int L, nst;
+    int R[HG_MAX_STAGES];
+};
+
+inline bool mixed_plan(int L, MixedPlan &p) {
+    if (L < 2 || L > 2048) return false;
+    p.L = L;
+    p.nst = 0;
+    int n = L;
+    auto push = [&](int r) {
+        if (p.nst >= HG_MAX_STAGES) return false;
+        p.R[p.nst++] = r;
+        n /= r;
+        return true;
+    };
+    while (n % 4 == 0)
+        if (!push(4)) return false;
+    while (n % 2 == 0)
+        if (!push(2)) return false;
+    for (int f = 3; n > 1 && f <= HG_MAX_RADIX; f += 2)
+        while (n % f == 0)
+            if (!push(f)) return false;
+    return n == 1;
+}
+
+template <typename T, int DIR, class LD, class ST>
+__global__ void __launch_bounds__(256) k_fft_pass_mixed(LD ld, ST st, PassGeom g, MixedPlan pl, int B,
+                                                        const cplx<T> *__restrict__ tw) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int L = pl.L;
+    cplx<T> *s0 = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *s1 = s0 + (size_t)B * L;
+    cplx<T> *tws = s1 + (size_t)B * L;
+    for (int e = threadIdx.x; e < L; e += blockDim.x) tws[e] = tw[e];
+    const bool contig = (g.n_inner == 1);
+    long long o0, i0;
+    if (contig) {
+        o0 = (long long)blockIdx.x * B;
+        i0 = 0;
+    } else {
+        const long long tiles_per_outer = (g.n_inner + B - 1) / B;
+        o0 = (long long)blockIdx.x / tiles_per_outer;
+        i0 = ((long long)blockIdx.x - o0 * tiles_per_outer) * B;
+    }
+    // element e of the tile: line b, position l (contiguous axis: whole lines; strided axis:
+    // B adjacent columns, so consecutive threads read consecutive addresses)
+    auto at = [&](int e, int &b, int &l, long long &o, long long &i) {
+        if (contig) {
+            b = e / L;
+            l = e - b * L;
+            o = o0 + b;
+            i = 0;
+        } else {
+            l = e / B;
+            b = e - l * B;
+            o = o0;
+            i = i0 + b;
+        }
+        return contig ? (o < g.n_outer) : (i < g.n_inner);
+    };
+    for (int e = threadIdx.x; e < B * L; e += blockDim.x) {
+        int b, l;
+        long long o, i;
+        const bool ok = at(e, b, l, o, i);
+        s0[(size_t)b * L + l] = ok ? ld(o, l, i) : mk<T>(0, 0);
+    }
+    __syncthreads();
+    cplx<T> *cur = s0, *nxt = s1;
+    int Ns = 1;
+    for (int sidx = 0; sidx < pl.nst; sidx++) {
+        const int R = pl.R[sidx], LR = L / R, NsR = Ns * R, step = L / NsR;
+        for (int e = threadIdx.x; e < B * L; e += blockDim.x) {
+            const int b = e / L, o = e - b * L;
+            const int blk = o / NsR, rem = o - blk * NsR, q = rem / Ns, k = rem - q * Ns;
+            const int j = blk * Ns + k, m = (k + q * Ns) * step;
+            const cplx<T> *line = cur + (size_t)b * L;
+            cplx<T> acc = line[j];
+            int ex = 0;
+            for (int r = 1; r < R; r++) {
+                ex += m;
+                if (ex >= L) ex -= L;
+                acc = acc + mul_tw<T, DIR>(line[j + r * LR], tws[ex]);
+            }
+            nxt[(size_t)b * L + o] = acc;
+        }
+        __syncthreads();
+        cplx<T> *t = cur;
+        cur = nxt;
+        nxt = t;
+        Ns = NsR;
+    }
+    for (int e = threadIdx.x; e < B * L; e += blockDim.x) {
+        int b, l;
+        long long o, i;
+        if (at(e, b, l, o, i)) st(o, l, i, cur[(size_t)b * L + l]);
+    }
+}
+
+template <typename T, int DIR, class LD, class ST>
+inline cudaError_t launch_fft_mixed(int L, LD ld, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
+    MixedPlan pl;
+    if (!mixed_plan(L, pl)) return cudaErrorInvalidValue;
+    // B lines per CTA: two line buffers and the twiddles within 96 KB
+    const int per = (int)((96 * 1024) / sizeof(cplx<T>));
+    const int B = std::max(1, std::min(64, (per - L) / (2 * L)));
+    const size_t smem = ((size_t)2 * B * L + L) * sizeof(cplx<T>);
+    auto kern = k_fft_pass_mixed<T, DIR, LD, ST>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const long long tiles = (g.n_inner == 1) ? (g.n_outer + B - 1) / B : g.n_outer * ((g.n_inner + B - 1) / B);
+    if (tiles <= 0) return cudaSuccess;
+    kern<<<(unsigned)tiles, 256, smem, stream>>>(ld, st, g, pl, B, tw);
+    return cudaGetLastError();
+}
+
+// Every length a pass accepts: the power-of-two register and Stockham kernels, and the
+// mixed-radix kernel for lengths whose prime factors are at most HG_MAX_RADIX.
+inline bool fft_any_length(int L) {
+    MixedPlan pl;
+    return fft_supported_length(L) || (L >= 8 && mixed_plan(L, pl));
 }
 
 }  // namespace HG_TU_NS

@@ -522,7 +522,8 @@ inline cudaError_t launch_fft2_L(LD ld, ST st, PassGeom g, const cplx<T> *tw, cu
     return cudaGetLastError();
 }
 
-// Any supported length: two-level register FFT up to 256, Stockham beyond.
+// Any supported length: the two-level register FFT for its lengths, the Stockham pass for
+// other powers of two, the mixed-radix pass for the rest.
 template <typename T, int DIR, class LD, class ST>
 inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
     switch (L) {
@@ -535,7 +536,9 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
         case 256: return launch_fft2_L<T, 256, DIR>(ld, st, g, tw, stream);
         case 512: return launch_fft2_L<T, 512, DIR>(ld, st, g, tw, stream);
         case 1024: return launch_fft2_L<T, 1024, DIR>(ld, st, g, tw, stream);
-        default: return launch_fft_pass<T, DIR>(L, ld, st, g, tw, stream);
+        default:
+            if (fft_supported_length(L)) return launch_fft_pass<T, DIR>(L, ld, st, g, tw, stream);
+            return launch_fft_mixed<T, DIR>(L, ld, st, g, tw, stream);
     }
 }
 

@@ -44,7 +44,8 @@ typedef struct hg_ctx hg_ctx;
  * (parameter.hpp:12-49).  kbin / rbin follow ToolClass::setKbin / setRbin
  * (tools.hpp:118-134): kbin[i] = kmin + i (kmax - kmin)/(n_kbin - 1). */
 typedef struct hg_config {
-    int n_mesh[3];      /* n_mesh_x/y/z; powers of two in [8, 1024] */
+    int n_mesh[3];      /* n_mesh_x/y/z: even, 8..2048, prime factors <= 31 (the 2PCF and the
+                           bispectrum / 3PCF shot noise: a power-of-two n_mesh_z <= 1024) */
     double boxsize[3];  /* boxsize_x/y/z */
     int assign;         /* HG_NGP / HG_CIC / HG_TSC / HG_PCS  (parameter "assignment") */
     int interlace;      /* 0/1, project extension (reference has no interlacing) */

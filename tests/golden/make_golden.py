@@ -16,6 +16,7 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --recon  (only recon.npz: BAO reconstruction)
     python tests/golden/make_golden.py --outside (only box_outside.npz: particles outside the box)
     python tests/golden/make_golden.py --long   (only box_long_axes.npz: 1024-point axes)
+    python tests/golden/make_golden.py --mixed  (only mixed_meshes.npz: non-power-of-two meshes)
     python tests/golden/make_golden.py --configs (only box_config_sizes.npz: 128^3 and 512^3)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
@@ -337,6 +338,43 @@ def make_long_axes():
     np.savez_compressed(os.path.join(HERE, "box_long_axes.npz"), **d)
 
 
+def make_mixed_meshes():
+    """Meshes that are not powers of two, with unequal cell sizes (the reference transforms
+    any n_mesh, e.g. its survey meshes 250 x 460 x 260): box P_l on a [60, 36, 50] mesh of a
+    [1000, 800, 900] box; survey scalars and P_l on [50, 92, 52] (factors 2, 5, 23, 13);
+    the survey reconstruction on a [30, 46, 26] mesh followed by P_l."""
+    d = {}
+    pos = lognormal_box(15000, 1000.0, ngrid=32, seed=23, exact_n=15000)
+    pos = pos * np.array([1.0, 0.8, 0.9])
+    bb = Binning(0.01, 0.13, 7, 4.0, 156.0, 20)
+    nmb, bsb = [60, 36, 50], [1000.0, 800.0, 900.0]
+    d.update(box_pos=pos, box_n_mesh=np.array(nmb), box_boxsize=np.array(bsb), box_binning=binning_arr(bb))
+    for assign in ("TSC", "CIC"):
+        for ell in (0, 2):
+            with ref_runner.RefRun() as r:
+                r.run("pk", pos, ell, 0, ell, nmb, bsb, bb, assign=assign)
+                d[f"box_pk_{assign}_{ell}"] = r.pk(ell)[1]
+    data, rand = survey_shell(3000, 60000, seed=24)
+    bs = Binning(0.004, 0.048, 12, 20.0, 140.0, 7)
+    nms = [50, 92, 52]
+    d.update(sv_data=data, sv_rand=rand, sv_n_mesh=np.array(nms), sv_boxsize=3500.0, sv_binning=binning_arr(bs))
+    for ell in (0, 2):
+        with ref_runner.RefRun() as r:
+            r.run("pk", data, ell, 0, ell, nms, 3500.0, bs, assign="TSC", randoms=rand)
+            d[f"sv_pk_{ell}"] = r.pk(ell)[1]
+            sc = r.survey_scalars()
+    for k, v in sc.items():
+        d[f"sv_scalars_{k}"] = v
+    nrec = [30, 46, 26]
+    d["sv_n_mesh_recon"] = np.array(nrec)
+    with ref_runner.RefRun() as r:
+        r.run("pk", data, 0, 0, 0, nms, 3500.0, bs, assign="TSC", randoms=rand, recon=(2.0, 40.0, nrec))
+        a = ref_runner._read_cols(os.path.join(r.out, "pk0_recon.dat"))
+        d["sv_recon_pk_0"] = a[:, 1] + 1j * a[:, 2]
+        d["sv_recon_D"], d["sv_recon_R"] = r.recon_positions()
+    np.savez_compressed(os.path.join(HERE, "mixed_meshes.npz"), **d)
+
+
 def make_recon():
     """BAO reconstruction (particle_reconstruction.hpp:12-402) through the reference's drivers:
     the shifted positions and the reconstructed P_l, survey (main.cpp:215-225, then
@@ -430,11 +468,13 @@ def make_config_sizes():
 
 
 def main():
-    if "--outside" in sys.argv or "--long" in sys.argv:
+    if "--outside" in sys.argv or "--long" in sys.argv or "--mixed" in sys.argv:
         if "--outside" in sys.argv:
             make_outside()
         if "--long" in sys.argv:
             make_long_axes()
+        if "--mixed" in sys.argv:
+            make_mixed_meshes()
         print("fixtures written")
         return
     if "--recon" in sys.argv:
@@ -529,6 +569,7 @@ def main():
     make_bk_256()
     make_outside()
     make_long_axes()
+    make_mixed_meshes()
     print("fixtures written")
 
 

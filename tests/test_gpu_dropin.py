@@ -119,6 +119,9 @@ def test_dropin_survey_files():
     n += compare_files(run_both("pk", data, (2, 0, 2), 64, 3500.0, bs, randoms=rand))
     n += compare_files(run_both("2PCF", data, (2, 0, 2), 64, 3500.0, bs, randoms=rand))
     n += compare_files(run_both("window2PCF", data, (2, 0, 2), 64, 3500.0, bs, randoms=rand))
+    m = load_golden("mixed_meshes.npz")  # a survey mesh that is not a power of two
+    n += compare_files(run_both("pk", m["sv_data"], (2, 0, 2), [int(v) for v in m["sv_n_mesh"]], 3500.0,
+                                binning_from(m["sv_binning"]), randoms=m["sv_rand"]))
     b3 = binning_from(g["w3_binning"])
     d3, r3 = g["w3_data"], g["w3_rand"]
     n += compare_files(run_both("bk", d3, (1, 1, 0), 32, 3500.0, b3, randoms=r3, ith=1))

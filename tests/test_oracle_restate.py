@@ -108,3 +108,16 @@ def test_restated_outside_box_matches_reference(assign):
         assert relerr(norm * pk, d[f"pk_{assign}_{ell}"], 1e-12) < 1e-10
     bk, sn, norm = R.bk_box(d["pos"], int(d["n_mesh"]), float(d["boxsize"]), kb, 0, 0, 0, R.SCHEMES[assign])
     assert relerr(norm * (bk - sn), d[f"bk_{assign}_000"], 1e-12) < 1e-10
+
+
+@pytest.mark.parametrize("assign", ["TSC", "CIC"])
+def test_restated_pk_mixed_mesh_matches_reference(assign):
+    """A [60, 36, 50] mesh of a [1000, 800, 900] box: lengths that are not powers of two and
+    unequal cells (numpy's FFT takes any length, as FFTW does for the reference)."""
+    d = load_golden("mixed_meshes.npz")
+    kb = kbins(d["box_binning"])
+    nm = [int(v) for v in d["box_n_mesh"]]
+    bs = [float(v) for v in d["box_boxsize"]]
+    for ell in (0, 2):
+        pk, nmode, norm = R.pk_box(d["box_pos"], nm, bs, kb, ell, R.SCHEMES[assign])
+        assert relerr(norm * pk, d[f"box_pk_{assign}_{ell}"], 1e-12) < 1e-10, ell
