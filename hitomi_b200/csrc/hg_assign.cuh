@@ -40,6 +40,7 @@ struct AssignGeom {
     double factor;      // 1/dV (field.hpp:76-77), used for the FP64 in-bounds mass
     double acc_factor;  // factor applied in the mesh accumulation (1/dV, or 1 for a mass mesh)
     float fix_bound;    // bound on |w acc_factor prod(w_axis)| per record (fixed-point accumulation)
+    double far[3];      // 2^30 L / n: coordinates at least this far from 0 are "far" (far_reduce)
 };
 
 __host__ __device__ __forceinline__ int stencil_width(int scheme) { return scheme + 1; }
@@ -367,7 +368,7 @@ struct Defer {
 __device__ __forceinline__ bool far_reduce(const AssignGeom &g, double pos[3]) {
     bool drop = false;
     for (int a = 0; a < 3; a++) {
-        if (fabs(pos[a] * double(g.n[a]) / g.L[a]) < 0x1p30) continue;
+        if (fabs(pos[a]) < g.far[a]) continue;  // (the threshold's rounding is immaterial at 2^30 cells)
         // separately rounded operations (no fused multiply-add): x - L floor(x / L)
         if (g.periodic) pos[a] = __dsub_rn(pos[a], __dmul_rn(g.L[a], floor(__ddiv_rn(pos[a], g.L[a]))));
         else drop = true;

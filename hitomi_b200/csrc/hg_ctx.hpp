@@ -10,6 +10,7 @@
 
 #include "hitomi_gpu.h"
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -39,6 +40,7 @@ struct MemBudget {
     size_t limit = 0;
     size_t used = 0;
     bool hit = false;
+    std::mutex m;  // a context's two engines may allocate from two host threads at once
 };
 // the budget of the API call running on this thread (null outside API calls)
 MemBudget *&current_budget();

@@ -65,7 +65,10 @@ struct DBuf {
     ~DBuf() { release(); }
     void release() {
         if (p) cudaFree(p);
-        if (p && owner) owner->used -= n;
+        if (p && owner) {
+            std::lock_guard<std::mutex> lk(owner->m);
+            owner->used -= n;
+        }
         p = nullptr;
         n = 0;
         owner = nullptr;
@@ -76,18 +79,25 @@ struct DBuf {
         release();
         const size_t want = bytes ? bytes : 16;
         MemBudget *b = current_budget();
-        if (b && b->limit && b->used + want > b->limit) {
-            b->hit = true;
-            return cudaErrorMemoryAllocation;
+        if (b) {  // reserve first, so two threads of one context cannot both pass the limit
+            std::lock_guard<std::mutex> lk(b->m);
+            if (b->limit && b->used + want > b->limit) {
+                b->hit = true;
+                return cudaErrorMemoryAllocation;
+            }
+            b->used += want;
         }
         cudaError_t e = cudaMalloc(&p, want);
         if (e != cudaSuccess) {
             p = nullptr;
+            if (b) {
+                std::lock_guard<std::mutex> lk(b->m);
+                b->used -= want;
+            }
             return e;
         }
         n = want;
         owner = b;
-        if (b) b->used += want;
         return e;
     }
 };
@@ -685,6 +695,7 @@ struct Engine : public hg_ctx {
         for (int q = 0; q < 3; q++) {
             a.t[q] = tile_t[q];
             a.nt[q] = g.n[q] / a.t[q];
+            a.far[q] = 0x1p30 * g.L[q] / double(g.n[q]);
         }
         a.factor = 1.0 / (g.volume / double(g.ntot));
         // FP64 form: the reference's density rho = sum w (1/dV) prod(w_axis).  FP32 form: the

@@ -564,8 +564,9 @@ constexpr ChainVariant kChainVariants[] = {
     {16, true, true, 0, false},  {16, false, true, 0, false},  {16, false, false, 0, false},
     {8, true, true, 0, false},   {8, false, false, 0, false},  {16, false, false, 3, false},
     {16, false, false, 4, false}, {8, false, false, 8, false}, {8, false, false, 4, true},
-    {16, false, false, 2, true},  {8, true, false, 4, true},   {8, false, false, 3, true}};
-constexpr int kNumChainVariants = 12;
+    {16, false, false, 2, true},  {8, true, false, 4, true},   {8, false, false, 3, true},
+    {8, false, true, 0, false}};
+constexpr int kNumChainVariants = 13;
 
 template <typename T, int L, int B, bool GS, bool PF>
 struct ChainCfg {
@@ -868,12 +869,13 @@ inline cudaError_t launch_chain_x_reg_L(int v, cplx<T> *t2, const cplx<T> *G, in
         case 11:
             if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 3>(t2, G, ns, K, s, plane, tw, ext, st);
             return cudaErrorInvalidValue;
+        case 12: return launch_chain_x_v<T, L, 8, false, true>(t2, G, ns, K, s, plane, tw, ext, st);
         default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, ext, st);
     }
 }
 
 // whether variant v exists for line length L (8 .. 11: the 12-values-per-thread 192 kernel)
-inline bool chain_variant_exists(int L, int v) { return v < 8 || L == 192; }
+inline bool chain_variant_exists(int L, int v) { return v < 8 || v > 11 || L == 192; }
 
 }  // namespace HG_TU_NS
 }  // namespace hg
