@@ -267,9 +267,15 @@ template <typename T, int L, bool COLS>
 struct Fft2Cfg {
     static constexpr int R2 = Split<L>::R2;
     // lines per CTA: columns (strided axes) or whole lines (contiguous axis); lengths
-    // >= 512 hold 32 values per thread, so their CTAs are capped at 256 threads
+    // >= 512 hold 32 values per thread, so their CTAs are capped at 256 threads.  FP64 rows
+    // shorter than 512 take half as many lines (128 threads): a 192-point FP64 row tile of 32
+    // lines needs 114 KB of shared memory, so one CTA (8 warps) filled an SM; 16 lines fit
+    // three (chain z passes 1.01 -> 0.85 ms per mock).  At 512 points, halved row tiles
+    // together with 4-column pipelined tiles made the density transform slower (1.85 ->
+    // 2.27 ms), so those keep 256 threads.
+    static constexpr int RB = (sizeof(T) == 8 && L < 512 ? 128 : 256) / R2;
     static constexpr int B = COLS ? ((L >= 512) ? 256 / R2 : ((sizeof(T) == 4) ? 32 : 16))
-                                  : (256 / R2 > 64 ? 64 : 256 / R2);
+                                  : (RB > 64 ? 64 : (RB < 1 ? 1 : RB));
     static constexpr int NT = R2 * B;
 };
 
@@ -331,7 +337,8 @@ template <typename T, int L>
 struct PipeCfg {
     static constexpr int R2 = Split<L>::R2;
     // columns per tile: the double buffer of FP64 1024-point tiles takes 4 columns to stay
-    // within the 227 KB a CTA may hold
+    // within the 227 KB a CTA may hold (at 512 points 4 columns, three CTAs per SM instead of
+    // one, measured slower together with halved 512-point row tiles)
     static constexpr int B = (L >= 1024 && sizeof(T) == 8) ? 4 : ((L >= 256) ? 8 : 16);
     static constexpr int NT = R2 * B;
     // double buffer, then the L twiddles (staged once per persistent CTA)
