@@ -107,14 +107,25 @@ class HgConfig(ctypes.Structure):
 
 
 _lib = None
+_lib_check = None
+# the check build (device-side bounds checks, -DHG_CHECK): python hitomi_b200/build.py --check
+LIB_CHECK_PATH = os.path.join(os.path.dirname(LIB_PATH), "libhitomi_b200_check.so")
 
 
-def load(path: str | None = None) -> ctypes.CDLL:
-    """Load the library once.  Raises OSError if it has not been built."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    p = path or LIB_PATH
+def load(path: str | None = None, check: bool = False) -> ctypes.CDLL:
+    """Load the library once (check=True: the check build, a separate handle).  Raises
+    OSError if it has not been built."""
+    global _lib, _lib_check
+    if check:
+        if _lib_check is None:
+            _lib_check = _declare(LIB_CHECK_PATH)
+        return _lib_check
+    if _lib is None:
+        _lib = _declare(path or LIB_PATH)
+    return _lib
+
+
+def _declare(p: str) -> ctypes.CDLL:
     if not os.path.exists(p):
         raise OSError(f"hitomi_b200 CUDA library not built: {p} is missing (run python hitomi_b200/build.py)")
     lib = ctypes.CDLL(p)
@@ -203,5 +214,4 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.hg_pk_box_spectrum_static.restype = ctypes.c_int
     lib.hg_last_timing.argtypes = [vp, c_dp, ctypes.POINTER(ctypes.c_longlong)]
     lib.hg_last_timing.restype = ctypes.c_int
-    _lib = lib
     return lib

@@ -76,8 +76,11 @@ def _dp(a: np.ndarray):
 
 class Context:
     def __init__(self, n_mesh, boxsize, binning: Binning, assign: str = "TSC", precision: str = "fp64",
-                 periodic: bool = False, interlace: bool = False, device: int = 0, fp64_stages=()):
-        self._lib = _lib.load()
+                 periodic: bool = False, interlace: bool = False, device: int = 0, fp64_stages=(),
+                 check_build: bool = False):
+        """check_build: run on the check library (device-side bounds checks at the
+        index-sensitive accesses; a failed check fails the call)."""
+        self._lib = _lib.load(check=check_build)
         cfg = _lib.HgConfig()
         nm = [int(n_mesh)] * 3 if np.isscalar(n_mesh) else [int(v) for v in n_mesh]
         bs = [float(boxsize)] * 3 if np.isscalar(boxsize) else [float(v) for v in boxsize]

@@ -12,6 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libhitomi_b200.so")
+# the check build: device-side bounds checks at the index-sensitive accesses (HG_CHECK)
+LIB_CHECK = os.path.join(HERE, "libhitomi_b200_check.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in
            ("hg_engine_fp32.cu", "hg_engine_fp64.cu", "hg_api.cu", "hg_static.cu", "hg_io.cpp")]
 OBJDIR = os.path.join(HERE, "_build")
@@ -27,41 +29,45 @@ def nvcc() -> str:
     return cand if os.path.exists(cand) else "nvcc"
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+def up_to_date(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(f) <= t for f in SOURCES + HEADERS)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, check: bool = False) -> str:
     """Compile each translation unit to an object (in parallel: the two engine precisions
-    are the long ones), then link the shared library."""
-    if not force and up_to_date():
-        return LIB
-    os.makedirs(OBJDIR, exist_ok=True)
+    are the long ones), then link the shared library.  check=True builds the check library
+    (libhitomi_b200_check.so: -DHG_CHECK, objects in their own folder)."""
+    lib = LIB_CHECK if check else LIB
+    if not force and up_to_date(lib):
+        return lib
+    objdir = os.path.join(OBJDIR, "check") if check else OBJDIR
+    os.makedirs(objdir, exist_ok=True)
     common = [
         "-gencode", "arch=compute_100a,code=sm_100a",
         "-O3", "-lineinfo", "-std=c++17",
         "-Xcompiler", "-fPIC",
         "-I", os.path.join(ROOT, "include"),
     ]
+    if check:
+        common.append("-DHG_CHECK")
     if verbose:
         common.append("-Xptxas=-v")
     objs, procs = [], []
     for src in SOURCES:
-        obj = os.path.join(OBJDIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+        obj = os.path.join(objdir, os.path.splitext(os.path.basename(src))[0] + ".o")
         objs.append(obj)
         procs.append(subprocess.Popen([nvcc()] + common + ["--split-compile=4", "-c", src, "-o", obj]))
     bad = [src for src, p in zip(SOURCES, procs) if p.wait() != 0]
     if bad:
         raise subprocess.CalledProcessError(1, "nvcc " + " ".join(os.path.basename(b) for b in bad))
     subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
-                    "-o", LIB + ".tmp"] + objs, check=True)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+                    "-o", lib + ".tmp"] + objs, check=True)
+    os.replace(lib + ".tmp", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
-    print(LIB)
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv, check="--check" in sys.argv))

@@ -555,7 +555,8 @@ __global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom 
             for (int q = 0; q < 8; q++) {
                 if (q < maxnt && tq[q] >= 0) {
                     const unsigned base = __shfl_sync(gq[q], bq[q], __ffs(gq[q]) - 1);
-                    rec[off[tq[q]] + base + __popc(gq[q] & lt)] = r;
+                    const unsigned ri = off[tq[q]] + base + __popc(gq[q] & lt);
+                    if (HG_IN_BOUNDS(ri < off[tq[q] + 1], HG_SITE_RECORD, ri)) rec[ri] = r;
                 }
             }
             continue;
@@ -568,7 +569,8 @@ __global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom 
                 unsigned base = 0;
                 if (lane == leader) base = atomicAdd(&cursor_back[t], (unsigned)__popc(grp));
                 base = __shfl_sync(grp, base, leader);
-                rec[off[t + 1] - 1u - (base + __popc(grp & lt))] = r;
+                const unsigned ri = off[t + 1] - 1u - (base + __popc(grp & lt));
+                if (HG_IN_BOUNDS(ri >= off[t] && ri < off[t + 1], HG_SITE_RECORD, ri)) rec[ri] = r;
             }
         }
     }
@@ -717,7 +719,8 @@ __device__ __forceinline__ void for_tile_cells(const AssignGeom &g, int tile, F 
         const int lx = r / g.t[1], ly = r - lx * g.t[1];
         const long long base =
             ((long long)(tx * g.t[0] + lx) * g.n[1] + (ty * g.t[1] + ly)) * g.n[2] + tz * g.t[2];
-        for (int lz = lane; lz < g.t[2]; lz += 32) f(r * g.t[2] + lz, base + lz);
+        for (int lz = lane; lz < g.t[2]; lz += 32)
+            if (HG_IN_BOUNDS(base + lz >= 0 && base + lz < g.ntot, HG_SITE_MESH_CELL, base + lz)) f(r * g.t[2] + lz, base + lz);
     }
 }
 
@@ -874,6 +877,7 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     }
     const T factor = (T)g.acc_factor;
     auto add = [&](int li, T v, T vi) {
+        if (!HG_IN_BOUNDS(li >= 0 && li < tcells, HG_SITE_TILE_CELL, li)) return;
         if (FIX64) {
             const double x = (double)v;
             const double hi = rint(x * 0x1p-40);
@@ -1023,6 +1027,7 @@ __global__ void k_tile_accum_src(const PRecS<T> *rec, const Chunk *ch, AssignGeo
         finv = ldexpf(1.0f, -sc);
     }
     auto add = [&](int li, T v, T vi) {
+        if (!HG_IN_BOUNDS(li >= 0 && li < tcells, HG_SITE_TILE_CELL, li)) return;
         if (FIX) {
             int hi, lo;
             fix_split((float)v, hi, lo);

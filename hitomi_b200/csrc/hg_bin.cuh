@@ -195,12 +195,12 @@ __global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt,
             zd v = mk<double>(0.0, 0.0);
             if (b.x >= 0) v = pk2 * ylm_reduced(lms.lm[q].l, lms.lm[q].m, kv[0], kv[1], kv[2]);
             const double sxr = group_sum(v.x, gx), sxi = group_sum(v.y, gx);
-            if (b.x >= 0 && lx) {
+            if (b.x >= 0 && lx && HG_IN_BOUNDS(b.x < nbin, HG_SITE_BIN, b.x)) {
                 atomicAdd(&sacc[2 * (b.x * lms.n + q)], sxr);
                 atomicAdd(&sacc[2 * (b.x * lms.n + q) + 1], sxi);
             }
             const double syr = group_sum(v.x, gy), syi = group_sum(v.y, gy);
-            if (b.y >= 0 && ly) {
+            if (b.y >= 0 && ly && HG_IN_BOUNDS(b.y < nbin, HG_SITE_BIN, b.y)) {
                 atomicAdd(&sacc[2 * (b.y * lms.n + q)], syr);
                 atomicAdd(&sacc[2 * (b.y * lms.n + q) + 1], syi);
             }
@@ -292,13 +292,13 @@ __global__ void k_pk_bin_terms(PkTerms<T> terms, F2 f2, Grid g, AxisTabs tabs, i
         const unsigned gy = __match_any_sync(0xffffffffu, b.y);
         const bool lx = (lane == __ffs(gx) - 1), ly = (lane == __ffs(gy) - 1);
         const double sxr = group_sum(v.x, gx), sxi = group_sum(v.y, gx);
-        if (b.x >= 0 && lx) {
+        if (b.x >= 0 && lx && HG_IN_BOUNDS(b.x < nbin, HG_SITE_BIN, b.x)) {
             atomicAdd(&sacc[2 * b.x], sxr);
             atomicAdd(&sacc[2 * b.x + 1], sxi);
             atomicAdd(&scnt[b.x], (unsigned long long)__popc(gx));
         }
         const double syr = group_sum(v.x, gy), syi = group_sum(v.y, gy);
-        if (b.y >= 0 && ly) {
+        if (b.y >= 0 && ly && HG_IN_BOUNDS(b.y < nbin, HG_SITE_BIN, b.y)) {
             atomicAdd(&sacc[2 * b.y], syr);
             atomicAdd(&sacc[2 * b.y + 1], syi);
             atomicAdd(&scnt[b.y], (unsigned long long)__popc(gy));

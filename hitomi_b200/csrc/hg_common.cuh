@@ -58,6 +58,36 @@ __device__ __forceinline__ cplx<double> mul_conj_rn(cplx<double> a, cplx<double>
 typedef cplx<double> zd;
 typedef cplx<float> zf;
 
+// Device-side bounds checks of the check build (-DHG_CHECK, libhitomi_b200_check.so): a
+// failed check counts itself in hg_check_word[0], the first one also records its site code
+// and the offending index, and the guarded access is skipped, so nothing faults; the engine
+// reads the word at the end of every API call and fails the call with that record.  Without
+// HG_CHECK every check is the constant true and compiles to nothing.
+#ifdef HG_CHECK
+__device__ unsigned long long hg_check_word[3];  // failures, site code, index
+__device__ __forceinline__ bool hg_check(bool ok, int site, long long index) {
+    if (ok) return true;
+    if (atomicAdd(&hg_check_word[0], 1ull) == 0ull) {
+        hg_check_word[1] = (unsigned long long)site;
+        hg_check_word[2] = (unsigned long long)index;
+    }
+    return false;
+}
+#define HG_IN_BOUNDS(cond, site, index) hg_check((cond), (site), (long long)(index))
+#else
+#define HG_IN_BOUNDS(cond, site, index) true
+#endif
+// check sites (the code a failed check reports)
+enum HgCheckSite {
+    HG_SITE_RECORD = 1,       // a particle record outside its tile's range (k_bin_scatter)
+    HG_SITE_TILE_CELL = 2,    // a stencil point outside the CTA's tile (k_tile_accum*)
+    HG_SITE_MESH_CELL = 3,    // a mesh cell outside the mesh (tile write-out)
+    HG_SITE_CROWD = 4,        // a staging slot outside the staging buffer
+    HG_SITE_BIN = 5,          // a coarse bin outside the binning arrays (k_pk_bin)
+    HG_SITE_CHAIN_ROW = 6,    // a chain row outside the kept cube (k_chain_x*)
+    HG_SITE_MIXED = 7,        // a mixed-radix line index outside the line (k_fft_pass_mixed)
+};
+
 // Wrapped integer mode / offset of array index i on an axis of n cells, the rule
 // of field.hpp:363-365: index i < n/2 is i, otherwise i - n.
 __host__ __device__ __forceinline__ int wrap_index(int i, int n) { return (i < n / 2) ? i : i - n; }

@@ -488,6 +488,20 @@ struct Engine : public hg_ctx {
         HG_CK(cudaEventElapsedTime(&ms, ev0, ev1));
         last_ms = ms;
         last_launches = launches;
+        check_word();
+    }
+    // check build: fail the call if a device-side bounds check failed (and clear the record)
+    void check_word() {
+#ifdef HG_CHECK
+        unsigned long long w[3] = {0, 0, 0};
+        HG_CK(cudaMemcpyFromSymbol(w, hg_check_word, sizeof(w)));
+        if (w[0]) {
+            const unsigned long long z[3] = {0, 0, 0};
+            HG_CK(cudaMemcpyToSymbol(hg_check_word, z, sizeof(z)));
+            throw HgError{"device bounds check failed " + std::to_string(w[0]) + " time(s); first at site " +
+                          std::to_string(w[1]) + ", index " + std::to_string((long long)w[2])};
+        }
+#endif
     }
 
     // ------------------------------------------------------------------ tables

@@ -366,6 +366,7 @@ __global__ void __launch_bounds__(256) k_fft_pass_mixed(LD ld, ST st, PassGeom g
             const int b = e / L, o = e - b * L;
             const int blk = o / NsR, rem = o - blk * NsR, q = rem / Ns, k = rem - q * Ns;
             const int j = blk * Ns + k, m = (k + q * Ns) * step;
+            if (!HG_IN_BOUNDS(j + (R - 1) * LR < L, HG_SITE_MIXED, j)) continue;
             const cplx<T> *line = cur + (size_t)b * L;
             cplx<T> acc = line[j];
             int ex = 0;

@@ -618,7 +618,10 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
     }
     __syncthreads();
     // shell j's input rows |n| <= e_j (the rows the pruned y pass wrote; ext null: all K)
-    auto ext_of = [&](int j) { return ext ? ext[j] : s; };
+    auto ext_of = [&](int j) {
+        const int e = ext ? ext[j] : s;
+        return HG_IN_BOUNDS(e <= s, HG_SITE_CHAIN_ROW, e) ? e : s;
+    };
     // those rows of shell j into Pb (row c = n + s; columns past the plane zero-filled)
     auto prefetch = [&](int j) {
         const cplx<T> *tj = t2 + (long long)j * K * plane;
@@ -790,7 +793,8 @@ __global__ void __launch_bounds__(16 * B, MINB)
     __syncthreads();
     for (int j = 0; j < ns; j++) {
         cplx<T> *tj = t2 + (long long)j * K * plane;
-        const int ej = ext ? ext[j] : s;  // shell j's input rows |n| <= e_j
+        int ej = ext ? ext[j] : s;  // shell j's input rows |n| <= e_j
+        if (!HG_IN_BOUNDS(ej <= s, HG_SITE_CHAIN_ROW, ej)) ej = s;
         cplx<T> v[12];
 #pragma unroll
         for (int n1 = 0; n1 < 12; n1++) {
