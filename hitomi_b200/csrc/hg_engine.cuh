@@ -257,7 +257,14 @@ struct Engine : public hg_ctx {
     double xi_k0 = 0.0;  // the k = 0 product the cached box correlation field was made with
     std::vector<int> orbit_lines, orbit_n2xy;  // per orbit: 4 (line, mirror) pairs; n_x^2 + n_y^2
     DBuf d_orbit_lines, d_orbit_n2xy;
-    long long n2dim = 0;
+    long long n2dim = 0;  // 3 (n/2)^2 + 1 style count of integer n^2 (k space; r space on equal cells)
+    // correlation-field histogram keys: integer n^2 = |x/dr|^2 on equal cells with a
+    // power-of-two z axis (the orbit / line kernels), else octant cells (k_xi_fold); per key
+    // the reference's |r| and the number of cells
+    bool xi_general = false;
+    long long nkey = 0;
+    std::vector<double> key_r, key_cells;
+    DBuf d_keyr;
     std::map<int, std::unique_ptr<BesselSpline>> splines;
     std::map<int, std::pair<std::unique_ptr<DBuf>, std::unique_ptr<DBuf>>> d_splines;
     std::map<int, std::unique_ptr<DBuf>> jtab_k;  // J_l[i][n2] at the k bins (geometry only)
@@ -347,6 +354,7 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(c.n_rbin >= 2 && c.rmax > c.rmin && c.rmin > 0.0, "need n_rbin >= 2 and 0 < rmin < rmax");
         g.volume = c.boxsize[0] * c.boxsize[1] * c.boxsize[2];
         g.ntot = (long long)c.n_mesh[0] * c.n_mesh[1] * c.n_mesh[2];
+        HG_REQUIRE(g.ntot <= (1LL << 31), "n_mesh: at most 2^31 cells in all");
         choose_tiles();
         wpow = c.assign + 1;
         // tools.hpp:118-134
@@ -1210,8 +1218,9 @@ struct Engine : public hg_ctx {
             int m = std::max(8, next_pow2(need));
             if (need > 128 && need <= 192) m = 192;  // 3 x 64: the register FFT's 24 x 8 split
             if (m >= g.n[a]) {
-                HG_REQUIRE(fft_supported_length(g.n[a]),
-                           "the bispectrum's shells reach the whole of a mesh axis that is not a power of two");
+                // the y and z chain passes take any length; the fused x pass a power of two
+                HG_REQUIRE(a != 0 || fft_supported_length(g.n[a]),
+                           "the bispectrum's shells reach the whole of n_mesh_x, which is not a power of two");
                 S.M[a] = g.n[a];
                 S.gs[a] = g.n[a] / 2;  // whole axis
             } else {
@@ -1552,11 +1561,19 @@ struct Engine : public hg_ctx {
     }
 
     // ------------------------------------------------------------------ shot noise (xi)
+    bool equal_cells() const {
+        return std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0];
+    }
     void build_orbits() {
-        if (!orbit_lines.empty()) return;
-        HG_REQUIRE(fft_supported_length(g.n[2]),
-                   "the correlation-field histograms (2PCF, bispectrum and 3PCF shot noise) need a power-of-two "
-                   "n_mesh_z in [8, 1024]");
+        if (nkey > 0) return;
+        n2dim = 0;
+        for (int a = 0; a < 3; a++) n2dim += (long long)(g.n[a] / 2) * (g.n[a] / 2);
+        n2dim += 1;
+        xi_general = !(equal_cells() && fft_supported_length(g.n[2]));
+        if (xi_general) {
+            build_octant_keys();
+            return;
+        }
         const int nx = g.n[0], ny = g.n[1];
         const bool swap = (nx == ny);
         for (int wx = 0; wx <= nx / 2; wx++)
@@ -1592,9 +1609,64 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemcpy(d_orbit_lines.p, orbit_lines.data(), sizeof(int) * orbit_lines.size(), cudaMemcpyHostToDevice));
         HG_CK(d_orbit_n2xy.ensure(sizeof(int) * orbit_n2xy.size()));
         HG_CK(cudaMemcpy(d_orbit_n2xy.p, orbit_n2xy.data(), sizeof(int) * orbit_n2xy.size(), cudaMemcpyHostToDevice));
-        n2dim = 0;
-        for (int a = 0; a < 3; a++) n2dim += (long long)(g.n[a] / 2) * (g.n[a] / 2);
-        n2dim += 1;
+        // keys n2: |r| = sqrt(n2 dr^2), cells per n2 from the per-axis counts of w^2
+        nkey = n2dim;
+        key_r.assign(nkey, 0.0);
+        const double dr = g.dr[0];
+        for (long long q = 0; q < nkey; q++) key_r[q] = std::sqrt(double(q) * (dr * dr));
+        std::vector<std::vector<double>> c1(3);
+        for (int a = 0; a < 3; a++) {
+            const int h = g.n[a] / 2;
+            c1[a].assign((size_t)h * h + 1, 0.0);
+            for (int i = 0; i < g.n[a]; i++) {
+                const int w = wrap_index(i, g.n[a]);
+                c1[a][(size_t)w * w] += 1.0;
+            }
+        }
+        key_cells.assign(nkey, 0.0);
+        for (size_t a = 0; a < c1[0].size(); a++) {
+            if (c1[0][a] == 0.0) continue;
+            for (size_t b = 0; b < c1[1].size(); b++) {
+                if (c1[1][b] == 0.0) continue;
+                for (size_t c = 0; c < c1[2].size(); c++)
+                    if (c1[2][c] != 0.0) key_cells[a + b + c] += c1[0][a] * c1[1][b] * c1[2][c];
+            }
+        }
+    }
+    // octant keys (a, b, c), 0 <= a <= n0/2 ...: |r| as the reference forms it per cell,
+    // sqrt(rx^2 + ry^2 + rz^2) with r_axis = (i < n/2 ? i : i - n) dr_axis (field.hpp:1040-1050)
+    void build_octant_keys() {
+        const int h0 = g.n[0] / 2 + 1, h1 = g.n[1] / 2 + 1, h2 = g.n[2] / 2 + 1;
+        nkey = (long long)h0 * h1 * h2;
+        key_r.assign(nkey, 0.0);
+        key_cells.assign(nkey, 0.0);
+        auto comp = [&](int a, int i) {  // the component of the octant's representative cell
+            const int n = g.n[a];
+            return double(i < n / 2 ? i : i - n) * g.dr[a];
+        };
+        auto mult = [&](int a, int i) { return (i == 0 || 2 * i == g.n[a]) ? 1.0 : 2.0; };
+        for (int a = 0; a < h0; a++)
+            for (int b = 0; b < h1; b++)
+                for (int c = 0; c < h2; c++) {
+                    const long long q = ((long long)a * h1 + b) * h2 + c;
+                    const double rx = comp(0, a), ry = comp(1, b), rz = comp(2, c);
+                    key_r[q] = std::sqrt(rx * rx + ry * ry + rz * rz);
+                    key_cells[q] = mult(0, a) * mult(1, b) * mult(2, c);
+                }
+        HG_CK(d_keyr.ensure(sizeof(double) * nkey));
+        HG_CK(cudaMemcpy(d_keyr.p, key_r.data(), sizeof(double) * nkey, cudaMemcpyHostToDevice));
+    }
+    // hist[h][key] of the transformed correlation field in xi (a full [n0][n1][n2] array)
+    void fold_hist(const HistSpec &hs, bool poly, double *hist) {
+        const unsigned blocks = (unsigned)std::min<long long>(grid1(nkey, 128), 148 * 16);
+        kb("xi_fold", double(g.ntot) * sizeof(C));
+        if (poly)
+            k_xi_fold<T, true><<<blocks, 128, 0, st>>>(dp<C>(xi), g.n[0], g.n[1], g.n[2], g.dr[0], g.dr[1], g.dr[2], hs,
+                                                       nkey, hist);
+        else
+            k_xi_fold<T, false><<<blocks, 128, 0, st>>>(dp<C>(xi), g.n[0], g.n[1], g.n[2], g.dr[0], g.dr[1], g.dr[2],
+                                                        hs, nkey, hist);
+        ke();
     }
 
     // a survey correlation-field spectrum (complex) synthesised into xi, then its x pass in place
@@ -1616,8 +1688,6 @@ struct Engine : public hg_ctx {
     // density N, bispec.hpp:913-921), delta0^2 for the 2PCF (dn against itself)
     void ensure_xi() { ensure_xi(delta0 * N0); }
     void ensure_xi(double k0prod) {
-        HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
-                   "bispectrum / 3PCF shot noise and the 2PCF need equal cell sizes on all axes");
         build_orbits();
         if (xi_valid && xi_k0 == k0prod) return;
         build_box_xi(half_spec(), double(slot[0].n), k0prod);
@@ -1632,6 +1702,13 @@ struct Engine : public hg_ctx {
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
         LdXiHat<T> ld{f, n2, xtabs, S, k0prod, invV};
+        if (xi_general) {  // the whole complex field, all three inverse passes (fold_hist reads it)
+            xi_x_pass(LdXiHatFull<T>{ld});
+            pass<+1>(n1, LdArr<T>{dp<C>(xi), n1, n2}, StArr<T>{dp<C>(xi), n1, n2}, n0, n2, "fft_xi_y");
+            pass<+1>(n2, LdArr<T>{dp<C>(xi), n2, 1}, StArr<T>{dp<C>(xi), n2, 1}, (long long)n0 * n1, 1, "fft_xi_z",
+                     double(g.ntot) * sizeof(C) * 2.0);
+            return;
+        }
         const long long yz = (long long)n1 * nh, tot = (long long)n0 * yz;
         unsigned blocks = (unsigned)std::min<long long>(grid1(tot, 256), 148 * 16);
         kb("xi_synth", double(tot) * sizeof(C) * 2.0);
@@ -1639,6 +1716,17 @@ struct Engine : public hg_ctx {
         ke();
         pass<+1>(n0, LdArr<T>{dp<C>(xi), n0, yz}, StArr<T>{dp<C>(xi), n0, yz}, 1, yz, "fft_xi_x");
         pass<+1>(n1, LdArr<T>{dp<C>(xi), n1, nh}, StArr<T>{dp<C>(xi), n1, nh}, n0, nh, "fft_xi_y");
+    }
+
+    // the box histograms of the current correlation field (hs.nh of them, [h][key], written
+    // whole): the orbit kernel on its equal-cell power-of-two meshes, the fold otherwise
+    void box_hist(const HistSpec &hs, double *hist) {
+        if (xi_general) {
+            fold_hist(hs, true, hist);
+            return;
+        }
+        HG_CK(cudaMemsetAsync(hist, 0, sizeof(double) * 2 * nkey * hs.nh, st));
+        launch_orbit(g.n[2], hs, (int)orbit_n2xy.size(), hist);
     }
 
     template <int L>
@@ -1736,16 +1824,15 @@ struct Engine : public hg_ctx {
                 for (const auto &c : cs) hs.term[h][hs.nterm[h]++] = YTerm{mp.l1, c.m1, mp.l2, c.m2, c.w};
                 orbit_weight_poly(hs, h);
             }
-            HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim * hs.nh));
-            HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim * hs.nh, st));
-            launch_orbit(g.n[2], hs, (int)orbit_n2xy.size(), dp<double>(hist_tmp));
+            HG_CK(hist_tmp.ensure(sizeof(double) * 2 * nkey * hs.nh));
+            box_hist(hs, dp<double>(hist_tmp));
             for (int h = 0; h < hs.nh; h++) {
                 const MP &mp = todo[t0 + h];
                 std::array<int, 3> key{mp.l1, mp.l2, mp.L};
                 auto &p = hist_mp[key];
                 if (!p) p = std::make_unique<DBuf>();
-                HG_CK(p->ensure(sizeof(double) * 2 * n2dim));
-                HG_CK(cudaMemcpyAsync(p->p, dp<double>(hist_tmp) + 2 * n2dim * h, sizeof(double) * 2 * n2dim,
+                HG_CK(p->ensure(sizeof(double) * 2 * nkey));
+                HG_CK(cudaMemcpyAsync(p->p, dp<double>(hist_tmp) + 2 * nkey * h, sizeof(double) * 2 * nkey,
                                       cudaMemcpyDeviceToDevice, st));
                 hist_ok.insert(key);
             }
@@ -1777,12 +1864,17 @@ struct Engine : public hg_ctx {
         HG_CK(d_kv.ensure(sizeof(double) * kbin.size()));
         HG_CK(cudaMemcpyAsync(d_kv.p, kbin.data(), sizeof(double) * kbin.size(), cudaMemcpyHostToDevice, st));
         auto J = std::make_unique<DBuf>();
-        HG_CK(J->ensure(sizeof(double) * kbin.size() * n2dim));
-        long long tot = (long long)kbin.size() * n2dim;
+        HG_CK(J->ensure(sizeof(double) * kbin.size() * nkey));
+        long long tot = (long long)kbin.size() * nkey;
         kb("bessel_table", double(tot) * 8.0);
-        k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n, s.xmin,
-                                                        s.dx, dp<double>(d_kv), (int)kbin.size(), g.dr[0], n2dim,
-                                                        dp<double>(*J));
+        if (xi_general)  // the octant keys' radii
+            k_bessel_table_r<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n,
+                                                              s.xmin, s.dx, dp<double>(d_kv), (int)kbin.size(),
+                                                              dp<double>(d_keyr), nkey, dp<double>(*J));
+        else
+            k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n,
+                                                            s.xmin, s.dx, dp<double>(d_kv), (int)kbin.size(), g.dr[0],
+                                                            n2dim, dp<double>(*J));
         ke();
         HG_CK(cudaStreamSynchronize(st));
         const double *p = dp<double>(*J);
@@ -1912,7 +2004,7 @@ struct Engine : public hg_ctx {
         HG_CK(snmat.ensure(sizeof(double2) * ns * ns));
         const double *J1 = jtab(mp.l1);
         const double *J2 = jtab(mp.l2);
-        const int nblk = sn_partial_blocks(n2dim);
+        const int nblk = sn_partial_blocks(nkey);
         const int rb = std::min(ns, HG_SN_MAXROWS);
         HG_CK(sn_part.ensure(sizeof(double) * 2 * (size_t)nblk * rb * rb));
         HG_CK(snblk.ensure(sizeof(double2) * (size_t)rb * rb));
@@ -1921,9 +2013,9 @@ struct Engine : public hg_ctx {
                 const int na = std::min(rb, ns - a0), nb = std::min(rb, ns - b0);
                 const size_t smem = sn_partial_smem(na, nb);
                 HG_CK(cudaFuncSetAttribute(k_sn_partial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-                kb("sn_matrix", double(na + 2 * nb + 2) * n2dim * 8.0);
-                k_sn_partial<<<nblk, HG_SN_THREADS, smem, st>>>(J1 + (size_t)a0 * n2dim, na, J2 + (size_t)b0 * n2dim,
-                                                                nb, hq, n2dim, dp<double>(sn_part));
+                kb("sn_matrix", double(na + 2 * nb + 2) * nkey * 8.0);
+                k_sn_partial<<<nblk, HG_SN_THREADS, smem, st>>>(J1 + (size_t)a0 * nkey, na, J2 + (size_t)b0 * nkey,
+                                                                nb, hq, nkey, dp<double>(sn_part));
                 ke();
                 kb("sn_matrix", double(nblk) * na * nb * 16.0);
                 k_sum_parts<<<grid1(sum_parts_threads((long long)na * nb), 256), 256, 0, st>>>(dp<double>(sn_part), nblk, na * nb,
@@ -2262,27 +2354,12 @@ struct Engine : public hg_ctx {
                    "the 3PCF needs a cubic box and mesh (j_l(|k| r) is tabulated on integer |n|^2)");
         build_orbits();
         if (!zfine.empty()) return;
-        const int n = g.n[0], h = n / 2;
-        // cells per n2 = |w|^2 (w the wrapped cell offset, field.hpp:1040-1043)
-        std::vector<long long> c1(h * h + 1, 0);
-        for (int i = 0; i < n; i++) {
-            int w = wrap_index(i, n);
-            c1[w * w]++;
-        }
-        std::vector<int> sq;
-        for (int v = 0; v <= h; v++) sq.push_back(v * v);
-        std::vector<double> cnt(n2dim, 0.0);
-        for (int a : sq)
-            for (int b : sq)
-                for (int c : sq) cnt[a + b + c] += double(c1[a]) * double(c1[b]) * double(c1[c]);
-        // rindex = int(|r| / 0.5 + 0.5), kept if < 10000 (field.hpp:1030-1053).  |r|^2 = n2 dr^2 is the
-        // reference's sum of (i dr)^2 exactly when those squares are exact (dyadic dr, e.g. an integer
-        // box over a power-of-two mesh).
-        const double dr = g.dr[0];
-        zfine.assign(n2dim, -1);
-        for (long long q = 0; q < n2dim; q++) {
-            double rmag = std::sqrt(double(q) * (dr * dr));
-            int ri = (int)(rmag / 0.5 + 0.5);
+        // rindex = int(|r| / 0.5 + 0.5), kept if < 10000 (field.hpp:1030-1053), per histogram key
+        // (on equal cells |r|^2 = n2 dr^2, the reference's sum of (i dr)^2 exactly when those
+        // squares are exact, e.g. an integer box over a power-of-two mesh)
+        zfine.assign(nkey, -1);
+        for (long long q = 0; q < nkey; q++) {
+            const int ri = (int)(key_r[q] / 0.5 + 0.5);
             if (ri < 10000) zfine[q] = ri;
         }
         // coarse bins from neighbouring half widths (field.hpp:1058-1085)
@@ -2300,9 +2377,9 @@ struct Engine : public hg_ctx {
             }
         }
         zcount.assign(nr, 0.0);
-        for (long long q = 0; q < n2dim; q++)
+        for (long long q = 0; q < nkey; q++)
             if (zfine[q] >= 0)
-                for (int j : zcoarse[zfine[q]]) zcount[j] += cnt[q];
+                for (int j : zcoarse[zfine[q]]) zcount[j] += key_cells[q];
     }
 
     // J_l[j][n2] = j_l(r_j dk sqrt(n2)) at the r bins (geometry only: cached for the context)
@@ -2507,13 +2584,13 @@ struct Engine : public hg_ctx {
         const double dV = g.volume / double(g.ntot);
         const int r0 = (ith < 0) ? 0 : ith, rows = (ith < 0) ? ns : 1;
         std::fill(sn_save, sn_save + 2 * mps.size() * (size_t)rows * ns, 0.0);
-        std::vector<double> hist(2 * n2dim);
+        std::vector<double> hist(2 * nkey);
         for (size_t q = 0; q < mps.size(); q++) {
             const MP &mp = mps[q];
             HG_CK(cudaMemcpyAsync(hist.data(), hists[q], sizeof(double) * hist.size(), cudaMemcpyDeviceToHost, st));
             HG_CK(cudaStreamSynchronize(st));
             std::vector<double> xr(ns, 0.0), xim(ns, 0.0);
-            for (long long n2 = 0; n2 < n2dim; n2++) {
+            for (long long n2 = 0; n2 < nkey; n2++) {
                 if (zfine[n2] < 0) continue;
                 for (int j : zcoarse[zfine[n2]]) {
                     xr[j] += hist[2 * n2];
@@ -2962,8 +3039,6 @@ struct Engine : public hg_ctx {
     // Yhat_l1m1(x) Yhat_l2m2(x), with xi_LM = FFT_+[(dn_LM conj N_00 - S3_LM C) / W^2 / V]
     // (calcShotNoiseForBispectrum_ijk field.hpp:1116-1160; bispec.hpp:124-196, 400-460)
     void survey_histograms(const std::vector<MP> &mps) {
-        HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
-                   "bispectrum / 3PCF shot noise needs equal cell sizes on all axes");
         build_orbits();
         std::vector<MP> todo;
         for (const auto &mp : mps) {
@@ -2976,8 +3051,8 @@ struct Engine : public hg_ctx {
         for (const auto &mp : todo) {
             auto &p = hist_sv[{mp.l1, mp.l2, mp.L}];
             if (!p) p = std::make_unique<DBuf>();
-            HG_CK(p->ensure(sizeof(double) * 2 * n2dim));
-            HG_CK(cudaMemsetAsync(p->p, 0, sizeof(double) * 2 * n2dim, st));
+            HG_CK(p->ensure(sizeof(double) * 2 * nkey));
+            HG_CK(cudaMemsetAsync(p->p, 0, sizeof(double) * 2 * nkey, st));
         }
         const double alpha = src_alpha;
         const SpecK n00 = sfield(sn_kind(), 0, 0, alpha);
@@ -3006,6 +3081,7 @@ struct Engine : public hg_ctx {
                 xi_x_pass(ld);
                 pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0],
                          g.n[2], "fft_xi_y");
+                if (xi_general) xi_z_pass();
                 for (size_t h0 = 0; h0 < hm.size(); h0 += HG_MAX_HIST) {
                     HistSpec hs;
                     memset(&hs, 0, sizeof(hs));
@@ -3017,19 +3093,35 @@ struct Engine : public hg_ctx {
                         for (const auto &c : e.second)
                             hs.term[h][hs.nterm[h]++] = YTerm{e.first.l1, c.m1, e.first.l2, c.m2, c.w};
                     }
-                    HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim * hs.nh));
-                    HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim * hs.nh, st));
-                    launch_line(hs, dp<double>(hist_tmp));
+                    HG_CK(hist_tmp.ensure(sizeof(double) * 2 * nkey * hs.nh));
+                    line_hist(hs, dp<double>(hist_tmp));
                     for (int h = 0; h < hs.nh; h++) {
                         const MP &mp = hm[h0 + h].first;
                         double *dst = dp<double>(*hist_sv[{mp.l1, mp.l2, mp.L}]);
-                        k_axpy<<<grid1(2 * n2dim, 256), 256, 0, st>>>(dst, dp<double>(hist_tmp) + 2 * n2dim * h,
-                                                                      2 * n2dim);
+                        k_axpy<<<grid1(2 * nkey, 256), 256, 0, st>>>(dst, dp<double>(hist_tmp) + 2 * nkey * h,
+                                                                      2 * nkey);
                         HG_CK(cudaGetLastError());
                     }
                 }
             }
         for (const auto &mp : todo) hist_sv_ok.insert({mp.l1, mp.l2, mp.L});
+    }
+
+    // the z inverse pass of a correlation field whose x and y passes are done, in place (the
+    // meshes that fold_hist serves)
+    void xi_z_pass() {
+        pass<+1>(g.n[2], LdArr<T>{dp<C>(xi), g.n[2], 1}, StArr<T>{dp<C>(xi), g.n[2], 1}, (long long)g.n[0] * g.n[1], 1,
+                 "fft_xi_z", double(g.ntot) * sizeof(C) * 2.0);
+    }
+    // histograms with azimuth-dependent weights ([h][key], written whole): the line kernel
+    // (z pass fused) on its meshes, the fold of the fully transformed field otherwise
+    void line_hist(const HistSpec &hs, double *hist) {
+        if (xi_general) {
+            fold_hist(hs, false, hist);
+            return;
+        }
+        HG_CK(cudaMemsetAsync(hist, 0, sizeof(double) * 2 * nkey * hs.nh, st));
+        launch_line(hs, hist);
     }
 
     static bool needs_los(const std::vector<MP> &mps) {
@@ -3317,30 +3409,12 @@ struct Engine : public hg_ctx {
     void xi2_geometry() {
         build_orbits();
         if (x2.built) return;
-        std::vector<std::vector<double>> c1(3);
-        for (int a = 0; a < 3; a++) {
-            const int h = g.n[a] / 2;
-            c1[a].assign((size_t)h * h + 1, 0.0);
-            for (int i = 0; i < g.n[a]; i++) {
-                const int w = wrap_index(i, g.n[a]);
-                c1[a][(size_t)w * w] += 1.0;
-            }
-        }
-        x2.cells.assign(n2dim, 0.0);
-        for (size_t a = 0; a < c1[0].size(); a++) {
-            if (c1[0][a] == 0.0) continue;
-            for (size_t b = 0; b < c1[1].size(); b++) {
-                if (c1[1][b] == 0.0) continue;
-                for (size_t c = 0; c < c1[2].size(); c++)
-                    if (c1[2][c] != 0.0) x2.cells[a + b + c] += c1[0][a] * c1[1][b] * c1[2][c];
-            }
-        }
+        x2.cells = key_cells;
         const int n_temp = 20000;
-        const double dr_temp = 0.5, dr = g.dr[0];
-        x2.fine.assign(n2dim, -1);
-        for (long long q = 0; q < n2dim; q++) {
-            const double rmag = std::sqrt(double(q) * (dr * dr));
-            const int ri = (int)(rmag / dr_temp + 0.5);
+        const double dr_temp = 0.5;
+        x2.fine.assign(nkey, -1);
+        for (long long q = 0; q < nkey; q++) {
+            const int ri = (int)(key_r[q] / dr_temp + 0.5);
             if (ri < n_temp) x2.fine[q] = ri;
         }
         const double dr_bin = rbin[1] - rbin[0];
@@ -3358,12 +3432,12 @@ struct Engine : public hg_ctx {
 
     // xi_save[j] = scale * (sum of hist over the n2 of bin j) / (cells of bin j)
     void xi2_bin(const double *d_hist, double scale, double *xi_save, int *n_mode) {
-        std::vector<double> h(2 * n2dim);
+        std::vector<double> h(2 * nkey);
         HG_CK(cudaMemcpyAsync(h.data(), d_hist, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
         HG_CK(cudaStreamSynchronize(st));
         const int nr = cfg.n_rbin;
         std::vector<double> xr(nr, 0.0), xim(nr, 0.0), nm(nr, 0.0);
-        for (long long q = 0; q < n2dim; q++) {
+        for (long long q = 0; q < nkey; q++) {
             const int f = x2.fine[q];
             if (f < 0) continue;
             for (int j : x2.coarse[f]) {
@@ -3384,8 +3458,6 @@ struct Engine : public hg_ctx {
     void xi_box_recon(int ell, double alpha, double *xi_save, int *n_mode, double *norm) override {
         HG_REQUIRE(ell >= 0, "ell must be >= 0");
         HG_REQUIRE(slot[0].set && slot[1].set, "the reconstructed 2PCF needs data (slot 0) and randoms (slot 1)");
-        HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
-                   "the 2PCF needs equal cell sizes on all axes");
         begin();
         invalidate_stats();
         src_kind = -1;
@@ -3399,9 +3471,8 @@ struct Engine : public hg_ctx {
         hs.parity[0] = (ell % 2 == 0) ? 1 : -1;
         hs.term[0][hs.nterm[0]++] = YTerm{ell, 0, 0, 0, 1.0};
         orbit_weight_poly(hs, 0);
-        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim));
-        HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim, st));
-        launch_orbit(g.n[2], hs, (int)orbit_n2xy.size(), dp<double>(hist_tmp));
+        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * nkey));
+        box_hist(hs, dp<double>(hist_tmp));
         xi2_bin(dp<double>(hist_tmp), double(2 * ell + 1), xi_save, n_mode);
         if (norm) *norm = g.volume / double(slot[0].n) / double(slot[0].n);
         end();
@@ -3421,9 +3492,8 @@ struct Engine : public hg_ctx {
         hs.parity[0] = (ell % 2 == 0) ? 1 : -1;
         hs.term[0][hs.nterm[0]++] = YTerm{ell, 0, 0, 0, 1.0};
         orbit_weight_poly(hs, 0);
-        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim));
-        HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim, st));
-        launch_orbit(g.n[2], hs, (int)orbit_n2xy.size(), dp<double>(hist_tmp));
+        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * nkey));
+        box_hist(hs, dp<double>(hist_tmp));
         xi2_bin(dp<double>(hist_tmp), double(2 * ell + 1), xi_save, n_mode);
         if (norm) *norm = g.volume / double(slot[0].n) / double(slot[0].n);
         end();
@@ -3438,17 +3508,15 @@ struct Engine : public hg_ctx {
         HG_REQUIRE(ell >= 0, "ell must be >= 0");
         if (window) require_randoms(ell > 0);
         else require_survey(ell > 0);
-        HG_REQUIRE(std::fabs(g.dr[0] - g.dr[1]) <= 1e-12 * g.dr[0] && std::fabs(g.dr[0] - g.dr[2]) <= 1e-12 * g.dr[0],
-                   "the 2PCF needs equal cell sizes on all axes");
         begin();
         set_source(window ? 2 : 1, window ? 0.0 : alpha);
         xi2_geometry();
         const SpecK f00 = sfield(delta_kind(), 0, 0, src_alpha);
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
         xi_valid = false;  // the box correlation field is overwritten
-        HG_CK(xi2acc.ensure(sizeof(double) * 2 * n2dim));
-        HG_CK(cudaMemsetAsync(xi2acc.p, 0, sizeof(double) * 2 * n2dim, st));
-        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * n2dim));
+        HG_CK(xi2acc.ensure(sizeof(double) * 2 * nkey));
+        HG_CK(cudaMemsetAsync(xi2acc.p, 0, sizeof(double) * 2 * nkey, st));
+        HG_CK(hist_tmp.ensure(sizeof(double) * 2 * nkey));
         for (int M = -ell; M <= ell; M++) {
             HistSpec hs;
             memset(&hs, 0, sizeof(hs));
@@ -3469,9 +3537,9 @@ struct Engine : public hg_ctx {
             xi_x_pass(ld);
             pass<+1>(g.n[1], LdArr<T>{dp<C>(xi), g.n[1], g.n[2]}, StArr<T>{dp<C>(xi), g.n[1], g.n[2]}, g.n[0], g.n[2],
                      "fft_xi_y");
-            HG_CK(cudaMemsetAsync(hist_tmp.p, 0, sizeof(double) * 2 * n2dim, st));
-            launch_line(hs, dp<double>(hist_tmp));
-            k_axpy<<<grid1(2 * n2dim, 256), 256, 0, st>>>(dp<double>(xi2acc), dp<double>(hist_tmp), 2 * n2dim);
+            if (xi_general) xi_z_pass();
+            line_hist(hs, dp<double>(hist_tmp));
+            k_axpy<<<grid1(2 * nkey, 256), 256, 0, st>>>(dp<double>(xi2acc), dp<double>(hist_tmp), 2 * nkey);
             HG_CK(cudaGetLastError());
         }
         xi2_bin(dp<double>(xi2acc), 1.0, xi_save, n_mode);

@@ -324,6 +324,18 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
     }
 };
 
+// The same spectrum as a complex field on the full grid (for k_synth: x = l, (y, z) = i), on
+// meshes whose correlation field is transformed whole (k_xi_fold)
+template <typename T>
+struct LdXiHatFull {
+    LdXiHat<T> h;
+    __device__ __forceinline__ cplx<T> operator()(long long, int l, long long i) const {
+        const unsigned ui = (unsigned)i;
+        const int iy = (int)(ui / (unsigned)h.n2), iz = (int)(ui - (unsigned)iy * (unsigned)h.n2);
+        return mk<T>(h.value(l, iy, iz), (T)0);
+    }
+};
+
 // The real correlation-field spectrum P of the box, two kz columns per complex value:
 // out[ix][iy][j] = P(ix, iy, 2j) + i P(ix, iy, 2j + 1)  ([n0][n1][n2/2]).  A complex
 // transform of these lines along x and y gives both planes' transforms at once; the
@@ -558,6 +570,61 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
     }
 }
 
+// The correlation-field histogram on any mesh (unequal cells, z lines of any length), from
+// the transformed field xi [n0][n1][n2] in memory: key q is an octant cell (a, b, c),
+// 0 <= a <= n0/2 ..., the cells (+-a, +-b, +-c) share the reference's |r| (rvec per axis
+// (i < n/2 ? i : i - n) dr_axis, field.hpp:1040-1050), and
+//   hist[h][q] = sum over those cells of xi(x) f_h(x),  f_h = sum_terms w Yhat_l1m1 Yhat_l2m2
+// at the cell's physical direction (POLY: m1 + m2 = 0, f_h as the Chebyshev polynomial in
+// mu = r_z / r, f0 at r = 0).  One thread per key gathers its mirror cells: no atomics.
+template <typename T, bool POLY>
+__global__ void k_xi_fold(const cplx<T> *__restrict__ xi, int n0, int n1, int n2, double dr0, double dr1, double dr2,
+                          HistSpec hs, long long nkey, double *hist) {
+    const int h1 = n1 / 2 + 1, h2 = n2 / 2 + 1;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nkey;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(q % h2), b = (int)((q / h2) % h1), a = (int)(q / ((long long)h1 * h2));
+        const int xs[2] = {a, n0 - a}, ys[2] = {b, n1 - b}, zs[2] = {c, n2 - c};
+        const int nxm = (a == 0 || 2 * a == n0) ? 1 : 2, nym = (b == 0 || 2 * b == n1) ? 1 : 2,
+                  nzm = (c == 0 || 2 * c == n2) ? 1 : 2;
+        zd acc[HG_MAX_HIST];
+        for (int h = 0; h < HG_MAX_HIST; h++) acc[h] = mk<double>(0.0, 0.0);
+        for (int u = 0; u < nxm; u++)
+            for (int v = 0; v < nym; v++)
+                for (int w = 0; w < nzm; w++) {
+                    const int ix = xs[u], iy = ys[v], iz = zs[w];
+                    const double rx = (double)(ix < n0 / 2 ? ix : ix - n0) * dr0;
+                    const double ry = (double)(iy < n1 / 2 ? iy : iy - n1) * dr1;
+                    const double rz = (double)(iz < n2 / 2 ? iz : iz - n2) * dr2;
+                    const cplx<T> x = xi[((long long)ix * n1 + iy) * n2 + iz];
+                    const zd val = mk<double>((double)x.x, (double)x.y);
+                    for (int h = 0; h < hs.nh; h++) {
+                        zd f;
+                        if (POLY) {
+                            const double r = sqrt(rx * rx + ry * ry + rz * rz);
+                            f = mk<double>((r > 0.0) ? cheb_eval(hs.cheb[h], hs.deg[h], rz / r) : hs.f0[h], 0.0);
+                        } else {
+                            f = mk<double>(0.0, 0.0);
+                            for (int k = 0; k < hs.nterm[h]; k++) {
+                                const YTerm &yt = hs.term[h][k];
+                                f = f + (ylm_reduced(yt.l1, yt.m1, rx, ry, rz) * ylm_reduced(yt.l2, yt.m2, rx, ry, rz)) *
+                                            yt.w;
+                            }
+                        }
+                        acc[h] = acc[h] + f * val;
+                    }
+                }
+        for (int h = 0; h < hs.nh; h++) {
+            hist[2 * ((long long)h * nkey + q)] = acc[h].x;
+            hist[2 * ((long long)h * nkey + q) + 1] = acc[h].y;
+        }
+    }
+}
+
+// J[i][q] = j_l(k_i r_q) at the keys' radii (the octant keys of k_xi_fold)
+__global__ void k_bessel_table_r(const double *sy, const double *sc, int sn, double xmin, double dx, const double *kv,
+                                 int nk, const double *rk, long long nkey, double *J);
+
 // y += x (n doubles)
 __global__ void k_axpy(double *y, const double *x, long long n) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -588,6 +655,16 @@ __global__ void k_bessel_table(const double *sy, const double *sc, int sn, doubl
     double r = dr * sqrt((double)n2);
     double x = kv[i] * r;
     double xmax = xmin + dx * double(sn - 1);
+    J[q] = (x <= xmax) ? spline_eval(sy, sc, sn, xmin, dx, x) : 0.0;
+}
+
+__global__ void k_bessel_table_r(const double *sy, const double *sc, int sn, double xmin, double dx, const double *kv,
+                                 int nk, const double *rk, long long nkey, double *J) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)nk * nkey) return;
+    const int i = (int)(q / nkey);
+    const double x = kv[i] * rk[q - (long long)i * nkey];
+    const double xmax = xmin + dx * double(sn - 1);
     J[q] = (x <= xmax) ? spline_eval(sy, sc, sn, xmin, dx, x) : 0.0;
 }
 

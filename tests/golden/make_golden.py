@@ -17,6 +17,7 @@ so the GPU tests need neither the reference sources nor the harness.
     python tests/golden/make_golden.py --outside (only box_outside.npz: particles outside the box)
     python tests/golden/make_golden.py --long   (only box_long_axes.npz: 1024-point axes)
     python tests/golden/make_golden.py --mixed  (only mixed_meshes.npz: non-power-of-two meshes)
+    python tests/golden/make_golden.py --general (only general_meshes.npz: B, 2PCF, 3PCF on such meshes)
     python tests/golden/make_golden.py --configs (only box_config_sizes.npz: 128^3 and 512^3)
     python tests/golden/make_golden.py --extensions (only box_extensions.npz: PCS and
         interlacing, from the numpy restatement oracle/restate.py; no harness needed)
@@ -375,6 +376,49 @@ def make_mixed_meshes():
     np.savez_compressed(os.path.join(HERE, "mixed_meshes.npz"), **d)
 
 
+def make_general_meshes():
+    """The correlation-field statistics on meshes whose histograms take the general (octant
+    key) path -- unequal cells, or a z axis that is not a power of two: box B and 2PCF on a
+    [64, 36, 50] mesh of a [1000, 800, 900] box; box B and 3PCF on a cubic [48, 48, 48] mesh;
+    survey B on [64, 92, 52] and the survey 2PCF on [50, 92, 52] (3500 Mpc/h cube)."""
+    d = {}
+    pos = lognormal_box(12000, 1000.0, ngrid=32, seed=25, exact_n=12000) * np.array([1.0, 0.8, 0.9])
+    nmb, bsb = [64, 36, 50], [1000.0, 800.0, 900.0]
+    bb = Binning(0.015, 0.075, 7, 20.0, 160.0, 8)
+    d.update(box_pos=pos, box_n_mesh=np.array(nmb), box_boxsize=np.array(bsb), box_binning=binning_arr(bb))
+    for mp in ((0, 0, 0), (2, 0, 2)):
+        with ref_runner.RefRun() as r:
+            r.run("bk", pos, *mp, nmb, bsb, bb, assign="TSC")
+            d["box_bk_" + "".join(map(str, mp))] = r.bk(*mp, bb.n_kbin)
+    for ell in (0, 2):
+        with ref_runner.RefRun() as r:
+            r.run("2PCF", pos, ell, 0, ell, nmb, bsb, bb, assign="TSC")
+            d[f"box_xi_{ell}"] = r.xi(ell)[1]
+    cub = lognormal_box(10000, 1000.0, ngrid=32, seed=26, exact_n=10000)
+    bc = Binning(0.01, 0.04, 4, 20.0, 140.0, 7)
+    d.update(cub_pos=cub, cub_n_mesh=48, cub_boxsize=1000.0, cub_binning=binning_arr(bc))
+    with ref_runner.RefRun() as r:
+        r.run("bk", cub, 2, 0, 2, 48, 1000.0, bc, assign="TSC")
+        d["cub_bk_202"] = r.bk(2, 0, 2, bc.n_kbin)
+    for mp in ((0, 0, 0), (1, 1, 0)):
+        with ref_runner.RefRun() as r:
+            r.run("3PCF", cub, *mp, 48, 1000.0, bc, assign="TSC")
+            d["cub_zeta_" + "".join(map(str, mp))] = r.zeta(*mp, bc.n_rbin)
+    data, rand = survey_shell(2000, 30000, seed=27)
+    bs = Binning(0.004, 0.02, 5, 150.0, 750.0, 5)
+    d.update(sv_data=data, sv_rand=rand, sv_boxsize=3500.0, sv_binning=binning_arr(bs),
+             sv_bk_n_mesh=np.array([64, 92, 52]), sv_xi_n_mesh=np.array([50, 92, 52]))
+    for mp in ((0, 0, 0), (2, 0, 2)):
+        with ref_runner.RefRun() as r:
+            r.run("bk", data, *mp, [64, 92, 52], 3500.0, bs, assign="TSC", randoms=rand)
+            d["sv_bk_" + "".join(map(str, mp))] = r.bk(*mp, bs.n_kbin)
+    for ell in (0, 2):
+        with ref_runner.RefRun() as r:
+            r.run("2PCF", data, ell, 0, ell, [50, 92, 52], 3500.0, bs, assign="TSC", randoms=rand)
+            d[f"sv_xi_{ell}"] = r.xi(ell)[1]
+    np.savez_compressed(os.path.join(HERE, "general_meshes.npz"), **d)
+
+
 def make_recon():
     """BAO reconstruction (particle_reconstruction.hpp:12-402) through the reference's drivers:
     the shifted positions and the reconstructed P_l, survey (main.cpp:215-225, then
@@ -468,13 +512,15 @@ def make_config_sizes():
 
 
 def main():
-    if "--outside" in sys.argv or "--long" in sys.argv or "--mixed" in sys.argv:
+    if "--outside" in sys.argv or "--long" in sys.argv or "--mixed" in sys.argv or "--general" in sys.argv:
         if "--outside" in sys.argv:
             make_outside()
         if "--long" in sys.argv:
             make_long_axes()
         if "--mixed" in sys.argv:
             make_mixed_meshes()
+        if "--general" in sys.argv:
+            make_general_meshes()
         print("fixtures written")
         return
     if "--recon" in sys.argv:
@@ -570,6 +616,7 @@ def main():
     make_outside()
     make_long_axes()
     make_mixed_meshes()
+    make_general_meshes()
     print("fixtures written")
 
 

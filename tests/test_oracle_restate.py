@@ -121,3 +121,14 @@ def test_restated_pk_mixed_mesh_matches_reference(assign):
     for ell in (0, 2):
         pk, nmode, norm = R.pk_box(d["box_pos"], nm, bs, kb, ell, R.SCHEMES[assign])
         assert relerr(norm * pk, d[f"box_pk_{assign}_{ell}"], 1e-12) < 1e-10, ell
+
+
+def test_restated_bk_unequal_cells_matches_reference():
+    """B_202 on a [64, 36, 50] mesh of a [1000, 800, 900] box: the shot noise's per-cell |r|
+    with unequal cells (the reference's field.hpp:1040-1050 rvec)."""
+    d = load_golden("general_meshes.npz")
+    kb = kbins(d["box_binning"])
+    nm = [int(v) for v in d["box_n_mesh"]]
+    bs = [float(v) for v in d["box_boxsize"]]
+    bk, sn, norm = R.bk_box(d["box_pos"], nm, bs, kb, 2, 0, 2, R.TSC)
+    assert relerr(norm * (bk - sn), d["box_bk_202"], 1e-12) < 1e-10
