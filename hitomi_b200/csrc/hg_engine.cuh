@@ -22,8 +22,10 @@
 // (family b, shell j) then gives the whole k1 x k2 matrix for every family a paired with b.
 //
 // Bispectrum shot noise.  xi(x) = IFFT[(|delta|^2 - N C)/W^2]/V is transformed on the full
-// mesh; its last pass is fused with a histogram over integer n^2 = |x/dr|^2 (cubic cells),
-// which turns sum_x j_l1(k1 r) j_l2(k2 r) xi Yhat1 Yhat2 into a sum over distinct radii.
+// mesh; its last pass is fused with a histogram over integer n^2 = |x/dr|^2 (equal cells,
+// power-of-two z), or, on other meshes, the whole field is folded into octant cells with
+// their exact |r|; either turns sum_x j_l1(k1 r) j_l2(k2 r) xi Yhat1 Yhat2 into a sum over
+// distinct radii.
 #include "hitomi_gpu.h"
 #include "hg_ctx.hpp"
 #include "hg_common.cuh"
@@ -2348,12 +2350,35 @@ struct Engine : public hg_ctx {
     }
 
     // ------------------------------------------------------------------ 3PCF (box)
+    // k-space keys of the 3PCF fields' j_l(|k| r): integer |n|^2 on a cubic box and mesh,
+    // octant modes (|wx|, |wy|, |wz|) with the reference's |k| otherwise
+    bool zk_octant = false;
+    long long nkk = 0;
+    DBuf d_kkr;
     void zeta_geometry() {
-        HG_REQUIRE(g.n[0] == g.n[1] && g.n[0] == g.n[2] && cfg.boxsize[0] == cfg.boxsize[1] &&
-                       cfg.boxsize[0] == cfg.boxsize[2],
-                   "the 3PCF needs a cubic box and mesh (j_l(|k| r) is tabulated on integer |n|^2)");
         build_orbits();
         if (!zfine.empty()) return;
+        zk_octant = !(g.n[0] == g.n[1] && g.n[0] == g.n[2] && cfg.boxsize[0] == cfg.boxsize[1] &&
+                      cfg.boxsize[0] == cfg.boxsize[2]);
+        if (zk_octant) {
+            const int h0 = g.n[0] / 2 + 1, h1 = g.n[1] / 2 + 1, h2 = g.n[2] / 2 + 1;
+            nkk = (long long)h0 * h1 * h2;
+            std::vector<double> kr(nkk);
+            auto comp = [&](int a, int i) {
+                const int n = g.n[a];
+                return double(i < n / 2 ? i : i - n) * g.dk[a];
+            };
+            for (int a = 0; a < h0; a++)
+                for (int b = 0; b < h1; b++)
+                    for (int c = 0; c < h2; c++) {
+                        const double kx = comp(0, a), ky = comp(1, b), kz = comp(2, c);
+                        kr[((long long)a * h1 + b) * h2 + c] = std::sqrt(kx * kx + ky * ky + kz * kz);
+                    }
+            HG_CK(d_kkr.ensure(sizeof(double) * nkk));
+            HG_CK(cudaMemcpy(d_kkr.p, kr.data(), sizeof(double) * nkk, cudaMemcpyHostToDevice));
+        } else {
+            nkk = n2dim;
+        }
         // rindex = int(|r| / 0.5 + 0.5), kept if < 10000 (field.hpp:1030-1053), per histogram key
         // (on equal cells |r|^2 = n2 dr^2, the reference's sum of (i dr)^2 exactly when those
         // squares are exact, e.g. an integer box over a power-of-two mesh)
@@ -2382,7 +2407,7 @@ struct Engine : public hg_ctx {
                 for (int j : zcoarse[zfine[q]]) zcount[j] += key_cells[q];
     }
 
-    // J_l[j][n2] = j_l(r_j dk sqrt(n2)) at the r bins (geometry only: cached for the context)
+    // J_l[j][key] = j_l(r_j |k|_key) at the r bins (keys: zeta_geometry; geometry only: cached)
     const double *jtab_rbins(int l) {
         auto it = jtab_r.find(l);
         if (it != jtab_r.end()) return dp<double>(*it->second);
@@ -2391,12 +2416,17 @@ struct Engine : public hg_ctx {
         HG_CK(d_rv.ensure(sizeof(double) * rbin.size()));
         HG_CK(cudaMemcpyAsync(d_rv.p, rbin.data(), sizeof(double) * rbin.size(), cudaMemcpyHostToDevice, st));
         auto J = std::make_unique<DBuf>();
-        HG_CK(J->ensure(sizeof(double) * rbin.size() * n2dim));
-        long long tot = (long long)rbin.size() * n2dim;
+        HG_CK(J->ensure(sizeof(double) * rbin.size() * nkk));
+        long long tot = (long long)rbin.size() * nkk;
         kb("bessel_table", double(tot) * 8.0);
-        k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n, s.xmin,
-                                                        s.dx, dp<double>(d_rv), (int)rbin.size(), g.dk[0], n2dim,
-                                                        dp<double>(*J));
+        if (zk_octant)
+            k_bessel_table_r<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n,
+                                                              s.xmin, s.dx, dp<double>(d_rv), (int)rbin.size(),
+                                                              dp<double>(d_kkr), nkk, dp<double>(*J));
+        else
+            k_bessel_table<<<grid1(tot, 256), 256, 0, st>>>(dp<double>(*sp.first), dp<double>(*sp.second), s.n,
+                                                            s.xmin, s.dx, dp<double>(d_rv), (int)rbin.size(), g.dk[0],
+                                                            n2dim, dp<double>(*J));
         ke();
         HG_CK(cudaStreamSynchronize(st));
         const double *p = dp<double>(*J);
@@ -2464,8 +2494,8 @@ struct Engine : public hg_ctx {
             HG_CK(zf[key]->ensure(need));
         }
         zeta_U(f.l, f.m);
-        const double *J = jtab_rbins(f.l) + (size_t)r0 * n2dim;
-        LdZetaField<T> ld{dp<C>(Uz), J, n2dim, g.n[0], g.n[1], g.n[2]};
+        const double *J = jtab_rbins(f.l) + (size_t)r0 * nkk;
+        LdZetaField<T> ld{dp<C>(Uz), J, nkk, g.n[0], g.n[1], g.n[2], zk_octant ? 1 : 0};
         full_inverse(ld, dp<C>(*p), nr, "zeta_fields");
         zf_ok.insert(key);
         return dp<C>(*p);

@@ -794,18 +794,22 @@ __global__ void k_zeta_U(Spec<T> f, Grid g, AxisTabs tabs, int wpow, int l, int 
 // Loader of the first inverse pass (along x) of the fields F_r = IFFT[j_l(|k| r) U(k)]
 // for a block of radii: o = radius within the block, l = ix, i = iy * nz + iz.
 // J[r][n2] = j_l(dk r sqrt(n2)) with n2 = |n|^2 of the wrapped mode (cubic box).
+// Other meshes (octant = 1): J[r][q] at the k-space octant key q = (|wx| h1 + |wy|) h2 + |wz|,
+// h_a = n_a / 2 + 1, whose |k| is the reference's sqrt(kx^2 + ky^2 + kz^2).
 template <typename T>
 struct LdZetaField {
     const cplx<T> *U;
     const double *J;  // rows of the block's radii
-    long long n2dim;
+    long long n2dim;  // keys per row
     int n0, n1, n2;
+    int octant;
     __device__ __forceinline__ cplx<T> operator()(long long o, int l, long long i) const {
         const unsigned ui = (unsigned)i;
         const int iy = (int)(ui / (unsigned)n2);
         const int iz = (int)(ui - (unsigned)iy * (unsigned)n2);
         int wx = wrap_index(l, n0), wy = wrap_index(iy, n1), wz = wrap_index(iz, n2);
-        long long q = (long long)wx * wx + (long long)wy * wy + (long long)wz * wz;
+        long long q = octant ? ((long long)abs(wx) * (n1 / 2 + 1) + abs(wy)) * (n2 / 2 + 1) + abs(wz)
+                             : (long long)wx * wx + (long long)wy * wy + (long long)wz * wz;
         double j = J[o * n2dim + q];
         cplx<T> u = U[(long long)l * n1 * n2 + i];
         return mk<T>((T)(j * (double)u.x), (T)(j * (double)u.y));

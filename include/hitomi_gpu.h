@@ -128,7 +128,7 @@ int hg_bk_box_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_kbin
  * (bispec.hpp:1205-1424).  ith_rbin >= 0 computes that r1 row, -1 all n_rbin rows;
  * zeta_save, sn_save: [rows][n_rbin] complex.  The shot noise sits only on the diagonal
  * r1 = r2 (bispec.hpp:1279-1285).  Output file value = norm * Re(zeta_save - sn_save)
- * (bispec.hpp:1402-1416), norm = V^3 / N^3.  Needs a cubic box and mesh. */
+ * (bispec.hpp:1402-1416), norm = V^3 / N^3. */
 int hg_zeta_box(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double *zeta_save, double *sn_save,
                 double *norm);
 
@@ -156,7 +156,7 @@ int hg_bk_survey_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_k
 
 /* Survey-geometry 3PCF multipole.  Replaces calcThreePointCorrelationFunction
  * (bispec.hpp:355-614).  Layout as hg_zeta_box; the shot noise sits on the diagonal;
- * *norm = V_survey^2 / (sum w_D)^3.  Needs a cubic box and mesh. */
+ * *norm = V_survey^2 / (sum w_D)^3. */
 int hg_zeta_survey(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double alpha, double vsurvey,
                    double *zeta_save, double *sn_save, double *norm);
 
@@ -204,7 +204,7 @@ int hg_xi_window(hg_ctx *ctx, int ell, double vsurvey, double *xi_save, int *n_m
  * calcThreePointWindowCorrelationFunction (bispec.hpp:617-874): the survey 3PCF of the
  * randoms alone, shot noise from their conj(Yhat) w^2 field minus sum_R w^2 Yhat_LM, on the
  * diagonal.  Layout as hg_zeta_box; *norm = V_survey^2 / (sum w_R)^3.  Output file value =
- * norm * Re(zeta_save - sn_save) (bispec.hpp:863-866).  Needs a cubic box and mesh. */
+ * norm * Re(zeta_save - sn_save) (bispec.hpp:863-866). */
 int hg_zeta_window(hg_ctx *ctx, int ell1, int ell2, int ELL, int ith_rbin, double vsurvey, double *zeta_save,
                    double *sn_save, double *norm);
 int hg_zeta_window_multi(hg_ctx *ctx, int n_multipoles, const int *ells, int ith_rbin, double vsurvey,

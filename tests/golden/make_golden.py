@@ -404,6 +404,10 @@ def make_general_meshes():
         with ref_runner.RefRun() as r:
             r.run("3PCF", cub, *mp, 48, 1000.0, bc, assign="TSC")
             d["cub_zeta_" + "".join(map(str, mp))] = r.zeta(*mp, bc.n_rbin)
+    for mp in ((0, 0, 0), (2, 0, 2)):  # the 3PCF on the non-cubic box (k-space octant keys)
+        with ref_runner.RefRun() as r:
+            r.run("3PCF", pos, *mp, nmb, bsb, bb, assign="TSC")
+            d["box_zeta_" + "".join(map(str, mp))] = r.zeta(*mp, bb.n_rbin)
     data, rand = survey_shell(2000, 30000, seed=27)
     bs = Binning(0.004, 0.02, 5, 150.0, 750.0, 5)
     d.update(sv_data=data, sv_rand=rand, sv_boxsize=3500.0, sv_binning=binning_arr(bs),

@@ -15,7 +15,7 @@ TOL = {"fp64": (1e-10, 1e-12), "fp32": (1e-4, 1e-3)}
 
 
 @pytest.mark.parametrize("form", ["fp64", "fp32"])
-def test_box_bk_and_xi_unequal_cells(form):
+def test_box_bk_xi_zeta_unequal_cells(form):
     from hitomi_b200.api import Context
     g = load_golden("general_meshes.npz")
     b = binning_from(g["box_binning"])
@@ -29,6 +29,10 @@ def test_box_bk_and_xi_unequal_cells(form):
         for ell in (0, 2):
             xi, nm, xnorm = c.xi_box(ell)
             assert relerr((xnorm * xi).real, g[f"box_xi_{ell}"], floor) < tol, ell
+        # the 3PCF on the non-cubic box: j_l(|k| r) at k-space octant keys
+        z, zs, zn = c.zeta_box_multi(mps)
+        for q, mp in enumerate(mps):
+            assert relerr((zn * (z[q] - zs[q])).real, g["box_zeta_" + "".join(map(str, mp))], floor) < tol, mp
 
 
 @pytest.mark.parametrize("form", ["fp64", "fp32"])

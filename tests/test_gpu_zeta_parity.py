@@ -103,14 +103,11 @@ def test_zeta_after_bispectrum_on_same_context():
         assert relerr(file_value(z, sn, norm), d["zeta_TSC_202"], 1e-12) < 1e-10
 
 
-def test_zeta_rejects_noncubic_and_bad_rows():
+def test_zeta_rejects_bad_rows():
+    """(Non-cubic meshes run: tests/test_gpu_general_meshes.py.)"""
     from hitomi_b200.api import Binning, Context, HitomiError
     b = Binning(0.02, 0.1, 5, 20.0, 140.0, 7)
     pos = np.random.default_rng(3).uniform(0, 400.0, size=(1000, 3))
-    with Context([16, 16, 32], 400.0, b, "TSC", "fp64") as c:
-        c.set_particles(0, pos)
-        with pytest.raises(HitomiError, match="cubic"):
-            c.zeta_box(0, 0, 0)
     with Context(16, 400.0, b, "TSC", "fp64") as c:
         c.set_particles(0, pos)
         with pytest.raises(HitomiError, match="ith_rbin"):
