@@ -36,6 +36,7 @@ struct AssignGeom {
     int periodic;     // 0 = reference flat-index rule
     double shift;     // added to the scaled position (0, or 0.5 for the interlaced copy)
     int t[3];         // tile extent per axis
+    int tsh[3];       // log2 t[a] when t[a] is a power of two, else -1 (tile_axis)
     int nt[3];        // tiles per axis
     double factor;      // 1/dV (field.hpp:76-77), used for the FP64 in-bounds mass
     double acc_factor;  // factor applied in the mesh accumulation (1/dV, or 1 for a mass mesh)
@@ -160,10 +161,6 @@ __device__ __forceinline__ bool effective_cell(const AssignGeom &g, int ix, int 
     return true;
 }
 
-__device__ __forceinline__ int tile_of(const AssignGeom &g, int cx, int cy, int cz) {
-    return ((cx / g.t[0]) * g.nt[1] + cy / g.t[1]) * g.nt[2] + cz / g.t[2];
-}
-
 struct PartSrc {
     const unsigned char *base;  // device copy of the caller's array of structs
     long long n;
@@ -254,13 +251,23 @@ struct TileList {
     bool sep;
 };
 
+// Tile of cell c (>= 0) along axis a: a shift for power-of-two tiles (the usual case), which
+// spares the binning passes six integer divisions per particle.
+__device__ __forceinline__ int tile_axis(const AssignGeom &g, int a, int c) {
+    return g.tsh[a] >= 0 ? (c >> g.tsh[a]) : c / g.t[a];
+}
+
+__device__ __forceinline__ int tile_of(const AssignGeom &g, int cx, int cy, int cz) {
+    return (tile_axis(g, 0, cx) * g.nt[1] + tile_axis(g, 1, cy)) * g.nt[2] + tile_axis(g, 2, cz);
+}
+
 __device__ __forceinline__ void tile_list(const AssignGeom &g, const int anc[3], TileList &tl, int *slow) {
     const int W = stencil_width(g.scheme), s0 = stencil_start(g.scheme);
     tl.sep = stencil_separable(g, anc);
     if (tl.sep) {
         for (int a = 0; a < 3; a++) {
-            tl.f[a] = axis_cell(g, a, anc[a] + s0) / g.t[a];
-            tl.l[a] = axis_cell(g, a, anc[a] + s0 + W - 1) / g.t[a];
+            tl.f[a] = tile_axis(g, a, axis_cell(g, a, anc[a] + s0));
+            tl.l[a] = tile_axis(g, a, axis_cell(g, a, anc[a] + s0 + W - 1));
             tl.c[a] = (tl.f[a] != tl.l[a]) ? 2 : 1;
         }
         tl.n = tl.c[0] * tl.c[1] * tl.c[2];
@@ -282,7 +289,9 @@ __device__ __forceinline__ void tile_list(const AssignGeom &g, const int anc[3],
 
 __device__ __forceinline__ int tile_at(const AssignGeom &g, const TileList &tl, const int *slow, int q) {
     if (!tl.sep) return slow[q];
-    const int qc = q % tl.c[2], qb = (q / tl.c[2]) % tl.c[1], qa = q / (tl.c[2] * tl.c[1]);
+    // q as a mixed-radix number over the axes' tile counts (each 1 or 2): bits, no division
+    const int sz = tl.c[2] - 1, sy = tl.c[1] - 1;
+    const int qc = q & sz, qb = (q >> sz) & sy, qa = q >> (sz + sy);
     const int tx = qa ? tl.l[0] : tl.f[0], ty = qb ? tl.l[1] : tl.f[1], tz = qc ? tl.l[2] : tl.f[2];
     return (tx * g.nt[1] + ty) * g.nt[2] + tz;
 }

@@ -99,6 +99,10 @@ struct hg_ctx {
     // B_raw and the shot noise of the box bispectrum, [q][ns][ns] complex (all rows)
     virtual std::vector<std::vector<double>> stage_bk_signal(const std::vector<hg::MP> &mps) = 0;
     virtual std::vector<std::vector<double>> stage_bk_shot(const std::vector<hg::MP> &mps) = 0;
+    // bin averages [nbin][ells.size()] complex of the box density's (|delta|^2 - N C) / W^2
+    // Yhat_l0 (the P_l bins before the 2l + 1 factor), from the P cache where those
+    // multipoles were binned already
+    virtual std::vector<double> stage_pk_terms(const std::vector<int> &ells) = 0;
     // kernels launched since the last call (added to the calling engine's count)
     virtual long long stage_take_launches() = 0;
 };

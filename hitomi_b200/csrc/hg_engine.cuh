@@ -124,6 +124,22 @@ inline X *dp(const DBuf &b) {
 
 inline unsigned grid1(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
+// CTAs of `kern` (bs threads, no dynamic shared memory) that are resident on the GPU at once:
+// the grid of a grid-stride kernel that runs as one wave (a grid of several waves leaves the
+// last one partly empty).  Queried once per kernel.
+template <class K>
+inline unsigned resident_grid(K kern, int bs) {
+    static int per_sm = 0;  // one static per kernel instantiation
+    if (per_sm == 0) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, bs, 0) != cudaSuccess || v < 1) v = 1;
+        per_sm = v;
+    }
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (unsigned)(sms * per_sm);
+}
+
 int next_pow2(int v) {
     int p = 1;
     while (p < v) p <<= 1;
@@ -191,6 +207,12 @@ struct Engine : public hg_ctx {
     DBuf H;     // half spectrum of dV (rho - nbar)
     DBuf H2;    // half spectrum of the half-cell shifted assignment (interlacing)
     bool dens_valid = false;
+    // FP32 engine whose density the FP64 engine computed: that FP64 half spectrum (valid while
+    // this density is), and whether H still waits for its narrowed copy.  The shot-noise
+    // correlation field reads the FP64 spectrum directly; H is narrowed only when a stage of
+    // this engine needs the spectrum itself (shell fields, G, the 3PCF, P binning).
+    const cplx<double> *H_wide = nullptr;
+    bool narrow_pending = false;
     struct PkBins {
         std::vector<double> avg;  // [nbin] complex bin averages before the (2l+1) factor
         std::vector<unsigned long long> nm;
@@ -635,7 +657,7 @@ struct Engine : public hg_ctx {
         }
         if (kind == 0) {
             box_density();
-            dsrc = SpecK{half_spec(), delta0, 0.0};
+            dsrc = SpecK{half_spec_unnarrowed(), delta0, 0.0};  // its readers narrow first
         } else {
             dsrc = sfield(delta_kind(), 0, 0, alpha);
         }
@@ -654,6 +676,8 @@ struct Engine : public hg_ctx {
     void invalidate() {
         src_kind = -1;
         dens_valid = false;
+        H_wide = nullptr;
+        narrow_pending = false;
         pk_cache.clear();
         sn_xi_cache.clear();
         Gm_ok.clear();
@@ -718,6 +742,9 @@ struct Engine : public hg_ctx {
         a.shift = shift;
         for (int q = 0; q < 3; q++) {
             a.t[q] = tile_t[q];
+            a.tsh[q] = -1;
+            for (int b = 0; b < 31; b++)
+                if ((1 << b) == a.t[q]) a.tsh[q] = b;
             a.nt[q] = g.n[q] / a.t[q];
             a.far[q] = 0x1p30 * g.L[q] / double(g.n[q]);
         }
@@ -750,7 +777,8 @@ struct Engine : public hg_ctx {
             if (srcs[q].n == 0) continue;  // an empty catalogue (no data for a window function)
             Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0, dp<unsigned>(defcnt) + ns,
                      dp<unsigned>(defcnt) + ns + 1};
-            const unsigned nb = (unsigned)std::min<long long>(grid1(srcs[q].n, 256), MASS_BLOCKS);
+            const unsigned nb = (unsigned)std::min<long long>(
+                grid1(srcs[q].n, 256), std::min<long long>(MASS_BLOCKS, resident_grid(k_bin_count, 256)));
             if (q < 2) mass_blocks[q] = (int)nb;
             kb("assign_bin_count", double(srcs[q].n) * 24.0);
             k_bin_count<<<nb, 256, 0, st>>>(srcs[q], ag, df, dp<unsigned>(cnt),
@@ -794,6 +822,8 @@ struct Engine : public hg_ctx {
             Defer df{dp<int>(deflist) + o, dp<unsigned>(defcnt) + q, 0, dp<unsigned>(defcnt) + ns,
                      dp<unsigned>(defcnt) + ns + 1};
             kb("assign_bin_scatter", double(srcs[q].n) * 24.0 + rec_bytes * double(srcs[q].n) / double(nsum));
+            // (several waves: one resident wave was measured slower here, 0.83 -> 0.96 ms per
+            // 1e7 particles, unlike the count pass)
             k_bin_scatter<MK><<<(unsigned)std::min<long long>(grid1(srcs[q].n, 256), 148 * 16), 256, 0, st>>>(
                 srcs[q], ag, mks[q], df, dp<unsigned>(off), dp<unsigned>(cursor), dp<unsigned>(cursor_back), recp);
             ke();
@@ -1026,7 +1056,28 @@ struct Engine : public hg_ctx {
         dens_valid = true;
     }
 
-    Spec<T> half_spec() const { return Spec<T>{dp<C>(H), g.n[0], g.n[1], g.n[2], 1}; }
+    // the density half spectrum in this engine's precision (narrowed first if it came from the
+    // FP64 engine and was not yet needed)
+    Spec<T> half_spec() {
+        narrow_density();
+        return half_spec_unnarrowed();
+    }
+    Spec<T> half_spec_unnarrowed() const { return Spec<T>{dp<C>(H), g.n[0], g.n[1], g.n[2], 1}; }
+    void narrow_density() {
+        if (!narrow_pending) return;
+        narrow_pending = false;
+        convert_spectrum(H_wide, true);
+    }
+    void convert_spectrum(const void *src, bool src_fp64) {
+        const long long n = (long long)g.n[0] * g.n[1] * (g.n[2] / 2 + 1);
+        const unsigned blocks = (unsigned)std::min<long long>(grid1(n, 256), 148 * 16);
+        kb("stage_convert", double(n) * (sizeof(C) + (src_fp64 ? 16.0 : 8.0)));
+        if (src_fp64)
+            k_convert_spec<double, T><<<blocks, 256, 0, st>>>(reinterpret_cast<const cplx<double> *>(src), dp<C>(H), n);
+        else
+            k_convert_spec<float, T><<<blocks, 256, 0, st>>>(reinterpret_cast<const cplx<float> *>(src), dp<C>(H), n);
+        ke();
+    }
 
     // ------------------------------------------------------------------ P binning
     // Averages over each k bin of  (f conj f - S C(k)) / W^2 * Yhat_lm(k)  for a list of (l, m)
@@ -1129,18 +1180,8 @@ struct Engine : public hg_ctx {
             }
     }
 
-    // powerspec.hpp:273-332
-    void pk_box(int ell, double *pk_save, int *n_mode, double *norm) override {
-        HG_REQUIRE(ell >= 0, "ell must be >= 0");
-        if (hi && (fp64_stages & HG_STAGE_DENSITY)) {  // binned from the FP64 spectrum
-            begin();
-            hi->pk_box(ell, pk_save, n_mode, norm);
-            launches += hi->stage_take_launches();
-            end();
-            return;
-        }
-        begin();
-        box_density();
+    // the box P_l bins of the current density (box_density() done), binned on first use
+    const PkBins &box_pk_bins(int ell) {
         if (!pk_cache.count(ell)) {
             // one pass over the modes bins the requested multipole together with the
             // others of the usual set (0, 2, 4) not yet binned for this density: the pass
@@ -1162,7 +1203,22 @@ struct Engine : public hg_ctx {
                 pb.nm = nm;
             }
         }
-        const PkBins &pb = pk_cache[ell];
+        return pk_cache[ell];
+    }
+
+    // powerspec.hpp:273-332
+    void pk_box(int ell, double *pk_save, int *n_mode, double *norm) override {
+        HG_REQUIRE(ell >= 0, "ell must be >= 0");
+        if (hi && (fp64_stages & HG_STAGE_DENSITY)) {  // binned from the FP64 spectrum
+            begin();
+            hi->pk_box(ell, pk_save, n_mode, norm);
+            launches += hi->stage_take_launches();
+            end();
+            return;
+        }
+        begin();
+        box_density();
+        const PkBins &pb = box_pk_bins(ell);
         for (int i = 0; i < cfg.n_kbin; i++) {
             pk_save[2 * i] = double(2 * ell + 1) * pb.avg[2 * i];
             pk_save[2 * i + 1] = double(2 * ell + 1) * pb.avg[2 * i + 1];
@@ -1553,6 +1609,7 @@ struct Engine : public hg_ctx {
         build_shells();
         HG_REQUIRE(n_ent() > 0, "no Fourier modes fall inside the k shells");
         if (!shD_valid) {
+            if (src_kind == 0) narrow_density();  // dsrc is the box density
             HG_CK(shD.ensure(sizeof(double2) * n_ent()));
             kb("shell_D", double(n_ent()) * (16.0 + sizeof(C)));
             k_shell_D<T><<<grid1(n_ent(), 256), 256, 0, st>>>(dp<ShellEnt>(shells.d_ent), n_ent(), dsrc.s, g, tabs,
@@ -1692,29 +1749,33 @@ struct Engine : public hg_ctx {
     void ensure_xi(double k0prod) {
         build_orbits();
         if (xi_valid && xi_k0 == k0prod) return;
-        build_box_xi(half_spec(), double(slot[0].n), k0prod);
+        if (H_wide)  // the FP64 engine's density: |delta|^2 formed from it, not from a narrowed copy
+            build_box_xi(Spec<double>{H_wide, g.n[0], g.n[1], g.n[2], 1}, double(slot[0].n), k0prod);
+        else
+            build_box_xi(half_spec(), double(slot[0].n), k0prod);
         xi_k0 = k0prod;
         xi_valid = true;
     }
 
     // The box correlation field of a real field's half spectrum f, (|f|^2 - S C) / W^2 / V,
     // after its x and y inverse passes, into xi (even and odd kz planes as one complex field)
-    void build_box_xi(const Spec<T> &f, double S, double k0prod) {
+    template <typename SE>
+    void build_box_xi(const Spec<SE> &f, double S, double k0prod) {
         const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2], nh = n2 / 2;
         HG_CK(xi.ensure(sizeof(C) * g.ntot));
         const double invV = 1.0 / g.volume;  // field.hpp:1122
-        LdXiHat<T> ld{f, n2, xtabs, S, k0prod, invV};
+        LdXiHat<T, SE> ld{f, n2, xtabs, S, k0prod, invV};
         if (xi_general) {  // the whole complex field, all three inverse passes (fold_hist reads it)
-            xi_x_pass(LdXiHatFull<T>{ld});
+            xi_x_pass(LdXiHatFull<T, SE>{ld});
             pass<+1>(n1, LdArr<T>{dp<C>(xi), n1, n2}, StArr<T>{dp<C>(xi), n1, n2}, n0, n2, "fft_xi_y");
             pass<+1>(n2, LdArr<T>{dp<C>(xi), n2, 1}, StArr<T>{dp<C>(xi), n2, 1}, (long long)n0 * n1, 1, "fft_xi_z",
                      double(g.ntot) * sizeof(C) * 2.0);
             return;
         }
         const long long yz = (long long)n1 * nh, tot = (long long)n0 * yz;
-        unsigned blocks = (unsigned)std::min<long long>(grid1(tot, 256), 148 * 16);
-        kb("xi_synth", double(tot) * sizeof(C) * 2.0);
-        k_synth_pairs<T, LdXiHat<T>><<<blocks, 256, 0, st>>>(ld, n0, n1, nh, dp<C>(xi));
+        const int bs = (int)std::min<long long>(256, (nh + 31) / 32 * 32);
+        kb("xi_synth", double(tot) * (sizeof(C) + sizeof(cplx<SE>)));
+        k_synth_pairs_rows<T, LdXiHat<T, SE>><<<dim3(n1, n0 / 2 + 1), bs, 0, st>>>(ld, n0, n1, nh, dp<C>(xi));
         ke();
         pass<+1>(n0, LdArr<T>{dp<C>(xi), n0, yz}, StArr<T>{dp<C>(xi), n0, yz}, 1, yz, "fft_xi_x");
         pass<+1>(n1, LdArr<T>{dp<C>(xi), n1, nh}, StArr<T>{dp<C>(xi), n1, nh}, n0, nh, "fft_xi_y");
@@ -2080,6 +2141,13 @@ struct Engine : public hg_ctx {
         end();
     }
 
+    // box P_l bin averages [nbin][ells] complex (before the 2l + 1 factor) of the current
+    // density, from the engine that computed it
+    std::vector<double> pk_terms(const std::vector<int> &ells) {
+        if (hi && (fp64_stages & HG_STAGE_DENSITY)) return hi->stage_pk_terms(ells);
+        return stage_pk_terms(ells);
+    }
+
     // the current box density on the FP64 engine: its own (HG_STAGE_DENSITY) or this one's
     // spectrum widened
     void hi_density() {
@@ -2110,7 +2178,25 @@ struct Engine : public hg_ctx {
         const int nl = (int)lms.size();
         std::vector<double> avg(2 * ns * std::max(nl, 1), 0.0);
         std::vector<unsigned long long> nm;
-        for (int b0 = 0; b0 < nl; b0 += HG_MAX_LM) {
+        bool m0 = true;
+        for (const LM &x : lms) m0 = m0 && x.m == 0;
+        if (m0 && nl > 0) {
+            // every term is a box P_l bin (m = 0, S = N): the P cache of this density, on the
+            // FP64 engine when it computed the density
+            std::vector<int> ells;
+            for (const LM &x : lms)
+                if (std::find(ells.begin(), ells.end(), x.l) == ells.end()) ells.push_back(x.l);
+            const std::vector<double> a = pk_terms(ells);
+            const int ne = (int)ells.size();
+            for (int u = 0; u < nl; u++) {
+                const int e = (int)(std::find(ells.begin(), ells.end(), lms[u].l) - ells.begin());
+                for (int j = 0; j < ns; j++) {
+                    avg[2 * (j * nl + u)] = a[2 * (j * ne + e)];
+                    avg[2 * (j * nl + u) + 1] = a[2 * (j * ne + e) + 1];
+                }
+            }
+        }
+        for (int b0 = 0; b0 < nl && !m0; b0 += HG_MAX_LM) {
             int b1 = std::min(nl, b0 + HG_MAX_LM);
             std::vector<LM> part(lms.begin() + b0, lms.begin() + b1);
             std::vector<double> a;
@@ -2322,13 +2408,14 @@ struct Engine : public hg_ctx {
     void stage_import_density(const void *src, bool src_fp64, double d0, double n0, double m0) override {
         const long long n = (long long)g.n[0] * g.n[1] * (g.n[2] / 2 + 1);
         HG_CK(H.ensure(sizeof(C) * n));
-        const unsigned blocks = (unsigned)std::min<long long>(grid1(n, 256), 148 * 16);
-        kb("stage_convert", double(n) * (sizeof(C) + (src_fp64 ? 16.0 : 8.0)));
-        if (src_fp64)
-            k_convert_spec<double, T><<<blocks, 256, 0, st>>>(reinterpret_cast<const cplx<double> *>(src), dp<C>(H), n);
-        else
-            k_convert_spec<float, T><<<blocks, 256, 0, st>>>(reinterpret_cast<const cplx<float> *>(src), dp<C>(H), n);
-        ke();
+        if (sizeof(T) == 4 && src_fp64) {  // narrowed when first needed (narrow_density)
+            H_wide = reinterpret_cast<const cplx<double> *>(src);
+            narrow_pending = true;
+        } else {
+            H_wide = nullptr;
+            narrow_pending = false;
+            convert_spectrum(src, src_fp64);
+        }
         delta0 = d0;
         N0 = n0;
         dens_mass = m0;
@@ -2342,6 +2429,19 @@ struct Engine : public hg_ctx {
     std::vector<std::vector<double>> stage_bk_shot(const std::vector<MP> &mps) override {
         set_source(0, 0.0);
         return bk_shot(mps);
+    }
+    std::vector<double> stage_pk_terms(const std::vector<int> &ells) override {
+        box_density();
+        const int ns = cfg.n_kbin, ne = (int)ells.size();
+        std::vector<double> a(2 * ns * ne);
+        for (int e = 0; e < ne; e++) {
+            const PkBins &pb = box_pk_bins(ells[e]);
+            for (int j = 0; j < ns; j++) {
+                a[2 * (j * ne + e)] = pb.avg[2 * j];
+                a[2 * (j * ne + e) + 1] = pb.avg[2 * j + 1];
+            }
+        }
+        return a;
     }
     long long stage_take_launches() override {
         const long long l = launches;
@@ -2437,6 +2537,7 @@ struct Engine : public hg_ctx {
     // U = Yhat_lm F / W / V on the full grid, F the given spectrum (the density by default)
     void zeta_U(int l, int m) { zeta_U_of(dsrc, l, m); }
     void zeta_U_of(const SpecK &src, int l, int m) {
+        if (src.s.p == dp<C>(H)) narrow_density();  // the box density
         HG_CK(Uz.ensure(sizeof(C) * g.ntot));
         unsigned blocks = (unsigned)std::min<long long>(grid1(g.ntot, 256), 148 * 16);
         kb("zeta_U", double(g.ntot) * (sizeof(C) * 1.5));

@@ -19,6 +19,7 @@
 
 #include "hg_common.cuh"
 #include "hg_fft.cuh"
+#include "hg_chain.cuh"
 
 namespace hg {
 // one copy per translation unit: each .cu file names its own HG_TU_NS, so the kernels and
@@ -327,7 +328,7 @@ inline size_t fft2_smem() {
     return ((size_t)XchgLayout<L, COLS, CF::B>::ELEMS + L) * sizeof(cplx<T>);  // exchange buffer, twiddles
 }
 
-// Strided passes over plain arrays (LdArr), software-pipelined: a persistent CTA walks its
+// Strided passes over arrays of rows (PipeArr, PipeRowsCompactL), software-pipelined: a persistent CTA walks its
 // tiles (L rows x PB columns) and, while it transforms one tile, the next one streams into the
 // other half of a double buffer with cp.async (no registers held, no wait until the data is
 // needed).  The tile's buffer then serves as the transform's exchange buffer.  Without this
@@ -338,11 +339,47 @@ struct PipeCfg {
     static constexpr int R2 = Split<L>::R2;
     // columns per tile: the double buffer of FP64 1024-point tiles takes 4 columns to stay
     // within the 227 KB a CTA may hold (at 512 points 4 columns, three CTAs per SM instead of
-    // one, measured slower together with halved 512-point row tiles)
-    static constexpr int B = (L >= 1024 && sizeof(T) == 8) ? 4 : ((L >= 256) ? 8 : 16);
+    // one, measured slower: the FP64 density transform 1.83 -> 2.45 ms)
+    // FP32 lines of 256 and 512 points take 16 columns (128-byte row segments; the FP32
+    // correlation-field passes at 512 points 0.34 -> 0.25 ms each against 8 columns)
+    static constexpr int B = (L >= 1024 && sizeof(T) == 8) ? 4
+                           : (L >= 256 && sizeof(T) == 8) ? 8
+                           : (L >= 1024) ? 8 : 16;
     static constexpr int NT = R2 * B;
     // double buffer, then the L twiddles (staged once per persistent CTA)
     static constexpr size_t smem() { return (2 * (size_t)L * B + L) * sizeof(cplx<T>); }
+};
+
+// Row sources of the pipelined pass: line(o) once per tile, then row(line, l) = the start of
+// row l of that line (inner elements contiguous), or nullptr for a row that is zero.
+template <typename T>
+struct PipeArr {  // [o][L][inner] (LdArr)
+    const cplx<T> *p;
+    long long L, inner;
+    using Line = const cplx<T> *;
+    __device__ __forceinline__ Line line(long long o) const { return p + o * L * inner; }
+    __device__ __forceinline__ const cplx<T> *row(Line b, int l) const { return b + (long long)l * inner; }
+};
+template <typename T>
+struct PipeRowsCompactL {  // LdRowsCompactL: rows |n| <= e_j,y of the compact line lines[q]
+    const cplx<T> *p;
+    int K, M, s;
+    long long inner;
+    const int *lines;
+    const int4 *ext;
+    int kx;
+    struct Line {
+        const cplx<T> *b;
+        int e;
+    };
+    __device__ __forceinline__ Line line(long long q) const {
+        const int o = lines[q];
+        return Line{p + (long long)o * K * inner, ext[o / kx].y};
+    }
+    __device__ __forceinline__ const cplx<T> *row(const Line &ln, int l) const {
+        const int n = (l < M / 2) ? l : l - M;
+        return (n >= -ln.e && n <= ln.e) ? ln.b + (long long)(n + s) * inner : nullptr;
+    }
 };
 
 __device__ __forceinline__ void cp_async_elem(void *sdst, const void *gsrc, int bytes, bool ok) {
@@ -353,9 +390,9 @@ __device__ __forceinline__ void cp_async_elem(void *sdst, const void *gsrc, int 
         asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(ok ? 16 : 0));
 }
 
-template <typename T, int L, int DIR, class ST>
+template <typename T, int L, int DIR, class SRC, class ST>
 __global__ void __launch_bounds__(PipeCfg<T, L>::NT)
-    k_fft2_pass_pipe(const cplx<T> *src, ST st, PassGeom g, const cplx<T> *__restrict__ tw) {
+    k_fft2_pass_pipe(SRC src, ST st, PassGeom g, const cplx<T> *__restrict__ tw) {
     using PC = PipeCfg<T, L>;
     using X = XchgLayout<L, true, PC::B>;
     constexpr int R1 = X::R1, R2 = X::R2, B = PC::B, NT = PC::NT;
@@ -367,14 +404,16 @@ __global__ void __launch_bounds__(PipeCfg<T, L>::NT)
     const long long tpo = (g.n_inner + B - 1) / B;
     const long long ntiles = g.n_outer * tpo;
     // element e of a tile (row e / B, column e % B), NT at a time
+    // rows the source does not hold (pruned rows) are zero-filled: cp.async with no source bytes
     auto prefetch = [&](long long tile, cplx<T> *dst) {
         const long long o = tile / tpo, i0 = (tile - o * tpo) * B;
+        const typename SRC::Line ln = src.line(o);
 #pragma unroll 4
         for (int e = threadIdx.x; e < L * B; e += NT) {
             const int l = e / B, c = e - l * B;
-            const bool ok = (i0 + c) < g.n_inner;
-            const long long off = (o * L + l) * g.n_inner + (ok ? i0 + c : 0);
-            cp_async_elem(dst + e, src + off, (int)sizeof(cplx<T>), ok);
+            const cplx<T> *row = src.row(ln, l);
+            const bool ok = (i0 + c) < g.n_inner && row != nullptr;
+            cp_async_elem(dst + e, ok ? row + i0 + c : src.p, (int)sizeof(cplx<T>), ok);
         }
         asm volatile("cp.async.commit_group;\n" ::);
     };
@@ -404,10 +443,10 @@ __global__ void __launch_bounds__(PipeCfg<T, L>::NT)
     asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
-template <typename T, int L, int DIR, class ST>
-inline cudaError_t launch_fft2_pipe(const cplx<T> *src, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
+template <typename T, int L, int DIR, class SRC, class ST>
+inline cudaError_t launch_fft2_pipe(SRC src, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
     using PC = PipeCfg<T, L>;
-    auto kern = k_fft2_pass_pipe<T, L, DIR, ST>;
+    auto kern = k_fft2_pass_pipe<T, L, DIR, SRC, ST>;
     const size_t smem = PC::smem();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -507,7 +546,14 @@ template <typename T, int L, int DIR, class LD, class ST>
 inline cudaError_t launch_fft2_L(LD ld, ST st, PassGeom g, const cplx<T> *tw, cudaStream_t stream) {
     if constexpr (IsLdArr<LD>::value) {
         // plain strided source: the pipelined pass (LdArr's inner stride is the pass's own)
-        if (g.n_inner > 1 && ld.inner == g.n_inner && ld.L == L) return launch_fft2_pipe<T, L, DIR>(ld.p, st, g, tw, stream);
+        if (g.n_inner > 1 && ld.inner == g.n_inner && ld.L == L)
+            return launch_fft2_pipe<T, L, DIR>(PipeArr<T>{ld.p, ld.L, ld.inner}, st, g, tw, stream);
+    }
+    if constexpr (std::is_same<LD, LdRowsCompactL<T>>::value) {
+        // the chain's pruned inverse y pass: compact rows, zero outside the shell's extent
+        if (g.n_inner > 1 && ld.inner == g.n_inner && ld.M == L)
+            return launch_fft2_pipe<T, L, DIR>(PipeRowsCompactL<T>{ld.p, ld.K, ld.M, ld.s, ld.inner, ld.lines, ld.ext, ld.kx},
+                                               st, g, tw, stream);
     }
     if (g.n_inner == 1) {
         using CF = Fft2Cfg<T, L, false>;

@@ -301,9 +301,10 @@ __global__ void k_pair_sum_items(const int *istart, const double2 *part, int ns_
 // Loader for the first inverse pass (along x) of
 //   xi(x) = (1/V) sum_k (f1 conj f2 - S C(k)) / W(k)^2 e^{ikx}   (field.hpp:1116-1160)
 // synthesising the k-space input from the half spectrum on the fly.
-template <typename T>
+// SE: the spectrum's element type (an FP32 field may read the FP64 density directly).
+template <typename T, typename SE = T>
 struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), separable tables
-    Spec<T> f;
+    Spec<SE> f;
     int n2;
     XiTabs xt;
     double S;
@@ -326,9 +327,9 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
 
 // The same spectrum as a complex field on the full grid (for k_synth: x = l, (y, z) = i), on
 // meshes whose correlation field is transformed whole (k_xi_fold)
-template <typename T>
+template <typename T, typename SE = T>
 struct LdXiHatFull {
-    LdXiHat<T> h;
+    LdXiHat<T, SE> h;
     __device__ __forceinline__ cplx<T> operator()(long long, int l, long long i) const {
         const unsigned ui = (unsigned)i;
         const int iy = (int)(ui / (unsigned)h.n2), iz = (int)(ui - (unsigned)iy * (unsigned)h.n2);
@@ -348,6 +349,23 @@ __global__ void k_synth_pairs(LD ld, int n0, int n1, int nh, cplx<T> *out) {
         int ix, iy, j;
         split3((unsigned)idx, (unsigned)n1, (unsigned)nh, ix, iy, j);
         out[idx] = mk<T>(ld.value(ix, iy, 2 * j), ld.value(ix, iy, 2 * j + 1));
+    }
+}
+
+// k_synth_pairs by mirror pairs of rows: the kz >= n2/2 + 1 half of row (x, y) is the
+// conjugate of the other row's (-x, -y) lower half, so a CTA that writes both rows of a pair
+// reads every spectrum element from HBM once (the pair's second read of it comes from the
+// cache) instead of twice.  Grid (n1, n0/2 + 1): CTA (y, x) takes row (x, y) and its mirror;
+// on the planes x = 0 and x = n0/2, which are their own mirrors, only y <= n1/2.
+template <typename T, class LD>
+__global__ void k_synth_pairs_rows(LD ld, int n0, int n1, int nh, cplx<T> *out) {
+    const int ix = blockIdx.y, iy = blockIdx.x;
+    if ((ix == 0 || 2 * ix == n0) && 2 * iy > n1) return;  // counted as the mirror of y' < n1/2
+    const int mx = (n0 - ix) % n0, my = (n1 - iy) % n1;
+    const long long r = (long long)ix * n1 + iy, m = (long long)mx * n1 + my;
+    for (int j = threadIdx.x; j < nh; j += blockDim.x) {
+        out[r * nh + j] = mk<T>(ld.value(ix, iy, 2 * j), ld.value(ix, iy, 2 * j + 1));
+        if (m != r) out[m * nh + j] = mk<T>(ld.value(mx, my, 2 * j), ld.value(mx, my, 2 * j + 1));
     }
 }
 

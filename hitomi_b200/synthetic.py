@@ -53,7 +53,7 @@ def lognormal_box(n_target: float, boxsize: float = 1000.0, ngrid: int = 256, am
     white = rng.standard_normal((ng, ng, ng))
     wk = np.fft.rfftn(white)
     dk = wk * np.sqrt(pk * ng ** 3 / vol)
-    delta_g = np.fft.irfftn(dk, s=(ng, ng, ng))
+    delta_g = np.fft.irfftn(dk, s=(ng, ng, ng), axes=(0, 1, 2))
     sig2 = float(np.var(delta_g))
     delta_ln = np.exp(delta_g - 0.5 * sig2) - 1.0
     cell = boxsize / ng
@@ -72,7 +72,7 @@ def lognormal_box(n_target: float, boxsize: float = 1000.0, ngrid: int = 256, am
     # Zel'dovich displacement Psi(k) = i k / k^2 delta_G(k), z component only
     with np.errstate(divide="ignore", invalid="ignore"):
         psi_k = np.where(k2 > 0, 1j * kz / k2, 0.0) * dk
-    psi_z = np.fft.irfftn(psi_k, s=(ng, ng, ng)).ravel()
+    psi_z = np.fft.irfftn(psi_k, s=(ng, ng, ng), axes=(0, 1, 2)).ravel()
     pos[:, 2] += f_growth * psi_z[idx]
     pos %= boxsize
     pos[pos >= boxsize] -= boxsize  # guard the round-up of x % L == L
