@@ -2,7 +2,9 @@
 //
 //   AxisTabs        per-axis sinc / sine tables with the reference's window index quirk
 //   Spec<T>         read access to a half or full spectrum
-//   k_pk_bin        binned  (f1 conj f2 - S C(k)) / W^2 * Yhat_lm(k)  (field.hpp:765-852)
+//   k_pk_bin_list   binned  (f1 conj f2 - S C(k)) / W^2 * Yhat_lm(k)  (field.hpp:765-852)
+//                   over the in-bin modes (k_pk_modes_*, once per context)
+//   k_pk_bin        the same over the whole mode cube (the allocation-free entry point)
 #pragma once
 
 #include "hg_common.cuh"
@@ -137,6 +139,8 @@ __device__ __forceinline__ double group_sum(double v, unsigned grp) {
     return s;
 }
 
+// P binning (as k_pk_bin_list below) over the whole mode cube [lo, lo + cnt), without a mode
+// list: the allocation-free entry point's (hg_static.cu), which has no room to keep one.
 // Whole warps walk the mode cube together (every lane runs every iteration, so full-warp
 // intrinsics are safe); lanes whose modes fall in the same bin pool their values through
 // shuffles and one of them adds the pooled value to the block's shared-memory bins, which
@@ -207,6 +211,139 @@ __global__ void k_pk_bin(F1 f1, F2 f2, Grid g, AxisTabs tabs, int3 lo, int3 cnt,
         }
         if (b.x >= 0 && lx) atomicAdd(&scnt[b.x], (unsigned long long)__popc(gx));
         if (b.y >= 0 && ly) atomicAdd(&scnt[b.y], (unsigned long long)__popc(gy));
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x)
+        if (sacc[q] != 0.0) atomicAdd(&acc[q], sacc[q]);
+    for (int q = threadIdx.x; q < nbin; q += blockDim.x)
+        if (scnt[q]) atomicAdd(&nmode[q], scnt[q]);
+}
+
+// The P-binning cube's modes that fall in some bin, with what the binning needs of each that
+// does not depend on the field (its array indices, bins, C(k), W(k), k), built once per
+// context: each binning then reads the spectrum at those modes only (k_pk_bin_list).
+struct PkMode {
+    int ix, iy, iz;
+    int2 b;
+    double C, wf;
+    double kv[3];
+};
+
+// Mode idx of the cube [lo, lo + cnt) of wrapped modes: array indices, k (the reference's FP64
+// expressions, kmag_exact) and the bins of the fine index int(|k| / 1e-4 + 0.5) through lut.
+__device__ __forceinline__ int2 pk_mode_at(const Grid &g, int3 lo, int3 cnt, const int2 *lut, int lutn, long long idx,
+                                           int &ix, int &iy, int &iz, double kv[3]) {
+    int nx, ny, nz;
+    split3((unsigned)idx, (unsigned)cnt.y, (unsigned)cnt.z, nx, ny, nz);
+    nx += lo.x;
+    ny += lo.y;
+    nz += lo.z;
+    ix = nx < 0 ? nx + g.n[0] : nx;
+    iy = ny < 0 ? ny + g.n[1] : ny;
+    iz = nz < 0 ? nz + g.n[2] : nz;
+    kv[0] = kcomp(wrap_index(ix, g.n[0]), g.dk[0]);
+    kv[1] = kcomp(wrap_index(iy, g.n[1]), g.dk[1]);
+    kv[2] = kcomp(wrap_index(iz, g.n[2]), g.dk[2]);
+    const double kmag = kmag_exact(kv[0], kv[1], kv[2]);
+    const int kindex = (int)__dadd_rn(__ddiv_rn(kmag, 0.0001), 0.5);
+    return (kindex < lutn) ? lut[kindex] : make_int2(-1, -1);
+}
+
+// flag[idx] = 1 when mode idx falls in a bin
+__global__ void k_pk_modes_flag(Grid g, int3 lo, int3 cnt, const int2 *lut, int lutn, unsigned *flag) {
+    const long long total = (long long)cnt.x * cnt.y * cnt.z;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        double kv[3];
+        flag[idx] = pk_mode_at(g, lo, cnt, lut, lutn, idx, ix, iy, iz, kv).x >= 0 ? 1u : 0u;
+    }
+}
+
+// the flagged modes at their exclusive-scan positions (cube order)
+__global__ void k_pk_modes_fill(Grid g, AxisTabs tabs, int3 lo, int3 cnt, const int2 *lut, int lutn, int assign,
+                                int wpow, const unsigned *pos, PkMode *out) {
+    const long long total = (long long)cnt.x * cnt.y * cnt.z;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        PkMode m;
+        m.b = pk_mode_at(g, lo, cnt, lut, lutn, idx, m.ix, m.iy, m.iz, m.kv);
+        if (m.b.x < 0) continue;
+        m.C = shot_tab(tabs, m.ix, m.iy, m.iz, assign);
+        m.wf = window_tab(tabs, m.ix, m.iy, m.iz, wpow);
+        out[pos[idx]] = m;
+    }
+}
+
+// Binned (f1 conj f2 - S C(k)) / W^2 * Yhat_lm(k) over the mode list (field.hpp:765-852);
+// acc: [nbin][nlm] complex, nmode: [nbin].  Whole warps walk the list together (every lane
+// runs every iteration, so full-warp intrinsics are safe); lanes whose modes fall in the same
+// bin pool their values through shuffles and one of them adds the pooled value to the
+// block's shared-memory bins, which keeps the number of (serialising) FP64 shared-memory
+// atomics near one per bin per warp step instead of one per mode.
+template <class F1, class F2>
+__global__ void k_pk_bin_list(F1 f1, F2 f2, const PkMode *modes, long long nmodes, int nbin, LMList lms, double S_re,
+                              double S_im, double *acc, unsigned long long *nmode, int k0_special, double k0_re,
+                              double k0_im) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sacc = reinterpret_cast<double *>(smem_raw);
+    unsigned long long *scnt = reinterpret_cast<unsigned long long *>(sacc + 2 * nbin * lms.n);
+    for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x) sacc[q] = 0.0;
+    for (int q = threadIdx.x; q < nbin; q += blockDim.x) scnt[q] = 0ull;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const long long wstride = (long long)gridDim.x * blockDim.x;
+    for (long long wbase = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); wbase < nmodes; wbase += wstride) {
+        const long long e = wbase + lane;
+        int2 b = make_int2(-1, -1);
+        zd pk2 = mk<double>(0.0, 0.0);
+        double kv[3] = {0.0, 0.0, 0.0};
+        if (e < nmodes) {
+            const PkMode m = modes[e];
+            b = m.b;
+            kv[0] = m.kv[0];
+            kv[1] = m.kv[1];
+            kv[2] = m.kv[2];
+            const zd d1 = f1.at(m.ix, m.iy, m.iz), d2 = f2.at(m.ix, m.iy, m.iz);
+            if (k0_special && m.ix == 0 && m.iy == 0 && m.iz == 0) {
+                pk2 = mk<double>(k0_re, k0_im);
+            } else {
+                pk2 = mul_conj_rn(d1, d2);
+            }
+            pk2 = pk2 - mk<double>(S_re * m.C, S_im * m.C);
+            const double w2 = m.wf * m.wf;
+            pk2 = mk<double>(pk2.x / w2, pk2.y / w2);
+        }
+        // the list runs in cube order, so a warp's modes share one or two bins: per distinct
+        // bin, a butterfly sum over the warp (log 32 shuffles, not one per member)
+        const int nq = lms.n > 0 ? lms.n : 1;  // (the mode counts are added in pass q = 0)
+        for (int q = 0; q < nq; q++) {
+            zd v = mk<double>(0.0, 0.0);
+            if (q < lms.n && b.x >= 0) v = pk2 * ylm_reduced(lms.lm[q].l, lms.lm[q].m, kv[0], kv[1], kv[2]);
+            for (int side = 0; side < 2; side++) {
+                const int mine = side ? b.y : b.x;
+                unsigned rem = __ballot_sync(0xffffffffu, mine >= 0);
+                while (rem) {
+                    const int u = __shfl_sync(0xffffffffu, mine, __ffs(rem) - 1);
+                    const bool in = (mine == u);
+                    const unsigned grp = __ballot_sync(0xffffffffu, in);
+                    double sr = in ? v.x : 0.0, si = in ? v.y : 0.0;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                        si += __shfl_xor_sync(0xffffffffu, si, o);
+                    }
+                    if (lane == 0 && HG_IN_BOUNDS(u < nbin, HG_SITE_BIN, u)) {
+                        if (q < lms.n) {
+                            atomicAdd(&sacc[2 * (u * lms.n + q)], sr);
+                            atomicAdd(&sacc[2 * (u * lms.n + q) + 1], si);
+                        }
+                        if (q == 0) atomicAdd(&scnt[u], (unsigned long long)__popc(grp));
+                    }
+                    rem &= ~grp;
+                }
+            }
+        }
     }
     __syncthreads();
     for (int q = threadIdx.x; q < 2 * nbin * lms.n; q += blockDim.x)

@@ -223,6 +223,8 @@ struct Engine : public hg_ctx {
 
     // binning scratch
     DBuf bin_acc, bin_cnt;
+    DBuf pk_modes;             // the binning cube's in-bin modes (PkMode), built on first use
+    long long n_pk_modes = -1;
 
     // bispectrum state (geometry: built once per context)
     struct ShellSet {
@@ -1114,13 +1116,18 @@ struct Engine : public hg_ctx {
         HG_CK(cudaMemsetAsync(bin_acc.p, 0, sizeof(double) * 2 * nbin * L.n, st));
         HG_CK(cudaMemsetAsync(bin_cnt.p, 0, sizeof(unsigned long long) * nbin, st));
         size_t smem = sizeof(double) * 2 * nbin * L.n + sizeof(unsigned long long) * nbin;
-        HG_CK(cudaFuncSetAttribute(k_pk_bin<T, F1, Spec<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        long long total = (long long)cn.x * cn.y * cn.z;
-        unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 8);
-        kb("pk_bin", double(total) * sizeof(C));
-        k_pk_bin<T, F1, Spec<T>><<<blocks, 256, smem, st>>>(f1, f2, g, tabs, lo, cn, dp<int2>(lut), lutn, nbin, L,
-                                               S_re, S_im, cfg.assign, wpow, dp<double>(bin_acc),
-                                               dp<unsigned long long>(bin_cnt), 0, 0.0, 0.0);
+        if (n_pk_modes < 0) build_pk_modes(lo, cn);
+        HG_CK(cudaFuncSetAttribute(k_pk_bin_list<F1, Spec<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // one resident wave (a partial second wave was a third of the kernel's time)
+        int per_sm = 1, sms = 148;
+        HG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pk_bin_list<F1, Spec<T>>, 256, smem));
+        HG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg.device));
+        const unsigned blocks =
+            (unsigned)std::max<long long>(1, std::min<long long>(grid1(n_pk_modes, 256), (long long)sms * std::max(per_sm, 1)));
+        kb("pk_bin", double(n_pk_modes) * (sizeof(PkMode) + 2.0 * sizeof(C)));
+        k_pk_bin_list<F1, Spec<T>><<<blocks, 256, smem, st>>>(f1, f2, dp<PkMode>(pk_modes), n_pk_modes, nbin, L, S_re,
+                                                              S_im, dp<double>(bin_acc), dp<unsigned long long>(bin_cnt),
+                                                              0, 0.0, 0.0);
         ke();
         std::vector<double> a(2 * nbin * L.n);
         nm.assign(nbin, 0);
@@ -1135,6 +1142,31 @@ struct Engine : public hg_ctx {
                     avg[2 * (j * L.n + q) + 1] = a[2 * (j * L.n + q) + 1] / double(nm[j]);
                 }
             }
+    }
+
+    // The binning cube's modes that fall in a bin (k_pk_modes_*), in cube order, once per context.
+    void build_pk_modes(int3 lo, int3 cn) {
+        const long long total = (long long)cn.x * cn.y * cn.z;
+        DBuf flag, pos;
+        HG_CK(flag.ensure(sizeof(unsigned) * (total + 1)));
+        HG_CK(pos.ensure(sizeof(unsigned) * (total + 1)));
+        HG_CK(cudaMemsetAsync(flag.p, 0, sizeof(unsigned) * (total + 1), st));
+        const unsigned blocks = (unsigned)std::min<long long>(grid1(total, 256), 148 * 8);
+        k_pk_modes_flag<<<blocks, 256, 0, st>>>(g, lo, cn, dp<int2>(lut), lutn, dp<unsigned>(flag));
+        HG_CK(cudaGetLastError());
+        size_t tb = 0;
+        HG_CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, dp<unsigned>(flag), dp<unsigned>(pos), total + 1, st));
+        HG_CK(cubtmp.ensure(tb));
+        HG_CK(cub::DeviceScan::ExclusiveSum(cubtmp.p, tb, dp<unsigned>(flag), dp<unsigned>(pos), total + 1, st));
+        unsigned nm = 0;
+        HG_CK(cudaMemcpyAsync(&nm, dp<unsigned>(pos) + total, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        HG_CK(cudaStreamSynchronize(st));
+        HG_CK(pk_modes.ensure(sizeof(PkMode) * std::max<unsigned>(nm, 1)));
+        k_pk_modes_fill<<<blocks, 256, 0, st>>>(g, tabs, lo, cn, dp<int2>(lut), lutn, cfg.assign, wpow,
+                                                dp<unsigned>(pos), dp<PkMode>(pk_modes));
+        HG_CK(cudaGetLastError());
+        HG_CK(cudaStreamSynchronize(st));  // flag and pos are released on return
+        n_pk_modes = nm;
     }
 
     // averages over each k bin of sum_q w_q (F_q conj f2 - S_q C) / W^2 Yhat_{l_q m_q}
@@ -1741,7 +1773,7 @@ struct Engine : public hg_ctx {
 
     // Box correlation field after its x and y inverse passes (cached per catalogue).  Its
     // spectrum P is real, so the even and odd kz planes travel as the real and imaginary
-    // parts of one complex field (k_synth_pairs: [n0][n1][n2/2] in xi): half the data
+    // parts of one complex field (k_synth_pairs_rows: [n0][n1][n2/2] in xi): half the data
     // through the x and y passes; the histogram kernel separates them before its z pass.
     // k0prod: (f1 conj f2)(k = 0), delta0 N0 for the bispectrum shot noise (dn against the
     // density N, bispec.hpp:913-921), delta0^2 for the 2PCF (dn against itself)
@@ -1775,7 +1807,8 @@ struct Engine : public hg_ctx {
         const long long yz = (long long)n1 * nh, tot = (long long)n0 * yz;
         const int bs = (int)std::min<long long>(256, (nh + 31) / 32 * 32);
         kb("xi_synth", double(tot) * (sizeof(C) + sizeof(cplx<SE>)));
-        k_synth_pairs_rows<T, LdXiHat<T, SE>><<<dim3(n1, n0 / 2 + 1), bs, 0, st>>>(ld, n0, n1, nh, dp<C>(xi));
+        HG_REQUIRE(f.half, "the box correlation field is synthesised from a half spectrum");
+        k_synth_pairs_rows<T, SE><<<dim3(n1, n0 / 2 + 1), bs, 0, st>>>(ld, n0, n1, nh, dp<C>(xi));
         ke();
         pass<+1>(n0, LdArr<T>{dp<C>(xi), n0, yz}, StArr<T>{dp<C>(xi), n0, yz}, 1, yz, "fft_xi_x");
         pass<+1>(n1, LdArr<T>{dp<C>(xi), n1, nh}, StArr<T>{dp<C>(xi), n1, nh}, n0, nh, "fft_xi_y");

@@ -341,7 +341,9 @@ struct PipeCfg {
     // within the 227 KB a CTA may hold (at 512 points 4 columns, three CTAs per SM instead of
     // one, measured slower: the FP64 density transform 1.83 -> 2.45 ms)
     // FP32 lines of 256 and 512 points take 16 columns (128-byte row segments; the FP32
-    // correlation-field passes at 512 points 0.34 -> 0.25 ms each against 8 columns)
+    // correlation-field passes at 512 points 0.34 -> 0.25 ms each against 8 columns).  (A
+    // 192-point FP64 variant with 16 threads and 12 values per thread per line, twice the
+    // warps per SM, was slower on the chain's y passes: 2.26 -> 2.34 ms per mock.)
     static constexpr int B = (L >= 1024 && sizeof(T) == 8) ? 4
                            : (L >= 256 && sizeof(T) == 8) ? 8
                            : (L >= 1024) ? 8 : 16;

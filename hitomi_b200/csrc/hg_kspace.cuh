@@ -1,7 +1,7 @@
 // hg_kspace.cuh -- k-space and configuration-space kernels of the estimators.
 //
 //   k_axis_tables   per-axis sinc / sine tables with the reference's window index quirk
-//   k_pk_bin        binned  (f1 conj f2 - S C(k)) / W^2 * Yhat_lm(k)  (field.hpp:765-852)
+//   (P binning: k_pk_bin_list, hg_bin.cuh)
 //   k_shell_D       delta(k)/W(k) for every (shell, mode) entry      (field.hpp:346-401)
 //   k_family_A      A_f,i(k) = Yhat_f(k) delta/W / n_i
 //   k_scatter_*     place k-space inputs on the compact shell / G cubes
@@ -318,6 +318,26 @@ struct LdXiHat {  // (|delta|^2 - S C(k)) / W(k)^2 / V  (field.hpp:1000-1020), s
             zd d = f.at(ix, iy, iz);
             p2 = d.x * d.x + d.y * d.y;
         }
+        return value_p2(ix, iy, iz, p2);
+    }
+    // the (x, y) factors of C, the interlaced image sum and 1 / W^2 (products formed in the same
+    // order as value_p2, so value_xyz gives identical values)
+    struct XY {
+        double c, d, iw;
+    };
+    __device__ __forceinline__ XY xy(int ix, int iy) const {
+        return XY{xt.cf[0][ix] * xt.cf[1][iy], xt.interlace ? xt.df[0][ix] * xt.df[1][iy] : 0.0,
+                  xt.iw2[0][ix] * xt.iw2[1][iy]};
+    }
+    __device__ __forceinline__ T value_xyz(const XY &a, bool k0mode, int iz, cplx<SE> e) const {
+        const double dx = (double)e.x, dy = (double)e.y;
+        const double p2 = k0mode ? k0 : dx * dx + dy * dy;
+        double C = a.c * xt.cf[2][iz];
+        if (xt.interlace) C = 0.5 * (C + a.d * xt.df[2][iz]);
+        const double iw = a.iw * xt.iw2[2][iz];
+        return (T)(invV * ((p2 - S * C) * iw));
+    }
+    __device__ __forceinline__ T value_p2(int ix, int iy, int iz, double p2) const {
         double C = xt.cf[0][ix] * xt.cf[1][iy] * xt.cf[2][iz];
         if (xt.interlace) C = 0.5 * (C + xt.df[0][ix] * xt.df[1][iy] * xt.df[2][iz]);
         double iw = xt.iw2[0][ix] * xt.iw2[1][iy] * xt.iw2[2][iz];
@@ -340,32 +360,32 @@ struct LdXiHatFull {
 // The real correlation-field spectrum P of the box, two kz columns per complex value:
 // out[ix][iy][j] = P(ix, iy, 2j) + i P(ix, iy, 2j + 1)  ([n0][n1][n2/2]).  A complex
 // transform of these lines along x and y gives both planes' transforms at once; the
-// histogram kernel separates them.
-template <typename T, class LD>
-__global__ void k_synth_pairs(LD ld, int n0, int n1, int nh, cplx<T> *out) {
-    const long long total = (long long)n0 * n1 * nh;
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        int ix, iy, j;
-        split3((unsigned)idx, (unsigned)n1, (unsigned)nh, ix, iy, j);
-        out[idx] = mk<T>(ld.value(ix, iy, 2 * j), ld.value(ix, iy, 2 * j + 1));
-    }
-}
-
-// k_synth_pairs by mirror pairs of rows: the kz >= n2/2 + 1 half of row (x, y) is the
+// histogram kernel separates them.  By mirror pairs of rows: the kz >= n2/2 + 1 half of row (x, y) is the
 // conjugate of the other row's (-x, -y) lower half, so a CTA that writes both rows of a pair
 // reads every spectrum element from HBM once (the pair's second read of it comes from the
 // cache) instead of twice.  Grid (n1, n0/2 + 1): CTA (y, x) takes row (x, y) and its mirror;
-// on the planes x = 0 and x = n0/2, which are their own mirrors, only y <= n1/2.
-template <typename T, class LD>
-__global__ void k_synth_pairs_rows(LD ld, int n0, int n1, int nh, cplx<T> *out) {
+// on the planes x = 0 and x = n0/2, which are their own mirrors, only y <= n1/2.  A thread's
+// four spectrum elements are addressed first and loaded together.
+template <typename T, typename SE>
+__global__ void k_synth_pairs_rows(LdXiHat<T, SE> ld, int n0, int n1, int nh, cplx<T> *out) {
     const int ix = blockIdx.y, iy = blockIdx.x;
     if ((ix == 0 || 2 * ix == n0) && 2 * iy > n1) return;  // counted as the mirror of y' < n1/2
     const int mx = (n0 - ix) % n0, my = (n1 - iy) % n1;
     const long long r = (long long)ix * n1 + iy, m = (long long)mx * n1 + my;
+    const int n2 = 2 * nh, hz = nh + 1;
+    const cplx<SE> *Hr = ld.f.p + r * hz, *Hm = ld.f.p + m * hz;
+    const typename LdXiHat<T, SE>::XY ar = ld.xy(ix, iy), am = ld.xy(mx, my);
+    const bool r0 = (ix == 0 && iy == 0), m0 = (mx == 0 && my == 0);
     for (int j = threadIdx.x; j < nh; j += blockDim.x) {
-        out[r * nh + j] = mk<T>(ld.value(ix, iy, 2 * j), ld.value(ix, iy, 2 * j + 1));
-        if (m != r) out[m * nh + j] = mk<T>(ld.value(mx, my, 2 * j), ld.value(mx, my, 2 * j + 1));
+        const int k0 = 2 * j, k1 = 2 * j + 1;
+        // kz < hz from the row itself, else (conjugated) from the mirror row at n2 - kz
+        const cplx<SE> *pa0 = (k0 < hz) ? Hr + k0 : Hm + (n2 - k0);
+        const cplx<SE> *pa1 = (k1 < hz) ? Hr + k1 : Hm + (n2 - k1);
+        const cplx<SE> *pb0 = (k0 < hz) ? Hm + k0 : Hr + (n2 - k0);
+        const cplx<SE> *pb1 = (k1 < hz) ? Hm + k1 : Hr + (n2 - k1);
+        const cplx<SE> a0 = *pa0, a1 = *pa1, b0 = *pb0, b1 = *pb1;
+        out[r * nh + j] = mk<T>(ld.value_xyz(ar, r0 && k0 == 0, k0, a0), ld.value_xyz(ar, false, k1, a1));
+        if (m != r) out[m * nh + j] = mk<T>(ld.value_xyz(am, m0 && k0 == 0, k0, b0), ld.value_xyz(am, false, k1, b1));
     }
 }
 
@@ -471,9 +491,18 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
     static_assert(B == 8, "two orbits of four representative lines per CTA");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *s = reinterpret_cast<cplx<T> *>(smem_raw);
+    // the CTA's two orbits: their representative lines (with mirrors) and n_x^2 + n_y^2,
+    // read once (the histogram phase consults them for every cell)
+    __shared__ int2 reps[8];
+    __shared__ int n2o[2];
+    if (threadIdx.x < 8) {
+        const int orb = 2 * blockIdx.x + (threadIdx.x >> 2);
+        reps[threadIdx.x] = (orb < n_orbits) ? orbit_reps[4 * orb + (threadIdx.x & 3)] : make_int2(-1, -1);
+        if ((threadIdx.x & 3) == 0) n2o[threadIdx.x >> 2] = (orb < n_orbits) ? orbit_n2xy[orb] : 0;
+    }
+    __syncthreads();
     const int b = threadIdx.x / R2, t = threadIdx.x % R2;
-    const int orb_b = 2 * blockIdx.x + (b >> 2);
-    const int2 rep = (orb_b < n_orbits) ? orbit_reps[4 * orb_b + (b & 3)] : make_int2(-1, -1);
+    const int2 rep = reps[b];
     const int line = rep.x, mirror = rep.y;
     // xi holds Z = A + i B ([n0][n1][L/2]) after the x and y passes, A and B the transforms
     // of the even and odd kz planes of the real spectrum: A(x) = (Z(x) + conj Z(-x)) / 2,
@@ -507,7 +536,7 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
         const int iz2 = (L - iz) % L;
         double er = 0, ei = 0, orr = 0, oi = 0;
         for (int bb = 4 * o; bb < 4 * o + 4; bb++) {
-            const int2 rb = orbit_reps[4 * orb + (bb & 3)];
+            const int2 rb = reps[bb];
             if (rb.x < 0) continue;
             const cplx<T> a = s[bb * LP + iz];
             const cplx<T> c = (iz2 == iz) ? mk<T>(0, 0) : s[bb * LP + iz2];
@@ -525,7 +554,7 @@ __global__ void __launch_bounds__(OrbitCfg<T, L>::NT)
             orr = er;
             oi = ei;
         }
-        const int n2xy = orbit_n2xy[orb];
+        const int n2xy = n2o[o];
         int wz = wrap_index(iz, L);
         long long n2 = (long long)n2xy + (long long)wz * wz;
         const double r = sqrt((double)n2);
@@ -687,13 +716,20 @@ __global__ void k_bessel_table_r(const double *sy, const double *sc, int sn, dou
 }
 
 // out[i1][i2] = sum_n2 J1[i1][n2] J2[i2][n2] hist[n2], as a skinny product J1 diag(h) J2^T.
-// Persistent blocks walk chunks of HG_SN_CHUNK values of n2; each chunk stages J1 and
-// J2 * hist (complex) in shared memory; a thread owns a 4 x 4 register tile of (i1, i2)
-// and one residue class of the chunk; residue groups are summed in shared memory and
-// each block writes its na x nb partial sums; k_sum_parts adds the partials in a fixed
-// order (deterministic).
+// Persistent blocks walk chunks of HG_SN_CHUNK values of n2; each chunk's J1 rows, J2 rows and
+// hist values stream into shared memory by cp.async (two stages: the next chunk loads while
+// the current one is summed); a thread owns a 4 x 4 register tile of (i1, i2) and one residue
+// class of the chunk; residue groups are summed in shared memory and each block writes its
+// na x nb partial sums; k_sum_parts adds the partials in a fixed order (deterministic).
 #define HG_SN_CHUNK 64
 #define HG_SN_THREADS 256
+// doubles of one stage: J1 and J2 rows (row r at r CHP + r / 4: one extra slot per tile of
+// four rows puts the rows that a warp's tiles read at the same c on different banks), hist
+__host__ __device__ inline int sn_off_b(int na4) { return 4 * na4 * (HG_SN_CHUNK + 1) + na4; }
+__host__ __device__ inline int sn_off_h(int na4, int nb4) {  // even: the hist values are read as double2
+    return (sn_off_b(na4) + 4 * nb4 * (HG_SN_CHUNK + 1) + nb4 + 1) & ~1;
+}
+__host__ __device__ inline int sn_stage_doubles(int na4, int nb4) { return sn_off_h(na4, nb4) + 2 * HG_SN_CHUNK; }
 __global__ void __launch_bounds__(HG_SN_THREADS)
     k_sn_partial(const double *__restrict__ J1, int na, const double *__restrict__ J2, int nb,
                  const double *__restrict__ hist, long long n2dim, double *part) {
@@ -702,45 +738,65 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
     const int na4 = (na + 3) / 4, nb4 = (nb + 3) / 4;
     const int ntile = na4 * nb4;
     const int ngroup = max(1, HG_SN_THREADS / ntile);
-    // row r of a staged operand starts at r CHP + r / 4: one extra slot per tile of four rows
-    // puts the rows that a warp's tiles read at the same c on different banks
-    double2 *sb = reinterpret_cast<double2 *>(smem_raw);  // [4 nb4][CHP] (+ nb4)  J2 * h
-    double *sa = reinterpret_cast<double *>(sb + (size_t)4 * nb4 * CHP + nb4);  // [4 na4][CHP] (+ na4)  J1
+    const int SD = sn_stage_doubles(na4, nb4);
+    double *stage0 = reinterpret_cast<double *>(smem_raw);
     const int t = threadIdx.x;
+    // padding rows (na <= r < 4 na4) feed only the tiles' unused accumulators: zero them once
+    for (int e = t; e < 2 * SD; e += blockDim.x) stage0[e] = 0.0;
+    __syncthreads();
     const int tile = t % ntile, grp = t / ntile;
     const bool active = (t < ntile * ngroup);
     const int ta = tile / nb4, tb = tile % nb4;
+    const int offb = sn_off_b(na4), offh = sn_off_h(na4, nb4);
     double acc[4][4][2];
 #pragma unroll
     for (int u = 0; u < 4; u++)
 #pragma unroll
         for (int v = 0; v < 4; v++) acc[u][v][0] = acc[u][v][1] = 0.0;
     const long long nchunk = (n2dim + CH - 1) / CH;
-    for (long long ch = blockIdx.x; ch < nchunk; ch += gridDim.x) {
+    // chunk ch into stage buf: values past n2dim are zero-filled (no source bytes)
+    auto prefetch = [&](long long ch, double *buf) {
         const long long n0 = ch * CH;
-        __syncthreads();
-        for (int e = t; e < 4 * na4 * CH; e += blockDim.x) {
-            int r = e / CH, c = e % CH;
-            bool ok = (r < na) && (n0 + c < n2dim);
-            sa[r * CHP + (r >> 2) + c] = ok ? J1[(long long)r * n2dim + n0 + c] : 0.0;
+        for (int e = t; e < na * CH; e += blockDim.x) {
+            const int r = e / CH, c = e - r * CH;
+            const bool ok = n0 + c < n2dim;
+            cp_async_elem(buf + r * CHP + (r >> 2) + c, J1 + (ok ? (long long)r * n2dim + n0 + c : 0), 8, ok);
         }
-        for (int e = t; e < 4 * nb4 * CH; e += blockDim.x) {
-            int r = e / CH, c = e % CH;
-            bool ok = (r < nb) && (n0 + c < n2dim);
-            double b = ok ? J2[(long long)r * n2dim + n0 + c] : 0.0;
-            double hr = ok ? hist[2 * (n0 + c)] : 0.0;
-            double hi = ok ? hist[2 * (n0 + c) + 1] : 0.0;
-            sb[r * CHP + (r >> 2) + c] = make_double2(b * hr, b * hi);
+        for (int e = t; e < nb * CH; e += blockDim.x) {
+            const int r = e / CH, c = e - r * CH;
+            const bool ok = n0 + c < n2dim;
+            cp_async_elem(buf + offb + r * CHP + (r >> 2) + c, J2 + (ok ? (long long)r * n2dim + n0 + c : 0), 8, ok);
         }
+        for (int e = t; e < 2 * CH; e += blockDim.x) {
+            const bool ok = n0 + (e >> 1) < n2dim;
+            cp_async_elem(buf + offh + e, hist + (ok ? 2 * n0 + e : 0), 8, ok);
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    int cur = 0;
+    long long ch = blockIdx.x;
+    if (ch < nchunk) prefetch(ch, stage0);
+    for (; ch < nchunk; ch += gridDim.x) {
+        const long long nx = ch + gridDim.x;
+        if (nx < nchunk) prefetch(nx, stage0 + (size_t)(cur ^ 1) * SD);
+        else asm volatile("cp.async.commit_group;\n" ::);  // one group per iteration
+        asm volatile("cp.async.wait_group 1;\n" ::);
         __syncthreads();
+        const double *sa = stage0 + (size_t)cur * SD;
+        const double *sj = sa + offb;
+        const double2 *sh = reinterpret_cast<const double2 *>(sa + offh);
         if (active) {
             for (int c = grp; c < CH; c += ngroup) {
                 double av[4];
                 double2 bv[4];
+                const double2 h = sh[c];
 #pragma unroll
                 for (int u = 0; u < 4; u++) av[u] = sa[(4 * ta + u) * CHP + ta + c];
 #pragma unroll
-                for (int v = 0; v < 4; v++) bv[v] = sb[(4 * tb + v) * CHP + tb + c];
+                for (int v = 0; v < 4; v++) {
+                    const double j = sj[(4 * tb + v) * CHP + tb + c];
+                    bv[v] = make_double2(j * h.x, j * h.y);
+                }
 #pragma unroll
                 for (int u = 0; u < 4; u++)
 #pragma unroll
@@ -750,7 +806,10 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
                     }
             }
         }
+        __syncthreads();  // this stage is the target of the prefetch two chunks on
+        cur ^= 1;
     }
+    asm volatile("cp.async.wait_group 0;\n" ::);
     __syncthreads();
     double2 *red = reinterpret_cast<double2 *>(smem_raw);
     for (int e = t; e < ntile * 16; e += blockDim.x) red[e] = make_double2(0.0, 0.0);
@@ -779,10 +838,10 @@ __global__ void __launch_bounds__(HG_SN_THREADS)
 
 #define HG_SN_MAXROWS 64  // rows per operand and launch (4 x 4 tiles, at most 256 of them)
 inline size_t sn_partial_smem(int na, int nb) {
-    const size_t na4 = (size_t)(na + 3) / 4, nb4 = (size_t)(nb + 3) / 4;
-    size_t stage = (sizeof(double2) * nb4 + sizeof(double) * na4) * (4 * (HG_SN_CHUNK + 1) + 1);
-    size_t red = sizeof(double2) * 16 * na4 * nb4;
-    return stage > red ? stage : red;
+    const int na4 = (na + 3) / 4, nb4 = (nb + 3) / 4;
+    size_t stages = sizeof(double) * 2 * (size_t)sn_stage_doubles(na4, nb4);
+    size_t red = sizeof(double2) * 16 * (size_t)na4 * nb4;
+    return stages > red ? stages : red;
 }
 inline int sn_partial_blocks(long long n2dim) {
     long long nchunk = (n2dim + HG_SN_CHUNK - 1) / HG_SN_CHUNK;
