@@ -547,16 +547,19 @@ __global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom 
         if (!df.pass) {
             // separable stencils meet at most 8 tiles: every counter atomic of the warp is
             // issued before any result is used, so their round trips overlap
+            // (and each tile's range start is read alongside, not after the atomic's return)
             int tq[8];
-            unsigned gq[8], bq[8];
+            unsigned gq[8], bq[8], oq[8];
 #pragma unroll
             for (int q = 0; q < 8; q++) {
                 tq[q] = -1;
                 gq[q] = 0u;
                 bq[q] = 0u;
+                oq[q] = 0u;
                 if (q < maxnt) {
                     tq[q] = (q < tl.n) ? tile_at(g, tl, slow, q) : -1;
                     gq[q] = __match_any_sync(0xffffffffu, tq[q]);
+                    if (tq[q] >= 0) oq[q] = __ldg(off + tq[q]);
                     if (tq[q] >= 0 && lane == __ffs(gq[q]) - 1) bq[q] = atomicAdd(&cursor[tq[q]], (unsigned)__popc(gq[q]));
                 }
             }
@@ -564,7 +567,7 @@ __global__ void __launch_bounds__(256, 3) k_bin_scatter(PartSrc src, AssignGeom 
             for (int q = 0; q < 8; q++) {
                 if (q < maxnt && tq[q] >= 0) {
                     const unsigned base = __shfl_sync(gq[q], bq[q], __ffs(gq[q]) - 1);
-                    const unsigned ri = off[tq[q]] + base + __popc(gq[q] & lt);
+                    const unsigned ri = oq[q] + base + __popc(gq[q] & lt);
                     if (HG_IN_BOUNDS(ri < off[tq[q] + 1], HG_SITE_RECORD, ri)) rec[ri] = r;
                 }
             }
@@ -888,6 +891,8 @@ __global__ void k_tile_accum(const PRec<T> *rec, const Chunk *ch, AssignGeom g, 
     auto add = [&](int li, T v, T vi) {
         if (!HG_IN_BOUNDS(li >= 0 && li < tcells, HG_SITE_TILE_CELL, li)) return;
         if (FIX64) {
+            // (rounding by adding 1.5 2^52 and taking the low word, without conversion
+            // instructions, was measured slower: 1.71 -> 1.85 ms per 512^3 mock)
             const double x = (double)v;
             const double hi = rint(x * 0x1p-40);
             const double r1 = x - hi * 0x1p40;  // exact

@@ -227,7 +227,14 @@ struct PkMode {
     int2 b;
     double C, wf;
     double kv[3];
+    zd y[3];  // Yhat_l0(k) for l = 0, 2, 4 (the box multipoles), as ylm_reduced gives them
 };
+
+// Yhat_lm(k) of a listed mode: the stored value for (l, 0), l = 0, 2, 4, else evaluated
+__device__ __forceinline__ zd pk_mode_ylm(const PkMode &m, int l, int mm) {
+    if (mm == 0 && (l == 0 || l == 2 || l == 4)) return m.y[l >> 1];
+    return ylm_reduced(l, mm, m.kv[0], m.kv[1], m.kv[2]);
+}
 
 // Mode idx of the cube [lo, lo + cnt) of wrapped modes: array indices, k (the reference's FP64
 // expressions, kmag_exact) and the bins of the fine index int(|k| / 1e-4 + 0.5) through lut.
@@ -271,6 +278,7 @@ __global__ void k_pk_modes_fill(Grid g, AxisTabs tabs, int3 lo, int3 cnt, const 
         if (m.b.x < 0) continue;
         m.C = shot_tab(tabs, m.ix, m.iy, m.iz, assign);
         m.wf = window_tab(tabs, m.ix, m.iy, m.iz, wpow);
+        for (int q = 0; q < 3; q++) m.y[q] = ylm_reduced(2 * q, 0, m.kv[0], m.kv[1], m.kv[2]);
         out[pos[idx]] = m;
     }
 }
@@ -297,13 +305,10 @@ __global__ void k_pk_bin_list(F1 f1, F2 f2, const PkMode *modes, long long nmode
         const long long e = wbase + lane;
         int2 b = make_int2(-1, -1);
         zd pk2 = mk<double>(0.0, 0.0);
-        double kv[3] = {0.0, 0.0, 0.0};
+        const PkMode *mp = modes + (e < nmodes ? e : 0);
         if (e < nmodes) {
-            const PkMode m = modes[e];
+            const PkMode &m = *mp;
             b = m.b;
-            kv[0] = m.kv[0];
-            kv[1] = m.kv[1];
-            kv[2] = m.kv[2];
             const zd d1 = f1.at(m.ix, m.iy, m.iz), d2 = f2.at(m.ix, m.iy, m.iz);
             if (k0_special && m.ix == 0 && m.iy == 0 && m.iz == 0) {
                 pk2 = mk<double>(k0_re, k0_im);
@@ -319,7 +324,7 @@ __global__ void k_pk_bin_list(F1 f1, F2 f2, const PkMode *modes, long long nmode
         const int nq = lms.n > 0 ? lms.n : 1;  // (the mode counts are added in pass q = 0)
         for (int q = 0; q < nq; q++) {
             zd v = mk<double>(0.0, 0.0);
-            if (q < lms.n && b.x >= 0) v = pk2 * ylm_reduced(lms.lm[q].l, lms.lm[q].m, kv[0], kv[1], kv[2]);
+            if (q < lms.n && b.x >= 0) v = pk2 * pk_mode_ylm(*mp, lms.lm[q].l, lms.lm[q].m);
             for (int side = 0; side < 2; side++) {
                 const int mine = side ? b.y : b.x;
                 unsigned rem = __ballot_sync(0xffffffffu, mine >= 0);

@@ -1831,7 +1831,8 @@ struct Engine : public hg_ctx {
         HG_CK(cudaFuncSetAttribute(k_xi_orbit_hist<T, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const C *twp = twiddles(L);
         kb("xi_orbit_hist", double(g.ntot / 2) * sizeof(C));
-        k_xi_orbit_hist<T, L><<<(n_orb + 1) / 2, OrbitCfg<T, L>::NT, smem, st>>>(
+        const int nblk = (n_orb + 1) / 2;
+        k_xi_orbit_hist<T, L><<<nblk, OrbitCfg<T, L>::NT, smem, st>>>(
             dp<C>(xi), dp<int2>(d_orbit_lines), dp<int>(d_orbit_n2xy), n_orb, twp, hs, n2dim, hist);
         ke();
     }
