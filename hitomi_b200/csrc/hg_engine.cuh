@@ -157,6 +157,12 @@ struct Fam {
 
 namespace {
 
+// p[0] = (re, im): a field's k = 0 value set on the stream, without a host copy and wait
+template <typename T>
+__global__ void k_set_k0(cplx<T> *p, T re, T im) {
+    p[0] = mk<T>(re, im);
+}
+
 // element-wise precision change of a complex array (the density spectrum between the
 // FP32 engine and its FP64 stages)
 template <typename S, typename D>
@@ -1050,11 +1056,9 @@ struct Engine : public hg_ctx {
         // k = 0 from the FP64 integral: sum_c (rho_c - nbar) dV
         delta0 = (dens_mass - nbar * double(g.ntot)) * dV;
         N0 = dens_mass * dV;
-        C z0;
-        z0.x = (T)delta0;
-        z0.y = (T)0;
-        HG_CK(cudaMemcpyAsync(H.p, &z0, sizeof(C), cudaMemcpyHostToDevice, st));
-        HG_CK(cudaStreamSynchronize(st));
+        kb("set_k0", double(sizeof(C)));
+        k_set_k0<T><<<1, 1, 0, st>>>(dp<C>(H), (T)delta0, (T)0);
+        ke();
         dens_valid = true;
     }
 
@@ -3101,11 +3105,9 @@ struct Engine : public hg_ctx {
             interlace_combine(dp<C>(*pb), dp<C>(sfield_tmp), real);
             k0 = {0.5 * (k0[0] + k1[0]), 0.5 * (k0[1] + k1[1])};
         }
-        C z0;
-        z0.x = (T)k0[0];
-        z0.y = (T)k0[1];
-        HG_CK(cudaMemcpyAsync(pb->p, &z0, sizeof(C), cudaMemcpyHostToDevice, st));
-        HG_CK(cudaStreamSynchronize(st));
+        kb("set_k0", double(sizeof(C)));
+        k_set_k0<T><<<1, 1, 0, st>>>(dp<C>(*pb), (T)k0[0], (T)k0[1]);
+        ke();
         sfk0[key] = k0;
         sf_ok.insert(key);
         return SpecK{Spec<T>{dp<C>(*pb), g.n[0], g.n[1], g.n[2], real ? 1 : 0}, k0[0], k0[1]};
