@@ -73,6 +73,42 @@ struct StRowsCompact {  // output [o][K][inner], keep compact rows only
     }
 };
 
+// Column pruning of the forward passes F2 and F3: the pair sums read Qhat only at shell
+// modes, so a z line (cx, cy) that no shell mode has is not transformed by F3, and F2 stores
+// per cx only the range of cy that holds such columns.
+template <typename T>
+struct StRowsCompactD {  // StRowsCompact that keeps, per cx, the rows cy in [cyr.x, cyr.y] only
+    cplx<T> *p;
+    int K, M, s;
+    long long inner;
+    int kx;             // lines (j, cx) per shell: o = j kx + cx
+    const int2 *cyr;    // [kx]: the smallest and largest cy of the needed columns (cx, cy)
+    __device__ __forceinline__ void operator()(long long o, int l, long long i, cplx<T> v) const {
+        const int c = pos_to_c(l, M, s);
+        const int2 r = cyr[(int)o % kx];  // the same for the whole line
+        if (c >= r.x && c <= r.y) p[(o * K + c) * inner + i] = v;
+    }
+};
+template <typename T>
+struct LdArrL {  // [o][L][inner] at line lines[q]
+    const cplx<T> *p;
+    long long L, inner;
+    const int *lines;
+    __device__ __forceinline__ cplx<T> operator()(long long q, int l, long long i) const {
+        return p[((long long)lines[q] * L + l) * inner + i];
+    }
+};
+template <typename T>
+struct StCubeL {  // StCube at line lines[q]
+    cplx<T> *p;
+    int K, M, s;
+    const int *lines;
+    __device__ __forceinline__ void operator()(long long q, int l, long long i, cplx<T> v) const {
+        const int c = pos_to_c(l, M, s);
+        if (c >= 0) p[(long long)lines[q] * K + c] = v;
+    }
+};
+
 // Shell-extent pruning of B1 and B2.  Shell j's modes reach |n_a| <= e_j,a only (e_j grows
 // with k_j; the cube side K = 2s+1 is set by the largest shell), so B1 transforms only the
 // lines (j, cx, cy) with |cx - s_x| <= e_j,x and |cy - s_y| <= e_j,y, and B2 only the lines

@@ -253,6 +253,11 @@ struct Engine : public hg_ctx {
         DBuf d_ext4, d_extx;        // int4 per shell (e_x, e_y, e_z, 0); e_x per shell
         DBuf d_lines1, d_lines2;
         long long nl1 = 0, nl2 = 0;
+        // forward-pass column pruning: per cx the range of cy of the columns (cx, cy) that some
+        // shell mode has (F2 rows), and the F3 lines (j, cx, cy) of those columns
+        DBuf d_cyr, d_lines3;
+        long long nl3 = 0;
+        double disc_frac = 1.0;
     } shells;
     // The catalogue the bispectrum and 3PCF read: the box density (kind 0) or the survey's
     // D - alpha R field (kind 1).  G fields are keyed by GK = (L, M): the Yhat_LM-weighted
@@ -1375,6 +1380,31 @@ struct Engine : public hg_ctx {
             if (!l1.empty()) HG_CK(cudaMemcpy(S.d_lines1.p, l1.data(), sizeof(int) * l1.size(), cudaMemcpyHostToDevice));
             HG_CK(S.d_lines2.ensure(sizeof(int) * std::max<size_t>(l2.size(), 1)));
             if (!l2.empty()) HG_CK(cudaMemcpy(S.d_lines2.p, l2.data(), sizeof(int) * l2.size(), cudaMemcpyHostToDevice));
+            std::vector<unsigned char> disc((size_t)S.K[0] * S.K[1], 0);
+            for (const ShellEnt &q : S.ent) {  // Qhat is read at -k of the shell modes k: both signs
+                disc[(size_t)(q.nx + S.s[0]) * S.K[1] + (q.ny + S.s[1])] = 1;
+                disc[(size_t)(S.s[0] - q.nx) * S.K[1] + (S.s[1] - q.ny)] = 1;
+            }
+            std::vector<int> l3;
+            for (int i = 0; i < S.ns; i++)
+                for (int c = 0; c < S.K[0] * S.K[1]; c++)
+                    if (disc[c]) l3.push_back(i * S.K[0] * S.K[1] + c);
+            S.nl3 = (long long)l3.size();
+            std::vector<int2> cyr(S.K[0], make_int2(1, 0));  // empty ranges by default
+            long long nr = 0;
+            for (int cx = 0; cx < S.K[0]; cx++) {
+                for (int cy = 0; cy < S.K[1]; cy++)
+                    if (disc[(size_t)cx * S.K[1] + cy]) {
+                        if (cyr[cx].x > cyr[cx].y) cyr[cx] = make_int2(cy, cy);
+                        cyr[cx].y = cy;
+                    }
+                if (cyr[cx].y >= cyr[cx].x) nr += cyr[cx].y - cyr[cx].x + 1;
+            }
+            S.disc_frac = disc.empty() ? 1.0 : double(nr) / double(disc.size());
+            HG_CK(S.d_cyr.ensure(sizeof(int2) * S.K[0]));
+            HG_CK(cudaMemcpy(S.d_cyr.p, cyr.data(), sizeof(int2) * S.K[0], cudaMemcpyHostToDevice));
+            HG_CK(S.d_lines3.ensure(sizeof(int) * std::max<size_t>(l3.size(), 1)));
+            if (!l3.empty()) HG_CK(cudaMemcpy(S.d_lines3.p, l3.data(), sizeof(int) * l3.size(), cudaMemcpyHostToDevice));
         }
         std::vector<double> inv(S.ns);
         for (int i = 0; i < S.ns; i++) inv[i] = S.nmode[i] ? 1.0 / double(S.nmode[i]) : 0.0;
@@ -1468,7 +1498,6 @@ struct Engine : public hg_ctx {
         const int Kx = S.K[0], Ky = S.K[1], Kz = S.K[2];
         const int Mx = S.M[0], My = S.M[1], Mz = S.M[2];
         ensure_chain_tmp((long long)ns * Kx * Ky * Mz, (long long)ns * Kx * My * Mz);
-        const long long o1 = (long long)ns * Kx * Ky;
         const long long o2 = (long long)ns * Kx;
         // inverse z and y passes over the lines inside each shell's extents only
         const ShellSet &SH = shells;
@@ -1488,10 +1517,12 @@ struct Engine : public hg_ctx {
         kb("chain_x_fused", (in_rows_x + double(ns) * Kx) * My * Mz * sizeof(C) + double(Mx) * My * Mz * sizeof(C));
         HG_CK(launch_chain_x_any(Mx, var, dp<C>(T2), Gp, ns, Kx, S.s[0], plane, extx));
         ke();
-        pass<-1>(My, LdArr<T>{dp<C>(T2), My, Mz}, StRowsCompact<T>{dp<C>(T1), Ky, My, S.s[1], Mz}, o2, Mz, "chain_y",
-                 double(o2) * (Ky + My) * Mz * sizeof(C));
-        pass<-1>(Mz, LdArr<T>{dp<C>(T1), Mz, 1}, StCube<T>{Q, Kz, Mz, S.s[2]}, o1, 1, "chain_z",
-                 double(o1) * (Kz + Mz) * sizeof(C));
+        // forward passes over the columns some shell mode has (the pair sums read nothing else)
+        pass<-1>(My, LdArr<T>{dp<C>(T2), My, Mz},
+                 StRowsCompactD<T>{dp<C>(T1), Ky, My, S.s[1], Mz, Kx, dp<int2>(SH.d_cyr)}, o2, Mz, "chain_y",
+                 double(o2) * (SH.disc_frac * Ky + My) * Mz * sizeof(C));
+        pass<-1>(Mz, LdArrL<T>{dp<C>(T1), Mz, 1, dp<int>(SH.d_lines3)}, StCubeL<T>{Q, Kz, Mz, S.s[2], dp<int>(SH.d_lines3)},
+                 SH.nl3, 1, "chain_z", double(SH.nl3) * (Kz + Mz) * sizeof(C));
     }
 
     cudaError_t launch_chain_x_any(int Mx, int var, C *t2, const C *Gp, int ns, int Kx, int s0, long long plane,
