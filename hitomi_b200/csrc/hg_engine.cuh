@@ -45,6 +45,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -1553,6 +1554,14 @@ struct Engine : public hg_ctx {
         if (Mx != 32 && Mx != 64 && Mx != 128 && Mx != 192 && Mx != 256) return 0;
         auto it = chain_tuned.find(Mx);
         if (it != chain_tuned.end()) return it->second.variant;
+        // HG_CHAIN_VARIANT=v: use variant v untimed (the tests run every variant this way)
+        if (const char *fv = std::getenv("HG_CHAIN_VARIANT")) {
+            const int v = std::atoi(fv);
+            HG_REQUIRE(v >= 0 && v < kNumChainVariants && chain_variant_exists(Mx, v),
+                       "HG_CHAIN_VARIANT names no chain variant for this transform length");
+            chain_tuned[Mx] = Tuned{v, std::vector<float>(kNumChainVariants, 0.f)};
+            return v;
+        }
         const size_t per_shell = sizeof(C) * (size_t)Kx * plane;
         const int nsh = (int)std::max<size_t>(1, std::min<size_t>((size_t)ns, (2ull << 30) / per_shell));
         const size_t bytes = per_shell * nsh;
@@ -1594,7 +1603,9 @@ struct Engine : public hg_ctx {
             const ChainVariant &cv = kChainVariants[kv.second.variant];
             snprintf(line, sizeof(line), "chain_x L=%d %s: variant %d (%s, B=%d, G %s, %s, %s)", kv.first,
                      sizeof(T) == 8 ? "fp64" : "fp32", kv.second.variant,
-                     cv.v12 ? "12 values per thread" : "two-level register transform", cv.B,
+                     cv.v12 ? "12 values per thread"
+                            : (cv.xr ? "two-level register transform, exchange in rounds" : "two-level register transform"),
+                     cv.B,
                      cv.gs ? "staged in shared memory" : "read from L2", cv.pf ? "cp.async prefetch" : "no prefetch",
                      cv.minb ? ("register cap for " + std::to_string(cv.minb) + " CTAs per SM").c_str()
                              : "default register budget");

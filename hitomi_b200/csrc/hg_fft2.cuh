@@ -247,6 +247,29 @@ __device__ __forceinline__ void line_fft2(cplx<T> *v, cplx<T> *S, int t, int b, 
     for (int d = 0; d < R1 / R2; d++) dft_reg<T, R2, DIR>(&v[d * R2]);
 }
 
+// line_fft2 (column layout) with the exchange in R1/R2 rounds through a buffer of R2 R2 B
+// elements (a third of L B at 192 = 24 x 8): round d moves the k1 in [d R2, (d+1) R2), which
+// are exactly the ones that round's step B reads (k1 = t + d R2).  Same values, same order
+// of operations, a smaller buffer for four more barriers.
+template <typename T, int L, int DIR, int B>
+__device__ __forceinline__ void line_fft2_q(cplx<T> *v, cplx<T> *S, int t, int b, const cplx<T> *__restrict__ tw) {
+    constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    dft_reg<T, R1, DIR>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < R1; k1++) v[k1] = mul_tw<T, DIR>(v[k1], tw[t * k1]);  // t k1 < R1 R2 = L
+#pragma unroll
+    for (int d = 0; d < R1 / R2; d++) {
+#pragma unroll
+        for (int q = 0; q < R2; q++) S[(q * R2 + t) * B + b] = v[d * R2 + q];
+        __syncthreads();
+#pragma unroll
+        for (int n2 = 0; n2 < R2; n2++) v[d * R2 + n2] = S[(t * R2 + n2) * B + b];
+        __syncthreads();
+    }
+#pragma unroll
+    for (int d = 0; d < R1 / R2; d++) dft_reg<T, R2, DIR>(&v[d * R2]);
+}
+
 // Register slot r = d R2 + k2 holds position k1 + R1 k2 with k1 = t + d R2.
 template <int L>
 __device__ __forceinline__ int pos_of_reg(int t, int r) {
@@ -608,29 +631,32 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
 // 0 keeps the default, 2 CTAs for FP32 and 1 for FP64).  The FP64 transform holds 24 complex
 // values per thread and is latency-bound at the two CTAs of 128 threads its 255 registers
 // allow; the capped variants trade spills for more warps in flight.
-// v12: the 192-point kernel with 12 values per thread (k_chain_x_192).
+// v12: the 192-point kernel with 12 values per thread (k_chain_x_192); xr: the exchange in
+// rounds (line_fft2_q), which lets a fourth staged FP64 CTA fit on an SM.
 struct ChainVariant {
     int B;
     bool gs, pf;
     int minb;
     bool v12;
+    bool xr;  // the exchange in rounds (line_fft2_q): a third of the exchange buffer at 192
 };
 constexpr ChainVariant kChainVariants[] = {
     {16, true, true, 0, false},  {16, false, true, 0, false},  {16, false, false, 0, false},
     {8, true, true, 0, false},   {8, false, false, 0, false},  {16, false, false, 3, false},
     {16, false, false, 4, false}, {8, false, false, 8, false}, {8, false, false, 4, true},
     {16, false, false, 2, true},  {8, true, false, 4, true},   {8, false, false, 3, true},
-    {8, false, true, 0, false}};
-constexpr int kNumChainVariants = 13;
+    {8, false, true, 0, false},   {8, true, true, 0, false, true}};
+constexpr int kNumChainVariants = 14;
 
-template <typename T, int L, int B, bool GS, bool PF>
+template <typename T, int L, int B, bool GS, bool PF, bool XR = false>
 struct ChainCfg {
     static constexpr int R2 = Split<L>::R2;
     static constexpr int NT = R2 * B;
-    // exchange buffer, G tile (GS), the next shell's K kept rows (PF), the L twiddles
+    // exchange buffer (XR: one round's R2 R2 B), G tile (GS), the next shell's K kept rows
+    // (PF), the L twiddles
+    static constexpr int XE = XR ? R2 * R2 * B : XchgLayout<L, true, B>::ELEMS;
     static size_t smem(int K) {
-        return sizeof(cplx<T>) * ((size_t)XchgLayout<L, true, B>::ELEMS + (GS ? (size_t)L * B : 0) +
-                                  (PF ? (size_t)K * B : 0) + (size_t)L);
+        return sizeof(cplx<T>) * ((size_t)XE + (GS ? (size_t)L * B : 0) + (PF ? (size_t)K * B : 0) + (size_t)L);
     }
 };
 
@@ -641,16 +667,16 @@ struct ChainCfg {
 // table is staged in shared memory once per CTA (the transforms read it on every shell; from
 // shared memory those reads wait less than L1 hits do), and the prefetch buffer holds only
 // the K kept rows, so that three FP64 CTAs of the staged variants fit on an SM.
-template <typename T, int L, int B, bool GS, bool PF, int MINB>
-__global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : ((sizeof(T) == 4) ? 2 : 1))
+template <typename T, int L, int B, bool GS, bool PF, int MINB, bool XR = false>
+__global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF, XR>::NT, MINB ? MINB : ((sizeof(T) == 4) ? 2 : 1))
     k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
                   const cplx<T> *__restrict__ tw, const int *__restrict__ ext) {
-    using CF = ChainCfg<T, L, B, GS, PF>;
+    using CF = ChainCfg<T, L, B, GS, PF, XR>;
     using X = XchgLayout<L, true, B>;
     constexpr int R1 = X::R1, R2 = X::R2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cplx<T> *S = reinterpret_cast<cplx<T> *>(smem_raw);
-    cplx<T> *Gs = S + X::ELEMS;              // [x][b] (GS)
+    cplx<T> *Gs = S + CF::XE;                // [x][b] (GS)
     cplx<T> *Pb = Gs + (GS ? L * B : 0);     // next shell's K kept rows, [c][b] (PF)
     cplx<T> *Tw = Pb + (PF ? K * B : 0);     // twiddles [L]
     const int t = threadIdx.x / B, b = threadIdx.x % B;
@@ -712,7 +738,8 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
                 v[n1] = (ok && n >= -ej && n <= ej) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
             }
         }
-        line_fft2<T, L, +1, true, B>(v, S, t, b, Tw);
+        if constexpr (XR) line_fft2_q<T, L, +1, B>(v, S, t, b, Tw);
+        else line_fft2<T, L, +1, true, B>(v, S, t, b, Tw);
         if constexpr (R1 == R2) {
 #pragma unroll
             for (int r = 0; r < R1; r++) v[r] = v[r] * g_at(pos_of_reg<L>(t, r));
@@ -726,7 +753,8 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF>::NT, MINB ? MINB : (
 #pragma unroll
             for (int n1 = 0; n1 < R1; n1++) v[n1] = u[n1];
         }
-        line_fft2<T, L, -1, true, B>(v, S, t, b, Tw);
+        if constexpr (XR) line_fft2_q<T, L, -1, B>(v, S, t, b, Tw);
+        else line_fft2<T, L, -1, true, B>(v, S, t, b, Tw);
         if (ok) {
 #pragma unroll
             for (int r = 0; r < R1; r++) {
@@ -891,16 +919,16 @@ inline cudaError_t launch_chain_x_192(cplx<T> *t2, const cplx<T> *G, int ns, int
     return cudaGetLastError();
 }
 
-template <typename T, int L, int B, bool GS, bool PF, int MINB = 0>
+template <typename T, int L, int B, bool GS, bool PF, int MINB = 0, bool XR = false>
 inline cudaError_t launch_chain_x_v(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
                                     const cplx<T> *tw, const int *ext, cudaStream_t st) {
-    using CF = ChainCfg<T, L, B, GS, PF>;
+    using CF = ChainCfg<T, L, B, GS, PF, XR>;
     const size_t smem = CF::smem(K);
-    cudaError_t e = cudaFuncSetAttribute(k_chain_x_reg<T, L, B, GS, PF, MINB>,
+    cudaError_t e = cudaFuncSetAttribute(k_chain_x_reg<T, L, B, GS, PF, MINB, XR>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const unsigned tiles = (unsigned)((plane + B - 1) / B);
-    k_chain_x_reg<T, L, B, GS, PF, MINB><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw, ext);
+    k_chain_x_reg<T, L, B, GS, PF, MINB, XR><<<tiles, CF::NT, smem, st>>>(t2, G, ns, K, s, plane, tw, ext);
     return cudaGetLastError();
 }
 
@@ -929,6 +957,7 @@ inline cudaError_t launch_chain_x_reg_L(int v, cplx<T> *t2, const cplx<T> *G, in
             if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 3>(t2, G, ns, K, s, plane, tw, ext, st);
             return cudaErrorInvalidValue;
         case 12: return launch_chain_x_v<T, L, 8, false, true>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 13: return launch_chain_x_v<T, L, 8, true, true, 0, true>(t2, G, ns, K, s, plane, tw, ext, st);
         default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, ext, st);
     }
 }

@@ -336,8 +336,9 @@ int hg_set_memory_limit(hg_ctx *ctx, long long bytes);
 long long hg_memory_in_use(const hg_ctx *ctx);
 
 /* The launch shapes the context's autotuner picked (one line per tuned kernel and grid: the
- * chosen variant and the measured time of every variant).  No counterpart in the
- * reference. */
+ * chosen variant and the measured time of every variant).  With HG_CHAIN_VARIANT=v in the
+ * environment a context uses chain variant v untimed (every variant gives the same result;
+ * an unknown v fails the bispectrum call).  No counterpart in the reference. */
 int hg_tuning(hg_ctx *ctx, char *buf, long long buflen);
 
 /* Allocation-free periodic-box power-spectrum multipole.  No counterpart in the reference:
