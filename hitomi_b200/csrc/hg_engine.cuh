@@ -1604,7 +1604,9 @@ struct Engine : public hg_ctx {
             snprintf(line, sizeof(line), "chain_x L=%d %s: variant %d (%s, B=%d, G %s, %s, %s)", kv.first,
                      sizeof(T) == 8 ? "fp64" : "fp32", kv.second.variant,
                      cv.v12 ? "12 values per thread"
-                            : (cv.xr ? "two-level register transform, exchange in rounds" : "two-level register transform"),
+                            : (cv.xr == 1   ? "two-level register transform, exchange in rounds"
+                               : cv.xr == 2 ? "two-level register transform, exchange in half rounds"
+                                            : "two-level register transform"),
                      cv.B,
                      cv.gs ? "staged in shared memory" : "read from L2", cv.pf ? "cp.async prefetch" : "no prefetch",
                      cv.minb ? ("register cap for " + std::to_string(cv.minb) + " CTAs per SM").c_str()

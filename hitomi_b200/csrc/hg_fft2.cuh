@@ -247,24 +247,48 @@ __device__ __forceinline__ void line_fft2(cplx<T> *v, cplx<T> *S, int t, int b, 
     for (int d = 0; d < R1 / R2; d++) dft_reg<T, R2, DIR>(&v[d * R2]);
 }
 
-// line_fft2 (column layout) with the exchange in R1/R2 rounds through a buffer of R2 R2 B
-// elements (a third of L B at 192 = 24 x 8): round d moves the k1 in [d R2, (d+1) R2), which
-// are exactly the ones that round's step B reads (k1 = t + d R2).  Same values, same order
-// of operations, a smaller buffer for four more barriers.
-template <typename T, int L, int DIR, int B>
+// line_fft2 (column layout) with the exchange in rounds of RS values of k1 through a buffer
+// of RS R2 B elements (RS = R2: a third of L B at 192 = 24 x 8; RS = R2 / 2: a sixth).  The
+// k1 of step B's block d are [d R2, (d+1) R2), which thread t reads at k1 = t + d R2; a block
+// moves in R2 / RS rounds, each thread keeping what it reads in u until the block's last
+// round has written its values out.  Same values, same order of operations.
+template <typename T, int L, int DIR, int B, int RS>
 __device__ __forceinline__ void line_fft2_q(cplx<T> *v, cplx<T> *S, int t, int b, const cplx<T> *__restrict__ tw) {
     constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+    static_assert(R2 % RS == 0, "rounds of a whole number per block");
     dft_reg<T, R1, DIR>(v);
 #pragma unroll
     for (int k1 = 1; k1 < R1; k1++) v[k1] = mul_tw<T, DIR>(v[k1], tw[t * k1]);  // t k1 < R1 R2 = L
+    if constexpr (RS == R2) {  // one round per block: its reads land in registers already written out
+#pragma unroll
+        for (int d = 0; d < R1 / R2; d++) {
+#pragma unroll
+            for (int q = 0; q < R2; q++) S[(q * R2 + t) * B + b] = v[d * R2 + q];
+            __syncthreads();
+#pragma unroll
+            for (int n2 = 0; n2 < R2; n2++) v[d * R2 + n2] = S[(t * R2 + n2) * B + b];
+            __syncthreads();
+        }
+#pragma unroll
+        for (int d = 0; d < R1 / R2; d++) dft_reg<T, R2, DIR>(&v[d * R2]);
+        return;
+    }
 #pragma unroll
     for (int d = 0; d < R1 / R2; d++) {
+        cplx<T> u[R2];
 #pragma unroll
-        for (int q = 0; q < R2; q++) S[(q * R2 + t) * B + b] = v[d * R2 + q];
-        __syncthreads();
+        for (int h = 0; h < R2 / RS; h++) {
 #pragma unroll
-        for (int n2 = 0; n2 < R2; n2++) v[d * R2 + n2] = S[(t * R2 + n2) * B + b];
-        __syncthreads();
+            for (int q = 0; q < RS; q++) S[(q * R2 + t) * B + b] = v[d * R2 + h * RS + q];
+            __syncthreads();
+            if (t >= h * RS && t < (h + 1) * RS) {
+#pragma unroll
+                for (int n2 = 0; n2 < R2; n2++) u[n2] = S[((t - h * RS) * R2 + n2) * B + b];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int n2 = 0; n2 < R2; n2++) v[d * R2 + n2] = u[n2];
     }
 #pragma unroll
     for (int d = 0; d < R1 / R2; d++) dft_reg<T, R2, DIR>(&v[d * R2]);
@@ -632,29 +656,32 @@ inline cudaError_t launch_pass_any(int L, LD ld, ST st, PassGeom g, const cplx<T
 // values per thread and is latency-bound at the two CTAs of 128 threads its 255 registers
 // allow; the capped variants trade spills for more warps in flight.
 // v12: the 192-point kernel with 12 values per thread (k_chain_x_192); xr: the exchange in
-// rounds (line_fft2_q), which lets a fourth staged FP64 CTA fit on an SM.
+// rounds (line_fft2_q), which lets a fourth (xr 1) or, with registers capped for five CTAs,
+// a fifth (xr 2) staged FP64 CTA fit on an SM.
 struct ChainVariant {
     int B;
     bool gs, pf;
     int minb;
     bool v12;
-    bool xr;  // the exchange in rounds (line_fft2_q): a third of the exchange buffer at 192
+    int xr;  // the exchange in rounds (line_fft2_q): 1 a third of the exchange buffer at 192,
+             // 2 a sixth
 };
 constexpr ChainVariant kChainVariants[] = {
     {16, true, true, 0, false},  {16, false, true, 0, false},  {16, false, false, 0, false},
     {8, true, true, 0, false},   {8, false, false, 0, false},  {16, false, false, 3, false},
     {16, false, false, 4, false}, {8, false, false, 8, false}, {8, false, false, 4, true},
     {16, false, false, 2, true},  {8, true, false, 4, true},   {8, false, false, 3, true},
-    {8, false, true, 0, false},   {8, true, true, 0, false, true}};
-constexpr int kNumChainVariants = 14;
+    {8, false, true, 0, false},   {8, true, true, 0, false, 1}, {8, true, true, 5, false, 2}};
+constexpr int kNumChainVariants = 15;
 
-template <typename T, int L, int B, bool GS, bool PF, bool XR = false>
+template <typename T, int L, int B, bool GS, bool PF, int XR = 0>
 struct ChainCfg {
     static constexpr int R2 = Split<L>::R2;
     static constexpr int NT = R2 * B;
-    // exchange buffer (XR: one round's R2 R2 B), G tile (GS), the next shell's K kept rows
-    // (PF), the L twiddles
-    static constexpr int XE = XR ? R2 * R2 * B : XchgLayout<L, true, B>::ELEMS;
+    // exchange buffer (XR: one round's RS R2 B, RS = R2 / XR), G tile (GS), the next shell's
+    // K kept rows (PF), the L twiddles
+    static constexpr int RS = XR ? R2 / XR : R2;
+    static constexpr int XE = XR ? RS * R2 * B : XchgLayout<L, true, B>::ELEMS;
     static size_t smem(int K) {
         return sizeof(cplx<T>) * ((size_t)XE + (GS ? (size_t)L * B : 0) + (PF ? (size_t)K * B : 0) + (size_t)L);
     }
@@ -667,7 +694,7 @@ struct ChainCfg {
 // table is staged in shared memory once per CTA (the transforms read it on every shell; from
 // shared memory those reads wait less than L1 hits do), and the prefetch buffer holds only
 // the K kept rows, so that three FP64 CTAs of the staged variants fit on an SM.
-template <typename T, int L, int B, bool GS, bool PF, int MINB, bool XR = false>
+template <typename T, int L, int B, bool GS, bool PF, int MINB, int XR = 0>
 __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF, XR>::NT, MINB ? MINB : ((sizeof(T) == 4) ? 2 : 1))
     k_chain_x_reg(cplx<T> *t2, const cplx<T> *__restrict__ G, int ns, int K, int s, long long plane,
                   const cplx<T> *__restrict__ tw, const int *__restrict__ ext) {
@@ -738,7 +765,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF, XR>::NT, MINB ? MINB
                 v[n1] = (ok && n >= -ej && n <= ej) ? tj[(long long)(n + s) * plane + i] : mk<T>(0, 0);
             }
         }
-        if constexpr (XR) line_fft2_q<T, L, +1, B>(v, S, t, b, Tw);
+        if constexpr (XR != 0) line_fft2_q<T, L, +1, B, CF::RS>(v, S, t, b, Tw);
         else line_fft2<T, L, +1, true, B>(v, S, t, b, Tw);
         if constexpr (R1 == R2) {
 #pragma unroll
@@ -753,7 +780,7 @@ __global__ void __launch_bounds__(ChainCfg<T, L, B, GS, PF, XR>::NT, MINB ? MINB
 #pragma unroll
             for (int n1 = 0; n1 < R1; n1++) v[n1] = u[n1];
         }
-        if constexpr (XR) line_fft2_q<T, L, -1, B>(v, S, t, b, Tw);
+        if constexpr (XR != 0) line_fft2_q<T, L, -1, B, CF::RS>(v, S, t, b, Tw);
         else line_fft2<T, L, -1, true, B>(v, S, t, b, Tw);
         if (ok) {
 #pragma unroll
@@ -919,7 +946,7 @@ inline cudaError_t launch_chain_x_192(cplx<T> *t2, const cplx<T> *G, int ns, int
     return cudaGetLastError();
 }
 
-template <typename T, int L, int B, bool GS, bool PF, int MINB = 0, bool XR = false>
+template <typename T, int L, int B, bool GS, bool PF, int MINB = 0, int XR = 0>
 inline cudaError_t launch_chain_x_v(cplx<T> *t2, const cplx<T> *G, int ns, int K, int s, long long plane,
                                     const cplx<T> *tw, const int *ext, cudaStream_t st) {
     using CF = ChainCfg<T, L, B, GS, PF, XR>;
@@ -957,7 +984,10 @@ inline cudaError_t launch_chain_x_reg_L(int v, cplx<T> *t2, const cplx<T> *G, in
             if constexpr (L == 192) return launch_chain_x_192<T, 8, false, 3>(t2, G, ns, K, s, plane, tw, ext, st);
             return cudaErrorInvalidValue;
         case 12: return launch_chain_x_v<T, L, 8, false, true>(t2, G, ns, K, s, plane, tw, ext, st);
-        case 13: return launch_chain_x_v<T, L, 8, true, true, 0, true>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 13: return launch_chain_x_v<T, L, 8, true, true, 0, 1>(t2, G, ns, K, s, plane, tw, ext, st);
+        case 14:
+            if constexpr (Split<L>::R2 % 2 == 0) return launch_chain_x_v<T, L, 8, true, true, 5, 2>(t2, G, ns, K, s, plane, tw, ext, st);
+            return cudaErrorInvalidValue;
         default: return launch_chain_x_v<T, L, 16, true, true>(t2, G, ns, K, s, plane, tw, ext, st);
     }
 }

@@ -1,7 +1,7 @@
 """Every launch shape of the fused chain x pass (kChainVariants, hg_fft2.cuh) gives the same
 bispectrum.  The autotuner keeps whichever variant is fastest on the first mock, so each one
 must be exact; HG_CHAIN_VARIANT forces one variant untimed.  256^3 mesh, shells to |n| = 35:
-the chains run on the 192^3 reduced grid, where all fourteen variants exist.  Reference
+the chains run on the 192^3 reduced grid, where all fifteen variants exist.  Reference
 values from the numpy restatement pinned to the reference; tolerances as the other parity
 tests."""
 import os
@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = {"fp64": 1e-10, "fp32": 1e-4}
 FLOOR = {"fp64": 1e-12, "fp32": 1e-3}
-N_VARIANTS = 14
+N_VARIANTS = 15
 
 
 @pytest.mark.parametrize("form", ["fp64", "fp32"])
