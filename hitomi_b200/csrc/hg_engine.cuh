@@ -130,12 +130,13 @@ inline unsigned grid1(long long n, int bs) { return (unsigned)((n + bs - 1) / bs
 // last one partly empty).  Queried once per kernel.
 template <class K>
 inline unsigned resident_grid(K kern, int bs) {
-    static int per_sm = 0;  // one static per kernel instantiation
-    if (per_sm == 0) {
+    // one per kernel instantiation, initialised once even when contexts on several host
+    // threads get here together (a function-local static)
+    static const int per_sm = [&] {
         int v = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, bs, 0) != cudaSuccess || v < 1) v = 1;
-        per_sm = v;
-    }
+        return v;
+    }();
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return (unsigned)(sms * per_sm);
