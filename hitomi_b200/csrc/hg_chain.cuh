@@ -110,11 +110,12 @@ struct StCubeL {  // StCube at line lines[q]
 };
 
 // Shell-extent pruning of B1 and B2.  Shell j's modes reach |n_a| <= e_j,a only (e_j grows
-// with k_j; the cube side K = 2s+1 is set by the largest shell), so B1 transforms only the
-// lines (j, cx, cy) with |cx - s_x| <= e_j,x and |cy - s_y| <= e_j,y, and B2 only the lines
-// (j, cx) with |cx - s_x| <= e_j,x: pass line q is line lines[q] of the full layout.  T1 and
-// T2 lines outside those sets are never written, and their readers (B2's rows, X's rows)
-// treat them as zero by the same extents.
+// with k_j; the cube side K = 2s+1 is set by the largest shell), so B2 transforms only the
+// lines (j, cx) with |cx - s_x| <= e_j,x, and B1 only the lines (j, cx, cy) whose cy lies in
+// the range of shell j's modes at that cx (a disc's row, narrower than |cy - s_y| <= e_j,y
+// away from cx = s_x): pass line q is line lines[q] of the full layout.  T1 and T2 lines
+// outside those sets are never written, and their readers (B2's rows, X's rows) treat them
+// as zero by the same ranges.
 template <typename T>
 struct LdCubeL {  // B1: compact cube line lines[q], kept modes |n_z| <= e_j,z
     const cplx<T> *p;
@@ -130,18 +131,18 @@ struct LdCubeL {  // B1: compact cube line lines[q], kept modes |n_z| <= e_j,z
     }
 };
 template <typename T>
-struct LdRowsCompactL {  // B2: [o][K][inner] at line lines[q], rows |n_y| <= e_j,y
+struct LdRowsCompactL {  // B2: [o][K][inner] at line lines[q], compact rows c in cyr[o]
     const cplx<T> *p;
     int K, M, s;
     long long inner;
     const int *lines;
-    const int4 *ext;
-    int kx;  // lines per shell
+    const int2 *cyr;  // per line (j, cx): the compact rows B1 wrote (shell j's modes' cy range)
     __device__ __forceinline__ cplx<T> operator()(long long q, int l, long long i) const {
         const int o = lines[q];
-        const int e = ext[o / kx].y;
+        const int2 r = cyr[o];
         const int n = (l < M / 2) ? l : l - M;
-        return (n >= -e && n <= e) ? p[((long long)o * K + n + s) * inner + i] : mk<T>(0, 0);
+        const int c = n + s;
+        return (c >= r.x && c <= r.y) ? p[((long long)o * K + c) * inner + i] : mk<T>(0, 0);
     }
 };
 template <typename T>

@@ -255,6 +255,7 @@ struct Engine : public hg_ctx {
         DBuf d_ext4, d_extx;        // int4 per shell (e_x, e_y, e_z, 0); e_x per shell
         DBuf d_lines1, d_lines2;
         long long nl1 = 0, nl2 = 0;
+        DBuf d_cyr1;  // [ns][Kx]: per (shell j, cx) the compact cy range of shell j's modes (B1 lines)
         // forward-pass column pruning: per cx the range of cy of the columns (cx, cy) that some
         // shell mode has (F2 rows), and the F3 lines (j, cx, cy) of those columns
         DBuf d_cyr, d_lines3;
@@ -1362,15 +1363,29 @@ struct Engine : public hg_ctx {
                 }
             std::vector<int4> e4(S.ns);
             std::vector<int> ex(S.ns), l1, l2;
+            // per (shell i, cx) the range of cy of shell i's modes: a z line (i, cx, cy) outside
+            // it holds no mode, so B1 skips it and B2 reads it as zero
+            std::vector<int2> cyr1((size_t)S.ns * S.K[0], make_int2(1, 0));
+            for (int i = 0; i < S.ns; i++)
+                for (int e = S.start[i]; e < S.start[i + 1]; e++) {
+                    const ShellEnt &q = S.ent[e];
+                    int2 &r = cyr1[(size_t)i * S.K[0] + q.nx + S.s[0]];
+                    const int cy = q.ny + S.s[1];
+                    if (r.x > r.y) r = make_int2(cy, cy);
+                    r.x = std::min(r.x, cy);
+                    r.y = std::max(r.y, cy);
+                }
             for (int i = 0; i < S.ns; i++) {
                 e4[i] = make_int4(S.ext[3 * i], S.ext[3 * i + 1], S.ext[3 * i + 2], 0);
                 ex[i] = S.ext[3 * i];
                 for (int cx = S.s[0] - ex[i]; cx <= S.s[0] + ex[i]; cx++) {
                     l2.push_back(i * S.K[0] + cx);
-                    for (int cy = S.s[1] - S.ext[3 * i + 1]; cy <= S.s[1] + S.ext[3 * i + 1]; cy++)
-                        l1.push_back((i * S.K[0] + cx) * S.K[1] + cy);
+                    const int2 r = cyr1[(size_t)i * S.K[0] + cx];
+                    for (int cy = r.x; cy <= r.y; cy++) l1.push_back((i * S.K[0] + cx) * S.K[1] + cy);
                 }
             }
+            HG_CK(S.d_cyr1.ensure(sizeof(int2) * cyr1.size()));
+            HG_CK(cudaMemcpy(S.d_cyr1.p, cyr1.data(), sizeof(int2) * cyr1.size(), cudaMemcpyHostToDevice));
             HG_REQUIRE((long long)S.ns * S.K[0] * S.K[1] < (1LL << 31), "too many chain lines");
             S.nl1 = (long long)l1.size();
             S.nl2 = (long long)l2.size();
@@ -1509,7 +1524,7 @@ struct Engine : public hg_ctx {
         for (int j = 0; j < ns; j++) in_rows_x += double(2 * SH.ext[3 * j] + 1);
         pass<+1>(Mz, LdCubeL<T>{dp<C>(Ac), Kz, Mz, S.s[2], lines1, ext4, Kx * Ky}, StArrL<T>{dp<C>(T1), Mz, 1, lines1},
                  SH.nl1, 1, "chain_z", double(SH.nl1) * (Kz + Mz) * sizeof(C));
-        pass<+1>(My, LdRowsCompactL<T>{dp<C>(T1), Ky, My, S.s[1], Mz, lines2, ext4, Kx},
+        pass<+1>(My, LdRowsCompactL<T>{dp<C>(T1), Ky, My, S.s[1], Mz, lines2, dp<int2>(SH.d_cyr1)},
                  StArrL<T>{dp<C>(T2), My, Mz, lines2}, SH.nl2, Mz, "chain_y",
                  double(SH.nl2) * (Ky + My) * Mz * sizeof(C));
         const C *Gp = dp<C>(Gsrc);

@@ -410,24 +410,25 @@ struct PipeArr {  // [o][L][inner] (LdArr)
     __device__ __forceinline__ const cplx<T> *row(Line b, int l) const { return b + (long long)l * inner; }
 };
 template <typename T>
-struct PipeRowsCompactL {  // LdRowsCompactL: rows |n| <= e_j,y of the compact line lines[q]
+struct PipeRowsCompactL {  // LdRowsCompactL: compact rows c in cyr[o] of the line o = lines[q]
     const cplx<T> *p;
     int K, M, s;
     long long inner;
     const int *lines;
-    const int4 *ext;
-    int kx;
+    const int2 *cyr;
     struct Line {
         const cplx<T> *b;
-        int e;
+        int lo, hi;
     };
     __device__ __forceinline__ Line line(long long q) const {
         const int o = lines[q];
-        return Line{p + (long long)o * K * inner, ext[o / kx].y};
+        const int2 r = cyr[o];
+        return Line{p + (long long)o * K * inner, r.x, r.y};
     }
     __device__ __forceinline__ const cplx<T> *row(const Line &ln, int l) const {
         const int n = (l < M / 2) ? l : l - M;
-        return (n >= -ln.e && n <= ln.e) ? ln.b + (long long)(n + s) * inner : nullptr;
+        const int c = n + s;
+        return (c >= ln.lo && c <= ln.hi) ? ln.b + (long long)c * inner : nullptr;
     }
 };
 
@@ -601,7 +602,7 @@ inline cudaError_t launch_fft2_L(LD ld, ST st, PassGeom g, const cplx<T> *tw, cu
     if constexpr (std::is_same<LD, LdRowsCompactL<T>>::value) {
         // the chain's pruned inverse y pass: compact rows, zero outside the shell's extent
         if (g.n_inner > 1 && ld.inner == g.n_inner && ld.M == L)
-            return launch_fft2_pipe<T, L, DIR>(PipeRowsCompactL<T>{ld.p, ld.K, ld.M, ld.s, ld.inner, ld.lines, ld.ext, ld.kx},
+            return launch_fft2_pipe<T, L, DIR>(PipeRowsCompactL<T>{ld.p, ld.K, ld.M, ld.s, ld.inner, ld.lines, ld.cyr},
                                                st, g, tw, stream);
     }
     if (g.n_inner == 1) {
