@@ -279,7 +279,8 @@ def cufft_reference(n_mesh, timing):
 
 
 def run_config(args) -> int:
-    """The other BASELINE configurations, measured end to end through the public API (the
+    """The other benchmark workloads (1: box P_l at 128^3, 2: box P_l at 512^3, 3: survey P_l,
+    5: batched P_l + zeta at 256^3), measured end to end through the public API (the
     catalogue copied from host memory every mock), both forms, FP32-vs-FP64 error per
     statistic; with --cpu also the reference's own code (oracle/_ref) timed on this host:
     directly where a mock takes seconds, else extrapolated from timed parts (stated)."""
@@ -515,7 +516,7 @@ def main():
                     help="profiling runs: device-resident steps only (no e2e, per-kernel or CPU legs)")
     ap.add_argument("--n-mesh", type=int, default=0, help="profiling size (not the headline workload)")
     ap.add_argument("--n-particles", type=float, default=0, help="profiling size (not the headline workload)")
-    ap.add_argument("--config", type=int, default=0, help="measure another BASELINE configuration (1, 2, 3, 5)")
+    ap.add_argument("--config", type=int, default=0, help="measure another workload: 1 box P_l 128^3, 2 box P_l 512^3, 3 survey P_l, 5 P_l + zeta batch")
     ap.add_argument("--n-mocks", type=int, default=8, help="mocks timed for --config 5")
     ap.add_argument("--cpu", action="store_true", help="with --config: also time the reference's CPU code")
     ap.add_argument("--stage-table", action="store_true",
